@@ -1,0 +1,291 @@
+#!/usr/bin/env python3
+"""Benchmark: dense dual-contouring extraction of the 1024^3 sharp-feature CSG grid.
+
+One step = one full extraction (mark + compaction, Hermite + averaging + QEF, quad
+emission in the CPU backend's order) of a 1024^3 float32 grid that is resident in HBM.
+Metric: Mcells/s = (nx-1)(ny-1)(nz-1) / step time, summed over ranks (each rank extracts
+its own grid: weak scaling, no collective on the data path).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--res 1024] [--impl reference]
+
+Under torchrun each rank runs on its LOCAL_RANK GPU; rank 0 prints one JSON line.
+``--impl reference`` times the CPU oracle (the FP64 restatement of the reference's
+CpuDualContouringBackend, which is single-threaded C++ in the reference and cannot be
+built here: it needs Eigen and libigl) with every host thread on a bounded z-slab of the
+same grid, and reports the same metric.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "phanty-sdf-cuda_b200"))
+
+# Launches of the engine's own kernels per extraction: mark, 3 scan passes, rank expansion,
+# edge normals, QEF, Jacobi list, FP64 vertices, 3 column-scan passes, face scatter,
+# FP64 vertices for windings, FP64 windings, face order.
+KERNELS_PER_STEP = 16
+# DRAM traffic of k_mark_compact per grid point, from the ncu capture summarised in
+# profiles/k_mark_compact_csg256.txt (dram__bytes_read.sum + dram__bytes_write.sum divided
+# by the grid points of that capture; scales with the number of points). None = not measured.
+MARK_TRAFFIC_BYTES_PER_POINT = None
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    sm.append(float(f[1]))
+                    mx = float(f[2])
+                except ValueError:
+                    continue
+                for n, v in zip(names, f[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(n)
+            os.unlink(self.path)
+        except Exception:
+            pass
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_grid(res, device):
+    from contouring_b200 import synth
+    return synth.csg(res, seed=0, device=device)
+
+
+def cpu_sample(values_cpu, dims, spacing, origin, zslab, threads):
+    """Time the CPU oracle on the bottom z-slab (zslab point planes) of the grid."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    nx, ny, nz = dims
+    kz = min(nz, zslab)
+    sub = values_cpu[: nx * ny * kz]
+    t0 = time.perf_counter()
+    r = O.dc_extract(sub, (nx, ny, kz), spacing, origin, threads=threads)
+    dt = time.perf_counter() - t0
+    cells = (nx - 1) * (ny - 1) * (kz - 1)
+    return cells / dt / 1e6, dt, cells, r["stats"]
+
+
+def run_reference(args, rank, world):
+    """CPU reference arm: the oracle port with all host threads, bounded slab per step."""
+    import numpy as np
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    vals, dims, spacing, origin = make_grid(args.res, "cpu")
+    v = vals.numpy()
+    zslab = args.ref_zslab
+    for _ in range(args.warmup):
+        cpu_sample(v, dims, spacing, origin, zslab, threads)
+    rates, secs = [], []
+    for _ in range(args.steps):
+        rate, dt, cells, _ = cpu_sample(v, dims, spacing, origin, zslab, threads)
+        rates.append(rate)
+        secs.append(dt)
+    value = float(np.median(rates))
+    sample = "z-slab of %dx%dx%d points (%d cells) of the %d^3 CSG grid per step" % (
+        dims[0], dims[1], zslab, cells, args.res)
+    line = {
+        "metric": "dc_extract_mcells_per_s", "value": round(value, 3), "unit": "Mcells/s",
+        "impl": "reference", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(1000 * float(np.median(secs)), 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "csg%d_dense_dc" % args.res, "grid": list(dims), "sample": sample},
+        "cpu_baseline": {"value": round(value, 3), "unit": "Mcells/s", "cores": threads,
+                         "kind": "port", "sample": sample},
+        "e2e": {"value": round(value, 3), "unit": "Mcells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--res", type=int, default=1024)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--ref-zslab", type=int, default=96, help="point planes per CPU sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import numpy as np
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from contouring_b200 import B200DualContouringBackend, DenseSdfGrid, DenseSdfGridDevice
+
+    dev = torch.device("cuda", local)
+    vals, dims, spacing, origin = make_grid(args.res, dev)
+    torch.cuda.synchronize()
+    be = B200DualContouringBackend(local)
+    stream = torch.cuda.current_stream()
+    gdev = DenseSdfGridDevice(*dims, *spacing, *origin, d_values=vals)
+    ncell = (dims[0] - 1) * (dims[1] - 1) * (dims[2] - 1)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        _, _, st = be.extract_tensor_ptr(gdev)
+    torch.cuda.synchronize()
+    barrier()
+    mark_ms, stats = [], None
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        barrier()
+        e0.record(stream)
+        for _ in range(args.steps):
+            _, _, stats = be.extract_tensor_ptr(gdev)
+            mark_ms.append(stats.marking_ms)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    ms_total = e0.elapsed_time(e1)
+    if dist is not None:
+        t = torch.tensor([ms_total], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_total = float(t.item())
+    ms_step = ms_total / args.steps
+    value = world * ncell / (ms_step / 1e3) / 1e6
+
+    # End to end through the public API: pinned host grid in, host mesh out, every step.
+    host = torch.empty(vals.numel(), dtype=torch.float32, pin_memory=True)
+    host.copy_(vals.cpu())
+    hgrid = DenseSdfGrid(*dims, *spacing, *origin, values=host.numpy())
+    mesh, _ = be.extract(hgrid)
+    torch.cuda.synchronize()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        mesh, est = be.extract(hgrid)
+    torch.cuda.synchronize()
+    e2e_s = (time.perf_counter() - t0) / max(1, args.e2e_steps)
+    if dist is not None:
+        t = torch.tensor([e2e_s], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = world * ncell / e2e_s / 1e6 if args.e2e_steps > 0 else None
+    h2d = 4 * vals.numel()
+    d2h = int(mesh.vertices.nbytes + mesh.faces.nbytes)
+
+    peak, peak_kind = _peaks()
+    npts = dims[0] * dims[1] * dims[2]
+    mark_avg_ms = float(np.mean(mark_ms))
+    mark_bytes = 4.0 * npts                       # algorithmic: every grid value read once
+    achieved = mark_bytes / (mark_avg_ms / 1e3) / 1e9
+    nv, nf = stats.vertex_count, stats.face_count
+    pipe_bytes = 4.0 * npts + 12.0 * nv + 16.0 * nf
+    pipe_gbs = pipe_bytes / (ms_step / 1e3) / 1e9
+    traffic = (MARK_TRAFFIC_BYTES_PER_POINT * npts) if MARK_TRAFFIC_BYTES_PER_POINT else None
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        rate, dt, cells, _ = cpu_sample(vals.cpu().numpy(), dims, spacing, origin, args.ref_zslab, threads)
+        cpu = {"value": round(rate, 3), "unit": "Mcells/s", "cores": threads, "kind": "port",
+               "sample": "z-slab %dx%dx%d points (%d cells) of the same grid, %.1f s" % (
+                   dims[0], dims[1], args.ref_zslab, cells, dt)}
+
+    if rank == 0:
+        line = {
+            "metric": "dc_extract_mcells_per_s", "value": round(value, 2), "unit": "Mcells/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_step, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": "csg%d_dense_dc" % args.res, "grid": list(dims),
+                       "cells": ncell, "vertices": nv, "quads": nf,
+                       "l2": "input (%.2f GB) larger than L2; no flush needed" % (4 * npts / 1e9),
+                       "parallelism": "replicas: one independent grid per rank"},
+            "roofline": {"bound": "hbm", "kernel": "k_mark_compact", "achieved": round(achieved, 1),
+                         "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                         "traffic": traffic, "peak_source": peak_kind,
+                         "algorithmic_bytes": mark_bytes, "avg_launch_ms": round(mark_avg_ms, 4)},
+            "pipeline_roofline": {"algorithmic_bytes": pipe_bytes, "achieved": round(pipe_gbs, 1),
+                                  "frac": round(pipe_gbs / peak, 4), "unit": "GB/s"},
+            "stage_ms": {"mark": round(stats.marking_ms, 4), "qef": round(stats.qef_ms, 4),
+                         "faces": round(stats.face_emission_ms, 4)},
+            "escalated_fp64_cells": stats.escalated_fp64_cells, "winding_fp64_faces": stats.winding_fp64_faces,
+            "e2e": {"value": round(e2e_value, 2) if e2e_value else None, "unit": "Mcells/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "ms_per_step": round(e2e_s * 1e3, 2)},
+            "gpu_launches": KERNELS_PER_STEP * args.steps,
+            "clocks": clk.summary(),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    be.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,158 @@
+/*
+ * dcb.h — C ABI of the B200 dual-contouring engine (libdcb.so).
+ *
+ * Plain pointers and sizes only; no C++ or torch types cross this boundary. A C++ class
+ * implementing the reference's IDualContouringBackend (include/dc_backend.h:80-84), the
+ * pybind / ctypes bindings and the CLI backend switch are thin layers over these calls.
+ *
+ * Conventions
+ *   - Every entry point returns an int status: DCB_OK (0) or a negative DCB_ERR_* code.
+ *     Nothing here calls exit() or traps the GPU (the reference exits the process on any
+ *     CUDA error: src/cuda/dc_cuda.cu:14-20).
+ *   - Grids are dense float32, x fastest: value(i,j,k) = values[i + nx*(j + ny*k)]
+ *     (include/dc_backend.h:13-21; src/cpp/dc_backend.cpp:61).
+ *   - Work is issued on the caller's stream; a handle owns its workspace and output
+ *     buffers and must not be used from two host threads at once.
+ */
+#ifndef DCB_H_
+#define DCB_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DCB_ABI_VERSION 1
+
+enum dcb_status {
+    DCB_OK = 0,
+    DCB_ERR_INVALID_ARGUMENT = -1,  /* null pointer, dims < 2, non-finite spacing, ... */
+    DCB_ERR_TOO_LARGE = -2,         /* grid or mesh exceeds the index limits below     */
+    DCB_ERR_CUDA = -3,              /* a CUDA runtime call failed (see dcb_last_error) */
+    DCB_ERR_OUT_OF_MEMORY = -4,     /* device or pinned-host allocation failed          */
+    DCB_ERR_TIMEOUT = -5,           /* a bounded device-side wait gave up               */
+    DCB_ERR_NOT_SUPPORTED = -6,     /* option combination not implemented               */
+    DCB_ERR_INTERNAL = -7           /* device-side consistency check failed             */
+};
+
+/* Limits: each grid axis <= 2^21 points and <= 65536 points along x; fewer than 2^31
+ * vertices and faces (faces are int32 indices, as in DualContouringMesh::faces). */
+
+/* Mirrors DenseSdfGrid (include/dc_backend.h:13-21) and DenseSdfGridDevice
+ * (include/dc_cuda.h:24-29). `values` is a host pointer for dcb_extract_host and a
+ * device pointer for dcb_extract_device (borrowed, never freed: dc_cuda.cu:679). */
+typedef struct {
+    int nx, ny, nz;
+    float vx, vy, vz;
+    float ox, oy, oz;
+    const float* values;
+} dcb_grid;
+
+enum dcb_method {
+    DCB_METHOD_DUAL_CONTOURING = 1,   /* ContouringMethod::DualContouring (contouring.h:21-25) */
+    DCB_METHOD_OURS = 2               /* outer/inner vertex refinement (contouring.cpp:1255-1328) */
+};
+
+/* Mirrors ContouringOptions (include/contouring.h:27-41) plus the B200 precision knobs. */
+typedef struct {
+    int method;                   /* dcb_method; the reference CPU backend forces DC      */
+    int outer_iters;              /* default 100 */
+    int inner_iters;              /* default 100 */
+    double mu;                    /* default 0.1 */
+    double dc_weight;             /* default 0.02 */
+    double sphere_weight;         /* default 1.0 */
+    double svd_threshold;         /* default 0.01: singular values <= this are truncated */
+    double fp64_escalation_cond;  /* FP32 solve escalates to FP64 when the condition
+                                     estimate of the retained spectrum exceeds this      */
+    double fp64_threshold_band;   /* ... or an eigenvalue lies within this relative band
+                                     of svd_threshold (rank decision ambiguous in FP32)  */
+    int emit_triangles;           /* 0: quads (DualContouringMesh), 1: triangulate_v1     */
+    int force_fp64;               /* 1: every cell takes the FP64 path (testing)          */
+} dcb_opts;
+
+/* Fill `o` with the reference defaults (contouring.h:27-41) and the B200 knobs. */
+void dcb_default_opts(dcb_opts* o);
+
+/* Field-compatible subset of DualContouringStats (include/dc_backend.h:44-78) plus the
+ * counters this engine adds. Times are device-side (CUDA events) in milliseconds. */
+typedef struct {
+    int nx, ny, nz;
+    int64_t total_cells;
+    int64_t active_cells;
+    int64_t vertex_count;
+    int64_t face_count;
+    float upload_ms;
+    float marking_ms;        /* fused mark + compaction kernel */
+    float compaction_ms;     /* 0: fused into marking */
+    float qef_ms;            /* Hermite + averaging + QEF (FP32 and FP64 passes) */
+    float face_emission_ms;  /* column scan + face scatter + ordering */
+    float download_ms;
+    float total_ms;
+    int64_t qef_fallback_count;     /* cells solved on the FP64 path */
+    int64_t clamp_count;            /* always 0: the CPU semantics never clamp */
+    int64_t escalated_fp64_cells;   /* == qef_fallback_count */
+    int64_t winding_fp64_faces;     /* faces whose orientation was re-decided in FP64 */
+    int64_t rank_hist[4];           /* retained-rank histogram of the QEF solves */
+} dcb_stats;
+
+/* Device-resident mesh; pointers are owned by the handle and stay valid until the next
+ * extract call on that handle or dcb_destroy. */
+typedef struct {
+    int64_t vertex_count;
+    int64_t face_count;
+    int verts_per_face;      /* 4 for quads, 3 for triangles */
+    float* vertices;         /* device, 3 floats per vertex */
+    int32_t* faces;          /* device, verts_per_face ints per face */
+    const uint64_t* cell_coords; /* device, per vertex: cell (i,j,k) packed i | j<<21 | k<<42 */
+} dcb_mesh_dev;
+
+/* Host mesh; pointers are owned by the handle (pinned) with the same lifetime. */
+typedef struct {
+    int64_t vertex_count;
+    int64_t face_count;
+    int verts_per_face;
+    const float* vertices;
+    const int32_t* faces;
+} dcb_mesh_host;
+
+typedef struct dcb_context* dcb_handle;
+
+/* Create a handle bound to CUDA device `device`. */
+int dcb_create(dcb_handle* out, int device);
+int dcb_destroy(dcb_handle h);
+
+/* Replaces CudaDualContouringBackend::extract_device (include/dc_cuda.h:31-35,
+ * src/cuda/dc_cuda.cu:652-847): grid->values is a device pointer. */
+int dcb_extract_device(dcb_handle h, const dcb_grid* grid, const dcb_opts* opts,
+                       dcb_mesh_dev* out, dcb_stats* stats, void* cuda_stream);
+
+/* Replaces IDualContouringBackend::extract (include/dc_backend.h:80-84;
+ * CpuDualContouringBackend::extract src/cpp/dc_backend.cpp:51-125 is the semantics):
+ * grid->values is a host pointer; upload, extraction and download all run on the stream
+ * and the call returns after the mesh is on the host. */
+int dcb_extract_host(dcb_handle h, const dcb_grid* grid, const dcb_opts* opts,
+                     dcb_mesh_host* out, dcb_stats* stats, void* cuda_stream);
+
+/* Copy the last mesh of `h` into caller-owned host arrays (3*V floats, vpf*F ints). */
+int dcb_copy_mesh_to_host(dcb_handle h, float* vertices, int32_t* faces, void* cuda_stream);
+
+/* Copy the last mesh of `h` into caller-owned DEVICE arrays (e.g. torch CUDA tensors). */
+int dcb_copy_mesh_device(dcb_handle h, float* vertices, int32_t* faces, void* cuda_stream);
+
+/* Copy the linear cell index (i + cx*(j + cy*k), cx = nx-1, cy = ny-1) of every vertex of
+ * the last mesh into a caller-owned host array of vertex_count entries. */
+int dcb_copy_cells_to_host(dcb_handle h, int64_t* cell_linear_index, void* cuda_stream);
+
+/* Human-readable text of a status code and of the last error on this handle. */
+const char* dcb_status_string(int status);
+const char* dcb_last_error(dcb_handle h);
+
+/* Version of the ABI compiled into the library. */
+int dcb_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DCB_H_ */

@@ -1,0 +1,89 @@
+"""ctypes wrapper around the CPU oracle library (TEST INFRASTRUCTURE ONLY).
+
+The oracle is the FP64 C++ restatement in ``oracle/dc_oracle.cpp`` of the reference's
+``CpuDualContouringBackend::extract`` (src/cpp/dc_backend.cpp:51-125).  Only ``tests/``,
+``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline / reference legs import this
+module, and only as the checker or the CPU baseline, never as the product path.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_DC_LIB = os.path.join(_HERE, "_build", "libdc_oracle.so")
+_MTS_LIB = os.path.join(_HERE, "_build", "libmts_oracle.so")
+_libs = {}
+
+
+def build():
+    """Compile the oracle libraries with the Makefile beside this file."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+class _Stats(ctypes.Structure):
+    _fields_ = [("total_cells", ctypes.c_int64), ("active_cells", ctypes.c_int64),
+                ("vertex_count", ctypes.c_int64), ("face_count", ctypes.c_int64),
+                ("total_ms", ctypes.c_double)]
+
+
+def _load(path):
+    if path not in _libs:
+        if not os.path.exists(path):
+            build()
+        _libs[path] = ctypes.CDLL(path)
+    return _libs[path]
+
+
+def _dc():
+    lib = _load(_DC_LIB)
+    if not getattr(lib, "_typed", False):
+        lib.dco_extract.restype = ctypes.c_void_p
+        lib.dco_extract.argtypes = [ctypes.c_int] * 3 + [ctypes.c_float] * 6 + [
+            ctypes.c_void_p, ctypes.c_double, ctypes.c_int, ctypes.POINTER(_Stats)]
+        lib.dco_num_vertices.restype = ctypes.c_int64
+        lib.dco_num_vertices.argtypes = [ctypes.c_void_p]
+        lib.dco_num_faces.restype = ctypes.c_int64
+        lib.dco_num_faces.argtypes = [ctypes.c_void_p]
+        lib.dco_copy.restype = None
+        lib.dco_copy.argtypes = [ctypes.c_void_p] * 6
+        lib.dco_free.restype = None
+        lib.dco_free.argtypes = [ctypes.c_void_p]
+        lib._typed = True
+    return lib
+
+
+def dc_extract(values, dims, spacing, origin, svd_threshold=0.01, threads=0):
+    """Run the restated CPU dual contouring on a dense x-fastest float32 grid.
+
+    ``values`` has ``nx*ny*nz`` float32 entries, index ``i + nx*(j + ny*k)``.
+    Returns a dict with FP64 vertices ``V`` (nv,3), int32 quads ``F`` (nf,4), the linear
+    index of each vertex's cell ``cells``, the eigenvalues of each cell's A^T A ``eig``,
+    the Hermite row count ``nrows`` and ``stats``.
+    """
+    nx, ny, nz = (int(d) for d in dims)
+    vals = np.ascontiguousarray(np.asarray(values, dtype=np.float32).reshape(-1))
+    if vals.size != nx * ny * nz:
+        raise ValueError("values has %d entries, expected %d" % (vals.size, nx * ny * nz))
+    lib = _dc()
+    st = _Stats()
+    h = lib.dco_extract(nx, ny, nz, float(spacing[0]), float(spacing[1]), float(spacing[2]),
+                        float(origin[0]), float(origin[1]), float(origin[2]),
+                        vals.ctypes.data, float(svd_threshold), int(threads), ctypes.byref(st))
+    if not h:
+        raise ValueError("oracle rejected the grid")
+    try:
+        nv = lib.dco_num_vertices(h)
+        nf = lib.dco_num_faces(h)
+        V = np.empty((nv, 3), np.float64)
+        F = np.empty((nf, 4), np.int32)
+        cells = np.empty(nv, np.int64)
+        eig = np.empty((nv, 3), np.float64)
+        nrows = np.empty(nv, np.int32)
+        lib.dco_copy(h, V.ctypes.data, F.ctypes.data, cells.ctypes.data, eig.ctypes.data,
+                     nrows.ctypes.data)
+    finally:
+        lib.dco_free(h)
+    stats = {k: getattr(st, k) for k, _ in _Stats._fields_}
+    return {"V": V, "F": F, "cells": cells, "eig": eig, "nrows": nrows, "stats": stats}

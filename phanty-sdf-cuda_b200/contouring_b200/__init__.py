@@ -1,0 +1,12 @@
+"""B200-native dual-contouring backend (drop-in for the reference's IDualContouringBackend).
+
+Public names mirror the reference module ``_contouring_cpp_module`` (src/cpp/bindings.cpp):
+``DenseSdfGrid``, ``DenseSdfGridDevice``, ``DualContouringMesh``, ``DualContouringStats``,
+``ContouringOptions``, ``ContouringMethod``; the new backend is ``B200DualContouringBackend``.
+"""
+from .backend import (B200DualContouringBackend, ContouringMethod, ContouringOptions, DcbError,
+                      DenseSdfGrid, DenseSdfGridDevice, DualContouringMesh, DualContouringStats)
+from . import _lib
+
+__all__ = ["B200DualContouringBackend", "ContouringMethod", "ContouringOptions", "DcbError",
+           "DenseSdfGrid", "DenseSdfGridDevice", "DualContouringMesh", "DualContouringStats"]

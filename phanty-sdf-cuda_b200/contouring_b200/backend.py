@@ -1,0 +1,265 @@
+"""Host-side mirror of the reference's Python/C++ backend API for the B200 engine.
+
+The reference exposes (src/cpp/bindings.cpp:127-268, module ``_contouring_cpp_module``):
+``DenseSdfGrid`` (nx..oz, values), ``DualContouringMesh`` (vertices, faces),
+``DualContouringStats`` and backends whose ``extract(grid)`` returns ``(mesh, stats)`` and
+whose CUDA variant also has ``extract_device(grid_device)``. This module provides the same
+names and call shapes for the new backend, :class:`B200DualContouringBackend`, on top of the
+C ABI in ``include/dcb.h``. Differences: ``vertices`` / ``faces`` are flat numpy arrays
+(float32 / int32) instead of Python lists, and errors raise :class:`DcbError` instead of
+terminating the process (the reference exits on CUDA errors: src/cuda/dc_cuda.cu:14-20).
+"""
+import ctypes
+import enum
+
+import numpy as np
+
+from . import _lib
+from ._lib import DcbError
+
+
+class ContouringMethod(enum.IntEnum):
+    """ContouringMethod (include/contouring.h:21-25)."""
+    MarchingCubes = 0
+    DualContouring = 1
+    Ours = 2
+
+
+class ContouringOptions:
+    """ContouringOptions (include/contouring.h:27-41) plus the B200 precision knobs."""
+
+    def __init__(self):
+        self.method = ContouringMethod.DualContouring
+        self.verbose = False
+        self.mu = 0.1
+        self.dc_weight = 0.02
+        self.sphere_weight = 1.0
+        self.svd_threshold = 0.01
+        self.outer_iters = 100
+        self.inner_iters = 100
+        self.hermite_update = True
+        self.new_hermite_pos_weight = 0.2
+        self.new_face_pos_weight = 0.2
+        self.new_hermite_normal_weight = 0.2
+        self.batch_size = 200000
+        d = _lib.DcbOpts()
+        try:
+            _lib.lib().dcb_default_opts(ctypes.byref(d))
+            self.fp64_escalation_cond = d.fp64_escalation_cond
+            self.fp64_threshold_band = d.fp64_threshold_band
+        except ImportError:
+            self.fp64_escalation_cond = 1e6
+            self.fp64_threshold_band = 0.05
+        self.emit_triangles = False
+        self.force_fp64 = False
+
+    def to_c(self):
+        o = _lib.default_opts()
+        if int(self.method) == ContouringMethod.MarchingCubes:
+            raise DcbError(_lib.DCB_ERR_NOT_SUPPORTED, "marching cubes is not part of this engine")
+        o.method = _lib.DCB_METHOD_OURS if int(self.method) == ContouringMethod.Ours else _lib.DCB_METHOD_DUAL_CONTOURING
+        o.outer_iters = int(self.outer_iters)
+        o.inner_iters = int(self.inner_iters)
+        o.mu = float(self.mu)
+        o.dc_weight = float(self.dc_weight)
+        o.sphere_weight = float(self.sphere_weight)
+        o.svd_threshold = float(self.svd_threshold)
+        o.fp64_escalation_cond = float(self.fp64_escalation_cond)
+        o.fp64_threshold_band = float(self.fp64_threshold_band)
+        o.emit_triangles = 1 if self.emit_triangles else 0
+        o.force_fp64 = 1 if self.force_fp64 else 0
+        return o
+
+
+class DenseSdfGrid:
+    """DenseSdfGrid (include/dc_backend.h:13-21): dense float32 grid, x fastest."""
+
+    def __init__(self, nx=0, ny=0, nz=0, vx=0.0, vy=0.0, vz=0.0, ox=0.0, oy=0.0, oz=0.0, values=None):
+        self.nx, self.ny, self.nz = nx, ny, nz
+        self.vx, self.vy, self.vz = vx, vy, vz
+        self.ox, self.oy, self.oz = ox, oy, oz
+        self.values = values if values is not None else []
+
+    @classmethod
+    def from_tuple(cls, t):
+        values, dims, spacing, origin = t
+        if hasattr(values, "detach"):
+            values = values.detach().cpu().numpy()
+        return cls(*dims, *spacing, *origin, values=np.asarray(values, np.float32).reshape(-1))
+
+
+class DenseSdfGridDevice:
+    """DenseSdfGridDevice (include/dc_cuda.h:24-29): ``d_values`` is a CUDA tensor or a raw
+    device pointer (int). The grid is borrowed, never freed by the backend."""
+
+    def __init__(self, nx=0, ny=0, nz=0, vx=0.0, vy=0.0, vz=0.0, ox=0.0, oy=0.0, oz=0.0, d_values=None):
+        self.nx, self.ny, self.nz = nx, ny, nz
+        self.vx, self.vy, self.vz = vx, vy, vz
+        self.ox, self.oy, self.oz = ox, oy, oz
+        self.d_values = d_values
+
+    def pointer(self):
+        v = self.d_values
+        if v is None:
+            return 0
+        if hasattr(v, "data_ptr"):
+            if not v.is_cuda or v.dtype.__repr__() != "torch.float32" or not v.is_contiguous():
+                raise DcbError(_lib.DCB_ERR_INVALID_ARGUMENT, "d_values must be a contiguous float32 CUDA tensor")
+            if v.numel() != self.nx * self.ny * self.nz:
+                raise DcbError(_lib.DCB_ERR_INVALID_ARGUMENT, "d_values has the wrong number of elements")
+            return v.data_ptr()
+        return int(v)
+
+
+class DualContouringMesh:
+    """DualContouringMesh (include/dc_backend.h:23-26): xyz per vertex, 4 ints per quad."""
+
+    def __init__(self, vertices=None, faces=None):
+        self.vertices = vertices if vertices is not None else np.zeros(0, np.float32)
+        self.faces = faces if faces is not None else np.zeros(0, np.int32)
+
+
+class DualContouringStats:
+    """DualContouringStats (include/dc_backend.h:44-78) plus the engine's own counters."""
+    _FIELDS = ("backend", "nx", "ny", "nz", "total_cells", "active_cells", "total_bricks", "active_bricks",
+               "upload_ms", "marking_ms", "compaction_ms", "active_brick_marking_ms",
+               "active_brick_compaction_ms", "active_cell_marking_ms", "active_cell_compaction_ms",
+               "qef_ms", "face_emission_ms", "face_count_ms", "face_prefix_sum_ms", "face_fill_ms",
+               "download_ms", "total_ms", "vertex_count", "face_count", "qef_fallback_count",
+               "clamp_count", "invalid_count", "ambiguous_cells", "multi_vertex_cells",
+               "one_vertex_cells", "two_vertex_cells", "split_rejection_count", "bad_qef_count",
+               "faces_skipped_due_to_missing_cluster")
+
+    def __init__(self):
+        for f in self._FIELDS:
+            setattr(self, f, "" if f == "backend" else 0)
+        self.escalated_fp64_cells = 0
+        self.winding_fp64_faces = 0
+        self.rank_hist = [0, 0, 0, 0]
+
+    @classmethod
+    def from_c(cls, st):
+        s = cls()
+        s.backend = "b200"
+        for f in ("nx", "ny", "nz", "total_cells", "active_cells", "vertex_count", "face_count",
+                  "upload_ms", "marking_ms", "compaction_ms", "qef_ms", "face_emission_ms",
+                  "download_ms", "total_ms", "qef_fallback_count", "clamp_count",
+                  "escalated_fp64_cells", "winding_fp64_faces"):
+            setattr(s, f, getattr(st, f))
+        s.active_cell_marking_ms = st.marking_ms
+        s.rank_hist = list(st.rank_hist)
+        return s
+
+    def as_dict(self):
+        d = {f: getattr(self, f) for f in self._FIELDS}
+        d.update(escalated_fp64_cells=self.escalated_fp64_cells, winding_fp64_faces=self.winding_fp64_faces,
+                 rank_hist=list(self.rank_hist))
+        return d
+
+
+def _current_stream():
+    try:
+        import torch
+        if torch.cuda.is_available() and torch.cuda.is_initialized():
+            return torch.cuda.current_stream().cuda_stream
+    except ImportError:
+        pass
+    return 0
+
+
+class B200DualContouringBackend:
+    """The B200 backend. ``extract`` has the semantics of the reference's
+    ``CpuDualContouringBackend::extract`` (src/cpp/dc_backend.cpp:51-125)."""
+
+    def __init__(self, device=0, options=None):
+        self._L = _lib.lib()
+        h = ctypes.c_void_p()
+        _lib.check(self._L.dcb_create(ctypes.byref(h), int(device)))
+        self._h = h
+        self.device = int(device)
+        self.options = options if options is not None else ContouringOptions()
+        self._last_nv = 0
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.dcb_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def _grid_c(g, ptr):
+        return _lib.DcbGrid(int(g.nx), int(g.ny), int(g.nz), float(g.vx), float(g.vy), float(g.vz),
+                            float(g.ox), float(g.oy), float(g.oz), ptr)
+
+    def extract(self, grid, stream=None):
+        """Host grid in, host mesh out: returns ``(DualContouringMesh, DualContouringStats)``."""
+        vals = np.ascontiguousarray(np.asarray(grid.values, dtype=np.float32).reshape(-1))
+        if vals.size != int(grid.nx) * int(grid.ny) * int(grid.nz):
+            raise DcbError(_lib.DCB_ERR_INVALID_ARGUMENT, "values has %d entries, expected nx*ny*nz" % vals.size)
+        gc = self._grid_c(grid, vals.ctypes.data)
+        st = _lib.DcbStats()
+        mh = _lib.DcbMeshHost()
+        s = _current_stream() if stream is None else stream
+        _lib.check(self._L.dcb_extract_host(self._h, ctypes.byref(gc), ctypes.byref(self.options.to_c()),
+                                            ctypes.byref(mh), ctypes.byref(st), ctypes.c_void_p(s)), self._h)
+        self._last_nv = mh.vertex_count
+        return self._host_mesh(mh), DualContouringStats.from_c(st)
+
+    @staticmethod
+    def _host_mesh(mh):
+        nv, nf, vpf = mh.vertex_count, mh.face_count, mh.verts_per_face
+        V = (np.ctypeslib.as_array(ctypes.cast(mh.vertices, ctypes.POINTER(ctypes.c_float)), shape=(3 * nv,)).copy()
+             if nv else np.zeros(0, np.float32))
+        F = (np.ctypeslib.as_array(ctypes.cast(mh.faces, ctypes.POINTER(ctypes.c_int32)), shape=(vpf * nf,)).copy()
+             if nf else np.zeros(0, np.int32))
+        return DualContouringMesh(V, F)
+
+    def active_cells(self, stream=None):
+        """Linear index (i + cx*(j + cy*k)) of the cell of every vertex of the last mesh."""
+        n = self._last_nv
+        out = np.empty(n, np.int64)
+        s = _current_stream() if stream is None else stream
+        _lib.check(self._L.dcb_copy_cells_to_host(self._h, out.ctypes.data if n else None, ctypes.c_void_p(s)), self._h)
+        return out
+
+    def extract_device(self, grid, stream=None):
+        """Device grid in (``DenseSdfGridDevice``), host mesh out, like the reference's
+        ``CudaDualContouringBackend::extract_device`` (src/cuda/dc_cuda.cu:652-847)."""
+        V, F, stats = self.extract_tensor_ptr(grid, stream)
+        nv, nf = stats.vertex_count, stats.face_count
+        hv = np.empty(3 * nv, np.float32)
+        hf = np.empty(4 * nf, np.int32)
+        s = _current_stream() if stream is None else stream
+        _lib.check(self._L.dcb_copy_mesh_to_host(self._h, hv.ctypes.data if nv else None,
+                                                 hf.ctypes.data if nf else None, ctypes.c_void_p(s)), self._h)
+        return DualContouringMesh(hv, hf), stats
+
+    def extract_tensor_ptr(self, grid, stream=None):
+        """Run on a device grid; returns the handle-owned device pointers (valid until the
+        next call) and the stats."""
+        gc = self._grid_c(grid, grid.pointer())
+        st = _lib.DcbStats()
+        md = _lib.DcbMeshDev()
+        s = _current_stream() if stream is None else stream
+        _lib.check(self._L.dcb_extract_device(self._h, ctypes.byref(gc), ctypes.byref(self.options.to_c()),
+                                              ctypes.byref(md), ctypes.byref(st), ctypes.c_void_p(s)), self._h)
+        self._last_nv = md.vertex_count
+        return md.vertices, md.faces, DualContouringStats.from_c(st)
+
+    def extract_tensor(self, values, dims, spacing, origin):
+        """torch convenience: CUDA float32 grid in, ``(V (nv,3) float32, F (nf,4) int32,
+        stats)`` CUDA tensors out (copied from the handle's buffers)."""
+        import torch
+        g = DenseSdfGridDevice(*dims, *spacing, *origin, d_values=values)
+        _, _, stats = self.extract_tensor_ptr(g)
+        V = torch.empty((stats.vertex_count, 3), dtype=torch.float32, device=values.device)
+        F = torch.empty((stats.face_count, 4), dtype=torch.int32, device=values.device)
+        s = torch.cuda.current_stream().cuda_stream
+        _lib.check(self._L.dcb_copy_mesh_device(self._h, V.data_ptr() if V.numel() else None,
+                                                F.data_ptr() if F.numel() else None, ctypes.c_void_p(s)), self._h)
+        return V, F, stats

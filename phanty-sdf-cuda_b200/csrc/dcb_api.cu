@@ -1,0 +1,475 @@
+// dcb_api.cu — handle, workspace and the C ABI declared in include/dcb.h.
+//
+// Pipeline of one extraction (all on the caller's stream):
+//   k_mark_compact   grid -> bits, super ranks, packed active list     (dcb_mark.cu)
+//   [host reads the active count: sizes the vertex buffers]
+//   k_vertex_fp32    Hermite + averaging + QEF, face masks, column counts (dcb_vertex.cu)
+//   k_vertex_fp64    escalated cells re-solved in FP64                 (dcb_vertex64.cu)
+//   scan             column counts -> column starts, face total       (dcb_faces.cu)
+//   k_face_scatter   quads into their columns, FP32 winding           (dcb_faces.cu)
+//   k_winding_fp64   uncertain windings re-decided in FP64            (dcb_vertex64.cu)
+//   k_face_order     rank by k inside each column -> final face list  (dcb_faces.cu)
+//   [host reads the face total and counters]
+// The reference backend allocates and frees everything per call and synchronises after
+// every stage (src/cuda/dc_cuda.cu:614-847); here buffers live in the handle and grow.
+#include <cstdio>
+#include <cstring>
+#include <cmath>
+#include <string>
+#include <algorithm>
+#include "dcb_kernels.cuh"
+#include "../../include/dcb.h"
+
+namespace dcb {
+
+// Small device-side counters, cleared at the start of every extraction.
+struct Counters {
+    int err;
+    unsigned int esc_count;
+    unsigned long long total_active;
+    unsigned int wind_count;
+    unsigned int hard_count;
+    unsigned int v64_count;
+    unsigned int pad;
+    unsigned long long rank_hist[4];
+    unsigned long long face_total;
+};
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+}  // namespace dcb
+
+using namespace dcb;
+
+struct dcb_context {
+    int device = 0;
+    int num_sms = 148;
+    std::string last_error;
+    cudaEvent_t ev[8] = {};
+    DevBuf grid, bits, super, list, seg_count, seg_start, counters, V, fmask, eflags, en, col_count, col_fill,
+        col_start, partials, esc_list, hard_list, hard_data, stage_quad, stage_key, faces, wind_items,
+        v64_index, v64_cells, V64;
+    void* h_counters = nullptr;       // pinned Counters
+    void* hV = nullptr; size_t hV_bytes = 0;
+    void* hF = nullptr; size_t hF_bytes = 0;
+    int64_t nv = 0, nf = 0;
+    int cx = 0, cy = 0;
+};
+
+namespace {
+
+int fail(dcb_context* h, int code, const std::string& msg) {
+    if (h) h->last_error = msg;
+    return code;
+}
+
+int cuda_fail(dcb_context* h, cudaError_t e, const char* what) {
+    std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+    if (e == cudaErrorMemoryAllocation) return fail(h, DCB_ERR_OUT_OF_MEMORY, m);
+    return fail(h, DCB_ERR_CUDA, m);
+}
+
+#define DCB_TRY(h, expr, what)                                   \
+    do {                                                         \
+        cudaError_t e_ = (expr);                                 \
+        if (e_ != cudaSuccess) return cuda_fail((h), e_, (what)); \
+    } while (0)
+
+cudaError_t ensure(DevBuf& b, size_t bytes) {
+    if (bytes == 0) bytes = 256;
+    if (b.bytes >= bytes) return cudaSuccess;
+    if (b.p) { cudaFree(b.p); b.p = nullptr; b.bytes = 0; }
+    const size_t want = bytes + bytes / 8;   // headroom for slowly growing workloads
+    cudaError_t e = cudaMalloc(&b.p, want);
+    if (e != cudaSuccess) { cudaGetLastError(); return e; }
+    b.bytes = want;
+    return cudaSuccess;
+}
+
+cudaError_t ensure_host(void*& p, size_t& have, size_t bytes) {
+    if (bytes == 0) bytes = 256;
+    if (have >= bytes) return cudaSuccess;
+    if (p) { cudaFreeHost(p); p = nullptr; have = 0; }
+    const size_t want = bytes + bytes / 8;
+    cudaError_t e = cudaMallocHost(&p, want);
+    if (e != cudaSuccess) { cudaGetLastError(); return e; }
+    have = want;
+    return cudaSuccess;
+}
+
+template <typename T> T* as(DevBuf& b) { return reinterpret_cast<T*>(b.p); }
+
+bool finite_pos(float x) { return std::isfinite(x); }
+
+int validate(dcb_context* h, const dcb_grid* g) {
+    if (!h) return DCB_ERR_INVALID_ARGUMENT;
+    if (!g || !g->values) return fail(h, DCB_ERR_INVALID_ARGUMENT, "grid or grid values is null");
+    if (g->nx < 2 || g->ny < 2 || g->nz < 2) return fail(h, DCB_ERR_INVALID_ARGUMENT, "grid needs at least 2 points per axis");
+    if (g->nx > 65536 || g->ny > (1 << 21) || g->nz > (1 << 21))
+        return fail(h, DCB_ERR_TOO_LARGE, "grid axis exceeds the index limits (nx <= 65536, ny,nz <= 2^21)");
+    if (!finite_pos(g->vx) || !finite_pos(g->vy) || !finite_pos(g->vz) || !finite_pos(g->ox) ||
+        !finite_pos(g->oy) || !finite_pos(g->oz))
+        return fail(h, DCB_ERR_INVALID_ARGUMENT, "grid spacing and origin must be finite");
+    const double cells = (double)(g->nx - 1) * (double)(g->ny - 1) * (double)(g->nz - 1);
+    if (cells >= 4.0e18) return fail(h, DCB_ERR_TOO_LARGE, "grid too large");
+    return DCB_OK;
+}
+
+float elapsed(cudaEvent_t a, cudaEvent_t b) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, a, b) != cudaSuccess) { cudaGetLastError(); return 0.f; }
+    return ms;
+}
+
+// Runs the pipeline on a device-resident grid; ev[1] must already be recorded.
+int run_pipeline(dcb_context* h, const dcb_grid* in, const dcb_opts* o, cudaStream_t s, dcb_stats* st) {
+    GridDesc g;
+    g.nx = in->nx; g.ny = in->ny; g.nz = in->nz;
+    g.cx = g.nx - 1; g.cy = g.ny - 1; g.cz = g.nz - 1;
+    g.W = ((g.cx + 31) / 32 + 7) / 8 * 8;
+    g.W8 = g.W / 8;
+    g.vx = in->vx; g.vy = in->vy; g.vz = in->vz;
+    g.ox = in->ox; g.oy = in->oy; g.oz = in->oz;
+    g.v = in->values;
+
+    const long long rows = (long long)g.cy * g.cz;
+    const long long ncell = (long long)g.cx * rows;
+    const long long cxcy = (long long)g.cx * g.cy;
+    const uintptr_t base = reinterpret_cast<uintptr_t>(g.v);
+    const int vec4 = (g.nx % 4 == 0 && (base % 16) == 0) ? 1 : 0;
+    const int tile_cells = 32 * mark_tile_words();
+    const int nxt = (g.cx + tile_cells - 1) / tile_cells;
+    const int R = std::min(mark_max_rows(), g.cy);
+    const long long nrb = (g.cy + R - 1) / R;
+    long long KZ = (g.cz * nxt * nrb + (long long)h->num_sms * 12 - 1) / ((long long)h->num_sms * 12);
+    KZ = std::max(8LL, std::min(64LL, KZ));
+    const long long nseg = rows * nxt;
+    if (nrb > 65535 || (g.cz + KZ - 1) / KZ > 65535) return fail(h, DCB_ERR_TOO_LARGE, "grid too large for the tiling");
+
+    DCB_TRY(h, ensure(h->bits, sizeof(uint32_t) * rows * g.W), "alloc bits");
+    DCB_TRY(h, ensure(h->super, sizeof(uint32_t) * rows * g.W8), "alloc ranks");
+    DCB_TRY(h, ensure(h->seg_count, sizeof(uint32_t) * nseg), "alloc segment counts");
+    DCB_TRY(h, ensure(h->seg_start, sizeof(uint32_t) * nseg), "alloc segment starts");
+    DCB_TRY(h, ensure(h->counters, sizeof(Counters)), "alloc counters");
+    DCB_TRY(h, ensure(h->col_count, sizeof(uint32_t) * 3 * cxcy), "alloc column counts");
+    DCB_TRY(h, ensure(h->col_fill, sizeof(uint32_t) * 3 * cxcy), "alloc column fill");
+    DCB_TRY(h, ensure(h->col_start, sizeof(uint32_t) * 3 * cxcy), "alloc column starts");
+    const long long plen = std::max(scan_partials_len(3 * cxcy), scan_partials_len(nseg));
+    DCB_TRY(h, ensure(h->partials, sizeof(uint32_t) * std::max(1LL, plen)), "alloc scan");
+    if (!h->h_counters) DCB_TRY(h, cudaMallocHost(&h->h_counters, sizeof(Counters)), "alloc pinned counters");
+
+    Counters* dc = as<Counters>(h->counters);
+    Counters* hc = reinterpret_cast<Counters*>(h->h_counters);
+
+    // 1) mark: active bits + per-segment counts; scan -> segment starts and the total.
+    DCB_TRY(h, cudaMemsetAsync(h->counters.p, 0, sizeof(Counters), s), "memset counters");
+    MarkParams mp;
+    mp.g = g; mp.R = R; mp.KZ = (int)KZ; mp.nxt = nxt;
+    mp.bits = as<uint32_t>(h->bits); mp.seg_count = as<uint32_t>(h->seg_count); mp.vec4 = vec4;
+    DCB_TRY(h, launch_mark(mp, s), "launch mark");
+    DCB_TRY(h, launch_scan(mp.seg_count, nseg, as<uint32_t>(h->partials), as<uint32_t>(h->seg_start),
+                           &dc->total_active, s), "launch segment scan");
+    DCB_TRY(h, cudaEventRecord(h->ev[2], s), "event");
+    DCB_TRY(h, cudaMemcpyAsync(hc, dc, sizeof(Counters), cudaMemcpyDeviceToHost, s), "read count");
+    DCB_TRY(h, cudaStreamSynchronize(s), "mark");
+    const long long nv = (long long)hc->total_active;
+    if (nv >= 0x7fffffffLL) return fail(h, DCB_ERR_TOO_LARGE, "more than 2^31-1 vertices");
+
+    h->nv = nv;
+    h->nf = 0;
+    h->cx = g.cx;
+    h->cy = g.cy;
+    if (st) {
+        st->nx = g.nx; st->ny = g.ny; st->nz = g.nz;
+        st->total_cells = ncell; st->active_cells = nv; st->vertex_count = nv;
+    }
+    if (nv == 0) {
+        DCB_TRY(h, cudaEventRecord(h->ev[3], s), "event");
+        DCB_TRY(h, cudaEventRecord(h->ev[4], s), "event");
+        return DCB_OK;
+    }
+
+    DCB_TRY(h, ensure(h->list, sizeof(uint64_t) * nv), "alloc active list");
+    DCB_TRY(h, ensure(h->V, sizeof(float) * 3 * nv), "alloc vertices");
+    DCB_TRY(h, ensure(h->fmask, nv), "alloc face masks");
+    DCB_TRY(h, ensure(h->eflags, nv), "alloc edge flags");
+    DCB_TRY(h, ensure(h->en, sizeof(float4) * 3 * nv), "alloc edge normals");
+    DCB_TRY(h, ensure(h->esc_list, sizeof(uint32_t) * nv), "alloc escalation list");
+    DCB_TRY(h, ensure(h->hard_list, sizeof(uint32_t) * nv), "alloc hard list");
+    DCB_TRY(h, ensure(h->hard_data, sizeof(float4) * 3 * nv), "alloc hard data");
+    DCB_TRY(h, ensure(h->stage_quad, sizeof(int4) * 3 * nv), "alloc face staging");
+    DCB_TRY(h, ensure(h->stage_key, sizeof(uint2) * 3 * nv), "alloc face keys");
+    DCB_TRY(h, ensure(h->faces, sizeof(int4) * 3 * nv), "alloc faces");
+    DCB_TRY(h, ensure(h->v64_index, sizeof(int) * nv), "alloc fp64 index");
+    // Exact upper bounds: at most 3 faces per owner cell, one FP64 vertex per cell.
+    const long long wind_cap = std::min(0x7fffffffLL, 3 * nv);
+    const long long v64_cap = nv;
+    DCB_TRY(h, ensure(h->wind_items, sizeof(uint4) * wind_cap), "alloc winding list");
+    DCB_TRY(h, ensure(h->v64_cells, sizeof(uint32_t) * v64_cap), "alloc fp64 cells");
+    DCB_TRY(h, ensure(h->V64, sizeof(double) * 3 * v64_cap), "alloc fp64 vertices");
+    DCB_TRY(h, cudaMemsetAsync(h->col_count.p, 0, sizeof(uint32_t) * 3 * cxcy, s), "memset");
+    DCB_TRY(h, cudaMemsetAsync(h->col_fill.p, 0, sizeof(uint32_t) * 3 * cxcy, s), "memset");
+    DCB_TRY(h, cudaMemsetAsync(h->v64_index.p, 0xff, sizeof(int) * nv, s), "memset");
+
+    // 2) ranks + list, edge normals, QEF (rank-1 fast path, Jacobi list, FP64 escalations).
+    ExpandParams xp;
+    xp.g = g; xp.nxt = nxt; xp.bits = mp.bits; xp.seg_count = mp.seg_count;
+    xp.seg_start = as<uint32_t>(h->seg_start); xp.super = as<uint32_t>(h->super); xp.list = as<uint64_t>(h->list);
+    DCB_TRY(h, launch_expand(xp, h->num_sms, s), "launch expand");
+    EdgeParams ep;
+    ep.g = g; ep.list = xp.list; ep.nactive = nv; ep.en = as<float4>(h->en); ep.eflags = as<uint8_t>(h->eflags);
+    ep.fmask = as<uint8_t>(h->fmask); ep.col_count = as<uint32_t>(h->col_count);
+    DCB_TRY(h, launch_edge_normals(ep, h->num_sms, s), "launch edge normals");
+    QefParams qp;
+    qp.g = g; qp.list = xp.list; qp.nactive = nv; qp.bits = mp.bits; qp.super = xp.super;
+    qp.en = ep.en; qp.eflags = ep.eflags; qp.V = as<float>(h->V);
+    qp.esc_list = as<uint32_t>(h->esc_list); qp.esc_count = &dc->esc_count;
+    qp.hard_list = as<uint32_t>(h->hard_list); qp.hard_data = as<float4>(h->hard_data); qp.hard_count = &dc->hard_count;
+    qp.rank_hist = dc->rank_hist;
+    qp.thr = (float)o->svd_threshold; qp.band = (float)o->fp64_threshold_band;
+    qp.cond_max = (float)std::min(o->fp64_escalation_cond, 3.0e38); qp.force64 = o->force_fp64;
+    DCB_TRY(h, launch_cell_qef(qp, h->num_sms, s), "launch qef");
+    DCB_TRY(h, launch_cell_jacobi(qp, nv, h->num_sms, s), "launch jacobi");
+    Vertex64Params v64;
+    v64.g = g; v64.list = xp.list; v64.cells = qp.esc_list; v64.count = &dc->esc_count; v64.cap = (unsigned int)nv;
+    v64.Vf = qp.V; v64.V64 = nullptr; v64.thr = o->svd_threshold;
+    DCB_TRY(h, launch_vertex_fp64(v64, nv, h->num_sms, s), "launch vertex fp64");
+    DCB_TRY(h, cudaEventRecord(h->ev[3], s), "event");
+
+    // 3) faces: column scan, scatter with FP32 winding, FP64 re-decisions, in-column order.
+    DCB_TRY(h, launch_scan(as<uint32_t>(h->col_count), 3 * cxcy, as<uint32_t>(h->partials),
+                           as<uint32_t>(h->col_start), &dc->face_total, s), "launch scan");
+    FaceParams fp;
+    fp.g = g; fp.list = xp.list; fp.nactive = nv; fp.fmask = ep.fmask; fp.V = qp.V;
+    fp.bits = mp.bits; fp.super = xp.super;
+    fp.col_start = as<uint32_t>(h->col_start); fp.col_count = as<uint32_t>(h->col_count);
+    fp.col_fill = as<uint32_t>(h->col_fill);
+    fp.stage_quad = as<int4>(h->stage_quad); fp.stage_key = as<uint2>(h->stage_key);
+    fp.wind_items = as<uint4>(h->wind_items); fp.wind_count = &dc->wind_count;
+    fp.wind_cap = (unsigned long long)wind_cap;
+    fp.v64_index = as<int>(h->v64_index); fp.v64_cells = as<uint32_t>(h->v64_cells);
+    fp.v64_count = &dc->v64_count; fp.v64_cap = (unsigned long long)v64_cap;
+    fp.err = &dc->err;
+    fp.hmax = std::max(std::fabs(g.vx), std::max(std::fabs(g.vy), std::fabs(g.vz)));
+    DCB_TRY(h, launch_face_scatter(fp, h->num_sms, s), "launch face scatter");
+    Vertex64Params w64;
+    w64.g = g; w64.list = xp.list; w64.cells = fp.v64_cells; w64.count = fp.v64_count; w64.cap = (unsigned int)v64_cap;
+    w64.Vf = nullptr; w64.V64 = as<double>(h->V64); w64.thr = o->svd_threshold;
+    DCB_TRY(h, launch_vertex_fp64(w64, v64_cap, h->num_sms, s), "launch fp64 vertices for windings");
+    Winding64Params wp;
+    wp.g = g; wp.items = fp.wind_items; wp.count = fp.wind_count; wp.cap = (unsigned int)wind_cap;
+    wp.quads = fp.stage_quad; wp.v64_index = fp.v64_index; wp.V64 = w64.V64; wp.err = &dc->err;
+    DCB_TRY(h, launch_winding_fp64(wp, wind_cap, h->num_sms, s), "launch winding fp64");
+    DCB_TRY(h, launch_face_order(fp.stage_quad, fp.stage_key, fp.col_start, fp.col_count, &dc->face_total,
+                                 as<int4>(h->faces), 3 * nv, h->num_sms, s), "launch face order");
+    DCB_TRY(h, cudaEventRecord(h->ev[4], s), "event");
+    DCB_TRY(h, cudaMemcpyAsync(hc, dc, sizeof(Counters), cudaMemcpyDeviceToHost, s), "read counters");
+    DCB_TRY(h, cudaStreamSynchronize(s), "pipeline");
+    if (hc->err) {
+        return fail(h, hc->err == kErrTimeout ? DCB_ERR_TIMEOUT : DCB_ERR_INTERNAL,
+                    hc->err == kErrOverflow ? "FP64 work list overflow" : "device error flag set");
+    }
+    h->nf = (int64_t)hc->face_total;
+    if (st) {
+        st->face_count = h->nf;
+        st->qef_fallback_count = hc->esc_count;
+        st->escalated_fp64_cells = hc->esc_count;
+        st->winding_fp64_faces = hc->wind_count;
+        for (int q = 0; q < 4; ++q) st->rank_hist[q] = (int64_t)hc->rank_hist[q];
+        st->clamp_count = 0;
+    }
+    return DCB_OK;
+}
+
+void fill_times(dcb_context* h, dcb_stats* st, bool upload) {
+    if (!st) return;
+    st->upload_ms = upload ? elapsed(h->ev[0], h->ev[1]) : 0.f;
+    st->marking_ms = elapsed(h->ev[1], h->ev[2]);
+    st->compaction_ms = 0.f;
+    st->qef_ms = elapsed(h->ev[2], h->ev[3]);
+    st->face_emission_ms = elapsed(h->ev[3], h->ev[4]);
+}
+
+}  // namespace
+
+extern "C" {
+
+void dcb_default_opts(dcb_opts* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->method = DCB_METHOD_DUAL_CONTOURING;
+    o->outer_iters = 100;
+    o->inner_iters = 100;
+    o->mu = 0.1;
+    o->dc_weight = 0.02;
+    o->sphere_weight = 1.0;
+    o->svd_threshold = 0.01;
+    o->fp64_escalation_cond = 1e6;
+    o->fp64_threshold_band = 0.05;
+    o->emit_triangles = 0;
+    o->force_fp64 = 0;
+}
+
+int dcb_abi_version(void) { return DCB_ABI_VERSION; }
+
+const char* dcb_status_string(int status) {
+    switch (status) {
+        case DCB_OK: return "ok";
+        case DCB_ERR_INVALID_ARGUMENT: return "invalid argument";
+        case DCB_ERR_TOO_LARGE: return "input exceeds index limits";
+        case DCB_ERR_CUDA: return "CUDA error";
+        case DCB_ERR_OUT_OF_MEMORY: return "out of memory";
+        case DCB_ERR_TIMEOUT: return "device wait timed out";
+        case DCB_ERR_NOT_SUPPORTED: return "not supported";
+        case DCB_ERR_INTERNAL: return "internal error";
+        default: return "unknown status";
+    }
+}
+
+const char* dcb_last_error(dcb_handle h) { return h ? h->last_error.c_str() : "null handle"; }
+
+int dcb_create(dcb_handle* out, int device) {
+    if (!out) return DCB_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess) { cudaGetLastError(); return DCB_ERR_CUDA; }
+    if (device < 0 || device >= count) return DCB_ERR_INVALID_ARGUMENT;
+    if (cudaSetDevice(device) != cudaSuccess) { cudaGetLastError(); return DCB_ERR_CUDA; }
+    dcb_context* h = new dcb_context();
+    h->device = device;
+    cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, device);
+    for (auto& ev : h->ev) {
+        if (cudaEventCreate(&ev) != cudaSuccess) { cudaGetLastError(); delete h; return DCB_ERR_CUDA; }
+    }
+    *out = h;
+    return DCB_OK;
+}
+
+int dcb_destroy(dcb_handle h) {
+    if (!h) return DCB_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(h->device);
+    DevBuf* bufs[] = {&h->grid, &h->bits, &h->super, &h->list, &h->seg_count, &h->seg_start, &h->counters,
+                      &h->V, &h->fmask, &h->eflags, &h->en, &h->col_count, &h->col_fill, &h->col_start,
+                      &h->partials, &h->esc_list, &h->hard_list, &h->hard_data, &h->stage_quad,
+                      &h->stage_key, &h->faces, &h->wind_items, &h->v64_index, &h->v64_cells, &h->V64};
+    for (DevBuf* b : bufs) if (b->p) cudaFree(b->p);
+    if (h->h_counters) cudaFreeHost(h->h_counters);
+    if (h->hV) cudaFreeHost(h->hV);
+    if (h->hF) cudaFreeHost(h->hF);
+    for (auto& ev : h->ev) if (ev) cudaEventDestroy(ev);
+    delete h;
+    return DCB_OK;
+}
+
+int dcb_extract_device(dcb_handle h, const dcb_grid* grid, const dcb_opts* opts, dcb_mesh_dev* out,
+                       dcb_stats* stats, void* cuda_stream) {
+    int rc = validate(h, grid);
+    if (rc != DCB_OK) return rc;
+    dcb_opts def;
+    dcb_default_opts(&def);
+    const dcb_opts* o = opts ? opts : &def;
+    if (o->method != DCB_METHOD_DUAL_CONTOURING) return fail(h, DCB_ERR_NOT_SUPPORTED, "only dual contouring is implemented");
+    if (o->emit_triangles) return fail(h, DCB_ERR_NOT_SUPPORTED, "triangle output is not implemented");
+    if (!(o->svd_threshold >= 0.0)) return fail(h, DCB_ERR_INVALID_ARGUMENT, "svd_threshold must be >= 0");
+    if (cudaSetDevice(h->device) != cudaSuccess) { cudaGetLastError(); return fail(h, DCB_ERR_CUDA, "set device"); }
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(cuda_stream);
+    if (stats) std::memset(stats, 0, sizeof(*stats));
+    DCB_TRY(h, cudaEventRecord(h->ev[0], s), "event");
+    DCB_TRY(h, cudaEventRecord(h->ev[1], s), "event");
+    rc = run_pipeline(h, grid, o, s, stats);
+    if (rc != DCB_OK) return rc;
+    fill_times(h, stats, false);
+    if (stats) stats->total_ms = elapsed(h->ev[1], h->ev[4]);
+    if (out) {
+        out->vertex_count = h->nv;
+        out->face_count = h->nf;
+        out->verts_per_face = 4;
+        out->vertices = as<float>(h->V);
+        out->faces = as<int32_t>(h->faces);
+        out->cell_coords = as<uint64_t>(h->list);
+    }
+    return DCB_OK;
+}
+
+int dcb_extract_host(dcb_handle h, const dcb_grid* grid, const dcb_opts* opts, dcb_mesh_host* out,
+                     dcb_stats* stats, void* cuda_stream) {
+    int rc = validate(h, grid);
+    if (rc != DCB_OK) return rc;
+    if (cudaSetDevice(h->device) != cudaSuccess) { cudaGetLastError(); return fail(h, DCB_ERR_CUDA, "set device"); }
+    dcb_opts def;
+    dcb_default_opts(&def);
+    const dcb_opts* o = opts ? opts : &def;
+    if (o->method != DCB_METHOD_DUAL_CONTOURING) return fail(h, DCB_ERR_NOT_SUPPORTED, "only dual contouring is implemented");
+    if (o->emit_triangles) return fail(h, DCB_ERR_NOT_SUPPORTED, "triangle output is not implemented");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(cuda_stream);
+    if (stats) std::memset(stats, 0, sizeof(*stats));
+    const size_t npts = (size_t)grid->nx * grid->ny * grid->nz;
+    DCB_TRY(h, ensure(h->grid, sizeof(float) * npts), "alloc grid");
+    DCB_TRY(h, cudaEventRecord(h->ev[0], s), "event");
+    DCB_TRY(h, cudaMemcpyAsync(h->grid.p, grid->values, sizeof(float) * npts, cudaMemcpyHostToDevice, s), "upload grid");
+    DCB_TRY(h, cudaEventRecord(h->ev[1], s), "event");
+    dcb_grid dg = *grid;
+    dg.values = as<float>(h->grid);
+    rc = run_pipeline(h, &dg, o, s, stats);
+    if (rc != DCB_OK) return rc;
+    DCB_TRY(h, ensure_host(h->hV, h->hV_bytes, sizeof(float) * 3 * h->nv), "alloc host vertices");
+    DCB_TRY(h, ensure_host(h->hF, h->hF_bytes, sizeof(int32_t) * 4 * h->nf), "alloc host faces");
+    if (h->nv) DCB_TRY(h, cudaMemcpyAsync(h->hV, h->V.p, sizeof(float) * 3 * h->nv, cudaMemcpyDeviceToHost, s), "download vertices");
+    if (h->nf) DCB_TRY(h, cudaMemcpyAsync(h->hF, h->faces.p, sizeof(int32_t) * 4 * h->nf, cudaMemcpyDeviceToHost, s), "download faces");
+    DCB_TRY(h, cudaEventRecord(h->ev[5], s), "event");
+    DCB_TRY(h, cudaStreamSynchronize(s), "download");
+    fill_times(h, stats, true);
+    if (stats) {
+        stats->download_ms = elapsed(h->ev[4], h->ev[5]);
+        stats->total_ms = elapsed(h->ev[0], h->ev[5]);
+    }
+    if (out) {
+        out->vertex_count = h->nv;
+        out->face_count = h->nf;
+        out->verts_per_face = 4;
+        out->vertices = reinterpret_cast<const float*>(h->hV);
+        out->faces = reinterpret_cast<const int32_t*>(h->hF);
+    }
+    return DCB_OK;
+}
+
+int dcb_copy_mesh_to_host(dcb_handle h, float* vertices, int32_t* faces, void* cuda_stream) {
+    if (!h) return DCB_ERR_INVALID_ARGUMENT;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(cuda_stream);
+    if (cudaSetDevice(h->device) != cudaSuccess) { cudaGetLastError(); return fail(h, DCB_ERR_CUDA, "set device"); }
+    if (vertices && h->nv) DCB_TRY(h, cudaMemcpyAsync(vertices, h->V.p, sizeof(float) * 3 * h->nv, cudaMemcpyDeviceToHost, s), "copy vertices");
+    if (faces && h->nf) DCB_TRY(h, cudaMemcpyAsync(faces, h->faces.p, sizeof(int32_t) * 4 * h->nf, cudaMemcpyDeviceToHost, s), "copy faces");
+    DCB_TRY(h, cudaStreamSynchronize(s), "copy mesh");
+    return DCB_OK;
+}
+
+int dcb_copy_mesh_device(dcb_handle h, float* vertices, int32_t* faces, void* cuda_stream) {
+    if (!h) return DCB_ERR_INVALID_ARGUMENT;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(cuda_stream);
+    if (cudaSetDevice(h->device) != cudaSuccess) { cudaGetLastError(); return fail(h, DCB_ERR_CUDA, "set device"); }
+    if (vertices && h->nv) DCB_TRY(h, cudaMemcpyAsync(vertices, h->V.p, sizeof(float) * 3 * h->nv, cudaMemcpyDeviceToDevice, s), "copy vertices");
+    if (faces && h->nf) DCB_TRY(h, cudaMemcpyAsync(faces, h->faces.p, sizeof(int32_t) * 4 * h->nf, cudaMemcpyDeviceToDevice, s), "copy faces");
+    return DCB_OK;
+}
+
+int dcb_copy_cells_to_host(dcb_handle h, int64_t* cell_linear_index, void* cuda_stream) {
+    if (!h || (!cell_linear_index && h->nv)) return DCB_ERR_INVALID_ARGUMENT;
+    if (h->nv == 0) return DCB_OK;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(cuda_stream);
+    if (cudaSetDevice(h->device) != cudaSuccess) { cudaGetLastError(); return fail(h, DCB_ERR_CUDA, "set device"); }
+    uint64_t* packed = reinterpret_cast<uint64_t*>(cell_linear_index);
+    DCB_TRY(h, cudaMemcpyAsync(packed, h->list.p, sizeof(uint64_t) * h->nv, cudaMemcpyDeviceToHost, s), "copy cells");
+    DCB_TRY(h, cudaStreamSynchronize(s), "copy cells");
+    for (int64_t r = 0; r < h->nv; ++r) {
+        const uint64_t p = packed[r];
+        const int64_t i = (int64_t)(p & 0x1FFFFF), j = (int64_t)((p >> 21) & 0x1FFFFF), k = (int64_t)(p >> 42);
+        cell_linear_index[r] = i + (int64_t)h->cx * (j + (int64_t)h->cy * k);
+    }
+    return DCB_OK;
+}
+
+}  // extern "C"

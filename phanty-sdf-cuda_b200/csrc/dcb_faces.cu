@@ -1,0 +1,250 @@
+// dcb_faces.cu — quad emission in the CPU backend's order and winding.
+//
+// The reference CPU loops (src/cpp/contouring.cpp:607-729) emit all X-edge quads, then Y,
+// then Z; within an axis the loops run i outermost and k innermost, and a quad is emitted
+// for every edge with s0*s1 < 0 whose four cells have vertices. Winding: swap c1 and c3
+// when (pb-pa)x(pd-pa) [fallback (pc-pa)x(pd-pa) if its squared norm < 1e-24] points
+// against gradientAt(p0) + gradientAt(p1) (contouring.cpp:624-641).
+// The reference GPU kernels emit in edge-major order instead (src/cuda/dc_cuda.cu:425-605).
+//
+// Order without a global sort: each face belongs to a "column" (axis, i, j) and the CPU
+// order is (axis, i, j, k). The vertex kernel counts faces per column (atomics); an
+// exclusive scan of the counts gives each column's start; the scatter places faces into
+// their column in arbitrary order; the ordering pass ranks each face by k inside its
+// column. Columns hold a handful of faces on real surfaces.
+// Winding is decided in FP32 with error margins; faces inside the margin are staged in
+// canonical order and re-decided from FP64 vertices (k_winding_fp64, dcb_vertex64.cu).
+#include "dcb_kernels.cuh"
+
+namespace dcb {
+
+// ---- exclusive scan of uint32 counts (three passes, 2048 items per block) --------------
+
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+__device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* s_warp, uint32_t& total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    uint32_t base = 0;
+    total = 0;
+#pragma unroll
+    for (int q = 0; q < kScanThreads / 32; ++q) {
+        const uint32_t s = s_warp[q];
+        if (q < warp) base += s;
+        total += s;
+    }
+    __syncthreads();
+    return base + incl - v;
+}
+
+__global__ void __launch_bounds__(kScanThreads)
+k_scan_partials(const uint32_t* __restrict__ in, long long n, uint32_t* partials) {
+    __shared__ uint32_t s_warp[kScanThreads / 32];
+    const long long base = (long long)blockIdx.x * kScanTile + (long long)threadIdx.x * kScanItems;
+    uint32_t s = 0;
+#pragma unroll
+    for (int q = 0; q < kScanItems; ++q) s += (base + q < n) ? in[base + q] : 0u;
+    uint32_t total;
+    block_excl_scan(s, s_warp, total);
+    if (threadIdx.x == 0) partials[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(kScanThreads)
+k_scan_single(uint32_t* partials, long long nb, unsigned long long* grand_total) {
+    __shared__ uint32_t s_warp[kScanThreads / 32];
+    uint32_t carry = 0;
+    for (long long c0 = 0; c0 < nb; c0 += kScanThreads) {
+        const long long idx = c0 + threadIdx.x;
+        const uint32_t v = idx < nb ? partials[idx] : 0u;
+        uint32_t total;
+        const uint32_t ex = block_excl_scan(v, s_warp, total);
+        if (idx < nb) partials[idx] = carry + ex;
+        carry += total;
+    }
+    if (threadIdx.x == 0) *grand_total = carry;
+}
+
+__global__ void __launch_bounds__(kScanThreads)
+k_scan_apply(const uint32_t* __restrict__ in, long long n, const uint32_t* __restrict__ partials,
+             uint32_t* __restrict__ out) {
+    __shared__ uint32_t s_warp[kScanThreads / 32];
+    const long long base = (long long)blockIdx.x * kScanTile + (long long)threadIdx.x * kScanItems;
+    uint32_t v[kScanItems];
+    uint32_t s = 0;
+#pragma unroll
+    for (int q = 0; q < kScanItems; ++q) { v[q] = (base + q < n) ? in[base + q] : 0u; s += v[q]; }
+    uint32_t total;
+    uint32_t run = block_excl_scan(s, s_warp, total) + partials[blockIdx.x];
+#pragma unroll
+    for (int q = 0; q < kScanItems; ++q) {
+        if (base + q < n) out[base + q] = run;
+        run += v[q];
+    }
+}
+
+cudaError_t launch_scan(const uint32_t* in, long long n, uint32_t* partials, uint32_t* out,
+                        unsigned long long* grand_total, cudaStream_t s) {
+    const long long nb = (n + kScanTile - 1) / kScanTile;
+    if (nb <= 0) return cudaSuccess;
+    k_scan_partials<<<(unsigned)nb, kScanThreads, 0, s>>>(in, n, partials);
+    k_scan_single<<<1, kScanThreads, 0, s>>>(partials, nb, grand_total);
+    k_scan_apply<<<(unsigned)nb, kScanThreads, 0, s>>>(in, n, partials, out);
+    return cudaGetLastError();
+}
+
+long long scan_partials_len(long long n) { return (n + kScanTile - 1) / kScanTile; }
+
+// ---- face scatter ----------------------------------------------------------------------
+
+
+// gradientAt (contouring.cpp:141-207) in FP32.
+__device__ __forceinline__ float3 grid_gradient32(const GridDesc& g, int i, int j, int k) {
+    const int im = max(i - 1, 0), ip = min(i + 1, g.nx - 1);
+    const int jm = max(j - 1, 0), jp = min(j + 1, g.ny - 1);
+    const int km = max(k - 1, 0), kp = min(k + 1, g.nz - 1);
+    float3 o = make_float3(0.f, 0.f, 0.f);
+    const float dx = pos_axis(g.ox, g.vx, ip) - pos_axis(g.ox, g.vx, im);
+    if (fabsf(dx) > 1e-12f) o.x = (__ldg(g.v + pidx(g, ip, j, k)) - __ldg(g.v + pidx(g, im, j, k))) / dx;
+    const float dy = pos_axis(g.oy, g.vy, jp) - pos_axis(g.oy, g.vy, jm);
+    if (fabsf(dy) > 1e-12f) o.y = (__ldg(g.v + pidx(g, i, jp, k)) - __ldg(g.v + pidx(g, i, jm, k))) / dy;
+    const float dz = pos_axis(g.oz, g.vz, kp) - pos_axis(g.oz, g.vz, km);
+    if (fabsf(dz) > 1e-12f) o.z = (__ldg(g.v + pidx(g, i, j, kp)) - __ldg(g.v + pidx(g, i, j, km))) / dz;
+    const float n2 = o.x * o.x + o.y * o.y + o.z * o.z;
+    if (n2 > 0.f) { const float r = rsqrtf(n2); o.x *= r; o.y *= r; o.z *= r; }
+    return o;
+}
+
+__device__ __forceinline__ float3 ldv(const float* V, uint32_t r) {
+    return make_float3(__ldg(V + 3 * (size_t)r), __ldg(V + 3 * (size_t)r + 1), __ldg(V + 3 * (size_t)r + 2));
+}
+__device__ __forceinline__ float3 sub3(float3 a, float3 b) { return make_float3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ float3 cross3(float3 a, float3 b) {
+    return make_float3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ float dot3(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+
+__global__ void __launch_bounds__(128)
+k_face_scatter(FaceParams P) {
+    const GridDesc& g = P.g;
+    const long long cxcy = (long long)g.cx * g.cy;
+    const float h2 = P.hmax * P.hmax;
+    for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < P.nactive;
+         r += (long long)gridDim.x * blockDim.x) {
+        const uint8_t fm = P.fmask[r];
+        if (!fm) continue;
+        int i, j, k;
+        unpack_cell(P.list[r], i, j, k);
+        const float3 g0 = grid_gradient32(g, i, j, k);
+#pragma unroll
+        for (int axis = 0; axis < 3; ++axis) {
+            if (!(fm & (1 << axis))) continue;
+            int c[4][3];
+            if (axis == 0) {
+                c[0][0] = i; c[0][1] = j - 1; c[0][2] = k - 1;  c[1][0] = i; c[1][1] = j; c[1][2] = k - 1;
+                c[3][0] = i; c[3][1] = j - 1; c[3][2] = k;
+            } else if (axis == 1) {
+                c[0][0] = i - 1; c[0][1] = j; c[0][2] = k - 1;  c[1][0] = i; c[1][1] = j; c[1][2] = k - 1;
+                c[3][0] = i - 1; c[3][1] = j; c[3][2] = k;
+            } else {
+                c[0][0] = i - 1; c[0][1] = j - 1; c[0][2] = k;  c[1][0] = i; c[1][1] = j - 1; c[1][2] = k;
+                c[3][0] = i - 1; c[3][1] = j; c[3][2] = k;
+            }
+            const uint32_t r0 = cell_rank(P.bits, P.super, g, c[0][0], c[0][1], c[0][2]);
+            const uint32_t r1 = cell_rank(P.bits, P.super, g, c[1][0], c[1][1], c[1][2]);
+            const uint32_t r2 = (uint32_t)r;
+            const uint32_t r3 = cell_rank(P.bits, P.super, g, c[3][0], c[3][1], c[3][2]);
+            const float3 g1 = grid_gradient32(g, i + (axis == 0), j + (axis == 1), k + (axis == 2));
+            const float3 gn = make_float3(g0.x + g1.x, g0.y + g1.y, g0.z + g1.z);
+            const float3 pa = ldv(P.V, r0), pb = ldv(P.V, r1), pc = ldv(P.V, r2), pd = ldv(P.V, r3);
+            float3 qn = cross3(sub3(pb, pa), sub3(pd, pa));
+            float qn2 = dot3(qn, qn);
+            // The reference switches to the other diagonal below |qn|^2 = 1e-24 (absolute):
+            // decide in FP64 near that switch and for near-degenerate quads.
+            const bool near_fallback = qn2 < 1e-6f * h2 * h2 || (qn2 > 1e-26f && qn2 < 1e-22f);
+            if (qn2 < 1e-24f) { qn = cross3(sub3(pc, pa), sub3(pd, pa)); qn2 = dot3(qn, qn); }
+            const float gn2 = dot3(gn, gn);
+            const float d = dot3(qn, gn);
+            const float qnl = sqrtf(qn2), gnl = sqrtf(gn2);
+            const bool uncertain = near_fallback || gn2 < 1e-4f ||
+                                   fabsf(d) <= (1e-3f * h2 + 1e-5f * qnl) * gnl;
+            bool swap = !uncertain && gn2 > 0.f && qn2 > 0.f && d < 0.f;
+            const long long col = axis * cxcy + (long long)i * g.cy + j;
+            const uint32_t slot = P.col_start[col] + atomicAdd(&P.col_fill[col], 1u);
+            P.stage_quad[slot] = swap ? make_int4((int)r0, (int)r3, (int)r2, (int)r1)
+                                      : make_int4((int)r0, (int)r1, (int)r2, (int)r3);
+            P.stage_key[slot] = make_uint2((uint32_t)k, (uint32_t)col);
+            if (uncertain) {
+                const unsigned int w = atomicAdd(P.wind_count, 1u);
+                if (w < P.wind_cap) {
+                    const uint64_t pk = pack_cell(i, j, k);
+                    P.wind_items[w] = make_uint4(slot, (uint32_t)axis, (uint32_t)pk, (uint32_t)(pk >> 32));
+                } else {
+                    set_error(P.err, kErrOverflow);
+                }
+                // request the FP64 vertex of each of the four cells once
+                const uint32_t rq[4] = {r0, r1, r2, r3};
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    if (atomicCAS(&P.v64_index[rq[q]], -1, -2) == -1) {
+                        const unsigned int v = atomicAdd(P.v64_count, 1u);
+                        if (v < P.v64_cap) {
+                            P.v64_cells[v] = rq[q];
+                            P.v64_index[rq[q]] = (int)v;
+                        } else {
+                            set_error(P.err, kErrOverflow);
+                        }
+                    }
+                }
+            }
+        }
+    }
+}
+
+cudaError_t launch_face_scatter(const FaceParams& P, int num_sms, cudaStream_t s) {
+    if (P.nactive <= 0) return cudaSuccess;
+    long long blocks = (P.nactive + 127) / 128;
+    const long long cap = (long long)num_sms * 16;
+    if (blocks > cap) blocks = cap;
+    k_face_scatter<<<(unsigned)blocks, 128, 0, s>>>(P);
+    return cudaGetLastError();
+}
+
+// ---- in-column ordering ----------------------------------------------------------------
+
+__global__ void __launch_bounds__(256)
+k_face_order(const int4* __restrict__ stage_quad, const uint2* __restrict__ stage_key,
+             const uint32_t* __restrict__ col_start, const uint32_t* __restrict__ col_count,
+             const unsigned long long* __restrict__ nfaces, int4* __restrict__ faces) {
+    const long long nf = (long long)*nfaces;
+    for (long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x; s < nf;
+         s += (long long)gridDim.x * blockDim.x) {
+        const uint2 key = stage_key[s];
+        const uint32_t start = col_start[key.y];
+        const uint32_t cnt = col_count[key.y];
+        uint32_t rank = 0;
+        for (uint32_t q = 0; q < cnt; ++q) rank += (stage_key[start + q].x < key.x) ? 1u : 0u;
+        faces[start + rank] = stage_quad[s];
+    }
+}
+
+cudaError_t launch_face_order(const int4* stage_quad, const uint2* stage_key, const uint32_t* col_start,
+                              const uint32_t* col_count, const unsigned long long* nfaces, int4* faces,
+                              long long max_faces, int num_sms, cudaStream_t s) {
+    if (max_faces <= 0) return cudaSuccess;
+    long long blocks = (max_faces + 255) / 256;
+    const long long cap = (long long)num_sms * 16;
+    if (blocks > cap) blocks = cap;
+    k_face_order<<<(unsigned)blocks, 256, 0, s>>>(stage_quad, stage_key, col_start, col_count, nfaces, faces);
+    return cudaGetLastError();
+}
+
+}  // namespace dcb

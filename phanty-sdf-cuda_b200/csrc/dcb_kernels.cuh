@@ -1,0 +1,121 @@
+// dcb_kernels.cuh — parameter blocks and launchers of the dual-contouring kernels.
+#pragma once
+#include "dcb_common.cuh"
+
+namespace dcb {
+
+struct MarkParams {
+    GridDesc g;
+    int R;                         // cell rows per tile (point rows = R + 1 <= 8)
+    int KZ;                        // cell planes per tile
+    int nxt;                       // x-tiles of 1024 cells per row
+    uint32_t* bits;                // [cy*cz][W]
+    uint32_t* seg_count;           // [cz*cy*nxt] active cells per (plane, row, x-tile)
+    int vec4;                      // rows are 16-byte aligned and nx % 4 == 0
+};
+cudaError_t launch_mark(const MarkParams& P, cudaStream_t s);
+int mark_tile_words();
+int mark_max_rows();
+
+struct ExpandParams {
+    GridDesc g;
+    int nxt;
+    const uint32_t* bits;
+    const uint32_t* seg_count;
+    const uint32_t* seg_start;     // exclusive scan of seg_count
+    uint32_t* super;               // [cy*cz][W8]
+    uint64_t* list;                // [active]
+};
+cudaError_t launch_expand(const ExpandParams& P, int num_sms, cudaStream_t s);
+
+struct EdgeParams {
+    GridDesc g;
+    const uint64_t* list;
+    long long nactive;
+    float4* en;                     // [3*active]: averaged normal of owned edge (cell, axis)
+    uint8_t* eflags;                // bit a: edge a averaged; bit 3+a: its normal is ill-conditioned
+    uint8_t* fmask;                 // bit a: cell owns a face on its min-corner edge a
+    uint32_t* col_count;            // [3][cx*cy]: a*cx*cy + i*cy + j
+};
+cudaError_t launch_edge_normals(const EdgeParams& P, int num_sms, cudaStream_t s);
+
+struct QefParams {
+    GridDesc g;
+    const uint64_t* list;
+    long long nactive;
+    const uint32_t* bits;
+    const uint32_t* super;
+    const float4* en;
+    const uint8_t* eflags;
+    float* V;
+    uint32_t* esc_list;
+    unsigned int* esc_count;
+    uint32_t* hard_list;            // cells not certified rank 1
+    float4* hard_data;              // [3 per hard cell]: A^T A (6), A^T b (3), centroid (3)
+    unsigned int* hard_count;
+    unsigned long long* rank_hist;  // [4]
+    float thr;
+    float band;
+    float cond_max;
+    int force64;
+};
+cudaError_t launch_cell_qef(const QefParams& P, int num_sms, cudaStream_t s);
+cudaError_t launch_cell_jacobi(const QefParams& P, long long max_items, int num_sms, cudaStream_t s);
+
+struct Vertex64Params {
+    GridDesc g;
+    const uint64_t* list;
+    const uint32_t* cells;          // ranks of the cells to solve
+    const unsigned int* count;
+    unsigned int cap;               // entries in cells; count may exceed it on overflow
+    float* Vf;                      // optional: float vertex at [rank]
+    double* V64;                    // optional: double vertex at [item]
+    double thr;
+};
+cudaError_t launch_vertex_fp64(const Vertex64Params& P, long long max_items, int num_sms, cudaStream_t s);
+
+struct Winding64Params {
+    GridDesc g;
+    const uint4* items;             // {staging slot, axis, packed cell lo, packed cell hi}
+    const unsigned int* count;
+    unsigned int cap;
+    int4* quads;                    // staging quads (rewritten in place)
+    const int* v64_index;           // [rank] -> item in V64, or -1
+    const double* V64;
+    int* err;
+};
+cudaError_t launch_winding_fp64(const Winding64Params& P, long long max_items, int num_sms, cudaStream_t s);
+
+cudaError_t launch_scan(const uint32_t* in, long long n, uint32_t* partials, uint32_t* out,
+                        unsigned long long* grand_total, cudaStream_t s);
+long long scan_partials_len(long long n);
+
+struct FaceParams {
+    GridDesc g;
+    const uint64_t* list;
+    long long nactive;
+    const uint8_t* fmask;
+    const float* V;
+    const uint32_t* bits;
+    const uint32_t* super;
+    const uint32_t* col_start;     // [3][cx*cy]
+    const uint32_t* col_count;
+    uint32_t* col_fill;
+    int4* stage_quad;
+    uint2* stage_key;              // {k, column}
+    uint4* wind_items;             // {slot, axis, packed lo, packed hi}
+    unsigned int* wind_count;
+    unsigned long long wind_cap;
+    int* v64_index;                // [rank] -> FP64 vertex slot (-1 none, -2 being claimed)
+    uint32_t* v64_cells;           // cells whose FP64 vertex the windings need
+    unsigned int* v64_count;
+    unsigned long long v64_cap;
+    int* err;
+    float hmax;                    // largest cell width (world units)
+};
+cudaError_t launch_face_scatter(const FaceParams& P, int num_sms, cudaStream_t s);
+cudaError_t launch_face_order(const int4* stage_quad, const uint2* stage_key, const uint32_t* col_start,
+                              const uint32_t* col_count, const unsigned long long* nfaces, int4* faces,
+                              long long max_faces, int num_sms, cudaStream_t s);
+
+}  // namespace dcb

@@ -1,0 +1,191 @@
+// dcb_mark.cu — markActiveCells and the order-preserving active-cell compaction.
+//
+// Semantics (reference CPU backend): a cell is active iff some corner < 0 and some corner
+// > 0 (Cell::Cell, src/cpp/Cell.cpp:57-77); vertex index = rank of the cell among active
+// cells in linear (k, j, i) order (extract_mesh_from_cells, src/cpp/contouring.cpp:513-524).
+// The reference GPU path uses one thread per cell, a byte flag per cell and a Thrust
+// copy_if (src/cuda/dc_cuda.cu:241-281, 701-712).
+//
+// k_mark_zmarch: a CTA owns a tile of R cell rows x 1024 cells along x and marches through
+// a chunk of KZ cell planes. Warp w streams point row j0+w of every point plane once
+// (float4 loads, the next plane prefetched into registers while the current one is
+// reduced), turns it into a negative-bit word and a positive-bit word per 32 points
+// (nibble + shuffle), and the cell words of plane k are bitwise ORs of the point words of
+// rows j, j+1 in planes k, k+1 and their one-bit shift along x. Each grid value crosses
+// HBM once and the SM (R+1)/R times. Outputs: the active bit words and the number of
+// active cells of every (plane, row, x-tile) segment, in linear order.
+// A scan of the segment counts gives each segment's first rank; k_expand_ranks then writes
+// the 256-cell super-word ranks and the packed active-cell list.
+#include "dcb_kernels.cuh"
+
+namespace dcb {
+
+constexpr int kMarkWarps = 8;          // point rows per tile (R + 1 <= 8)
+constexpr int kTileWords = 32;         // cell words per x-tile (1024 cells)
+constexpr int kPtWords = kTileWords + 1;
+constexpr int kChunks = (kPtWords + 3) / 4;   // 128-point chunks per point-row segment
+
+struct RowRegs {
+    float4 v[kChunks];
+};
+
+// Load the kPtWords*32 points of one point-row segment starting at x0 into registers.
+// VEC4: lane l holds points x0+128c+4l..+3 of chunk c; scalar: component q holds point
+// x0+128c+32q+l.
+template <bool VEC4>
+__device__ __forceinline__ void load_row(const float* __restrict__ row, int x0, int nx, int lane, RowRegs& R) {
+#pragma unroll
+    for (int c = 0; c < kChunks; ++c) {
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (VEC4) {
+            const int x = x0 + 128 * c + 4 * lane;
+            if (x < nx) v = __ldg(reinterpret_cast<const float4*>(row + x));
+        } else {
+            const int x = x0 + 128 * c + lane;
+            if (x < nx) v.x = __ldg(row + x);
+            if (x + 32 < nx) v.y = __ldg(row + x + 32);
+            if (x + 64 < nx) v.z = __ldg(row + x + 64);
+            if (x + 96 < nx) v.w = __ldg(row + x + 96);
+        }
+        R.v[c] = v;
+    }
+}
+
+// Negative / positive bit words of the loaded segment (word q covers points x0+32q..+31).
+template <bool VEC4>
+__device__ __forceinline__ void row_words(const RowRegs& R, int lane, uint32_t* nw, uint32_t* pw) {
+#pragma unroll
+    for (int c = 0; c < kChunks; ++c) {
+        const float4 v = R.v[c];
+        if (VEC4) {
+            uint32_t n = (v.x < 0.f ? 1u : 0u) | (v.y < 0.f ? 2u : 0u) | (v.z < 0.f ? 4u : 0u) | (v.w < 0.f ? 8u : 0u);
+            uint32_t p = (v.x > 0.f ? 1u : 0u) | (v.y > 0.f ? 2u : 0u) | (v.z > 0.f ? 4u : 0u) | (v.w > 0.f ? 8u : 0u);
+            const int sh = 4 * (lane & 7);
+            n <<= sh;
+            p <<= sh;
+#pragma unroll
+            for (int o = 1; o < 8; o <<= 1) {
+                n |= __shfl_xor_sync(0xffffffffu, n, o);
+                p |= __shfl_xor_sync(0xffffffffu, p, o);
+            }
+            const int w = 4 * c + (lane >> 3);
+            if ((lane & 7) == 0 && w < kPtWords) { nw[w] = n; pw[w] = p; }
+        } else {
+            const float q[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+            for (int s = 0; s < 4; ++s) {
+                const uint32_t n = __ballot_sync(0xffffffffu, q[s] < 0.f);
+                const uint32_t p = __ballot_sync(0xffffffffu, q[s] > 0.f);
+                const int w = 4 * c + s;
+                if (lane == 0 && w < kPtWords) { nw[w] = n; pw[w] = p; }
+            }
+        }
+    }
+}
+
+template <bool VEC4>
+__global__ void __launch_bounds__(kMarkWarps * 32)
+k_mark_zmarch(MarkParams P) {
+    __shared__ uint32_t s_nw[2][kMarkWarps][kPtWords];
+    __shared__ uint32_t s_pw[2][kMarkWarps][kPtWords];
+    const GridDesc& g = P.g;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int xt = blockIdx.x;                 // x-tile
+    const int j0 = blockIdx.y * P.R;           // first cell row
+    const int kb = blockIdx.z * P.KZ;          // first cell plane
+    const int rows = min(P.R, g.cy - j0);
+    const int ke = min(g.cz, kb + P.KZ);
+    const int x0 = xt * kTileWords * 32;       // first point / cell of the tile
+    const bool loader = warp <= rows;          // point rows j0..j0+rows
+    const float* base = g.v + (int64_t)(j0 + (loader ? warp : 0)) * g.nx;
+    const int64_t plane = (int64_t)g.nx * g.ny;
+
+    RowRegs cur;
+    if (loader) {
+        load_row<VEC4>(base + (int64_t)kb * plane, x0, g.nx, lane, cur);
+        row_words<VEC4>(cur, lane, s_nw[kb & 1][warp], s_pw[kb & 1][warp]);
+        load_row<VEC4>(base + (int64_t)(kb + 1) * plane, x0, g.nx, lane, cur);
+    }
+    const int wglob = xt * kTileWords + lane;  // this lane's cell word in the row
+    const int valid = g.cx - 32 * wglob;
+    const uint32_t vmask = valid >= 32 ? 0xffffffffu : (valid > 0 ? ((1u << valid) - 1u) : 0u);
+
+    for (int k = kb; k < ke; ++k) {
+        const int p1 = (k + 1) & 1, p0 = k & 1;
+        if (loader) {
+            row_words<VEC4>(cur, lane, s_nw[p1][warp], s_pw[p1][warp]);
+            if (k + 2 <= ke) load_row<VEC4>(base + (int64_t)(k + 2) * plane, x0, g.nx, lane, cur);
+        }
+        __syncthreads();
+        if (warp < rows) {
+            const int r = warp;
+            const uint32_t n0 = s_nw[p0][r][lane] | s_nw[p0][r + 1][lane] | s_nw[p1][r][lane] | s_nw[p1][r + 1][lane];
+            const uint32_t n1 = s_nw[p0][r][lane + 1] | s_nw[p0][r + 1][lane + 1] | s_nw[p1][r][lane + 1] | s_nw[p1][r + 1][lane + 1];
+            const uint32_t q0 = s_pw[p0][r][lane] | s_pw[p0][r + 1][lane] | s_pw[p1][r][lane] | s_pw[p1][r + 1][lane];
+            const uint32_t q1 = s_pw[p0][r][lane + 1] | s_pw[p0][r + 1][lane + 1] | s_pw[p1][r][lane + 1] | s_pw[p1][r + 1][lane + 1];
+            const uint32_t act = (n0 | (n0 >> 1) | (n1 << 31)) & (q0 | (q0 >> 1) | (q1 << 31)) & vmask;
+            const int64_t row = (int64_t)(j0 + r) + (int64_t)g.cy * k;
+            if (wglob < g.W) P.bits[row * g.W + wglob] = act;
+            uint32_t cnt = __popc(act);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+            if (lane == 0) P.seg_count[row * P.nxt + xt] = cnt;
+        }
+        __syncthreads();
+    }
+}
+
+// Warp per (row, x-tile) segment: global ranks of its super words and the packed list.
+__global__ void __launch_bounds__(256)
+k_expand_ranks(ExpandParams P) {
+    const GridDesc& g = P.g;
+    const int lane = threadIdx.x & 31;
+    const long long nseg = (long long)g.cy * g.cz * P.nxt;
+    for (long long s = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < nseg;
+         s += ((long long)gridDim.x * blockDim.x) >> 5) {
+        if (P.seg_count[s] == 0) continue;           // warp-uniform
+        const long long row = s / P.nxt;
+        const int xt = (int)(s - row * P.nxt);
+        const int w = xt * kTileWords + lane;
+        const uint32_t act = (w < g.W) ? P.bits[row * g.W + w] : 0u;
+        const uint32_t c = __popc(act);
+        uint32_t incl = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        const uint32_t first = P.seg_start[s] + incl - c;
+        if (w < g.W && (w & 7) == 0) P.super[row * g.W8 + (w >> 3)] = first;
+        const int j = (int)(row % g.cy), k = (int)(row / g.cy);
+        uint32_t m = act, q = 0;
+        while (m) {
+            const int b = __ffs(m) - 1;
+            m &= m - 1;
+            P.list[first + q] = pack_cell(32 * w + b, j, k);
+            ++q;
+        }
+    }
+}
+
+cudaError_t launch_mark(const MarkParams& P, cudaStream_t s) {
+    dim3 grid((unsigned)P.nxt, (unsigned)((P.g.cy + P.R - 1) / P.R), (unsigned)((P.g.cz + P.KZ - 1) / P.KZ));
+    if (P.vec4) k_mark_zmarch<true><<<grid, kMarkWarps * 32, 0, s>>>(P);
+    else        k_mark_zmarch<false><<<grid, kMarkWarps * 32, 0, s>>>(P);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_expand(const ExpandParams& P, int num_sms, cudaStream_t s) {
+    const long long nseg = (long long)P.g.cy * P.g.cz * P.nxt;
+    long long blocks = (nseg * 32 + 255) / 256;
+    const long long cap = (long long)num_sms * 32;
+    if (blocks > cap) blocks = cap;
+    if (blocks < 1) blocks = 1;
+    k_expand_ranks<<<(unsigned)blocks, 256, 0, s>>>(P);
+    return cudaGetLastError();
+}
+
+int mark_tile_words() { return kTileWords; }
+int mark_max_rows() { return kMarkWarps - 1; }
+
+}  // namespace dcb

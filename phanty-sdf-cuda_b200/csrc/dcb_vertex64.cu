@@ -1,0 +1,326 @@
+// dcb_vertex64.cu — FP64 vertices for cells the FP32 path does not trust, and FP64
+// re-decision of uncertain face orientations. Compiled with --fmad=false: every double
+// operation is rounded as written, like the reference's x86-64 CPU build, so a cell on this
+// path reproduces the CPU backend's double arithmetic (Cell.cpp:57-361,
+// hermite_update.cpp:171-438, contouring.cpp:141-207, 624-641).
+//
+// One warp per cell: lane e (< 12) forms the Hermite sample of edge e and, when the edge is
+// averaged, the three neighbours' own samples of that edge; lane 0 then accumulates A^T A,
+// A^T b and the centroid in edge order (the CPU's std::map order), so the summation order
+// is the CPU's, and runs the Jacobi eigen-decomposition and the truncated pseudo-inverse.
+#include "dcb_kernels.cuh"
+
+namespace dcb {
+
+namespace f64 {
+
+struct Cell64 {
+    double cs[8];
+    double cp[8][3];
+};
+
+__device__ __forceinline__ double sq3(const double* a) { return a[0] * a[0] + a[1] * a[1] + a[2] * a[2]; }
+__device__ __forceinline__ void normalize3(double* a) {
+    const double z = sq3(a);
+    if (z > 0.0) { const double s = sqrt(z); a[0] /= s; a[1] /= s; a[2] /= s; }
+}
+
+__device__ void load_cell(const GridDesc& g, int i, int j, int k, Cell64& C) {
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        const int gi = i + corner_dx(c), gj = j + corner_dy(c), gk = k + corner_dz(c);
+        C.cs[c] = (double)__ldg(g.v + pidx(g, gi, gj, gk));
+        C.cp[c][0] = (double)pos_axis(g.ox, g.vx, gi);
+        C.cp[c][1] = (double)pos_axis(g.oy, g.vy, gj);
+        C.cp[c][2] = (double)pos_axis(g.oz, g.vz, gk);
+    }
+}
+
+__device__ bool active(const Cell64& C) {
+    bool neg = false, pos = false;
+    for (int c = 0; c < 8; ++c) { if (C.cs[c] < 0) neg = true; if (C.cs[c] > 0) pos = true; }
+    return neg && pos;
+}
+
+// gradientAtPointUsingTrilinear (Cell.cpp:80-155).
+__device__ void tri_grad(const Cell64& C, const double p[3], double g[3]) {
+    const double S000 = C.cs[0], S100 = C.cs[1], S110 = C.cs[2], S010 = C.cs[3];
+    const double S001 = C.cs[4], S101 = C.cs[5], S111 = C.cs[6], S011 = C.cs[7];
+    const double x0 = C.cp[0][0], x1 = C.cp[1][0];
+    const double y0 = C.cp[0][1], y1 = C.cp[3][1];
+    const double z0 = C.cp[0][2], z1 = C.cp[4][2];
+    const double dx = x1 - x0, dy = y1 - y0, dz = z1 - z0;
+    const double eps = 1e-12;
+    double u = 0.5, v = 0.5, w = 0.5;
+    if (fabs(dx) > eps) u = (p[0] - x0) / dx;
+    if (fabs(dy) > eps) v = (p[1] - y0) / dy;
+    if (fabs(dz) > eps) w = (p[2] - z0) / dz;
+    u = fmax(0.0, fmin(1.0, u));
+    v = fmax(0.0, fmin(1.0, v));
+    w = fmax(0.0, fmin(1.0, w));
+    const double omu = 1.0 - u, omv = 1.0 - v, omw = 1.0 - w;
+    const double df_du = (S100 - S000) * omv * omw + (S110 - S010) * v * omw
+                       + (S101 - S001) * omv * w + (S111 - S011) * v * w;
+    const double df_dv = (S010 - S000) * omu * omw + (S110 - S100) * u * omw
+                       + (S011 - S001) * omu * w + (S111 - S101) * u * w;
+    const double df_dw = (S001 - S000) * omu * omv + (S101 - S100) * u * omv
+                       + (S011 - S010) * omu * v + (S111 - S110) * u * v;
+    g[0] = g[1] = g[2] = 0.0;
+    if (fabs(dx) > eps) g[0] = df_du / dx;
+    if (fabs(dy) > eps) g[1] = df_dv / dy;
+    if (fabs(dz) > eps) g[2] = df_dw / dz;
+}
+
+// Hermite sample of local edge e of a cell (Cell.cpp:176-212). Returns false if no crossing.
+__device__ bool hermite(const Cell64& C, int e, double p[3], double n[3]) {
+    const int a = edge_a(e), b = edge_b(e);
+    const double fa = C.cs[a], fb = C.cs[b];
+    if (fa * fb > 0.0) return false;
+    const double t = (fa - 0.0) / (fa - fb + 1e-16);
+    for (int d = 0; d < 3; ++d) p[d] = (1.0 - t) * C.cp[a][d] + t * C.cp[b][d];
+    tri_grad(C, p, n);
+    if (sqrt(sq3(n)) > 0.0) normalize3(n);
+    return true;
+}
+
+// get_edge_idx_from_grid_vertices (hermite_update.cpp:41-91).
+__device__ int edge_of(int ci, int cj, int ck, int i0, int j0, int k0, int i1, int j1, int k1) {
+    const int di0 = i0 - ci, dj0 = j0 - cj, dk0 = k0 - ck;
+    const int di1 = i1 - ci, dj1 = j1 - cj, dk1 = k1 - ck;
+    for (int e = 0; e < 12; ++e) {
+        const int a = edge_a(e), b = edge_b(e);
+        const bool fwd = di0 == corner_dx(a) && dj0 == corner_dy(a) && dk0 == corner_dz(a) &&
+                         di1 == corner_dx(b) && dj1 == corner_dy(b) && dk1 == corner_dz(b);
+        const bool bwd = di0 == corner_dx(b) && dj0 == corner_dy(b) && dk0 == corner_dz(b) &&
+                         di1 == corner_dx(a) && dj1 == corner_dy(a) && dk1 == corner_dz(a);
+        if (fwd || bwd) return e;
+    }
+    return -1;
+}
+
+// Hermite sample of edge e of cell (i,j,k) with the 4-cell averaged normal when the edge
+// qualifies (hermite_update.cpp:171-438).
+__device__ bool edge_sample(const GridDesc& g, const Cell64& C, int i, int j, int k, int e, double p[3], double n[3]) {
+    if (!hermite(C, e, p, n)) return false;
+    const int a = edge_a(e), b = edge_b(e);
+    const int Pa[3] = {i + corner_dx(a), j + corner_dy(a), k + corner_dz(a)};
+    const int Pb[3] = {i + corner_dx(b), j + corner_dy(b), k + corner_dz(b)};
+    int Pm[3], PM[3];
+    for (int d = 0; d < 3; ++d) { Pm[d] = min(Pa[d], Pb[d]); PM[d] = max(Pa[d], Pb[d]); }
+    const bool in0 = Pm[0] > 0 && Pm[0] < g.nx - 1 && Pm[1] > 0 && Pm[1] < g.ny - 1 && Pm[2] > 0 && Pm[2] < g.nz - 1;
+    const bool in1 = PM[0] > 0 && PM[0] < g.nx - 1 && PM[1] > 0 && PM[1] < g.ny - 1 && PM[2] > 0 && PM[2] < g.nz - 1;
+    if (!in0 && !in1) return true;
+    const int axis = Pa[0] != Pb[0] ? 0 : (Pa[1] != Pb[1] ? 1 : 2);
+    const int d1 = axis == 0 ? 1 : 0;
+    const int d2 = axis == 2 ? 1 : 2;
+    double nq[4][3];
+    for (int q = 0; q < 4; ++q) {
+        int cc[3] = {Pm[0], Pm[1], Pm[2]};
+        if (q & 1) cc[d1] -= 1;
+        if (q & 2) cc[d2] -= 1;
+        if (cc[0] == i && cc[1] == j && cc[2] == k) {
+            nq[q][0] = n[0]; nq[q][1] = n[1]; nq[q][2] = n[2];
+            continue;
+        }
+        Cell64 X;
+        load_cell(g, cc[0], cc[1], cc[2], X);
+        if (!active(X)) return true;
+        const int ex = edge_of(cc[0], cc[1], cc[2], Pm[0], Pm[1], Pm[2], PM[0], PM[1], PM[2]);
+        double px[3];
+        if (ex < 0 || !hermite(X, ex, px, nq[q])) return true;
+    }
+    double acc[3] = {0.0, 0.0, 0.0};
+    for (int q = 0; q < 4; ++q) {
+        if (sqrt(sq3(nq[q])) > 0) { acc[0] += nq[q][0]; acc[1] += nq[q][1]; acc[2] += nq[q][2]; }
+    }
+    normalize3(acc);
+    n[0] = acc[0]; n[1] = acc[1]; n[2] = acc[2];
+    return true;
+}
+
+// Cyclic Jacobi, same sweep order and stopping rule as the CPU restatement.
+__device__ void jacobi3(double a[3][3], double V[3][3]) {
+    for (int r = 0; r < 3; ++r) for (int c = 0; c < 3; ++c) V[r][c] = (r == c) ? 1.0 : 0.0;
+    for (int sweep = 0; sweep < 64; ++sweep) {
+        const double off = a[0][1] * a[0][1] + a[0][2] * a[0][2] + a[1][2] * a[1][2];
+        const double diag = a[0][0] * a[0][0] + a[1][1] * a[1][1] + a[2][2] * a[2][2];
+        if (off <= 1e-36 * diag || off == 0.0) break;
+        for (int p = 0; p < 2; ++p) {
+            for (int q = p + 1; q < 3; ++q) {
+                const double apq = a[p][q];
+                if (apq == 0.0) continue;
+                const double theta = (a[q][q] - a[p][p]) / (2.0 * apq);
+                const double t = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+                const double c = 1.0 / sqrt(t * t + 1.0), s = t * c;
+                for (int r = 0; r < 3; ++r) {
+                    const double arp = a[r][p], arq = a[r][q];
+                    a[r][p] = c * arp - s * arq;
+                    a[r][q] = s * arp + c * arq;
+                }
+                for (int r = 0; r < 3; ++r) {
+                    const double apr = a[p][r], aqr = a[q][r];
+                    a[p][r] = c * apr - s * aqr;
+                    a[q][r] = s * apr + c * aqr;
+                }
+                for (int r = 0; r < 3; ++r) {
+                    const double vrp = V[r][p], vrq = V[r][q];
+                    V[r][p] = c * vrp - s * vrq;
+                    V[r][q] = s * vrp + c * vrq;
+                }
+            }
+        }
+    }
+}
+
+// FP64 vertex of active cell (i,j,k), computed by the whole warp; valid in lane 0.
+__device__ void cell_vertex_warp(const GridDesc& g, int i, int j, int k, double thr, double out[3]) {
+    const int lane = threadIdx.x & 31;
+    Cell64 C;
+    load_cell(g, i, j, k, C);
+    double p[3] = {0, 0, 0}, n[3] = {0, 0, 0};
+    const bool has = lane < 12 ? edge_sample(g, C, i, j, k, lane, p, n) : false;
+    const uint32_t mask = __ballot_sync(0xffffffffu, has);
+    double ATA[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, ATb[3] = {0, 0, 0}, c[3] = {0, 0, 0};
+    int m = 0;
+    for (int e = 0; e < 12; ++e) {           // edge order = the CPU's std::map order
+        double pe[3], ne[3];
+        for (int d = 0; d < 3; ++d) {
+            pe[d] = __shfl_sync(0xffffffffu, p[d], e);
+            ne[d] = __shfl_sync(0xffffffffu, n[d], e);
+        }
+        if (!(mask & (1u << e))) continue;
+        if (sqrt(sq3(ne)) > 0.0) normalize3(ne);
+        const double bb = ne[0] * pe[0] + ne[1] * pe[1] + ne[2] * pe[2];
+        for (int r = 0; r < 3; ++r) {
+            for (int s = 0; s < 3; ++s) ATA[r][s] += ne[r] * ne[s];
+            ATb[r] += ne[r] * bb;
+        }
+        for (int d = 0; d < 3; ++d) c[d] += pe[d];
+        ++m;
+    }
+    if (lane != 0) return;
+    for (int d = 0; d < 3; ++d) c[d] /= double(m);
+    double A[3][3], V[3][3];
+    for (int r = 0; r < 3; ++r) for (int s = 0; s < 3; ++s) A[r][s] = ATA[r][s];
+    jacobi3(A, V);
+    const double lam[3] = {A[0][0], A[1][1], A[2][2]};
+    double rhs[3];
+    for (int r = 0; r < 3; ++r) rhs[r] = ATb[r] - (ATA[r][0] * c[0] + ATA[r][1] * c[1] + ATA[r][2] * c[2]);
+    double x[3] = {c[0], c[1], c[2]};
+    for (int q = 0; q < 3; ++q) {
+        const double sv = fabs(lam[q]);
+        if (sv > thr) {
+            const double proj = V[0][q] * rhs[0] + V[1][q] * rhs[1] + V[2][q] * rhs[2];
+            const double coef = proj / sv;
+            for (int d = 0; d < 3; ++d) x[d] += V[d][q] * coef;
+        }
+    }
+    out[0] = x[0]; out[1] = x[1]; out[2] = x[2];
+}
+
+// gradientAt (contouring.cpp:141-207).
+__device__ void grid_gradient(const GridDesc& g, int i, int j, int k, double out[3]) {
+    const int im = max(i - 1, 0), ip = min(i + 1, g.nx - 1);
+    const int jm = max(j - 1, 0), jp = min(j + 1, g.ny - 1);
+    const int km = max(k - 1, 0), kp = min(k + 1, g.nz - 1);
+    out[0] = out[1] = out[2] = 0.0;
+    const double dx = (double)pos_axis(g.ox, g.vx, ip) - (double)pos_axis(g.ox, g.vx, im);
+    if (fabs(dx) > 1e-12) out[0] = ((double)__ldg(g.v + pidx(g, ip, j, k)) - (double)__ldg(g.v + pidx(g, im, j, k))) / dx;
+    const double dy = (double)pos_axis(g.oy, g.vy, jp) - (double)pos_axis(g.oy, g.vy, jm);
+    if (fabs(dy) > 1e-12) out[1] = ((double)__ldg(g.v + pidx(g, i, jp, k)) - (double)__ldg(g.v + pidx(g, i, jm, k))) / dy;
+    const double dz = (double)pos_axis(g.oz, g.vz, kp) - (double)pos_axis(g.oz, g.vz, km);
+    if (fabs(dz) > 1e-12) out[2] = ((double)__ldg(g.v + pidx(g, i, j, kp)) - (double)__ldg(g.v + pidx(g, i, j, km))) / dz;
+    const double nrm = sqrt(sq3(out));
+    if (nrm > 0.0) { out[0] /= nrm; out[1] /= nrm; out[2] /= nrm; }
+}
+
+}  // namespace f64
+
+// Warp per listed cell. Writes the float vertex (Vf[rank]) and/or the double one (V64[t]).
+__global__ void __launch_bounds__(128)
+k_vertex_fp64(Vertex64Params P) {
+    const unsigned int n = min(*P.count, P.cap);
+    const int lane = threadIdx.x & 31;
+    const unsigned int warps = (gridDim.x * blockDim.x) >> 5;
+    for (unsigned int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < n; t += warps) {
+        const uint32_t r = P.cells[t];
+        int i, j, k;
+        unpack_cell(P.list[r], i, j, k);
+        double x[3];
+        f64::cell_vertex_warp(P.g, i, j, k, P.thr, x);
+        if (lane == 0) {
+            if (P.Vf) {
+                P.Vf[3 * (size_t)r + 0] = (float)x[0];
+                P.Vf[3 * (size_t)r + 1] = (float)x[1];
+                P.Vf[3 * (size_t)r + 2] = (float)x[2];
+            }
+            if (P.V64) {
+                P.V64[3 * (size_t)t + 0] = x[0];
+                P.V64[3 * (size_t)t + 1] = x[1];
+                P.V64[3 * (size_t)t + 2] = x[2];
+            }
+        }
+    }
+}
+
+cudaError_t launch_vertex_fp64(const Vertex64Params& P, long long max_items, int num_sms, cudaStream_t s) {
+    if (max_items <= 0) return cudaSuccess;
+    long long blocks = (max_items * 32 + 127) / 128;
+    const long long cap = (long long)num_sms * 16;
+    if (blocks > cap) blocks = cap;
+    k_vertex_fp64<<<(unsigned)blocks, 128, 0, s>>>(P);
+    return cudaGetLastError();
+}
+
+// Thread per uncertain face: orientation exactly as extract_mesh_from_cells decides it
+// (contouring.cpp:624-641) from the FP64 vertices of its four cells and FP64 gradients.
+// Uncertain faces were staged in canonical order c0, c1, c2, c3.
+__global__ void __launch_bounds__(128)
+k_winding_fp64(Winding64Params P) {
+    const unsigned int n = min(*P.count, P.cap);
+    for (unsigned int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const uint4 it = P.items[t];
+        const int axis = (int)it.y;
+        int i, j, k;
+        unpack_cell(((uint64_t)it.w << 32) | it.z, i, j, k);
+        const int4 q4 = P.quads[it.x];
+        const int rr[4] = {q4.x, q4.y, q4.z, q4.w};
+        double pv[4][3];
+        bool ok = true;
+        for (int q = 0; q < 4; ++q) {
+            const int idx = P.v64_index[rr[q]];
+            if (idx < 0) { ok = false; break; }
+            for (int d = 0; d < 3; ++d) pv[q][d] = P.V64[3 * (size_t)idx + d];
+        }
+        if (!ok) { set_error(P.err, kErrInternal); continue; }
+        double g0[3], g1[3];
+        f64::grid_gradient(P.g, i, j, k, g0);
+        f64::grid_gradient(P.g, i + (axis == 0), j + (axis == 1), k + (axis == 2), g1);
+        const double gn[3] = {g0[0] + g1[0], g0[1] + g1[1], g0[2] + g1[2]};
+        const double ba[3] = {pv[1][0] - pv[0][0], pv[1][1] - pv[0][1], pv[1][2] - pv[0][2]};
+        const double da[3] = {pv[3][0] - pv[0][0], pv[3][1] - pv[0][1], pv[3][2] - pv[0][2]};
+        double qn[3] = {ba[1] * da[2] - ba[2] * da[1], ba[2] * da[0] - ba[0] * da[2], ba[0] * da[1] - ba[1] * da[0]};
+        if (f64::sq3(qn) < 1e-24) {
+            const double ca[3] = {pv[2][0] - pv[0][0], pv[2][1] - pv[0][1], pv[2][2] - pv[0][2]};
+            qn[0] = ca[1] * da[2] - ca[2] * da[1];
+            qn[1] = ca[2] * da[0] - ca[0] * da[2];
+            qn[2] = ca[0] * da[1] - ca[1] * da[0];
+        }
+        bool swap = false;
+        if (f64::sq3(gn) > 0 && f64::sq3(qn) > 0) {
+            if (qn[0] * gn[0] + qn[1] * gn[1] + qn[2] * gn[2] < 0.0) swap = true;
+        }
+        if (swap) P.quads[it.x] = make_int4(q4.x, q4.w, q4.z, q4.y);
+    }
+}
+
+cudaError_t launch_winding_fp64(const Winding64Params& P, long long max_items, int num_sms, cudaStream_t s) {
+    if (max_items <= 0) return cudaSuccess;
+    long long blocks = (max_items + 127) / 128;
+    const long long cap = (long long)num_sms * 8;
+    if (blocks > cap) blocks = cap;
+    k_winding_fp64<<<(unsigned)blocks, 128, 0, s>>>(P);
+    return cudaGetLastError();
+}
+
+}  // namespace dcb
