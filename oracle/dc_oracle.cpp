@@ -267,9 +267,36 @@ typedef struct {
  * threads <= 0 uses every OpenMP thread; 1 reproduces the reference's single thread.
  * Returns an opaque handle (free with dco_free) or NULL on invalid input.
  */
+static void* extract_impl(int nx, int ny, int nz, float vx, float vy, float vz,
+                          float ox, float oy, float oz, const double* px, const double* py,
+                          const double* pz, const float* values, double svd_threshold,
+                          int threads, dco_stats* st);
+
 void* dco_extract(int nx, int ny, int nz, float vx, float vy, float vz,
                   float ox, float oy, float oz, const float* values,
                   double svd_threshold, int threads, dco_stats* st) {
+    return extract_impl(nx, ny, nz, vx, vy, vz, ox, oy, oz, nullptr, nullptr, nullptr, values,
+                        svd_threshold, threads, st);
+}
+
+/*
+ * Same, with explicit grid-point coordinates per axis (px[nx], py[ny], pz[nz]) instead of
+ * origin + i * spacing. Used to run the restatement on a window of a larger grid with the
+ * larger grid's own float positions.
+ */
+void* dco_extract_pos(int nx, int ny, int nz, const double* px, const double* py, const double* pz,
+                      const float* values, double svd_threshold, int threads, dco_stats* st) {
+    if (!px || !py || !pz) return nullptr;
+    return extract_impl(nx, ny, nz, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, px, py, pz, values, svd_threshold,
+                        threads, st);
+}
+
+}  // extern "C"
+
+static void* extract_impl(int nx, int ny, int nz, float vx, float vy, float vz,
+                          float ox, float oy, float oz, const double* px, const double* py,
+                          const double* pz, const float* values, double svd_threshold,
+                          int threads, dco_stats* st) {
     if (nx < 2 || ny < 2 || nz < 2 || !values) return nullptr;
     auto t0 = std::chrono::high_resolution_clock::now();
 #ifdef _OPENMP
@@ -282,9 +309,9 @@ void* dco_extract(int nx, int ny, int nz, float vx, float vy, float vz,
     g.v = values;
     // dc_backend.cpp:63-65: float arithmetic, then stored into a double matrix.
     g.gx.resize(nx); g.gy.resize(ny); g.gz.resize(nz);
-    for (int i = 0; i < nx; ++i) { float f = (float)i; float pr = f * vx; float s = ox + pr; g.gx[i] = (double)s; }
-    for (int j = 0; j < ny; ++j) { float f = (float)j; float pr = f * vy; float s = oy + pr; g.gy[j] = (double)s; }
-    for (int k = 0; k < nz; ++k) { float f = (float)k; float pr = f * vz; float s = oz + pr; g.gz[k] = (double)s; }
+    for (int i = 0; i < nx; ++i) { float f = (float)i; float pr = f * vx; float s = ox + pr; g.gx[i] = px ? px[i] : (double)s; }
+    for (int j = 0; j < ny; ++j) { float f = (float)j; float pr = f * vy; float s = oy + pr; g.gy[j] = py ? py[j] : (double)s; }
+    for (int k = 0; k < nz; ++k) { float f = (float)k; float pr = f * vz; float s = oz + pr; g.gz[k] = pz ? pz[k] : (double)s; }
 
     const int cx = nx - 1, cy = ny - 1, cz = nz - 1;
     const int64_t ncell = (int64_t)cx * cy * cz;
@@ -469,6 +496,8 @@ void* dco_extract(int nx, int ny, int nz, float vx, float vy, float vz,
     }
     return R;
 }
+
+extern "C" {
 
 int64_t dco_num_vertices(void* h) { return h ? (int64_t)((Result*)h)->cells.size() : 0; }
 int64_t dco_num_faces(void* h) { return h ? (int64_t)((Result*)h)->F.size() / 4 : 0; }

@@ -50,8 +50,44 @@ def _dc():
         lib.dco_copy.argtypes = [ctypes.c_void_p] * 6
         lib.dco_free.restype = None
         lib.dco_free.argtypes = [ctypes.c_void_p]
+        lib.dco_extract_pos.restype = ctypes.c_void_p
+        lib.dco_extract_pos.argtypes = [ctypes.c_int] * 3 + [ctypes.c_void_p] * 4 + [
+            ctypes.c_double, ctypes.c_int, ctypes.POINTER(_Stats)]
         lib._typed = True
     return lib
+
+
+def _collect(lib, h, st):
+    if not h:
+        raise ValueError("oracle rejected the grid")
+    try:
+        nv = lib.dco_num_vertices(h)
+        nf = lib.dco_num_faces(h)
+        V = np.empty((nv, 3), np.float64)
+        F = np.empty((nf, 4), np.int32)
+        cells = np.empty(nv, np.int64)
+        eig = np.empty((nv, 3), np.float64)
+        nrows = np.empty(nv, np.int32)
+        lib.dco_copy(h, V.ctypes.data, F.ctypes.data, cells.ctypes.data, eig.ctypes.data,
+                     nrows.ctypes.data)
+    finally:
+        lib.dco_free(h)
+    stats = {k: getattr(st, k) for k, _ in _Stats._fields_}
+    return {"V": V, "F": F, "cells": cells, "eig": eig, "nrows": nrows, "stats": stats}
+
+
+def dc_extract_positions(values, dims, px, py, pz, svd_threshold=0.01, threads=0):
+    """Like dc_extract, with explicit float64 grid-point coordinates per axis."""
+    nx, ny, nz = (int(d) for d in dims)
+    vals = np.ascontiguousarray(np.asarray(values, dtype=np.float32).reshape(-1))
+    axes = [np.ascontiguousarray(np.asarray(a, dtype=np.float64)) for a in (px, py, pz)]
+    if vals.size != nx * ny * nz or [a.size for a in axes] != [nx, ny, nz]:
+        raise ValueError("shape mismatch")
+    lib = _dc()
+    st = _Stats()
+    h = lib.dco_extract_pos(nx, ny, nz, axes[0].ctypes.data, axes[1].ctypes.data, axes[2].ctypes.data,
+                            vals.ctypes.data, float(svd_threshold), int(threads), ctypes.byref(st))
+    return _collect(lib, h, st)
 
 
 def dc_extract(values, dims, spacing, origin, svd_threshold=0.01, threads=0):

@@ -49,7 +49,7 @@ class ContouringOptions:
             self.fp64_threshold_band = d.fp64_threshold_band
         except ImportError:
             self.fp64_escalation_cond = 1e6
-            self.fp64_threshold_band = 0.05
+            self.fp64_threshold_band = 0.01
         self.emit_triangles = False
         self.force_fp64 = False
 

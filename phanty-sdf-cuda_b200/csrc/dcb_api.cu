@@ -1,12 +1,17 @@
 // dcb_api.cu — handle, workspace and the C ABI declared in include/dcb.h.
 //
 // Pipeline of one extraction (all on the caller's stream):
-//   k_mark_compact   grid -> bits, super ranks, packed active list     (dcb_mark.cu)
+//   k_mark_zmarch    grid -> active bits, per-segment counts           (dcb_mark.cu)
+//   scan             segment counts -> segment first ranks, total     (dcb_faces.cu)
 //   [host reads the active count: sizes the vertex buffers]
-//   k_vertex_fp32    Hermite + averaging + QEF, face masks, column counts (dcb_vertex.cu)
-//   k_vertex_fp64    escalated cells re-solved in FP64                 (dcb_vertex64.cu)
+//   k_expand_ranks   super-word ranks + packed active-cell list        (dcb_mark.cu)
+//   k_cell_qef       Hermite + averaging + QEF (rank-1 certified), face masks, column
+//                    counts; other cells listed                        (dcb_vertex.cu)
+//   k_cell_jacobi    listed cells solved with FP32 Jacobi              (dcb_vertex.cu)
+//   k_vertex_fp64    cells FP32 does not trust, re-solved in FP64      (dcb_vertex64.cu)
 //   scan             column counts -> column starts, face total       (dcb_faces.cu)
 //   k_face_scatter   quads into their columns, FP32 winding           (dcb_faces.cu)
+//   k_vertex_fp64    FP64 vertices of the cells of uncertain windings  (dcb_vertex64.cu)
 //   k_winding_fp64   uncertain windings re-decided in FP64            (dcb_vertex64.cu)
 //   k_face_order     rank by k inside each column -> final face list  (dcb_faces.cu)
 //   [host reads the face total and counters]
@@ -49,7 +54,7 @@ struct dcb_context {
     int num_sms = 148;
     std::string last_error;
     cudaEvent_t ev[8] = {};
-    DevBuf grid, bits, super, list, seg_count, seg_start, counters, V, fmask, eflags, en, col_count, col_fill,
+    DevBuf grid, bits, super, list, seg_count, seg_start, counters, V, vclass, fmask, col_count, col_fill,
         col_start, partials, esc_list, hard_list, hard_data, stage_quad, stage_key, faces, wind_items,
         v64_index, v64_cells, V64;
     void* h_counters = nullptr;       // pinned Counters
@@ -195,8 +200,7 @@ int run_pipeline(dcb_context* h, const dcb_grid* in, const dcb_opts* o, cudaStre
     DCB_TRY(h, ensure(h->list, sizeof(uint64_t) * nv), "alloc active list");
     DCB_TRY(h, ensure(h->V, sizeof(float) * 3 * nv), "alloc vertices");
     DCB_TRY(h, ensure(h->fmask, nv), "alloc face masks");
-    DCB_TRY(h, ensure(h->eflags, nv), "alloc edge flags");
-    DCB_TRY(h, ensure(h->en, sizeof(float4) * 3 * nv), "alloc edge normals");
+    DCB_TRY(h, ensure(h->vclass, nv), "alloc vertex classes");
     DCB_TRY(h, ensure(h->esc_list, sizeof(uint32_t) * nv), "alloc escalation list");
     DCB_TRY(h, ensure(h->hard_list, sizeof(uint32_t) * nv), "alloc hard list");
     DCB_TRY(h, ensure(h->hard_data, sizeof(float4) * 3 * nv), "alloc hard data");
@@ -214,18 +218,14 @@ int run_pipeline(dcb_context* h, const dcb_grid* in, const dcb_opts* o, cudaStre
     DCB_TRY(h, cudaMemsetAsync(h->col_fill.p, 0, sizeof(uint32_t) * 3 * cxcy, s), "memset");
     DCB_TRY(h, cudaMemsetAsync(h->v64_index.p, 0xff, sizeof(int) * nv, s), "memset");
 
-    // 2) ranks + list, edge normals, QEF (rank-1 fast path, Jacobi list, FP64 escalations).
+    // 2) ranks + list, QEF with fused edge normals (rank-1 fast path, Jacobi list, FP64).
     ExpandParams xp;
     xp.g = g; xp.nxt = nxt; xp.bits = mp.bits; xp.seg_count = mp.seg_count;
     xp.seg_start = as<uint32_t>(h->seg_start); xp.super = as<uint32_t>(h->super); xp.list = as<uint64_t>(h->list);
     DCB_TRY(h, launch_expand(xp, h->num_sms, s), "launch expand");
-    EdgeParams ep;
-    ep.g = g; ep.list = xp.list; ep.nactive = nv; ep.en = as<float4>(h->en); ep.eflags = as<uint8_t>(h->eflags);
-    ep.fmask = as<uint8_t>(h->fmask); ep.col_count = as<uint32_t>(h->col_count);
-    DCB_TRY(h, launch_edge_normals(ep, h->num_sms, s), "launch edge normals");
     QefParams qp;
-    qp.g = g; qp.list = xp.list; qp.nactive = nv; qp.bits = mp.bits; qp.super = xp.super;
-    qp.en = ep.en; qp.eflags = ep.eflags; qp.V = as<float>(h->V);
+    qp.g = g; qp.list = xp.list; qp.nactive = nv; qp.V = as<float>(h->V); qp.vclass = as<uint8_t>(h->vclass);
+    qp.fmask = as<uint8_t>(h->fmask); qp.col_count = as<uint32_t>(h->col_count);
     qp.esc_list = as<uint32_t>(h->esc_list); qp.esc_count = &dc->esc_count;
     qp.hard_list = as<uint32_t>(h->hard_list); qp.hard_data = as<float4>(h->hard_data); qp.hard_count = &dc->hard_count;
     qp.rank_hist = dc->rank_hist;
@@ -235,7 +235,7 @@ int run_pipeline(dcb_context* h, const dcb_grid* in, const dcb_opts* o, cudaStre
     DCB_TRY(h, launch_cell_jacobi(qp, nv, h->num_sms, s), "launch jacobi");
     Vertex64Params v64;
     v64.g = g; v64.list = xp.list; v64.cells = qp.esc_list; v64.count = &dc->esc_count; v64.cap = (unsigned int)nv;
-    v64.Vf = qp.V; v64.V64 = nullptr; v64.thr = o->svd_threshold;
+    v64.Vf = qp.V; v64.vclass = qp.vclass; v64.V64 = nullptr; v64.thr = o->svd_threshold;
     DCB_TRY(h, launch_vertex_fp64(v64, nv, h->num_sms, s), "launch vertex fp64");
     DCB_TRY(h, cudaEventRecord(h->ev[3], s), "event");
 
@@ -243,7 +243,7 @@ int run_pipeline(dcb_context* h, const dcb_grid* in, const dcb_opts* o, cudaStre
     DCB_TRY(h, launch_scan(as<uint32_t>(h->col_count), 3 * cxcy, as<uint32_t>(h->partials),
                            as<uint32_t>(h->col_start), &dc->face_total, s), "launch scan");
     FaceParams fp;
-    fp.g = g; fp.list = xp.list; fp.nactive = nv; fp.fmask = ep.fmask; fp.V = qp.V;
+    fp.g = g; fp.list = xp.list; fp.nactive = nv; fp.fmask = qp.fmask; fp.V = qp.V; fp.vclass = qp.vclass;
     fp.bits = mp.bits; fp.super = xp.super;
     fp.col_start = as<uint32_t>(h->col_start); fp.col_count = as<uint32_t>(h->col_count);
     fp.col_fill = as<uint32_t>(h->col_fill);
@@ -257,7 +257,7 @@ int run_pipeline(dcb_context* h, const dcb_grid* in, const dcb_opts* o, cudaStre
     DCB_TRY(h, launch_face_scatter(fp, h->num_sms, s), "launch face scatter");
     Vertex64Params w64;
     w64.g = g; w64.list = xp.list; w64.cells = fp.v64_cells; w64.count = fp.v64_count; w64.cap = (unsigned int)v64_cap;
-    w64.Vf = nullptr; w64.V64 = as<double>(h->V64); w64.thr = o->svd_threshold;
+    w64.Vf = nullptr; w64.vclass = nullptr; w64.V64 = as<double>(h->V64); w64.thr = o->svd_threshold;
     DCB_TRY(h, launch_vertex_fp64(w64, v64_cap, h->num_sms, s), "launch fp64 vertices for windings");
     Winding64Params wp;
     wp.g = g; wp.items = fp.wind_items; wp.count = fp.wind_count; wp.cap = (unsigned int)wind_cap;
@@ -308,7 +308,7 @@ void dcb_default_opts(dcb_opts* o) {
     o->sphere_weight = 1.0;
     o->svd_threshold = 0.01;
     o->fp64_escalation_cond = 1e6;
-    o->fp64_threshold_band = 0.05;
+    o->fp64_threshold_band = 0.01;
     o->emit_triangles = 0;
     o->force_fp64 = 0;
 }
@@ -353,7 +353,7 @@ int dcb_destroy(dcb_handle h) {
     if (!h) return DCB_ERR_INVALID_ARGUMENT;
     cudaSetDevice(h->device);
     DevBuf* bufs[] = {&h->grid, &h->bits, &h->super, &h->list, &h->seg_count, &h->seg_start, &h->counters,
-                      &h->V, &h->fmask, &h->eflags, &h->en, &h->col_count, &h->col_fill, &h->col_start,
+                      &h->V, &h->vclass, &h->fmask, &h->col_count, &h->col_fill, &h->col_start,
                       &h->partials, &h->esc_list, &h->hard_list, &h->hard_data, &h->stage_quad,
                       &h->stage_key, &h->faces, &h->wind_items, &h->v64_index, &h->v64_cells, &h->V64};
     for (DevBuf* b : bufs) if (b->p) cudaFree(b->p);

@@ -106,18 +106,19 @@ long long scan_partials_len(long long n) { return (n + kScanTile - 1) / kScanTil
 // ---- face scatter ----------------------------------------------------------------------
 
 
-// gradientAt (contouring.cpp:141-207) in FP32.
+// gradientAt (contouring.cpp:141-207) in FP32 (orientation tests only: a 2-ulp quotient is
+// far inside the uncertainty margin, and uncertain faces are re-decided in FP64).
 __device__ __forceinline__ float3 grid_gradient32(const GridDesc& g, int i, int j, int k) {
     const int im = max(i - 1, 0), ip = min(i + 1, g.nx - 1);
     const int jm = max(j - 1, 0), jp = min(j + 1, g.ny - 1);
     const int km = max(k - 1, 0), kp = min(k + 1, g.nz - 1);
     float3 o = make_float3(0.f, 0.f, 0.f);
     const float dx = pos_axis(g.ox, g.vx, ip) - pos_axis(g.ox, g.vx, im);
-    if (fabsf(dx) > 1e-12f) o.x = (__ldg(g.v + pidx(g, ip, j, k)) - __ldg(g.v + pidx(g, im, j, k))) / dx;
+    if (fabsf(dx) > 1e-12f) o.x = __fdividef(__ldg(g.v + pidx(g, ip, j, k)) - __ldg(g.v + pidx(g, im, j, k)), dx);
     const float dy = pos_axis(g.oy, g.vy, jp) - pos_axis(g.oy, g.vy, jm);
-    if (fabsf(dy) > 1e-12f) o.y = (__ldg(g.v + pidx(g, i, jp, k)) - __ldg(g.v + pidx(g, i, jm, k))) / dy;
+    if (fabsf(dy) > 1e-12f) o.y = __fdividef(__ldg(g.v + pidx(g, i, jp, k)) - __ldg(g.v + pidx(g, i, jm, k)), dy);
     const float dz = pos_axis(g.oz, g.vz, kp) - pos_axis(g.oz, g.vz, km);
-    if (fabsf(dz) > 1e-12f) o.z = (__ldg(g.v + pidx(g, i, j, kp)) - __ldg(g.v + pidx(g, i, j, km))) / dz;
+    if (fabsf(dz) > 1e-12f) o.z = __fdividef(__ldg(g.v + pidx(g, i, j, kp)) - __ldg(g.v + pidx(g, i, j, km)), dz);
     const float n2 = o.x * o.x + o.y * o.y + o.z * o.z;
     if (n2 > 0.f) { const float r = rsqrtf(n2); o.x *= r; o.y *= r; o.z *= r; }
     return o;
@@ -136,7 +137,6 @@ __global__ void __launch_bounds__(128)
 k_face_scatter(FaceParams P) {
     const GridDesc& g = P.g;
     const long long cxcy = (long long)g.cx * g.cy;
-    const float h2 = P.hmax * P.hmax;
     for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < P.nactive;
          r += (long long)gridDim.x * blockDim.x) {
         const uint8_t fm = P.fmask[r];
@@ -144,38 +144,53 @@ k_face_scatter(FaceParams P) {
         int i, j, k;
         unpack_cell(P.list[r], i, j, k);
         const float3 g0 = grid_gradient32(g, i, j, k);
+        // Ranks of the face cells. All four cells of a face are active, so a cell's x-1
+        // neighbour in a face is the previous active cell in linear order (rank - 1).
+        uint32_t r_k1 = 0xffffffffu, r_j1 = 0xffffffffu, r_jk = 0xffffffffu;
+        if (fm & 3) r_k1 = cell_rank(P.bits, P.super, g, i, j, k - 1);
+        if (fm & 5) r_j1 = cell_rank(P.bits, P.super, g, i, j - 1, k);
+        if (fm & 1) r_jk = cell_rank(P.bits, P.super, g, i, j - 1, k - 1);
 #pragma unroll
         for (int axis = 0; axis < 3; ++axis) {
             if (!(fm & (1 << axis))) continue;
-            int c[4][3];
-            if (axis == 0) {
-                c[0][0] = i; c[0][1] = j - 1; c[0][2] = k - 1;  c[1][0] = i; c[1][1] = j; c[1][2] = k - 1;
-                c[3][0] = i; c[3][1] = j - 1; c[3][2] = k;
-            } else if (axis == 1) {
-                c[0][0] = i - 1; c[0][1] = j; c[0][2] = k - 1;  c[1][0] = i; c[1][1] = j; c[1][2] = k - 1;
-                c[3][0] = i - 1; c[3][1] = j; c[3][2] = k;
-            } else {
-                c[0][0] = i - 1; c[0][1] = j - 1; c[0][2] = k;  c[1][0] = i; c[1][1] = j - 1; c[1][2] = k;
-                c[3][0] = i - 1; c[3][1] = j; c[3][2] = k;
-            }
-            const uint32_t r0 = cell_rank(P.bits, P.super, g, c[0][0], c[0][1], c[0][2]);
-            const uint32_t r1 = cell_rank(P.bits, P.super, g, c[1][0], c[1][1], c[1][2]);
+            uint32_t r0, r1, r3;
+            if (axis == 0) { r0 = r_jk; r1 = r_k1; r3 = r_j1; }                      // (i,j-1,k-1) (i,j,k-1) (i,j-1,k)
+            else if (axis == 1) { r0 = r_k1 - 1u; r1 = r_k1; r3 = (uint32_t)r - 1u; } // (i-1,j,k-1) (i,j,k-1) (i-1,j,k)
+            else { r0 = r_j1 - 1u; r1 = r_j1; r3 = (uint32_t)r - 1u; }              // (i-1,j-1,k) (i,j-1,k) (i-1,j,k)
             const uint32_t r2 = (uint32_t)r;
-            const uint32_t r3 = cell_rank(P.bits, P.super, g, c[3][0], c[3][1], c[3][2]);
             const float3 g1 = grid_gradient32(g, i + (axis == 0), j + (axis == 1), k + (axis == 2));
             const float3 gn = make_float3(g0.x + g1.x, g0.y + g1.y, g0.z + g1.z);
             const float3 pa = ldv(P.V, r0), pb = ldv(P.V, r1), pc = ldv(P.V, r2), pd = ldv(P.V, r3);
-            float3 qn = cross3(sub3(pb, pa), sub3(pd, pa));
+            // Bound on each stored vertex's deviation from the CPU's double vertex: its
+            // solve class (in cell widths) plus one ulp of the stored float coordinates.
+            float dv = 0.f;
+            {
+                const uint8_t cls[4] = {P.vclass[r0], P.vclass[r1], P.vclass[r2], P.vclass[r3]};
+                const float3 pv[4] = {pa, pb, pc, pd};
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const float ce = cls[q] == kVcRank1 ? 2e-6f : (cls[q] == kVcJacobi ? 1e-4f : 0.f);
+                    const float mag = fmaxf(fabsf(pv[q].x), fmaxf(fabsf(pv[q].y), fabsf(pv[q].z)));
+                    dv = fmaxf(dv, ce * P.hmax + mag * 1.2e-7f);
+                }
+            }
+            const float3 ba = sub3(pb, pa), da = sub3(pd, pa), ca = sub3(pc, pa);
+            float3 qn = cross3(ba, da);
             float qn2 = dot3(qn, qn);
+            // |qn| error bound of the FP32 cross product from the vertex bounds
+            const float lb = sqrtf(dot3(ba, ba)), ld = sqrtf(dot3(da, da)), lc = sqrtf(dot3(ca, ca));
+            float dq = 2.f * dv * (lb + ld + 2.f * dv);
             // The reference switches to the other diagonal below |qn|^2 = 1e-24 (absolute):
-            // decide in FP64 near that switch and for near-degenerate quads.
-            const bool near_fallback = qn2 < 1e-6f * h2 * h2 || (qn2 > 1e-26f && qn2 < 1e-22f);
-            if (qn2 < 1e-24f) { qn = cross3(sub3(pc, pa), sub3(pd, pa)); qn2 = dot3(qn, qn); }
+            // decide in FP64 whenever the bound straddles that switch.
+            const float qnl0 = sqrtf(qn2);
+            const bool near_fallback = (qnl0 - dq) < 1e-12f && (qnl0 + dq) >= 1e-12f;
+            if (qn2 < 1e-24f) { qn = cross3(ca, da); qn2 = dot3(qn, qn); dq = 2.f * dv * (lc + ld + 2.f * dv); }
             const float gn2 = dot3(gn, gn);
             const float d = dot3(qn, gn);
             const float qnl = sqrtf(qn2), gnl = sqrtf(gn2);
+            // gradient sum: FP32 quotients and normalisation, ~1e-6 relative
             const bool uncertain = near_fallback || gn2 < 1e-4f ||
-                                   fabsf(d) <= (1e-3f * h2 + 1e-5f * qnl) * gnl;
+                                   fabsf(d) <= 4.f * dq * gnl + 1e-5f * qnl * gnl;
             bool swap = !uncertain && gn2 > 0.f && qn2 > 0.f && d < 0.f;
             const long long col = axis * cxcy + (long long)i * g.cy + j;
             const uint32_t slot = P.col_start[col] + atomicAdd(&P.col_fill[col], 1u);

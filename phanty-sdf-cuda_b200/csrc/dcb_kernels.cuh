@@ -28,26 +28,18 @@ struct ExpandParams {
 };
 cudaError_t launch_expand(const ExpandParams& P, int num_sms, cudaStream_t s);
 
-struct EdgeParams {
-    GridDesc g;
-    const uint64_t* list;
-    long long nactive;
-    float4* en;                     // [3*active]: averaged normal of owned edge (cell, axis)
-    uint8_t* eflags;                // bit a: edge a averaged; bit 3+a: its normal is ill-conditioned
-    uint8_t* fmask;                 // bit a: cell owns a face on its min-corner edge a
-    uint32_t* col_count;            // [3][cx*cy]: a*cx*cy + i*cy + j
-};
-cudaError_t launch_edge_normals(const EdgeParams& P, int num_sms, cudaStream_t s);
+// Error class of a stored vertex (cell widths, before the float rounding of the output):
+// 0 = certified rank-1 FP32 solve (<= 2e-6), 1 = FP32 Jacobi (<= 1e-4), 2 = FP64 path.
+enum VertexClass : uint8_t { kVcRank1 = 0, kVcJacobi = 1, kVcFp64 = 2 };
 
 struct QefParams {
     GridDesc g;
     const uint64_t* list;
     long long nactive;
-    const uint32_t* bits;
-    const uint32_t* super;
-    const float4* en;
-    const uint8_t* eflags;
     float* V;
+    uint8_t* vclass;                // [active] VertexClass
+    uint8_t* fmask;                 // bit a: cell owns a face on its min-corner edge a
+    uint32_t* col_count;            // [3][cx*cy]: a*cx*cy + i*cy + j
     uint32_t* esc_list;
     unsigned int* esc_count;
     uint32_t* hard_list;            // cells not certified rank 1
@@ -69,6 +61,7 @@ struct Vertex64Params {
     const unsigned int* count;
     unsigned int cap;               // entries in cells; count may exceed it on overflow
     float* Vf;                      // optional: float vertex at [rank]
+    uint8_t* vclass;                // optional: set to kVcFp64 at [rank] with Vf
     double* V64;                    // optional: double vertex at [item]
     double thr;
 };
@@ -96,6 +89,7 @@ struct FaceParams {
     long long nactive;
     const uint8_t* fmask;
     const float* V;
+    const uint8_t* vclass;
     const uint32_t* bits;
     const uint32_t* super;
     const uint32_t* col_start;     // [3][cx*cy]

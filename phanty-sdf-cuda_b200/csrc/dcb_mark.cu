@@ -135,35 +135,46 @@ k_mark_zmarch(MarkParams P) {
     }
 }
 
-// Warp per (row, x-tile) segment: global ranks of its super words and the packed list.
+// Warp per group of 32 consecutive (row, x-tile) segments: the non-empty ones (ballot) get
+// the global ranks of their super words and their part of the packed active-cell list.
 __global__ void __launch_bounds__(256)
 k_expand_ranks(ExpandParams P) {
     const GridDesc& g = P.g;
     const int lane = threadIdx.x & 31;
     const long long nseg = (long long)g.cy * g.cz * P.nxt;
-    for (long long s = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < nseg;
-         s += ((long long)gridDim.x * blockDim.x) >> 5) {
-        if (P.seg_count[s] == 0) continue;           // warp-uniform
-        const long long row = s / P.nxt;
-        const int xt = (int)(s - row * P.nxt);
-        const int w = xt * kTileWords + lane;
-        const uint32_t act = (w < g.W) ? P.bits[row * g.W + w] : 0u;
-        const uint32_t c = __popc(act);
-        uint32_t incl = c;
+    const long long ngroups = (nseg + 31) / 32;
+    for (long long grp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; grp < ngroups;
+         grp += ((long long)gridDim.x * blockDim.x) >> 5) {
+        const long long s0 = grp * 32;
+        const uint32_t cnt = (s0 + lane < nseg) ? P.seg_count[s0 + lane] : 0u;
+        uint32_t live = __ballot_sync(0xffffffffu, cnt != 0);
+        const uint32_t my_start = (s0 + lane < nseg && cnt) ? P.seg_start[s0 + lane] : 0u;
+        while (live) {
+            const int b = __ffs(live) - 1;
+            live &= live - 1;
+            const long long s = s0 + b;
+            const uint32_t seg_first = __shfl_sync(0xffffffffu, my_start, b);
+            const long long row = s / P.nxt;
+            const int xt = (int)(s - row * P.nxt);
+            const int w = xt * kTileWords + lane;
+            const uint32_t act = (w < g.W) ? P.bits[row * g.W + w] : 0u;
+            const uint32_t c = __popc(act);
+            uint32_t incl = c;
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += t;
-        }
-        const uint32_t first = P.seg_start[s] + incl - c;
-        if (w < g.W && (w & 7) == 0) P.super[row * g.W8 + (w >> 3)] = first;
-        const int j = (int)(row % g.cy), k = (int)(row / g.cy);
-        uint32_t m = act, q = 0;
-        while (m) {
-            const int b = __ffs(m) - 1;
-            m &= m - 1;
-            P.list[first + q] = pack_cell(32 * w + b, j, k);
-            ++q;
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += t;
+            }
+            const uint32_t first = seg_first + incl - c;
+            if (w < g.W && (w & 7) == 0) P.super[row * g.W8 + (w >> 3)] = first;
+            const int j = (int)(row % g.cy), k = (int)(row / g.cy);
+            uint32_t m = act, q = 0;
+            while (m) {
+                const int bb = __ffs(m) - 1;
+                m &= m - 1;
+                P.list[first + q] = pack_cell(32 * w + bb, j, k);
+                ++q;
+            }
         }
     }
 }
@@ -177,7 +188,7 @@ cudaError_t launch_mark(const MarkParams& P, cudaStream_t s) {
 
 cudaError_t launch_expand(const ExpandParams& P, int num_sms, cudaStream_t s) {
     const long long nseg = (long long)P.g.cy * P.g.cz * P.nxt;
-    long long blocks = (nseg * 32 + 255) / 256;
+    long long blocks = ((nseg + 31) / 32 * 32 + 255) / 256;
     const long long cap = (long long)num_sms * 32;
     if (blocks > cap) blocks = cap;
     if (blocks < 1) blocks = 1;

@@ -18,15 +18,16 @@
 // epsilon (src/cuda/dc_cuda.cu:283-423); none of that is reproduced.
 //
 // Work split:
-//   k_edge_normals   one thread per active cell, for each of its min-corner edges (the
-//                    edges it owns): the averaged normal, computed once per grid edge. On an
-//                    edge every trilinear gradient reduces to the edge difference plus two
-//                    bilinear differences, so the four cells' gradients need 10 grid values.
-//   k_cell_qef       one thread per active cell: Hermite positions in cell-local units, the
-//                    owners' averaged normals (or the own normal off the averaging set), the
-//                    centred normal equations with Kahan sums, and the solve when the
-//                    spectrum is provably rank 1 (power iteration + trace test); every other
-//                    cell is appended to a compact list.
+//   k_cell_qef       one thread per active cell. Each lane walks only its own crossing
+//                    edges. On an edge every trilinear gradient reduces to the edge difference
+//                    plus two bilinear differences, so the four cells' normals of an averaged
+//                    edge need 10 grid values; every cell sharing the edge recomputes the same
+//                    average (no storage, no neighbour lookups). Hermite positions are kept in
+//                    cell-local units, the centred normal equations are summed with Kahan
+//                    compensation, and the cell is solved at once when its spectrum is
+//                    provably rank 1 (power iteration + trace test); every other cell is
+//                    appended to a compact list. The kernel also emits the face mask of the
+//                    cell's three min-corner edges and the per-column face counts.
 //   k_cell_jacobi    the listed cells: cyclic Jacobi in FP32.
 // FP32 is not trusted when an eigenvalue sits within a relative band of the threshold,
 // when the retained condition exceeds the limit, or when a normal's direction is decided
@@ -60,7 +61,7 @@ __device__ __forceinline__ float3 normalized(float3 a) {
 __device__ __forceinline__ float lerp_t(float fa, float fb) {
     const float d = fa - fb;
     if (fabsf(d) < 1e-6f) return (float)((double)fa / ((double)fa - (double)fb + 1e-16));
-    return fa / d;
+    return __fdividef(fa, d);   // |t| <= 1 here: the 2-ulp quotient is far inside the FP32 budget
 }
 __device__ __forceinline__ bool active_at(const GridDesc& g, int i, int j, int k) {
     bool neg = false, pos = false;
@@ -79,104 +80,6 @@ __device__ __forceinline__ int3 add3(int3 a, int axis, int d) {
 __device__ __forceinline__ int comp(int3 a, int axis) { return axis == 0 ? a.x : (axis == 1 ? a.y : a.z); }
 __device__ __forceinline__ float ldp(const GridDesc& g, int3 p) { return ldv(g, p.x, p.y, p.z); }
 
-// ---- k_edge_normals ---------------------------------------------------------------------
-
-__global__ void __launch_bounds__(128)
-k_edge_normals(EdgeParams P) {
-    const GridDesc& g = P.g;
-    const long long cxcy = (long long)g.cx * g.cy;
-    for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < P.nactive;
-         r += (long long)gridDim.x * blockDim.x) {
-        int i, j, k;
-        unpack_cell(P.list[r], i, j, k);
-        const int3 P0 = make_int3(i, j, k);
-        const float s0 = ldv(g, i, j, k);
-        const bool in0 = i > 0 && i < g.nx - 1 && j > 0 && j < g.ny - 1 && k > 0 && k < g.nz - 1;
-        uint8_t flags = 0, fm = 0;
-        for (int a = 0; a < 3; ++a) {
-            const int3 P1 = add3(P0, a, 1);
-            const float s1 = ldp(g, P1);
-            // faces owned by this cell (contouring.cpp:609-729 loop ranges)
-            if (strict_change(s0, s1)) {
-                const bool ok = (a == 0) ? (j >= 1 && k >= 1) : (a == 1) ? (i >= 1 && k >= 1) : (i >= 1 && j >= 1);
-                if (ok) {
-                    fm |= (uint8_t)(1 << a);
-                    atomicAdd(&P.col_count[a * cxcy + (long long)i * g.cy + j], 1u);
-                }
-            }
-            if (!hermite_crossing(s0, s1)) continue;
-            const bool in1 = P1.x > 0 && P1.x < g.nx - 1 && P1.y > 0 && P1.y < g.ny - 1 && P1.z > 0 && P1.z < g.nz - 1;
-            if (!(in0 || in1)) continue;
-            const int d1 = a == 0 ? 1 : 0;
-            const int d2 = a == 2 ? 1 : 2;
-            if (!strict_change(s0, s1)) {
-                // zero endpoint: the four cells are not automatically active
-                bool all = true;
-                for (int q = 0; q < 4 && all; ++q) {
-                    int3 c = P0;
-                    if (q & 1) c = add3(c, d1, -1);
-                    if (q & 2) c = add3(c, d2, -1);
-                    all = active_at(g, c.x, c.y, c.z);
-                }
-                if (!all) continue;
-            }
-            // Along-edge sample of each cell in its own EDGE_PAIRS orientation: X edges start
-            // at local x=1 when local y=1, Y edges at local y=1 when local x=0, Z edges at z=0.
-            const float t_lo = lerp_t(s0, s1), t_hi = lerp_t(s1, s0);
-            const float ga = (s1 - s0) / width_axis(g, a, comp(P0, a));
-            const float ba = fabsf(ga);
-            // perpendicular differences at both edge ends: forward (m=0) and backward (m=1)
-            const float a0p = ldp(g, add3(P0, d1, 1)) - s0, a0m = s0 - ldp(g, add3(P0, d1, -1));
-            const float a1p = ldp(g, add3(P1, d1, 1)) - s1, a1m = s1 - ldp(g, add3(P1, d1, -1));
-            const float b0p = ldp(g, add3(P0, d2, 1)) - s0, b0m = s0 - ldp(g, add3(P0, d2, -1));
-            const float b1p = ldp(g, add3(P1, d2, 1)) - s1, b1m = s1 - ldp(g, add3(P1, d2, -1));
-            const float rw1p = 1.f / width_axis(g, d1, comp(P0, d1)), rw1m = 1.f / width_axis(g, d1, comp(P0, d1) - 1);
-            const float rw2p = 1.f / width_axis(g, d2, comp(P0, d2)), rw2m = 1.f / width_axis(g, d2, comp(P0, d2) - 1);
-            float3 acc = make_float3(0.f, 0.f, 0.f);
-            bool ill = false;
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const int m1 = q & 1, m2 = q >> 1;
-                const bool start_high = (a == 0) ? (m1 == 1) : (a == 1) ? (m1 == 0) : false;
-                const float u = start_high ? 1.f - t_hi : t_lo;
-                const float e1lo = m1 ? a0m : a0p, e1hi = m1 ? a1m : a1p;
-                const float e2lo = m2 ? b0m : b0p, e2hi = m2 ? b1m : b1p;
-                const float rw1 = m1 ? rw1m : rw1p, rw2 = m2 ? rw2m : rw2p;
-                const float g1 = ((1.f - u) * e1lo + u * e1hi) * rw1;
-                const float g2 = ((1.f - u) * e2lo + u * e2hi) * rw2;
-                const float bb1 = ((1.f - u) * fabsf(e1lo) + u * fabsf(e1hi)) * rw1;
-                const float bb2 = ((1.f - u) * fabsf(e2lo) + u * fabsf(e2hi)) * rw2;
-                float3 gv;
-                if (a == 0) gv = make_float3(ga, g1, g2);
-                else if (a == 1) gv = make_float3(g1, ga, g2);
-                else gv = make_float3(g1, g2, ga);
-                const float gn2 = gv.x * gv.x + gv.y * gv.y + gv.z * gv.z;
-                if (gn2 <= kNormalCond2 * (ba * ba + bb1 * bb1 + bb2 * bb2)) ill = true;
-                const float3 n = normalized(gv);
-                if (gn2 > 0.f) { acc.x += n.x; acc.y += n.y; acc.z += n.z; }
-            }
-            if (acc.x * acc.x + acc.y * acc.y + acc.z * acc.z < 1e-4f) ill = true;
-            const float3 n = normalized(acc);
-            P.en[3 * r + a] = make_float4(n.x, n.y, n.z, 0.f);
-            flags |= (uint8_t)(1 << a);
-            if (ill) flags |= (uint8_t)(8 << a);
-        }
-        P.eflags[r] = flags;
-        P.fmask[r] = fm;
-    }
-}
-
-cudaError_t launch_edge_normals(const EdgeParams& P, int num_sms, cudaStream_t s) {
-    if (P.nactive <= 0) return cudaSuccess;
-    long long blocks = (P.nactive + 127) / 128;
-    const long long cap = (long long)num_sms * 32;
-    if (blocks > cap) blocks = cap;
-    k_edge_normals<<<(unsigned)blocks, 128, 0, s>>>(P);
-    return cudaGetLastError();
-}
-
-// ---- k_cell_qef -------------------------------------------------------------------------
-
 __device__ __forceinline__ void kahan_add(float& s, float& c, float x) {
     const float y = x - c;
     const float t = s + y;
@@ -184,15 +87,9 @@ __device__ __forceinline__ void kahan_add(float& s, float& c, float x) {
     s = t;
 }
 
-__device__ __forceinline__ bool bit_active(const uint32_t* __restrict__ bits, const GridDesc& g, int i, int j, int k) {
-    if (i >= g.cx || j >= g.cy || k >= g.cz) return false;
-    const int64_t row = (int64_t)j + (int64_t)g.cy * k;
-    return (__ldg(bits + row * g.W + (i >> 5)) >> (i & 31)) & 1u;
-}
-
-// Full trilinear gradient of cell (i,j,k) at local (u,v,w) (Cell.cpp:80-155), world units,
-// with the same cancellation test as the edge kernel. Only used off the averaging set.
-__device__ float3 own_gradient(const GridDesc& g, const float c[8], float u, float v, float w,
+// Full trilinear gradient of a cell at local (u,v,w) (Cell.cpp:80-155) in world units, with
+// a cancellation test. Only used for edges outside the averaging set.
+__device__ float3 own_gradient(const float c[8], float u, float v, float w,
                                float rdx, float rdy, float rdz, bool& ill) {
     const float S000 = c[0], S100 = c[1], S110 = c[2], S010 = c[3];
     const float S001 = c[4], S101 = c[5], S111 = c[6], S011 = c[7];
@@ -213,27 +110,147 @@ __device__ float3 own_gradient(const GridDesc& g, const float c[8], float u, flo
     return gr;
 }
 
-// Local -> world and store (double for the final combination: one float rounding).
+// Edge geometry of a cell, packed: bits 0-1 axis, 2-4 low-endpoint offset (x,y,z),
+// 5 the cell's EDGE_PAIRS orientation starts at the low endpoint, 6-8 low corner index,
+// 9-11 high corner index.
+__host__ __device__ constexpr uint32_t edge_geo(int e) {
+    return (uint32_t)(corner_dx(edge_a(e)) != corner_dx(edge_b(e)) ? 0 : (corner_dy(edge_a(e)) != corner_dy(edge_b(e)) ? 1 : 2)) |
+           ((uint32_t)corner_dx((corner_dx(edge_a(e)) + corner_dy(edge_a(e)) + corner_dz(edge_a(e)) <=
+                                 corner_dx(edge_b(e)) + corner_dy(edge_b(e)) + corner_dz(edge_b(e))) ? edge_a(e) : edge_b(e)) << 2) |
+           ((uint32_t)corner_dy((corner_dx(edge_a(e)) + corner_dy(edge_a(e)) + corner_dz(edge_a(e)) <=
+                                 corner_dx(edge_b(e)) + corner_dy(edge_b(e)) + corner_dz(edge_b(e))) ? edge_a(e) : edge_b(e)) << 3) |
+           ((uint32_t)corner_dz((corner_dx(edge_a(e)) + corner_dy(edge_a(e)) + corner_dz(edge_a(e)) <=
+                                 corner_dx(edge_b(e)) + corner_dy(edge_b(e)) + corner_dz(edge_b(e))) ? edge_a(e) : edge_b(e)) << 4) |
+           ((uint32_t)((corner_dx(edge_a(e)) + corner_dy(edge_a(e)) + corner_dz(edge_a(e)) <=
+                        corner_dx(edge_b(e)) + corner_dy(edge_b(e)) + corner_dz(edge_b(e))) ? 1 : 0) << 5) |
+           ((uint32_t)((corner_dx(edge_a(e)) + corner_dy(edge_a(e)) + corner_dz(edge_a(e)) <=
+                        corner_dx(edge_b(e)) + corner_dy(edge_b(e)) + corner_dz(edge_b(e))) ? edge_a(e) : edge_b(e)) << 6) |
+           ((uint32_t)((corner_dx(edge_a(e)) + corner_dy(edge_a(e)) + corner_dz(edge_a(e)) <=
+                        corner_dx(edge_b(e)) + corner_dy(edge_b(e)) + corner_dz(edge_b(e))) ? edge_b(e) : edge_a(e)) << 9);
+}
+__constant__ uint32_t c_edge_geo[12] = {edge_geo(0), edge_geo(1), edge_geo(2), edge_geo(3), edge_geo(4), edge_geo(5),
+                                        edge_geo(6), edge_geo(7), edge_geo(8), edge_geo(9), edge_geo(10), edge_geo(11)};
+
+// Widths (and reciprocals) of the cells i-1, i, i+1 along each axis, exact float
+// differences of the float grid positions (the CPU forms positions the same way).
+struct Widths {
+    float w[3][3];   // [axis][offset+1]
+    float r[3][3];
+};
+__device__ __forceinline__ void cell_widths(const GridDesc& g, int i, int j, int k, Widths& W) {
+    const int idx[3] = {i, j, k};
+    const float o[3] = {g.ox, g.oy, g.oz}, v[3] = {g.vx, g.vy, g.vz};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        float pm = pos_axis(o[a], v[a], idx[a] - 1), p0 = pos_axis(o[a], v[a], idx[a]);
+        float p1 = pos_axis(o[a], v[a], idx[a] + 1), p2 = pos_axis(o[a], v[a], idx[a] + 2);
+        W.w[a][0] = p0 - pm; W.w[a][1] = p1 - p0; W.w[a][2] = p2 - p1;
+#pragma unroll
+        for (int q = 0; q < 3; ++q) W.r[a][q] = 1.f / W.w[a][q];
+    }
+}
+
+// W.r[a][q] for runtime a, q with literal array indices only (keeps W in registers).
+__device__ __forceinline__ float pick_r(const Widths& W, int a, int q) {
+    const float r0 = q == 0 ? W.r[0][0] : (q == 1 ? W.r[0][1] : W.r[0][2]);
+    const float r1 = q == 0 ? W.r[1][0] : (q == 1 ? W.r[1][1] : W.r[1][2]);
+    const float r2 = q == 0 ? W.r[2][0] : (q == 1 ? W.r[2][1] : W.r[2][2]);
+    return a == 0 ? r0 : (a == 1 ? r1 : r2);
+}
+
+// Hermite normal of one crossing edge: the 4-cell average when the edge is in the averaging
+// set, else the cell's own trilinear normal at its sample. The average is a function of
+// the edge alone, so every cell sharing the edge computes the same value.
+// lo: global low endpoint; o1/o2: offset (0/1) of the low endpoint from the cell along d1/d2.
+__device__ float3 edge_normal(const GridDesc& g, int3 lo, int axis, int o1, int o2, float s_lo, float s_hi,
+                              float t_lo, float pu, float pv, float pw, const float cc[8],
+                              const Widths& W, bool& ill) {
+    const int3 hi = add3(lo, axis, 1);
+    const bool in0 = lo.x > 0 && lo.x < g.nx - 1 && lo.y > 0 && lo.y < g.ny - 1 && lo.z > 0 && lo.z < g.nz - 1;
+    const bool in1 = hi.x > 0 && hi.x < g.nx - 1 && hi.y > 0 && hi.y < g.ny - 1 && hi.z > 0 && hi.z < g.nz - 1;
+    const int d1 = axis == 0 ? 1 : 0;
+    const int d2 = axis == 2 ? 1 : 2;
+    bool avg = in0 || in1;
+    if (avg && !strict_change(s_lo, s_hi)) {
+        // zero endpoint: the four cells are not automatically active
+        for (int q = 0; q < 4 && avg; ++q) {
+            int3 c = lo;
+            if (q & 1) c = add3(c, d1, -1);
+            if (q & 2) c = add3(c, d2, -1);
+            avg = active_at(g, c.x, c.y, c.z);
+        }
+    }
+    if (!avg) return normalized(own_gradient(cc, pu, pv, pw, W.r[0][1], W.r[1][1], W.r[2][1], ill));
+    // Along-edge sample of each cell in its own EDGE_PAIRS orientation: X edges start at
+    // local x=1 when local y=1, Y edges at local y=1 when local x=0, Z edges at z=0. A cell
+    // starting at the high end samples at 1 - t_hi, which equals t_lo unless |s_lo - s_hi| is
+    // tiny (both t are then formed in double, exactly as the CPU forms them).
+    const float u_hi = fabsf(s_lo - s_hi) < 1e-6f ? 1.f - lerp_t(s_hi, s_lo) : t_lo;
+    const int64_t st1 = d1 == 0 ? 1 : (int64_t)g.nx;
+    const int64_t st2 = d2 == 1 ? (int64_t)g.nx : (int64_t)g.nx * g.ny;
+    const float* plo = g.v + pidx(g, lo.x, lo.y, lo.z);
+    const float* phi = g.v + pidx(g, hi.x, hi.y, hi.z);
+    const float ga = (s_hi - s_lo) * pick_r(W, axis, 1);
+    // perpendicular differences at both edge ends: forward (m=0) and backward (m=1)
+    const float a0p = __ldg(plo + st1) - s_lo, a0m = s_lo - __ldg(plo - st1);
+    const float a1p = __ldg(phi + st1) - s_hi, a1m = s_hi - __ldg(phi - st1);
+    const float b0p = __ldg(plo + st2) - s_lo, b0m = s_lo - __ldg(plo - st2);
+    const float b1p = __ldg(phi + st2) - s_hi, b1m = s_hi - __ldg(phi - st2);
+    // widths of the cells on either side of the edge: the cell index along d is
+    // (cell coordinate + o) for m = 0 and one less for m = 1
+    const float rw1p = pick_r(W, d1, 1 + o1), rw1m = pick_r(W, d1, o1);
+    const float rw2p = pick_r(W, d2, 1 + o2), rw2m = pick_r(W, d2, o2);
+    // one cancellation bound per edge (>= each cell's own bound)
+    const float m1v = fmaxf(fmaxf(fabsf(a0p), fabsf(a1p)) * rw1p, fmaxf(fabsf(a0m), fabsf(a1m)) * rw1m);
+    const float m2v = fmaxf(fmaxf(fabsf(b0p), fabsf(b1p)) * rw2p, fmaxf(fabsf(b0m), fabsf(b1m)) * rw2m);
+    const float bound2 = kNormalCond2 * (ga * ga + m1v * m1v + m2v * m2v);
+    float3 acc = make_float3(0.f, 0.f, 0.f);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int m1 = q & 1, m2 = q >> 1;
+        const bool start_high = (axis == 0) ? (m1 == 1) : (axis == 1) ? (m1 == 0) : false;
+        const float u = start_high ? u_hi : t_lo;
+        const float e1lo = m1 ? a0m : a0p, e1hi = m1 ? a1m : a1p;
+        const float e2lo = m2 ? b0m : b0p, e2hi = m2 ? b1m : b1p;
+        const float g1 = (e1lo + u * (e1hi - e1lo)) * (m1 ? rw1m : rw1p);
+        const float g2 = (e2lo + u * (e2hi - e2lo)) * (m2 ? rw2m : rw2p);
+        float3 gv;
+        if (axis == 0) gv = make_float3(ga, g1, g2);
+        else if (axis == 1) gv = make_float3(g1, ga, g2);
+        else gv = make_float3(g1, g2, ga);
+        const float gn2 = gv.x * gv.x + gv.y * gv.y + gv.z * gv.z;
+        if (gn2 <= bound2) ill = true;
+        if (gn2 > 0.f) {
+            const float rn = rsqrtf(gn2);
+            acc.x += gv.x * rn; acc.y += gv.y * rn; acc.z += gv.z * rn;
+        }
+    }
+    if (acc.x * acc.x + acc.y * acc.y + acc.z * acc.z < 1e-4f) ill = true;
+    return normalized(acc);
+}
+
+// Local -> world: one double combination per axis, one float rounding.
 __device__ __forceinline__ void store_vertex(const QefParams& P, long long r, int i, int j, int k,
-                                             float cu, float cv, float cw, float wx, float wy, float wz) {
+                                             float Lx, float Ly, float Lz) {
     const GridDesc& g = P.g;
     const float wx1 = width_axis(g, 0, i), wy1 = width_axis(g, 1, j), wz1 = width_axis(g, 2, k);
-    const double fy = (double)wy1 / (double)wx1, fz = (double)wz1 / (double)wx1;
-    const double Lx = (double)cu + (double)wx, Ly = (double)cv + (double)wy / fy, Lz = (double)cw + (double)wz / fz;
-    P.V[3 * r + 0] = (float)((double)pos_axis(g.ox, g.vx, i) + (double)wx1 * Lx);
-    P.V[3 * r + 1] = (float)((double)pos_axis(g.oy, g.vy, j) + (double)wy1 * Ly);
-    P.V[3 * r + 2] = (float)((double)pos_axis(g.oz, g.vz, k) + (double)wz1 * Lz);
+    P.V[3 * r + 0] = (float)((double)pos_axis(g.ox, g.vx, i) + (double)wx1 * (double)Lx);
+    P.V[3 * r + 1] = (float)((double)pos_axis(g.oy, g.vy, j) + (double)wy1 * (double)Ly);
+    P.V[3 * r + 2] = (float)((double)pos_axis(g.oz, g.vz, k) + (double)wz1 * (double)Lz);
 }
+
+// ---- k_cell_qef -------------------------------------------------------------------------
 
 __global__ void __launch_bounds__(128)
 k_cell_qef(QefParams P) {
     const GridDesc& g = P.g;
-    __shared__ unsigned int s_hist[2];
-    __shared__ float s_c[8][128];    // per-thread corner values (dynamically indexed below)
-    __shared__ float s_tt[12][128];  // per-thread lerp parameters
+    __shared__ unsigned int s_hist;
+    __shared__ float s_c[8][128];    // per-thread corner values (dynamically indexed)
+    __shared__ float s_t[12][128];   // per-thread lerp parameter of each crossing edge
     const int tid = threadIdx.x;
-    if (tid < 2) s_hist[tid] = 0;
+    if (tid == 0) s_hist = 0;
     __syncthreads();
+    const long long cxcy = (long long)g.cx * g.cy;
     for (long long r = (long long)blockIdx.x * blockDim.x + tid; r < P.nactive;
          r += (long long)gridDim.x * blockDim.x) {
         int i, j, k;
@@ -244,76 +261,64 @@ k_cell_qef(QefParams P) {
             c[q] = ldv(g, i + corner_dx(q), j + corner_dy(q), k + corner_dz(q));
             s_c[q][tid] = c[q];
         }
+        // Faces owned by this cell: its min-corner X, Y, Z edges (contouring.cpp:609-729).
+        uint8_t fm = 0;
+        if (j >= 1 && k >= 1 && strict_change(c[0], c[1])) {
+            fm |= 1; atomicAdd(&P.col_count[0 * cxcy + (long long)i * g.cy + j], 1u);
+        }
+        if (i >= 1 && k >= 1 && strict_change(c[0], c[3])) {
+            fm |= 2; atomicAdd(&P.col_count[1 * cxcy + (long long)i * g.cy + j], 1u);
+        }
+        if (i >= 1 && j >= 1 && strict_change(c[0], c[4])) {
+            fm |= 4; atomicAdd(&P.col_count[2 * cxcy + (long long)i * g.cy + j], 1u);
+        }
+        P.fmask[r] = fm;
 
-        // Pass 1: crossing edges, their t, centroid in local units.
+        // Pass 1: crossing edges and the centroid in local units.
         uint32_t hmask = 0;
         float cu = 0.f, cv = 0.f, cw = 0.f;
-        int m = 0;
 #pragma unroll
         for (int e = 0; e < 12; ++e) {
             const int a = edge_a(e), b = edge_b(e);
             if (!hermite_crossing(c[a], c[b])) continue;
-            const float t = lerp_t(c[a], c[b]);
-            s_tt[e][tid] = t;
             hmask |= 1u << e;
+            const float t = lerp_t(c[a], c[b]);
+            s_t[e][tid] = t;
             float pu = (float)corner_dx(a), pv = (float)corner_dy(a), pw = (float)corner_dz(a);
             if (corner_dx(a) != corner_dx(b)) pu = corner_dx(a) ? 1.f - t : t;
             if (corner_dy(a) != corner_dy(b)) pv = corner_dy(a) ? 1.f - t : t;
             if (corner_dz(a) != corner_dz(b)) pw = corner_dz(a) ? 1.f - t : t;
             cu += pu; cv += pv; cw += pw;
-            ++m;
         }
-        const float invm = 1.f / (float)m;
+        const float invm = 1.f / (float)__popc(hmask);
         cu *= invm; cv *= invm; cw *= invm;
-        const float wx1 = width_axis(g, 0, i), wy1 = width_axis(g, 1, j), wz1 = width_axis(g, 2, k);
-        const float fy = wy1 / wx1, fz = wz1 / wx1;
-        const float rdx = 1.f / wx1, rdy = 1.f / wy1, rdz = 1.f / wz1;
+        Widths W;
+        cell_widths(g, i, j, k, W);
+        const float fy = W.w[1][1] * W.r[0][1], fz = W.w[2][1] * W.r[0][1];
 
-        // Pass 2: normals and the centred normal equations (Kahan).
+        // Pass 2: each lane walks its own crossing edges (warp iterations = max count).
         float M00 = 0, M01 = 0, M02 = 0, M11 = 0, M12 = 0, M22 = 0, R0 = 0, R1 = 0, R2 = 0;
         float K00 = 0, K01 = 0, K02 = 0, K11 = 0, K12 = 0, K22 = 0, Q0 = 0, Q1 = 0, Q2 = 0;
         bool ill = false;
-        const uint8_t myflags = P.eflags[r];
-        for (int e = 0; e < 12; ++e) {
-            if (!(hmask & (1u << e))) continue;
-            const int a = edge_a(e), b = edge_b(e);
-            const int Ax = corner_dx(a), Ay = corner_dy(a), Az = corner_dz(a);
-            const int Bx = corner_dx(b), By = corner_dy(b), Bz = corner_dz(b);
-            const float t = s_tt[e][tid];
-            float pu = (float)Ax, pv = (float)Ay, pw = (float)Az;
-            int axis;
-            if (Ax != Bx) { pu = Ax ? 1.f - t : t; axis = 0; }
-            else if (Ay != By) { pv = Ay ? 1.f - t : t; axis = 1; }
-            else { pw = Az ? 1.f - t : t; axis = 2; }
-            // owner = cell at the edge's minimum endpoint
-            const int ox = min(Ax, Bx), oy = min(Ay, By), oz = min(Az, Bz);
-            float3 n;
-            bool have = false;
-            if ((ox | oy | oz) == 0) {
-                if (myflags & (1 << axis)) {
-                    const float4 v = P.en[3 * r + axis];
-                    n = make_float3(v.x, v.y, v.z);
-                    ill |= (myflags >> (3 + axis)) & 1;
-                    have = true;
-                }
-            } else if (bit_active(P.bits, g, i + ox, j + oy, k + oz)) {
-                const uint32_t ro = (ox == 1 && oy == 0 && oz == 0)
-                                        ? (uint32_t)r + 1u
-                                        : cell_rank(P.bits, P.super, g, i + ox, j + oy, k + oz);
-                const uint8_t fl = P.eflags[ro];
-                if (fl & (1 << axis)) {
-                    const float4 v = P.en[3 * (size_t)ro + axis];
-                    n = make_float3(v.x, v.y, v.z);
-                    ill |= (fl >> (3 + axis)) & 1;
-                    have = true;
-                }
-            }
-            if (!have) {
-                float cc[8];
-#pragma unroll
-                for (int q = 0; q < 8; ++q) cc[q] = s_c[q][tid];
-                n = normalized(own_gradient(g, cc, pu, pv, pw, rdx, rdy, rdz, ill));
-            }
+        uint32_t rem = hmask;
+        while (rem) {
+            const int e = __ffs(rem) - 1;
+            rem &= rem - 1;
+            const uint32_t geo = c_edge_geo[e];
+            const int axis = geo & 3;
+            const int lox = (geo >> 2) & 1, loy = (geo >> 3) & 1, loz = (geo >> 4) & 1;
+            const bool own_low = (geo >> 5) & 1;
+            const float s_lo = s_c[(geo >> 6) & 7][tid], s_hi = s_c[(geo >> 9) & 7][tid];
+            // this cell's own sample (pass 1): t in its own orientation
+            const float t = s_t[e][tid];
+            const float along = own_low ? t : 1.f - t;
+            const float t_lo = own_low ? t : lerp_t(s_lo, s_hi);
+            const float pu = axis == 0 ? along : (float)lox;
+            const float pv = axis == 1 ? along : (float)loy;
+            const float pw = axis == 2 ? along : (float)loz;
+            const int o1 = axis == 0 ? loy : lox, o2 = axis == 2 ? loy : loz;
+            const float3 n = edge_normal(g, make_int3(i + lox, j + loy, k + loz), axis, o1, o2, s_lo, s_hi, t_lo,
+                                         pu, pv, pw, c, W, ill);
             const float qx = pu - cu, qy = (pv - cv) * fy, qz = (pw - cw) * fz;
             const float nb = n.x * qx + n.y * qy + n.z * qz;
             kahan_add(M00, K00, n.x * n.x); kahan_add(M01, K01, n.x * n.y); kahan_add(M02, K02, n.x * n.z);
@@ -325,7 +330,7 @@ k_cell_qef(QefParams P) {
             // FP32 cannot be trusted: the FP64 path recomputes this cell from the grid.
             const unsigned int slot = atomicAdd(P.esc_count, 1u);
             P.esc_list[slot] = (uint32_t)r;
-            store_vertex(P, r, i, j, k, cu, cv, cw, 0.f, 0.f, 0.f);
+            store_vertex(P, r, i, j, k, cu, cv, cw);
             continue;
         }
         // Rank-1 certificate: lambda1 by power iteration, lambda2 + lambda3 = trace - lambda1.
@@ -349,21 +354,19 @@ k_cell_qef(QefParams P) {
         // certified rank 1 with lambda2/lambda1 < 0.01: four power steps converge to ~1e-8
         if (lam1 > thr * (1.f + P.band) && rest < thr * (1.f - P.band) && rest < 0.01f * lam1) {
             const float proj = (x0 * R0 + x1 * R1 + x2 * R2) / lam1;
-            store_vertex(P, r, i, j, k, cu, cv, cw, x0 * proj, x1 * proj, x2 * proj);
-            atomicAdd(&s_hist[0], 1u);
+            store_vertex(P, r, i, j, k, cu + x0 * proj, cv + x1 * proj / fy, cw + x2 * proj / fz);
+            P.vclass[r] = kVcRank1;
+            atomicAdd(&s_hist, 1u);
         } else {
             const unsigned int slot = atomicAdd(P.hard_count, 1u);
             P.hard_list[slot] = (uint32_t)r;
             P.hard_data[3 * (size_t)slot + 0] = make_float4(M00, M01, M02, M11);
             P.hard_data[3 * (size_t)slot + 1] = make_float4(M12, M22, R0, R1);
             P.hard_data[3 * (size_t)slot + 2] = make_float4(R2, cu, cv, cw);
-            atomicAdd(&s_hist[1], 1u);
         }
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        if (s_hist[0]) atomicAdd(P.rank_hist + 1, (unsigned long long)s_hist[0]);
-    }
+    if (threadIdx.x == 0 && s_hist) atomicAdd(P.rank_hist + 1, (unsigned long long)s_hist);
 }
 
 cudaError_t launch_cell_qef(const QefParams& P, int num_sms, cudaStream_t s) {
@@ -387,6 +390,7 @@ __device__ __forceinline__ void jacobi3f(float a[3][3], float V[3][3]) {
         const float off = a[0][1] * a[0][1] + a[0][2] * a[0][2] + a[1][2] * a[1][2];
         const float diag = a[0][0] * a[0][0] + a[1][1] * a[1][1] + a[2][2] * a[2][2];
         if (off <= 1e-14f * diag || off == 0.f) break;
+#pragma unroll
         for (int pq = 0; pq < 3; ++pq) {
             const int p = pq == 2 ? 1 : 0;
             const int q = pq == 0 ? 1 : 2;
@@ -453,7 +457,10 @@ k_cell_jacobi(QefParams P) {
             const unsigned int slot = atomicAdd(P.esc_count, 1u);
             P.esc_list[slot] = r;
         }
-        store_vertex(P, r, i, j, k, d2.y, d2.z, d2.w, wx, wy, wz);
+        const GridDesc& g = P.g;
+        const float wx1 = width_axis(g, 0, i), wy1 = width_axis(g, 1, j), wz1 = width_axis(g, 2, k);
+        store_vertex(P, r, i, j, k, d2.y + wx, d2.z + wy * (wx1 / wy1), d2.w + wz * (wx1 / wz1));
+        P.vclass[r] = kVcJacobi;
     }
     __syncthreads();
     if (threadIdx.x < 4 && s_hist[threadIdx.x]) atomicAdd(P.rank_hist + threadIdx.x, (unsigned long long)s_hist[threadIdx.x]);

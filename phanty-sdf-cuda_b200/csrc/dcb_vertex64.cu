@@ -83,19 +83,13 @@ __device__ bool hermite(const Cell64& C, int e, double p[3], double n[3]) {
     return true;
 }
 
-// get_edge_idx_from_grid_vertices (hermite_update.cpp:41-91).
-__device__ int edge_of(int ci, int cj, int ck, int i0, int j0, int k0, int i1, int j1, int k1) {
-    const int di0 = i0 - ci, dj0 = j0 - cj, dk0 = k0 - ck;
-    const int di1 = i1 - ci, dj1 = j1 - cj, dk1 = k1 - ck;
-    for (int e = 0; e < 12; ++e) {
-        const int a = edge_a(e), b = edge_b(e);
-        const bool fwd = di0 == corner_dx(a) && dj0 == corner_dy(a) && dk0 == corner_dz(a) &&
-                         di1 == corner_dx(b) && dj1 == corner_dy(b) && dk1 == corner_dz(b);
-        const bool bwd = di0 == corner_dx(b) && dj0 == corner_dy(b) && dk0 == corner_dz(b) &&
-                         di1 == corner_dx(a) && dj1 == corner_dy(a) && dk1 == corner_dz(a);
-        if (fwd || bwd) return e;
-    }
-    return -1;
+// The cell's local index of a grid edge along `axis` at local perpendicular coordinates
+// (l1, l2) in {0,1}: the unique match get_edge_idx_from_grid_vertices finds, as a table.
+__device__ __forceinline__ int local_edge(int axis, int l1, int l2) {
+    const int q = l1 + 2 * l2;
+    if (axis == 0) return 2 * q;                          // (y,z): 00->0 10->2 01->4 11->6
+    if (axis == 1) return q == 0 ? 3 : q == 1 ? 1 : q == 2 ? 7 : 5;   // (x,z)
+    return q == 0 ? 8 : q == 1 ? 9 : q == 2 ? 11 : 10;    // (x,y)
 }
 
 // Hermite sample of edge e of cell (i,j,k) with the 4-cell averaged normal when the edge
@@ -125,7 +119,7 @@ __device__ bool edge_sample(const GridDesc& g, const Cell64& C, int i, int j, in
         Cell64 X;
         load_cell(g, cc[0], cc[1], cc[2], X);
         if (!active(X)) return true;
-        const int ex = edge_of(cc[0], cc[1], cc[2], Pm[0], Pm[1], Pm[2], PM[0], PM[1], PM[2]);
+        const int ex = local_edge(axis, Pm[d1] - cc[d1], Pm[d2] - cc[d2]);
         double px[3];
         if (ex < 0 || !hermite(X, ex, px, nq[q])) return true;
     }
@@ -172,25 +166,117 @@ __device__ void jacobi3(double a[3][3], double V[3][3]) {
     }
 }
 
+// One (edge, cell) task of the 4-cell averaging: cell q around edge e of the centre cell
+// (q = 0 owner at the edge's minimum endpoint, 1 = -d1, 2 = -d2, 3 = both).
+struct Task64 {
+    double n[3];
+    double p[3];
+    int flags;   // bit0 valid sample, bit1 cell active, bit2 edge inside, bit3 own cell
+};
+
+__device__ void run_task(const GridDesc& g, const Cell64& C, int i, int j, int k, int T, Task64& R) {
+    R.flags = 0;
+    R.n[0] = R.n[1] = R.n[2] = 0.0;
+    R.p[0] = R.p[1] = R.p[2] = 0.0;
+    const int e = T >> 2, q = T & 3;
+    const int a = edge_a(e), b = edge_b(e);
+    if (C.cs[a] * C.cs[b] > 0.0) return;                 // no Hermite sample on this edge
+    const int Pa[3] = {i + corner_dx(a), j + corner_dy(a), k + corner_dz(a)};
+    const int Pb[3] = {i + corner_dx(b), j + corner_dy(b), k + corner_dz(b)};
+    int Pm[3], PM[3];
+    for (int d = 0; d < 3; ++d) { Pm[d] = min(Pa[d], Pb[d]); PM[d] = max(Pa[d], Pb[d]); }
+    const bool in0 = Pm[0] > 0 && Pm[0] < g.nx - 1 && Pm[1] > 0 && Pm[1] < g.ny - 1 && Pm[2] > 0 && Pm[2] < g.nz - 1;
+    const bool in1 = PM[0] > 0 && PM[0] < g.nx - 1 && PM[1] > 0 && PM[1] < g.ny - 1 && PM[2] > 0 && PM[2] < g.nz - 1;
+    const int axis = Pa[0] != Pb[0] ? 0 : (Pa[1] != Pb[1] ? 1 : 2);
+    const int d1 = axis == 0 ? 1 : 0;
+    const int d2 = axis == 2 ? 1 : 2;
+    int cc[3] = {Pm[0], Pm[1], Pm[2]};
+    if (q & 1) cc[d1] -= 1;
+    if (q & 2) cc[d2] -= 1;
+    const bool own = cc[0] == i && cc[1] == j && cc[2] == k;
+    if (in0 || in1) R.flags |= 4;
+    if (own) {
+        hermite(C, e, R.p, R.n);
+        R.flags |= 1 | 2 | 8;
+        return;
+    }
+    if (!(in0 || in1)) return;                            // neighbours only matter when averaged
+    Cell64 X;
+    load_cell(g, cc[0], cc[1], cc[2], X);
+    if (!active(X)) return;
+    R.flags |= 2;
+    const int ex = local_edge(axis, Pm[d1] - cc[d1], Pm[d2] - cc[d2]);
+    if (hermite(X, ex, R.p, R.n)) R.flags |= 1;
+}
+
+__device__ __forceinline__ double shfl_d(double v, int src) { return __shfl_sync(0xffffffffu, v, src); }
+
 // FP64 vertex of active cell (i,j,k), computed by the whole warp; valid in lane 0.
 __device__ void cell_vertex_warp(const GridDesc& g, int i, int j, int k, double thr, double out[3]) {
     const int lane = threadIdx.x & 31;
     Cell64 C;
     load_cell(g, i, j, k, C);
-    double p[3] = {0, 0, 0}, n[3] = {0, 0, 0};
-    const bool has = lane < 12 ? edge_sample(g, C, i, j, k, lane, p, n) : false;
+    // 48 tasks (12 edges x 4 cells): lane L runs tasks L and L + 32.
+    Task64 t0, t1;
+    run_task(g, C, i, j, k, lane, t0);
+    if (lane < 16) run_task(g, C, i, j, k, lane + 32, t1);
+    else t1.flags = 0, t1.n[0] = t1.n[1] = t1.n[2] = 0.0, t1.p[0] = t1.p[1] = t1.p[2] = 0.0;
+    // Lane e (< 12) gathers the four tasks of edge e: task 4e+q lives in lane (4e+q) & 31,
+    // slot (4e+q) >> 5.
+    double nq[4][3], po[3] = {0, 0, 0}, no[3] = {0, 0, 0};
+    int fq[4];
+    for (int q = 0; q < 4; ++q) {
+        const int T = 4 * lane + q;
+        const int src = T & 31;
+        const bool hi = T >= 32;
+        double a0[3], a1[3], b0[3], b1[3];
+        for (int d = 0; d < 3; ++d) {
+            a0[d] = shfl_d(t0.n[d], src); a1[d] = shfl_d(t1.n[d], src);
+            b0[d] = shfl_d(t0.p[d], src); b1[d] = shfl_d(t1.p[d], src);
+        }
+        const int f0 = __shfl_sync(0xffffffffu, t0.flags, src), f1 = __shfl_sync(0xffffffffu, t1.flags, src);
+        fq[q] = hi ? f1 : f0;
+        for (int d = 0; d < 3; ++d) nq[q][d] = hi ? a1[d] : a0[d];
+        if (fq[q] & 8) {
+            for (int d = 0; d < 3; ++d) { no[d] = nq[q][d]; po[d] = hi ? b1[d] : b0[d]; }
+        }
+    }
+    bool has = false;
+    double p[3] = {0, 0, 0}, n[3] = {0, 0, 0}, b = 0.0;
+    if (lane < 12) {
+        int own_q = -1;
+        for (int q = 0; q < 4; ++q) if (fq[q] & 8) own_q = q;
+        has = own_q >= 0;
+        if (has) {
+            p[0] = po[0]; p[1] = po[1]; p[2] = po[2];
+            n[0] = no[0]; n[1] = no[1]; n[2] = no[2];
+            // averaging (hermite_update.cpp:334-438): inside, all four cells active
+            bool all = (fq[0] & 4) != 0;
+            for (int q = 0; q < 4; ++q) all = all && (fq[q] & 3) == 3;
+            if (all) {
+                double acc[3] = {0.0, 0.0, 0.0};
+                for (int q = 0; q < 4; ++q) {
+                    if (sqrt(sq3(nq[q])) > 0) { acc[0] += nq[q][0]; acc[1] += nq[q][1]; acc[2] += nq[q][2]; }
+                }
+                normalize3(acc);
+                n[0] = acc[0]; n[1] = acc[1]; n[2] = acc[2];
+            }
+            // Cell::update row (Cell.cpp:298-311), independent per row: normalise, b = n.p
+            if (sqrt(sq3(n)) > 0.0) normalize3(n);
+            b = n[0] * p[0] + n[1] * p[1] + n[2] * p[2];
+        }
+    }
     const uint32_t mask = __ballot_sync(0xffffffffu, has);
     double ATA[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, ATb[3] = {0, 0, 0}, c[3] = {0, 0, 0};
     int m = 0;
     for (int e = 0; e < 12; ++e) {           // edge order = the CPU's std::map order
         double pe[3], ne[3];
         for (int d = 0; d < 3; ++d) {
-            pe[d] = __shfl_sync(0xffffffffu, p[d], e);
-            ne[d] = __shfl_sync(0xffffffffu, n[d], e);
+            pe[d] = shfl_d(p[d], e);
+            ne[d] = shfl_d(n[d], e);
         }
+        const double bb = shfl_d(b, e);
         if (!(mask & (1u << e))) continue;
-        if (sqrt(sq3(ne)) > 0.0) normalize3(ne);
-        const double bb = ne[0] * pe[0] + ne[1] * pe[1] + ne[2] * pe[2];
         for (int r = 0; r < 3; ++r) {
             for (int s = 0; s < 3; ++s) ATA[r][s] += ne[r] * ne[s];
             ATb[r] += ne[r] * bb;
@@ -253,6 +339,7 @@ k_vertex_fp64(Vertex64Params P) {
                 P.Vf[3 * (size_t)r + 0] = (float)x[0];
                 P.Vf[3 * (size_t)r + 1] = (float)x[1];
                 P.Vf[3 * (size_t)r + 2] = (float)x[2];
+                if (P.vclass) P.vclass[r] = kVcFp64;
             }
             if (P.V64) {
                 P.V64[3 * (size_t)t + 0] = x[0];
