@@ -144,6 +144,24 @@ int dcb_copy_mesh_device(dcb_handle h, float* vertices, int32_t* faces, void* cu
  * the last mesh into a caller-owned host array of vertex_count entries. */
 int dcb_copy_cells_to_host(dcb_handle h, int64_t* cell_linear_index, void* cuda_stream);
 
+/* Active-cell marking and compaction without any device allocation (no counterpart in
+ * the reference). For callers that cannot let the library call cudaMalloc: applications
+ * that hand out all device memory from their own budget or pool, and latency-sensitive
+ * loops in which an allocation's implicit device synchronisation is not acceptable.
+ * grid->values is a device pointer; `cells` is a caller-owned DEVICE array of `capacity`
+ * entries that receives the linear index i + cx*(j + cy*k) (cx = nx-1, cy = ny-1) of every
+ * active cell in ascending order, i.e. the vertex numbering of the extraction; `*count`
+ * (host) receives the number of active cells. Returns DCB_ERR_TOO_LARGE with *count set
+ * when capacity is too small, and DCB_ERR_TOO_LARGE when the grid's scratch exceeds the
+ * fixed 16 MiB scratch array (a 450^3 grid fits; the bound is checked on every call).
+ * Scratch lives in one file-scope device array shared by all calls on a device and kept
+ * between calls: calls whose work overlaps on the GPU race. The first call on a device
+ * resolves the array's address (cudaGetSymbolAddress); make that first call before any
+ * stream capture. Runs on the current device and the given stream and returns after the
+ * result is complete. */
+int dcb_mark_active_cells_noalloc(const dcb_grid* grid, int64_t* cells, int64_t capacity,
+                                  int64_t* count, void* cuda_stream);
+
 /* Human-readable text of a status code and of the last error on this handle. */
 const char* dcb_status_string(int status);
 const char* dcb_last_error(dcb_handle h);

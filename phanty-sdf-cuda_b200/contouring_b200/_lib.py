@@ -26,6 +26,7 @@ EXPORTED = (
     "dcb_default_opts", "dcb_abi_version", "dcb_status_string", "dcb_last_error",
     "dcb_create", "dcb_destroy", "dcb_extract_device", "dcb_extract_host",
     "dcb_copy_mesh_to_host", "dcb_copy_mesh_device", "dcb_copy_cells_to_host",
+    "dcb_mark_active_cells_noalloc",
 )
 
 
@@ -111,6 +112,9 @@ def lib():
     L.dcb_copy_mesh_device.restype = ctypes.c_int
     L.dcb_copy_cells_to_host.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
     L.dcb_copy_cells_to_host.restype = ctypes.c_int
+    L.dcb_mark_active_cells_noalloc.argtypes = [P(DcbGrid), ctypes.c_void_p, ctypes.c_int64,
+                                                P(ctypes.c_int64), ctypes.c_void_p]
+    L.dcb_mark_active_cells_noalloc.restype = ctypes.c_int
     _lib = L
     return L
 
