@@ -108,3 +108,25 @@ def test_invalid_arguments(backend):
         backend.extract(DenseSdfGrid(4, 4, 4, 0.1, 0.1, 0.1, 0, 0, 0, np.zeros(10, np.float32)))
     with pytest.raises(DcbError):
         backend.extract(DenseSdfGrid(4, 4, 4, float("nan"), 0.1, 0.1, 0, 0, 0, np.zeros(64, np.float32)))
+
+
+def _golden():
+    import glob
+    import os
+    return sorted(glob.glob(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "dc_*.npz")))
+
+
+@pytest.mark.parametrize("path", _golden(), ids=lambda p: p.rsplit("/", 1)[-1][3:-4])
+def test_engine_matches_golden(backend, path):
+    """The committed oracle fixtures, checked without running the oracle."""
+    from contouring_b200 import DenseSdfGrid
+    from dc_compare import VERTEX_TOL
+    g = np.load(path)
+    grid = DenseSdfGrid(*[int(x) for x in g["dims"]], *[float(x) for x in g["spacing"]],
+                        *[float(x) for x in g["origin"]], values=g["values"])
+    mesh, stats = backend.extract(grid)
+    assert np.array_equal(backend.active_cells(), g["cells"])
+    assert np.array_equal(mesh.faces.reshape(-1, 4), g["F"])
+    V = mesh.vertices.reshape(-1, 3).astype(np.float64)
+    if len(V):
+        assert (np.abs(V - g["V"]) / g["spacing"].astype(np.float64)).max() <= VERTEX_TOL
