@@ -11,8 +11,8 @@ its own grid: weak scaling, no collective on the data path).
 Under torchrun each rank runs on its LOCAL_RANK GPU; rank 0 prints one JSON line.
 ``--impl reference`` times the CPU oracle (the FP64 restatement of the reference's
 CpuDualContouringBackend, which is single-threaded C++ in the reference and cannot be
-built here: it needs Eigen and libigl) with every host thread on a bounded z-slab of the
-same grid, and reports the same metric.
+built here: it needs Eigen and libigl) with every host thread on a bounded sample of the
+same grid (8 z-slabs spread evenly over it), and reports the same metric.
 """
 import argparse
 import json
@@ -30,9 +30,10 @@ sys.path.insert(0, os.path.join(ROOT, "phanty-sdf-cuda_b200"))
 # edge normals, QEF, Jacobi list, FP64 vertices, 3 column-scan passes, face scatter,
 # FP64 vertices for windings, FP64 windings, face order.
 KERNELS_PER_STEP = 16
-# DRAM traffic of k_mark_compact per grid point, from the ncu capture summarised in
-# profiles/k_mark_compact_csg256.txt (dram__bytes_read.sum + dram__bytes_write.sum divided
-# by the grid points of that capture; scales with the number of points). None = not measured.
+# DRAM traffic of k_mark_zmarch per grid point, from the ncu capture summarised in
+# profiles/k_mark_zmarch_csg512.md (dram__bytes_read.sum + dram__bytes_write.sum divided by
+# the grid points of that capture; the kernel streams the grid once, so traffic scales with
+# the number of points). None = not measured.
 MARK_TRAFFIC_BYTES_PER_POINT = None
 
 
@@ -104,39 +105,73 @@ def make_grid(res, device):
     return synth.csg(res, seed=0, device=device)
 
 
-def cpu_sample(values_cpu, dims, spacing, origin, zslab, threads):
-    """Time the CPU oracle on the bottom z-slab (zslab point planes) of the grid."""
+SAMPLE_SLABS = 8
+
+
+def slab_ranges(nz, planes_total):
+    """Point-plane ranges of SAMPLE_SLABS z-slabs spread evenly over the grid, about
+    planes_total planes in all (each slab at least 2 planes)."""
+    per = max(2, planes_total // SAMPLE_SLABS)
+    out = []
+    for s in range(SAMPLE_SLABS):
+        c = int((s + 0.5) * nz / SAMPLE_SLABS)
+        k0 = max(0, min(nz - per, c - per // 2))
+        out.append((k0, k0 + per))
+    return out
+
+
+def grid_axes(dims, spacing, origin):
+    """Float grid-point coordinates o + float(i) * v per axis, widened to FP64."""
+    import numpy as np
+    return [(np.float32(origin[a]) + np.arange(dims[a], dtype=np.float32) * np.float32(spacing[a])).astype(np.float64)
+            for a in range(3)]
+
+
+def cpu_sample(slabs, dims, spacing, origin, threads):
+    """Time the CPU oracle on z-slabs of the grid: ``slabs`` = [((k0, k1), float32 values of
+    planes k0..k1-1)]. Returns (Mcells/s, seconds, cells)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
-    nx, ny, nz = dims
-    kz = min(nz, zslab)
-    sub = values_cpu[: nx * ny * kz]
-    t0 = time.perf_counter()
-    r = O.dc_extract(sub, (nx, ny, kz), spacing, origin, threads=threads)
-    dt = time.perf_counter() - t0
-    cells = (nx - 1) * (ny - 1) * (kz - 1)
-    return cells / dt / 1e6, dt, cells, r["stats"]
+    nx, ny, _ = dims
+    ax = grid_axes(dims, spacing, origin)
+    dt, cells = 0.0, 0
+    for (k0, k1), v in slabs:
+        t0 = time.perf_counter()
+        O.dc_extract_positions(v, (nx, ny, k1 - k0), ax[0], ax[1], ax[2][k0:k1], threads=threads)
+        dt += time.perf_counter() - t0
+        cells += (nx - 1) * (ny - 1) * (k1 - k0 - 1)
+    return cells / dt / 1e6, dt, cells
+
+
+def _sample_text(dims, ranges, cells, res):
+    return "%d z-slabs of %dx%dx%d points spread over the %d^3 CSG grid (%d cells, %.1f%% of the grid)" % (
+        len(ranges), dims[0], dims[1], ranges[0][1] - ranges[0][0], res, cells,
+        100.0 * cells / ((dims[0] - 1) * (dims[1] - 1) * (dims[2] - 1)))
 
 
 def run_reference(args, rank, world):
-    """CPU reference arm: the oracle port with all host threads, bounded slab per step."""
+    """CPU reference arm: the oracle port with all host threads on a bounded, evenly spread
+    sample of the same grid per step."""
     import numpy as np
+    from contouring_b200 import synth
     if rank != 0:
         return 0
     threads = os.cpu_count() or 1
-    vals, dims, spacing, origin = make_grid(args.res, "cpu")
-    v = vals.numpy()
-    zslab = args.ref_zslab
+    dims = (args.res,) * 3
+    ranges = slab_ranges(args.res, args.ref_zslab)
+    slabs = []
+    for r in ranges:
+        v, _, spacing, origin = synth.csg(args.res, seed=0, device="cpu", planes=r)
+        slabs.append((r, v.numpy()))
     for _ in range(args.warmup):
-        cpu_sample(v, dims, spacing, origin, zslab, threads)
+        cpu_sample(slabs, dims, spacing, origin, threads)
     rates, secs = [], []
     for _ in range(args.steps):
-        rate, dt, cells, _ = cpu_sample(v, dims, spacing, origin, zslab, threads)
+        rate, dt, cells = cpu_sample(slabs, dims, spacing, origin, threads)
         rates.append(rate)
         secs.append(dt)
     value = float(np.median(rates))
-    sample = "z-slab of %dx%dx%d points (%d cells) of the %d^3 CSG grid per step" % (
-        dims[0], dims[1], zslab, cells, args.res)
+    sample = _sample_text(dims, ranges, cells, args.res)
     line = {
         "metric": "dc_extract_mcells_per_s", "value": round(value, 3), "unit": "Mcells/s",
         "impl": "reference", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -159,7 +194,7 @@ def main():
     ap.add_argument("--res", type=int, default=1024)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=5)
-    ap.add_argument("--ref-zslab", type=int, default=96, help="point planes per CPU sample")
+    ap.add_argument("--ref-zslab", type=int, default=96, help="point planes per CPU sample (over 8 slabs)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
@@ -250,10 +285,12 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        rate, dt, cells, _ = cpu_sample(vals.cpu().numpy(), dims, spacing, origin, args.ref_zslab, threads)
+        ranges = slab_ranges(dims[2], args.ref_zslab)
+        plane = dims[0] * dims[1]
+        slabs = [(r, vals[r[0] * plane:r[1] * plane].cpu().numpy()) for r in ranges]
+        rate, dt, cells = cpu_sample(slabs, dims, spacing, origin, threads)
         cpu = {"value": round(rate, 3), "unit": "Mcells/s", "cores": threads, "kind": "port",
-               "sample": "z-slab %dx%dx%d points (%d cells) of the same grid, %.1f s" % (
-                   dims[0], dims[1], args.ref_zslab, cells, dt)}
+               "sample": _sample_text(dims, ranges, cells, args.res) + ", %.1f s" % dt}
 
     if rank == 0:
         line = {
@@ -265,13 +302,14 @@ def main():
                        "cells": ncell, "vertices": nv, "quads": nf,
                        "l2": "input (%.2f GB) larger than L2; no flush needed" % (4 * npts / 1e9),
                        "parallelism": "replicas: one independent grid per rank"},
-            "roofline": {"bound": "hbm", "kernel": "k_mark_compact", "achieved": round(achieved, 1),
+            "roofline": {"bound": "hbm", "kernel": "k_mark_zmarch", "achieved": round(achieved, 1),
                          "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
                          "traffic": traffic, "peak_source": peak_kind,
                          "algorithmic_bytes": mark_bytes, "avg_launch_ms": round(mark_avg_ms, 4)},
             "pipeline_roofline": {"algorithmic_bytes": pipe_bytes, "achieved": round(pipe_gbs, 1),
                                   "frac": round(pipe_gbs / peak, 4), "unit": "GB/s"},
-            "stage_ms": {"mark": round(stats.marking_ms, 4), "qef": round(stats.qef_ms, 4),
+            "stage_ms": {"mark": round(stats.marking_ms, 4), "scan": round(stats.compaction_ms, 4),
+                         "qef": round(stats.qef_ms, 4),
                          "faces": round(stats.face_emission_ms, 4)},
             "escalated_fp64_cells": stats.escalated_fp64_cells, "winding_fp64_faces": stats.winding_fp64_faces,
             "e2e": {"value": round(e2e_value, 2) if e2e_value else None, "unit": "Mcells/s", "h2d_bytes_per_step": h2d,

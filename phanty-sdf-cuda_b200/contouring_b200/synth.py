@@ -27,11 +27,17 @@ def _grid_params(res, lo, hi):
     return (res, res, res), (step, step, step), (float(np.float32(lo)),) * 3
 
 
-def _eval_slabs(dims, spacing, origin, fn, device, slab_points=1 << 26):
+def _eval_slabs(dims, spacing, origin, fn, device, slab_points=1 << 26, planes=None):
+    """Evaluate fn (FP64 points -> FP64 values) at the grid points, slab by slab, cast to
+    float32. ``planes`` = (k0, k1) limits the evaluation to z planes k0..k1-1 (the same
+    values as the full grid has there)."""
     nx, ny, nz = dims
     xs = _axis(nx, origin[0], spacing[0], device).double()
     ys = _axis(ny, origin[1], spacing[1], device).double()
     zs = _axis(nz, origin[2], spacing[2], device).double()
+    if planes is not None:
+        zs = zs[planes[0]:planes[1]]
+        nz = zs.numel()
     out = torch.empty(nx * ny * nz, dtype=torch.float32, device=device)
     per = max(1, slab_points // (nx * ny))
     for k0 in range(0, nz, per):
@@ -105,14 +111,18 @@ def _csg_fn(prims, holes, device):
     return fn
 
 
-def csg(res=1024, seed=0, lo=-0.5, hi=0.5, device="cpu"):
+def csg(res=1024, seed=0, lo=-0.5, hi=0.5, device="cpu", planes=None):
     """Sharp-feature CSG: 16 boxes (half-extents U(0.05,0.2)) and 8 capped cylinders
     (radius U(0.03,0.1), height U(0.1,0.4)) under random rotations with centres
-    U(-0.3,0.3)^3, minus 4 spheres of radius U(0.05,0.15); exact CSG min/max distances."""
+    U(-0.3,0.3)^3, minus 4 spheres of radius U(0.05,0.15); exact CSG min/max distances.
+    ``planes`` = (k0, k1) returns only z planes k0..k1-1 of the res^3 grid; dims then
+    report those planes while spacing and origin stay the full grid's."""
     dims, spacing, origin = _grid_params(res, lo, hi)
     prims, holes = csg_scene(seed)
     vals = _eval_slabs(dims, spacing, origin, _csg_fn(prims, holes, device), device,
-                       slab_points=1 << 24)
+                       slab_points=1 << 24, planes=planes)
+    if planes is not None:
+        dims = (dims[0], dims[1], vals.numel() // (dims[0] * dims[1]))
     return vals, dims, spacing, origin
 
 

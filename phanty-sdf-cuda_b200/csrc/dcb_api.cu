@@ -175,6 +175,7 @@ int run_pipeline(dcb_context* h, const dcb_grid* in, const dcb_opts* o, cudaStre
     mp.g = g; mp.R = R; mp.KZ = (int)KZ; mp.nxt = nxt;
     mp.bits = as<uint32_t>(h->bits); mp.seg_count = as<uint32_t>(h->seg_count); mp.vec4 = vec4;
     DCB_TRY(h, launch_mark(mp, s), "launch mark");
+    DCB_TRY(h, cudaEventRecord(h->ev[6], s), "event");
     DCB_TRY(h, launch_scan(mp.seg_count, nseg, as<uint32_t>(h->partials), as<uint32_t>(h->seg_start),
                            &dc->total_active, s), "launch segment scan");
     DCB_TRY(h, cudaEventRecord(h->ev[2], s), "event");
@@ -287,8 +288,8 @@ int run_pipeline(dcb_context* h, const dcb_grid* in, const dcb_opts* o, cudaStre
 void fill_times(dcb_context* h, dcb_stats* st, bool upload) {
     if (!st) return;
     st->upload_ms = upload ? elapsed(h->ev[0], h->ev[1]) : 0.f;
-    st->marking_ms = elapsed(h->ev[1], h->ev[2]);
-    st->compaction_ms = 0.f;
+    st->marking_ms = elapsed(h->ev[1], h->ev[6]);       // the mark kernel alone
+    st->compaction_ms = elapsed(h->ev[6], h->ev[2]);    // segment scan
     st->qef_ms = elapsed(h->ev[2], h->ev[3]);
     st->face_emission_ms = elapsed(h->ev[3], h->ev[4]);
 }
