@@ -83,9 +83,9 @@ typedef struct {
     int64_t vertex_count;
     int64_t face_count;
     float upload_ms;
-    float marking_ms;        /* fused mark + compaction kernel */
-    float compaction_ms;     /* 0: fused into marking */
-    float qef_ms;            /* Hermite + averaging + QEF (FP32 and FP64 passes) */
+    float marking_ms;        /* the mark kernel (active bits + segment counts) */
+    float compaction_ms;     /* segment scan */
+    float qef_ms;            /* rank expansion, Hermite + averaging + QEF (FP32 and FP64) */
     float face_emission_ms;  /* column scan + face scatter + ordering */
     float download_ms;
     float total_ms;
