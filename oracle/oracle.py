@@ -123,3 +123,27 @@ def dc_extract(values, dims, spacing, origin, svd_threshold=0.01, threads=0):
         lib.dco_free(h)
     stats = {k: getattr(st, k) for k, _ in _Stats._fields_}
     return {"V": V, "F": F, "cells": cells, "eig": eig, "nrows": nrows, "stats": stats}
+
+
+def triangulate(V, F):
+    """triangulate_v1 (src/cpp/contouring.cpp:88-113) with orient_triangles_for_quad
+    (:40-86): quad (a,b,c,d) -> (a,b,c), (a,c,d), each flipped when its normal points against
+    the quad normal (pb-pa)x(pd-pa) [fallback (pc-pa)x(pd-pa) below 1e-24; none below that
+    too]. V are the FP64 vertices, F the quads; returns int32 triangles (2 per quad)."""
+    F = np.asarray(F, np.int64).reshape(-1, 4)
+    V = np.asarray(V, np.float64)
+    a, b, c, d = F[:, 0], F[:, 1], F[:, 2], F[:, 3]
+    pa, pb, pc, pd = V[a], V[b], V[c], V[d]
+
+    def dot(u, v):
+        return (u[:, 0] * v[:, 0] + u[:, 1] * v[:, 1]) + u[:, 2] * v[:, 2]
+    qn = np.cross(pb - pa, pd - pa)
+    fb = dot(qn, qn) < 1e-24
+    qn[fb] = np.cross(pc - pa, pd - pa)[fb]
+    orient = ~(dot(qn, qn) < 1e-24)
+    flip0 = orient & (dot(np.cross(pb - pa, pc - pa), qn) < 0.0)
+    flip1 = orient & (dot(np.cross(pc - pa, pd - pa), qn) < 0.0)
+    T = np.empty((len(F), 2, 3), np.int64)
+    T[:, 0, 0], T[:, 0, 1], T[:, 0, 2] = a, np.where(flip0, c, b), np.where(flip0, b, c)
+    T[:, 1, 0], T[:, 1, 1], T[:, 1, 2] = a, np.where(flip1, d, c), np.where(flip1, c, d)
+    return T.reshape(-1, 3).astype(np.int32)

@@ -179,6 +179,7 @@ class B200DualContouringBackend:
         self.device = int(device)
         self.options = options if options is not None else ContouringOptions()
         self._last_nv = 0
+        self._last_vpf = 4
 
     def close(self):
         if getattr(self, "_h", None):
@@ -208,6 +209,7 @@ class B200DualContouringBackend:
         _lib.check(self._L.dcb_extract_host(self._h, ctypes.byref(gc), ctypes.byref(self.options.to_c()),
                                             ctypes.byref(mh), ctypes.byref(st), ctypes.c_void_p(s)), self._h)
         self._last_nv = mh.vertex_count
+        self._last_vpf = mh.verts_per_face
         return self._host_mesh(mh), DualContouringStats.from_c(st)
 
     @staticmethod
@@ -233,7 +235,7 @@ class B200DualContouringBackend:
         V, F, stats = self.extract_tensor_ptr(grid, stream)
         nv, nf = stats.vertex_count, stats.face_count
         hv = np.empty(3 * nv, np.float32)
-        hf = np.empty(4 * nf, np.int32)
+        hf = np.empty(self._last_vpf * nf, np.int32)
         s = _current_stream() if stream is None else stream
         _lib.check(self._L.dcb_copy_mesh_to_host(self._h, hv.ctypes.data if nv else None,
                                                  hf.ctypes.data if nf else None, ctypes.c_void_p(s)), self._h)
@@ -249,6 +251,7 @@ class B200DualContouringBackend:
         _lib.check(self._L.dcb_extract_device(self._h, ctypes.byref(gc), ctypes.byref(self.options.to_c()),
                                               ctypes.byref(md), ctypes.byref(st), ctypes.c_void_p(s)), self._h)
         self._last_nv = md.vertex_count
+        self._last_vpf = md.verts_per_face
         return md.vertices, md.faces, DualContouringStats.from_c(st)
 
     def extract_tensor(self, values, dims, spacing, origin):
@@ -258,7 +261,7 @@ class B200DualContouringBackend:
         g = DenseSdfGridDevice(*dims, *spacing, *origin, d_values=values)
         _, _, stats = self.extract_tensor_ptr(g)
         V = torch.empty((stats.vertex_count, 3), dtype=torch.float32, device=values.device)
-        F = torch.empty((stats.face_count, 4), dtype=torch.int32, device=values.device)
+        F = torch.empty((stats.face_count, self._last_vpf), dtype=torch.int32, device=values.device)
         s = torch.cuda.current_stream().cuda_stream
         _lib.check(self._L.dcb_copy_mesh_device(self._h, V.data_ptr() if V.numel() else None,
                                                 F.data_ptr() if F.numel() else None, ctypes.c_void_p(s)), self._h)

@@ -35,7 +35,7 @@ struct Counters {
     unsigned int wind_count;
     unsigned int hard_count;
     unsigned int v64_count;
-    unsigned int pad;
+    unsigned int tri_count;           // quads whose triangle orientation goes to FP64
     unsigned long long rank_hist[4];
     unsigned long long face_total;
 };
@@ -56,11 +56,12 @@ struct dcb_context {
     cudaEvent_t ev[8] = {};
     DevBuf grid, bits, super, list, seg_count, seg_start, counters, V, vclass, fmask, col_count, col_fill,
         col_start, partials, esc_list, hard_list, hard_data, stage_quad, stage_key, faces, wind_items,
-        v64_index, v64_cells, V64;
+        v64_index, v64_cells, V64, tris, tri_items;
     void* h_counters = nullptr;       // pinned Counters
     void* hV = nullptr; size_t hV_bytes = 0;
     void* hF = nullptr; size_t hF_bytes = 0;
-    int64_t nv = 0, nf = 0;
+    int64_t nv = 0, nf = 0;           // vertices; output faces (quads or triangles)
+    int vpf = 4;                      // output vertices per face
     int cx = 0, cy = 0;
 };
 
@@ -106,6 +107,9 @@ cudaError_t ensure_host(void*& p, size_t& have, size_t bytes) {
 }
 
 template <typename T> T* as(DevBuf& b) { return reinterpret_cast<T*>(b.p); }
+
+// The output face array of the last extraction: quads, or their triangles.
+int32_t* face_ptr(dcb_context* h) { return reinterpret_cast<int32_t*>(h->vpf == 3 ? h->tris.p : h->faces.p); }
 
 bool finite_pos(float x) { return std::isfinite(x); }
 
@@ -186,6 +190,7 @@ int run_pipeline(dcb_context* h, const dcb_grid* in, const dcb_opts* o, cudaStre
 
     h->nv = nv;
     h->nf = 0;
+    h->vpf = o->emit_triangles ? 3 : 4;
     h->cx = g.cx;
     h->cy = g.cy;
     if (st) {
@@ -266,6 +271,24 @@ int run_pipeline(dcb_context* h, const dcb_grid* in, const dcb_opts* o, cudaStre
     DCB_TRY(h, launch_winding_fp64(wp, wind_cap, h->num_sms, s), "launch winding fp64");
     DCB_TRY(h, launch_face_order(fp.stage_quad, fp.stage_key, fp.col_start, fp.col_count, &dc->face_total,
                                  as<int4>(h->faces), 3 * nv, h->num_sms, s), "launch face order");
+    if (o->emit_triangles) {
+        // 4) quads -> triangles; FP64 vertices for the quads FP32 cannot orient (the winding
+        // pass's FP64 vertices are recomputed too: same values, and few).
+        DCB_TRY(h, ensure(h->tris, sizeof(int) * 6 * 3 * nv), "alloc triangles");
+        DCB_TRY(h, ensure(h->tri_items, sizeof(uint32_t) * wind_cap), "alloc triangle list");
+        TriParams tp;
+        tp.quads = as<int4>(h->faces); tp.nquads = &dc->face_total; tp.V = qp.V; tp.vclass = qp.vclass;
+        tp.hmax = fp.hmax; tp.tris = as<int>(h->tris); tp.items = as<uint32_t>(h->tri_items);
+        tp.item_count = &dc->tri_count; tp.item_cap = (unsigned int)wind_cap;
+        tp.v64_index = fp.v64_index; tp.v64_cells = fp.v64_cells; tp.v64_count = fp.v64_count;
+        tp.v64_cap = fp.v64_cap; tp.err = &dc->err;
+        DCB_TRY(h, launch_triangulate(tp, 3 * nv, h->num_sms, s), "launch triangulate");
+        DCB_TRY(h, launch_vertex_fp64(w64, v64_cap, h->num_sms, s), "launch fp64 vertices for triangles");
+        Tri64Params t64;
+        t64.quads = tp.quads; t64.items = tp.items; t64.count = tp.item_count; t64.cap = tp.item_cap;
+        t64.v64_index = fp.v64_index; t64.V64 = w64.V64; t64.tris = tp.tris; t64.err = &dc->err;
+        DCB_TRY(h, launch_tri_fp64(t64, wind_cap, h->num_sms, s), "launch triangle fp64");
+    }
     DCB_TRY(h, cudaEventRecord(h->ev[4], s), "event");
     DCB_TRY(h, cudaMemcpyAsync(hc, dc, sizeof(Counters), cudaMemcpyDeviceToHost, s), "read counters");
     DCB_TRY(h, cudaStreamSynchronize(s), "pipeline");
@@ -273,7 +296,8 @@ int run_pipeline(dcb_context* h, const dcb_grid* in, const dcb_opts* o, cudaStre
         return fail(h, hc->err == kErrTimeout ? DCB_ERR_TIMEOUT : DCB_ERR_INTERNAL,
                     hc->err == kErrOverflow ? "FP64 work list overflow" : "device error flag set");
     }
-    h->nf = (int64_t)hc->face_total;
+    h->vpf = o->emit_triangles ? 3 : 4;
+    h->nf = (int64_t)hc->face_total * (o->emit_triangles ? 2 : 1);
     if (st) {
         st->face_count = h->nf;
         st->qef_fallback_count = hc->esc_count;
@@ -356,7 +380,8 @@ int dcb_destroy(dcb_handle h) {
     DevBuf* bufs[] = {&h->grid, &h->bits, &h->super, &h->list, &h->seg_count, &h->seg_start, &h->counters,
                       &h->V, &h->vclass, &h->fmask, &h->col_count, &h->col_fill, &h->col_start,
                       &h->partials, &h->esc_list, &h->hard_list, &h->hard_data, &h->stage_quad,
-                      &h->stage_key, &h->faces, &h->wind_items, &h->v64_index, &h->v64_cells, &h->V64};
+                      &h->stage_key, &h->faces, &h->wind_items, &h->v64_index, &h->v64_cells, &h->V64,
+                      &h->tris, &h->tri_items};
     for (DevBuf* b : bufs) if (b->p) cudaFree(b->p);
     if (h->h_counters) cudaFreeHost(h->h_counters);
     if (h->hV) cudaFreeHost(h->hV);
@@ -374,7 +399,6 @@ int dcb_extract_device(dcb_handle h, const dcb_grid* grid, const dcb_opts* opts,
     dcb_default_opts(&def);
     const dcb_opts* o = opts ? opts : &def;
     if (o->method != DCB_METHOD_DUAL_CONTOURING) return fail(h, DCB_ERR_NOT_SUPPORTED, "only dual contouring is implemented");
-    if (o->emit_triangles) return fail(h, DCB_ERR_NOT_SUPPORTED, "triangle output is not implemented");
     if (!(o->svd_threshold >= 0.0)) return fail(h, DCB_ERR_INVALID_ARGUMENT, "svd_threshold must be >= 0");
     if (cudaSetDevice(h->device) != cudaSuccess) { cudaGetLastError(); return fail(h, DCB_ERR_CUDA, "set device"); }
     cudaStream_t s = reinterpret_cast<cudaStream_t>(cuda_stream);
@@ -388,9 +412,9 @@ int dcb_extract_device(dcb_handle h, const dcb_grid* grid, const dcb_opts* opts,
     if (out) {
         out->vertex_count = h->nv;
         out->face_count = h->nf;
-        out->verts_per_face = 4;
+        out->verts_per_face = h->vpf;
         out->vertices = as<float>(h->V);
-        out->faces = as<int32_t>(h->faces);
+        out->faces = face_ptr(h);
         out->cell_coords = as<uint64_t>(h->list);
     }
     return DCB_OK;
@@ -405,7 +429,6 @@ int dcb_extract_host(dcb_handle h, const dcb_grid* grid, const dcb_opts* opts, d
     dcb_default_opts(&def);
     const dcb_opts* o = opts ? opts : &def;
     if (o->method != DCB_METHOD_DUAL_CONTOURING) return fail(h, DCB_ERR_NOT_SUPPORTED, "only dual contouring is implemented");
-    if (o->emit_triangles) return fail(h, DCB_ERR_NOT_SUPPORTED, "triangle output is not implemented");
     cudaStream_t s = reinterpret_cast<cudaStream_t>(cuda_stream);
     if (stats) std::memset(stats, 0, sizeof(*stats));
     const size_t npts = (size_t)grid->nx * grid->ny * grid->nz;
@@ -418,9 +441,9 @@ int dcb_extract_host(dcb_handle h, const dcb_grid* grid, const dcb_opts* opts, d
     rc = run_pipeline(h, &dg, o, s, stats);
     if (rc != DCB_OK) return rc;
     DCB_TRY(h, ensure_host(h->hV, h->hV_bytes, sizeof(float) * 3 * h->nv), "alloc host vertices");
-    DCB_TRY(h, ensure_host(h->hF, h->hF_bytes, sizeof(int32_t) * 4 * h->nf), "alloc host faces");
+    DCB_TRY(h, ensure_host(h->hF, h->hF_bytes, sizeof(int32_t) * h->vpf * h->nf), "alloc host faces");
     if (h->nv) DCB_TRY(h, cudaMemcpyAsync(h->hV, h->V.p, sizeof(float) * 3 * h->nv, cudaMemcpyDeviceToHost, s), "download vertices");
-    if (h->nf) DCB_TRY(h, cudaMemcpyAsync(h->hF, h->faces.p, sizeof(int32_t) * 4 * h->nf, cudaMemcpyDeviceToHost, s), "download faces");
+    if (h->nf) DCB_TRY(h, cudaMemcpyAsync(h->hF, face_ptr(h), sizeof(int32_t) * h->vpf * h->nf, cudaMemcpyDeviceToHost, s), "download faces");
     DCB_TRY(h, cudaEventRecord(h->ev[5], s), "event");
     DCB_TRY(h, cudaStreamSynchronize(s), "download");
     fill_times(h, stats, true);
@@ -431,7 +454,7 @@ int dcb_extract_host(dcb_handle h, const dcb_grid* grid, const dcb_opts* opts, d
     if (out) {
         out->vertex_count = h->nv;
         out->face_count = h->nf;
-        out->verts_per_face = 4;
+        out->verts_per_face = h->vpf;
         out->vertices = reinterpret_cast<const float*>(h->hV);
         out->faces = reinterpret_cast<const int32_t*>(h->hF);
     }
@@ -443,7 +466,7 @@ int dcb_copy_mesh_to_host(dcb_handle h, float* vertices, int32_t* faces, void* c
     cudaStream_t s = reinterpret_cast<cudaStream_t>(cuda_stream);
     if (cudaSetDevice(h->device) != cudaSuccess) { cudaGetLastError(); return fail(h, DCB_ERR_CUDA, "set device"); }
     if (vertices && h->nv) DCB_TRY(h, cudaMemcpyAsync(vertices, h->V.p, sizeof(float) * 3 * h->nv, cudaMemcpyDeviceToHost, s), "copy vertices");
-    if (faces && h->nf) DCB_TRY(h, cudaMemcpyAsync(faces, h->faces.p, sizeof(int32_t) * 4 * h->nf, cudaMemcpyDeviceToHost, s), "copy faces");
+    if (faces && h->nf) DCB_TRY(h, cudaMemcpyAsync(faces, face_ptr(h), sizeof(int32_t) * h->vpf * h->nf, cudaMemcpyDeviceToHost, s), "copy faces");
     DCB_TRY(h, cudaStreamSynchronize(s), "copy mesh");
     return DCB_OK;
 }
@@ -453,7 +476,7 @@ int dcb_copy_mesh_device(dcb_handle h, float* vertices, int32_t* faces, void* cu
     cudaStream_t s = reinterpret_cast<cudaStream_t>(cuda_stream);
     if (cudaSetDevice(h->device) != cudaSuccess) { cudaGetLastError(); return fail(h, DCB_ERR_CUDA, "set device"); }
     if (vertices && h->nv) DCB_TRY(h, cudaMemcpyAsync(vertices, h->V.p, sizeof(float) * 3 * h->nv, cudaMemcpyDeviceToDevice, s), "copy vertices");
-    if (faces && h->nf) DCB_TRY(h, cudaMemcpyAsync(faces, h->faces.p, sizeof(int32_t) * 4 * h->nf, cudaMemcpyDeviceToDevice, s), "copy faces");
+    if (faces && h->nf) DCB_TRY(h, cudaMemcpyAsync(faces, face_ptr(h), sizeof(int32_t) * h->vpf * h->nf, cudaMemcpyDeviceToDevice, s), "copy faces");
     return DCB_OK;
 }
 

@@ -133,6 +133,37 @@ __device__ __forceinline__ float3 cross3(float3 a, float3 b) {
 }
 __device__ __forceinline__ float dot3(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 
+// Bound on each stored vertex's deviation from the CPU's double vertex: its solve class (in
+// cell widths) plus one ulp of the stored float coordinates; the largest of the four.
+__device__ __forceinline__ float quad_vertex_bound(const uint8_t* __restrict__ vclass, uint32_t r0, uint32_t r1,
+                                                  uint32_t r2, uint32_t r3, float3 pa, float3 pb, float3 pc,
+                                                  float3 pd, float hmax) {
+    const uint8_t cls[4] = {vclass[r0], vclass[r1], vclass[r2], vclass[r3]};
+    const float3 pv[4] = {pa, pb, pc, pd};
+    float dv = 0.f;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const float ce = cls[q] == kVcRank1 ? 2e-6f : (cls[q] == kVcJacobi ? 1e-4f : 0.f);
+        const float mag = fmaxf(fabsf(pv[q].x), fmaxf(fabsf(pv[q].y), fabsf(pv[q].z)));
+        dv = fmaxf(dv, ce * hmax + mag * 1.2e-7f);
+    }
+    return dv;
+}
+
+// Ask for the FP64 vertex of cell rank r once (v64_index: -1 none, -2 being claimed).
+__device__ __forceinline__ void request_fp64_vertex(int* v64_index, uint32_t* v64_cells, unsigned int* v64_count,
+                                                    unsigned long long v64_cap, int* err, uint32_t r) {
+    if (atomicCAS(&v64_index[r], -1, -2) == -1) {
+        const unsigned int v = atomicAdd(v64_count, 1u);
+        if (v < v64_cap) {
+            v64_cells[v] = r;
+            v64_index[r] = (int)v;
+        } else {
+            set_error(err, kErrOverflow);
+        }
+    }
+}
+
 __global__ void __launch_bounds__(128)
 k_face_scatter(FaceParams P) {
     const GridDesc& g = P.g;
@@ -161,19 +192,7 @@ k_face_scatter(FaceParams P) {
             const float3 g1 = grid_gradient32(g, i + (axis == 0), j + (axis == 1), k + (axis == 2));
             const float3 gn = make_float3(g0.x + g1.x, g0.y + g1.y, g0.z + g1.z);
             const float3 pa = ldv(P.V, r0), pb = ldv(P.V, r1), pc = ldv(P.V, r2), pd = ldv(P.V, r3);
-            // Bound on each stored vertex's deviation from the CPU's double vertex: its
-            // solve class (in cell widths) plus one ulp of the stored float coordinates.
-            float dv = 0.f;
-            {
-                const uint8_t cls[4] = {P.vclass[r0], P.vclass[r1], P.vclass[r2], P.vclass[r3]};
-                const float3 pv[4] = {pa, pb, pc, pd};
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const float ce = cls[q] == kVcRank1 ? 2e-6f : (cls[q] == kVcJacobi ? 1e-4f : 0.f);
-                    const float mag = fmaxf(fabsf(pv[q].x), fmaxf(fabsf(pv[q].y), fabsf(pv[q].z)));
-                    dv = fmaxf(dv, ce * P.hmax + mag * 1.2e-7f);
-                }
-            }
+            const float dv = quad_vertex_bound(P.vclass, r0, r1, r2, r3, pa, pb, pc, pd, P.hmax);
             const float3 ba = sub3(pb, pa), da = sub3(pd, pa), ca = sub3(pc, pa);
             float3 qn = cross3(ba, da);
             float qn2 = dot3(qn, qn);
@@ -208,17 +227,8 @@ k_face_scatter(FaceParams P) {
                 // request the FP64 vertex of each of the four cells once
                 const uint32_t rq[4] = {r0, r1, r2, r3};
 #pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    if (atomicCAS(&P.v64_index[rq[q]], -1, -2) == -1) {
-                        const unsigned int v = atomicAdd(P.v64_count, 1u);
-                        if (v < P.v64_cap) {
-                            P.v64_cells[v] = rq[q];
-                            P.v64_index[rq[q]] = (int)v;
-                        } else {
-                            set_error(P.err, kErrOverflow);
-                        }
-                    }
-                }
+                for (int q = 0; q < 4; ++q)
+                    request_fp64_vertex(P.v64_index, P.v64_cells, P.v64_count, P.v64_cap, P.err, rq[q]);
             }
         }
     }
@@ -259,6 +269,70 @@ cudaError_t launch_face_order(const int4* stage_quad, const uint2* stage_key, co
     const long long cap = (long long)num_sms * 16;
     if (blocks > cap) blocks = cap;
     k_face_order<<<(unsigned)blocks, 256, 0, s>>>(stage_quad, stage_key, col_start, col_count, nfaces, faces);
+    return cudaGetLastError();
+}
+
+// ---- quad -> triangles -----------------------------------------------------------------
+//
+// triangulate_v1 (contouring.cpp:88-113): quad (a,b,c,d) -> (a,b,c), (a,c,d); each triangle
+// is flipped (second and third index swapped) when its normal points against the quad
+// normal (pb-pa)x(pd-pa), with the fallback (pc-pa)x(pd-pa) below a squared norm of 1e-24 and
+// no orientation at all when that is below 1e-24 too (orient_triangles_for_quad,
+// contouring.cpp:40-86). Decided here in FP32 with the vertex error bounds; quads whose
+// decision the bounds do not settle are listed and re-decided from FP64 vertices
+// (k_tri_fp64).
+__global__ void __launch_bounds__(256)
+k_triangulate(TriParams P) {
+    const long long nq = (long long)*P.nquads;
+    for (long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x; f < nq;
+         f += (long long)gridDim.x * blockDim.x) {
+        const int4 q = P.quads[f];
+        const uint32_t a = (uint32_t)q.x, b = (uint32_t)q.y, c = (uint32_t)q.z, d = (uint32_t)q.w;
+        const float3 pa = ldv(P.V, a), pb = ldv(P.V, b), pc = ldv(P.V, c), pd = ldv(P.V, d);
+        const float dv = quad_vertex_bound(P.vclass, a, b, c, d, pa, pb, pc, pd, P.hmax);
+        const float3 ba = sub3(pb, pa), ca = sub3(pc, pa), da = sub3(pd, pa);
+        const float lb = sqrtf(dot3(ba, ba)), lc = sqrtf(dot3(ca, ca)), ld = sqrtf(dot3(da, da));
+        float3 qn = cross3(ba, da);
+        float dq = 2.f * dv * (lb + ld + 2.f * dv);
+        float qnl = sqrtf(dot3(qn, qn));
+        bool uncertain = (qnl - dq) < 1e-12f && (qnl + dq) >= 1e-12f;    // straddles the switch
+        if (qnl * qnl < 1e-24f) {
+            qn = cross3(ca, da);
+            dq = 2.f * dv * (lc + ld + 2.f * dv);
+            qnl = sqrtf(dot3(qn, qn));
+            uncertain |= (qnl - dq) < 1e-12f && (qnl + dq) >= 1e-12f;   // straddles "no orientation"
+        }
+        const bool orient = qnl * qnl >= 1e-24f;
+        const float3 t0 = cross3(ba, ca), t1 = cross3(ca, da);
+        const float dt0 = 2.f * dv * (lb + lc + 2.f * dv), dt1 = 2.f * dv * (lc + ld + 2.f * dv);
+        const float t0l = sqrtf(dot3(t0, t0)), t1l = sqrtf(dot3(t1, t1));
+        const float d0 = dot3(t0, qn), d1 = dot3(t1, qn);
+        if (orient) {
+            uncertain |= fabsf(d0) <= 4.f * (dt0 * qnl + t0l * dq + dt0 * dq) + 1e-5f * t0l * qnl;
+            uncertain |= fabsf(d1) <= 4.f * (dt1 * qnl + t1l * dq + dt1 * dq) + 1e-5f * t1l * qnl;
+        }
+        const bool flip0 = orient && d0 < 0.f, flip1 = orient && d1 < 0.f;
+        int* t = P.tris + 6 * f;
+        t[0] = (int)a; t[1] = flip0 ? (int)c : (int)b; t[2] = flip0 ? (int)b : (int)c;
+        t[3] = (int)a; t[4] = flip1 ? (int)d : (int)c; t[5] = flip1 ? (int)c : (int)d;
+        if (uncertain) {
+            const unsigned int w = atomicAdd(P.item_count, 1u);
+            if (w < P.item_cap) P.items[w] = (uint32_t)f;
+            else set_error(P.err, kErrOverflow);
+            request_fp64_vertex(P.v64_index, P.v64_cells, P.v64_count, P.v64_cap, P.err, a);
+            request_fp64_vertex(P.v64_index, P.v64_cells, P.v64_count, P.v64_cap, P.err, b);
+            request_fp64_vertex(P.v64_index, P.v64_cells, P.v64_count, P.v64_cap, P.err, c);
+            request_fp64_vertex(P.v64_index, P.v64_cells, P.v64_count, P.v64_cap, P.err, d);
+        }
+    }
+}
+
+cudaError_t launch_triangulate(const TriParams& P, long long max_quads, int num_sms, cudaStream_t s) {
+    if (max_quads <= 0) return cudaSuccess;
+    long long blocks = (max_quads + 255) / 256;
+    const long long cap = (long long)num_sms * 16;
+    if (blocks > cap) blocks = cap;
+    k_triangulate<<<(unsigned)blocks, 256, 0, s>>>(P);
     return cudaGetLastError();
 }
 

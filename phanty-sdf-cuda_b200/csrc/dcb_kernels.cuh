@@ -112,4 +112,34 @@ cudaError_t launch_face_order(const int4* stage_quad, const uint2* stage_key, co
                               const uint32_t* col_count, const unsigned long long* nfaces, int4* faces,
                               long long max_faces, int num_sms, cudaStream_t s);
 
+struct TriParams {
+    const int4* quads;             // final quads
+    const unsigned long long* nquads;
+    const float* V;
+    const uint8_t* vclass;
+    float hmax;
+    int* tris;                     // 2 triangles (6 ints) per quad
+    uint32_t* items;               // quads whose orientation FP32 cannot settle
+    unsigned int* item_count;
+    unsigned int item_cap;
+    int* v64_index;
+    uint32_t* v64_cells;
+    unsigned int* v64_count;
+    unsigned long long v64_cap;
+    int* err;
+};
+cudaError_t launch_triangulate(const TriParams& P, long long max_quads, int num_sms, cudaStream_t s);
+
+struct Tri64Params {
+    const int4* quads;
+    const uint32_t* items;
+    const unsigned int* count;
+    unsigned int cap;
+    const int* v64_index;
+    const double* V64;
+    int* tris;
+    int* err;
+};
+cudaError_t launch_tri_fp64(const Tri64Params& P, long long max_items, int num_sms, cudaStream_t s);
+
 }  // namespace dcb

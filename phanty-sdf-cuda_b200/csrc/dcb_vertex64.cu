@@ -410,4 +410,52 @@ cudaError_t launch_winding_fp64(const Winding64Params& P, long long max_items, i
     return cudaGetLastError();
 }
 
+// Thread per listed quad: the triangle orientations of triangulate_v1 /
+// orient_triangles_for_quad (contouring.cpp:40-113) from the FP64 vertices.
+__global__ void __launch_bounds__(128)
+k_tri_fp64(Tri64Params P) {
+    const unsigned int n = min(*P.count, P.cap);
+    for (unsigned int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const uint32_t f = P.items[t];
+        const int4 q4 = P.quads[f];
+        const int rr[4] = {q4.x, q4.y, q4.z, q4.w};
+        double pv[4][3];
+        bool ok = true;
+        for (int q = 0; q < 4; ++q) {
+            const int idx = P.v64_index[rr[q]];
+            if (idx < 0) { ok = false; break; }
+            for (int d = 0; d < 3; ++d) pv[q][d] = P.V64[3 * (size_t)idx + d];
+        }
+        if (!ok) { set_error(P.err, kErrInternal); continue; }
+        const double ba[3] = {pv[1][0] - pv[0][0], pv[1][1] - pv[0][1], pv[1][2] - pv[0][2]};
+        const double ca[3] = {pv[2][0] - pv[0][0], pv[2][1] - pv[0][1], pv[2][2] - pv[0][2]};
+        const double da[3] = {pv[3][0] - pv[0][0], pv[3][1] - pv[0][1], pv[3][2] - pv[0][2]};
+        double qn[3] = {ba[1] * da[2] - ba[2] * da[1], ba[2] * da[0] - ba[0] * da[2], ba[0] * da[1] - ba[1] * da[0]};
+        if (f64::sq3(qn) < 1e-24) {
+            qn[0] = ca[1] * da[2] - ca[2] * da[1];
+            qn[1] = ca[2] * da[0] - ca[0] * da[2];
+            qn[2] = ca[0] * da[1] - ca[1] * da[0];
+        }
+        bool flip0 = false, flip1 = false;
+        if (!(f64::sq3(qn) < 1e-24)) {
+            const double t0[3] = {ba[1] * ca[2] - ba[2] * ca[1], ba[2] * ca[0] - ba[0] * ca[2], ba[0] * ca[1] - ba[1] * ca[0]};
+            const double t1[3] = {ca[1] * da[2] - ca[2] * da[1], ca[2] * da[0] - ca[0] * da[2], ca[0] * da[1] - ca[1] * da[0]};
+            flip0 = t0[0] * qn[0] + t0[1] * qn[1] + t0[2] * qn[2] < 0.0;
+            flip1 = t1[0] * qn[0] + t1[1] * qn[1] + t1[2] * qn[2] < 0.0;
+        }
+        int* o = P.tris + 6 * (size_t)f;
+        o[0] = rr[0]; o[1] = flip0 ? rr[2] : rr[1]; o[2] = flip0 ? rr[1] : rr[2];
+        o[3] = rr[0]; o[4] = flip1 ? rr[3] : rr[2]; o[5] = flip1 ? rr[2] : rr[3];
+    }
+}
+
+cudaError_t launch_tri_fp64(const Tri64Params& P, long long max_items, int num_sms, cudaStream_t s) {
+    if (max_items <= 0) return cudaSuccess;
+    long long blocks = (max_items + 127) / 128;
+    const long long cap = (long long)num_sms * 8;
+    if (blocks > cap) blocks = cap;
+    k_tri_fp64<<<(unsigned)blocks, 128, 0, s>>>(P);
+    return cudaGetLastError();
+}
+
 }  // namespace dcb

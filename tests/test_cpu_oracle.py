@@ -152,3 +152,28 @@ def test_threads_do_not_change_results():
 def test_rejects_bad_shapes():
     with pytest.raises(ValueError):
         O.dc_extract(np.zeros(10, np.float32), (2, 2, 2), (1, 1, 1), (0, 0, 0))
+
+
+def test_triangulate_splits_and_orients():
+    """triangulate_v1 on the oracle's sphere: two triangles per quad along the a-c diagonal,
+    each wound like its quad, so the triangle mesh is closed and consistently oriented."""
+    vals, dims, sp, org = _np(_synth().cli_sphere(24))
+    r = O.dc_extract(vals, dims, sp, org)
+    T = O.triangulate(r["V"], r["F"])
+    assert T.shape == (2 * len(r["F"]), 3)
+    F = r["F"]
+    assert np.array_equal(np.sort(T[0::2], 1), np.sort(F[:, [0, 1, 2]], 1))
+    assert np.array_equal(np.sort(T[1::2], 1), np.sort(F[:, [0, 2, 3]], 1))
+    e = np.concatenate([T[:, [0, 1]], T[:, [1, 2]], T[:, [2, 0]]]).astype(np.int64)
+    key = e[:, 0] * (1 << 32) + e[:, 1]
+    assert len(np.unique(key)) == len(key)
+    assert np.array_equal(np.sort(key), np.sort(e[:, 1] * (1 << 32) + e[:, 0]))
+
+
+def test_triangulate_flips_against_the_quad_normal():
+    """A quad whose second triangle folds back is flipped; a degenerate quad is left as is."""
+    V = np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0], [0.2, 0.1, 0.0]], np.float64)
+    T = O.triangulate(V, np.array([[0, 1, 2, 3]]))
+    assert T.tolist() == [[0, 1, 2], [0, 3, 2]]
+    Z = np.zeros((4, 3))
+    assert O.triangulate(Z, np.array([[0, 1, 2, 3]])).tolist() == [[0, 1, 2], [0, 2, 3]]

@@ -130,3 +130,24 @@ def test_engine_matches_golden(backend, path):
     V = mesh.vertices.reshape(-1, 3).astype(np.float64)
     if len(V):
         assert (np.abs(V - g["V"]) / g["spacing"].astype(np.float64)).max() <= VERTEX_TOL
+
+
+@pytest.mark.parametrize("name", ["sphere32", "csg96", "noise_zeros17x23x9", "ternary", "sphere_zero_shell"])
+def test_triangles_match_oracle(backend, name):
+    """emit_triangles: triangulate_v1 of the quads, oriented from the FP64 vertices; the
+    triangles equal the oracle's triangulation of its own quads exactly."""
+    import oracle as O
+    from contouring_b200 import DenseSdfGrid
+    from dc_compare import run_oracle
+    t = _cases()[name]()
+    backend.options.emit_triangles = True
+    try:
+        mesh, stats = backend.extract(DenseSdfGrid.from_tuple(t))
+        V2, F2, st2 = backend.extract_tensor(t[0].cuda(), t[1], t[2], t[3])
+    finally:
+        backend.options.emit_triangles = False
+    ref = run_oracle(t)
+    T = O.triangulate(ref["V"], ref["F"])
+    assert stats.face_count == len(T) == 2 * len(ref["F"])
+    assert np.array_equal(mesh.faces.reshape(-1, 3), T)
+    assert np.array_equal(F2.cpu().numpy(), T)
