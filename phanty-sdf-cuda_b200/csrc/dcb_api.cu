@@ -62,6 +62,7 @@ struct dcb_context {
     void* hF = nullptr; size_t hF_bytes = 0;
     int64_t nv = 0, nf = 0;           // vertices; output faces (quads or triangles)
     int vpf = 4;                      // output vertices per face
+    int mark_ctas[2] = {0, 0};        // resident mark CTAs per SM (scalar, float4 loads)
     int cx = 0, cy = 0;
 };
 
@@ -153,8 +154,11 @@ int run_pipeline(dcb_context* h, const dcb_grid* in, const dcb_opts* o, cudaStre
     const int nxt = (g.cx + tile_cells - 1) / tile_cells;
     const int R = std::min(mark_max_rows(), g.cy);
     const long long nrb = (g.cy + R - 1) / R;
-    long long KZ = (g.cz * nxt * nrb + (long long)h->num_sms * 12 - 1) / ((long long)h->num_sms * 12);
-    KZ = std::max(8LL, std::min(64LL, KZ));
+    // About four CTAs per resident slot, each marching 8..64 planes (a single long wave
+    // measured slower at 1024^3: 0.887 vs 0.848 ms).
+    if (h->mark_ctas[vec4] == 0) h->mark_ctas[vec4] = mark_ctas_per_sm(vec4);
+    const long long slots = (long long)h->num_sms * h->mark_ctas[vec4] * 4;
+    const long long KZ = std::max(8LL, std::min(64LL, (g.cz * nxt * nrb + slots - 1) / slots));
     const long long nseg = rows * nxt;
     if (nrb > 65535 || (g.cz + KZ - 1) / KZ > 65535) return fail(h, DCB_ERR_TOO_LARGE, "grid too large for the tiling");
 

@@ -15,6 +15,7 @@ struct MarkParams {
 };
 cudaError_t launch_mark(const MarkParams& P, cudaStream_t s);
 int mark_tile_words();
+int mark_ctas_per_sm(int vec4);   // resident CTAs of the mark kernel per SM
 int mark_max_rows();
 
 struct ExpandParams {

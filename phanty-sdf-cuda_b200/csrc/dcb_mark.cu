@@ -196,6 +196,14 @@ cudaError_t launch_expand(const ExpandParams& P, int num_sms, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+int mark_ctas_per_sm(int vec4) {
+    int n = 0;
+    const cudaError_t e = vec4 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_mark_zmarch<true>, kMarkWarps * 32, 0)
+                               : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_mark_zmarch<false>, kMarkWarps * 32, 0);
+    if (e != cudaSuccess) { cudaGetLastError(); return 1; }
+    return n > 0 ? n : 1;
+}
+
 int mark_tile_words() { return kTileWords; }
 int mark_max_rows() { return kMarkWarps - 1; }
 
