@@ -162,6 +162,35 @@ int dcb_copy_cells_to_host(dcb_handle h, int64_t* cell_linear_index, void* cuda_
 int dcb_mark_active_cells_noalloc(const dcb_grid* grid, int64_t* cells, int64_t capacity,
                                   int64_t* count, void* cuda_stream);
 
+/* ---- mesh -> signed distance grid ------------------------------------------------------ */
+
+typedef struct {
+    int64_t num_bins;          /* spatial bins (about 8 grid points a side) */
+    int64_t bin_entries;       /* (bin, triangle) pairs */
+    int64_t flood_passes;      /* exterior-flood launches until nothing changed */
+    int64_t exterior_points;   /* far points that ended exterior (+10) */
+    float bins_ms;             /* triangle records, binning, in-bin ordering */
+    float band_ms;             /* closest-triangle distances near the surface */
+    float sign_ms;             /* far / exterior masks and the exterior flood */
+    float relax_ms;            /* far values and the 4 relaxation passes */
+    float total_ms;
+} dcb_sdf_stats;
+
+/* Replaces compute_mesh_sdf_device_cuda (include/mesh_to_sdf.h; src/cuda/mesh_to_sdf_cuda.cu:
+ * 740-1009, without voxelisation): vertices (float xyz) and faces (int32 triangles) are DEVICE
+ * arrays; out_values is a caller-owned DEVICE array of nx*ny*nz floats (x fastest) that
+ * receives the signed distances, ready for dcb_extract_device. Returns
+ * DCB_ERR_INVALID_ARGUMENT if a face index is out of range. */
+int dcb_mesh_to_sdf_device(dcb_handle h, const float* vertices, int64_t num_vertices, const int32_t* faces,
+                           int64_t num_faces, int nx, int ny, int nz, float ox, float oy, float oz, float vx,
+                           float vy, float vz, float* out_values, dcb_sdf_stats* stats, void* cuda_stream);
+
+/* Replaces compute_mesh_sdf_cuda (same file): host vertices and faces in, host values out
+ * (nx*ny*nz floats); returns after the values are on the host. */
+int dcb_mesh_to_sdf_host(dcb_handle h, const float* vertices, int64_t num_vertices, const int32_t* faces,
+                         int64_t num_faces, int nx, int ny, int nz, float ox, float oy, float oz, float vx,
+                         float vy, float vz, float* out_values, dcb_sdf_stats* stats, void* cuda_stream);
+
 /* Human-readable text of a status code and of the last error on this handle. */
 const char* dcb_status_string(int status);
 const char* dcb_last_error(dcb_handle h);

@@ -1,7 +1,9 @@
 """ctypes wrapper around the CPU oracle library (TEST INFRASTRUCTURE ONLY).
 
 The oracle is the FP64 C++ restatement in ``oracle/dc_oracle.cpp`` of the reference's
-``CpuDualContouringBackend::extract`` (src/cpp/dc_backend.cpp:51-125).  Only ``tests/``,
+``CpuDualContouringBackend::extract`` (src/cpp/dc_backend.cpp:51-125), and the float
+restatement in ``oracle/mts_oracle.cpp`` of its mesh -> SDF conversion
+(src/cuda/mesh_to_sdf_cuda.cu:740-1009).  Only ``tests/``,
 ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline / reference legs import this
 module, and only as the checker or the CPU baseline, never as the product path.
 """
@@ -147,3 +149,57 @@ def triangulate(V, F):
     T[:, 0, 0], T[:, 0, 1], T[:, 0, 2] = a, np.where(flip0, c, b), np.where(flip0, b, c)
     T[:, 1, 0], T[:, 1, 1], T[:, 1, 2] = a, np.where(flip1, d, c), np.where(flip1, c, d)
     return T.reshape(-1, 3).astype(np.int32)
+
+
+class _MtsStats(ctypes.Structure):
+    _fields_ = [("num_bins", ctypes.c_int64), ("bin_entries", ctypes.c_int64),
+                ("band_points", ctypes.c_int64), ("exterior_filled", ctypes.c_int64)]
+
+
+def _mts():
+    lib = _load(_MTS_LIB)
+    if not getattr(lib, "_typed", False):
+        common = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64] + [ctypes.c_int] * 3 + \
+                 [ctypes.c_float] * 6
+        lib.mts_compute.argtypes = common + [ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(_MtsStats)]
+        lib.mts_compute.restype = ctypes.c_int
+        lib.mts_band_values.argtypes = common + [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_void_p]
+        lib.mts_band_values.restype = ctypes.c_int
+        lib._typed = True
+    return lib
+
+
+def _mesh_args(V, F):
+    V = np.ascontiguousarray(np.asarray(V, np.float32).reshape(-1, 3))
+    F = np.ascontiguousarray(np.asarray(F, np.int32).reshape(-1, 3))
+    if len(F) and (F.min() < 0 or F.max() >= len(V)):
+        raise ValueError("face index out of range")
+    return V, F
+
+
+def mesh_to_sdf(V, F, dims, origin, spacing, threads=0):
+    """The whole mesh -> SDF conversion; returns (float32 values, nx*ny*nz, x fastest; stats)."""
+    V, F = _mesh_args(V, F)
+    nx, ny, nz = (int(d) for d in dims)
+    out = np.empty(nx * ny * nz, np.float32)
+    st = _MtsStats()
+    rc = _mts().mts_compute(V.ctypes.data, len(V), F.ctypes.data, len(F), nx, ny, nz,
+                            *[float(x) for x in origin], *[float(x) for x in spacing], int(threads),
+                            out.ctypes.data, ctypes.byref(st))
+    if rc != 0:
+        raise ValueError("oracle rejected the input")
+    return out, {k: getattr(st, k) for k, _ in _MtsStats._fields_}
+
+
+def mesh_band_values(V, F, dims, origin, spacing, idx, threads=0):
+    """Band values (before the sign fill and relaxation) at the listed linear point indices."""
+    V, F = _mesh_args(V, F)
+    nx, ny, nz = (int(d) for d in dims)
+    idx = np.ascontiguousarray(np.asarray(idx, np.int64))
+    out = np.empty(len(idx), np.float32)
+    rc = _mts().mts_band_values(V.ctypes.data, len(V), F.ctypes.data, len(F), nx, ny, nz,
+                                *[float(x) for x in origin], *[float(x) for x in spacing],
+                                idx.ctypes.data, len(idx), int(threads), out.ctypes.data)
+    if rc != 0:
+        raise ValueError("oracle rejected the input")
+    return out

@@ -5,8 +5,10 @@ Public names mirror the reference module ``_contouring_cpp_module`` (src/cpp/bin
 ``ContouringOptions``, ``ContouringMethod``; the new backend is ``B200DualContouringBackend``.
 """
 from .backend import (B200DualContouringBackend, ContouringMethod, ContouringOptions, DcbError,
-                      DenseSdfGrid, DenseSdfGridDevice, DualContouringMesh, DualContouringStats)
+                      DenseSdfGrid, DenseSdfGridDevice, DualContouringMesh, DualContouringStats,
+                      MeshSdfStats, mesh_to_sdf_cuda, mesh_to_sdf_tensor)
 from . import _lib
 
 __all__ = ["B200DualContouringBackend", "ContouringMethod", "ContouringOptions", "DcbError",
-           "DenseSdfGrid", "DenseSdfGridDevice", "DualContouringMesh", "DualContouringStats"]
+           "DenseSdfGrid", "DenseSdfGridDevice", "DualContouringMesh", "DualContouringStats",
+           "MeshSdfStats", "mesh_to_sdf_cuda", "mesh_to_sdf_tensor"]

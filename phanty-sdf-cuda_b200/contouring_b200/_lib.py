@@ -26,7 +26,7 @@ EXPORTED = (
     "dcb_default_opts", "dcb_abi_version", "dcb_status_string", "dcb_last_error",
     "dcb_create", "dcb_destroy", "dcb_extract_device", "dcb_extract_host",
     "dcb_copy_mesh_to_host", "dcb_copy_mesh_device", "dcb_copy_cells_to_host",
-    "dcb_mark_active_cells_noalloc",
+    "dcb_mark_active_cells_noalloc", "dcb_mesh_to_sdf_device", "dcb_mesh_to_sdf_host",
 )
 
 
@@ -67,6 +67,13 @@ class DcbMeshHost(ctypes.Structure):
     _fields_ = [("vertex_count", ctypes.c_int64), ("face_count", ctypes.c_int64),
                 ("verts_per_face", ctypes.c_int), ("vertices", ctypes.c_void_p),
                 ("faces", ctypes.c_void_p)]
+
+
+class DcbSdfStats(ctypes.Structure):
+    _fields_ = [("num_bins", ctypes.c_int64), ("bin_entries", ctypes.c_int64),
+                ("flood_passes", ctypes.c_int64), ("exterior_points", ctypes.c_int64),
+                ("bins_ms", ctypes.c_float), ("band_ms", ctypes.c_float), ("sign_ms", ctypes.c_float),
+                ("relax_ms", ctypes.c_float), ("total_ms", ctypes.c_float)]
 
 
 class DcbError(RuntimeError):
@@ -115,6 +122,11 @@ def lib():
     L.dcb_mark_active_cells_noalloc.argtypes = [P(DcbGrid), ctypes.c_void_p, ctypes.c_int64,
                                                 P(ctypes.c_int64), ctypes.c_void_p]
     L.dcb_mark_active_cells_noalloc.restype = ctypes.c_int
+    sdf_args = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64] + \
+        [ctypes.c_int] * 3 + [ctypes.c_float] * 6 + [ctypes.c_void_p, P(DcbSdfStats), ctypes.c_void_p]
+    for name in ("dcb_mesh_to_sdf_device", "dcb_mesh_to_sdf_host"):
+        getattr(L, name).argtypes = sdf_args
+        getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L
 

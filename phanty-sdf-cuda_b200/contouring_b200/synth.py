@@ -219,3 +219,80 @@ def sphere_with_zero_shell(res=40, radius=0.3):
     v = vals.clone()
     v[v.abs() < 0.2 * spacing[0]] = 0.0
     return v, dims, spacing, origin
+
+
+# ---- triangle meshes for the mesh -> SDF conversion -------------------------------------
+
+def icosphere(subdiv=4):
+    """Unit icosphere: the icosahedron (vertices (0,+-1,+-p), (+-1,+-p,0), (+-p,0,+-1), p the
+    golden ratio, faces = the 20 mutually adjacent vertex triples, wound outward), each
+    triangle split into 4 at its edge midpoints ``subdiv`` times, vertices projected onto the
+    sphere. Returns float64 vertices (10*4^s + 2, 3) and int64 faces (20*4^s, 3)."""
+    p = (1.0 + 5 ** 0.5) / 2.0
+    V = []
+    for a in (-1.0, 1.0):
+        for b in (-p, p):
+            V += [(0.0, a, b), (a, b, 0.0), (b, 0.0, a)]
+    V = np.array(V, np.float64)
+    d = np.linalg.norm(V[:, None] - V[None], axis=-1)
+    adj = np.isclose(d, 2.0)
+    F = []
+    for i in range(12):
+        for j in range(i + 1, 12):
+            for k in range(j + 1, 12):
+                if adj[i, j] and adj[j, k] and adj[i, k]:
+                    tri = [i, j, k]
+                    if np.dot(np.cross(V[j] - V[i], V[k] - V[i]), V[i] + V[j] + V[k]) < 0:
+                        tri = [i, k, j]
+                    F.append(tri)
+    V = V / np.linalg.norm(V, axis=1, keepdims=True)
+    F = np.array(F, np.int64)
+    for _ in range(subdiv):
+        mid = {}
+        verts = list(V)
+
+        def midpoint(a, b):
+            key = (a, b) if a < b else (b, a)
+            if key not in mid:
+                m = verts[a] + verts[b]
+                verts.append(m / np.linalg.norm(m))
+                mid[key] = len(verts) - 1
+            return mid[key]
+        nf = []
+        for a, b, c in F.tolist():
+            ab, bc, ca = midpoint(a, b), midpoint(b, c), midpoint(c, a)
+            nf += [[a, ab, ca], [b, bc, ab], [c, ca, bc], [ab, bc, ca]]
+        V, F = np.array(verts), np.array(nf, np.int64)
+    return V, F
+
+
+def icosphere_scene(n_spheres=32, subdiv=4, seed=0, noise=0.002):
+    """Union (concatenation) of ``n_spheres`` icospheres: radius U(0.05,0.2), centre
+    U(-0.3,0.3)^3, every vertex displaced along its normal by N(0, noise). Returns float32
+    vertices (n, 3) and int32 triangles (m, 3); 32 spheres of subdivision 4 give 81,984
+    vertices and 163,840 triangles."""
+    rng = np.random.default_rng(seed)
+    U, T = icosphere(subdiv)
+    centres = rng.uniform(-0.3, 0.3, (n_spheres, 3))
+    radii = rng.uniform(0.05, 0.2, n_spheres)
+    Vs, Fs = [], []
+    for s in range(n_spheres):
+        r = radii[s] + rng.normal(0.0, noise, len(U))
+        Vs.append(centres[s] + r[:, None] * U)
+        Fs.append(T + s * len(U))
+    return np.concatenate(Vs).astype(np.float32), np.concatenate(Fs).astype(np.int32)
+
+
+def mesh_grid(V, res):
+    """Grid of res^3 points over the mesh bounding box grown by 8% of its diagonal, in float
+    arithmetic like the CLI's OBJ import (dc_cli.cpp:160-187). Returns dims, spacing, origin."""
+    V = np.asarray(V, np.float32)
+    lo = V.min(axis=0).astype(np.float32)
+    hi = V.max(axis=0).astype(np.float32)
+    e = (hi - lo).astype(np.float32)
+    diag = np.float32(np.sqrt(np.float32(np.float32(e[0] * e[0] + e[1] * e[1]) + e[2] * e[2])))
+    pad = np.float32(diag * np.float32(0.08)) if diag > 0 else np.float32(0.1)
+    lo = (lo - pad).astype(np.float32)
+    hi = (hi + pad).astype(np.float32)
+    sp = ((hi - lo) / np.float32(res - 1)).astype(np.float32)
+    return (res, res, res), tuple(float(x) for x in sp), tuple(float(x) for x in lo)

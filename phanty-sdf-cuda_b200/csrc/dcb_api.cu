@@ -57,6 +57,10 @@ struct dcb_context {
     DevBuf grid, bits, super, list, seg_count, seg_start, counters, V, vclass, fmask, col_count, col_fill,
         col_start, partials, esc_list, hard_list, hard_data, stage_quad, stage_key, faces, wind_items,
         v64_index, v64_cells, V64, tris, tri_items;
+    // mesh -> SDF workspace
+    DevBuf m_verts, m_faces, m_out, m_tris, m_bin_count, m_bin_start, m_bin_fill, m_bin_scratch, m_bin_tris,
+        m_bin_active, m_active_list, m_axis_start, m_far, m_ext, m_tmp, m_partials, m_counters;
+    void* h_sdf_counters = nullptr;   // pinned SdfCounters
     void* h_counters = nullptr;       // pinned Counters
     void* hV = nullptr; size_t hV_bytes = 0;
     void* hF = nullptr; size_t hF_bytes = 0;
@@ -322,6 +326,109 @@ void fill_times(dcb_context* h, dcb_stats* st, bool upload) {
     st->face_emission_ms = elapsed(h->ev[3], h->ev[4]);
 }
 
+struct SdfCounters {
+    int err;
+    int changed;
+    unsigned long long total_entries;
+    unsigned long long exterior;
+    unsigned int active_bins;
+    unsigned int work_next;
+};
+
+bool finite_pos_spacing(float v) { return std::isfinite(v) && v > 0.f; }
+
+// The mesh -> SDF pipeline on device arrays; out has nx*ny*nz floats.
+int run_mesh_sdf(dcb_context* h, const float* d_verts, int64_t nv, const int32_t* d_faces, int64_t nf, int nx,
+                 int ny, int nz, float ox, float oy, float oz, float vx, float vy, float vz, float* out,
+                 dcb_sdf_stats* st, cudaStream_t s) {
+    if (nx < 1 || ny < 1 || nz < 1) return fail(h, DCB_ERR_INVALID_ARGUMENT, "grid needs at least 1 point per axis");
+    if (nv < 0 || nf < 0 || (nf > 0 && (!d_verts || !d_faces)) || !out)
+        return fail(h, DCB_ERR_INVALID_ARGUMENT, "null mesh or output array");
+    if (nv > 0x7fffffffLL || nf > 0x7fffffffLL) return fail(h, DCB_ERR_TOO_LARGE, "more than 2^31-1 vertices or faces");
+    if (!finite_pos_spacing(vx) || !finite_pos_spacing(vy) || !finite_pos_spacing(vz) || !std::isfinite(ox) ||
+        !std::isfinite(oy) || !std::isfinite(oz))
+        return fail(h, DCB_ERR_INVALID_ARGUMENT, "spacing must be finite and positive, origin finite");
+    SdfParams P;
+    std::memset(&P, 0, sizeof(P));
+    P.nx = nx; P.ny = ny; P.nz = nz;
+    P.ox = ox; P.oy = oy; P.oz = oz; P.vx = vx; P.vy = vy; P.vz = vz;
+    sdf_bin_geometry(P);
+    if (P.nbins > 0x7fffffffLL) return fail(h, DCB_ERR_TOO_LARGE, "too many bins");
+    P.verts = d_verts; P.faces = d_faces; P.nv = nv; P.nf = nf; P.out = out;
+    const long long rows = (long long)ny * nz;
+    DCB_TRY(h, ensure(h->m_tris, sdf_tri_record_bytes() * (size_t)std::max<int64_t>(1, nf)), "alloc triangle records");
+    DCB_TRY(h, ensure(h->m_bin_count, sizeof(uint32_t) * P.nbins), "alloc bins");
+    DCB_TRY(h, ensure(h->m_bin_start, sizeof(uint32_t) * P.nbins), "alloc bins");
+    DCB_TRY(h, ensure(h->m_bin_fill, sizeof(uint32_t) * P.nbins), "alloc bins");
+    DCB_TRY(h, ensure(h->m_bin_active, P.nbins), "alloc bins");
+    DCB_TRY(h, ensure(h->m_active_list, sizeof(uint32_t) * P.nbins), "alloc bins");
+    DCB_TRY(h, ensure(h->m_axis_start, sizeof(int) * (P.gx + P.gy + P.gz + 3)), "alloc bins");
+    DCB_TRY(h, ensure(h->m_partials, sizeof(uint32_t) * std::max(1LL, scan_partials_len(P.nbins))), "alloc scan");
+    DCB_TRY(h, ensure(h->m_far, sizeof(uint32_t) * rows * P.W), "alloc masks");
+    DCB_TRY(h, ensure(h->m_ext, sizeof(uint32_t) * rows * P.W), "alloc masks");
+    DCB_TRY(h, ensure(h->m_tmp, sizeof(float) * (size_t)nx * ny * nz), "alloc relaxation buffer");
+    DCB_TRY(h, ensure(h->m_counters, sizeof(SdfCounters)), "alloc counters");
+    if (!h->h_sdf_counters) DCB_TRY(h, cudaMallocHost(&h->h_sdf_counters, sizeof(SdfCounters)), "alloc pinned counters");
+    SdfCounters* dc = as<SdfCounters>(h->m_counters);
+    SdfCounters* hc = reinterpret_cast<SdfCounters*>(h->h_sdf_counters);
+    P.tris = as<float>(h->m_tris);
+    P.bin_count = as<uint32_t>(h->m_bin_count); P.bin_start = as<uint32_t>(h->m_bin_start);
+    P.bin_fill = as<uint32_t>(h->m_bin_fill); P.bin_active = as<uint8_t>(h->m_bin_active);
+    P.active_list = as<uint32_t>(h->m_active_list); P.axis_start = as<int>(h->m_axis_start);
+    P.far = as<uint32_t>(h->m_far); P.ext = as<uint32_t>(h->m_ext); P.err = &dc->err;
+    P.active_count = &dc->active_bins; P.work_next = &dc->work_next;
+
+    cudaEvent_t* ev = h->ev;
+    DCB_TRY(h, cudaEventRecord(ev[0], s), "event");
+    DCB_TRY(h, cudaMemsetAsync(dc, 0, sizeof(SdfCounters), s), "memset");
+    DCB_TRY(h, cudaMemsetAsync(P.bin_count, 0, sizeof(uint32_t) * P.nbins, s), "memset");
+    DCB_TRY(h, cudaMemsetAsync(P.bin_fill, 0, sizeof(uint32_t) * P.nbins, s), "memset");
+    DCB_TRY(h, launch_sdf_prep(P, h->num_sms, s), "launch triangle records");
+    DCB_TRY(h, launch_scan(P.bin_count, P.nbins, as<uint32_t>(h->m_partials), P.bin_start, &dc->total_entries, s),
+            "launch bin scan");
+    DCB_TRY(h, cudaMemcpyAsync(hc, dc, sizeof(SdfCounters), cudaMemcpyDeviceToHost, s), "read counters");
+    DCB_TRY(h, cudaStreamSynchronize(s), "bins");
+    if (hc->err == kErrInvalid) return fail(h, DCB_ERR_INVALID_ARGUMENT, "a face index is out of range");
+    const unsigned long long entries = hc->total_entries;
+    if (entries >= 0xffffffffULL) return fail(h, DCB_ERR_TOO_LARGE, "more than 2^32-1 bin entries");
+    DCB_TRY(h, ensure(h->m_bin_scratch, sizeof(uint32_t) * std::max(1ULL, entries)), "alloc bin entries");
+    DCB_TRY(h, ensure(h->m_bin_tris, sizeof(uint32_t) * std::max(1ULL, entries)), "alloc bin entries");
+    P.bin_scratch = as<uint32_t>(h->m_bin_scratch); P.bin_tris = as<uint32_t>(h->m_bin_tris);
+    DCB_TRY(h, launch_sdf_bins(P, h->num_sms, s), "launch binning");
+    DCB_TRY(h, cudaEventRecord(ev[1], s), "event");
+    DCB_TRY(h, launch_sdf_band(P, h->num_sms, s), "launch band");
+    DCB_TRY(h, cudaEventRecord(ev[2], s), "event");
+    DCB_TRY(h, launch_sdf_masks(P, h->num_sms, s), "launch masks");
+    int64_t passes = 0;
+    for (;;) {
+        DCB_TRY(h, cudaMemsetAsync(&dc->changed, 0, sizeof(int), s), "memset");
+        DCB_TRY(h, launch_sdf_flood(P, &dc->changed, h->num_sms, s), "launch flood");
+        DCB_TRY(h, cudaMemcpyAsync(&hc->changed, &dc->changed, sizeof(int), cudaMemcpyDeviceToHost, s), "read flag");
+        DCB_TRY(h, cudaStreamSynchronize(s), "flood");
+        ++passes;
+        if (!hc->changed) break;
+        if (passes > 1000000) return fail(h, DCB_ERR_INTERNAL, "exterior flood did not converge");
+    }
+    DCB_TRY(h, cudaEventRecord(ev[3], s), "event");
+    DCB_TRY(h, launch_sdf_finish(P, &dc->exterior, as<float>(h->m_tmp), h->num_sms, s), "launch finish");
+    DCB_TRY(h, cudaEventRecord(ev[4], s), "event");
+    DCB_TRY(h, cudaMemcpyAsync(hc, dc, sizeof(SdfCounters), cudaMemcpyDeviceToHost, s), "read counters");
+    DCB_TRY(h, cudaStreamSynchronize(s), "mesh to sdf");
+    if (hc->err) return fail(h, hc->err == kErrInvalid ? DCB_ERR_INVALID_ARGUMENT : DCB_ERR_INTERNAL, "device error flag set");
+    if (st) {
+        st->num_bins = P.nbins;
+        st->bin_entries = (int64_t)entries;
+        st->flood_passes = passes;
+        st->exterior_points = (int64_t)hc->exterior;
+        st->bins_ms = elapsed(ev[0], ev[1]);
+        st->band_ms = elapsed(ev[1], ev[2]);
+        st->sign_ms = elapsed(ev[2], ev[3]);
+        st->relax_ms = elapsed(ev[3], ev[4]);
+        st->total_ms = elapsed(ev[0], ev[4]);
+    }
+    return DCB_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -385,9 +492,13 @@ int dcb_destroy(dcb_handle h) {
                       &h->V, &h->vclass, &h->fmask, &h->col_count, &h->col_fill, &h->col_start,
                       &h->partials, &h->esc_list, &h->hard_list, &h->hard_data, &h->stage_quad,
                       &h->stage_key, &h->faces, &h->wind_items, &h->v64_index, &h->v64_cells, &h->V64,
-                      &h->tris, &h->tri_items};
+                      &h->tris, &h->tri_items, &h->m_verts, &h->m_faces, &h->m_out, &h->m_tris,
+                      &h->m_bin_count, &h->m_bin_start, &h->m_bin_fill, &h->m_bin_scratch, &h->m_bin_tris,
+                      &h->m_bin_active, &h->m_active_list, &h->m_axis_start, &h->m_far, &h->m_ext, &h->m_tmp,
+                      &h->m_partials, &h->m_counters};
     for (DevBuf* b : bufs) if (b->p) cudaFree(b->p);
     if (h->h_counters) cudaFreeHost(h->h_counters);
+    if (h->h_sdf_counters) cudaFreeHost(h->h_sdf_counters);
     if (h->hV) cudaFreeHost(h->hV);
     if (h->hF) cudaFreeHost(h->hF);
     for (auto& ev : h->ev) if (ev) cudaEventDestroy(ev);
@@ -497,6 +608,42 @@ int dcb_copy_cells_to_host(dcb_handle h, int64_t* cell_linear_index, void* cuda_
         const int64_t i = (int64_t)(p & 0x1FFFFF), j = (int64_t)((p >> 21) & 0x1FFFFF), k = (int64_t)(p >> 42);
         cell_linear_index[r] = i + (int64_t)h->cx * (j + (int64_t)h->cy * k);
     }
+    return DCB_OK;
+}
+
+int dcb_mesh_to_sdf_device(dcb_handle h, const float* vertices, int64_t num_vertices, const int32_t* faces,
+                           int64_t num_faces, int nx, int ny, int nz, float ox, float oy, float oz, float vx,
+                           float vy, float vz, float* out_values, dcb_sdf_stats* stats, void* cuda_stream) {
+    if (!h) return DCB_ERR_INVALID_ARGUMENT;
+    if (cudaSetDevice(h->device) != cudaSuccess) { cudaGetLastError(); return fail(h, DCB_ERR_CUDA, "set device"); }
+    if (stats) std::memset(stats, 0, sizeof(*stats));
+    return run_mesh_sdf(h, vertices, num_vertices, faces, num_faces, nx, ny, nz, ox, oy, oz, vx, vy, vz, out_values,
+                        stats, reinterpret_cast<cudaStream_t>(cuda_stream));
+}
+
+int dcb_mesh_to_sdf_host(dcb_handle h, const float* vertices, int64_t num_vertices, const int32_t* faces,
+                         int64_t num_faces, int nx, int ny, int nz, float ox, float oy, float oz, float vx,
+                         float vy, float vz, float* out_values, dcb_sdf_stats* stats, void* cuda_stream) {
+    if (!h) return DCB_ERR_INVALID_ARGUMENT;
+    if (!out_values || num_vertices < 0 || num_faces < 0 || (num_faces > 0 && (!vertices || !faces)))
+        return fail(h, DCB_ERR_INVALID_ARGUMENT, "null mesh or output array");
+    if (nx < 1 || ny < 1 || nz < 1) return fail(h, DCB_ERR_INVALID_ARGUMENT, "grid needs at least 1 point per axis");
+    if (cudaSetDevice(h->device) != cudaSuccess) { cudaGetLastError(); return fail(h, DCB_ERR_CUDA, "set device"); }
+    if (stats) std::memset(stats, 0, sizeof(*stats));
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(cuda_stream);
+    const size_t npts = (size_t)nx * ny * nz;
+    DCB_TRY(h, ensure(h->m_verts, sizeof(float) * 3 * (size_t)std::max<int64_t>(1, num_vertices)), "alloc vertices");
+    DCB_TRY(h, ensure(h->m_faces, sizeof(int32_t) * 3 * (size_t)std::max<int64_t>(1, num_faces)), "alloc faces");
+    DCB_TRY(h, ensure(h->m_out, sizeof(float) * npts), "alloc values");
+    if (num_vertices)
+        DCB_TRY(h, cudaMemcpyAsync(h->m_verts.p, vertices, sizeof(float) * 3 * num_vertices, cudaMemcpyHostToDevice, s), "upload vertices");
+    if (num_faces)
+        DCB_TRY(h, cudaMemcpyAsync(h->m_faces.p, faces, sizeof(int32_t) * 3 * num_faces, cudaMemcpyHostToDevice, s), "upload faces");
+    const int rc = run_mesh_sdf(h, as<float>(h->m_verts), num_vertices, as<int32_t>(h->m_faces), num_faces, nx, ny, nz,
+                                ox, oy, oz, vx, vy, vz, as<float>(h->m_out), stats, s);
+    if (rc != DCB_OK) return rc;
+    DCB_TRY(h, cudaMemcpyAsync(out_values, h->m_out.p, sizeof(float) * npts, cudaMemcpyDeviceToHost, s), "download values");
+    DCB_TRY(h, cudaStreamSynchronize(s), "download values");
     return DCB_OK;
 }
 

@@ -90,7 +90,7 @@ __device__ __forceinline__ bool hermite_crossing(float a, float b) {
 }
 
 // Error flags written by kernels (first error wins).
-enum DeviceError : int { kErrNone = 0, kErrTimeout = 1, kErrInternal = 2, kErrOverflow = 3 };
+enum DeviceError : int { kErrNone = 0, kErrTimeout = 1, kErrInternal = 2, kErrOverflow = 3, kErrInvalid = 4 };
 
 __device__ __forceinline__ void set_error(int* flag, int code) { atomicCAS(flag, 0, code); }
 

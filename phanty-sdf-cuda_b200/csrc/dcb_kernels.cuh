@@ -143,4 +143,42 @@ struct Tri64Params {
 };
 cudaError_t launch_tri_fp64(const Tri64Params& P, long long max_items, int num_sms, cudaStream_t s);
 
+// ---- mesh -> SDF (dcb_mesh_sdf.cu) ----
+struct SdfParams {
+    int nx, ny, nz;
+    float ox, oy, oz, vx, vy, vz;
+    int gx, gy, gz;                // bins per axis
+    float bdx, bdy, bdz;           // bin size
+    float margin;                  // bounding-box growth of a triangle before binning
+    float min_box;                 // smallest bin size
+    long long nbins;
+    int W;                         // 32-point words per x row (flood masks)
+    const float* verts;
+    const int* faces;
+    long long nv, nf;
+    float* tris;                   // sdf_tri_record_bytes() per triangle
+    uint32_t* bin_count;
+    uint32_t* bin_start;
+    uint32_t* bin_fill;
+    uint32_t* bin_scratch;         // bin entries as scattered
+    uint32_t* bin_tris;            // bin entries in ascending triangle order
+    uint8_t* bin_active;
+    uint32_t* active_list;         // active bins (any order)
+    unsigned int* active_count;
+    unsigned int* work_next;       // next active bin for the band kernel
+    int* axis_start;               // first point of every bin per axis: [gx+1][gy+1][gz+1]
+    float* out;                    // nx*ny*nz values
+    uint32_t* far;                 // [nz*ny][W] bits: value is far
+    uint32_t* ext;                 // [nz*ny][W] bits: exterior
+    int* err;
+};
+void sdf_bin_geometry(SdfParams& P);
+size_t sdf_tri_record_bytes();     // bytes of one triangle record in SdfParams::tris
+cudaError_t launch_sdf_prep(const SdfParams& P, int num_sms, cudaStream_t s);
+cudaError_t launch_sdf_bins(const SdfParams& P, int num_sms, cudaStream_t s);
+cudaError_t launch_sdf_band(const SdfParams& P, int num_sms, cudaStream_t s);
+cudaError_t launch_sdf_masks(const SdfParams& P, int num_sms, cudaStream_t s);
+cudaError_t launch_sdf_flood(const SdfParams& P, int* changed, int num_sms, cudaStream_t s);
+cudaError_t launch_sdf_finish(const SdfParams& P, unsigned long long* filled, float* tmp, int num_sms, cudaStream_t s);
+
 }  // namespace dcb

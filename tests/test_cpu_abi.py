@@ -59,7 +59,8 @@ def test_struct_layouts_match_the_header():
     ctypes mirrors."""
     from contouring_b200 import _lib
     structs = {"dcb_grid": _lib.DcbGrid, "dcb_opts": _lib.DcbOpts, "dcb_stats": _lib.DcbStats,
-               "dcb_mesh_dev": _lib.DcbMeshDev, "dcb_mesh_host": _lib.DcbMeshHost}
+               "dcb_mesh_dev": _lib.DcbMeshDev, "dcb_mesh_host": _lib.DcbMeshHost,
+               "dcb_sdf_stats": _lib.DcbSdfStats}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "dcb.h"', "int main(void) {"]
     for cname, py in structs.items():
         lines.append('printf("%s %%zu\\n", sizeof(%s));' % (cname, cname))
