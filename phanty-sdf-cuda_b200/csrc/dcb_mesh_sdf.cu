@@ -27,7 +27,8 @@
 //                   first grid point of every bin per axis; k_fill_far sets every value far
 //   k_band          persistent CTAs take active bins from a work counter; the 27-bin
 //                   visiting sequence is the same for every point of a bin, so its triangle
-//                   records stream through shared memory once per 512 points (2 per thread). A triangle whose bounding sphere
+//                   records stream through shared memory once per 8 cubes of 4x4x4 points
+//                   (a cube per warp, 2 points per thread). A triangle whose bounding sphere
 //                   provably lies beyond a point's running minimum plus the tie tolerance is
 //                   skipped — the reference loop would ignore it at that point of the
 //                   sequence, so skipping it changes no bit. The test runs first for a whole
@@ -273,7 +274,7 @@ __global__ void __launch_bounds__(256) k_fill_far(SdfParams P) {
 
 constexpr int kBandThreads = 256;
 constexpr int kBandChunk = 256;   // triangle records staged per pass (20 KB)
-constexpr int kBandPts = 2;       // grid points per thread
+constexpr int kBandPts = 2;       // grid points per thread (a 4x4x4 cube per warp)
 
 // Running closest-triangle state of one grid point.
 struct BandPoint {
@@ -294,15 +295,13 @@ __device__ __forceinline__ float reach_of(float best, float pm) {
 // The record is read from shared memory by the caller (s_rec = the record's 5 float4s).
 __device__ __forceinline__ void visit(BandPoint& q, float pm, const float4 (&s_rec)[kTriF4], float veps) {
     const float4 ts = s_rec[0];
-    const float4 ta = s_rec[1];
-    if (!(ta.w > 0.f)) return;                          // area <= 1e-12: skipped
-    const float4 tn = s_rec[4];
     if (q.best != kFar) {
         const float dx = q.p.x - ts.x, dy = q.p.y - ts.y, dz = q.p.z - ts.z;
         const float d2 = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmul_rn(dz, dz)));
-        const float reach2 = __fmul_rn(__fmul_rn(q.reach, q.reach), 1.00002f);
         const float lim = q.reach + ts.w;
         if (d2 > __fmul_rn(__fmul_rn(lim, lim), 1.00002f)) return;
+        const float4 tn = s_rec[4];
+        const float reach2 = __fmul_rn(__fmul_rn(q.reach, q.reach), 1.00002f);
         const float allow = 2e-5f * (pm + fabsf(ts.x) + fabsf(ts.y) + fabsf(ts.z) + ts.w);
         const float h = __fmaf_rn(dx, tn.x, __fmaf_rn(dy, tn.y, __fmul_rn(dz, tn.z)));
         const float hh = fmaxf(0.f, fabsf(h) - allow);
@@ -310,22 +309,28 @@ __device__ __forceinline__ void visit(BandPoint& q, float pm, const float4 (&s_r
         const float ll = fmaxf(0.f, lat - ts.w - allow);
         if (__fmaf_rn(hh, hh, __fmul_rn(ll, ll)) > reach2) return;
     }
+    const float4 ta = s_rec[1];
+    if (!(ta.w > 0.f)) return;                          // area <= 1e-12: skipped
     const float4 tb = s_rec[2], tc = s_rec[3];
     const float3 v0 = f3(ta.x, ta.y, ta.z), v1 = f3(tb.x, tb.y, tb.z), v2 = f3(tc.x, tc.y, tc.z);
     float3 cp;
     const float d = point_triangle(q.p, v0, v1, v2, cp);
+    const float tol = 1e-5f * (q.best + 1e-8f);
+    const bool replace = d < q.best - tol;
+    if (!replace && !(fabsf(d - q.best) <= tol)) return;   // ignored: its weight is never used
+    // weight: the doubled area, or the angle at a vertex the closest point sits on
     float w = ta.w;
     const float3 c0v = sub(cp, v0), c1v = sub(cp, v1), c2v = sub(cp, v2);
     if (dot(c0v, c0v) < veps) w = angle_at(sub(v1, v0), sub(v2, v0), w);
     else if (dot(c1v, c1v) < veps) w = angle_at(sub(v0, v1), sub(v2, v1), w);
     else if (dot(c2v, c2v) < veps) w = angle_at(sub(v0, v2), sub(v1, v2), w);
-    const float tol = 1e-5f * (q.best + 1e-8f);
-    if (d < q.best - tol) {
+    const float4 tn = s_rec[4];
+    if (replace) {
         q.best = d;
         q.bp = cp;
         q.bn = f3(w * tn.x, w * tn.y, w * tn.z);
         q.reach = reach_of(d, pm);
-    } else if (fabsf(d - q.best) <= tol) {
+    } else {
         q.bn = f3(q.bn.x + w * tn.x, q.bn.y + w * tn.y, q.bn.z + w * tn.z);
     }
 }
@@ -352,8 +357,11 @@ __global__ void __launch_bounds__(kBandThreads, 2) k_band(SdfParams P) {
         const int y0 = ys_[by], y1 = ys_[by + 1];
         const int z0 = zs_[bz], z1 = zs_[bz + 1];
         const int sx = x1 - x0, sy = y1 - y0, sz = z1 - z0;
-        const int npts = max(0, sx) * max(0, sy) * max(0, sz);
-        if (npts == 0) continue;
+        if (sx <= 0 || sy <= 0 || sz <= 0) continue;
+        // points go to warps in 4x4x4 cubes (lane: 4x4x2, the second point 2 planes up), so
+        // that a warp's point box, used to cull triangles, stays small
+        const int cx4 = (sx + 3) / 4, cy4 = (sy + 3) / 4, cz4 = (sz + 3) / 4;
+        const int ncubes = cx4 * cy4 * cz4;
         // visiting sequence: centre bin, then the shell of radius 1 in z, y, x order; lane t of
         // warp 0 takes the t-th of the 27 slots, a warp scan gives the starts
         __syncthreads();
@@ -381,17 +389,18 @@ __global__ void __launch_bounds__(kBandThreads, 2) k_band(SdfParams P) {
         __syncthreads();
         const uint32_t L = s_seq_start[27];
         const float veps = 1e-6f * P.min_box * P.min_box;
-        for (int p0 = 0; p0 < npts; p0 += kBandThreads * kBandPts) {
+        for (int cube0 = 0; cube0 < ncubes; cube0 += kBandThreads / 32) {
             BandPoint q[kBandPts];
             float pm[kBandPts];
             bool mine[kBandPts];
             int pidx[kBandPts][3];
+            const int cube = cube0 + (threadIdx.x >> 5);
+            const int ccx = cube % cx4, ccy = (cube / cx4) % cy4, ccz = cube / (cx4 * cy4);
 #pragma unroll
             for (int u = 0; u < kBandPts; ++u) {
-                const int pi = p0 + threadIdx.x + u * kBandThreads;
-                mine[u] = pi < npts;
-                const int ix = x0 + (mine[u] ? pi % sx : 0), iy = y0 + (mine[u] ? (pi / sx) % sy : 0),
-                          iz = z0 + (mine[u] ? pi / (sx * sy) : 0);
+                const int lx = 4 * ccx + (lane & 3), ly = 4 * ccy + ((lane >> 2) & 3), lz = 4 * ccz + (lane >> 4) + 2 * u;
+                mine[u] = cube < ncubes && lx < sx && ly < sy && lz < sz;
+                const int ix = x0 + (mine[u] ? lx : 0), iy = y0 + (mine[u] ? ly : 0), iz = z0 + (mine[u] ? lz : 0);
                 pidx[u][0] = ix; pidx[u][1] = iy; pidx[u][2] = iz;
                 q[u].p = f3(P.ox + (float)ix * P.vx, P.oy + (float)iy * P.vy, P.oz + (float)iz * P.vz);
                 pm[u] = fmaxf(fabsf(q[u].p.x), fmaxf(fabsf(q[u].p.y), fabsf(q[u].p.z)));
