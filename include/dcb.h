@@ -140,8 +140,9 @@ int dcb_copy_mesh_to_host(dcb_handle h, float* vertices, int32_t* faces, void* c
 /* Copy the last mesh of `h` into caller-owned DEVICE arrays (e.g. torch CUDA tensors). */
 int dcb_copy_mesh_device(dcb_handle h, float* vertices, int32_t* faces, void* cuda_stream);
 
-/* Copy the linear cell index (i + cx*(j + cy*k), cx = nx-1, cy = ny-1) of every vertex of
- * the last mesh into a caller-owned host array of vertex_count entries. */
+/* Copy the linear cell index (i + cx*(j + cy*k), cx = nx-1, cy = ny-1, of the vertex's own
+ * grid for a batch) of every vertex of the last mesh into a caller-owned host array of
+ * vertex_count entries. */
 int dcb_copy_cells_to_host(dcb_handle h, int64_t* cell_linear_index, void* cuda_stream);
 
 /* Active-cell marking and compaction without any device allocation (no counterpart in
@@ -161,6 +162,32 @@ int dcb_copy_cells_to_host(dcb_handle h, int64_t* cell_linear_index, void* cuda_
  * result is complete. */
 int dcb_mark_active_cells_noalloc(const dcb_grid* grid, int64_t* cells, int64_t capacity,
                                   int64_t* count, void* cuda_stream);
+
+/* ---- batches of grids ------------------------------------------------------------------- */
+
+/* The meshes of a batch, concatenated grid by grid in device memory. Grid b's vertices are
+ * vertices[3*vertex_offset[b] .. 3*vertex_offset[b+1]) and its faces
+ * faces[vpf*face_offset[b] .. vpf*face_offset[b+1]); face indices count from the first vertex
+ * of their own grid, so every grid's part is exactly its single-grid extraction. The offset
+ * arrays (n+1 entries, host memory) and the device arrays are owned by the handle and stay
+ * valid until the next extract call on it. */
+typedef struct {
+    int64_t vertex_count;
+    int64_t face_count;
+    int verts_per_face;
+    float* vertices;
+    int32_t* faces;
+    const int64_t* vertex_offset;
+    const int64_t* face_offset;
+} dcb_batch_mesh;
+
+/* Batched extraction (no counterpart in the reference, whose callers loop over grids): n
+ * device grids of any sizes in one pass of the pipeline. Each kernel runs once over all
+ * grids (the mark over all grids' tiles, the scans over all grids' segments and face
+ * columns, the vertex and face kernels over one queue of all active cells), with two host
+ * synchronisations per batch instead of two per grid. stats holds batch totals. */
+int dcb_extract_batch_device(dcb_handle h, const dcb_grid* grids, int n, const dcb_opts* opts,
+                             dcb_batch_mesh* out, dcb_stats* stats, void* cuda_stream);
 
 /* ---- mesh -> signed distance grid ------------------------------------------------------ */
 

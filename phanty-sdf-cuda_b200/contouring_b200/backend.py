@@ -254,6 +254,42 @@ class B200DualContouringBackend:
         self._last_vpf = md.verts_per_face
         return md.vertices, md.faces, DualContouringStats.from_c(st)
 
+    def extract_batch_ptr(self, grids, stream=None):
+        """Batched extraction into the handle's device buffers (valid until the next call);
+        returns the raw ``DcbBatchMesh`` and the batch's stats."""
+        n = len(grids)
+        arr = (_lib.DcbGrid * n)()
+        for b, (values, dims, spacing, origin) in enumerate(grids):
+            d = DenseSdfGridDevice(*dims, *spacing, *origin, d_values=values)
+            arr[b] = self._grid_c(d, d.pointer())
+        st = _lib.DcbStats()
+        out = _lib.DcbBatchMesh()
+        s = _current_stream() if stream is None else stream
+        _lib.check(self._L.dcb_extract_batch_device(self._h, arr, n, ctypes.byref(self.options.to_c()),
+                                                    ctypes.byref(out), ctypes.byref(st), ctypes.c_void_p(s)), self._h)
+        self._last_nv = out.vertex_count
+        self._last_vpf = out.verts_per_face
+        return out, DualContouringStats.from_c(st)
+
+    def extract_batch(self, grids, stream=None):
+        """Batched extraction of ``grids`` = [(CUDA float32 values, dims, spacing, origin)] in one
+        pass of the pipeline. Returns ``[(V (nv,3) float32, F (nf,vpf) int32)]`` CUDA tensors per
+        grid (faces index their own grid's vertices) and the batch's totals as stats."""
+        import torch
+        n = len(grids)
+        s = _current_stream() if stream is None else stream
+        out, stats = self.extract_batch_ptr(grids, s)
+        vpf = out.verts_per_face
+        dev = grids[0][0].device
+        V = torch.empty((out.vertex_count, 3), dtype=torch.float32, device=dev)
+        F = torch.empty((out.face_count, vpf), dtype=torch.int32, device=dev)
+        _lib.check(self._L.dcb_copy_mesh_device(self._h, V.data_ptr() if V.numel() else None,
+                                                F.data_ptr() if F.numel() else None, ctypes.c_void_p(s)), self._h)
+        vo = [out.vertex_offset[b] for b in range(n + 1)]
+        fo = [out.face_offset[b] for b in range(n + 1)]
+        meshes = [(V[vo[b]:vo[b + 1]], F[fo[b]:fo[b + 1]]) for b in range(n)]
+        return meshes, stats
+
     def extract_tensor(self, values, dims, spacing, origin):
         """torch convenience: CUDA float32 grid in, ``(V (nv,3) float32, F (nf,4) int32,
         stats)`` CUDA tensors out (copied from the handle's buffers)."""

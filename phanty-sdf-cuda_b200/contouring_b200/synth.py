@@ -128,6 +128,22 @@ def csg(res=1024, seed=0, lo=-0.5, hi=0.5, device="cpu", planes=None):
 
 # ---- the reference's own generators (dc_cli.cpp:49-118, dc_tests.cpp:14-215), in float32 ----
 
+def csg_batch(n=256, seed=0, resolutions=(32, 48, 64, 96, 128, 192), lo=-0.5, hi=0.5, device="cpu"):
+    """n seeded CSG shapes at uneven resolutions: shape s draws its resolution uniformly from
+    ``resolutions`` and a random mix of 1-16 boxes, 0-8 capped cylinders and 0-4 subtracted
+    spheres with the distributions of ``csg``. Returns [(values, dims, spacing, origin)]."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for s in range(n):
+        res = int(rng.choice(resolutions))
+        nb, nc, nh = int(rng.integers(1, 17)), int(rng.integers(0, 9)), int(rng.integers(0, 5))
+        prims, holes = csg_scene(int(rng.integers(0, 2 ** 31)), nb, nc, nh)
+        dims, spacing, origin = _grid_params(res, lo, hi)
+        vals = _eval_slabs(dims, spacing, origin, _csg_fn(prims, holes, device), device, slab_points=1 << 24)
+        out.append((vals, dims, spacing, origin))
+    return out
+
+
 def _cli_axes(res):
     v = np.float32(2.0) / np.float32(res - 1)
     o = np.float32(-1.0)

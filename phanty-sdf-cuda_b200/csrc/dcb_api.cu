@@ -22,6 +22,7 @@
 #include <cmath>
 #include <string>
 #include <algorithm>
+#include <vector>
 #include "dcb_kernels.cuh"
 #include "../../include/dcb.h"
 
@@ -68,6 +69,13 @@ struct dcb_context {
     int vpf = 4;                      // output vertices per face
     int mark_ctas[2] = {0, 0};        // resident mark CTAs per SM (scalar, float4 loads)
     int cx = 0, cy = 0;
+    // batch layout table (device + pinned staging) and the last batch's per-grid offsets
+    DevBuf table;
+    void* h_table = nullptr; size_t h_table_bytes = 0;
+    void* h_offsets = nullptr; size_t h_offsets_bytes = 0;
+    int batch_n = 1;
+    std::vector<int> batch_cx, batch_cy;
+    std::vector<int64_t> vert_offsets, face_offsets;
 };
 
 namespace {
@@ -138,60 +146,164 @@ float elapsed(cudaEvent_t a, cudaEvent_t b) {
     return ms;
 }
 
-// Runs the pipeline on a device-resident grid; ev[1] must already be recorded.
-int run_pipeline(dcb_context* h, const dcb_grid* in, const dcb_opts* o, cudaStream_t s, dcb_stats* st) {
-    GridDesc g;
-    g.nx = in->nx; g.ny = in->ny; g.nz = in->nz;
-    g.cx = g.nx - 1; g.cy = g.ny - 1; g.cz = g.nz - 1;
-    g.W = ((g.cx + 31) / 32 + 7) / 8 * 8;
-    g.W8 = g.W / 8;
-    g.vx = in->vx; g.vy = in->vy; g.vz = in->vz;
-    g.ox = in->ox; g.oy = in->oy; g.oz = in->oz;
-    g.v = in->values;
+// Host copy of a batch's layout (per-grid offsets of the concatenated arrays, mark tiling).
+struct BatchLayout {
+    std::vector<GridSlot> slots;
+    std::vector<long long> seg_off, col_off;          // n + 1
+    std::vector<int> tile_slot[2];                    // grids of the scalar / float4 mark launch
+    std::vector<long long> tile_off[2];               // their first tiles (+ total)
+    long long bits = 0, super = 0, nseg = 0, ncol = 0, ncell = 0;
+    float hmax = 0.f;
+};
 
-    const long long rows = (long long)g.cy * g.cz;
-    const long long ncell = (long long)g.cx * rows;
-    const long long cxcy = (long long)g.cx * g.cy;
-    const uintptr_t base = reinterpret_cast<uintptr_t>(g.v);
-    const int vec4 = (g.nx % 4 == 0 && (base % 16) == 0) ? 1 : 0;
+int layout_batch(dcb_context* h, const dcb_grid* in, int n, BatchLayout& L) {
+    L.slots.resize(n);
+    L.seg_off.assign(n + 1, 0);
+    L.col_off.assign(n + 1, 0);
+    for (int v = 0; v < 2; ++v) { L.tile_slot[v].clear(); L.tile_off[v].assign(1, 0); }
     const int tile_cells = 32 * mark_tile_words();
-    const int nxt = (g.cx + tile_cells - 1) / tile_cells;
-    const int R = std::min(mark_max_rows(), g.cy);
-    const long long nrb = (g.cy + R - 1) / R;
-    // About four CTAs per resident slot, each marching 8..64 planes (a single long wave
-    // measured slower at 1024^3: 0.887 vs 0.848 ms).
-    if (h->mark_ctas[vec4] == 0) h->mark_ctas[vec4] = mark_ctas_per_sm(vec4);
-    const long long slots = (long long)h->num_sms * h->mark_ctas[vec4] * 4;
-    const long long KZ = std::max(8LL, std::min(64LL, (g.cz * nxt * nrb + slots - 1) / slots));
-    const long long nseg = rows * nxt;
-    if (nrb > 65535 || (g.cz + KZ - 1) / KZ > 65535) return fail(h, DCB_ERR_TOO_LARGE, "grid too large for the tiling");
+    for (int b = 0; b < n; ++b) {
+        GridSlot& S = L.slots[b];
+        GridDesc& g = S.g;
+        g.nx = in[b].nx; g.ny = in[b].ny; g.nz = in[b].nz;
+        g.cx = g.nx - 1; g.cy = g.ny - 1; g.cz = g.nz - 1;
+        g.W = ((g.cx + 31) / 32 + 7) / 8 * 8;
+        g.W8 = g.W / 8;
+        g.vx = in[b].vx; g.vy = in[b].vy; g.vz = in[b].vz;
+        g.ox = in[b].ox; g.oy = in[b].oy; g.oz = in[b].oz;
+        g.v = in[b].values;
+        const long long rows = (long long)g.cy * g.cz;
+        S.vec4 = (g.nx % 4 == 0 && (reinterpret_cast<uintptr_t>(g.v) % 16) == 0) ? 1 : 0;
+        S.nxt = (g.cx + tile_cells - 1) / tile_cells;
+        S.R = std::min(mark_max_rows(), g.cy);
+        S.nrb = (g.cy + S.R - 1) / S.R;
+        // About four CTAs per resident slot, each marching 8..64 planes (a single long wave
+        // measured slower at 1024^3: 0.887 vs 0.848 ms).
+        if (h->mark_ctas[S.vec4] == 0) h->mark_ctas[S.vec4] = mark_ctas_per_sm(S.vec4);
+        const long long slots = (long long)h->num_sms * h->mark_ctas[S.vec4] * 4;
+        S.KZ = (int)std::max(8LL, std::min(64LL, (g.cz * S.nxt * (long long)S.nrb + slots - 1) / slots));
+        S.nzc = (g.cz + S.KZ - 1) / S.KZ;
+        S.bits_off = L.bits;
+        S.super_off = L.super;
+        S.seg_off = L.nseg;
+        S.col_off = L.ncol;
+        L.seg_off[b] = L.nseg;
+        L.col_off[b] = L.ncol;
+        L.bits += rows * g.W;
+        L.super += rows * g.W8;
+        L.nseg += rows * S.nxt;
+        L.ncol += 3LL * g.cx * g.cy;
+        L.ncell += (long long)g.cx * rows;
+        L.tile_slot[S.vec4].push_back(b);
+        L.tile_off[S.vec4].push_back(L.tile_off[S.vec4].back() + (long long)S.nxt * S.nrb * S.nzc);
+        L.hmax = std::max(L.hmax, std::max(std::fabs(g.vx), std::max(std::fabs(g.vy), std::fabs(g.vz))));
+    }
+    L.seg_off[n] = L.nseg;
+    L.col_off[n] = L.ncol;
+    for (int v = 0; v < 2; ++v)
+        if (L.tile_off[v].back() > 0x7fffffffLL) return fail(h, DCB_ERR_TOO_LARGE, "grid too large for the tiling");
+    if (L.nseg >= 0xffffffffLL || L.ncol >= 0xffffffffLL) return fail(h, DCB_ERR_TOO_LARGE, "batch too large");
+    return DCB_OK;
+}
 
-    DCB_TRY(h, ensure(h->bits, sizeof(uint32_t) * rows * g.W), "alloc bits");
-    DCB_TRY(h, ensure(h->super, sizeof(uint32_t) * rows * g.W8), "alloc ranks");
+// Device copy of the layout: slots | seg_off | col_off | vert_off | face_off | tile lists.
+struct TableView {
+    BatchTable B;
+    unsigned long long* vert_off;
+    unsigned long long* face_off;
+    const int* tile_slot[2];
+    const long long* tile_off[2];
+};
+
+size_t align_up(size_t x) { return (x + 255) & ~size_t(255); }
+
+int upload_table(dcb_context* h, const BatchLayout& L, cudaStream_t s, TableView& T) {
+    const int n = (int)L.slots.size();
+    const size_t o_slots = 0;
+    const size_t o_seg = align_up(o_slots + sizeof(GridSlot) * n);
+    const size_t o_col = align_up(o_seg + sizeof(long long) * (n + 1));
+    const size_t o_vert = align_up(o_col + sizeof(long long) * (n + 1));
+    const size_t o_face = align_up(o_vert + sizeof(unsigned long long) * (n + 1));
+    const size_t o_ts0 = align_up(o_face + sizeof(unsigned long long) * (n + 1));
+    const size_t o_ts1 = align_up(o_ts0 + sizeof(int) * L.tile_slot[0].size() + 1);
+    const size_t o_to0 = align_up(o_ts1 + sizeof(int) * L.tile_slot[1].size() + 1);
+    const size_t o_to1 = align_up(o_to0 + sizeof(long long) * L.tile_off[0].size());
+    const size_t total = align_up(o_to1 + sizeof(long long) * L.tile_off[1].size());
+    DCB_TRY(h, ensure(h->table, total), "alloc batch table");
+    DCB_TRY(h, ensure_host(h->h_table, h->h_table_bytes, total), "alloc pinned batch table");
+    char* hb = reinterpret_cast<char*>(h->h_table);
+    std::memcpy(hb + o_slots, L.slots.data(), sizeof(GridSlot) * n);
+    std::memcpy(hb + o_seg, L.seg_off.data(), sizeof(long long) * (n + 1));
+    std::memcpy(hb + o_col, L.col_off.data(), sizeof(long long) * (n + 1));
+    std::memcpy(hb + o_ts0, L.tile_slot[0].data(), sizeof(int) * L.tile_slot[0].size());
+    std::memcpy(hb + o_ts1, L.tile_slot[1].data(), sizeof(int) * L.tile_slot[1].size());
+    std::memcpy(hb + o_to0, L.tile_off[0].data(), sizeof(long long) * L.tile_off[0].size());
+    std::memcpy(hb + o_to1, L.tile_off[1].data(), sizeof(long long) * L.tile_off[1].size());
+    DCB_TRY(h, cudaMemcpyAsync(h->table.p, hb, total, cudaMemcpyHostToDevice, s), "upload batch table");
+    char* db = reinterpret_cast<char*>(h->table.p);
+    T.B.s0 = L.slots[0];
+    T.B.slots = reinterpret_cast<const GridSlot*>(db + o_slots);
+    T.B.n = n;
+    T.B.seg_off = reinterpret_cast<const long long*>(db + o_seg);
+    T.B.col_off = reinterpret_cast<const long long*>(db + o_col);
+    T.vert_off = reinterpret_cast<unsigned long long*>(db + o_vert);
+    T.face_off = reinterpret_cast<unsigned long long*>(db + o_face);
+    T.B.vert_off = T.vert_off;
+    T.tile_slot[0] = reinterpret_cast<const int*>(db + o_ts0);
+    T.tile_slot[1] = reinterpret_cast<const int*>(db + o_ts1);
+    T.tile_off[0] = reinterpret_cast<const long long*>(db + o_to0);
+    T.tile_off[1] = reinterpret_cast<const long long*>(db + o_to1);
+    return DCB_OK;
+}
+
+// Runs the pipeline on n device-resident grids as one batch (a single extraction is n = 1);
+// ev[1] must already be recorded. Vertices are numbered over the whole batch while running;
+// for n > 1 the faces are rebased to their own grid's vertices at the end.
+int run_batch(dcb_context* h, const dcb_grid* in, int n, const dcb_opts* o, cudaStream_t s, dcb_stats* st) {
+    BatchLayout L;
+    int rc = layout_batch(h, in, n, L);
+    if (rc != DCB_OK) return rc;
+    TableView T;
+    rc = upload_table(h, L, s, T);
+    if (rc != DCB_OK) return rc;
+    const long long nseg = L.nseg, ncol = L.ncol;
+
+    DCB_TRY(h, ensure(h->bits, sizeof(uint32_t) * L.bits), "alloc bits");
+    DCB_TRY(h, ensure(h->super, sizeof(uint32_t) * L.super), "alloc ranks");
     DCB_TRY(h, ensure(h->seg_count, sizeof(uint32_t) * nseg), "alloc segment counts");
     DCB_TRY(h, ensure(h->seg_start, sizeof(uint32_t) * nseg), "alloc segment starts");
     DCB_TRY(h, ensure(h->counters, sizeof(Counters)), "alloc counters");
-    DCB_TRY(h, ensure(h->col_count, sizeof(uint32_t) * 3 * cxcy), "alloc column counts");
-    DCB_TRY(h, ensure(h->col_fill, sizeof(uint32_t) * 3 * cxcy), "alloc column fill");
-    DCB_TRY(h, ensure(h->col_start, sizeof(uint32_t) * 3 * cxcy), "alloc column starts");
-    const long long plen = std::max(scan_partials_len(3 * cxcy), scan_partials_len(nseg));
+    DCB_TRY(h, ensure(h->col_count, sizeof(uint32_t) * ncol), "alloc column counts");
+    DCB_TRY(h, ensure(h->col_fill, sizeof(uint32_t) * ncol), "alloc column fill");
+    DCB_TRY(h, ensure(h->col_start, sizeof(uint32_t) * ncol), "alloc column starts");
+    const long long plen = std::max(scan_partials_len(ncol), scan_partials_len(nseg));
     DCB_TRY(h, ensure(h->partials, sizeof(uint32_t) * std::max(1LL, plen)), "alloc scan");
     if (!h->h_counters) DCB_TRY(h, cudaMallocHost(&h->h_counters, sizeof(Counters)), "alloc pinned counters");
+    DCB_TRY(h, ensure_host(h->h_offsets, h->h_offsets_bytes, 2 * sizeof(unsigned long long) * (n + 1)), "alloc pinned offsets");
+    unsigned long long* h_vert_off = reinterpret_cast<unsigned long long*>(h->h_offsets);
+    unsigned long long* h_face_off = h_vert_off + (n + 1);
 
     Counters* dc = as<Counters>(h->counters);
     Counters* hc = reinterpret_cast<Counters*>(h->h_counters);
 
     // 1) mark: active bits + per-segment counts; scan -> segment starts and the total.
     DCB_TRY(h, cudaMemsetAsync(h->counters.p, 0, sizeof(Counters), s), "memset counters");
-    MarkParams mp;
-    mp.g = g; mp.R = R; mp.KZ = (int)KZ; mp.nxt = nxt;
-    mp.bits = as<uint32_t>(h->bits); mp.seg_count = as<uint32_t>(h->seg_count); mp.vec4 = vec4;
-    DCB_TRY(h, launch_mark(mp, s), "launch mark");
+    for (int v = 0; v < 2; ++v) {
+        if (L.tile_slot[v].empty()) continue;
+        MarkParams mp;
+        mp.B = T.B; mp.tile_slot = T.tile_slot[v]; mp.tile_off = T.tile_off[v];
+        mp.m = (int)L.tile_slot[v].size(); mp.ntiles = L.tile_off[v].back();
+        mp.bits = as<uint32_t>(h->bits); mp.seg_count = as<uint32_t>(h->seg_count);
+        DCB_TRY(h, launch_mark(mp, v, s), "launch mark");
+    }
     DCB_TRY(h, cudaEventRecord(h->ev[6], s), "event");
-    DCB_TRY(h, launch_scan(mp.seg_count, nseg, as<uint32_t>(h->partials), as<uint32_t>(h->seg_start),
+    DCB_TRY(h, launch_scan(as<uint32_t>(h->seg_count), nseg, as<uint32_t>(h->partials), as<uint32_t>(h->seg_start),
                            &dc->total_active, s), "launch segment scan");
+    DCB_TRY(h, launch_vert_offsets(T.B, as<uint32_t>(h->seg_start), &dc->total_active, T.vert_off, s), "vertex offsets");
     DCB_TRY(h, cudaEventRecord(h->ev[2], s), "event");
     DCB_TRY(h, cudaMemcpyAsync(hc, dc, sizeof(Counters), cudaMemcpyDeviceToHost, s), "read count");
+    DCB_TRY(h, cudaMemcpyAsync(h_vert_off, T.vert_off, sizeof(unsigned long long) * (n + 1), cudaMemcpyDeviceToHost, s),
+            "read vertex offsets");
     DCB_TRY(h, cudaStreamSynchronize(s), "mark");
     const long long nv = (long long)hc->total_active;
     if (nv >= 0x7fffffffLL) return fail(h, DCB_ERR_TOO_LARGE, "more than 2^31-1 vertices");
@@ -199,11 +311,17 @@ int run_pipeline(dcb_context* h, const dcb_grid* in, const dcb_opts* o, cudaStre
     h->nv = nv;
     h->nf = 0;
     h->vpf = o->emit_triangles ? 3 : 4;
-    h->cx = g.cx;
-    h->cy = g.cy;
+    h->cx = L.slots[0].g.cx;
+    h->cy = L.slots[0].g.cy;
+    h->batch_n = n;
+    h->batch_cx.resize(n); h->batch_cy.resize(n);
+    h->vert_offsets.assign(n + 1, 0);
+    h->face_offsets.assign(n + 1, 0);
+    for (int b = 0; b < n; ++b) { h->batch_cx[b] = L.slots[b].g.cx; h->batch_cy[b] = L.slots[b].g.cy; }
+    for (int b = 0; b <= n; ++b) h->vert_offsets[b] = (int64_t)h_vert_off[b];
     if (st) {
-        st->nx = g.nx; st->ny = g.ny; st->nz = g.nz;
-        st->total_cells = ncell; st->active_cells = nv; st->vertex_count = nv;
+        st->nx = L.slots[0].g.nx; st->ny = L.slots[0].g.ny; st->nz = L.slots[0].g.nz;
+        st->total_cells = L.ncell; st->active_cells = nv; st->vertex_count = nv;
     }
     if (nv == 0) {
         DCB_TRY(h, cudaEventRecord(h->ev[3], s), "event");
@@ -228,17 +346,17 @@ int run_pipeline(dcb_context* h, const dcb_grid* in, const dcb_opts* o, cudaStre
     DCB_TRY(h, ensure(h->wind_items, sizeof(uint4) * wind_cap), "alloc winding list");
     DCB_TRY(h, ensure(h->v64_cells, sizeof(uint32_t) * v64_cap), "alloc fp64 cells");
     DCB_TRY(h, ensure(h->V64, sizeof(double) * 3 * v64_cap), "alloc fp64 vertices");
-    DCB_TRY(h, cudaMemsetAsync(h->col_count.p, 0, sizeof(uint32_t) * 3 * cxcy, s), "memset");
-    DCB_TRY(h, cudaMemsetAsync(h->col_fill.p, 0, sizeof(uint32_t) * 3 * cxcy, s), "memset");
+    DCB_TRY(h, cudaMemsetAsync(h->col_count.p, 0, sizeof(uint32_t) * ncol, s), "memset");
+    DCB_TRY(h, cudaMemsetAsync(h->col_fill.p, 0, sizeof(uint32_t) * ncol, s), "memset");
     DCB_TRY(h, cudaMemsetAsync(h->v64_index.p, 0xff, sizeof(int) * nv, s), "memset");
 
     // 2) ranks + list, QEF with fused edge normals (rank-1 fast path, Jacobi list, FP64).
     ExpandParams xp;
-    xp.g = g; xp.nxt = nxt; xp.bits = mp.bits; xp.seg_count = mp.seg_count;
+    xp.B = T.B; xp.nseg = nseg; xp.bits = as<uint32_t>(h->bits); xp.seg_count = as<uint32_t>(h->seg_count);
     xp.seg_start = as<uint32_t>(h->seg_start); xp.super = as<uint32_t>(h->super); xp.list = as<uint64_t>(h->list);
     DCB_TRY(h, launch_expand(xp, h->num_sms, s), "launch expand");
     QefParams qp;
-    qp.g = g; qp.list = xp.list; qp.nactive = nv; qp.V = as<float>(h->V); qp.vclass = as<uint8_t>(h->vclass);
+    qp.B = T.B; qp.list = xp.list; qp.nactive = nv; qp.V = as<float>(h->V); qp.vclass = as<uint8_t>(h->vclass);
     qp.fmask = as<uint8_t>(h->fmask); qp.col_count = as<uint32_t>(h->col_count);
     qp.esc_list = as<uint32_t>(h->esc_list); qp.esc_count = &dc->esc_count;
     qp.hard_list = as<uint32_t>(h->hard_list); qp.hard_data = as<float4>(h->hard_data); qp.hard_count = &dc->hard_count;
@@ -248,17 +366,19 @@ int run_pipeline(dcb_context* h, const dcb_grid* in, const dcb_opts* o, cudaStre
     DCB_TRY(h, launch_cell_qef(qp, h->num_sms, s), "launch qef");
     DCB_TRY(h, launch_cell_jacobi(qp, nv, h->num_sms, s), "launch jacobi");
     Vertex64Params v64;
-    v64.g = g; v64.list = xp.list; v64.cells = qp.esc_list; v64.count = &dc->esc_count; v64.cap = (unsigned int)nv;
+    v64.B = T.B; v64.list = xp.list; v64.cells = qp.esc_list; v64.count = &dc->esc_count; v64.cap = (unsigned int)nv;
     v64.Vf = qp.V; v64.vclass = qp.vclass; v64.V64 = nullptr; v64.thr = o->svd_threshold;
     DCB_TRY(h, launch_vertex_fp64(v64, nv, h->num_sms, s), "launch vertex fp64");
     DCB_TRY(h, cudaEventRecord(h->ev[3], s), "event");
 
     // 3) faces: column scan, scatter with FP32 winding, FP64 re-decisions, in-column order.
-    DCB_TRY(h, launch_scan(as<uint32_t>(h->col_count), 3 * cxcy, as<uint32_t>(h->partials),
+    DCB_TRY(h, launch_scan(as<uint32_t>(h->col_count), ncol, as<uint32_t>(h->partials),
                            as<uint32_t>(h->col_start), &dc->face_total, s), "launch scan");
+    if (n > 1)
+        DCB_TRY(h, launch_face_offsets(T.B, as<uint32_t>(h->col_start), &dc->face_total, T.face_off, s), "face offsets");
     FaceParams fp;
-    fp.g = g; fp.list = xp.list; fp.nactive = nv; fp.fmask = qp.fmask; fp.V = qp.V; fp.vclass = qp.vclass;
-    fp.bits = mp.bits; fp.super = xp.super;
+    fp.B = T.B; fp.list = xp.list; fp.nactive = nv; fp.fmask = qp.fmask; fp.V = qp.V; fp.vclass = qp.vclass;
+    fp.bits = xp.bits; fp.super = xp.super;
     fp.col_start = as<uint32_t>(h->col_start); fp.col_count = as<uint32_t>(h->col_count);
     fp.col_fill = as<uint32_t>(h->col_fill);
     fp.stage_quad = as<int4>(h->stage_quad); fp.stage_key = as<uint2>(h->stage_key);
@@ -267,14 +387,14 @@ int run_pipeline(dcb_context* h, const dcb_grid* in, const dcb_opts* o, cudaStre
     fp.v64_index = as<int>(h->v64_index); fp.v64_cells = as<uint32_t>(h->v64_cells);
     fp.v64_count = &dc->v64_count; fp.v64_cap = (unsigned long long)v64_cap;
     fp.err = &dc->err;
-    fp.hmax = std::max(std::fabs(g.vx), std::max(std::fabs(g.vy), std::fabs(g.vz)));
+    fp.hmax = L.hmax;
     DCB_TRY(h, launch_face_scatter(fp, h->num_sms, s), "launch face scatter");
     Vertex64Params w64;
-    w64.g = g; w64.list = xp.list; w64.cells = fp.v64_cells; w64.count = fp.v64_count; w64.cap = (unsigned int)v64_cap;
+    w64.B = T.B; w64.list = xp.list; w64.cells = fp.v64_cells; w64.count = fp.v64_count; w64.cap = (unsigned int)v64_cap;
     w64.Vf = nullptr; w64.vclass = nullptr; w64.V64 = as<double>(h->V64); w64.thr = o->svd_threshold;
     DCB_TRY(h, launch_vertex_fp64(w64, v64_cap, h->num_sms, s), "launch fp64 vertices for windings");
     Winding64Params wp;
-    wp.g = g; wp.items = fp.wind_items; wp.count = fp.wind_count; wp.cap = (unsigned int)wind_cap;
+    wp.B = T.B; wp.items = fp.wind_items; wp.count = fp.wind_count; wp.cap = (unsigned int)wind_cap;
     wp.quads = fp.stage_quad; wp.v64_index = fp.v64_index; wp.V64 = w64.V64; wp.err = &dc->err;
     DCB_TRY(h, launch_winding_fp64(wp, wind_cap, h->num_sms, s), "launch winding fp64");
     DCB_TRY(h, launch_face_order(fp.stage_quad, fp.stage_key, fp.col_start, fp.col_count, &dc->face_total,
@@ -297,6 +417,15 @@ int run_pipeline(dcb_context* h, const dcb_grid* in, const dcb_opts* o, cudaStre
         t64.v64_index = fp.v64_index; t64.V64 = w64.V64; t64.tris = tp.tris; t64.err = &dc->err;
         DCB_TRY(h, launch_tri_fp64(t64, wind_cap, h->num_sms, s), "launch triangle fp64");
     }
+    if (n > 1) {
+        // 5) faces refer to vertices of their own grid
+        if (o->emit_triangles)
+            DCB_TRY(h, launch_localize_faces(T.vert_off, T.face_off, n, as<int>(h->tris), 3, 6 * nv, h->num_sms, s), "localize");
+        else
+            DCB_TRY(h, launch_localize_faces(T.vert_off, T.face_off, n, as<int>(h->faces), 4, 3 * nv, h->num_sms, s), "localize");
+        DCB_TRY(h, cudaMemcpyAsync(h_face_off, T.face_off, sizeof(unsigned long long) * (n + 1),
+                                   cudaMemcpyDeviceToHost, s), "read face offsets");
+    }
     DCB_TRY(h, cudaEventRecord(h->ev[4], s), "event");
     DCB_TRY(h, cudaMemcpyAsync(hc, dc, sizeof(Counters), cudaMemcpyDeviceToHost, s), "read counters");
     DCB_TRY(h, cudaStreamSynchronize(s), "pipeline");
@@ -304,8 +433,11 @@ int run_pipeline(dcb_context* h, const dcb_grid* in, const dcb_opts* o, cudaStre
         return fail(h, hc->err == kErrTimeout ? DCB_ERR_TIMEOUT : DCB_ERR_INTERNAL,
                     hc->err == kErrOverflow ? "FP64 work list overflow" : "device error flag set");
     }
+    const int fpq = o->emit_triangles ? 2 : 1;
     h->vpf = o->emit_triangles ? 3 : 4;
-    h->nf = (int64_t)hc->face_total * (o->emit_triangles ? 2 : 1);
+    h->nf = (int64_t)hc->face_total * fpq;
+    if (n > 1) for (int b = 0; b <= n; ++b) h->face_offsets[b] = (int64_t)h_face_off[b] * fpq;
+    else { h->face_offsets[0] = 0; h->face_offsets[1] = h->nf; }
     if (st) {
         st->face_count = h->nf;
         st->qef_fallback_count = hc->esc_count;
@@ -315,6 +447,10 @@ int run_pipeline(dcb_context* h, const dcb_grid* in, const dcb_opts* o, cudaStre
         st->clamp_count = 0;
     }
     return DCB_OK;
+}
+
+int run_pipeline(dcb_context* h, const dcb_grid* in, const dcb_opts* o, cudaStream_t s, dcb_stats* st) {
+    return run_batch(h, in, 1, o, s, st);
 }
 
 void fill_times(dcb_context* h, dcb_stats* st, bool upload) {
@@ -495,10 +631,12 @@ int dcb_destroy(dcb_handle h) {
                       &h->tris, &h->tri_items, &h->m_verts, &h->m_faces, &h->m_out, &h->m_tris,
                       &h->m_bin_count, &h->m_bin_start, &h->m_bin_fill, &h->m_bin_scratch, &h->m_bin_tris,
                       &h->m_bin_active, &h->m_active_list, &h->m_axis_start, &h->m_far, &h->m_ext, &h->m_tmp,
-                      &h->m_partials, &h->m_counters};
+                      &h->m_partials, &h->m_counters, &h->table};
     for (DevBuf* b : bufs) if (b->p) cudaFree(b->p);
     if (h->h_counters) cudaFreeHost(h->h_counters);
     if (h->h_sdf_counters) cudaFreeHost(h->h_sdf_counters);
+    if (h->h_table) cudaFreeHost(h->h_table);
+    if (h->h_offsets) cudaFreeHost(h->h_offsets);
     if (h->hV) cudaFreeHost(h->hV);
     if (h->hF) cudaFreeHost(h->hF);
     for (auto& ev : h->ev) if (ev) cudaEventDestroy(ev);
@@ -531,6 +669,40 @@ int dcb_extract_device(dcb_handle h, const dcb_grid* grid, const dcb_opts* opts,
         out->vertices = as<float>(h->V);
         out->faces = face_ptr(h);
         out->cell_coords = as<uint64_t>(h->list);
+    }
+    return DCB_OK;
+}
+
+int dcb_extract_batch_device(dcb_handle h, const dcb_grid* grids, int n, const dcb_opts* opts,
+                             dcb_batch_mesh* out, dcb_stats* stats, void* cuda_stream) {
+    if (!h) return DCB_ERR_INVALID_ARGUMENT;
+    if (!grids || n < 1) return fail(h, DCB_ERR_INVALID_ARGUMENT, "empty batch");
+    for (int b = 0; b < n; ++b) {
+        const int rc = validate(h, grids + b);
+        if (rc != DCB_OK) return rc;
+    }
+    dcb_opts def;
+    dcb_default_opts(&def);
+    const dcb_opts* o = opts ? opts : &def;
+    if (o->method != DCB_METHOD_DUAL_CONTOURING) return fail(h, DCB_ERR_NOT_SUPPORTED, "only dual contouring is implemented");
+    if (!(o->svd_threshold >= 0.0)) return fail(h, DCB_ERR_INVALID_ARGUMENT, "svd_threshold must be >= 0");
+    if (cudaSetDevice(h->device) != cudaSuccess) { cudaGetLastError(); return fail(h, DCB_ERR_CUDA, "set device"); }
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(cuda_stream);
+    if (stats) std::memset(stats, 0, sizeof(*stats));
+    DCB_TRY(h, cudaEventRecord(h->ev[0], s), "event");
+    DCB_TRY(h, cudaEventRecord(h->ev[1], s), "event");
+    const int rc = run_batch(h, grids, n, o, s, stats);
+    if (rc != DCB_OK) return rc;
+    fill_times(h, stats, false);
+    if (stats) stats->total_ms = elapsed(h->ev[1], h->ev[4]);
+    if (out) {
+        out->vertex_count = h->nv;
+        out->face_count = h->nf;
+        out->verts_per_face = h->vpf;
+        out->vertices = as<float>(h->V);
+        out->faces = face_ptr(h);
+        out->vertex_offset = h->vert_offsets.data();
+        out->face_offset = h->face_offsets.data();
     }
     return DCB_OK;
 }
@@ -603,10 +775,13 @@ int dcb_copy_cells_to_host(dcb_handle h, int64_t* cell_linear_index, void* cuda_
     uint64_t* packed = reinterpret_cast<uint64_t*>(cell_linear_index);
     DCB_TRY(h, cudaMemcpyAsync(packed, h->list.p, sizeof(uint64_t) * h->nv, cudaMemcpyDeviceToHost, s), "copy cells");
     DCB_TRY(h, cudaStreamSynchronize(s), "copy cells");
+    int b = 0;
     for (int64_t r = 0; r < h->nv; ++r) {
+        while (h->batch_n > 1 && b + 1 < h->batch_n && r >= h->vert_offsets[b + 1]) ++b;
+        const int64_t cx = h->batch_n > 1 ? h->batch_cx[b] : h->cx, cy = h->batch_n > 1 ? h->batch_cy[b] : h->cy;
         const uint64_t p = packed[r];
         const int64_t i = (int64_t)(p & 0x1FFFFF), j = (int64_t)((p >> 21) & 0x1FFFFF), k = (int64_t)(p >> 42);
-        cell_linear_index[r] = i + (int64_t)h->cx * (j + (int64_t)h->cy * k);
+        cell_linear_index[r] = i + cx * (j + cy * k);
     }
     return DCB_OK;
 }

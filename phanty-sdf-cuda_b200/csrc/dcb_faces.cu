@@ -164,23 +164,28 @@ __device__ __forceinline__ void request_fp64_vertex(int* v64_index, uint32_t* v6
     }
 }
 
+template <bool ONE>
 __global__ void __launch_bounds__(128)
-k_face_scatter(FaceParams P) {
-    const GridDesc& g = P.g;
-    const long long cxcy = (long long)g.cx * g.cy;
+k_face_scatter(const __grid_constant__ FaceParams P) {
     for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < P.nactive;
          r += (long long)gridDim.x * blockDim.x) {
         const uint8_t fm = P.fmask[r];
         if (!fm) continue;
+        const int gi = ONE ? 0 : slot_of_rank(P.B, (unsigned long long)r);
+        const GridSlot& S = slot_ref<ONE>(P.B, gi);
+        const GridDesc& g = S.g;
+        const long long cxcy = (long long)g.cx * g.cy;
+        const uint32_t* const bits = P.bits + S.bits_off;
+        const uint32_t* const super = P.super + S.super_off;
         int i, j, k;
         unpack_cell(P.list[r], i, j, k);
         const float3 g0 = grid_gradient32(g, i, j, k);
         // Ranks of the face cells. All four cells of a face are active, so a cell's x-1
         // neighbour in a face is the previous active cell in linear order (rank - 1).
         uint32_t r_k1 = 0xffffffffu, r_j1 = 0xffffffffu, r_jk = 0xffffffffu;
-        if (fm & 3) r_k1 = cell_rank(P.bits, P.super, g, i, j, k - 1);
-        if (fm & 5) r_j1 = cell_rank(P.bits, P.super, g, i, j - 1, k);
-        if (fm & 1) r_jk = cell_rank(P.bits, P.super, g, i, j - 1, k - 1);
+        if (fm & 3) r_k1 = cell_rank(bits, super, g, i, j, k - 1);
+        if (fm & 5) r_j1 = cell_rank(bits, super, g, i, j - 1, k);
+        if (fm & 1) r_jk = cell_rank(bits, super, g, i, j - 1, k - 1);
 #pragma unroll
         for (int axis = 0; axis < 3; ++axis) {
             if (!(fm & (1 << axis))) continue;
@@ -211,7 +216,7 @@ k_face_scatter(FaceParams P) {
             const bool uncertain = near_fallback || gn2 < 1e-4f ||
                                    fabsf(d) <= 4.f * dq * gnl + 1e-5f * qnl * gnl;
             bool swap = !uncertain && gn2 > 0.f && qn2 > 0.f && d < 0.f;
-            const long long col = axis * cxcy + (long long)i * g.cy + j;
+            const long long col = S.col_off + axis * cxcy + (long long)i * g.cy + j;
             const uint32_t slot = P.col_start[col] + atomicAdd(&P.col_fill[col], 1u);
             P.stage_quad[slot] = swap ? make_int4((int)r0, (int)r3, (int)r2, (int)r1)
                                       : make_int4((int)r0, (int)r1, (int)r2, (int)r3);
@@ -220,7 +225,7 @@ k_face_scatter(FaceParams P) {
                 const unsigned int w = atomicAdd(P.wind_count, 1u);
                 if (w < P.wind_cap) {
                     const uint64_t pk = pack_cell(i, j, k);
-                    P.wind_items[w] = make_uint4(slot, (uint32_t)axis, (uint32_t)pk, (uint32_t)(pk >> 32));
+                    P.wind_items[w] = make_uint4(slot, (uint32_t)axis | ((uint32_t)gi << 2), (uint32_t)pk, (uint32_t)(pk >> 32));
                 } else {
                     set_error(P.err, kErrOverflow);
                 }
@@ -239,7 +244,8 @@ cudaError_t launch_face_scatter(const FaceParams& P, int num_sms, cudaStream_t s
     long long blocks = (P.nactive + 127) / 128;
     const long long cap = (long long)num_sms * 16;
     if (blocks > cap) blocks = cap;
-    k_face_scatter<<<(unsigned)blocks, 128, 0, s>>>(P);
+    if (P.B.n == 1) k_face_scatter<true><<<(unsigned)blocks, 128, 0, s>>>(P);
+    else            k_face_scatter<false><<<(unsigned)blocks, 128, 0, s>>>(P);
     return cudaGetLastError();
 }
 
@@ -269,6 +275,47 @@ cudaError_t launch_face_order(const int4* stage_quad, const uint2* stage_key, co
     const long long cap = (long long)num_sms * 16;
     if (blocks > cap) blocks = cap;
     k_face_order<<<(unsigned)blocks, 256, 0, s>>>(stage_quad, stage_key, col_start, col_count, nfaces, faces);
+    return cudaGetLastError();
+}
+
+// ---- batch bookkeeping ------------------------------------------------------------------
+
+// face_off[b] = col_start[col_off[b]], face_off[n] = total: the first face of every grid.
+__global__ void k_face_offsets(BatchTable B, const uint32_t* __restrict__ col_start,
+                               const unsigned long long* __restrict__ total, unsigned long long* face_off) {
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b <= B.n; b += gridDim.x * blockDim.x)
+        face_off[b] = b < B.n ? (unsigned long long)col_start[B.col_off[b]] : *total;
+}
+
+cudaError_t launch_face_offsets(const BatchTable& B, const uint32_t* col_start, const unsigned long long* total,
+                                unsigned long long* face_off, cudaStream_t s) {
+    k_face_offsets<<<(B.n + 1 + 255) / 256, 256, 0, s>>>(B, col_start, total, face_off);
+    return cudaGetLastError();
+}
+
+// Face vertex indices from batch-global ranks to ranks within the face's own grid. faces
+// holds vpf ints per face; face f of the batch belongs to the grid b with
+// face_off[b] * fpq <= f < face_off[b+1] * fpq (fpq = faces per quad: 1, or 2 for triangles).
+__global__ void __launch_bounds__(256) k_localize_faces(const unsigned long long* __restrict__ vert_off,
+                                                        const unsigned long long* __restrict__ face_off, int n,
+                                                        int* faces, int vpf) {
+    const int fpq = vpf == 3 ? 2 : 1;
+    const unsigned long long nf = face_off[n] * fpq;
+    for (unsigned long long f = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; f < nf;
+         f += (unsigned long long)gridDim.x * blockDim.x) {
+        const int b = slot_search(face_off, n, f / fpq);
+        const int base = (int)vert_off[b];
+        for (int q = 0; q < vpf; ++q) faces[f * vpf + q] -= base;
+    }
+}
+
+cudaError_t launch_localize_faces(const unsigned long long* vert_off, const unsigned long long* face_off, int n,
+                                  int* faces, int vpf, long long max_faces, int num_sms, cudaStream_t s) {
+    if (max_faces <= 0) return cudaSuccess;
+    long long blocks = (max_faces + 255) / 256;
+    const long long cap = (long long)num_sms * 16;
+    if (blocks > cap) blocks = cap;
+    k_localize_faces<<<(unsigned)blocks, 256, 0, s>>>(vert_off, face_off, n, faces, vpf);
     return cudaGetLastError();
 }
 

@@ -4,43 +4,107 @@
 
 namespace dcb {
 
-struct MarkParams {
+// One grid of a batch; a single extraction is a batch of one. The per-grid arrays of the
+// pipeline (active bits, super ranks, segment counts, face columns) are concatenated grid
+// by grid; the offsets below locate a grid's part. Vertex ranks are global over the batch
+// (the segment scan runs over all grids), so the vertices of grid b are the contiguous
+// ranks [vert_off[b], vert_off[b+1]).
+struct GridSlot {
     GridDesc g;
-    int R;                         // cell rows per tile (point rows = R + 1 <= 8)
-    int KZ;                        // cell planes per tile
-    int nxt;                       // x-tiles of 1024 cells per row
-    uint32_t* bits;                // [cy*cz][W]
-    uint32_t* seg_count;           // [cz*cy*nxt] active cells per (plane, row, x-tile)
+    long long bits_off;            // first word of the grid's active bits (rows * W)
+    long long super_off;           // first super word (rows * W8)
+    long long seg_off;             // first segment (rows * nxt)
+    long long col_off;             // first face column (3 * cx * cy)
+    int R;                         // mark: cell rows per tile (point rows = R + 1 <= 8)
+    int KZ;                        // mark: cell planes per tile
+    int nxt;                       // mark: x-tiles of 1024 cells per row
+    int nrb;                       // mark: row blocks
+    int nzc;                       // mark: z-chunks
     int vec4;                      // rows are 16-byte aligned and nx % 4 == 0
 };
-cudaError_t launch_mark(const MarkParams& P, cudaStream_t s);
+
+struct BatchTable {
+    GridSlot s0;                           // the grid when n == 1 (read from kernel parameters)
+    const GridSlot* slots;                 // [n], device
+    int n;
+    const long long* seg_off;              // [n+1] first segment per grid
+    const long long* col_off;              // [n+1] first face column per grid
+    const unsigned long long* vert_off;    // [n+1] first vertex rank per grid (after the scan)
+};
+
+// Largest index b in [0, n) with offs[b] <= x (offsets ascending, offs[0] = 0).
+template <typename T>
+__device__ __forceinline__ int slot_search(const T* __restrict__ offs, int n, T x) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(offs + mid) <= x) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+// The hot kernels are instantiated twice: ONE (a single grid, its slot in the kernel
+// parameters, as fast as a kernel without batch support) and batch (slots in global memory).
+template <bool ONE>
+__device__ __forceinline__ const GridSlot& slot_ref(const BatchTable& B, int gi) {
+    return ONE ? B.s0 : B.slots[gi];
+}
+__device__ __forceinline__ int slot_of_rank(const BatchTable& B, unsigned long long r) {
+    return B.n == 1 ? 0 : slot_search(B.vert_off, B.n, r);
+}
+__device__ __forceinline__ int slot_of_segment(const BatchTable& B, long long s) {
+    return B.n == 1 ? 0 : slot_search(B.seg_off, B.n, s);
+}
+__device__ __forceinline__ int slot_of_column(const BatchTable& B, long long c) {
+    return B.n == 1 ? 0 : slot_search(B.col_off, B.n, c);
+}
+
+struct MarkParams {
+    BatchTable B;
+    const int* tile_slot;          // [m] the grids of this launch (all share the load path)
+    const long long* tile_off;     // [m+1] first tile of each of them
+    int m;
+    long long ntiles;
+    uint32_t* bits;                // all grids' active bits
+    uint32_t* seg_count;           // all grids' segment counts
+};
+cudaError_t launch_mark(const MarkParams& P, int vec4, cudaStream_t s);
 int mark_tile_words();
 int mark_ctas_per_sm(int vec4);   // resident CTAs of the mark kernel per SM
 int mark_max_rows();
 
 struct ExpandParams {
-    GridDesc g;
-    int nxt;
+    BatchTable B;
+    long long nseg;                // segments of all grids
     const uint32_t* bits;
     const uint32_t* seg_count;
-    const uint32_t* seg_start;     // exclusive scan of seg_count
-    uint32_t* super;               // [cy*cz][W8]
-    uint64_t* list;                // [active]
+    const uint32_t* seg_start;     // exclusive scan of seg_count (global ranks)
+    uint32_t* super;               // all grids' super ranks
+    uint64_t* list;                // [active] packed cells, grid-local coordinates
 };
 cudaError_t launch_expand(const ExpandParams& P, int num_sms, cudaStream_t s);
+
+// vert_off[b] = seg_start[seg_off[b]] (b < n), vert_off[n] = total.
+cudaError_t launch_vert_offsets(const BatchTable& B, const uint32_t* seg_start, const unsigned long long* total,
+                                unsigned long long* vert_off, cudaStream_t s);
+// face_off[b] = col_start[col_off[b]] (b < n), face_off[n] = total.
+cudaError_t launch_face_offsets(const BatchTable& B, const uint32_t* col_start, const unsigned long long* total,
+                                unsigned long long* face_off, cudaStream_t s);
+// Global vertex ranks in the faces -> ranks within each face's grid (vpf ints per face).
+cudaError_t launch_localize_faces(const unsigned long long* vert_off, const unsigned long long* face_off, int n,
+                                  int* faces, int vpf, long long max_faces, int num_sms, cudaStream_t s);
 
 // Error class of a stored vertex (cell widths, before the float rounding of the output):
 // 0 = certified rank-1 FP32 solve (<= 2e-6), 1 = FP32 Jacobi (<= 1e-4), 2 = FP64 path.
 enum VertexClass : uint8_t { kVcRank1 = 0, kVcJacobi = 1, kVcFp64 = 2 };
 
 struct QefParams {
-    GridDesc g;
+    BatchTable B;
     const uint64_t* list;
     long long nactive;
     float* V;
     uint8_t* vclass;                // [active] VertexClass
     uint8_t* fmask;                 // bit a: cell owns a face on its min-corner edge a
-    uint32_t* col_count;            // [3][cx*cy]: a*cx*cy + i*cy + j
+    uint32_t* col_count;            // per grid [3][cx*cy]: col_off + a*cx*cy + i*cy + j
     uint32_t* esc_list;
     unsigned int* esc_count;
     uint32_t* hard_list;            // cells not certified rank 1
@@ -56,7 +120,7 @@ cudaError_t launch_cell_qef(const QefParams& P, int num_sms, cudaStream_t s);
 cudaError_t launch_cell_jacobi(const QefParams& P, long long max_items, int num_sms, cudaStream_t s);
 
 struct Vertex64Params {
-    GridDesc g;
+    BatchTable B;
     const uint64_t* list;
     const uint32_t* cells;          // ranks of the cells to solve
     const unsigned int* count;
@@ -69,8 +133,8 @@ struct Vertex64Params {
 cudaError_t launch_vertex_fp64(const Vertex64Params& P, long long max_items, int num_sms, cudaStream_t s);
 
 struct Winding64Params {
-    GridDesc g;
-    const uint4* items;             // {staging slot, axis, packed cell lo, packed cell hi}
+    BatchTable B;
+    const uint4* items;             // {staging slot, axis | grid << 2, packed cell lo, packed cell hi}
     const unsigned int* count;
     unsigned int cap;
     int4* quads;                    // staging quads (rewritten in place)
@@ -85,7 +149,7 @@ cudaError_t launch_scan(const uint32_t* in, long long n, uint32_t* partials, uin
 long long scan_partials_len(long long n);
 
 struct FaceParams {
-    GridDesc g;
+    BatchTable B;
     const uint64_t* list;
     long long nactive;
     const uint8_t* fmask;
@@ -93,12 +157,12 @@ struct FaceParams {
     const uint8_t* vclass;
     const uint32_t* bits;
     const uint32_t* super;
-    const uint32_t* col_start;     // [3][cx*cy]
+    const uint32_t* col_start;     // per grid [3][cx*cy] (global column index)
     const uint32_t* col_count;
     uint32_t* col_fill;
     int4* stage_quad;
     uint2* stage_key;              // {k, column}
-    uint4* wind_items;             // {slot, axis, packed lo, packed hi}
+    uint4* wind_items;             // {slot, axis | grid << 2, packed lo, packed hi}
     unsigned int* wind_count;
     unsigned long long wind_cap;
     int* v64_index;                // [rank] -> FP64 vertex slot (-1 none, -2 being claimed)
@@ -106,7 +170,7 @@ struct FaceParams {
     unsigned int* v64_count;
     unsigned long long v64_cap;
     int* err;
-    float hmax;                    // largest cell width (world units)
+    float hmax;                    // largest cell width of the batch (world units)
 };
 cudaError_t launch_face_scatter(const FaceParams& P, int num_sms, cudaStream_t s);
 cudaError_t launch_face_order(const int4* stage_quad, const uint2* stage_key, const uint32_t* col_start,

@@ -83,18 +83,26 @@ __device__ __forceinline__ void row_words(const RowRegs& R, int lane, uint32_t* 
     }
 }
 
-template <bool VEC4>
+template <bool VEC4, bool ONE>
 __global__ void __launch_bounds__(kMarkWarps * 32)
-k_mark_zmarch(MarkParams P) {
+k_mark_zmarch(const __grid_constant__ MarkParams P) {
     __shared__ uint32_t s_nw[2][kMarkWarps][kPtWords];
     __shared__ uint32_t s_pw[2][kMarkWarps][kPtWords];
-    const GridDesc& g = P.g;
+    // tile -> grid of the batch -> (x-tile, row block, z-chunk), x-tile fastest
+    const long long tile = blockIdx.x;
+    const int mi = (ONE || P.m == 1) ? 0 : slot_search(P.tile_off, P.m, tile);
+    const GridSlot& S = slot_ref<ONE>(P.B, ONE ? 0 : P.tile_slot[mi]);
+    const GridDesc& g = S.g;
+    const int R = S.R, KZ = S.KZ, nxt = S.nxt;
+    const long long local = ONE ? tile : tile - P.tile_off[mi];
+    const int xt = (int)(local % nxt);         // x-tile
+    const int j0 = (int)((local / nxt) % S.nrb) * R;   // first cell row
+    const int kb = (int)(local / ((long long)nxt * S.nrb)) * KZ;   // first cell plane
+    uint32_t* const bits = P.bits + S.bits_off;
+    uint32_t* const seg_count = P.seg_count + S.seg_off;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int xt = blockIdx.x;                 // x-tile
-    const int j0 = blockIdx.y * P.R;           // first cell row
-    const int kb = blockIdx.z * P.KZ;          // first cell plane
-    const int rows = min(P.R, g.cy - j0);
-    const int ke = min(g.cz, kb + P.KZ);
+    const int rows = min(R, g.cy - j0);
+    const int ke = min(g.cz, kb + KZ);
     const int x0 = xt * kTileWords * 32;       // first point / cell of the tile
     const bool loader = warp <= rows;          // point rows j0..j0+rows
     const float* base = g.v + (int64_t)(j0 + (loader ? warp : 0)) * g.nx;
@@ -125,11 +133,11 @@ k_mark_zmarch(MarkParams P) {
             const uint32_t q1 = s_pw[p0][r][lane + 1] | s_pw[p0][r + 1][lane + 1] | s_pw[p1][r][lane + 1] | s_pw[p1][r + 1][lane + 1];
             const uint32_t act = (n0 | (n0 >> 1) | (n1 << 31)) & (q0 | (q0 >> 1) | (q1 << 31)) & vmask;
             const int64_t row = (int64_t)(j0 + r) + (int64_t)g.cy * k;
-            if (wglob < g.W) P.bits[row * g.W + wglob] = act;
+            if (wglob < g.W) bits[row * g.W + wglob] = act;
             uint32_t cnt = __popc(act);
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
-            if (lane == 0) P.seg_count[row * P.nxt + xt] = cnt;
+            if (lane == 0) seg_count[row * nxt + xt] = cnt;
         }
         __syncthreads();
     }
@@ -137,27 +145,32 @@ k_mark_zmarch(MarkParams P) {
 
 // Warp per group of 32 consecutive (row, x-tile) segments: the non-empty ones (ballot) get
 // the global ranks of their super words and their part of the packed active-cell list.
+template <bool ONE>
 __global__ void __launch_bounds__(256)
-k_expand_ranks(ExpandParams P) {
-    const GridDesc& g = P.g;
+k_expand_ranks(const __grid_constant__ ExpandParams P) {
     const int lane = threadIdx.x & 31;
-    const long long nseg = (long long)g.cy * g.cz * P.nxt;
+    const long long nseg = P.nseg;
     const long long ngroups = (nseg + 31) / 32;
     for (long long grp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; grp < ngroups;
          grp += ((long long)gridDim.x * blockDim.x) >> 5) {
         const long long s0 = grp * 32;
-        const uint32_t cnt = (s0 + lane < nseg) ? P.seg_count[s0 + lane] : 0u;
+        const bool have = s0 + lane < nseg;
+        const uint32_t cnt = have ? P.seg_count[s0 + lane] : 0u;
         uint32_t live = __ballot_sync(0xffffffffu, cnt != 0);
-        const uint32_t my_start = (s0 + lane < nseg && cnt) ? P.seg_start[s0 + lane] : 0u;
+        const uint32_t my_start = (have && cnt) ? P.seg_start[s0 + lane] : 0u;
+        const int my_slot = (!ONE && have && cnt) ? slot_of_segment(P.B, s0 + lane) : 0;
         while (live) {
             const int b = __ffs(live) - 1;
             live &= live - 1;
             const long long s = s0 + b;
             const uint32_t seg_first = __shfl_sync(0xffffffffu, my_start, b);
-            const long long row = s / P.nxt;
-            const int xt = (int)(s - row * P.nxt);
+            const GridSlot& S = slot_ref<ONE>(P.B, __shfl_sync(0xffffffffu, my_slot, b));
+            const GridDesc& g = S.g;
+            const long long ls = s - S.seg_off;            // segment within its grid
+            const long long row = ls / S.nxt;
+            const int xt = (int)(ls - row * S.nxt);
             const int w = xt * kTileWords + lane;
-            const uint32_t act = (w < g.W) ? P.bits[row * g.W + w] : 0u;
+            const uint32_t act = (w < g.W) ? P.bits[S.bits_off + row * g.W + w] : 0u;
             const uint32_t c = __popc(act);
             uint32_t incl = c;
 #pragma unroll
@@ -166,7 +179,7 @@ k_expand_ranks(ExpandParams P) {
                 if (lane >= o) incl += t;
             }
             const uint32_t first = seg_first + incl - c;
-            if (w < g.W && (w & 7) == 0) P.super[row * g.W8 + (w >> 3)] = first;
+            if (w < g.W && (w & 7) == 0) P.super[S.super_off + row * g.W8 + (w >> 3)] = first;
             const int j = (int)(row % g.cy), k = (int)(row / g.cy);
             uint32_t m = act, q = 0;
             while (m) {
@@ -179,27 +192,47 @@ k_expand_ranks(ExpandParams P) {
     }
 }
 
-cudaError_t launch_mark(const MarkParams& P, cudaStream_t s) {
-    dim3 grid((unsigned)P.nxt, (unsigned)((P.g.cy + P.R - 1) / P.R), (unsigned)((P.g.cz + P.KZ - 1) / P.KZ));
-    if (P.vec4) k_mark_zmarch<true><<<grid, kMarkWarps * 32, 0, s>>>(P);
-    else        k_mark_zmarch<false><<<grid, kMarkWarps * 32, 0, s>>>(P);
+// vert_off[b] = seg_start[seg_off[b]], vert_off[n] = total: the first vertex rank of every grid.
+__global__ void k_vert_offsets(BatchTable B, const uint32_t* __restrict__ seg_start,
+                               const unsigned long long* __restrict__ total, unsigned long long* vert_off) {
+    for (int b = blockIdx.x * blockDim.x + threadIdx.x; b <= B.n; b += gridDim.x * blockDim.x)
+        vert_off[b] = b < B.n ? (unsigned long long)seg_start[B.seg_off[b]] : *total;
+}
+
+cudaError_t launch_vert_offsets(const BatchTable& B, const uint32_t* seg_start, const unsigned long long* total,
+                                unsigned long long* vert_off, cudaStream_t s) {
+    k_vert_offsets<<<(B.n + 1 + 255) / 256, 256, 0, s>>>(B, seg_start, total, vert_off);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mark(const MarkParams& P, int vec4, cudaStream_t s) {
+    if (P.ntiles <= 0) return cudaSuccess;
+    const bool one = P.B.n == 1;
+    if (vec4) {
+        if (one) k_mark_zmarch<true, true><<<(unsigned)P.ntiles, kMarkWarps * 32, 0, s>>>(P);
+        else     k_mark_zmarch<true, false><<<(unsigned)P.ntiles, kMarkWarps * 32, 0, s>>>(P);
+    } else {
+        if (one) k_mark_zmarch<false, true><<<(unsigned)P.ntiles, kMarkWarps * 32, 0, s>>>(P);
+        else     k_mark_zmarch<false, false><<<(unsigned)P.ntiles, kMarkWarps * 32, 0, s>>>(P);
+    }
     return cudaGetLastError();
 }
 
 cudaError_t launch_expand(const ExpandParams& P, int num_sms, cudaStream_t s) {
-    const long long nseg = (long long)P.g.cy * P.g.cz * P.nxt;
+    const long long nseg = P.nseg;
     long long blocks = ((nseg + 31) / 32 * 32 + 255) / 256;
     const long long cap = (long long)num_sms * 32;
     if (blocks > cap) blocks = cap;
     if (blocks < 1) blocks = 1;
-    k_expand_ranks<<<(unsigned)blocks, 256, 0, s>>>(P);
+    if (P.B.n == 1) k_expand_ranks<true><<<(unsigned)blocks, 256, 0, s>>>(P);
+    else            k_expand_ranks<false><<<(unsigned)blocks, 256, 0, s>>>(P);
     return cudaGetLastError();
 }
 
 int mark_ctas_per_sm(int vec4) {
     int n = 0;
-    const cudaError_t e = vec4 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_mark_zmarch<true>, kMarkWarps * 32, 0)
-                               : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_mark_zmarch<false>, kMarkWarps * 32, 0);
+    const cudaError_t e = vec4 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_mark_zmarch<true, true>, kMarkWarps * 32, 0)
+                               : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_mark_zmarch<false, true>, kMarkWarps * 32, 0);
     if (e != cudaSuccess) { cudaGetLastError(); return 1; }
     return n > 0 ? n : 1;
 }

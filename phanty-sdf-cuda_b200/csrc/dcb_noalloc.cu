@@ -45,6 +45,18 @@ cudaError_t scratch_address(int device, void** out) {
 
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
+// The grid as a batch of one: its slot and offset tables (see dcb_kernels.cuh).
+struct Table {
+    GridSlot slot;
+    long long seg_off[2];
+    long long col_off[2];
+    unsigned long long vert_off[2];
+    long long tile_off[2];
+    int tile_slot[2];
+};
+
+__global__ void k_store_table(Table* dst, Table src) { *dst = src; }
+
 // Packed (i | j<<21 | k<<42) -> linear index i + cx*(j + cy*k), in place.
 __global__ void k_packed_to_linear(uint64_t* cells, long long n, int cx, int cy) {
     for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (long long)gridDim.x * blockDim.x) {
@@ -83,9 +95,31 @@ extern "C" int dcb_mark_active_cells_noalloc(const dcb_grid* grid, int64_t* cell
     const int nxt = (g.cx + tile_cells - 1) / tile_cells;
     const long long nseg = rows * nxt;
 
-    // Scratch layout, each part 256-byte aligned: total | bits | super | seg_count |
+    int sms = 148;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) { cudaGetLastError(); return DCB_ERR_CUDA; }
+    // The grid as a batch of one: its slot and offset tables also live in the scratch array.
+    GridSlot slot;
+    slot.g = g;
+    slot.bits_off = 0; slot.super_off = 0; slot.seg_off = 0; slot.col_off = 0;
+    slot.nxt = nxt;
+    slot.R = std::min(mark_max_rows(), g.cy);
+    slot.nrb = (g.cy + slot.R - 1) / slot.R;
+    slot.KZ = (int)std::max(8LL, std::min(64LL, ((long long)g.cz * nxt * slot.nrb + (long long)sms * 12 - 1) / ((long long)sms * 12)));
+    slot.nzc = (g.cz + slot.KZ - 1) / slot.KZ;
+    const uintptr_t vaddr = reinterpret_cast<uintptr_t>(g.v);
+    slot.vec4 = (g.nx % 4 == 0 && (vaddr % 16) == 0) ? 1 : 0;
+    const long long ntiles = (long long)nxt * slot.nrb * slot.nzc;
+    if (ntiles > 0x7fffffffLL) return DCB_ERR_TOO_LARGE;
+    Table ht;
+    std::memset(&ht, 0, sizeof(ht));
+    ht.slot = slot;
+    ht.seg_off[1] = nseg;
+    ht.tile_off[1] = ntiles;
+
+    // Scratch layout, each part 256-byte aligned: table | total | bits | super | seg_count |
     // seg_start | scan partials. Grids that need more than the array are rejected.
-    const size_t off_total = 0;
+    const size_t off_table = 0;
+    const size_t off_total = align256(off_table + sizeof(Table));
     const size_t off_bits = align256(off_total + sizeof(unsigned long long));
     const size_t off_super = align256(off_bits + sizeof(uint32_t) * (size_t)rows * g.W);
     const size_t off_count = align256(off_super + sizeof(uint32_t) * (size_t)rows * g.W8);
@@ -98,24 +132,21 @@ extern "C" int dcb_mark_active_cells_noalloc(const dcb_grid* grid, int64_t* cell
     if (scratch_address(device, &base) != cudaSuccess) { cudaGetLastError(); return DCB_ERR_CUDA; }
     unsigned char* sb = static_cast<unsigned char*>(base);
     unsigned long long* total = reinterpret_cast<unsigned long long*>(sb + off_total);
+    Table* dt = reinterpret_cast<Table*>(sb + off_table);
 
-    // The array keeps the previous call's contents: clear the counter this call reads.
+    // The array keeps the previous call's contents: write this call's table (a one-thread
+    // kernel takes it by value) and clear the counter this call reads.
+    k_store_table<<<1, 1, 0, s>>>(dt, ht);
+    if (cudaGetLastError() != cudaSuccess) return DCB_ERR_CUDA;
     if (cudaMemsetAsync(total, 0, sizeof(unsigned long long), s) != cudaSuccess) { cudaGetLastError(); return DCB_ERR_CUDA; }
 
-    int sms = 148;
-    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) { cudaGetLastError(); return DCB_ERR_CUDA; }
+    BatchTable B;
+    B.s0 = slot; B.slots = &dt->slot; B.n = 1; B.seg_off = dt->seg_off; B.col_off = dt->col_off; B.vert_off = dt->vert_off;
     MarkParams mp;
-    mp.g = g;
-    mp.R = std::min(mark_max_rows(), g.cy);
-    const long long nrb = (g.cy + mp.R - 1) / mp.R;
-    mp.KZ = (int)std::max(8LL, std::min(64LL, (g.cz * nxt * nrb + (long long)sms * 12 - 1) / ((long long)sms * 12)));
-    mp.nxt = nxt;
+    mp.B = B; mp.tile_slot = dt->tile_slot; mp.tile_off = dt->tile_off; mp.m = 1; mp.ntiles = ntiles;
     mp.bits = reinterpret_cast<uint32_t*>(sb + off_bits);
     mp.seg_count = reinterpret_cast<uint32_t*>(sb + off_count);
-    const uintptr_t vaddr = reinterpret_cast<uintptr_t>(g.v);
-    mp.vec4 = (g.nx % 4 == 0 && (vaddr % 16) == 0) ? 1 : 0;
-    if (nrb > 65535 || (g.cz + mp.KZ - 1) / mp.KZ > 65535) return DCB_ERR_TOO_LARGE;
-    if (launch_mark(mp, s) != cudaSuccess) { cudaGetLastError(); return DCB_ERR_CUDA; }
+    if (launch_mark(mp, slot.vec4, s) != cudaSuccess) { cudaGetLastError(); return DCB_ERR_CUDA; }
     uint32_t* seg_start = reinterpret_cast<uint32_t*>(sb + off_start);
     if (launch_scan(mp.seg_count, nseg, reinterpret_cast<uint32_t*>(sb + off_part), seg_start, total, s) != cudaSuccess) {
         cudaGetLastError();
@@ -132,7 +163,7 @@ extern "C" int dcb_mark_active_cells_noalloc(const dcb_grid* grid, int64_t* cell
     if (n == 0) return DCB_OK;
 
     ExpandParams xp;
-    xp.g = g; xp.nxt = nxt; xp.bits = mp.bits; xp.seg_count = mp.seg_count; xp.seg_start = seg_start;
+    xp.B = B; xp.nseg = nseg; xp.bits = mp.bits; xp.seg_count = mp.seg_count; xp.seg_start = seg_start;
     xp.super = reinterpret_cast<uint32_t*>(sb + off_super);
     xp.list = reinterpret_cast<uint64_t*>(cells);
     if (launch_expand(xp, sms, s) != cudaSuccess) { cudaGetLastError(); return DCB_ERR_CUDA; }

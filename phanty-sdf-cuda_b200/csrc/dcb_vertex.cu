@@ -230,9 +230,8 @@ __device__ float3 edge_normal(const GridDesc& g, int3 lo, int axis, int o1, int 
 }
 
 // Local -> world: one double combination per axis, one float rounding.
-__device__ __forceinline__ void store_vertex(const QefParams& P, long long r, int i, int j, int k,
+__device__ __forceinline__ void store_vertex(const QefParams& P, const GridDesc& g, long long r, int i, int j, int k,
                                              float Lx, float Ly, float Lz) {
-    const GridDesc& g = P.g;
     const float wx1 = width_axis(g, 0, i), wy1 = width_axis(g, 1, j), wz1 = width_axis(g, 2, k);
     P.V[3 * r + 0] = (float)((double)pos_axis(g.ox, g.vx, i) + (double)wx1 * (double)Lx);
     P.V[3 * r + 1] = (float)((double)pos_axis(g.oy, g.vy, j) + (double)wy1 * (double)Ly);
@@ -241,18 +240,21 @@ __device__ __forceinline__ void store_vertex(const QefParams& P, long long r, in
 
 // ---- k_cell_qef -------------------------------------------------------------------------
 
+template <bool ONE>
 __global__ void __launch_bounds__(128)
-k_cell_qef(QefParams P) {
-    const GridDesc& g = P.g;
+k_cell_qef(const __grid_constant__ QefParams P) {
     __shared__ unsigned int s_hist;
     __shared__ float s_c[8][128];    // per-thread corner values (dynamically indexed)
     __shared__ float s_t[12][128];   // per-thread lerp parameter of each crossing edge
     const int tid = threadIdx.x;
     if (tid == 0) s_hist = 0;
     __syncthreads();
-    const long long cxcy = (long long)g.cx * g.cy;
     for (long long r = (long long)blockIdx.x * blockDim.x + tid; r < P.nactive;
          r += (long long)gridDim.x * blockDim.x) {
+        const GridSlot& S = slot_ref<ONE>(P.B, ONE ? 0 : slot_of_rank(P.B, (unsigned long long)r));
+        const GridDesc& g = S.g;
+        const long long cxcy = (long long)g.cx * g.cy;
+        uint32_t* const col_count = P.col_count + S.col_off;
         int i, j, k;
         unpack_cell(P.list[r], i, j, k);
         float c[8];
@@ -264,13 +266,13 @@ k_cell_qef(QefParams P) {
         // Faces owned by this cell: its min-corner X, Y, Z edges (contouring.cpp:609-729).
         uint8_t fm = 0;
         if (j >= 1 && k >= 1 && strict_change(c[0], c[1])) {
-            fm |= 1; atomicAdd(&P.col_count[0 * cxcy + (long long)i * g.cy + j], 1u);
+            fm |= 1; atomicAdd(&col_count[0 * cxcy + (long long)i * g.cy + j], 1u);
         }
         if (i >= 1 && k >= 1 && strict_change(c[0], c[3])) {
-            fm |= 2; atomicAdd(&P.col_count[1 * cxcy + (long long)i * g.cy + j], 1u);
+            fm |= 2; atomicAdd(&col_count[1 * cxcy + (long long)i * g.cy + j], 1u);
         }
         if (i >= 1 && j >= 1 && strict_change(c[0], c[4])) {
-            fm |= 4; atomicAdd(&P.col_count[2 * cxcy + (long long)i * g.cy + j], 1u);
+            fm |= 4; atomicAdd(&col_count[2 * cxcy + (long long)i * g.cy + j], 1u);
         }
         P.fmask[r] = fm;
 
@@ -330,7 +332,7 @@ k_cell_qef(QefParams P) {
             // FP32 cannot be trusted: the FP64 path recomputes this cell from the grid.
             const unsigned int slot = atomicAdd(P.esc_count, 1u);
             P.esc_list[slot] = (uint32_t)r;
-            store_vertex(P, r, i, j, k, cu, cv, cw);
+            store_vertex(P, g, r, i, j, k, cu, cv, cw);
             continue;
         }
         // Rank-1 certificate: lambda1 by power iteration, lambda2 + lambda3 = trace - lambda1.
@@ -354,7 +356,7 @@ k_cell_qef(QefParams P) {
         // certified rank 1 with lambda2/lambda1 < 0.01: four power steps converge to ~1e-8
         if (lam1 > thr * (1.f + P.band) && rest < thr * (1.f - P.band) && rest < 0.01f * lam1) {
             const float proj = (x0 * R0 + x1 * R1 + x2 * R2) / lam1;
-            store_vertex(P, r, i, j, k, cu + x0 * proj, cv + x1 * proj / fy, cw + x2 * proj / fz);
+            store_vertex(P, g, r, i, j, k, cu + x0 * proj, cv + x1 * proj / fy, cw + x2 * proj / fz);
             P.vclass[r] = kVcRank1;
             atomicAdd(&s_hist, 1u);
         } else {
@@ -374,7 +376,8 @@ cudaError_t launch_cell_qef(const QefParams& P, int num_sms, cudaStream_t s) {
     long long blocks = (P.nactive + 127) / 128;
     const long long cap = (long long)num_sms * 32;
     if (blocks > cap) blocks = cap;
-    k_cell_qef<<<(unsigned)blocks, 128, 0, s>>>(P);
+    if (P.B.n == 1) k_cell_qef<true><<<(unsigned)blocks, 128, 0, s>>>(P);
+    else            k_cell_qef<false><<<(unsigned)blocks, 128, 0, s>>>(P);
     return cudaGetLastError();
 }
 
@@ -457,9 +460,9 @@ k_cell_jacobi(QefParams P) {
             const unsigned int slot = atomicAdd(P.esc_count, 1u);
             P.esc_list[slot] = r;
         }
-        const GridDesc& g = P.g;
+        const GridDesc g = P.B.slots[slot_of_rank(P.B, r)].g;
         const float wx1 = width_axis(g, 0, i), wy1 = width_axis(g, 1, j), wz1 = width_axis(g, 2, k);
-        store_vertex(P, r, i, j, k, d2.y + wx, d2.z + wy * (wx1 / wy1), d2.w + wz * (wx1 / wz1));
+        store_vertex(P, g, r, i, j, k, d2.y + wx, d2.z + wy * (wx1 / wy1), d2.w + wz * (wx1 / wz1));
         P.vclass[r] = kVcJacobi;
     }
     __syncthreads();

@@ -332,8 +332,9 @@ k_vertex_fp64(Vertex64Params P) {
         const uint32_t r = P.cells[t];
         int i, j, k;
         unpack_cell(P.list[r], i, j, k);
+        const GridDesc g = P.B.slots[slot_of_rank(P.B, r)].g;
         double x[3];
-        f64::cell_vertex_warp(P.g, i, j, k, P.thr, x);
+        f64::cell_vertex_warp(g, i, j, k, P.thr, x);
         if (lane == 0) {
             if (P.Vf) {
                 P.Vf[3 * (size_t)r + 0] = (float)x[0];
@@ -367,7 +368,8 @@ k_winding_fp64(Winding64Params P) {
     const unsigned int n = min(*P.count, P.cap);
     for (unsigned int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
         const uint4 it = P.items[t];
-        const int axis = (int)it.y;
+        const int axis = (int)(it.y & 3u);
+        const GridDesc g = P.B.slots[it.y >> 2].g;
         int i, j, k;
         unpack_cell(((uint64_t)it.w << 32) | it.z, i, j, k);
         const int4 q4 = P.quads[it.x];
@@ -381,8 +383,8 @@ k_winding_fp64(Winding64Params P) {
         }
         if (!ok) { set_error(P.err, kErrInternal); continue; }
         double g0[3], g1[3];
-        f64::grid_gradient(P.g, i, j, k, g0);
-        f64::grid_gradient(P.g, i + (axis == 0), j + (axis == 1), k + (axis == 2), g1);
+        f64::grid_gradient(g, i, j, k, g0);
+        f64::grid_gradient(g, i + (axis == 0), j + (axis == 1), k + (axis == 2), g1);
         const double gn[3] = {g0[0] + g1[0], g0[1] + g1[1], g0[2] + g1[2]};
         const double ba[3] = {pv[1][0] - pv[0][0], pv[1][1] - pv[0][1], pv[1][2] - pv[0][2]};
         const double da[3] = {pv[3][0] - pv[0][0], pv[3][1] - pv[0][1], pv[3][2] - pv[0][2]};

@@ -60,7 +60,7 @@ def test_struct_layouts_match_the_header():
     from contouring_b200 import _lib
     structs = {"dcb_grid": _lib.DcbGrid, "dcb_opts": _lib.DcbOpts, "dcb_stats": _lib.DcbStats,
                "dcb_mesh_dev": _lib.DcbMeshDev, "dcb_mesh_host": _lib.DcbMeshHost,
-               "dcb_sdf_stats": _lib.DcbSdfStats}
+               "dcb_sdf_stats": _lib.DcbSdfStats, "dcb_batch_mesh": _lib.DcbBatchMesh}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "dcb.h"', "int main(void) {"]
     for cname, py in structs.items():
         lines.append('printf("%s %%zu\\n", sizeof(%s));' % (cname, cname))
