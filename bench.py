@@ -213,16 +213,18 @@ def run_batch_workload(args):
     def sequential():
         for v, d, sp, o in grids:
             be.extract_tensor_ptr(DenseSdfGridDevice(*d, *sp, *o, d_values=v))
-    for _ in range(max(1, args.warmup // 2)):
-        sequential()
-    torch.cuda.synchronize()
-    e0.record(stream)
-    reps = max(1, args.steps // 4)
-    for _ in range(reps):
-        sequential()
-    e1.record(stream)
-    torch.cuda.synchronize()
-    ms_seq = e0.elapsed_time(e1) / reps
+    ms_seq = None
+    if not args.no_sequential:
+        for _ in range(max(1, args.warmup // 2)):
+            sequential()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        reps = max(1, args.steps // 4)
+        for _ in range(reps):
+            sequential()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms_seq = e0.elapsed_time(e1) / reps
     line = {
         "metric": "dc_extract_mcells_per_s", "value": round(ncell / (ms_batch / 1e3) / 1e6, 2), "unit": "Mcells/s",
         "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_batch, 4),
@@ -231,7 +233,9 @@ def run_batch_workload(args):
                    "resolutions": [32, 48, 64, 96, 128, 192], "vertices": st.vertex_count, "quads": st.face_count},
         "stage_ms": {"mark": round(st.marking_ms, 4), "scan": round(st.compaction_ms, 4),
                      "qef": round(st.qef_ms, 4), "faces": round(st.face_emission_ms, 4)},
-        "sequential_plain_ms": round(ms_seq, 3), "batched_speedup": round(ms_seq / ms_batch, 2),
+        "escalated_fp64_cells": st.escalated_fp64_cells, "winding_fp64_faces": st.winding_fp64_faces,
+        "sequential_plain_ms": round(ms_seq, 3) if ms_seq else None,
+        "batched_speedup": round(ms_seq / ms_batch, 2) if ms_seq else None,
     }
     print(json.dumps(line), flush=True)
     be.close()
@@ -248,6 +252,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--ref-zslab", type=int, default=96, help="point planes per CPU sample (over 8 slabs)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-sequential", action="store_true", help="batch256: skip the one-by-one comparison")
     ap.add_argument("--workload", default="csg1024", choices=["csg1024", "batch256"],
                     help="batch256: 256 uneven CSG grids batched vs one by one (not the headline)")
     args = ap.parse_args()

@@ -70,7 +70,7 @@ struct dcb_context {
     int mark_ctas[2] = {0, 0};        // resident mark CTAs per SM (scalar, float4 loads)
     int cx = 0, cy = 0;
     // batch layout table (device + pinned staging) and the last batch's per-grid offsets
-    DevBuf table;
+    DevBuf table, cell_slot;
     void* h_table = nullptr; size_t h_table_bytes = 0;
     void* h_offsets = nullptr; size_t h_offsets_bytes = 0;
     int batch_n = 1;
@@ -150,8 +150,9 @@ float elapsed(cudaEvent_t a, cudaEvent_t b) {
 struct BatchLayout {
     std::vector<GridSlot> slots;
     std::vector<long long> seg_off, col_off;          // n + 1
-    std::vector<int> tile_slot[2];                    // grids of the scalar / float4 mark launch
-    std::vector<long long> tile_off[2];               // their first tiles (+ total)
+    // mark launches: index vec4 + 2 * narrow (scalar/float4 loads x 1024/256-cell tiles)
+    std::vector<int> tile_slot[4];                    // grids of each mark launch
+    std::vector<long long> tile_off[4];               // their first tiles (+ total)
     long long bits = 0, super = 0, nseg = 0, ncol = 0, ncell = 0;
     float hmax = 0.f;
 };
@@ -160,8 +161,7 @@ int layout_batch(dcb_context* h, const dcb_grid* in, int n, BatchLayout& L) {
     L.slots.resize(n);
     L.seg_off.assign(n + 1, 0);
     L.col_off.assign(n + 1, 0);
-    for (int v = 0; v < 2; ++v) { L.tile_slot[v].clear(); L.tile_off[v].assign(1, 0); }
-    const int tile_cells = 32 * mark_tile_words();
+    for (int v = 0; v < 4; ++v) { L.tile_slot[v].clear(); L.tile_off[v].assign(1, 0); }
     for (int b = 0; b < n; ++b) {
         GridSlot& S = L.slots[b];
         GridDesc& g = S.g;
@@ -174,7 +174,9 @@ int layout_batch(dcb_context* h, const dcb_grid* in, int n, BatchLayout& L) {
         g.v = in[b].values;
         const long long rows = (long long)g.cy * g.cz;
         S.vec4 = (g.nx % 4 == 0 && (reinterpret_cast<uintptr_t>(g.v) % 16) == 0) ? 1 : 0;
-        S.nxt = (g.cx + tile_cells - 1) / tile_cells;
+        // grids at most 256 cells wide march 256-cell x-tiles (less idle width)
+        S.tw = g.cx <= 32 * mark_narrow_tile_words() ? mark_narrow_tile_words() : mark_tile_words();
+        S.nxt = (g.cx + 32 * S.tw - 1) / (32 * S.tw);
         S.R = std::min(mark_max_rows(), g.cy);
         S.nrb = (g.cy + S.R - 1) / S.R;
         // About four CTAs per resident slot, each marching 8..64 planes (a single long wave
@@ -194,13 +196,15 @@ int layout_batch(dcb_context* h, const dcb_grid* in, int n, BatchLayout& L) {
         L.nseg += rows * S.nxt;
         L.ncol += 3LL * g.cx * g.cy;
         L.ncell += (long long)g.cx * rows;
-        L.tile_slot[S.vec4].push_back(b);
-        L.tile_off[S.vec4].push_back(L.tile_off[S.vec4].back() + (long long)S.nxt * S.nrb * S.nzc);
-        L.hmax = std::max(L.hmax, std::max(std::fabs(g.vx), std::max(std::fabs(g.vy), std::fabs(g.vz))));
+        const int grp = S.vec4 + 2 * (S.tw == mark_narrow_tile_words() ? 1 : 0);
+        L.tile_slot[grp].push_back(b);
+        L.tile_off[grp].push_back(L.tile_off[grp].back() + (long long)S.nxt * S.nrb * S.nzc);
+        S.hmax = std::max(std::fabs(g.vx), std::max(std::fabs(g.vy), std::fabs(g.vz)));
+        L.hmax = std::max(L.hmax, S.hmax);
     }
     L.seg_off[n] = L.nseg;
     L.col_off[n] = L.ncol;
-    for (int v = 0; v < 2; ++v)
+    for (int v = 0; v < 4; ++v)
         if (L.tile_off[v].back() > 0x7fffffffLL) return fail(h, DCB_ERR_TOO_LARGE, "grid too large for the tiling");
     if (L.nseg >= 0xffffffffLL || L.ncol >= 0xffffffffLL) return fail(h, DCB_ERR_TOO_LARGE, "batch too large");
     return DCB_OK;
@@ -211,8 +215,8 @@ struct TableView {
     BatchTable B;
     unsigned long long* vert_off;
     unsigned long long* face_off;
-    const int* tile_slot[2];
-    const long long* tile_off[2];
+    const int* tile_slot[4];
+    const long long* tile_off[4];
 };
 
 size_t align_up(size_t x) { return (x + 255) & ~size_t(255); }
@@ -224,21 +228,21 @@ int upload_table(dcb_context* h, const BatchLayout& L, cudaStream_t s, TableView
     const size_t o_col = align_up(o_seg + sizeof(long long) * (n + 1));
     const size_t o_vert = align_up(o_col + sizeof(long long) * (n + 1));
     const size_t o_face = align_up(o_vert + sizeof(unsigned long long) * (n + 1));
-    const size_t o_ts0 = align_up(o_face + sizeof(unsigned long long) * (n + 1));
-    const size_t o_ts1 = align_up(o_ts0 + sizeof(int) * L.tile_slot[0].size() + 1);
-    const size_t o_to0 = align_up(o_ts1 + sizeof(int) * L.tile_slot[1].size() + 1);
-    const size_t o_to1 = align_up(o_to0 + sizeof(long long) * L.tile_off[0].size());
-    const size_t total = align_up(o_to1 + sizeof(long long) * L.tile_off[1].size());
+    size_t o_ts[4], o_to[4];
+    size_t at = align_up(o_face + sizeof(unsigned long long) * (n + 1));
+    for (int v = 0; v < 4; ++v) { o_ts[v] = at; at = align_up(at + sizeof(int) * L.tile_slot[v].size() + 1); }
+    for (int v = 0; v < 4; ++v) { o_to[v] = at; at = align_up(at + sizeof(long long) * L.tile_off[v].size()); }
+    const size_t total = at;
     DCB_TRY(h, ensure(h->table, total), "alloc batch table");
     DCB_TRY(h, ensure_host(h->h_table, h->h_table_bytes, total), "alloc pinned batch table");
     char* hb = reinterpret_cast<char*>(h->h_table);
     std::memcpy(hb + o_slots, L.slots.data(), sizeof(GridSlot) * n);
     std::memcpy(hb + o_seg, L.seg_off.data(), sizeof(long long) * (n + 1));
     std::memcpy(hb + o_col, L.col_off.data(), sizeof(long long) * (n + 1));
-    std::memcpy(hb + o_ts0, L.tile_slot[0].data(), sizeof(int) * L.tile_slot[0].size());
-    std::memcpy(hb + o_ts1, L.tile_slot[1].data(), sizeof(int) * L.tile_slot[1].size());
-    std::memcpy(hb + o_to0, L.tile_off[0].data(), sizeof(long long) * L.tile_off[0].size());
-    std::memcpy(hb + o_to1, L.tile_off[1].data(), sizeof(long long) * L.tile_off[1].size());
+    for (int v = 0; v < 4; ++v) {
+        std::memcpy(hb + o_ts[v], L.tile_slot[v].data(), sizeof(int) * L.tile_slot[v].size());
+        std::memcpy(hb + o_to[v], L.tile_off[v].data(), sizeof(long long) * L.tile_off[v].size());
+    }
     DCB_TRY(h, cudaMemcpyAsync(h->table.p, hb, total, cudaMemcpyHostToDevice, s), "upload batch table");
     char* db = reinterpret_cast<char*>(h->table.p);
     T.B.s0 = L.slots[0];
@@ -249,10 +253,11 @@ int upload_table(dcb_context* h, const BatchLayout& L, cudaStream_t s, TableView
     T.vert_off = reinterpret_cast<unsigned long long*>(db + o_vert);
     T.face_off = reinterpret_cast<unsigned long long*>(db + o_face);
     T.B.vert_off = T.vert_off;
-    T.tile_slot[0] = reinterpret_cast<const int*>(db + o_ts0);
-    T.tile_slot[1] = reinterpret_cast<const int*>(db + o_ts1);
-    T.tile_off[0] = reinterpret_cast<const long long*>(db + o_to0);
-    T.tile_off[1] = reinterpret_cast<const long long*>(db + o_to1);
+    T.B.cell_slot = nullptr;
+    for (int v = 0; v < 4; ++v) {
+        T.tile_slot[v] = reinterpret_cast<const int*>(db + o_ts[v]);
+        T.tile_off[v] = reinterpret_cast<const long long*>(db + o_to[v]);
+    }
     return DCB_OK;
 }
 
@@ -288,13 +293,13 @@ int run_batch(dcb_context* h, const dcb_grid* in, int n, const dcb_opts* o, cuda
 
     // 1) mark: active bits + per-segment counts; scan -> segment starts and the total.
     DCB_TRY(h, cudaMemsetAsync(h->counters.p, 0, sizeof(Counters), s), "memset counters");
-    for (int v = 0; v < 2; ++v) {
+    for (int v = 0; v < 4; ++v) {
         if (L.tile_slot[v].empty()) continue;
         MarkParams mp;
         mp.B = T.B; mp.tile_slot = T.tile_slot[v]; mp.tile_off = T.tile_off[v];
         mp.m = (int)L.tile_slot[v].size(); mp.ntiles = L.tile_off[v].back();
         mp.bits = as<uint32_t>(h->bits); mp.seg_count = as<uint32_t>(h->seg_count);
-        DCB_TRY(h, launch_mark(mp, v, s), "launch mark");
+        DCB_TRY(h, launch_mark(mp, v & 1, (v & 2) ? mark_narrow_tile_words() : mark_tile_words(), s), "launch mark");
     }
     DCB_TRY(h, cudaEventRecord(h->ev[6], s), "event");
     DCB_TRY(h, launch_scan(as<uint32_t>(h->seg_count), nseg, as<uint32_t>(h->partials), as<uint32_t>(h->seg_start),
@@ -340,6 +345,10 @@ int run_batch(dcb_context* h, const dcb_grid* in, int n, const dcb_opts* o, cuda
     DCB_TRY(h, ensure(h->stage_key, sizeof(uint2) * 3 * nv), "alloc face keys");
     DCB_TRY(h, ensure(h->faces, sizeof(int4) * 3 * nv), "alloc faces");
     DCB_TRY(h, ensure(h->v64_index, sizeof(int) * nv), "alloc fp64 index");
+    if (n > 1) {
+        DCB_TRY(h, ensure(h->cell_slot, sizeof(uint32_t) * nv), "alloc vertex grids");
+        T.B.cell_slot = as<uint32_t>(h->cell_slot);
+    }
     // Exact upper bounds: at most 3 faces per owner cell, one FP64 vertex per cell.
     const long long wind_cap = std::min(0x7fffffffLL, 3 * nv);
     const long long v64_cap = nv;
@@ -354,6 +363,8 @@ int run_batch(dcb_context* h, const dcb_grid* in, int n, const dcb_opts* o, cuda
     ExpandParams xp;
     xp.B = T.B; xp.nseg = nseg; xp.bits = as<uint32_t>(h->bits); xp.seg_count = as<uint32_t>(h->seg_count);
     xp.seg_start = as<uint32_t>(h->seg_start); xp.super = as<uint32_t>(h->super); xp.list = as<uint64_t>(h->list);
+    xp.cell_slot = n > 1 ? as<uint32_t>(h->cell_slot) : nullptr;
+    xp.B.cell_slot = nullptr;                      // expand finds grids by segment
     DCB_TRY(h, launch_expand(xp, h->num_sms, s), "launch expand");
     QefParams qp;
     qp.B = T.B; qp.list = xp.list; qp.nactive = nv; qp.V = as<float>(h->V); qp.vclass = as<uint8_t>(h->vclass);
@@ -405,6 +416,7 @@ int run_batch(dcb_context* h, const dcb_grid* in, int n, const dcb_opts* o, cuda
         DCB_TRY(h, ensure(h->tris, sizeof(int) * 6 * 3 * nv), "alloc triangles");
         DCB_TRY(h, ensure(h->tri_items, sizeof(uint32_t) * wind_cap), "alloc triangle list");
         TriParams tp;
+        tp.B = T.B;
         tp.quads = as<int4>(h->faces); tp.nquads = &dc->face_total; tp.V = qp.V; tp.vclass = qp.vclass;
         tp.hmax = fp.hmax; tp.tris = as<int>(h->tris); tp.items = as<uint32_t>(h->tri_items);
         tp.item_count = &dc->tri_count; tp.item_cap = (unsigned int)wind_cap;
@@ -631,7 +643,7 @@ int dcb_destroy(dcb_handle h) {
                       &h->tris, &h->tri_items, &h->m_verts, &h->m_faces, &h->m_out, &h->m_tris,
                       &h->m_bin_count, &h->m_bin_start, &h->m_bin_fill, &h->m_bin_scratch, &h->m_bin_tris,
                       &h->m_bin_active, &h->m_active_list, &h->m_axis_start, &h->m_far, &h->m_ext, &h->m_tmp,
-                      &h->m_partials, &h->m_counters, &h->table};
+                      &h->m_partials, &h->m_counters, &h->table, &h->cell_slot};
     for (DevBuf* b : bufs) if (b->p) cudaFree(b->p);
     if (h->h_counters) cudaFreeHost(h->h_counters);
     if (h->h_sdf_counters) cudaFreeHost(h->h_sdf_counters);

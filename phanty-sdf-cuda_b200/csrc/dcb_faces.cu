@@ -197,7 +197,7 @@ k_face_scatter(const __grid_constant__ FaceParams P) {
             const float3 g1 = grid_gradient32(g, i + (axis == 0), j + (axis == 1), k + (axis == 2));
             const float3 gn = make_float3(g0.x + g1.x, g0.y + g1.y, g0.z + g1.z);
             const float3 pa = ldv(P.V, r0), pb = ldv(P.V, r1), pc = ldv(P.V, r2), pd = ldv(P.V, r3);
-            const float dv = quad_vertex_bound(P.vclass, r0, r1, r2, r3, pa, pb, pc, pd, P.hmax);
+            const float dv = quad_vertex_bound(P.vclass, r0, r1, r2, r3, pa, pb, pc, pd, S.hmax);
             const float3 ba = sub3(pb, pa), da = sub3(pd, pa), ca = sub3(pc, pa);
             float3 qn = cross3(ba, da);
             float qn2 = dot3(qn, qn);
@@ -336,7 +336,9 @@ k_triangulate(TriParams P) {
         const int4 q = P.quads[f];
         const uint32_t a = (uint32_t)q.x, b = (uint32_t)q.y, c = (uint32_t)q.z, d = (uint32_t)q.w;
         const float3 pa = ldv(P.V, a), pb = ldv(P.V, b), pc = ldv(P.V, c), pd = ldv(P.V, d);
-        const float dv = quad_vertex_bound(P.vclass, a, b, c, d, pa, pb, pc, pd, P.hmax);
+        // the quad's grid (its first vertex's) gives the cell width of the bound
+        const float hmax = P.B.n == 1 ? P.B.s0.hmax : (P.B.cell_slot ? P.B.slots[P.B.cell_slot[a]].hmax : P.hmax);
+        const float dv = quad_vertex_bound(P.vclass, a, b, c, d, pa, pb, pc, pd, hmax);
         const float3 ba = sub3(pb, pa), ca = sub3(pc, pa), da = sub3(pd, pa);
         const float lb = sqrtf(dot3(ba, ba)), lc = sqrtf(dot3(ca, ca)), ld = sqrtf(dot3(da, da));
         float3 qn = cross3(ba, da);

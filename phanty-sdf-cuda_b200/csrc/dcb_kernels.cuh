@@ -21,6 +21,8 @@ struct GridSlot {
     int nrb;                       // mark: row blocks
     int nzc;                       // mark: z-chunks
     int vec4;                      // rows are 16-byte aligned and nx % 4 == 0
+    int tw;                        // mark: cell words per x-tile (32, or 8 for narrow grids)
+    float hmax;                    // largest cell width of the grid (world units)
 };
 
 struct BatchTable {
@@ -30,6 +32,7 @@ struct BatchTable {
     const long long* seg_off;              // [n+1] first segment per grid
     const long long* col_off;              // [n+1] first face column per grid
     const unsigned long long* vert_off;    // [n+1] first vertex rank per grid (after the scan)
+    const uint32_t* cell_slot;             // [active] grid of every vertex rank (n > 1, after expand)
 };
 
 // Largest index b in [0, n) with offs[b] <= x (offsets ascending, offs[0] = 0).
@@ -49,7 +52,8 @@ __device__ __forceinline__ const GridSlot& slot_ref(const BatchTable& B, int gi)
     return ONE ? B.s0 : B.slots[gi];
 }
 __device__ __forceinline__ int slot_of_rank(const BatchTable& B, unsigned long long r) {
-    return B.n == 1 ? 0 : slot_search(B.vert_off, B.n, r);
+    if (B.n == 1) return 0;
+    return B.cell_slot ? (int)__ldg(B.cell_slot + r) : slot_search(B.vert_off, B.n, r);
 }
 __device__ __forceinline__ int slot_of_segment(const BatchTable& B, long long s) {
     return B.n == 1 ? 0 : slot_search(B.seg_off, B.n, s);
@@ -60,15 +64,16 @@ __device__ __forceinline__ int slot_of_column(const BatchTable& B, long long c) 
 
 struct MarkParams {
     BatchTable B;
-    const int* tile_slot;          // [m] the grids of this launch (all share the load path)
+    const int* tile_slot;          // [m] the grids of this launch (all share load path and tile width)
     const long long* tile_off;     // [m+1] first tile of each of them
     int m;
     long long ntiles;
     uint32_t* bits;                // all grids' active bits
     uint32_t* seg_count;           // all grids' segment counts
 };
-cudaError_t launch_mark(const MarkParams& P, int vec4, cudaStream_t s);
+cudaError_t launch_mark(const MarkParams& P, int vec4, int tw, cudaStream_t s);
 int mark_tile_words();
+int mark_narrow_tile_words();
 int mark_ctas_per_sm(int vec4);   // resident CTAs of the mark kernel per SM
 int mark_max_rows();
 
@@ -80,6 +85,7 @@ struct ExpandParams {
     const uint32_t* seg_start;     // exclusive scan of seg_count (global ranks)
     uint32_t* super;               // all grids' super ranks
     uint64_t* list;                // [active] packed cells, grid-local coordinates
+    uint32_t* cell_slot;           // [active] grid of every vertex (batches only; may be null)
 };
 cudaError_t launch_expand(const ExpandParams& P, int num_sms, cudaStream_t s);
 
@@ -170,7 +176,7 @@ struct FaceParams {
     unsigned int* v64_count;
     unsigned long long v64_cap;
     int* err;
-    float hmax;                    // largest cell width of the batch (world units)
+    float hmax;                    // unused: each grid's slot holds its own cell width
 };
 cudaError_t launch_face_scatter(const FaceParams& P, int num_sms, cudaStream_t s);
 cudaError_t launch_face_order(const int4* stage_quad, const uint2* stage_key, const uint32_t* col_start,
@@ -178,11 +184,12 @@ cudaError_t launch_face_order(const int4* stage_quad, const uint2* stage_key, co
                               long long max_faces, int num_sms, cudaStream_t s);
 
 struct TriParams {
+    BatchTable B;
     const int4* quads;             // final quads
     const unsigned long long* nquads;
     const float* V;
     const uint8_t* vclass;
-    float hmax;
+    float hmax;                    // largest cell width of the batch (when grids are unknown)
     int* tris;                     // 2 triangles (6 ints) per quad
     uint32_t* items;               // quads whose orientation FP32 cannot settle
     unsigned int* item_count;

@@ -22,20 +22,25 @@ namespace dcb {
 
 constexpr int kMarkWarps = 8;          // point rows per tile (R + 1 <= 8)
 constexpr int kTileWords = 32;         // cell words per x-tile (1024 cells)
-constexpr int kPtWords = kTileWords + 1;
-constexpr int kChunks = (kPtWords + 3) / 4;   // 128-point chunks per point-row segment
+constexpr int kNarrowTileWords = 8;    // x-tile of grids at most 256 cells wide
+// TW cell words per x-tile: TW + 1 point words, loaded as 128-point chunks.
+template <int TW> struct Tile {
+    static constexpr int kPtWords = TW + 1;
+    static constexpr int kChunks = (kPtWords + 3) / 4;
+};
 
+template <int TW>
 struct RowRegs {
-    float4 v[kChunks];
+    float4 v[Tile<TW>::kChunks];
 };
 
 // Load the kPtWords*32 points of one point-row segment starting at x0 into registers.
 // VEC4: lane l holds points x0+128c+4l..+3 of chunk c; scalar: component q holds point
 // x0+128c+32q+l.
-template <bool VEC4>
-__device__ __forceinline__ void load_row(const float* __restrict__ row, int x0, int nx, int lane, RowRegs& R) {
+template <bool VEC4, int TW>
+__device__ __forceinline__ void load_row(const float* __restrict__ row, int x0, int nx, int lane, RowRegs<TW>& R) {
 #pragma unroll
-    for (int c = 0; c < kChunks; ++c) {
+    for (int c = 0; c < Tile<TW>::kChunks; ++c) {
         float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
         if (VEC4) {
             const int x = x0 + 128 * c + 4 * lane;
@@ -52,10 +57,11 @@ __device__ __forceinline__ void load_row(const float* __restrict__ row, int x0, 
 }
 
 // Negative / positive bit words of the loaded segment (word q covers points x0+32q..+31).
-template <bool VEC4>
-__device__ __forceinline__ void row_words(const RowRegs& R, int lane, uint32_t* nw, uint32_t* pw) {
+template <bool VEC4, int TW>
+__device__ __forceinline__ void row_words(const RowRegs<TW>& R, int lane, uint32_t* nw, uint32_t* pw) {
+    constexpr int kPtWords = Tile<TW>::kPtWords;
 #pragma unroll
-    for (int c = 0; c < kChunks; ++c) {
+    for (int c = 0; c < Tile<TW>::kChunks; ++c) {
         const float4 v = R.v[c];
         if (VEC4) {
             uint32_t n = (v.x < 0.f ? 1u : 0u) | (v.y < 0.f ? 2u : 0u) | (v.z < 0.f ? 4u : 0u) | (v.w < 0.f ? 8u : 0u);
@@ -83,9 +89,10 @@ __device__ __forceinline__ void row_words(const RowRegs& R, int lane, uint32_t* 
     }
 }
 
-template <bool VEC4, bool ONE>
+template <bool VEC4, bool ONE, int TW>
 __global__ void __launch_bounds__(kMarkWarps * 32)
 k_mark_zmarch(const __grid_constant__ MarkParams P) {
+    constexpr int kPtWords = Tile<TW>::kPtWords;
     __shared__ uint32_t s_nw[2][kMarkWarps][kPtWords];
     __shared__ uint32_t s_pw[2][kMarkWarps][kPtWords];
     // tile -> grid of the batch -> (x-tile, row block, z-chunk), x-tile fastest
@@ -103,37 +110,39 @@ k_mark_zmarch(const __grid_constant__ MarkParams P) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int rows = min(R, g.cy - j0);
     const int ke = min(g.cz, kb + KZ);
-    const int x0 = xt * kTileWords * 32;       // first point / cell of the tile
+    const int x0 = xt * TW * 32;               // first point / cell of the tile
     const bool loader = warp <= rows;          // point rows j0..j0+rows
     const float* base = g.v + (int64_t)(j0 + (loader ? warp : 0)) * g.nx;
     const int64_t plane = (int64_t)g.nx * g.ny;
 
-    RowRegs cur;
+    RowRegs<TW> cur;
     if (loader) {
-        load_row<VEC4>(base + (int64_t)kb * plane, x0, g.nx, lane, cur);
-        row_words<VEC4>(cur, lane, s_nw[kb & 1][warp], s_pw[kb & 1][warp]);
-        load_row<VEC4>(base + (int64_t)(kb + 1) * plane, x0, g.nx, lane, cur);
+        load_row<VEC4, TW>(base + (int64_t)kb * plane, x0, g.nx, lane, cur);
+        row_words<VEC4, TW>(cur, lane, s_nw[kb & 1][warp], s_pw[kb & 1][warp]);
+        load_row<VEC4, TW>(base + (int64_t)(kb + 1) * plane, x0, g.nx, lane, cur);
     }
-    const int wglob = xt * kTileWords + lane;  // this lane's cell word in the row
+    const bool word_lane = TW == 32 || lane < TW;   // lanes beyond the tile's words idle
+    const int wglob = xt * TW + lane;          // this lane's cell word in the row
     const int valid = g.cx - 32 * wglob;
-    const uint32_t vmask = valid >= 32 ? 0xffffffffu : (valid > 0 ? ((1u << valid) - 1u) : 0u);
+    const uint32_t vmask = !word_lane ? 0u : valid >= 32 ? 0xffffffffu : (valid > 0 ? ((1u << valid) - 1u) : 0u);
+    const int wl = word_lane ? lane : 0;
 
     for (int k = kb; k < ke; ++k) {
         const int p1 = (k + 1) & 1, p0 = k & 1;
         if (loader) {
-            row_words<VEC4>(cur, lane, s_nw[p1][warp], s_pw[p1][warp]);
-            if (k + 2 <= ke) load_row<VEC4>(base + (int64_t)(k + 2) * plane, x0, g.nx, lane, cur);
+            row_words<VEC4, TW>(cur, lane, s_nw[p1][warp], s_pw[p1][warp]);
+            if (k + 2 <= ke) load_row<VEC4, TW>(base + (int64_t)(k + 2) * plane, x0, g.nx, lane, cur);
         }
         __syncthreads();
         if (warp < rows) {
             const int r = warp;
-            const uint32_t n0 = s_nw[p0][r][lane] | s_nw[p0][r + 1][lane] | s_nw[p1][r][lane] | s_nw[p1][r + 1][lane];
-            const uint32_t n1 = s_nw[p0][r][lane + 1] | s_nw[p0][r + 1][lane + 1] | s_nw[p1][r][lane + 1] | s_nw[p1][r + 1][lane + 1];
-            const uint32_t q0 = s_pw[p0][r][lane] | s_pw[p0][r + 1][lane] | s_pw[p1][r][lane] | s_pw[p1][r + 1][lane];
-            const uint32_t q1 = s_pw[p0][r][lane + 1] | s_pw[p0][r + 1][lane + 1] | s_pw[p1][r][lane + 1] | s_pw[p1][r + 1][lane + 1];
+            const uint32_t n0 = s_nw[p0][r][wl] | s_nw[p0][r + 1][wl] | s_nw[p1][r][wl] | s_nw[p1][r + 1][wl];
+            const uint32_t n1 = s_nw[p0][r][wl + 1] | s_nw[p0][r + 1][wl + 1] | s_nw[p1][r][wl + 1] | s_nw[p1][r + 1][wl + 1];
+            const uint32_t q0 = s_pw[p0][r][wl] | s_pw[p0][r + 1][wl] | s_pw[p1][r][wl] | s_pw[p1][r + 1][wl];
+            const uint32_t q1 = s_pw[p0][r][wl + 1] | s_pw[p0][r + 1][wl + 1] | s_pw[p1][r][wl + 1] | s_pw[p1][r + 1][wl + 1];
             const uint32_t act = (n0 | (n0 >> 1) | (n1 << 31)) & (q0 | (q0 >> 1) | (q1 << 31)) & vmask;
             const int64_t row = (int64_t)(j0 + r) + (int64_t)g.cy * k;
-            if (wglob < g.W) bits[row * g.W + wglob] = act;
+            if (word_lane && wglob < g.W) bits[row * g.W + wglob] = act;
             uint32_t cnt = __popc(act);
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
@@ -164,13 +173,15 @@ k_expand_ranks(const __grid_constant__ ExpandParams P) {
             live &= live - 1;
             const long long s = s0 + b;
             const uint32_t seg_first = __shfl_sync(0xffffffffu, my_start, b);
-            const GridSlot& S = slot_ref<ONE>(P.B, __shfl_sync(0xffffffffu, my_slot, b));
+            const int sslot = __shfl_sync(0xffffffffu, my_slot, b);   // converged: before the per-lane loop
+            const GridSlot& S = slot_ref<ONE>(P.B, sslot);
             const GridDesc& g = S.g;
             const long long ls = s - S.seg_off;            // segment within its grid
             const long long row = ls / S.nxt;
             const int xt = (int)(ls - row * S.nxt);
-            const int w = xt * kTileWords + lane;
-            const uint32_t act = (w < g.W) ? P.bits[S.bits_off + row * g.W + w] : 0u;
+            const int w = xt * S.tw + lane;
+            const bool word_lane = lane < S.tw;
+            const uint32_t act = (word_lane && w < g.W) ? P.bits[S.bits_off + row * g.W + w] : 0u;
             const uint32_t c = __popc(act);
             uint32_t incl = c;
 #pragma unroll
@@ -179,13 +190,14 @@ k_expand_ranks(const __grid_constant__ ExpandParams P) {
                 if (lane >= o) incl += t;
             }
             const uint32_t first = seg_first + incl - c;
-            if (w < g.W && (w & 7) == 0) P.super[S.super_off + row * g.W8 + (w >> 3)] = first;
+            if (word_lane && w < g.W && (w & 7) == 0) P.super[S.super_off + row * g.W8 + (w >> 3)] = first;
             const int j = (int)(row % g.cy), k = (int)(row / g.cy);
             uint32_t m = act, q = 0;
             while (m) {
                 const int bb = __ffs(m) - 1;
                 m &= m - 1;
                 P.list[first + q] = pack_cell(32 * w + bb, j, k);
+                if (!ONE && P.cell_slot) P.cell_slot[first + q] = (uint32_t)sslot;
                 ++q;
             }
         }
@@ -205,15 +217,21 @@ cudaError_t launch_vert_offsets(const BatchTable& B, const uint32_t* seg_start, 
     return cudaGetLastError();
 }
 
-cudaError_t launch_mark(const MarkParams& P, int vec4, cudaStream_t s) {
+template <bool VEC4, bool ONE>
+void launch_mark_tw(const MarkParams& P, int tw, cudaStream_t s) {
+    if (tw == kNarrowTileWords) k_mark_zmarch<VEC4, ONE, kNarrowTileWords><<<(unsigned)P.ntiles, kMarkWarps * 32, 0, s>>>(P);
+    else                        k_mark_zmarch<VEC4, ONE, kTileWords><<<(unsigned)P.ntiles, kMarkWarps * 32, 0, s>>>(P);
+}
+
+cudaError_t launch_mark(const MarkParams& P, int vec4, int tw, cudaStream_t s) {
     if (P.ntiles <= 0) return cudaSuccess;
     const bool one = P.B.n == 1;
     if (vec4) {
-        if (one) k_mark_zmarch<true, true><<<(unsigned)P.ntiles, kMarkWarps * 32, 0, s>>>(P);
-        else     k_mark_zmarch<true, false><<<(unsigned)P.ntiles, kMarkWarps * 32, 0, s>>>(P);
+        if (one) launch_mark_tw<true, true>(P, tw, s);
+        else     launch_mark_tw<true, false>(P, tw, s);
     } else {
-        if (one) k_mark_zmarch<false, true><<<(unsigned)P.ntiles, kMarkWarps * 32, 0, s>>>(P);
-        else     k_mark_zmarch<false, false><<<(unsigned)P.ntiles, kMarkWarps * 32, 0, s>>>(P);
+        if (one) launch_mark_tw<false, true>(P, tw, s);
+        else     launch_mark_tw<false, false>(P, tw, s);
     }
     return cudaGetLastError();
 }
@@ -231,13 +249,14 @@ cudaError_t launch_expand(const ExpandParams& P, int num_sms, cudaStream_t s) {
 
 int mark_ctas_per_sm(int vec4) {
     int n = 0;
-    const cudaError_t e = vec4 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_mark_zmarch<true, true>, kMarkWarps * 32, 0)
-                               : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_mark_zmarch<false, true>, kMarkWarps * 32, 0);
+    const cudaError_t e = vec4 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_mark_zmarch<true, true, kTileWords>, kMarkWarps * 32, 0)
+                               : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_mark_zmarch<false, true, kTileWords>, kMarkWarps * 32, 0);
     if (e != cudaSuccess) { cudaGetLastError(); return 1; }
     return n > 0 ? n : 1;
 }
 
 int mark_tile_words() { return kTileWords; }
+int mark_narrow_tile_words() { return kNarrowTileWords; }
 int mark_max_rows() { return kMarkWarps - 1; }
 
 }  // namespace dcb

@@ -13,6 +13,7 @@
 // it keeps the last call's contents, so the counters are cleared at the start of each call
 // and two calls whose work overlaps on the GPU race on it.
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <mutex>
 #include "dcb_kernels.cuh"
@@ -102,6 +103,8 @@ extern "C" int dcb_mark_active_cells_noalloc(const dcb_grid* grid, int64_t* cell
     slot.g = g;
     slot.bits_off = 0; slot.super_off = 0; slot.seg_off = 0; slot.col_off = 0;
     slot.nxt = nxt;
+    slot.tw = mark_tile_words();
+    slot.hmax = std::max(std::fabs(g.vx), std::max(std::fabs(g.vy), std::fabs(g.vz)));
     slot.R = std::min(mark_max_rows(), g.cy);
     slot.nrb = (g.cy + slot.R - 1) / slot.R;
     slot.KZ = (int)std::max(8LL, std::min(64LL, ((long long)g.cz * nxt * slot.nrb + (long long)sms * 12 - 1) / ((long long)sms * 12)));
@@ -141,12 +144,12 @@ extern "C" int dcb_mark_active_cells_noalloc(const dcb_grid* grid, int64_t* cell
     if (cudaMemsetAsync(total, 0, sizeof(unsigned long long), s) != cudaSuccess) { cudaGetLastError(); return DCB_ERR_CUDA; }
 
     BatchTable B;
-    B.s0 = slot; B.slots = &dt->slot; B.n = 1; B.seg_off = dt->seg_off; B.col_off = dt->col_off; B.vert_off = dt->vert_off;
+    B.s0 = slot; B.slots = &dt->slot; B.n = 1; B.cell_slot = nullptr; B.seg_off = dt->seg_off; B.col_off = dt->col_off; B.vert_off = dt->vert_off;
     MarkParams mp;
     mp.B = B; mp.tile_slot = dt->tile_slot; mp.tile_off = dt->tile_off; mp.m = 1; mp.ntiles = ntiles;
     mp.bits = reinterpret_cast<uint32_t*>(sb + off_bits);
     mp.seg_count = reinterpret_cast<uint32_t*>(sb + off_count);
-    if (launch_mark(mp, slot.vec4, s) != cudaSuccess) { cudaGetLastError(); return DCB_ERR_CUDA; }
+    if (launch_mark(mp, slot.vec4, slot.tw, s) != cudaSuccess) { cudaGetLastError(); return DCB_ERR_CUDA; }
     uint32_t* seg_start = reinterpret_cast<uint32_t*>(sb + off_start);
     if (launch_scan(mp.seg_count, nseg, reinterpret_cast<uint32_t*>(sb + off_part), seg_start, total, s) != cudaSuccess) {
         cudaGetLastError();
@@ -163,7 +166,7 @@ extern "C" int dcb_mark_active_cells_noalloc(const dcb_grid* grid, int64_t* cell
     if (n == 0) return DCB_OK;
 
     ExpandParams xp;
-    xp.B = B; xp.nseg = nseg; xp.bits = mp.bits; xp.seg_count = mp.seg_count; xp.seg_start = seg_start;
+    xp.B = B; xp.nseg = nseg; xp.cell_slot = nullptr; xp.bits = mp.bits; xp.seg_count = mp.seg_count; xp.seg_start = seg_start;
     xp.super = reinterpret_cast<uint32_t*>(sb + off_super);
     xp.list = reinterpret_cast<uint64_t*>(cells);
     if (launch_expand(xp, sms, s) != cudaSuccess) { cudaGetLastError(); return DCB_ERR_CUDA; }
