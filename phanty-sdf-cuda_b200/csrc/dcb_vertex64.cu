@@ -4,10 +4,10 @@
 // path reproduces the CPU backend's double arithmetic (Cell.cpp:57-361,
 // hermite_update.cpp:171-438, contouring.cpp:141-207, 624-641).
 //
-// One warp per cell: lane e (< 12) forms the Hermite sample of edge e and, when the edge is
-// averaged, the three neighbours' own samples of that edge; lane 0 then accumulates A^T A,
-// A^T b and the centroid in edge order (the CPU's std::map order), so the summation order
-// is the CPU's, and runs the Jacobi eigen-decomposition and the truncated pseudo-inverse.
+// Per cell: the Hermite samples (with the three neighbours' own samples of an averaged edge),
+// then A^T A, A^T b and the centroid summed in edge order (the CPU's std::map order), the
+// Jacobi eigen-decomposition and the truncated pseudo-inverse; a warp per cell (samples in
+// parallel, lane 0 sums and solves) when cells are few, a thread per cell when many.
 #include "dcb_kernels.cuh"
 
 namespace dcb {
@@ -304,6 +304,47 @@ __device__ void cell_vertex_warp(const GridDesc& g, int i, int j, int k, double 
     out[0] = x[0]; out[1] = x[1]; out[2] = x[2];
 }
 
+// FP64 vertex of active cell (i,j,k), by one thread: Hermite samples with their averaged
+// normals in edge order (the CPU's std::map order), A^T A, A^T b and the centroid summed in
+// that order, then the Jacobi eigen-decomposition and the truncated pseudo-inverse about the
+// centroid (Cell.cpp:284-361). A thread per cell keeps every lane busy on the serial solve.
+__device__ void cell_vertex_thread(const GridDesc& g, int i, int j, int k, double thr, double out[3]) {
+    Cell64 C;
+    load_cell(g, i, j, k, C);
+    double ATA[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, ATb[3] = {0, 0, 0}, c[3] = {0, 0, 0};
+    int m = 0;
+    for (int e = 0; e < 12; ++e) {
+        double p[3], n[3];
+        if (!edge_sample(g, C, i, j, k, e, p, n)) continue;
+        // Cell::update row (Cell.cpp:298-311): normalise, b = n.p
+        if (sqrt(sq3(n)) > 0.0) normalize3(n);
+        const double bb = n[0] * p[0] + n[1] * p[1] + n[2] * p[2];
+        for (int r = 0; r < 3; ++r) {
+            for (int s = 0; s < 3; ++s) ATA[r][s] += n[r] * n[s];
+            ATb[r] += n[r] * bb;
+        }
+        for (int d = 0; d < 3; ++d) c[d] += p[d];
+        ++m;
+    }
+    for (int d = 0; d < 3; ++d) c[d] /= double(m);
+    double A[3][3], V[3][3];
+    for (int r = 0; r < 3; ++r) for (int s = 0; s < 3; ++s) A[r][s] = ATA[r][s];
+    jacobi3(A, V);
+    const double lam[3] = {A[0][0], A[1][1], A[2][2]};
+    double rhs[3];
+    for (int r = 0; r < 3; ++r) rhs[r] = ATb[r] - (ATA[r][0] * c[0] + ATA[r][1] * c[1] + ATA[r][2] * c[2]);
+    double x[3] = {c[0], c[1], c[2]};
+    for (int q = 0; q < 3; ++q) {
+        const double sv = fabs(lam[q]);
+        if (sv > thr) {
+            const double proj = V[0][q] * rhs[0] + V[1][q] * rhs[1] + V[2][q] * rhs[2];
+            const double coef = proj / sv;
+            for (int d = 0; d < 3; ++d) x[d] += V[d][q] * coef;
+        }
+    }
+    out[0] = x[0]; out[1] = x[1]; out[2] = x[2];
+}
+
 // gradientAt (contouring.cpp:141-207).
 __device__ void grid_gradient(const GridDesc& g, int i, int j, int k, double out[3]) {
     const int im = max(i - 1, 0), ip = min(i + 1, g.nx - 1);
@@ -322,38 +363,54 @@ __device__ void grid_gradient(const GridDesc& g, int i, int j, int k, double out
 
 }  // namespace f64
 
-// Warp per listed cell. Writes the float vertex (Vf[rank]) and/or the double one (V64[t]).
+__device__ __forceinline__ void store64(const Vertex64Params& P, uint32_t r, unsigned int t, const double x[3]) {
+    if (P.Vf) {
+        P.Vf[3 * (size_t)r + 0] = (float)x[0];
+        P.Vf[3 * (size_t)r + 1] = (float)x[1];
+        P.Vf[3 * (size_t)r + 2] = (float)x[2];
+        if (P.vclass) P.vclass[r] = kVcFp64;
+    }
+    if (P.V64) {
+        P.V64[3 * (size_t)t + 0] = x[0];
+        P.V64[3 * (size_t)t + 1] = x[1];
+        P.V64[3 * (size_t)t + 2] = x[2];
+    }
+}
+
+// Listed cells' FP64 vertices: Vf[rank] (float) and/or V64[t] (double). With at most one cell
+// per warp of the launch, a warp shares each cell's 48 samples (short latency); with more,
+// a thread takes a whole cell (every lane busy). Both give the same bits.
 __global__ void __launch_bounds__(128)
 k_vertex_fp64(Vertex64Params P) {
     const unsigned int n = min(*P.count, P.cap);
-    const int lane = threadIdx.x & 31;
     const unsigned int warps = (gridDim.x * blockDim.x) >> 5;
-    for (unsigned int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < n; t += warps) {
+    if (n <= warps) {
+        const int lane = threadIdx.x & 31;
+        for (unsigned int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < n; t += warps) {
+            const uint32_t r = P.cells[t];
+            int i, j, k;
+            unpack_cell(P.list[r], i, j, k);
+            const GridDesc g = P.B.slots[slot_of_rank(P.B, r)].g;
+            double x[3];
+            f64::cell_vertex_warp(g, i, j, k, P.thr, x);
+            if (lane == 0) store64(P, r, t, x);
+        }
+        return;
+    }
+    for (unsigned int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
         const uint32_t r = P.cells[t];
         int i, j, k;
         unpack_cell(P.list[r], i, j, k);
         const GridDesc g = P.B.slots[slot_of_rank(P.B, r)].g;
         double x[3];
-        f64::cell_vertex_warp(g, i, j, k, P.thr, x);
-        if (lane == 0) {
-            if (P.Vf) {
-                P.Vf[3 * (size_t)r + 0] = (float)x[0];
-                P.Vf[3 * (size_t)r + 1] = (float)x[1];
-                P.Vf[3 * (size_t)r + 2] = (float)x[2];
-                if (P.vclass) P.vclass[r] = kVcFp64;
-            }
-            if (P.V64) {
-                P.V64[3 * (size_t)t + 0] = x[0];
-                P.V64[3 * (size_t)t + 1] = x[1];
-                P.V64[3 * (size_t)t + 2] = x[2];
-            }
-        }
+        f64::cell_vertex_thread(g, i, j, k, P.thr, x);
+        store64(P, r, t, x);
     }
 }
 
 cudaError_t launch_vertex_fp64(const Vertex64Params& P, long long max_items, int num_sms, cudaStream_t s) {
     if (max_items <= 0) return cudaSuccess;
-    long long blocks = (max_items * 32 + 127) / 128;
+    long long blocks = (max_items + 127) / 128;
     const long long cap = (long long)num_sms * 16;
     if (blocks > cap) blocks = cap;
     k_vertex_fp64<<<(unsigned)blocks, 128, 0, s>>>(P);
