@@ -218,6 +218,22 @@ int dcb_mesh_to_sdf_host(dcb_handle h, const float* vertices, int64_t num_vertic
                          int64_t num_faces, int nx, int ny, int nz, float ox, float oy, float oz, float vx,
                          float vy, float vz, float* out_values, dcb_sdf_stats* stats, void* cuda_stream);
 
+/* ---- adjoint of the vertices ------------------------------------------------------------ */
+
+/* Gradient of a loss with respect to the grid values, given its gradient with respect to the
+ * vertices of the LAST single-grid extraction on this handle (no counterpart in the reference,
+ * whose backends are forward-only). grid must be the grid that extraction ran on (device
+ * values, unchanged since) and opts the same options. dL_dvertices is a device array of
+ * 3*vertex_count floats; dL_dgrid a device array of nx*ny*nz floats that receives the
+ * gradient (added to what it holds when accumulate != 0, else overwritten). Topology is held
+ * fixed: the active cells, the Hermite edges and the rank of every cell's QEF solve are those
+ * of the extraction. Each vertex is differentiated through its FP64 solve: the 4-cell averaged
+ * Hermite normals, the trilinear gradients and crossings of the cell and its neighbours (the
+ * 4x4x4 stencil), and the truncated pseudo-inverse by its implicit derivative. Sums into
+ * dL_dgrid use float atomics, so their order (and the last bits) may vary between calls. */
+int dcb_backward(dcb_handle h, const dcb_grid* grid, const dcb_opts* opts, const float* dL_dvertices,
+                 float* dL_dgrid, int accumulate, void* cuda_stream);
+
 /* Human-readable text of a status code and of the last error on this handle. */
 const char* dcb_status_string(int status);
 const char* dcb_last_error(dcb_handle h);

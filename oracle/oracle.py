@@ -3,7 +3,9 @@
 The oracle is the FP64 C++ restatement in ``oracle/dc_oracle.cpp`` of the reference's
 ``CpuDualContouringBackend::extract`` (src/cpp/dc_backend.cpp:51-125), and the float
 restatement in ``oracle/mts_oracle.cpp`` of its mesh -> SDF conversion
-(src/cuda/mesh_to_sdf_cuda.cu:740-1009).  Only ``tests/``,
+(src/cuda/mesh_to_sdf_cuda.cu:740-1009), and ``oracle/dc_adjoint_oracle.cpp``: the per-cell
+FP64 vertex as a template run with double (for finite differences) and with dual numbers
+(the FP64 reference Jacobian of each vertex with respect to its 4x4x4 stencil).  Only ``tests/``,
 ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline / reference legs import this
 module, and only as the checker or the CPU baseline, never as the product path.
 """
@@ -16,6 +18,7 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _DC_LIB = os.path.join(_HERE, "_build", "libdc_oracle.so")
 _MTS_LIB = os.path.join(_HERE, "_build", "libmts_oracle.so")
+_ADJ_LIB = os.path.join(_HERE, "_build", "libdc_adjoint_oracle.so")
 _libs = {}
 
 
@@ -202,4 +205,79 @@ def mesh_band_values(V, F, dims, origin, spacing, idx, threads=0):
                                 idx.ctypes.data, len(idx), int(threads), out.ctypes.data)
     if rc != 0:
         raise ValueError("oracle rejected the input")
+    return out
+
+
+def _adj():
+    lib = _load(_ADJ_LIB)
+    if not getattr(lib, "_typed", False):
+        args = [ctypes.c_int] * 3 + [ctypes.c_void_p] * 6 + [ctypes.c_int64, ctypes.c_double, ctypes.c_void_p]
+        lib.dca_cell_vertices.argtypes = args + [ctypes.c_void_p, ctypes.c_int]
+        lib.dca_cell_vertices.restype = ctypes.c_int
+        lib.dca_cell_jacobians.argtypes = args + [ctypes.c_void_p, ctypes.c_int]
+        lib.dca_cell_jacobians.restype = ctypes.c_int
+        lib._typed = True
+    return lib
+
+
+def _adj_args(values, dims, axes, cells):
+    nx, ny, nz = (int(d) for d in dims)
+    v = np.asarray(values).reshape(-1)
+    if v.dtype == np.float64:
+        vf, vd = None, np.ascontiguousarray(v)
+    else:
+        vf, vd = np.ascontiguousarray(v, dtype=np.float32), None
+    ax = [np.ascontiguousarray(np.asarray(a, np.float64)) for a in axes]
+    if (vf if vf is not None else vd).size != nx * ny * nz or [a.size for a in ax] != [nx, ny, nz]:
+        raise ValueError("shape mismatch")
+    cells = np.ascontiguousarray(np.asarray(cells, np.int64))
+    keep = (vf, vd, ax, cells)
+    ptr = lambda a: None if a is None else a.ctypes.data
+    return keep, [nx, ny, nz, ax[0].ctypes.data, ax[1].ctypes.data, ax[2].ctypes.data, ptr(vf), ptr(vd),
+                  cells.ctypes.data, len(cells)]
+
+
+def cell_vertices(values, dims, axes, cells, svd_threshold=0.01, threads=0, return_kept=False):
+    """FP64 vertices of the listed active cells (linear i + cx*(j + cy*k)); ``values`` float32
+    or float64 (nx*ny*nz, x fastest), ``axes`` the float64 grid-point coordinates per axis.
+    With ``return_kept`` also the number of eigenvalues each cell's solve keeps."""
+    keep, args = _adj_args(values, dims, axes, cells)
+    out = np.empty((len(keep[3]), 3), np.float64)
+    kept = np.empty(len(keep[3]), np.int32)
+    if _adj().dca_cell_vertices(*args, float(svd_threshold), out.ctypes.data, kept.ctypes.data, int(threads)) != 0:
+        raise ValueError("oracle rejected the grid")
+    return (out, kept) if return_kept else out
+
+
+def cell_jacobians(values, dims, axes, cells, svd_threshold=0.01, threads=0):
+    """(vertices (n,3), jac (n,3,64)): the FP64 reference Jacobian of each listed cell's vertex
+    with respect to the values of its stencil, slot s = grid point (i-1+s%4, j-1+(s//4)%4,
+    k-1+s//16), by forward-mode automatic differentiation."""
+    keep, args = _adj_args(values, dims, axes, cells)
+    n = len(keep[3])
+    out = np.empty((n, 3), np.float64)
+    jac = np.empty((n, 3, 64), np.float64)
+    if _adj().dca_cell_jacobians(*args, float(svd_threshold), out.ctypes.data, jac.ctypes.data, int(threads)) != 0:
+        raise ValueError("oracle rejected the grid")
+    return out, jac
+
+
+def vertex_vjp(values, dims, axes, cells, grad_vertices, svd_threshold=0.01, threads=0):
+    """FP64 reference adjoint: d(loss)/d(grid values) (float64, nx*ny*nz) from
+    d(loss)/d(vertices) of the listed cells, as the sum of J^T g over the cells."""
+    nx, ny, nz = (int(d) for d in dims)
+    cells = np.asarray(cells, np.int64)
+    _, jac = cell_jacobians(values, dims, axes, cells, svd_threshold, threads)
+    contrib = np.einsum("nds,nd->ns", jac, np.asarray(grad_vertices, np.float64))
+    cx, cy = nx - 1, ny - 1
+    i, j, k = cells % cx, (cells // cx) % cy, cells // (cx * cy)
+    s = np.arange(64)
+    gi = i[:, None] - 1 + s % 4
+    gj = j[:, None] - 1 + (s // 4) % 4
+    gk = k[:, None] - 1 + s // 16
+    inside = (gi >= 0) & (gi < nx) & (gj >= 0) & (gj < ny) & (gk >= 0) & (gk < nz)
+    if np.any(contrib[~inside] != 0.0):
+        raise AssertionError("derivative with respect to a point outside the grid")
+    out = np.zeros(nx * ny * nz, np.float64)
+    np.add.at(out, (gi + nx * (gj + ny * gk))[inside], contrib[inside])
     return out

@@ -9,6 +9,14 @@ from .backend import (B200DualContouringBackend, ContouringMethod, ContouringOpt
                       MeshSdfStats, mesh_to_sdf_cuda, mesh_to_sdf_tensor)
 from . import _lib
 
+
+def __getattr__(name):
+    # torch is imported only by the differentiable path
+    if name in ("dual_contour", "DualContourFunction"):
+        from . import autograd
+        return getattr(autograd, name)
+    raise AttributeError(name)
+
 __all__ = ["B200DualContouringBackend", "ContouringMethod", "ContouringOptions", "DcbError",
            "DenseSdfGrid", "DenseSdfGridDevice", "DualContouringMesh", "DualContouringStats",
-           "MeshSdfStats", "mesh_to_sdf_cuda", "mesh_to_sdf_tensor"]
+           "MeshSdfStats", "mesh_to_sdf_cuda", "mesh_to_sdf_tensor", "dual_contour", "DualContourFunction"]

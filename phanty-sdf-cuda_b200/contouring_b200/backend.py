@@ -180,6 +180,7 @@ class B200DualContouringBackend:
         self.options = options if options is not None else ContouringOptions()
         self._last_nv = 0
         self._last_vpf = 4
+        self._generation = 0          # counts extractions; a backward needs its forward's
 
     def close(self):
         if getattr(self, "_h", None):
@@ -210,6 +211,7 @@ class B200DualContouringBackend:
                                             ctypes.byref(mh), ctypes.byref(st), ctypes.c_void_p(s)), self._h)
         self._last_nv = mh.vertex_count
         self._last_vpf = mh.verts_per_face
+        self._generation += 1
         return self._host_mesh(mh), DualContouringStats.from_c(st)
 
     @staticmethod
@@ -252,6 +254,7 @@ class B200DualContouringBackend:
                                               ctypes.byref(md), ctypes.byref(st), ctypes.c_void_p(s)), self._h)
         self._last_nv = md.vertex_count
         self._last_vpf = md.verts_per_face
+        self._generation += 1
         return md.vertices, md.faces, DualContouringStats.from_c(st)
 
     def extract_batch_ptr(self, grids, stream=None):
@@ -269,6 +272,7 @@ class B200DualContouringBackend:
                                                     ctypes.byref(out), ctypes.byref(st), ctypes.c_void_p(s)), self._h)
         self._last_nv = out.vertex_count
         self._last_vpf = out.verts_per_face
+        self._generation += 1
         return out, DualContouringStats.from_c(st)
 
     def extract_batch(self, grids, stream=None):
@@ -302,6 +306,31 @@ class B200DualContouringBackend:
         _lib.check(self._L.dcb_copy_mesh_device(self._h, V.data_ptr() if V.numel() else None,
                                                 F.data_ptr() if F.numel() else None, ctypes.c_void_p(s)), self._h)
         return V, F, stats
+
+
+    def backward_tensor(self, values, dims, spacing, origin, grad_vertices, out=None, accumulate=False):
+        """d(loss)/d(grid values) from d(loss)/d(vertices) of the LAST single-grid extraction on
+        this backend, which must have run on ``values`` (unchanged) with the same options:
+        float32 CUDA tensors in, a float32 CUDA tensor of nx*ny*nz out (``out`` if given; added
+        to when ``accumulate``)."""
+        import torch
+        n = int(dims[0]) * int(dims[1]) * int(dims[2])
+        dV = grad_vertices.to(torch.float32).contiguous()
+        if dV.numel() != 3 * self._last_nv or not dV.is_cuda:
+            raise DcbError(_lib.DCB_ERR_INVALID_ARGUMENT, "grad_vertices must be a CUDA tensor of (vertex_count, 3)")
+        if out is None:
+            out = torch.empty(n, dtype=torch.float32, device=values.device)
+            accumulate = False
+        elif out.numel() != n or out.dtype != torch.float32 or not out.is_cuda or not out.is_contiguous():
+            raise DcbError(_lib.DCB_ERR_INVALID_ARGUMENT, "out must be a contiguous float32 CUDA tensor of nx*ny*nz")
+        g = DenseSdfGridDevice(*dims, *spacing, *origin, d_values=values)
+        gc = self._grid_c(g, g.pointer())
+        s = torch.cuda.current_stream().cuda_stream
+        _lib.check(self._L.dcb_backward(self._h, ctypes.byref(gc), ctypes.byref(self.options.to_c()),
+                                        ctypes.c_void_p(dV.data_ptr() if dV.numel() else None),
+                                        ctypes.c_void_p(out.data_ptr()), int(bool(accumulate)),
+                                        ctypes.c_void_p(s)), self._h)
+        return out
 
 
 class MeshSdfStats:

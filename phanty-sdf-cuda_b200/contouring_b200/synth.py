@@ -221,6 +221,21 @@ def rbf_sphere(res=128, radius=0.3, n_rbf=64, seed=0, lo=-0.5, hi=0.5, device="c
     return vals, dims, spacing, origin
 
 
+def rbf_sphere_points(n=50000, radius=0.3, n_rbf=64, seed=1):
+    """n points on a second perturbed sphere: directions uniform on the sphere, radius
+    0.3 + sum_q a_q exp(-|0.3 u - c_q|^2 / w_q^2) with the RBF parameters of
+    ``rbf_sphere(seed=seed)``. float64 (n, 3)."""
+    rng = np.random.default_rng(seed)
+    cs = rng.uniform(-0.4, 0.4, (n_rbf, 3))
+    amp = rng.uniform(-0.03, 0.03, n_rbf)
+    wid = rng.uniform(0.03, 0.08, n_rbf)
+    u = np.random.default_rng(seed + 1000).normal(size=(n, 3))
+    u /= np.linalg.norm(u, axis=1, keepdims=True)
+    q = radius * u
+    r = radius + (amp[None] * np.exp(-((q[:, None, :] - cs[None]) ** 2).sum(-1) / (wid[None] ** 2))).sum(1)
+    return u * r[:, None]
+
+
 def ternary(dims, seed=0):
     """Values drawn from {-1, 0, +1}: maximal ties and exact zeros."""
     rng = np.random.default_rng(seed)

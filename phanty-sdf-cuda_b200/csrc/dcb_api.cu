@@ -57,7 +57,7 @@ struct dcb_context {
     cudaEvent_t ev[8] = {};
     DevBuf grid, bits, super, list, seg_count, seg_start, counters, V, vclass, fmask, col_count, col_fill,
         col_start, partials, esc_list, hard_list, hard_data, stage_quad, stage_key, faces, wind_items,
-        v64_index, v64_cells, V64, tris, tri_items;
+        v64_index, v64_cells, V64, tris, tri_items, adj_rows, adj_owners;
     // mesh -> SDF workspace
     DevBuf m_verts, m_faces, m_out, m_tris, m_bin_count, m_bin_start, m_bin_fill, m_bin_scratch, m_bin_tris,
         m_bin_active, m_active_list, m_axis_start, m_far, m_ext, m_tmp, m_partials, m_counters;
@@ -643,7 +643,7 @@ int dcb_destroy(dcb_handle h) {
                       &h->tris, &h->tri_items, &h->m_verts, &h->m_faces, &h->m_out, &h->m_tris,
                       &h->m_bin_count, &h->m_bin_start, &h->m_bin_fill, &h->m_bin_scratch, &h->m_bin_tris,
                       &h->m_bin_active, &h->m_active_list, &h->m_axis_start, &h->m_far, &h->m_ext, &h->m_tmp,
-                      &h->m_partials, &h->m_counters, &h->table, &h->cell_slot};
+                      &h->m_partials, &h->m_counters, &h->table, &h->cell_slot, &h->adj_rows, &h->adj_owners};
     for (DevBuf* b : bufs) if (b->p) cudaFree(b->p);
     if (h->h_counters) cudaFreeHost(h->h_counters);
     if (h->h_sdf_counters) cudaFreeHost(h->h_sdf_counters);
@@ -795,6 +795,45 @@ int dcb_copy_cells_to_host(dcb_handle h, int64_t* cell_linear_index, void* cuda_
         const int64_t i = (int64_t)(p & 0x1FFFFF), j = (int64_t)((p >> 21) & 0x1FFFFF), k = (int64_t)(p >> 42);
         cell_linear_index[r] = i + cx * (j + cy * k);
     }
+    return DCB_OK;
+}
+
+int dcb_backward(dcb_handle h, const dcb_grid* grid, const dcb_opts* opts, const float* dL_dvertices,
+                 float* dL_dgrid, int accumulate, void* cuda_stream) {
+    int rc = validate(h, grid);
+    if (rc != DCB_OK) return rc;
+    dcb_opts def;
+    dcb_default_opts(&def);
+    const dcb_opts* o = opts ? opts : &def;
+    if (o->method != DCB_METHOD_DUAL_CONTOURING) return fail(h, DCB_ERR_NOT_SUPPORTED, "only dual contouring is implemented");
+    if (!(o->svd_threshold >= 0.0)) return fail(h, DCB_ERR_INVALID_ARGUMENT, "svd_threshold must be >= 0");
+    if (h->batch_n != 1 || h->cx != grid->nx - 1 || h->cy != grid->ny - 1)
+        return fail(h, DCB_ERR_INVALID_ARGUMENT, "backward needs the grid of the last single-grid extraction");
+    if (!dL_dgrid || (h->nv > 0 && !dL_dvertices)) return fail(h, DCB_ERR_INVALID_ARGUMENT, "null gradient array");
+    if (cudaSetDevice(h->device) != cudaSuccess) { cudaGetLastError(); return fail(h, DCB_ERR_CUDA, "set device"); }
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(cuda_stream);
+    const size_t npts = (size_t)grid->nx * grid->ny * grid->nz;
+    if (!accumulate) DCB_TRY(h, cudaMemsetAsync(dL_dgrid, 0, sizeof(float) * npts, s), "clear grid gradient");
+    if (h->nv == 0) return DCB_OK;
+    BatchLayout L;
+    rc = layout_batch(h, grid, 1, L);
+    if (rc != DCB_OK) return rc;
+    if (12 * h->nv >= 0xffffffffLL) return fail(h, DCB_ERR_TOO_LARGE, "too many vertices for the adjoint");
+    DCB_TRY(h, ensure(h->adj_rows, sizeof(AdjointRow) * 12 * (size_t)h->nv), "alloc adjoint rows");
+    DCB_TRY(h, ensure(h->adj_owners, sizeof(uint32_t) * (12 * (size_t)h->nv + 64)), "alloc adjoint owners");
+    AdjointParams P;
+    P.rows = as<AdjointRow>(h->adj_rows);
+    P.bits = as<uint32_t>(h->bits);
+    P.super = as<uint32_t>(h->super);
+    P.owners = as<uint32_t>(h->adj_owners);
+    P.owner_count = as<uint32_t>(h->adj_owners) + 12 * (size_t)h->nv + 32;
+    P.g = L.slots[0].g;
+    P.list = as<uint64_t>(h->list);
+    P.nactive = h->nv;
+    P.dV = dL_dvertices;
+    P.dgrid = dL_dgrid;
+    P.thr = o->svd_threshold;
+    DCB_TRY(h, launch_vertex_adjoint(P, h->num_sms, s), "launch vertex adjoint");
     return DCB_OK;
 }
 

@@ -214,6 +214,29 @@ struct Tri64Params {
 };
 cudaError_t launch_tri_fp64(const Tri64Params& P, long long max_items, int num_sms, cudaStream_t s);
 
+// ---- adjoint of the vertices (dcb_vertex64.cu) ----
+// One row (cell, local edge) of the adjoint's workspace: after the first pass the row's normal
+// (a) and point (b); after the second their gradients. flags: 0 no sample, 1 row, 2 gradients.
+struct AdjointRow {
+    double a[3];
+    double b[3];
+    long long flags;
+};
+struct AdjointParams {
+    GridDesc g;
+    const uint64_t* list;
+    long long nactive;
+    const float* dV;               // [3 * active] d(loss)/d(vertex)
+    float* dgrid;                  // [nx*ny*nz] d(loss)/d(grid value), accumulated
+    AdjointRow* rows;              // [12 * active] workspace
+    const uint32_t* bits;          // the extraction's active bits and super-word ranks
+    const uint32_t* super;
+    uint32_t* owners;              // [12 * active] rows (cell * 12 + edge) that own their edge
+    unsigned int* owner_count;
+    double thr;
+};
+cudaError_t launch_vertex_adjoint(const AdjointParams& P, int num_sms, cudaStream_t s);
+
 // ---- mesh -> SDF (dcb_mesh_sdf.cu) ----
 struct SdfParams {
     int nx, ny, nz;

@@ -361,6 +361,165 @@ __device__ void grid_gradient(const GridDesc& g, int i, int j, int k, double out
     if (nrm > 0.0) { out[0] /= nrm; out[1] /= nrm; out[2] /= nrm; }
 }
 
+// ---- adjoint of the vertex map -----------------------------------------------------------
+//
+// v(cell) = c + M r with c the mean Hermite point, A = sum n n^T, r = sum n n^T (p - c) and
+// M = sum over retained eigenpairs (lambda > thr) of u u^T / lambda. For a gradient g of the
+// loss at v, with the rank held fixed (topology fixed), the implicit derivative of the
+// truncated pseudo-inverse gives
+//   r_bar = M g,   c_bar = g - A r_bar,
+//   A_bar = -sym((M g)(M r)^T)
+//           + sum_{q retained, p truncated} [(g.u_p)(u_q.r) + (g.u_q)(u_p.r)] sym(u_p u_q^T)
+//             / ((lambda_q - lambda_p) lambda_q)
+// (the retained-retained pairs combine into the -M dA M term, smooth even for equal
+// eigenvalues; a retained-truncated pair has the gap lambda_q - lambda_p > 0). Then per
+// Hermite sample (p_e, n_e): n_bar = 2 A_bar n + (n.(p-c)) r_bar + (r_bar.n)(p-c),
+// p_bar = (r_bar.n) n + c_bar/m, back through the normalisations, the 4-cell average, the
+// trilinear gradients and t = fa/(fa - fb + 1e-16) to the grid values of the 4x4x4 stencil.
+
+// A cell's own sample on local edge e, with what its backward needs.
+struct Sample {
+    double t, p[3], g[3], gn, n[3];
+};
+
+__device__ bool sample_fwd(const Cell64& C, int e, Sample& S) {
+    const int a = edge_a(e), b = edge_b(e);
+    const double fa = C.cs[a], fb = C.cs[b];
+    if (fa * fb > 0.0) return false;
+    S.t = (fa - 0.0) / (fa - fb + 1e-16);
+    for (int d = 0; d < 3; ++d) S.p[d] = (1.0 - S.t) * C.cp[a][d] + S.t * C.cp[b][d];
+    tri_grad(C, S.p, S.g);
+    S.gn = sqrt(sq3(S.g));
+    for (int d = 0; d < 3; ++d) S.n[d] = S.g[d];
+    if (S.gn > 0.0) normalize3(S.n);
+    return true;
+}
+
+// Backward of the trilinear gradient (Cell.cpp:80-155): gbar -> corner values Sbar, point pbar.
+__device__ void tri_grad_bwd(const Cell64& C, const double p[3], const double gb[3], double Sb[8], double pb[3]) {
+    const double S000 = C.cs[0], S100 = C.cs[1], S110 = C.cs[2], S010 = C.cs[3];
+    const double S001 = C.cs[4], S101 = C.cs[5], S111 = C.cs[6], S011 = C.cs[7];
+    const double x0 = C.cp[0][0], x1 = C.cp[1][0];
+    const double y0 = C.cp[0][1], y1 = C.cp[3][1];
+    const double z0 = C.cp[0][2], z1 = C.cp[4][2];
+    const double dx = x1 - x0, dy = y1 - y0, dz = z1 - z0;
+    const double eps = 1e-12;
+    double u = 0.5, v = 0.5, w = 0.5;
+    bool fu = false, fv = false, fw = false;           // inside [0,1]: the point moves it
+    if (fabs(dx) > eps) { u = (p[0] - x0) / dx; fu = u >= 0.0 && u <= 1.0; }
+    if (fabs(dy) > eps) { v = (p[1] - y0) / dy; fv = v >= 0.0 && v <= 1.0; }
+    if (fabs(dz) > eps) { w = (p[2] - z0) / dz; fw = w >= 0.0 && w <= 1.0; }
+    u = fmax(0.0, fmin(1.0, u)); v = fmax(0.0, fmin(1.0, v)); w = fmax(0.0, fmin(1.0, w));
+    const double omu = 1.0 - u, omv = 1.0 - v, omw = 1.0 - w;
+    const double ax = fabs(dx) > eps ? gb[0] / dx : 0.0;   // d(loss)/d(df_du)
+    const double ay = fabs(dy) > eps ? gb[1] / dy : 0.0;
+    const double az = fabs(dz) > eps ? gb[2] / dz : 0.0;
+    // corners
+    Sb[1] += ax * omv * omw; Sb[0] -= ax * omv * omw; Sb[2] += ax * v * omw; Sb[3] -= ax * v * omw;
+    Sb[5] += ax * omv * w;   Sb[4] -= ax * omv * w;   Sb[6] += ax * v * w;   Sb[7] -= ax * v * w;
+    Sb[3] += ay * omu * omw; Sb[0] -= ay * omu * omw; Sb[2] += ay * u * omw; Sb[1] -= ay * u * omw;
+    Sb[7] += ay * omu * w;   Sb[4] -= ay * omu * w;   Sb[6] += ay * u * w;   Sb[5] -= ay * u * w;
+    Sb[4] += az * omu * omv; Sb[0] -= az * omu * omv; Sb[5] += az * u * omv; Sb[1] -= az * u * omv;
+    Sb[7] += az * omu * v;   Sb[3] -= az * omu * v;   Sb[6] += az * u * v;   Sb[2] -= az * u * v;
+    // parametric coordinates
+    const double dux = -(S100 - S000) * omw + (S110 - S010) * omw - (S101 - S001) * w + (S111 - S011) * w;   // d df_du / dv
+    const double dwx = -(S100 - S000) * omv - (S110 - S010) * v + (S101 - S001) * omv + (S111 - S011) * v;  // d df_du / dw
+    const double duy = -(S010 - S000) * omw + (S110 - S100) * omw - (S011 - S001) * w + (S111 - S101) * w;   // d df_dv / du
+    const double dwy = -(S010 - S000) * omu - (S110 - S100) * u + (S011 - S001) * omu + (S111 - S101) * u;  // d df_dv / dw
+    const double duz = -(S001 - S000) * omv + (S101 - S100) * omv - (S011 - S010) * v + (S111 - S110) * v;   // d df_dw / du
+    const double dvz = -(S001 - S000) * omu - (S101 - S100) * u + (S011 - S010) * omu + (S111 - S110) * u;  // d df_dw / dv
+    const double ub = ay * duy + az * duz, vb = ax * dux + az * dvz, wb = ax * dwx + ay * dwy;
+    if (fu) pb[0] += ub / dx;
+    if (fv) pb[1] += vb / dy;
+    if (fw) pb[2] += wb / dz;
+}
+
+// Backward of one sample of cell (ci,cj,ck) on local edge e: nbar at its normalised normal,
+// pbar at its point; the grid values' adjoints are added into dgrid.
+__device__ void sample_bwd(const GridDesc& g, const Cell64& C, int ci, int cj, int ck, int e, const Sample& S,
+                           const double nb[3], const double pbar[3], float* dgrid) {
+    double gb[3];
+    if (S.gn > 0.0) {
+        const double nn = S.n[0] * nb[0] + S.n[1] * nb[1] + S.n[2] * nb[2];
+        for (int d = 0; d < 3; ++d) gb[d] = (nb[d] - S.n[d] * nn) / S.gn;
+    } else {
+        for (int d = 0; d < 3; ++d) gb[d] = nb[d];
+    }
+    double Sb[8] = {0, 0, 0, 0, 0, 0, 0, 0}, pb[3] = {pbar[0], pbar[1], pbar[2]};
+    tri_grad_bwd(C, S.p, gb, Sb, pb);
+    const int a = edge_a(e), b = edge_b(e);
+    double tb = 0.0;
+    for (int d = 0; d < 3; ++d) tb += pb[d] * (C.cp[b][d] - C.cp[a][d]);
+    const double fa = C.cs[a], fb = C.cs[b];
+    if (fa != 0.0 || fb != 0.0) {          // both zero: t = 0 jumps under any change, no derivative
+        const double D = fa - fb + 1e-16;
+        Sb[a] += tb * (-fb + 1e-16) / (D * D);
+        Sb[b] += tb * fa / (D * D);
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+        if (Sb[q] != 0.0) atomicAdd(dgrid + pidx(g, ci + corner_dx(q), cj + corner_dy(q), ck + corner_dz(q)), (float)Sb[q]);
+}
+
+// The four cells of an averaged edge (hermite_update.cpp:171-332) in the CPU's sum order:
+// q = 0 the cell at the edge's minimum endpoint, 1 = -d1, 2 = -d2, 3 = both.
+__device__ bool edge_cells(const GridDesc& g, int i, int j, int k, int e, int cc[4][3], int ex[4]) {
+    const int a = edge_a(e), b = edge_b(e);
+    const int Pa[3] = {i + corner_dx(a), j + corner_dy(a), k + corner_dz(a)};
+    const int Pb[3] = {i + corner_dx(b), j + corner_dy(b), k + corner_dz(b)};
+    int Pm[3], PM[3];
+    for (int d = 0; d < 3; ++d) { Pm[d] = min(Pa[d], Pb[d]); PM[d] = max(Pa[d], Pb[d]); }
+    const bool in0 = Pm[0] > 0 && Pm[0] < g.nx - 1 && Pm[1] > 0 && Pm[1] < g.ny - 1 && Pm[2] > 0 && Pm[2] < g.nz - 1;
+    const bool in1 = PM[0] > 0 && PM[0] < g.nx - 1 && PM[1] > 0 && PM[1] < g.ny - 1 && PM[2] > 0 && PM[2] < g.nz - 1;
+    if (!in0 && !in1) return false;
+    const int axis = Pa[0] != Pb[0] ? 0 : (Pa[1] != Pb[1] ? 1 : 2);
+    const int d1 = axis == 0 ? 1 : 0;
+    const int d2 = axis == 2 ? 1 : 2;
+    for (int q = 0; q < 4; ++q) {
+        cc[q][0] = Pm[0]; cc[q][1] = Pm[1]; cc[q][2] = Pm[2];
+        if (q & 1) cc[q][d1] -= 1;
+        if (q & 2) cc[q][d2] -= 1;
+        ex[q] = local_edge(axis, Pm[d1] - cc[q][d1], Pm[d2] - cc[q][d2]);
+    }
+    return true;
+}
+
+// The QEF part of the adjoint: from the sums A, A^T b, the centroid c and the vertex gradient
+// vb, the gradients of A (symmetric, Ab), of r = A^T b - A c (rb) and of c (cb).
+__device__ void qef_adjoint(const double A[3][3], const double ATb[3], const double c[3], double thr,
+                            const double vb[3], double Ab[3][3], double rb[3], double cb[3]) {
+    double E[3][3], U[3][3];
+    for (int r = 0; r < 3; ++r) for (int s2 = 0; s2 < 3; ++s2) E[r][s2] = A[r][s2];
+    jacobi3(E, U);
+    double lam[3];                          // |eigenvalue| for the retained, signed for the rest
+    bool keep[3];
+    for (int q = 0; q < 3; ++q) { keep[q] = fabs(E[q][q]) > thr; lam[q] = keep[q] ? fabs(E[q][q]) : E[q][q]; }
+    double r[3];
+    for (int d = 0; d < 3; ++d) r[d] = ATb[d] - (A[d][0] * c[0] + A[d][1] * c[1] + A[d][2] * c[2]);
+    // M g, M r, projections on the eigenvectors
+    double ug[3], ur[3], Mg[3] = {0, 0, 0}, Mr[3] = {0, 0, 0};
+    for (int q = 0; q < 3; ++q) {
+        ug[q] = U[0][q] * vb[0] + U[1][q] * vb[1] + U[2][q] * vb[2];
+        ur[q] = U[0][q] * r[0] + U[1][q] * r[1] + U[2][q] * r[2];
+        if (!keep[q]) continue;
+        for (int d = 0; d < 3; ++d) { Mg[d] += U[d][q] * ug[q] / lam[q]; Mr[d] += U[d][q] * ur[q] / lam[q]; }
+    }
+    for (int x = 0; x < 3; ++x)
+        for (int y = 0; y < 3; ++y) Ab[x][y] = -0.5 * (Mg[x] * Mr[y] + Mr[x] * Mg[y]);
+    for (int q = 0; q < 3; ++q) {
+        if (!keep[q]) continue;
+        for (int pp = 0; pp < 3; ++pp) {
+            if (keep[pp]) continue;
+            const double wpq = 1.0 / ((lam[q] - lam[pp]) * lam[q]);
+            const double coef = wpq * (ug[pp] * ur[q] + ug[q] * ur[pp]);
+            for (int x = 0; x < 3; ++x)
+                for (int y = 0; y < 3; ++y) Ab[x][y] += 0.5 * coef * (U[x][pp] * U[y][q] + U[x][q] * U[y][pp]);
+        }
+    }
+    for (int d = 0; d < 3; ++d) rb[d] = Mg[d];
+    for (int d = 0; d < 3; ++d) cb[d] = vb[d] - (A[d][0] * rb[0] + A[d][1] * rb[1] + A[d][2] * rb[2]);
+}
+
 }  // namespace f64
 
 __device__ __forceinline__ void store64(const Vertex64Params& P, uint32_t r, unsigned int t, const double x[3]) {
@@ -506,6 +665,269 @@ k_tri_fp64(Tri64Params P) {
         o[0] = rr[0]; o[1] = flip0 ? rr[2] : rr[1]; o[2] = flip0 ? rr[1] : rr[2];
         o[3] = rr[0]; o[4] = flip1 ? rr[3] : rr[2]; o[5] = flip1 ? rr[2] : rr[3];
     }
+}
+
+// The adjoint runs in three passes. A grid edge with a crossing is shared by up to four active
+// cells, each of which has a row (its Hermite sample as Cell::update uses it) for it; the first
+// active cell around the edge (in the averaging's cell order, or the cell itself for an edge
+// that is not averaged) owns the edge and handles all its rows, so every sample is computed
+// once per pass.
+//   k_adjoint_owners thread per (cell, local edge): rows without a crossing cleared, owners listed
+//   k_adjoint_rows   four lanes per owner, one per cell of the edge: the edge's samples, the
+//                    average, and each cell's row (normal a, point b)
+//   k_adjoint_cells  thread per cell: the sums in edge order, the solve's adjoint, and per row
+//                    the gradients of its normal and point (written over the row)
+//   k_adjoint_push   four lanes per owner: back through the normalisations and the average to
+//                    the samples, and from them to the grid values
+namespace {
+
+__device__ __forceinline__ bool cell_active_bit(const AdjointParams& P, int i, int j, int k) {
+    const uint32_t w = __ldg(P.bits + ((long long)j + (long long)P.g.cy * k) * P.g.W + (i >> 5));
+    return (w >> (i & 31)) & 1u;
+}
+
+// The cells of edge e of cell (i,j,k) that have a row for it: n = 1 (the cell itself) for an
+// edge that is not averaged, else the four cells in averaging order with their activity. Returns
+// false when another cell owns the edge.
+struct EdgeGroup {
+    int n;
+    bool avg;
+    int cc[4][3];
+    int ex[4];
+    bool act[4];
+};
+
+__device__ bool edge_group(const AdjointParams& P, int i, int j, int k, int e, EdgeGroup& G) {
+    const bool inside = f64::edge_cells(P.g, i, j, k, e, G.cc, G.ex);
+    if (!inside) {
+        G.n = 1; G.avg = false;
+        G.cc[0][0] = i; G.cc[0][1] = j; G.cc[0][2] = k; G.ex[0] = e; G.act[0] = true;
+        return true;
+    }
+    G.n = 4;
+    int first = -1;
+    bool all = true;
+    for (int q = 0; q < 4; ++q) {
+        const bool own = G.cc[q][0] == i && G.cc[q][1] == j && G.cc[q][2] == k;
+        G.act[q] = own || cell_active_bit(P, G.cc[q][0], G.cc[q][1], G.cc[q][2]);
+        if (own) G.ex[q] = e;
+        if (G.act[q] && first < 0) first = q;
+        all = all && G.act[q];
+    }
+    G.avg = all;                 // all four active: each has a sample on the shared edge
+    return G.cc[first][0] == i && G.cc[first][1] == j && G.cc[first][2] == k;
+}
+
+__device__ __forceinline__ long long row_index(const AdjointParams& P, const int c[3], int ex) {
+    return 12LL * cell_rank(P.bits, P.super, P.g, c[0], c[1], c[2]) + ex;
+}
+
+}  // namespace
+
+// Rows without a crossing are cleared; rows that own their edge are listed.
+__global__ void __launch_bounds__(128)
+k_adjoint_owners(AdjointParams P) {
+    const long long nrow = 12 * P.nactive;
+    const int lane = threadIdx.x & 31;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    // warp-uniform loop: one atomic per warp appends the warp's owners
+    for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < nrow; base += stride) {
+        const long long t = base + lane;
+        bool own = false;
+        if (t < nrow) {
+            const long long r = t / 12;
+            const int e = (int)(t - 12 * r);
+            int i, j, k;
+            unpack_cell(P.list[r], i, j, k);
+            const int a = edge_a(e), b = edge_b(e);
+            const float fa = __ldg(P.g.v + pidx(P.g, i + corner_dx(a), j + corner_dy(a), k + corner_dz(a)));
+            const float fb = __ldg(P.g.v + pidx(P.g, i + corner_dx(b), j + corner_dy(b), k + corner_dz(b)));
+            if ((double)fa * (double)fb > 0.0) {
+                P.rows[t].flags = 0;
+            } else {
+                EdgeGroup G;
+                own = edge_group(P, i, j, k, e, G);
+            }
+        }
+        const uint32_t m = __ballot_sync(0xffffffffu, own);
+        if (m == 0) continue;
+        unsigned int first = 0;
+        if (lane == __ffs(m) - 1) first = atomicAdd(P.owner_count, (unsigned int)__popc(m));
+        first = __shfl_sync(0xffffffffu, first, __ffs(m) - 1);
+        if (own) P.owners[first + __popc(m & ((1u << lane) - 1u))] = (uint32_t)t;
+    }
+}
+
+// A quad of lanes per listed edge, lane q for cell q of the edge's group. Loops are warp-uniform
+// (the quad shuffles need every lane).
+struct QuadSlot {
+    EdgeGroup G;
+    bool valid, mine;
+    f64::Sample S;
+};
+
+__device__ void quad_load(const AdjointParams& P, long long o, long long count, int q, QuadSlot& Q) {
+    Q.valid = o < count;
+    Q.mine = false;
+    Q.S.t = Q.S.gn = 0.0;
+    for (int d = 0; d < 3; ++d) Q.S.p[d] = Q.S.g[d] = Q.S.n[d] = 0.0;
+    if (!Q.valid) return;
+    const long long t = P.owners[o];
+    const long long r = t / 12;
+    const int e = (int)(t - 12 * r);
+    int i, j, k;
+    unpack_cell(P.list[r], i, j, k);
+    edge_group(P, i, j, k, e, Q.G);
+    Q.mine = q < Q.G.n && Q.G.act[q];
+    if (!Q.mine) return;
+    f64::Cell64 X;
+    f64::load_cell(P.g, Q.G.cc[q][0], Q.G.cc[q][1], Q.G.cc[q][2], X);
+    f64::sample_fwd(X, Q.G.ex[q], Q.S);
+}
+
+// The normalised sum of the quad's non-zero sample normals, summed in cell order
+// (hermite_update.cpp:334-438); acc before normalisation in accum.
+__device__ void quad_average(const f64::Sample& S, int lane, double out[3], double accum[3]) {
+    double acc[3] = {0.0, 0.0, 0.0};
+    for (int u = 0; u < 4; ++u) {
+        double nu[3];
+        for (int d = 0; d < 3; ++d) nu[d] = f64::shfl_d(S.n[d], (lane & ~3) | u);
+        if (sqrt(f64::sq3(nu)) > 0) { acc[0] += nu[0]; acc[1] += nu[1]; acc[2] += nu[2]; }
+    }
+    for (int d = 0; d < 3; ++d) { accum[d] = acc[d]; out[d] = acc[d]; }
+    f64::normalize3(out);
+}
+
+__global__ void __launch_bounds__(128)
+k_adjoint_rows(AdjointParams P) {
+    const long long count = *P.owner_count;
+    const int lane = threadIdx.x & 31, q = lane & 3;
+    const long long stride = (long long)gridDim.x * blockDim.x / 4;
+    for (long long base = ((long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31)) / 4; base < count; base += stride) {
+        QuadSlot Q;
+        quad_load(P, base + (lane >> 2), count, q, Q);
+        double avgn[3], acc[3];
+        quad_average(Q.S, lane, avgn, acc);
+        if (!Q.mine) continue;
+        double n[3];
+        for (int d = 0; d < 3; ++d) n[d] = Q.G.avg ? avgn[d] : Q.S.n[d];
+        if (sqrt(f64::sq3(n)) > 0.0) f64::normalize3(n);      // Cell::update (Cell.cpp:298-311)
+        AdjointRow& R = P.rows[row_index(P, Q.G.cc[q], Q.G.ex[q])];
+        for (int d = 0; d < 3; ++d) { R.a[d] = n[d]; R.b[d] = Q.S.p[d]; }
+        R.flags = 1;
+    }
+}
+
+__global__ void __launch_bounds__(128)
+k_adjoint_cells(AdjointParams P) {
+    for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < P.nactive;
+         r += (long long)gridDim.x * blockDim.x) {
+        AdjointRow* rows = P.rows + 12 * r;
+        const double vb[3] = {P.dV[3 * r], P.dV[3 * r + 1], P.dV[3 * r + 2]};
+        if (vb[0] == 0.0 && vb[1] == 0.0 && vb[2] == 0.0) {
+            for (int e = 0; e < 12; ++e) rows[e].flags = 0;
+            continue;
+        }
+        double A[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, ATb[3] = {0, 0, 0}, c[3] = {0, 0, 0};
+        int m = 0;
+        for (int e = 0; e < 12; ++e) {                   // edge order = the CPU's std::map order
+            const AdjointRow& R = rows[e];
+            if (!R.flags) continue;
+            const double bb = R.a[0] * R.b[0] + R.a[1] * R.b[1] + R.a[2] * R.b[2];
+            for (int x = 0; x < 3; ++x) {
+                for (int y = 0; y < 3; ++y) A[x][y] += R.a[x] * R.a[y];
+                ATb[x] += R.a[x] * bb;
+            }
+            for (int d = 0; d < 3; ++d) c[d] += R.b[d];
+            ++m;
+        }
+        if (m == 0) continue;
+        for (int d = 0; d < 3; ++d) c[d] /= double(m);
+        double Ab[3][3], rb[3], cb[3];
+        f64::qef_adjoint(A, ATb, c, P.thr, vb, Ab, rb, cb);
+        for (int e = 0; e < 12; ++e) {
+            AdjointRow& R = rows[e];
+            if (!R.flags) continue;
+            const double n[3] = {R.a[0], R.a[1], R.a[2]};
+            double pc[3];
+            for (int d = 0; d < 3; ++d) pc[d] = R.b[d] - c[d];
+            const double npc = n[0] * pc[0] + n[1] * pc[1] + n[2] * pc[2];
+            const double rn = rb[0] * n[0] + rb[1] * n[1] + rb[2] * n[2];
+            for (int d = 0; d < 3; ++d) {
+                R.a[d] = 2.0 * (Ab[d][0] * n[0] + Ab[d][1] * n[1] + Ab[d][2] * n[2]) + npc * rb[d] + rn * pc[d];
+                R.b[d] = rn * n[d] + cb[d] / double(m);
+            }
+            R.flags = 2;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(128)
+k_adjoint_push(AdjointParams P) {
+    const long long count = *P.owner_count;
+    const int lane = threadIdx.x & 31, q = lane & 3;
+    const long long stride = (long long)gridDim.x * blockDim.x / 4;
+    for (long long base = ((long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31)) / 4; base < count; base += stride) {
+        QuadSlot Q;
+        quad_load(P, base + (lane >> 2), count, q, Q);
+        double avgn[3], acc[3];
+        quad_average(Q.S, lane, avgn, acc);
+        const bool avg = Q.valid && Q.G.avg;
+        // this lane's row gradients, back through Cell::update's normalisation
+        double nbar[3] = {0.0, 0.0, 0.0}, pb[3] = {0.0, 0.0, 0.0};
+        if (Q.mine) {
+            const AdjointRow& R = P.rows[row_index(P, Q.G.cc[q], Q.G.ex[q])];
+            if (R.flags == 2) {
+                double npre[3];
+                for (int d = 0; d < 3; ++d) { npre[d] = avg ? avgn[d] : Q.S.n[d]; pb[d] = R.b[d]; }
+                const double npn = sqrt(f64::sq3(npre));
+                if (npn > 0.0) {
+                    const double n[3] = {npre[0] / npn, npre[1] / npn, npre[2] / npn};
+                    const double tt = n[0] * R.a[0] + n[1] * R.a[1] + n[2] * R.a[2];
+                    for (int d = 0; d < 3; ++d) nbar[d] = (R.a[d] - n[d] * tt) / npn;
+                } else {
+                    for (int d = 0; d < 3; ++d) nbar[d] = R.a[d];
+                }
+            }
+        }
+        // averaged edge: n_pre = normalize(acc) is shared, so its gradient is the quad's sum
+        double sum[3] = {0.0, 0.0, 0.0};
+        for (int u = 0; u < 4; ++u)
+            for (int d = 0; d < 3; ++d) sum[d] += f64::shfl_d(nbar[d], (lane & ~3) | u);
+        if (!Q.mine) continue;
+        if (avg) {
+            const double accn = sqrt(f64::sq3(acc));
+            const bool used = sqrt(f64::sq3(Q.S.n)) > 0;
+            double ab[3] = {0.0, 0.0, 0.0};
+            if (accn > 0.0 && used) {
+                const double tt = avgn[0] * sum[0] + avgn[1] * sum[1] + avgn[2] * sum[2];
+                for (int d = 0; d < 3; ++d) ab[d] = (sum[d] - avgn[d] * tt) / accn;
+            }
+            for (int d = 0; d < 3; ++d) nbar[d] = ab[d];
+        }
+        const bool any = nbar[0] != 0.0 || nbar[1] != 0.0 || nbar[2] != 0.0 || pb[0] != 0.0 || pb[1] != 0.0 ||
+                         pb[2] != 0.0;
+        if (!any) continue;
+        f64::Cell64 X;
+        f64::load_cell(P.g, Q.G.cc[q][0], Q.G.cc[q][1], Q.G.cc[q][2], X);
+        f64::sample_bwd(P.g, X, Q.G.cc[q][0], Q.G.cc[q][1], Q.G.cc[q][2], Q.G.ex[q], Q.S, nbar, pb, P.dgrid);
+    }
+}
+
+cudaError_t launch_vertex_adjoint(const AdjointParams& P, int num_sms, cudaStream_t s) {
+    if (P.nactive <= 0) return cudaSuccess;
+    const long long cap = (long long)num_sms * 32;
+    const long long rb = std::min(cap, (12 * P.nactive + 127) / 128);
+    const long long cb = std::min(cap, (P.nactive + 127) / 128);
+    cudaError_t err = cudaMemsetAsync(P.owner_count, 0, sizeof(unsigned int), s);
+    if (err != cudaSuccess) return err;
+    // owners <= rows with a crossing; a quad of lanes each
+    const long long qb = std::min(cap, (4 * 12 * P.nactive / 3 + 127) / 128 + 1);
+    k_adjoint_owners<<<(unsigned)rb, 128, 0, s>>>(P);
+    k_adjoint_rows<<<(unsigned)qb, 128, 0, s>>>(P);
+    k_adjoint_cells<<<(unsigned)cb, 128, 0, s>>>(P);
+    k_adjoint_push<<<(unsigned)qb, 128, 0, s>>>(P);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_tri_fp64(const Tri64Params& P, long long max_items, int num_sms, cudaStream_t s) {
