@@ -23,7 +23,7 @@
 extern "C" {
 #endif
 
-#define DCB_ABI_VERSION 1
+#define DCB_ABI_VERSION 2
 
 enum dcb_status {
     DCB_OK = 0,
@@ -69,6 +69,14 @@ typedef struct {
                                      of svd_threshold (rank decision ambiguous in FP32)  */
     int emit_triangles;           /* 0: quads (DualContouringMesh), 1: triangulate_v1     */
     int force_fp64;               /* 1: every cell takes the FP64 path (testing)          */
+    /* DCB_METHOD_OURS only (ContouringOptions, contouring.h:27-41): */
+    int hermite_update;           /* default 1: PCA update of Hermite normals and points   */
+    int batch_size;               /* default 200000: spheres per outer iteration at least */
+    double new_hermite_pos_weight;    /* default 0.2 */
+    double new_face_pos_weight;       /* default 0.2 */
+    double new_hermite_normal_weight; /* default 0.2 */
+    uint64_t seed;                /* random fill of the sphere batch (the reference draws
+                                     from std::random_device; here it is seeded)          */
 } dcb_opts;
 
 /* Fill `o` with the reference defaults (contouring.h:27-41) and the B200 knobs. */

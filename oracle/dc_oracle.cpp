@@ -252,6 +252,84 @@ struct Result {
 
 }  // namespace
 
+// extract_mesh_from_cells quads (contouring.cpp:607-729) from vertices V: X edges, then Y, then
+// Z; i outermost, k innermost. Each i-slice is produced independently and concatenated.
+static void emit_quads(const Grid& g, const std::vector<int32_t>& vid, const double* V, int nth,
+                       std::vector<int32_t>& F) {
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    const int cx = nx - 1, cy = ny - 1, cz = nz - 1;
+    (void)nth; (void)ny; (void)nz;
+    auto vcell = [&](int a, int b, int c) -> int32_t {
+        if (a < 0 || a >= cx || b < 0 || b >= cy || c < 0 || c >= cz) return -1;
+        return vid[g.cidx(a, b, c)];
+    };
+    auto emit = [&](std::vector<int32_t>& out, int i0, int j0, int k0, int i1, int j1, int k1,
+                    int32_t c0, int32_t c1, int32_t c2, int32_t c3) {
+        double g0[3], g1[3];
+        grid_gradient(g, i0, j0, k0, g0);
+        grid_gradient(g, i1, j1, k1, g1);
+        double gn[3] = {g0[0] + g1[0], g0[1] + g1[1], g0[2] + g1[2]};
+        const double* pa = &V[3 * (int64_t)c0];
+        const double* pb = &V[3 * (int64_t)c1];
+        const double* pc = &V[3 * (int64_t)c2];
+        const double* pd = &V[3 * (int64_t)c3];
+        double ba[3] = {pb[0] - pa[0], pb[1] - pa[1], pb[2] - pa[2]};
+        double da[3] = {pd[0] - pa[0], pd[1] - pa[1], pd[2] - pa[2]};
+        double qn[3];
+        cross3(ba, da, qn);
+        if (sqnorm3(qn) < 1e-24) {
+            double ca[3] = {pc[0] - pa[0], pc[1] - pa[1], pc[2] - pa[2]};
+            cross3(ca, da, qn);
+        }
+        if (sqnorm3(gn) > 0 && sqnorm3(qn) > 0) {
+            if (dot3(qn, gn) < 0.0) std::swap(c1, c3);
+        }
+        out.push_back(c0); out.push_back(c1); out.push_back(c2); out.push_back(c3);
+    };
+    auto sc = [&](int i0, int j0, int k0, int i1, int j1, int k1) {
+        double s0 = g.S(i0, j0, k0), s1 = g.S(i1, j1, k1);
+        return s0 * s1 < 0.0;
+    };
+    for (int axis = 0; axis < 3; ++axis) {
+        int ilo = axis == 0 ? 0 : 1;
+        std::vector<std::vector<int32_t>> parts(cx);
+#pragma omp parallel for num_threads(nth) schedule(dynamic, 1)
+        for (int i = ilo; i < cx; ++i) {
+            auto& out = parts[i];
+            if (axis == 0) {
+                for (int j = 1; j < cy; ++j)
+                    for (int k = 1; k < cz; ++k) {
+                        if (!sc(i, j, k, i + 1, j, k)) continue;
+                        int32_t c0 = vcell(i, j - 1, k - 1), c1 = vcell(i, j, k - 1);
+                        int32_t c2 = vcell(i, j, k), c3 = vcell(i, j - 1, k);
+                        if (c0 < 0 || c1 < 0 || c2 < 0 || c3 < 0) continue;
+                        emit(out, i, j, k, i + 1, j, k, c0, c1, c2, c3);
+                    }
+            } else if (axis == 1) {
+                for (int j = 0; j < cy; ++j)
+                    for (int k = 1; k < cz; ++k) {
+                        if (!sc(i, j, k, i, j + 1, k)) continue;
+                        int32_t c0 = vcell(i - 1, j, k - 1), c1 = vcell(i, j, k - 1);
+                        int32_t c2 = vcell(i, j, k), c3 = vcell(i - 1, j, k);
+                        if (c0 < 0 || c1 < 0 || c2 < 0 || c3 < 0) continue;
+                        emit(out, i, j, k, i, j + 1, k, c0, c1, c2, c3);
+                    }
+            } else {
+                for (int j = 1; j < cy; ++j)
+                    for (int k = 0; k < cz; ++k) {
+                        if (!sc(i, j, k, i, j, k + 1)) continue;
+                        int32_t c0 = vcell(i - 1, j - 1, k), c1 = vcell(i, j - 1, k);
+                        int32_t c2 = vcell(i, j, k), c3 = vcell(i - 1, j, k);
+                        if (c0 < 0 || c1 < 0 || c2 < 0 || c3 < 0) continue;
+                        emit(out, i, j, k, i, j, k + 1, c0, c1, c2, c3);
+                    }
+            }
+        }
+        for (auto& p : parts) F.insert(F.end(), p.begin(), p.end());
+    }
+
+}
+
 extern "C" {
 
 typedef struct {
@@ -270,7 +348,7 @@ typedef struct {
 static void* extract_impl(int nx, int ny, int nz, float vx, float vy, float vz,
                           float ox, float oy, float oz, const double* px, const double* py,
                           const double* pz, const float* values, double svd_threshold,
-                          int threads, dco_stats* st);
+                          int threads, dco_stats* st, std::vector<Hermite>* keep_hermite = nullptr);
 
 void* dco_extract(int nx, int ny, int nz, float vx, float vy, float vz,
                   float ox, float oy, float oz, const float* values,
@@ -296,7 +374,7 @@ void* dco_extract_pos(int nx, int ny, int nz, const double* px, const double* py
 static void* extract_impl(int nx, int ny, int nz, float vx, float vy, float vz,
                           float ox, float oy, float oz, const double* px, const double* py,
                           const double* pz, const float* values, double svd_threshold,
-                          int threads, dco_stats* st) {
+                          int threads, dco_stats* st, std::vector<Hermite>* keep_hermite) {
     if (nx < 2 || ny < 2 || nz < 2 || !values) return nullptr;
     auto t0 = std::chrono::high_resolution_clock::now();
 #ifdef _OPENMP
@@ -412,78 +490,11 @@ static void* extract_impl(int nx, int ny, int nz, float vx, float vy, float vz,
         for (int e = 0; e < 12; ++e) m += (H[r].mask >> e) & 1;
         R->nrows[r] = m;
     }
-    H.clear(); H.shrink_to_fit();
+    if (keep_hermite) *keep_hermite = std::move(H);
+    else { H.clear(); H.shrink_to_fit(); }
 
-    // 5) extract_mesh_from_cells quads (contouring.cpp:607-729): X edges, then Y, then Z;
-    //    i outermost, k innermost. Each i-slice is produced independently and concatenated.
-    auto vcell = [&](int a, int b, int c) -> int32_t {
-        if (a < 0 || a >= cx || b < 0 || b >= cy || c < 0 || c >= cz) return -1;
-        return vid[g.cidx(a, b, c)];
-    };
-    auto emit = [&](std::vector<int32_t>& out, int i0, int j0, int k0, int i1, int j1, int k1,
-                    int32_t c0, int32_t c1, int32_t c2, int32_t c3) {
-        double g0[3], g1[3];
-        grid_gradient(g, i0, j0, k0, g0);
-        grid_gradient(g, i1, j1, k1, g1);
-        double gn[3] = {g0[0] + g1[0], g0[1] + g1[1], g0[2] + g1[2]};
-        const double* pa = &R->V[3 * (int64_t)c0];
-        const double* pb = &R->V[3 * (int64_t)c1];
-        const double* pc = &R->V[3 * (int64_t)c2];
-        const double* pd = &R->V[3 * (int64_t)c3];
-        double ba[3] = {pb[0] - pa[0], pb[1] - pa[1], pb[2] - pa[2]};
-        double da[3] = {pd[0] - pa[0], pd[1] - pa[1], pd[2] - pa[2]};
-        double qn[3];
-        cross3(ba, da, qn);
-        if (sqnorm3(qn) < 1e-24) {
-            double ca[3] = {pc[0] - pa[0], pc[1] - pa[1], pc[2] - pa[2]};
-            cross3(ca, da, qn);
-        }
-        if (sqnorm3(gn) > 0 && sqnorm3(qn) > 0) {
-            if (dot3(qn, gn) < 0.0) std::swap(c1, c3);
-        }
-        out.push_back(c0); out.push_back(c1); out.push_back(c2); out.push_back(c3);
-    };
-    auto sc = [&](int i0, int j0, int k0, int i1, int j1, int k1) {
-        double s0 = g.S(i0, j0, k0), s1 = g.S(i1, j1, k1);
-        return s0 * s1 < 0.0;
-    };
-    for (int axis = 0; axis < 3; ++axis) {
-        int ilo = axis == 0 ? 0 : 1;
-        std::vector<std::vector<int32_t>> parts(cx);
-#pragma omp parallel for num_threads(nth) schedule(dynamic, 1)
-        for (int i = ilo; i < cx; ++i) {
-            auto& out = parts[i];
-            if (axis == 0) {
-                for (int j = 1; j < cy; ++j)
-                    for (int k = 1; k < cz; ++k) {
-                        if (!sc(i, j, k, i + 1, j, k)) continue;
-                        int32_t c0 = vcell(i, j - 1, k - 1), c1 = vcell(i, j, k - 1);
-                        int32_t c2 = vcell(i, j, k), c3 = vcell(i, j - 1, k);
-                        if (c0 < 0 || c1 < 0 || c2 < 0 || c3 < 0) continue;
-                        emit(out, i, j, k, i + 1, j, k, c0, c1, c2, c3);
-                    }
-            } else if (axis == 1) {
-                for (int j = 0; j < cy; ++j)
-                    for (int k = 1; k < cz; ++k) {
-                        if (!sc(i, j, k, i, j + 1, k)) continue;
-                        int32_t c0 = vcell(i - 1, j, k - 1), c1 = vcell(i, j, k - 1);
-                        int32_t c2 = vcell(i, j, k), c3 = vcell(i - 1, j, k);
-                        if (c0 < 0 || c1 < 0 || c2 < 0 || c3 < 0) continue;
-                        emit(out, i, j, k, i, j + 1, k, c0, c1, c2, c3);
-                    }
-            } else {
-                for (int j = 1; j < cy; ++j)
-                    for (int k = 0; k < cz; ++k) {
-                        if (!sc(i, j, k, i, j, k + 1)) continue;
-                        int32_t c0 = vcell(i - 1, j - 1, k), c1 = vcell(i, j - 1, k);
-                        int32_t c2 = vcell(i, j, k), c3 = vcell(i - 1, j, k);
-                        if (c0 < 0 || c1 < 0 || c2 < 0 || c3 < 0) continue;
-                        emit(out, i, j, k, i, j, k + 1, c0, c1, c2, c3);
-                    }
-            }
-        }
-        for (auto& p : parts) R->F.insert(R->F.end(), p.begin(), p.end());
-    }
+    // 5) extract_mesh_from_cells quads (contouring.cpp:607-729).
+    emit_quads(g, vid, R->V.data(), nth, R->F);
 
     auto t1 = std::chrono::high_resolution_clock::now();
     R->ms = std::chrono::duration<double, std::milli>(t1 - t0).count();

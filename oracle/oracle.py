@@ -19,6 +19,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 _DC_LIB = os.path.join(_HERE, "_build", "libdc_oracle.so")
 _MTS_LIB = os.path.join(_HERE, "_build", "libmts_oracle.so")
 _ADJ_LIB = os.path.join(_HERE, "_build", "libdc_adjoint_oracle.so")
+_OURS_LIB = os.path.join(_HERE, "_build", "libours_oracle.so")
 _libs = {}
 
 
@@ -281,3 +282,45 @@ def vertex_vjp(values, dims, axes, cells, grad_vertices, svd_threshold=0.01, thr
     out = np.zeros(nx * ny * nz, np.float64)
     np.add.at(out, (gi + nx * (gj + ny * gk))[inside], contrib[inside])
     return out
+
+
+class _OursOpts(ctypes.Structure):
+    _fields_ = [("outer_iters", ctypes.c_int), ("inner_iters", ctypes.c_int), ("mu", ctypes.c_double),
+                ("dc_weight", ctypes.c_double), ("sphere_weight", ctypes.c_double),
+                ("svd_threshold", ctypes.c_double), ("hermite_update", ctypes.c_int), ("batch_size", ctypes.c_int),
+                ("new_hermite_pos_weight", ctypes.c_double), ("new_face_pos_weight", ctypes.c_double),
+                ("new_hermite_normal_weight", ctypes.c_double), ("seed", ctypes.c_uint64)]
+
+
+def ours(values, dims, spacing, origin, outer_iters=100, inner_iters=100, mu=0.1, dc_weight=0.02,
+         sphere_weight=1.0, svd_threshold=0.01, hermite_update=True, batch_size=200000,
+         new_hermite_pos_weight=0.2, new_face_pos_weight=0.2, new_hermite_normal_weight=0.2, seed=0x5eed,
+         threads=0):
+    """The restated outer/inner refinement (ContouringMethod::Ours) on a dense float32 grid:
+    dict with FP64 vertices ``V``, wound quads ``F`` and the active ``cells``."""
+    lib = _load(_OURS_LIB)
+    if not getattr(lib, "_typed", False):
+        lib.dco_ours.restype = ctypes.c_void_p
+        lib.dco_ours.argtypes = [ctypes.c_int] * 3 + [ctypes.c_float] * 6 + [
+            ctypes.c_void_p, ctypes.POINTER(_OursOpts), ctypes.c_int, ctypes.POINTER(_Stats)]
+        lib.dco_num_vertices.restype = ctypes.c_int64
+        lib.dco_num_vertices.argtypes = [ctypes.c_void_p]
+        lib.dco_num_faces.restype = ctypes.c_int64
+        lib.dco_num_faces.argtypes = [ctypes.c_void_p]
+        lib.dco_copy.restype = None
+        lib.dco_copy.argtypes = [ctypes.c_void_p] * 6
+        lib.dco_free.restype = None
+        lib.dco_free.argtypes = [ctypes.c_void_p]
+        lib._typed = True
+    nx, ny, nz = (int(d) for d in dims)
+    vals = np.ascontiguousarray(np.asarray(values, dtype=np.float32).reshape(-1))
+    if vals.size != nx * ny * nz:
+        raise ValueError("shape mismatch")
+    o = _OursOpts(int(outer_iters), int(inner_iters), float(mu), float(dc_weight), float(sphere_weight),
+                  float(svd_threshold), int(bool(hermite_update)), int(batch_size), float(new_hermite_pos_weight),
+                  float(new_face_pos_weight), float(new_hermite_normal_weight), int(seed))
+    st = _Stats()
+    h = lib.dco_ours(nx, ny, nz, float(spacing[0]), float(spacing[1]), float(spacing[2]),
+                     float(origin[0]), float(origin[1]), float(origin[2]), vals.ctypes.data, ctypes.byref(o),
+                     int(threads), ctypes.byref(st))
+    return _collect(lib, h, st)

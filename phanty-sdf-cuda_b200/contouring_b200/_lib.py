@@ -43,7 +43,9 @@ class DcbOpts(ctypes.Structure):
                 ("mu", ctypes.c_double), ("dc_weight", ctypes.c_double), ("sphere_weight", ctypes.c_double),
                 ("svd_threshold", ctypes.c_double), ("fp64_escalation_cond", ctypes.c_double),
                 ("fp64_threshold_band", ctypes.c_double), ("emit_triangles", ctypes.c_int),
-                ("force_fp64", ctypes.c_int)]
+                ("force_fp64", ctypes.c_int), ("hermite_update", ctypes.c_int), ("batch_size", ctypes.c_int),
+                ("new_hermite_pos_weight", ctypes.c_double), ("new_face_pos_weight", ctypes.c_double),
+                ("new_hermite_normal_weight", ctypes.c_double), ("seed", ctypes.c_uint64)]
 
 
 class DcbStats(ctypes.Structure):

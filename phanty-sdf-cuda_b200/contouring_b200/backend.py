@@ -52,6 +52,7 @@ class ContouringOptions:
             self.fp64_threshold_band = 0.01
         self.emit_triangles = False
         self.force_fp64 = False
+        self.seed = 0x5eed
 
     def to_c(self):
         o = _lib.default_opts()
@@ -68,6 +69,12 @@ class ContouringOptions:
         o.fp64_threshold_band = float(self.fp64_threshold_band)
         o.emit_triangles = 1 if self.emit_triangles else 0
         o.force_fp64 = 1 if self.force_fp64 else 0
+        o.hermite_update = 1 if self.hermite_update else 0
+        o.batch_size = int(self.batch_size)
+        o.new_hermite_pos_weight = float(self.new_hermite_pos_weight)
+        o.new_face_pos_weight = float(self.new_face_pos_weight)
+        o.new_hermite_normal_weight = float(self.new_hermite_normal_weight)
+        o.seed = int(self.seed)
         return o
 
 

@@ -57,7 +57,7 @@ struct dcb_context {
     cudaEvent_t ev[8] = {};
     DevBuf grid, bits, super, list, seg_count, seg_start, counters, V, vclass, fmask, col_count, col_fill,
         col_start, partials, esc_list, hard_list, hard_data, stage_quad, stage_key, faces, wind_items,
-        v64_index, v64_cells, V64, tris, tri_items, adj_rows, adj_owners;
+        v64_index, v64_cells, V64, tris, tri_items, adj_rows, adj_owners, ours_ws;
     // mesh -> SDF workspace
     DevBuf m_verts, m_faces, m_out, m_tris, m_bin_count, m_bin_start, m_bin_fill, m_bin_scratch, m_bin_tris,
         m_bin_active, m_active_list, m_axis_start, m_far, m_ext, m_tmp, m_partials, m_counters;
@@ -465,6 +465,87 @@ int run_pipeline(dcb_context* h, const dcb_grid* in, const dcb_opts* o, cudaStre
     return run_batch(h, in, 1, o, s, st);
 }
 
+// The outer/inner refinement (contouring.cpp:1255-1328): a dual-contouring extraction, then
+// the refinement of its vertices; the mesh's topology is the extraction's.
+int run_ours(dcb_context* h, const dcb_grid* in, const dcb_opts* o, cudaStream_t s, dcb_stats* st) {
+    if (o->outer_iters < 0 || o->inner_iters < 0 || o->batch_size < 0 || !(o->mu >= 0.0) ||
+        !std::isfinite(o->dc_weight) || !(o->sphere_weight >= 0.0) || !std::isfinite(o->new_face_pos_weight) ||
+        !std::isfinite(o->new_hermite_pos_weight) || !std::isfinite(o->new_hermite_normal_weight))
+        return fail(h, DCB_ERR_INVALID_ARGUMENT, "invalid refinement options");
+    dcb_opts dc = *o;
+    dc.method = DCB_METHOD_DUAL_CONTOURING;
+    dc.emit_triangles = 0;
+    int rc = run_batch(h, in, 1, &dc, s, st);
+    if (rc != DCB_OK) return rc;
+    const long long nv = h->nv, nq = h->nf;
+    const long long npts = (long long)in->nx * in->ny * in->nz;
+    if (npts >= 0xffffffffLL) return fail(h, DCB_ERR_TOO_LARGE, "grid too large for the refinement");
+    BatchLayout L;
+    rc = layout_batch(h, in, 1, L);
+    if (rc != DCB_OK) return rc;
+    size_t cub_bytes = 0;
+    const size_t ws = ours_workspace_bytes(nv, nq, npts, &cub_bytes);
+    DCB_TRY(h, ensure(h->ours_ws, ws), "alloc refinement workspace");
+    const bool tri = o->emit_triangles != 0;
+    if (tri) DCB_TRY(h, ensure(h->tris, sizeof(int32_t) * 6 * (size_t)std::max(1LL, nq)), "alloc triangles");
+    OursRun R;
+    std::memset(&R, 0, sizeof(R));
+    OursParams& P = R.P;
+    P.g = L.slots[0].g;
+    P.list = as<uint64_t>(h->list);
+    P.nv = nv;
+    P.bits = as<uint32_t>(h->bits);
+    P.super = as<uint32_t>(h->super);
+    P.dc_faces = as<int4>(h->faces);
+    P.nq = nq;
+    P.out_V = as<float>(h->V);
+    P.out_faces = tri ? as<int4>(h->tris) : as<int4>(h->faces);
+    // cell_diagonal (contouring.cpp:788-804) over the float grid positions
+    const int n3[3] = {in->nx, in->ny, in->nz};
+    const float o3[3] = {in->ox, in->oy, in->oz}, v3[3] = {in->vx, in->vy, in->vz};
+    double hmin = 0.0;
+    for (int a = 0; a < 3; ++a) {
+        const double p0 = (double)(o3[a] + (float)0 * v3[a]);
+        const double p1 = (double)(o3[a] + (float)(n3[a] - 1) * v3[a]);
+        const double mn = std::min(p0, p1), mx = std::max(p0, p1);
+        P.gmin[a] = mn;
+        P.gd[a] = (mx - mn) / (double)(n3[a] - 1);
+        P.lo[a] = mn;
+        P.hi[a] = mx > mn ? mx : mn + 1.0;
+        hmin = a == 0 ? P.gd[a] : std::min(hmin, P.gd[a]);
+    }
+    P.cell_diag = hmin * std::sqrt(3.0);
+    P.inner_iters = o->inner_iters;
+    P.mu = o->mu;
+    P.dc_weight = o->dc_weight;
+    P.sphere_weight = o->sphere_weight;
+    P.thr = o->svd_threshold;
+    P.wface = o->new_face_pos_weight;
+    P.wnormal = o->new_hermite_normal_weight;
+    P.wpos = o->new_hermite_pos_weight;
+    Counters* dc_counters = as<Counters>(h->counters);
+    P.err = &dc_counters->err;
+    R.workspace = h->ours_ws.p;
+    R.cub_bytes = cub_bytes;
+    R.outer_iters = o->outer_iters;
+    R.hermite_update = o->hermite_update;
+    R.batch_size = o->batch_size;
+    R.seed = o->seed;
+    R.triangles = tri ? 1 : 0;
+    R.num_sms = h->num_sms;
+    DCB_TRY(h, cudaMemsetAsync(&dc_counters->err, 0, sizeof(int), s), "clear error flag");
+    DCB_TRY(h, ours_run(R, s), "refinement");
+    Counters* hc = reinterpret_cast<Counters*>(h->h_counters);
+    DCB_TRY(h, cudaMemcpyAsync(hc, dc_counters, sizeof(Counters), cudaMemcpyDeviceToHost, s), "read counters");
+    DCB_TRY(h, cudaEventRecord(h->ev[4], s), "event");
+    DCB_TRY(h, cudaStreamSynchronize(s), "refinement");
+    if (hc->err) return fail(h, DCB_ERR_INTERNAL, "refinement: BVH traversal stack overflow");
+    h->vpf = tri ? 3 : 4;
+    h->nf = tri ? 2 * nq : nq;
+    if (st) { st->face_count = h->nf; st->vertex_count = nv; }
+    return DCB_OK;
+}
+
 void fill_times(dcb_context* h, dcb_stats* st, bool upload) {
     if (!st) return;
     st->upload_ms = upload ? elapsed(h->ev[0], h->ev[1]) : 0.f;
@@ -595,6 +676,12 @@ void dcb_default_opts(dcb_opts* o) {
     o->fp64_threshold_band = 0.01;
     o->emit_triangles = 0;
     o->force_fp64 = 0;
+    o->hermite_update = 1;
+    o->batch_size = 200000;
+    o->new_hermite_pos_weight = 0.2;
+    o->new_face_pos_weight = 0.2;
+    o->new_hermite_normal_weight = 0.2;
+    o->seed = 0x5eed;
 }
 
 int dcb_abi_version(void) { return DCB_ABI_VERSION; }
@@ -643,7 +730,7 @@ int dcb_destroy(dcb_handle h) {
                       &h->tris, &h->tri_items, &h->m_verts, &h->m_faces, &h->m_out, &h->m_tris,
                       &h->m_bin_count, &h->m_bin_start, &h->m_bin_fill, &h->m_bin_scratch, &h->m_bin_tris,
                       &h->m_bin_active, &h->m_active_list, &h->m_axis_start, &h->m_far, &h->m_ext, &h->m_tmp,
-                      &h->m_partials, &h->m_counters, &h->table, &h->cell_slot, &h->adj_rows, &h->adj_owners};
+                      &h->m_partials, &h->m_counters, &h->table, &h->cell_slot, &h->adj_rows, &h->adj_owners, &h->ours_ws};
     for (DevBuf* b : bufs) if (b->p) cudaFree(b->p);
     if (h->h_counters) cudaFreeHost(h->h_counters);
     if (h->h_sdf_counters) cudaFreeHost(h->h_sdf_counters);
@@ -663,14 +750,15 @@ int dcb_extract_device(dcb_handle h, const dcb_grid* grid, const dcb_opts* opts,
     dcb_opts def;
     dcb_default_opts(&def);
     const dcb_opts* o = opts ? opts : &def;
-    if (o->method != DCB_METHOD_DUAL_CONTOURING) return fail(h, DCB_ERR_NOT_SUPPORTED, "only dual contouring is implemented");
+    if (o->method != DCB_METHOD_DUAL_CONTOURING && o->method != DCB_METHOD_OURS)
+        return fail(h, DCB_ERR_NOT_SUPPORTED, "unknown method");
     if (!(o->svd_threshold >= 0.0)) return fail(h, DCB_ERR_INVALID_ARGUMENT, "svd_threshold must be >= 0");
     if (cudaSetDevice(h->device) != cudaSuccess) { cudaGetLastError(); return fail(h, DCB_ERR_CUDA, "set device"); }
     cudaStream_t s = reinterpret_cast<cudaStream_t>(cuda_stream);
     if (stats) std::memset(stats, 0, sizeof(*stats));
     DCB_TRY(h, cudaEventRecord(h->ev[0], s), "event");
     DCB_TRY(h, cudaEventRecord(h->ev[1], s), "event");
-    rc = run_pipeline(h, grid, o, s, stats);
+    rc = o->method == DCB_METHOD_OURS ? run_ours(h, grid, o, s, stats) : run_pipeline(h, grid, o, s, stats);
     if (rc != DCB_OK) return rc;
     fill_times(h, stats, false);
     if (stats) stats->total_ms = elapsed(h->ev[1], h->ev[4]);
@@ -696,7 +784,8 @@ int dcb_extract_batch_device(dcb_handle h, const dcb_grid* grids, int n, const d
     dcb_opts def;
     dcb_default_opts(&def);
     const dcb_opts* o = opts ? opts : &def;
-    if (o->method != DCB_METHOD_DUAL_CONTOURING) return fail(h, DCB_ERR_NOT_SUPPORTED, "only dual contouring is implemented");
+    if (o->method != DCB_METHOD_DUAL_CONTOURING)
+        return fail(h, DCB_ERR_NOT_SUPPORTED, "batches run dual contouring only");
     if (!(o->svd_threshold >= 0.0)) return fail(h, DCB_ERR_INVALID_ARGUMENT, "svd_threshold must be >= 0");
     if (cudaSetDevice(h->device) != cudaSuccess) { cudaGetLastError(); return fail(h, DCB_ERR_CUDA, "set device"); }
     cudaStream_t s = reinterpret_cast<cudaStream_t>(cuda_stream);
@@ -727,7 +816,9 @@ int dcb_extract_host(dcb_handle h, const dcb_grid* grid, const dcb_opts* opts, d
     dcb_opts def;
     dcb_default_opts(&def);
     const dcb_opts* o = opts ? opts : &def;
-    if (o->method != DCB_METHOD_DUAL_CONTOURING) return fail(h, DCB_ERR_NOT_SUPPORTED, "only dual contouring is implemented");
+    if (o->method != DCB_METHOD_DUAL_CONTOURING && o->method != DCB_METHOD_OURS)
+        return fail(h, DCB_ERR_NOT_SUPPORTED, "unknown method");
+    if (!(o->svd_threshold >= 0.0)) return fail(h, DCB_ERR_INVALID_ARGUMENT, "svd_threshold must be >= 0");
     cudaStream_t s = reinterpret_cast<cudaStream_t>(cuda_stream);
     if (stats) std::memset(stats, 0, sizeof(*stats));
     const size_t npts = (size_t)grid->nx * grid->ny * grid->nz;
@@ -737,7 +828,7 @@ int dcb_extract_host(dcb_handle h, const dcb_grid* grid, const dcb_opts* opts, d
     DCB_TRY(h, cudaEventRecord(h->ev[1], s), "event");
     dcb_grid dg = *grid;
     dg.values = as<float>(h->grid);
-    rc = run_pipeline(h, &dg, o, s, stats);
+    rc = o->method == DCB_METHOD_OURS ? run_ours(h, &dg, o, s, stats) : run_pipeline(h, &dg, o, s, stats);
     if (rc != DCB_OK) return rc;
     DCB_TRY(h, ensure_host(h->hV, h->hV_bytes, sizeof(float) * 3 * h->nv), "alloc host vertices");
     DCB_TRY(h, ensure_host(h->hF, h->hF_bytes, sizeof(int32_t) * h->vpf * h->nf), "alloc host faces");
@@ -805,7 +896,7 @@ int dcb_backward(dcb_handle h, const dcb_grid* grid, const dcb_opts* opts, const
     dcb_opts def;
     dcb_default_opts(&def);
     const dcb_opts* o = opts ? opts : &def;
-    if (o->method != DCB_METHOD_DUAL_CONTOURING) return fail(h, DCB_ERR_NOT_SUPPORTED, "only dual contouring is implemented");
+    if (o->method != DCB_METHOD_DUAL_CONTOURING) return fail(h, DCB_ERR_NOT_SUPPORTED, "the adjoint covers dual contouring only");
     if (!(o->svd_threshold >= 0.0)) return fail(h, DCB_ERR_INVALID_ARGUMENT, "svd_threshold must be >= 0");
     if (h->batch_n != 1 || h->cx != grid->nx - 1 || h->cy != grid->ny - 1)
         return fail(h, DCB_ERR_INVALID_ARGUMENT, "backward needs the grid of the last single-grid extraction");

@@ -237,6 +237,68 @@ struct AdjointParams {
 };
 cudaError_t launch_vertex_adjoint(const AdjointParams& P, int num_sms, cudaStream_t s);
 
+// ---- outer/inner vertex refinement (dcb_ours.cu) ----
+// FP64 state of one active cell (the Cell members the refinement uses, Cell.h:44-115).
+struct OursCell {
+    double v[3];          // vertex
+    double hp[12][3];     // Hermite points, by local edge
+    double hn[12][3];     // Hermite normals
+    double fi[6][3];      // face points, by face (0:+X 1:-X 2:+Y 3:-Y 4:+Z 5:-Z)
+    int hmask;            // edges with a Hermite sample
+    int fmask;            // faces with a point
+};
+struct OursParams {
+    GridDesc g;
+    const uint64_t* list;
+    long long nv;
+    const uint32_t* bits;
+    const uint32_t* super;
+    const int4* dc_faces;           // the extraction's quads
+    long long nq;
+    float* out_V;                   // [3 nv] refined vertices
+    int4* out_faces;                // [nq] quads, or [2 nq] triangles (6 ints per quad)
+    double lo[3], hi[3];            // box of the Morton codes
+    double gmin[3], gd[3];          // grid minimum and cell size (cell_diagonal, contouring.cpp:788-804)
+    double cell_diag;
+    int inner_iters;
+    double mu, dc_weight, sphere_weight, thr, wface, wnormal, wpos;
+    int* err;
+    // workspace (set by ours_run)
+    OursCell* cells;
+    double* Vm;                     // [3 nv] the current mesh's vertices
+    int4* quads;                    // [nq] canonical cell order of each quad
+    double* gsum;                   // [3 nq] gradient sums of the quads' grid edges
+    const uint32_t* sel;            // selected grid points (sphere centres)
+    long long nsel;
+    int* sel_cell;                  // [nsel] cell rank or -1
+    unsigned int* cell_count;
+    unsigned int* cell_start;
+    unsigned int* cell_fill;
+    uint32_t* cell_spheres;         // grid points by cell, by radius
+    long long nt;                   // triangles
+    unsigned long long* mkeys;
+    unsigned long long* mkeys_sorted;
+    int2* child;                    // internal nodes: children (< 0: ~leaf)
+    int* parent;                    // [2 nt]: internal nodes, then leaves at nt - 1 + leaf
+    float4* bmin;
+    float4* bmax;
+    unsigned int* flags;
+    double* tri9;                   // [9 nt] triangle vertices
+};
+struct OursRun {
+    OursParams P;
+    void* workspace;
+    size_t cub_bytes;
+    int outer_iters;
+    int hermite_update;
+    long long batch_size;
+    unsigned long long seed;
+    int triangles;
+    int num_sms;
+};
+size_t ours_workspace_bytes(long long nv, long long nq, long long npts, size_t* cub_bytes);
+cudaError_t ours_run(OursRun& R, cudaStream_t s);
+
 // ---- mesh -> SDF (dcb_mesh_sdf.cu) ----
 struct SdfParams {
     int nx, ny, nz;
