@@ -453,11 +453,19 @@ void* dco_ours(int nx, int ny, int nz, float vx, float vy, float vz, float ox, f
             }
             for (int d = 0; d < 3; ++d) cen[d] /= double(m);
             double v[3] = {S.v[0], S.v[1], S.v[2]};
+            const size_t nsph = S.spheres.size(), cs = (nsph + 31) / 32;
             for (int iter = 0; iter < o->inner_iters; ++iter) {
                 const double prev[3] = {v[0], v[1], v[2]};
                 double A[3][3], b[3];
                 for (int a = 0; a < 3; ++a) { b[a] = h0[a]; for (int c = 0; c < 3; ++c) A[a][c] = H0[a][c]; }
-                for (int64_t gidx : S.spheres) {
+                // sphere rows summed in 32 chunks of consecutive spheres, each from zero,
+                // added in chunk order (the engine's order, for a thread or a warp per cell)
+                for (size_t l = 0; l < 32; ++l) {
+                    const size_t lo = l * cs, hi = std::min(nsph, lo + cs);
+                    if (lo >= hi) break;
+                    double PA[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, Pb[3] = {0, 0, 0};
+                    for (size_t si = lo; si < hi; ++si) {
+                    const int64_t gidx = S.spheres[si];
                     double c[3];
                     point(gidx, c);
                     const double sval = (double)values[gidx];
@@ -498,8 +506,13 @@ void* dco_ours(int nx, int ny, int nz, float vx, float vy, float vz, float ox, f
                     for (int a = 0; a < 3; ++a) row[a] = alpha * ssw * dv[a];
                     const double rb = ssw * ((dot3(q, dv) - beta * dot3(Hp, dv)) - gamma * dot3(Fp, dv));
                     for (int a = 0; a < 3; ++a) {
-                        for (int c2 = 0; c2 < 3; ++c2) A[a][c2] += row[a] * row[c2];
-                        b[a] += row[a] * rb;
+                        for (int c2 = 0; c2 < 3; ++c2) PA[a][c2] += row[a] * row[c2];
+                        Pb[a] += row[a] * rb;
+                    }
+                    }
+                    for (int a = 0; a < 3; ++a) {
+                        for (int c2 = 0; c2 < 3; ++c2) A[a][c2] += PA[a][c2];
+                        b[a] += Pb[a];
                     }
                 }
                 for (int a = 0; a < 3; ++a) { A[a][a] += smu * smu; b[a] += smu * (smu * prev[a]); }

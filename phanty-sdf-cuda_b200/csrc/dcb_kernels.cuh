@@ -275,6 +275,8 @@ struct OursParams {
     unsigned int* cell_start;
     unsigned int* cell_fill;
     uint32_t* cell_spheres;         // grid points by cell, by radius
+    uint32_t* heavy;                // cells with many spheres (a warp each)
+    unsigned int* heavy_count;
     long long nt;                   // triangles
     unsigned long long* mkeys;
     unsigned long long* mkeys_sorted;

@@ -192,6 +192,9 @@ __device__ __forceinline__ unsigned long long splitmix64(unsigned long long x) {
 
 }  // namespace
 
+// Cells with at least this many spheres run their inner loop on a warp (a chunk per lane).
+constexpr unsigned int kWarpCellSpheres = 8;
+
 // ---- setup -------------------------------------------------------------------------------
 
 // Per cell: Hermite points and normals as the refinement starts (after Cell::update and the
@@ -516,6 +519,7 @@ __global__ void __launch_bounds__(128) k_ours_scatter(OursParams P) {
 __global__ void __launch_bounds__(128) k_ours_sort(OursParams P) {
     for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < P.nv; r += (long long)gridDim.x * blockDim.x) {
         const unsigned int n = P.cell_count[r];
+        if (n >= kWarpCellSpheres) P.heavy[atomicAdd(P.heavy_count, 1u)] = (uint32_t)r;
         if (n < 2) continue;
         uint32_t* a = P.cell_spheres + P.cell_start[r];
         auto less = [&](uint32_t x, uint32_t y) {
@@ -654,120 +658,194 @@ __global__ void __launch_bounds__(128) k_ours_hermite(OursParams P) {
     }
 }
 
+// One sphere's row of Cell::minimize_qef (Cell.cpp:400-446) for a cell whose vertex is prev:
+// its closest point on the local fan (first minimum in fan order), the point on the sphere,
+// the barycentric blend of (vertex, Hermite point, face point). False if the row is skipped.
+__device__ bool sphere_row(const OursParams& P, const OursCell& S, const int* fan, int nfan, const double* prev,
+                           uint32_t gidx, double ssw, double row[3], double& rb) {
+    double c[3];
+    point_of(P.g, gidx, c);
+    const double sval = (double)__ldg(P.g.v + gidx);
+    const double rs = fabs(sval);
+    double best = DBL_MAX, tm[3] = {0, 0, 0};
+    int bf = 0;
+    for (int f = 0; f < nfan; ++f) {
+        const int e = fan[f] & 15, d = fan[f] >> 4;
+        double q[3];
+        tri_closest(c, prev, S.hp[e], S.fi[d], q);
+        double dd[3] = {q[0] - c[0], q[1] - c[1], q[2] - c[2]};
+        const double d2 = dot3(dd, dd);
+        if (d2 < best) { best = d2; bf = f; tm[0] = q[0]; tm[1] = q[1]; tm[2] = q[2]; }
+    }
+    const int e = fan[bf] & 15, d = fan[bf] >> 4;
+    const double* Hp = S.hp[e];
+    const double* Fp = S.fi[d];
+    double ct[3];
+    for (int a = 0; a < 3; ++a) ct[a] = tm[a] - c[a];
+    const double rho0 = norm3(ct);
+    double qs[3];
+    if (rho0 < 1e-9) for (int a = 0; a < 3; ++a) qs[a] = c[a];
+    else for (int a = 0; a < 3; ++a) qs[a] = c[a] + (ct[a] / rho0) * rs;
+    double bc[3];
+    barycentric(tm, prev, Hp, Fp, bc);
+    double alpha = bc[0], beta = bc[1], gamma = bc[2];
+    if (fabs(alpha) < 1e-6) { alpha = 1.0; beta = 0.0; gamma = 0.0; }
+    double tt[3], ctt[3];
+    for (int a = 0; a < 3; ++a) { tt[a] = alpha * prev[a] + beta * Hp[a] + gamma * Fp[a]; ctt[a] = tt[a] - c[a]; }
+    const double rho = norm3(ctt);
+    double qc[3];
+    for (int a = 0; a < 3; ++a) qc[a] = qs[a] - c[a];
+    const double radius = norm3(qc);
+    if (rho > radius && sval < 0.0) return false;          // sign -1 (Cell.cpp:419-426)
+    double q[3];
+    if (rho < 1e-9) for (int a = 0; a < 3; ++a) q[a] = c[a];
+    else for (int a = 0; a < 3; ++a) q[a] = c[a] + (ctt[a] / rho) * radius;
+    double dv[3];
+    for (int a = 0; a < 3; ++a) dv[a] = q[a] - c[a];
+    for (int a = 0; a < 3; ++a) row[a] = alpha * ssw * dv[a];
+    rb = ssw * ((dot3(q, dv) - beta * dot3(Hp, dv)) - gamma * dot3(Fp, dv));
+    return true;
+}
+
+// Sphere rows of one chunk, summed in order from zero: 6 entries of the symmetric A^T A
+// (00 01 02 11 12 22) and 3 of A^T b.
+__device__ void chunk_sums(const OursParams& P, const OursCell& S, const int* fan, int nfan, const double* prev,
+                           const uint32_t* sph, unsigned int lo, unsigned int hi, double ssw, double acc[9]) {
+    for (int q = 0; q < 9; ++q) acc[q] = 0.0;
+    for (unsigned int s = lo; s < hi; ++s) {
+        double row[3], rb;
+        if (!sphere_row(P, S, fan, nfan, prev, sph[s], ssw, row, rb)) continue;
+        acc[0] += row[0] * row[0]; acc[1] += row[0] * row[1]; acc[2] += row[0] * row[2];
+        acc[3] += row[1] * row[1]; acc[4] += row[1] * row[2]; acc[5] += row[2] * row[2];
+        acc[6] += row[0] * rb; acc[7] += row[1] * rb; acc[8] += row[2] * rb;
+    }
+}
+
+// The local fan of a cell: (vertex, Hermite point on edge e, face point d) for each face d
+// with a point and each of its four edges with a Hermite point, in face then edge order.
+__device__ int cell_fan(const OursCell& S, int fan[24]) {
+    int nfan = 0;
+    for (int d = 0; d < 6; ++d) {
+        if (!(S.fmask & (1 << d))) continue;
+        for (int u = 0; u < 4; ++u) {
+            const int e = edge_of_corners(kFaceCorners[d][u], kFaceCorners[d][(u + 1) & 3]);
+            if (e >= 0 && (S.hmask & (1 << e))) fan[nfan++] = e | (d << 4);
+        }
+    }
+    return nfan;
+}
+
+// The Hermite rows dc_weight * n_e in edge order and the Hermite centroid.
+__device__ void hermite_rows(const OursParams& P, const OursCell& S, double H0[9], double cen[3]) {
+    for (int q = 0; q < 9; ++q) H0[q] = 0.0;
+    cen[0] = cen[1] = cen[2] = 0.0;
+    int m = 0;
+    for (int e = 0; e < 12; ++e) {
+        if (!(S.hmask & (1 << e))) continue;
+        double sn[3];
+        for (int d = 0; d < 3; ++d) sn[d] = P.dc_weight * S.hn[e][d];
+        const double b = dot3(sn, S.hp[e]);
+        H0[0] += sn[0] * sn[0]; H0[1] += sn[0] * sn[1]; H0[2] += sn[0] * sn[2];
+        H0[3] += sn[1] * sn[1]; H0[4] += sn[1] * sn[2]; H0[5] += sn[2] * sn[2];
+        H0[6] += sn[0] * b; H0[7] += sn[1] * b; H0[8] += sn[2] * b;
+        for (int d = 0; d < 3; ++d) cen[d] += S.hp[e][d];
+        ++m;
+    }
+    for (int d = 0; d < 3; ++d) cen[d] /= double(m);
+}
+
+// solve_quadratic_system (Cell.cpp:324-361) with the proximal rows sqrt(mu) * I added.
+__device__ void inner_solve(const OursParams& P, const double Acc[9], const double* prev, const double cen[3],
+                            double smu, double x[3]) {
+    double A[3][3] = {{Acc[0], Acc[1], Acc[2]}, {Acc[1], Acc[3], Acc[4]}, {Acc[2], Acc[4], Acc[5]}};
+    double b[3] = {Acc[6], Acc[7], Acc[8]};
+    for (int a = 0; a < 3; ++a) { A[a][a] += smu * smu; b[a] += smu * (smu * prev[a]); }
+    double E[3][3], U[3][3];
+    for (int a = 0; a < 3; ++a) for (int c = 0; c < 3; ++c) E[a][c] = A[a][c];
+    f64::jacobi3(E, U);
+    double rhs[3];
+    for (int a = 0; a < 3; ++a) rhs[a] = b[a] - (A[a][0] * cen[0] + A[a][1] * cen[1] + A[a][2] * cen[2]);
+    x[0] = cen[0]; x[1] = cen[1]; x[2] = cen[2];
+    for (int q = 0; q < 3; ++q) {
+        const double sv = fabs(E[q][q]);
+        if (sv > P.thr) {
+            const double coef = (U[0][q] * rhs[0] + U[1][q] * rhs[1] + U[2][q] * rhs[2]) / sv;
+            for (int a = 0; a < 3; ++a) x[a] += U[a][q] * coef;
+        }
+    }
+}
+
 // The inner loop of one cell (contouring.cpp:1288-1309): refine_vertex_from_face_intersections
 // (vertex_refinement.cpp:201-280) + Cell::minimize_qef (Cell.cpp:364-473) until the vertex
-// moves less than 1e-6.
+// moves less than 1e-6. The sphere rows are summed in 32 chunks of consecutive spheres, each
+// from zero, added in chunk order: the same sums whether a thread or a warp computes them.
 __global__ void __launch_bounds__(128) k_ours_inner(OursParams P) {
     for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < P.nv; r += (long long)gridDim.x * blockDim.x) {
         OursCell& S = P.cells[r];
-        const int hmask = S.hmask, fmask = S.fmask;
         const unsigned int nsph = P.cell_count[r];
-        if (!fmask || !nsph || !hmask) continue;
-        // the local fan: (vertex, Hermite point on edge e, face point d) for each face d with a
-        // point and each of its four edges with a Hermite point, in face then edge order
+        if (!S.fmask || !nsph || !S.hmask || nsph >= kWarpCellSpheres) continue;
         int fan[24];
-        int nfan = 0;
-        for (int d = 0; d < 6; ++d) {
-            if (!(fmask & (1 << d))) continue;
-            for (int u = 0; u < 4; ++u) {
-                const int e = edge_of_corners(kFaceCorners[d][u], kFaceCorners[d][(u + 1) & 3]);
-                if (e >= 0 && (hmask & (1 << e))) fan[nfan++] = e | (d << 4);
-            }
-        }
+        const int nfan = cell_fan(S, fan);
         if (!nfan) continue;
         const uint32_t* sph = P.cell_spheres + P.cell_start[r];
-        // constant rows: dc_weight * n_e (Hermite, edge order); centroid of the Hermite points
-        double H0[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, h0[3] = {0, 0, 0}, cen[3] = {0, 0, 0};
-        int m = 0;
-        for (int e = 0; e < 12; ++e) {
-            if (!(hmask & (1 << e))) continue;
-            double sn[3];
-            for (int d = 0; d < 3; ++d) sn[d] = P.dc_weight * S.hn[e][d];
-            const double b = dot3(sn, S.hp[e]);
-            for (int a = 0; a < 3; ++a) {
-                for (int c = 0; c < 3; ++c) H0[a][c] += sn[a] * sn[c];
-                h0[a] += sn[a] * b;
-            }
-            for (int d = 0; d < 3; ++d) cen[d] += S.hp[e][d];
-            ++m;
-        }
-        for (int d = 0; d < 3; ++d) cen[d] /= double(m);
+        double H0[9], cen[3];
+        hermite_rows(P, S, H0, cen);
         const double ssw = sqrt(P.sphere_weight), smu = sqrt(P.mu);
+        const unsigned int cs = (nsph + 31) / 32;
         double v[3] = {S.v[0], S.v[1], S.v[2]};
         for (int it = 0; it < P.inner_iters; ++it) {
             const double prev[3] = {v[0], v[1], v[2]};
-            double A[3][3], b[3];
-            for (int a = 0; a < 3; ++a) { b[a] = h0[a]; for (int c = 0; c < 3; ++c) A[a][c] = H0[a][c]; }
-            for (unsigned int s = 0; s < nsph; ++s) {
-                const uint32_t gidx = sph[s];
-                double c[3];
-                point_of(P.g, gidx, c);
-                const double sval = (double)__ldg(P.g.v + gidx);
-                const double rs = fabs(sval);
-                // closest point of the fan to the sphere centre (first minimum in fan order)
-                double best = DBL_MAX, tm[3] = {0, 0, 0};
-                int bf = 0;
-                for (int f = 0; f < nfan; ++f) {
-                    const int e = fan[f] & 15, d = fan[f] >> 4;
-                    double q[3];
-                    tri_closest(c, prev, S.hp[e], S.fi[d], q);
-                    double dd[3] = {q[0] - c[0], q[1] - c[1], q[2] - c[2]};
-                    const double d2 = dot3(dd, dd);
-                    if (d2 < best) { best = d2; bf = f; tm[0] = q[0]; tm[1] = q[1]; tm[2] = q[2]; }
-                }
-                const int e = fan[bf] & 15, d = fan[bf] >> 4;
-                const double* Hp = S.hp[e];
-                const double* Fp = S.fi[d];
-                double ct[3];
-                for (int a = 0; a < 3; ++a) ct[a] = tm[a] - c[a];
-                const double rho0 = norm3(ct);
-                double qs[3];
-                if (rho0 < 1e-9) for (int a = 0; a < 3; ++a) qs[a] = c[a];
-                else for (int a = 0; a < 3; ++a) qs[a] = c[a] + (ct[a] / rho0) * rs;
-                double bc[3];
-                barycentric(tm, prev, Hp, Fp, bc);
-                // the sphere's row of minimize_qef
-                double alpha = bc[0], beta = bc[1], gamma = bc[2];
-                if (fabs(alpha) < 1e-6) { alpha = 1.0; beta = 0.0; gamma = 0.0; }
-                double tt[3], ctt[3];
-                for (int a = 0; a < 3; ++a) { tt[a] = alpha * prev[a] + beta * Hp[a] + gamma * Fp[a]; ctt[a] = tt[a] - c[a]; }
-                const double rho = norm3(ctt);
-                double qc[3];
-                for (int a = 0; a < 3; ++a) qc[a] = qs[a] - c[a];
-                const double radius = norm3(qc);
-                if (rho > radius && sval < 0.0) continue;          // sign -1 (contouring.cpp:893)
-                double q[3];
-                if (rho < 1e-9) for (int a = 0; a < 3; ++a) q[a] = c[a];
-                else for (int a = 0; a < 3; ++a) q[a] = c[a] + (ctt[a] / rho) * radius;
-                double dv[3], row[3];
-                for (int a = 0; a < 3; ++a) dv[a] = q[a] - c[a];
-                for (int a = 0; a < 3; ++a) row[a] = alpha * ssw * dv[a];
-                const double rb = ssw * ((dot3(q, dv) - beta * dot3(Hp, dv)) - gamma * dot3(Fp, dv));
-                for (int a = 0; a < 3; ++a) {
-                    for (int c2 = 0; c2 < 3; ++c2) A[a][c2] += row[a] * row[c2];
-                    b[a] += row[a] * rb;
-                }
+            double Acc[9];
+            for (int q = 0; q < 9; ++q) Acc[q] = H0[q];
+            for (unsigned int l = 0; l < 32; ++l) {
+                const unsigned int lo = l * cs, hi = min(nsph, lo + cs);
+                if (lo >= hi) break;
+                double part[9];
+                chunk_sums(P, S, fan, nfan, prev, sph, lo, hi, ssw, part);
+                for (int q = 0; q < 9; ++q) Acc[q] += part[q];
             }
-            for (int a = 0; a < 3; ++a) { A[a][a] += smu * smu; b[a] += smu * (smu * prev[a]); }
-            // solve_quadratic_system (Cell.cpp:324-361): truncated pseudo-inverse about the centroid
-            double E[3][3], U[3][3];
-            for (int a = 0; a < 3; ++a) for (int c = 0; c < 3; ++c) E[a][c] = A[a][c];
-            f64::jacobi3(E, U);
-            double rhs[3];
-            for (int a = 0; a < 3; ++a) rhs[a] = b[a] - (A[a][0] * cen[0] + A[a][1] * cen[1] + A[a][2] * cen[2]);
-            double x[3] = {cen[0], cen[1], cen[2]};
-            for (int q = 0; q < 3; ++q) {
-                const double sv = fabs(E[q][q]);
-                if (sv > P.thr) {
-                    const double coef = (U[0][q] * rhs[0] + U[1][q] * rhs[1] + U[2][q] * rhs[2]) / sv;
-                    for (int a = 0; a < 3; ++a) x[a] += U[a][q] * coef;
-                }
-            }
-            for (int a = 0; a < 3; ++a) v[a] = x[a];
+            inner_solve(P, Acc, prev, cen, smu, v);
             double dm[3] = {v[0] - prev[0], v[1] - prev[1], v[2] - prev[2]};
             if (norm3(dm) < 1e-6) break;
         }
         for (int a = 0; a < 3; ++a) S.v[a] = v[a];
+    }
+}
+
+// The same inner loop for the cells with many spheres, a warp per cell.
+__global__ void __launch_bounds__(128) k_ours_inner_warp(OursParams P) {
+    const int lane = threadIdx.x & 31;
+    const unsigned int nheavy = *P.heavy_count;
+    for (long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < nheavy;
+         w += ((long long)gridDim.x * blockDim.x) >> 5) {
+        const long long r = P.heavy[w];
+        OursCell& S = P.cells[r];
+        const unsigned int nsph = P.cell_count[r];
+        if (!S.fmask || !S.hmask) continue;                  // warp-uniform
+        int fan[24];
+        const int nfan = cell_fan(S, fan);
+        if (!nfan) continue;
+        const uint32_t* sph = P.cell_spheres + P.cell_start[r];
+        double H0[9], cen[3];
+        hermite_rows(P, S, H0, cen);
+        const double ssw = sqrt(P.sphere_weight), smu = sqrt(P.mu);
+        const unsigned int cs = (nsph + 31) / 32;
+        const unsigned int lo = min(nsph, lane * cs), hi = min(nsph, lo + cs);
+        double v[3] = {S.v[0], S.v[1], S.v[2]};
+        for (int it = 0; it < P.inner_iters; ++it) {
+            const double prev[3] = {v[0], v[1], v[2]};
+            double part[9];
+            chunk_sums(P, S, fan, nfan, prev, sph, lo, hi, ssw, part);
+            double Acc[9];
+            for (int q = 0; q < 9; ++q) Acc[q] = H0[q];
+            const int nchunks = (int)((nsph + cs - 1) / cs);      // warp-uniform
+            for (int l = 0; l < nchunks; ++l)
+                for (int q = 0; q < 9; ++q) Acc[q] += __shfl_sync(0xffffffffu, part[q], l);
+            inner_solve(P, Acc, prev, cen, smu, v);
+            double dm[3] = {v[0] - prev[0], v[1] - prev[1], v[2] - prev[2]};
+            if (norm3(dm) < 1e-6) break;
+        }
+        if (lane == 0) for (int a = 0; a < 3; ++a) S.v[a] = v[a];
     }
 }
 
@@ -814,13 +892,17 @@ size_t ours_workspace_bytes(long long nv, long long nq, long long npts, size_t* 
                                    (int)std::max(1LL, nt));
     cub::DeviceRadixSort::SortPairs(nullptr, tb2, (unsigned long long*)nullptr, (unsigned long long*)nullptr,
                                     (uint32_t*)nullptr, (uint32_t*)nullptr, (int)std::max(1LL, npts));
-    *cub_bytes = std::max(tb1, tb2);
+    size_t tb3 = 0;
+    cub::DeviceRadixSort::SortKeys(nullptr, tb3, (uint32_t*)nullptr, (uint32_t*)nullptr, (int)std::max(1LL, npts));
+    *cub_bytes = std::max(tb1, std::max(tb2, tb3));
     size_t b = 0;
     b += al(sizeof(OursCell) * nv) + al(sizeof(double) * 3 * nv);            // cells, Vm
     b += al(sizeof(int4) * nq) + al(sizeof(double) * 3 * nq);               // quads, gsum
     b += 3 * al(sizeof(uint32_t) * npts) + al(sizeof(int) * npts);           // sel, band/rest, sel_cell
     b += al(sizeof(unsigned long long) * npts) * 2 + al(sizeof(uint32_t) * npts);  // fill keys/values
     b += 3 * al(sizeof(unsigned int) * (nv + 1)) + al(sizeof(uint32_t) * npts);    // count/start/fill, spheres
+    b += al(sizeof(uint32_t) * (nv + 1));                                    // cells with many spheres
+    b += al(sizeof(uint32_t) * npts);                                        // selected points, sorted
     b += 2 * al(sizeof(unsigned long long) * nt) + al(sizeof(int2) * nt) + al(sizeof(int) * 2 * nt);
     b += 2 * al(sizeof(float4) * 2 * nt) + al(sizeof(unsigned int) * nt) + al(sizeof(double) * 9 * nt);
     b += al(sizeof(uint32_t) * (scan_partials_len(nv + 1) + 1)) + al(64);    // scan partials, counters
@@ -849,6 +931,7 @@ cudaError_t ours_run(OursRun& R, cudaStream_t s) {
     P.cell_start = (unsigned int*)take(sizeof(unsigned int) * (nv + 1));
     P.cell_fill = (unsigned int*)take(sizeof(unsigned int) * (nv + 1));
     P.cell_spheres = (uint32_t*)take(sizeof(uint32_t) * npts);
+    P.heavy = (uint32_t*)take(sizeof(uint32_t) * (nv + 1));
     P.mkeys = (unsigned long long*)take(sizeof(unsigned long long) * nt);
     P.mkeys_sorted = (unsigned long long*)take(sizeof(unsigned long long) * nt);
     P.child = (int2*)take(sizeof(int2) * nt);
@@ -860,7 +943,9 @@ cudaError_t ours_run(OursRun& R, cudaStream_t s) {
     uint32_t* partials = (uint32_t*)take(sizeof(uint32_t) * (scan_partials_len(nv + 1) + 1));
     unsigned int* counters = (unsigned int*)take(64);
     void* cub_temp = take(R.cub_bytes);
-    P.sel = sel;
+    uint32_t* sel_sorted = (uint32_t*)take(sizeof(uint32_t) * npts);
+    P.heavy_count = counters + 8;
+    P.sel = sel_sorted;
     P.nt = nt;
     const int sms = R.num_sms;
     cudaError_t e;
@@ -893,8 +978,12 @@ cudaError_t ours_run(OursRun& R, cudaStream_t s) {
                 OURS_TRY(cub::DeviceRadixSort::SortPairs(cub_temp, tb2, fk, fk2, rest, fv2, (int)nrest, 0, 64, s));
                 OURS_TRY(cudaMemcpyAsync(sel + nband, fv2, sizeof(uint32_t) * nfill, cudaMemcpyDeviceToDevice, s));
             }
+            // query in grid order: neighbouring threads walk the same part of the tree
+            size_t tb3 = R.cub_bytes;
+            OURS_TRY(cub::DeviceRadixSort::SortKeys(cub_temp, tb3, sel, sel_sorted, (int)P.nsel, 0, 32, s));
             OURS_TRY(cudaMemsetAsync(P.cell_count, 0, sizeof(unsigned int) * (nv + 1), s));
             OURS_TRY(cudaMemsetAsync(P.cell_fill, 0, sizeof(unsigned int) * (nv + 1), s));
+            OURS_TRY(cudaMemsetAsync(P.heavy_count, 0, sizeof(unsigned int), s));
             k_ours_query<<<grid_for(P.nsel, 128, sms), 128, 0, s>>>(P);
             OURS_TRY(launch_scan(P.cell_count, nv, partials, P.cell_start,
                                  reinterpret_cast<unsigned long long*>(counters + 4), s));
@@ -902,10 +991,12 @@ cudaError_t ours_run(OursRun& R, cudaStream_t s) {
             k_ours_sort<<<grid_for(nv, 128, sms), 128, 0, s>>>(P);
         } else {
             OURS_TRY(cudaMemsetAsync(P.cell_count, 0, sizeof(unsigned int) * (nv + 1), s));
+            OURS_TRY(cudaMemsetAsync(P.heavy_count, 0, sizeof(unsigned int), s));
         }
         k_ours_faces<<<grid_for(nv, 128, sms), 128, 0, s>>>(P);
         if (R.hermite_update && it > 0) k_ours_hermite<<<grid_for(12 * nv, 128, sms), 128, 0, s>>>(P);
         k_ours_inner<<<grid_for(nv, 128, sms), 128, 0, s>>>(P);
+        k_ours_inner_warp<<<grid_for(32 * nv, 128, sms), 128, 0, s>>>(P);
         k_ours_mesh<<<grid_for(nv, 128, sms), 128, 0, s>>>(P);
         OURS_TRY(cudaGetLastError());
     }
