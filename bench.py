@@ -242,6 +242,112 @@ def run_batch_workload(args):
     return 0
 
 
+def _timed(fn, steps, warmup):
+    """CUDA-event milliseconds per call of fn on the current stream, after warm-up."""
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def _side_line(metric, value, unit, ms, args, config, **extra):
+    line = {"metric": metric, "value": round(value, 3), "unit": unit, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if "ours" in metric or "fwd_bwd" in metric else "f32",
+            "data": "synthetic", "config": config}
+    line.update(extra)
+    print(json.dumps(line), flush=True)
+
+
+def run_adjoint_workload(args):
+    """The differentiable workload: a 128^3 sphere (r = 0.3) perturbed by 64 Gaussian RBFs; a
+    step is the extraction, the gradient of the mean squared distance from the vertices to their
+    nearest of 50,000 points on a second perturbed sphere (nearest points found once, then held
+    fixed), and the adjoint into a dense d(loss)/d(grid)."""
+    import torch
+    from contouring_b200 import B200DualContouringBackend, DenseSdfGridDevice, synth
+    torch.cuda.set_device(0)
+    vals, dims, sp, org = synth.rbf_sphere(128, device="cuda")
+    T = torch.from_numpy(synth.rbf_sphere_points(50000, seed=1)).cuda().float()
+    be = B200DualContouringBackend(0)
+    g = DenseSdfGridDevice(*dims, *sp, *org, d_values=vals)
+    V, F, st = be.extract_tensor(vals, dims, sp, org)
+    nn = torch.cat([torch.cdist(V[a:a + 8192], T).argmin(1) for a in range(0, len(V), 8192)])
+    tgt = T[nn]
+    out = torch.empty(vals.numel(), dtype=torch.float32, device="cuda")
+    ncell = (dims[0] - 1) * (dims[1] - 1) * (dims[2] - 1)
+
+    def fwd():
+        be.extract_tensor_ptr(g)
+
+    def fwd_bwd():
+        Vt, _, _ = be.extract_tensor(vals, dims, sp, org)
+        dV = (2.0 / len(Vt)) * (Vt - tgt)
+        be.backward_tensor(vals, dims, sp, org, dV, out=out)
+
+    ms_f = _timed(fwd, args.steps, args.warmup)
+    ms_fb = _timed(fwd_bwd, args.steps, args.warmup)
+    _side_line("dc_fwd_bwd_mcells_per_s", ncell / (ms_fb / 1e3) / 1e6, "Mcells/s", ms_fb, args,
+               {"workload": "rbf_sphere128_adjoint", "grid": list(dims), "vertices": st.vertex_count,
+                "targets": 50000},
+               forward_ms=round(ms_f, 4), fwd_bwd_over_fwd=round(ms_fb / ms_f, 3), gpu_launches=KERNELS_PER_STEP + 5)
+    be.close()
+    return 0
+
+
+def run_ours_workload(args):
+    """The refinement (ContouringMethod::Ours, 100 outer x 100 inner iterations) of the 128^3
+    sphere (r = 0.35); a step is the extraction and its full refinement."""
+    import torch
+    from contouring_b200 import (B200DualContouringBackend, ContouringMethod, ContouringOptions,
+                                 DenseSdfGridDevice, synth)
+    torch.cuda.set_device(0)
+    vals, dims, sp, org = synth.sphere(128, radius=0.35, device="cuda")
+    be = B200DualContouringBackend(0)
+    o = ContouringOptions()
+    o.method = ContouringMethod.Ours
+    be.options = o
+    g = DenseSdfGridDevice(*dims, *sp, *org, d_values=vals)
+    st = be.extract_tensor_ptr(g)[2]
+    ms = _timed(lambda: be.extract_tensor_ptr(g), args.steps, args.warmup)
+    ncell = (dims[0] - 1) * (dims[1] - 1) * (dims[2] - 1)
+    _side_line("dc_ours_mcells_per_s", ncell / (ms / 1e3) / 1e6, "Mcells/s", ms, args,
+               {"workload": "sphere128_ours", "grid": list(dims), "outer_iters": o.outer_iters,
+                "inner_iters": o.inner_iters, "vertices": st.vertex_count})
+    be.close()
+    return 0
+
+
+def run_mesh_workload(args):
+    """mesh_to_sdf: 32 icospheres (163,840 triangles) into a 512^3 grid on the mesh's padded box;
+    a step is one conversion of device-resident vertices and faces."""
+    import torch
+    from contouring_b200 import B200DualContouringBackend, mesh_to_sdf_tensor, synth
+    torch.cuda.set_device(0)
+    V, F = synth.icosphere_scene()
+    dims, sp, org = synth.mesh_grid(V, 512)
+    Vd, Fd = torch.from_numpy(V).cuda(), torch.from_numpy(F).cuda()
+    be = B200DualContouringBackend(0)
+    out = torch.empty(dims[0] * dims[1] * dims[2], dtype=torch.float32, device="cuda")
+    ms = _timed(lambda: mesh_to_sdf_tensor(be, Vd, Fd, dims, org, sp, out=out), args.steps, args.warmup)
+    _, st = mesh_to_sdf_tensor(be, Vd, Fd, dims, org, sp, out=out)      # stage times of a warm call
+    npts = dims[0] * dims[1] * dims[2]
+    _side_line("mesh_to_sdf_mpoints_per_s", npts / (ms / 1e3) / 1e6, "Mpoints/s", ms, args,
+               {"workload": "icospheres32_mesh_to_sdf512", "grid": list(dims), "triangles": len(F)},
+               stage_ms={"bins": round(st.bins_ms, 4), "band": round(st.band_ms, 4), "sign": round(st.sign_ms, 4),
+                         "relax": round(st.relax_ms, 4)})
+    be.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -253,8 +359,10 @@ def main():
     ap.add_argument("--ref-zslab", type=int, default=96, help="point planes per CPU sample (over 8 slabs)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-sequential", action="store_true", help="batch256: skip the one-by-one comparison")
-    ap.add_argument("--workload", default="csg1024", choices=["csg1024", "batch256"],
-                    help="batch256: 256 uneven CSG grids batched vs one by one (not the headline)")
+    ap.add_argument("--workload", default="csg1024", choices=["csg1024", "batch256", "adjoint128", "ours128", "mesh512"],
+                    help="side workloads (not the headline): batch256 = 256 uneven CSG grids batched vs one "
+                         "by one; adjoint128 = forward + adjoint; ours128 = the full refinement; mesh512 = "
+                         "mesh_to_sdf")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -266,6 +374,12 @@ def main():
         return run_reference(args, rank, world)
     if args.workload == "batch256":
         return run_batch_workload(args)
+    if args.workload == "adjoint128":
+        return run_adjoint_workload(args)
+    if args.workload == "ours128":
+        return run_ours_workload(args)
+    if args.workload == "mesh512":
+        return run_mesh_workload(args)
 
     import numpy as np
     import torch
