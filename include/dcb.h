@@ -197,6 +197,15 @@ typedef struct {
 int dcb_extract_batch_device(dcb_handle h, const dcb_grid* grids, int n, const dcb_opts* opts,
                              dcb_batch_mesh* out, dcb_stats* stats, void* cuda_stream);
 
+/* Tile autotuner for the mark kernel (no counterpart in the reference): times the mark
+ * launches of these device grids (one batch) for every combination of CTAs per resident
+ * slot (waves 1, 2, 4, 8) and x-tile width (256-cell tiles for grids at most 0, 256, 512 or
+ * 1024 cells wide, 1024-cell tiles otherwise), and keeps the fastest for this handle's later
+ * extractions. The results of an extraction do not depend on the tiling. The chosen waves,
+ * width limit and the median mark time (ms) are returned through the optional pointers. */
+int dcb_autotune_mark(dcb_handle h, const dcb_grid* grids, int n, int* waves_out, int* narrow_cells_out,
+                      float* best_ms_out, void* cuda_stream);
+
 /* ---- mesh -> signed distance grid ------------------------------------------------------ */
 
 typedef struct {

@@ -282,6 +282,20 @@ class B200DualContouringBackend:
         self._generation += 1
         return out, DualContouringStats.from_c(st)
 
+    def autotune_mark(self, grids, stream=None):
+        """Time the mark kernel's tilings on ``grids`` = [(CUDA float32 values, dims, spacing,
+        origin)] and keep the fastest for this backend; returns (waves, narrow_cells, ms)."""
+        n = len(grids)
+        arr = (_lib.DcbGrid * n)()
+        for b, (values, dims, spacing, origin) in enumerate(grids):
+            d = DenseSdfGridDevice(*dims, *spacing, *origin, d_values=values)
+            arr[b] = self._grid_c(d, d.pointer())
+        w, nc, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_float()
+        s = _current_stream() if stream is None else stream
+        _lib.check(self._L.dcb_autotune_mark(self._h, arr, n, ctypes.byref(w), ctypes.byref(nc), ctypes.byref(ms),
+                                             ctypes.c_void_p(s)), self._h)
+        return w.value, nc.value, ms.value
+
     def extract_batch(self, grids, stream=None):
         """Batched extraction of ``grids`` = [(CUDA float32 values, dims, spacing, origin)] in one
         pass of the pipeline. Returns ``[(V (nv,3) float32, F (nf,vpf) int32)]`` CUDA tensors per

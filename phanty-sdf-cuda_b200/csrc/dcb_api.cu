@@ -68,6 +68,10 @@ struct dcb_context {
     int64_t nv = 0, nf = 0;           // vertices; output faces (quads or triangles)
     int vpf = 4;                      // output vertices per face
     int mark_ctas[2] = {0, 0};        // resident mark CTAs per SM (scalar, float4 loads)
+    // mark tiling (dcb_autotune_mark): CTAs per resident mark slot, and the widest grid
+    // (cells along x) that marches 256-cell x-tiles instead of 1024-cell ones
+    int tune_waves = 4;
+    int tune_narrow_cells = 256;
     int cx = 0, cy = 0;
     // batch layout table (device + pinned staging) and the last batch's per-grid offsets
     DevBuf table, cell_slot;
@@ -175,14 +179,14 @@ int layout_batch(dcb_context* h, const dcb_grid* in, int n, BatchLayout& L) {
         const long long rows = (long long)g.cy * g.cz;
         S.vec4 = (g.nx % 4 == 0 && (reinterpret_cast<uintptr_t>(g.v) % 16) == 0) ? 1 : 0;
         // grids at most 256 cells wide march 256-cell x-tiles (less idle width)
-        S.tw = g.cx <= 32 * mark_narrow_tile_words() ? mark_narrow_tile_words() : mark_tile_words();
+        S.tw = g.cx <= h->tune_narrow_cells ? mark_narrow_tile_words() : mark_tile_words();
         S.nxt = (g.cx + 32 * S.tw - 1) / (32 * S.tw);
         S.R = std::min(mark_max_rows(), g.cy);
         S.nrb = (g.cy + S.R - 1) / S.R;
         // About four CTAs per resident slot, each marching 8..64 planes (a single long wave
         // measured slower at 1024^3: 0.887 vs 0.848 ms).
         if (h->mark_ctas[S.vec4] == 0) h->mark_ctas[S.vec4] = mark_ctas_per_sm(S.vec4);
-        const long long slots = (long long)h->num_sms * h->mark_ctas[S.vec4] * 4;
+        const long long slots = (long long)h->num_sms * h->mark_ctas[S.vec4] * h->tune_waves;
         S.KZ = (int)std::max(8LL, std::min(64LL, (g.cz * S.nxt * (long long)S.nrb + slots - 1) / slots));
         S.nzc = (g.cz + S.KZ - 1) / S.KZ;
         S.bits_off = L.bits;
@@ -261,6 +265,19 @@ int upload_table(dcb_context* h, const BatchLayout& L, cudaStream_t s, TableView
     return DCB_OK;
 }
 
+// The mark launches of a batch (one per group of grids with the same load width and tile).
+int launch_marks(dcb_context* h, const BatchLayout& L, const TableView& T, cudaStream_t s) {
+    for (int v = 0; v < 4; ++v) {
+        if (L.tile_slot[v].empty()) continue;
+        MarkParams mp;
+        mp.B = T.B; mp.tile_slot = T.tile_slot[v]; mp.tile_off = T.tile_off[v];
+        mp.m = (int)L.tile_slot[v].size(); mp.ntiles = L.tile_off[v].back();
+        mp.bits = as<uint32_t>(h->bits); mp.seg_count = as<uint32_t>(h->seg_count);
+        DCB_TRY(h, launch_mark(mp, v & 1, (v & 2) ? mark_narrow_tile_words() : mark_tile_words(), s), "launch mark");
+    }
+    return DCB_OK;
+}
+
 // Runs the pipeline on n device-resident grids as one batch (a single extraction is n = 1);
 // ev[1] must already be recorded. Vertices are numbered over the whole batch while running;
 // for n > 1 the faces are rebased to their own grid's vertices at the end.
@@ -293,14 +310,8 @@ int run_batch(dcb_context* h, const dcb_grid* in, int n, const dcb_opts* o, cuda
 
     // 1) mark: active bits + per-segment counts; scan -> segment starts and the total.
     DCB_TRY(h, cudaMemsetAsync(h->counters.p, 0, sizeof(Counters), s), "memset counters");
-    for (int v = 0; v < 4; ++v) {
-        if (L.tile_slot[v].empty()) continue;
-        MarkParams mp;
-        mp.B = T.B; mp.tile_slot = T.tile_slot[v]; mp.tile_off = T.tile_off[v];
-        mp.m = (int)L.tile_slot[v].size(); mp.ntiles = L.tile_off[v].back();
-        mp.bits = as<uint32_t>(h->bits); mp.seg_count = as<uint32_t>(h->seg_count);
-        DCB_TRY(h, launch_mark(mp, v & 1, (v & 2) ? mark_narrow_tile_words() : mark_tile_words(), s), "launch mark");
-    }
+    rc = launch_marks(h, L, T, s);
+    if (rc != DCB_OK) return rc;
     DCB_TRY(h, cudaEventRecord(h->ev[6], s), "event");
     DCB_TRY(h, launch_scan(as<uint32_t>(h->seg_count), nseg, as<uint32_t>(h->partials), as<uint32_t>(h->seg_start),
                            &dc->total_active, s), "launch segment scan");
@@ -886,6 +897,58 @@ int dcb_copy_cells_to_host(dcb_handle h, int64_t* cell_linear_index, void* cuda_
         const int64_t i = (int64_t)(p & 0x1FFFFF), j = (int64_t)((p >> 21) & 0x1FFFFF), k = (int64_t)(p >> 42);
         cell_linear_index[r] = i + cx * (j + cy * k);
     }
+    return DCB_OK;
+}
+
+int dcb_autotune_mark(dcb_handle h, const dcb_grid* grids, int n, int* waves_out, int* narrow_cells_out,
+                      float* best_ms_out, void* cuda_stream) {
+    if (!h) return DCB_ERR_INVALID_ARGUMENT;
+    if (!grids || n < 1) return fail(h, DCB_ERR_INVALID_ARGUMENT, "empty batch");
+    for (int b = 0; b < n; ++b) {
+        const int rc = validate(h, grids + b);
+        if (rc != DCB_OK) return rc;
+    }
+    if (cudaSetDevice(h->device) != cudaSuccess) { cudaGetLastError(); return fail(h, DCB_ERR_CUDA, "set device"); }
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(cuda_stream);
+    static const int kWaves[4] = {1, 2, 4, 8};
+    static const int kNarrow[4] = {0, 256, 512, 1024};
+    const int keep_w = h->tune_waves, keep_n = h->tune_narrow_cells;
+    float best = 1e30f;
+    int best_w = keep_w, best_n = keep_n;
+    for (int a = 0; a < 4; ++a) {
+        for (int c = 0; c < 4; ++c) {
+            h->tune_waves = kWaves[a];
+            h->tune_narrow_cells = kNarrow[c];
+            BatchLayout L;
+            int rc = layout_batch(h, grids, n, L);
+            if (rc == DCB_OK) {
+                TableView T;
+                rc = upload_table(h, L, s, T);
+                if (rc == DCB_OK) {
+                    DCB_TRY(h, ensure(h->bits, sizeof(uint32_t) * L.bits), "alloc bits");
+                    DCB_TRY(h, ensure(h->seg_count, sizeof(uint32_t) * L.nseg), "alloc segment counts");
+                    float ms[3];
+                    for (int r = 0; r < 4 && rc == DCB_OK; ++r) {       // one warm-up, three timed
+                        DCB_TRY(h, cudaEventRecord(h->ev[0], s), "event");
+                        rc = launch_marks(h, L, T, s);
+                        DCB_TRY(h, cudaEventRecord(h->ev[1], s), "event");
+                        DCB_TRY(h, cudaEventSynchronize(h->ev[1]), "autotune");
+                        if (r > 0) ms[r - 1] = elapsed(h->ev[0], h->ev[1]);
+                    }
+                    if (rc == DCB_OK) {
+                        std::sort(ms, ms + 3);
+                        if (ms[1] < best) { best = ms[1]; best_w = kWaves[a]; best_n = kNarrow[c]; }
+                    }
+                }
+            }
+            if (rc != DCB_OK) { h->tune_waves = keep_w; h->tune_narrow_cells = keep_n; return rc; }
+        }
+    }
+    h->tune_waves = best_w;
+    h->tune_narrow_cells = best_n;
+    if (waves_out) *waves_out = best_w;
+    if (narrow_cells_out) *narrow_cells_out = best_n;
+    if (best_ms_out) *best_ms_out = best;
     return DCB_OK;
 }
 

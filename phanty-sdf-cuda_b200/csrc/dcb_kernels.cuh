@@ -275,6 +275,7 @@ struct OursParams {
     unsigned int* cell_start;
     unsigned int* cell_fill;
     uint32_t* cell_spheres;         // grid points by cell, by radius
+    int* prev_tri;                  // [npts] closest triangle of each grid point last time
     uint32_t* heavy;                // cells with many spheres (a warp each)
     unsigned int* heavy_count;
     long long nt;                   // triangles

@@ -436,12 +436,13 @@ __device__ __forceinline__ double box_d2(const OursParams& P, long long node, co
 // Closest point of the mesh to p (point_mesh_squared_distance, contouring.cpp:869): among
 // equally close triangles the one of smallest index, so the answer does not depend on the
 // traversal order (nodes as close as the best so far are still visited).
-__device__ double bvh_closest(const OursParams& P, const double* p, double* best_c) {
+// seed: a triangle to test first (the previous outer iteration's answer for this point), or -1;
+// the answer does not depend on it, only the number of nodes visited does.
+__device__ double bvh_closest(const OursParams& P, const double* p, double* best_c, long long seed, int& out_t) {
     const long long n = P.nt;
     double best = DBL_MAX;
     long long best_t = 0x7fffffffffffffffLL;
-    auto leaf = [&](long long L) {
-        const long long t = (long long)(P.mkeys_sorted[L] & 0xffffffffull);
+    auto test = [&](long long t) {
         const double* T = P.tri9 + 9 * t;
         double q[3];
         tri_closest(p, T, T + 3, T + 6, q);
@@ -452,7 +453,9 @@ __device__ double bvh_closest(const OursParams& P, const double* p, double* best
             best_c[0] = q[0]; best_c[1] = q[1]; best_c[2] = q[2];
         }
     };
-    if (n == 1) { leaf(0); return best; }
+    auto leaf = [&](long long L) { test((long long)(P.mkeys_sorted[L] & 0xffffffffull)); };
+    if (seed >= 0 && seed < n) test(seed);
+    if (n == 1) { leaf(0); out_t = (int)best_t; return best; }
     int stack[96];
     int sp = 0;
     stack[sp++] = 0;
@@ -476,6 +479,7 @@ __device__ double bvh_closest(const OursParams& P, const double* p, double* best
             }
         }
     }
+    out_t = (int)best_t;
     return best;
 }
 
@@ -486,7 +490,9 @@ __global__ void __launch_bounds__(128) k_ours_query(OursParams P) {
         const long long gidx = P.sel[s];
         double c[3], C[3];
         point_of(P.g, gidx, c);
-        const double d2 = bvh_closest(P, c, C);
+        int t = -1;
+        const double d2 = bvh_closest(P, c, C, P.prev_tri[gidx], t);
+        P.prev_tri[gidx] = t;
         const double radius = fabs((double)__ldg(P.g.v + gidx));
         int rank = -1;
         if (d2 < DBL_MAX && sqrt(d2) - radius < P.cell_diag) {
@@ -903,6 +909,7 @@ size_t ours_workspace_bytes(long long nv, long long nq, long long npts, size_t* 
     b += 3 * al(sizeof(unsigned int) * (nv + 1)) + al(sizeof(uint32_t) * npts);    // count/start/fill, spheres
     b += al(sizeof(uint32_t) * (nv + 1));                                    // cells with many spheres
     b += al(sizeof(uint32_t) * npts);                                        // selected points, sorted
+    b += al(sizeof(int) * npts);                                             // last closest triangle per point
     b += 2 * al(sizeof(unsigned long long) * nt) + al(sizeof(int2) * nt) + al(sizeof(int) * 2 * nt);
     b += 2 * al(sizeof(float4) * 2 * nt) + al(sizeof(unsigned int) * nt) + al(sizeof(double) * 9 * nt);
     b += al(sizeof(uint32_t) * (scan_partials_len(nv + 1) + 1)) + al(64);    // scan partials, counters
@@ -944,6 +951,7 @@ cudaError_t ours_run(OursRun& R, cudaStream_t s) {
     unsigned int* counters = (unsigned int*)take(64);
     void* cub_temp = take(R.cub_bytes);
     uint32_t* sel_sorted = (uint32_t*)take(sizeof(uint32_t) * npts);
+    P.prev_tri = (int*)take(sizeof(int) * npts);
     P.heavy_count = counters + 8;
     P.sel = sel_sorted;
     P.nt = nt;
@@ -951,6 +959,7 @@ cudaError_t ours_run(OursRun& R, cudaStream_t s) {
     cudaError_t e;
 #define OURS_TRY(x) do { e = (x); if (e != cudaSuccess) return e; } while (0)
     OURS_TRY(cudaMemsetAsync(counters, 0, 64, s));
+    OURS_TRY(cudaMemsetAsync(P.prev_tri, 0xff, sizeof(int) * npts, s));
     k_ours_init<<<grid_for(nv, 128, sms), 128, 0, s>>>(P);
     k_ours_quads<<<grid_for(nq, 128, sms), 128, 0, s>>>(P);
     k_ours_select<<<grid_for(npts, 256, sms), 256, 0, s>>>(P, npts, band, rest, counters);

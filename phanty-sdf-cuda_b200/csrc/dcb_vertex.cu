@@ -241,7 +241,7 @@ __device__ __forceinline__ void store_vertex(const QefParams& P, const GridDesc&
 // ---- k_cell_qef -------------------------------------------------------------------------
 
 template <bool ONE>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, 5)
 k_cell_qef(const __grid_constant__ QefParams P) {
     __shared__ unsigned int s_hist;
     __shared__ float s_c[8][128];    // per-thread corner values (dynamically indexed)

@@ -78,3 +78,19 @@ def test_benchmark_batch(backend):
         assert np.array_equal(parts[b][0], V1) and np.array_equal(parts[b][1], F1)
     print("batch: %d grids, %d cells, %d vertices, %d faces, %.2f ms" % (
         len(grids), st.total_cells, st.vertex_count, st.face_count, st.total_ms))
+
+
+def test_autotune_keeps_the_results(backend):
+    """The mark tile autotuner picks one of its candidate tilings and the extraction's output
+    does not change with it."""
+    import torch
+    from contouring_b200 import synth
+    grids = synth.csg_batch(24, seed=5, device="cuda")
+    before, _ = backend.extract_batch(grids)
+    before = [(V.clone(), F.clone()) for V, F in before]
+    waves, narrow, ms = backend.autotune_mark(grids)
+    assert waves in (1, 2, 4, 8) and narrow in (0, 256, 512, 1024) and ms > 0
+    after, _ = backend.extract_batch(grids)
+    for (Va, Fa), (Vb, Fb) in zip(before, after):
+        assert torch.equal(Va, Vb) and torch.equal(Fa, Fb)
+    print("autotuned mark tiling: %d waves, 256-cell tiles up to %d cells wide, %.3f ms" % (waves, narrow, ms))
