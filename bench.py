@@ -350,6 +350,76 @@ def run_mesh_workload(args):
     return 0
 
 
+def run_refcuda_workload(args):
+    """Same-GPU speed bar: the reference's own CUDA dense backend
+    (CudaDualContouringBackend::extract_device, built from its source into oracle/_ref/)
+    against this engine on the same device-resident 512^3 CSG grid, both from the device grid
+    to a host mesh, wall clock with the device synchronised (the reference times itself with a
+    host clock the same way). 512^3 because the reference indexes grid edges with 32-bit ints
+    and cannot run at 1024^3. Its vertices differ (no normal averaging, clamping): speed only."""
+    import ctypes
+    import torch
+    from contouring_b200 import B200DualContouringBackend, DenseSdfGridDevice
+    path = os.path.join(ROOT, "oracle", "_ref", "libref_dc_cuda.so")
+    if not os.path.exists(path):
+        print(json.dumps({"impl": "reference_cuda", "unavailable": "oracle/_ref/libref_dc_cuda.so was not built"}))
+        return 0
+    torch.cuda.set_device(0)
+    res = 512
+    vals, dims, sp, org = make_grid(res, torch.device("cuda", 0))
+    torch.cuda.synchronize()
+    ref = ctypes.CDLL(path)
+    ref.refdc_extract_device.argtypes = [ctypes.c_int] * 3 + [ctypes.c_float] * 6 + [ctypes.c_void_p] + \
+        [ctypes.POINTER(ctypes.c_double)] * 2 + [ctypes.POINTER(ctypes.c_int64)] * 2
+    ref.refdc_extract_device.restype = ctypes.c_int
+    rms, rstage, rnv, rnf = ctypes.c_double(), ctypes.c_double(), ctypes.c_int64(), ctypes.c_int64()
+    ref_stage = []
+
+    def ref_call():
+        rc = ref.refdc_extract_device(*dims, *sp, *org, vals.data_ptr(), ctypes.byref(rms), ctypes.byref(rstage),
+                                      ctypes.byref(rnv), ctypes.byref(rnf))
+        if rc != 0:
+            raise RuntimeError("reference CUDA backend refused the grid (%d)" % rc)
+        torch.cuda.synchronize()
+        ref_stage.append(rstage.value)
+
+    be = B200DualContouringBackend(0)
+    g = DenseSdfGridDevice(*dims, *sp, *org, d_values=vals)
+
+    def ours_call():
+        mesh, _ = be.extract_device(g)
+        return mesh
+
+    def wall(fn, steps, warmup):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(steps):
+            t0 = time.perf_counter()
+            fn()
+            torch.cuda.synchronize()
+            ts.append((time.perf_counter() - t0) * 1e3)
+        return statistics.median(ts)
+
+    ms_ref = wall(ref_call, args.steps, args.warmup)
+    ref_kernels = statistics.median(ref_stage[args.warmup:])
+    ms_ours = wall(ours_call, args.steps, args.warmup)
+    ms_ours_dev = _timed(lambda: be.extract_tensor_ptr(g), args.steps, args.warmup)
+    mesh = ours_call()
+    ncell = (dims[0] - 1) * (dims[1] - 1) * (dims[2] - 1)
+    _side_line("dc_extract_to_host_mcells_per_s", ncell / (ms_ours / 1e3) / 1e6, "Mcells/s", ms_ours, args,
+               {"workload": "csg512_device_grid_to_host_mesh", "grid": list(dims)},
+               reference_cuda={"ms_per_step": round(ms_ref, 3), "mcells_per_s": round(ncell / (ms_ref / 1e3) / 1e6, 1),
+                               "stage_kernels_ms": round(ref_kernels, 3), "vertices": rnv.value, "quads": rnf.value},
+               device_only_ms=round(ms_ours_dev, 4),
+               vertices=len(mesh.vertices) // 3, quads=len(mesh.faces) // 4,
+               speedup_vs_reference_cuda=round(ms_ref / ms_ours, 2),
+               device_speedup_vs_reference_cuda_stages=round(ref_kernels / ms_ours_dev, 2))
+    be.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -361,10 +431,10 @@ def main():
     ap.add_argument("--ref-zslab", type=int, default=96, help="point planes per CPU sample (over 8 slabs)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-sequential", action="store_true", help="batch256: skip the one-by-one comparison")
-    ap.add_argument("--workload", default="csg1024", choices=["csg1024", "batch256", "adjoint128", "ours128", "mesh512"],
+    ap.add_argument("--workload", default="csg1024", choices=["csg1024", "batch256", "adjoint128", "ours128", "mesh512", "refcuda512"],
                     help="side workloads (not the headline): batch256 = 256 uneven CSG grids batched vs one "
                          "by one; adjoint128 = forward + adjoint; ours128 = the full refinement; mesh512 = "
-                         "mesh_to_sdf")
+                         "mesh_to_sdf; refcuda512 = the reference's CUDA backend vs this engine at 512^3")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -382,6 +452,8 @@ def main():
         return run_ours_workload(args)
     if args.workload == "mesh512":
         return run_mesh_workload(args)
+    if args.workload == "refcuda512":
+        return run_refcuda_workload(args)
 
     import numpy as np
     import torch

@@ -1,0 +1,36 @@
+// ref_cuda_harness.cu — TEST INFRASTRUCTURE ONLY: a C entry point around the reference's own
+// CUDA dense backend (CudaDualContouringBackend::extract_device, src/cuda/dc_cuda.cu:652-847,
+// compiled from the reference's source by oracle/Makefile's `ref` target into oracle/_ref/).
+// It is a same-GPU speed bar for bench.py's refcuda512 workload and nothing else: its
+// vertices differ from the CPU backend's (no normal averaging, clamping into the cell).
+//
+// The reference indexes cells and grid edges with 32-bit ints; this entry point refuses
+// grids whose interior-edge count does not fit, where that code would index out of range.
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "dc_cuda.h"
+
+// total_ms: the backend's own host-clock time of the call (allocation, kernels, download);
+// stage_ms: the sum of its own CUDA-event stage times (mark, compaction, QEF, faces).
+extern "C" int refdc_extract_device(int nx, int ny, int nz, float vx, float vy, float vz, float ox, float oy,
+                                    float oz, const float* d_values, double* total_ms, double* stage_ms,
+                                    int64_t* vertex_count, int64_t* face_count) {
+    if (nx < 3 || ny < 3 || nz < 3 || !d_values) return -1;
+    const long long cx = nx - 1, cy = ny - 1, cz = nz - 1;
+    const long long edges = cx * (cy - 1) * (cz - 1) + (cx - 1) * cy * (cz - 1) + (cx - 1) * (cy - 1) * cz;
+    const long long points = (long long)nx * ny * nz;
+    if (edges >= 0x7fffffffLL || points >= 0x7fffffffLL) return -2;
+    DenseSdfGridDevice g;
+    g.nx = nx; g.ny = ny; g.nz = nz;
+    g.vx = vx; g.vy = vy; g.vz = vz;
+    g.ox = ox; g.oy = oy; g.oz = oz;
+    g.d_values = d_values;
+    CudaDualContouringBackend be;
+    DualContouringStats st;
+    DualContouringMesh m = be.extract_device(g, st);
+    if (total_ms) *total_ms = st.total_ms;
+    if (stage_ms) *stage_ms = (double)st.marking_ms + st.compaction_ms + st.qef_ms + st.face_emission_ms;
+    if (vertex_count) *vertex_count = (int64_t)(m.vertices.size() / 3);
+    if (face_count) *face_count = (int64_t)(m.faces.size() / 4);
+    return 0;
+}

@@ -192,13 +192,28 @@ k_expand_ranks(const __grid_constant__ ExpandParams P) {
             const uint32_t first = seg_first + incl - c;
             if (word_lane && w < g.W && (w & 7) == 0) P.super[S.super_off + row * g.W8 + (w >> 3)] = first;
             const int j = (int)(row % g.cy), k = (int)(row / g.cy);
-            uint32_t m = act, q = 0;
-            while (m) {
-                const int bb = __ffs(m) - 1;
-                m &= m - 1;
-                P.list[first + q] = pack_cell(32 * w + bb, j, k);
-                if (!ONE && P.cell_slot) P.cell_slot[first + q] = (uint32_t)sslot;
-                ++q;
+            // the segment's active cells, 32 at a time: lane l takes the (base+l)-th, found by a
+            // binary search over the words' inclusive counts and a popcount select in its word
+            const uint32_t n = __shfl_sync(0xffffffffu, incl, 31);
+            const int w0 = xt * S.tw;
+            for (uint32_t base = 0; base < n; base += 32) {
+                const uint32_t idx = base + lane;
+                int lo = 0;                                    // first word with incl > idx
+#pragma unroll
+                for (int st = 16; st >= 1; st >>= 1) {
+                    const uint32_t v = __shfl_sync(0xffffffffu, incl, lo + st - 1);
+                    if (v <= idx) lo += st;
+                }
+                const uint32_t word = __shfl_sync(0xffffffffu, act, lo);
+                const uint32_t before = __shfl_sync(0xffffffffu, incl - c, lo);
+                if (idx >= n) continue;
+                const uint32_t r = idx - before;               // r-th set bit of the word
+                int pos = 0;
+#pragma unroll
+                for (int st = 16; st >= 1; st >>= 1)
+                    if ((uint32_t)__popc(word & ((1u << (pos + st)) - 1u)) <= r) pos += st;
+                P.list[seg_first + idx] = pack_cell(32 * (w0 + lo) + pos, j, k);
+                if (!ONE && P.cell_slot) P.cell_slot[seg_first + idx] = (uint32_t)sslot;
             }
         }
     }
