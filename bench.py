@@ -37,6 +37,23 @@ KERNELS_PER_STEP = 16
 MARK_TRAFFIC_BYTES_PER_POINT = (554.966272e6 + 19.405056e6) / 512 ** 3
 
 
+def max_over_ranks(local, dist, device):
+    """The slowest rank's time: every rank takes part in the MAX all-reduce (the job's time is
+    the max over ranks); without a process group, the local value."""
+    if dist is None or not dist.is_initialized():
+        return float(local)
+    import torch
+    t = torch.tensor([float(local)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_value(world, cells_per_rank, ms_per_step):
+    """Whole-job Mcells/s: every rank extracts its own grid of the same size (replicas, weak
+    scaling), so the job processes world * cells per step in the slowest rank's time."""
+    return world * cells_per_rank / (ms_per_step / 1e3) / 1e6
+
+
 def _peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -493,13 +510,9 @@ def main():
         e1.record(stream)
         torch.cuda.synchronize()
     barrier()
-    ms_total = e0.elapsed_time(e1)
-    if dist is not None:
-        t = torch.tensor([ms_total], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_total = float(t.item())
+    ms_total = max_over_ranks(e0.elapsed_time(e1), dist, dev)
     ms_step = ms_total / args.steps
-    value = world * ncell / (ms_step / 1e3) / 1e6
+    value = job_value(world, ncell, ms_step)
 
     # End to end through the public API: pinned host grid in, host mesh out, every step.
     host = torch.empty(vals.numel(), dtype=torch.float32, pin_memory=True)
@@ -512,12 +525,8 @@ def main():
     for _ in range(args.e2e_steps):
         mesh, est = be.extract(hgrid)
     torch.cuda.synchronize()
-    e2e_s = (time.perf_counter() - t0) / max(1, args.e2e_steps)
-    if dist is not None:
-        t = torch.tensor([e2e_s], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    e2e_value = world * ncell / e2e_s / 1e6 if args.e2e_steps > 0 else None
+    e2e_s = max_over_ranks((time.perf_counter() - t0) / max(1, args.e2e_steps), dist, dev)
+    e2e_value = job_value(world, ncell, e2e_s * 1e3) if args.e2e_steps > 0 else None
     h2d = 4 * vals.numel()
     d2h = int(mesh.vertices.nbytes + mesh.faces.nbytes)
 

@@ -486,6 +486,7 @@ int run_ours(dcb_context* h, const dcb_grid* in, const dcb_opts* o, cudaStream_t
     dcb_opts dc = *o;
     dc.method = DCB_METHOD_DUAL_CONTOURING;
     dc.emit_triangles = 0;
+    dc.svd_threshold = 0.01;            // Cell::update's solve (Cell.cpp:314) ignores the options
     int rc = run_batch(h, in, 1, &dc, s, st);
     if (rc != DCB_OK) return rc;
     const long long nv = h->nv, nq = h->nf;

@@ -229,7 +229,7 @@ __global__ void __launch_bounds__(128) k_ours_init(OursParams P) {
         S.hmask = hmask;
         S.fmask = 0;
         double x[3];
-        f64::cell_vertex_thread(P.g, i, j, k, P.thr, x);
+        f64::cell_vertex_thread(P.g, i, j, k, 0.01, x);        // Cell::update's threshold (Cell.cpp:314)
         for (int d = 0; d < 3; ++d) P.Vm[3 * r + d] = x[d];
     }
 }
