@@ -276,6 +276,25 @@ __global__ void __launch_bounds__(256) k_ours_select(OursParams P, long long npt
     }
 }
 
+__device__ __forceinline__ unsigned long long spread21(unsigned long long v) {
+    v &= 0x1fffffull;
+    v = (v | (v << 32)) & 0x1f00000000ffffull;
+    v = (v | (v << 16)) & 0x1f0000ff0000ffull;
+    v = (v | (v << 8)) & 0x100f00f00f00f00full;
+    v = (v | (v << 4)) & 0x10c30c30c30c30c3ull;
+    v = (v | (v << 2)) & 0x1249249249249249ull;
+    return v;
+}
+
+// Morton keys of the selected grid points: the queries of a warp then cover a compact block.
+__global__ void k_ours_point_keys(OursParams P, const uint32_t* sel, long long n, unsigned long long* keys) {
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const long long g = sel[t];
+        const unsigned long long i = g % P.g.nx, j = (g / P.g.nx) % P.g.ny, k = g / ((long long)P.g.nx * P.g.ny);
+        keys[t] = spread21(i) | (spread21(j) << 1) | (spread21(k) << 2);
+    }
+}
+
 // Random keys of the fill candidates for one outer iteration (seeded).
 __global__ void k_ours_fill_keys(const uint32_t* rest, long long n, unsigned long long seed, int it,
                                  unsigned long long* keys) {
@@ -987,9 +1006,10 @@ cudaError_t ours_run(OursRun& R, cudaStream_t s) {
                 OURS_TRY(cub::DeviceRadixSort::SortPairs(cub_temp, tb2, fk, fk2, rest, fv2, (int)nrest, 0, 64, s));
                 OURS_TRY(cudaMemcpyAsync(sel + nband, fv2, sizeof(uint32_t) * nfill, cudaMemcpyDeviceToDevice, s));
             }
-            // query in grid order: neighbouring threads walk the same part of the tree
+            // query in Morton order: a warp's points form a compact block of the grid
+            k_ours_point_keys<<<grid_for(P.nsel, 256, sms), 256, 0, s>>>(P, sel, P.nsel, fk);
             size_t tb3 = R.cub_bytes;
-            OURS_TRY(cub::DeviceRadixSort::SortKeys(cub_temp, tb3, sel, sel_sorted, (int)P.nsel, 0, 32, s));
+            OURS_TRY(cub::DeviceRadixSort::SortPairs(cub_temp, tb3, fk, fk2, sel, sel_sorted, (int)P.nsel, 0, 63, s));
             OURS_TRY(cudaMemsetAsync(P.cell_count, 0, sizeof(unsigned int) * (nv + 1), s));
             OURS_TRY(cudaMemsetAsync(P.cell_fill, 0, sizeof(unsigned int) * (nv + 1), s));
             OURS_TRY(cudaMemsetAsync(P.heavy_count, 0, sizeof(unsigned int), s));

@@ -88,7 +88,7 @@ def test_random_fill_matches(backend):
 def test_options_without_hermite_update(backend):
     import oracle as O
     vals, dims, sp, org = _grid("rbf32")
-    kw = dict(outer_iters=3, inner_iters=20, hermite_update=False, mu=0.05, dc_weight=0.05)
+    kw = dict(outer_iters=3, inner_iters=20, hermite_update=False, mu=0.05, dc_weight=0.05, svd_threshold=0.05)
     V, F, st = _run(backend, vals, dims, sp, org, **kw)
     _compare(V, F, O.ours(vals.numpy(), dims, sp, org, **kw), sp, "no-hermite-update")
 
