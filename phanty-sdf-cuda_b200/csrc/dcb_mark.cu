@@ -152,8 +152,12 @@ k_mark_zmarch(const __grid_constant__ MarkParams P) {
     }
 }
 
-// Warp per group of 32 consecutive (row, x-tile) segments: the non-empty ones (ballot) get
-// the global ranks of their super words and their part of the packed active-cell list.
+// Segments with at most this many active cells are expanded by one lane.
+constexpr uint32_t kLaneSegmentCells = 96;
+
+// Warp per group of 32 consecutive (row, x-tile) segments: the non-empty ones get the global
+// ranks of their super words and their part of the packed active-cell list — a lane per
+// segment with few active cells, the whole warp per segment with many.
 template <bool ONE>
 __global__ void __launch_bounds__(256)
 k_expand_ranks(const __grid_constant__ ExpandParams P) {
@@ -168,6 +172,37 @@ k_expand_ranks(const __grid_constant__ ExpandParams P) {
         uint32_t live = __ballot_sync(0xffffffffu, cnt != 0);
         const uint32_t my_start = (have && cnt) ? P.seg_start[s0 + lane] : 0u;
         const int my_slot = (!ONE && have && cnt) ? slot_of_segment(P.B, s0 + lane) : 0;
+        // segments with few active cells: a lane each (no shuffles); the rest cooperatively
+        const bool light = have && cnt != 0 && cnt <= kLaneSegmentCells;
+        if (light) {
+            const GridSlot& S = slot_ref<ONE>(P.B, my_slot);
+            const GridDesc& g = S.g;
+            const long long ls = s0 + lane - S.seg_off;
+            const long long row = ls / S.nxt;
+            const int wb = (int)(ls - row * S.nxt) * S.tw;
+            const int nw = min(S.tw, g.W - wb);
+            const int j = (int)(row % g.cy), k = (int)(row / g.cy);
+            const uint4* words = reinterpret_cast<const uint4*>(P.bits + S.bits_off + row * g.W + wb);
+            uint32_t rank = my_start;
+            for (int q4 = 0; q4 < nw; q4 += 4) {
+                const uint4 v = __ldg(words + (q4 >> 2));
+                const uint32_t ws[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int w = wb + q4 + u;
+                    if ((w & 7) == 0) P.super[S.super_off + row * g.W8 + (w >> 3)] = rank;
+                    uint32_t m = ws[u];
+                    while (m) {
+                        const int bb = __ffs(m) - 1;
+                        m &= m - 1;
+                        P.list[rank] = pack_cell(32 * w + bb, j, k);
+                        if (!ONE && P.cell_slot) P.cell_slot[rank] = (uint32_t)my_slot;
+                        ++rank;
+                    }
+                }
+            }
+        }
+        live &= ~__ballot_sync(0xffffffffu, light);
         while (live) {
             const int b = __ffs(live) - 1;
             live &= live - 1;
