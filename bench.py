@@ -359,10 +359,39 @@ def run_mesh_workload(args):
     ms = _timed(lambda: mesh_to_sdf_tensor(be, Vd, Fd, dims, org, sp, out=out), args.steps, args.warmup)
     _, st = mesh_to_sdf_tensor(be, Vd, Fd, dims, org, sp, out=out)      # stage times of a warm call
     npts = dims[0] * dims[1] * dims[2]
+    extra = {}
+    ref_path = os.path.join(ROOT, "oracle", "_ref", "libref_dc_cuda.so")
+    if os.path.exists(ref_path):
+        # same-GPU speed bar: the reference's own CUDA conversion (its own timer: mesh upload,
+        # grid allocation, conversion); it caps the exterior flood at 40 passes, so a few far
+        # values can differ: compared by sign only
+        import ctypes
+        import numpy as np
+        ref = ctypes.CDLL(ref_path)
+        ref.refsdf_compute.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int] + \
+            [ctypes.c_int] * 3 + [ctypes.c_float] * 6 + [ctypes.POINTER(ctypes.c_float), ctypes.c_void_p]
+        ref.refsdf_compute.restype = ctypes.c_int
+        Vc = np.ascontiguousarray(V, np.float32)
+        Fc = np.ascontiguousarray(F, np.int32)
+        rms = ctypes.c_float()
+        ts = []
+        for q in range(args.warmup + args.steps):
+            if ref.refsdf_compute(Vc.ctypes.data, len(Vc), Fc.ctypes.data, len(Fc), *dims, *org, *sp,
+                                  ctypes.byref(rms), None) != 0:
+                raise RuntimeError("reference conversion refused the grid")
+            if q >= args.warmup:
+                ts.append(rms.value)
+        host = np.empty(npts, np.float32)
+        ref.refsdf_compute(Vc.ctypes.data, len(Vc), Fc.ctypes.data, len(Fc), *dims, *org, *sp, ctypes.byref(rms),
+                           host.ctypes.data)
+        ours = out.cpu().numpy()
+        ms_ref = statistics.median(ts)
+        extra["reference_cuda"] = {"ms_per_step": round(ms_ref, 3), "sign_agreement": float(np.mean(np.sign(ours) == np.sign(host))),
+                                   "speedup": round(ms_ref / ms, 2)}
     _side_line("mesh_to_sdf_mpoints_per_s", npts / (ms / 1e3) / 1e6, "Mpoints/s", ms, args,
                {"workload": "icospheres32_mesh_to_sdf512", "grid": list(dims), "triangles": len(F)},
                stage_ms={"bins": round(st.bins_ms, 4), "band": round(st.band_ms, 4), "sign": round(st.sign_ms, 4),
-                         "relax": round(st.relax_ms, 4)})
+                         "relax": round(st.relax_ms, 4)}, **extra)
     be.close()
     return 0
 

@@ -34,3 +34,30 @@ extern "C" int refdc_extract_device(int nx, int ny, int nz, float vx, float vy, 
     if (face_count) *face_count = (int64_t)(m.faces.size() / 4);
     return 0;
 }
+
+// The reference's own mesh -> SDF conversion (compute_mesh_sdf_device_cuda,
+// src/cuda/mesh_to_sdf_cuda.cu:740-1009) on host vertices and faces; *ms receives its own
+// timer (upload, allocation, conversion). When out_host is given, the values are copied there
+// (nx*ny*nz floats). The device grid is freed before returning. Grids whose point count does
+// not fit the reference's 32-bit indices are refused.
+#include "mesh_to_sdf.h"
+
+// DenseSdfGrid's key function lives in the reference's dc_backend.cpp, which needs Eigen and
+// libigl; the conversion above only constructs a DenseSdfGrid in its host variant and never
+// samples it, so a stand-in definition provides the vtable.
+float DenseSdfGrid::sample(float, float, float) const { return 0.f; }
+
+extern "C" int refsdf_compute(const float* vertices, int num_vertices, const int* faces, int num_faces, int nx,
+                              int ny, int nz, float ox, float oy, float oz, float vx, float vy, float vz,
+                              float* ms, float* out_host) {
+    if (nx < 2 || ny < 2 || nz < 2 || !vertices || !faces) return -1;
+    if ((long long)nx * ny * nz >= 0x7fffffffLL) return -2;
+    float t = 0.f;
+    DenseSdfGridDevice g = compute_mesh_sdf_device_cuda(vertices, num_vertices, faces, num_faces, nx, ny, nz, ox, oy,
+                                                        oz, vx, vy, vz, &t, false, 256);
+    if (ms) *ms = t;
+    if (out_host)
+        cudaMemcpy(out_host, g.d_values, sizeof(float) * (size_t)nx * ny * nz, cudaMemcpyDeviceToHost);
+    free_mesh_sdf_device_cuda(g);
+    return 0;
+}
