@@ -72,7 +72,7 @@ struct dcb_context {
     // (cells along x) that marches 256-cell x-tiles instead of 1024-cell ones
     int tune_waves = 4;
     int tune_narrow_cells = 256;
-    int cx = 0, cy = 0;
+    int cx = 0, cy = 0, cz = 0;
     // batch layout table (device + pinned staging) and the last batch's per-grid offsets
     DevBuf table, cell_slot;
     void* h_table = nullptr; size_t h_table_bytes = 0;
@@ -329,6 +329,7 @@ int run_batch(dcb_context* h, const dcb_grid* in, int n, const dcb_opts* o, cuda
     h->vpf = o->emit_triangles ? 3 : 4;
     h->cx = L.slots[0].g.cx;
     h->cy = L.slots[0].g.cy;
+    h->cz = L.slots[0].g.cz;
     h->batch_n = n;
     h->batch_cx.resize(n); h->batch_cy.resize(n);
     h->vert_offsets.assign(n + 1, 0);
@@ -962,7 +963,7 @@ int dcb_backward(dcb_handle h, const dcb_grid* grid, const dcb_opts* opts, const
     const dcb_opts* o = opts ? opts : &def;
     if (o->method != DCB_METHOD_DUAL_CONTOURING) return fail(h, DCB_ERR_NOT_SUPPORTED, "the adjoint covers dual contouring only");
     if (!(o->svd_threshold >= 0.0)) return fail(h, DCB_ERR_INVALID_ARGUMENT, "svd_threshold must be >= 0");
-    if (h->batch_n != 1 || h->cx != grid->nx - 1 || h->cy != grid->ny - 1)
+    if (h->batch_n != 1 || h->cx != grid->nx - 1 || h->cy != grid->ny - 1 || h->cz != grid->nz - 1)
         return fail(h, DCB_ERR_INVALID_ARGUMENT, "backward needs the grid of the last single-grid extraction");
     if (!dL_dgrid || (h->nv > 0 && !dL_dvertices)) return fail(h, DCB_ERR_INVALID_ARGUMENT, "null gradient array");
     if (cudaSetDevice(h->device) != cudaSuccess) { cudaGetLastError(); return fail(h, DCB_ERR_CUDA, "set device"); }
