@@ -338,7 +338,7 @@ k_vertex_fp64(Vertex64Params P) {
 cudaError_t launch_vertex_fp64(const Vertex64Params& P, long long max_items, int num_sms, cudaStream_t s) {
     if (max_items <= 0) return cudaSuccess;
     long long blocks = (max_items + 127) / 128;
-    const long long cap = (long long)num_sms * 4;
+    const long long cap = (long long)num_sms * 16;     // warp mode up to 9,472 cells
     if (blocks > cap) blocks = cap;
     k_vertex_fp64<<<(unsigned)blocks, 128, 0, s>>>(P);
     return cudaGetLastError();
