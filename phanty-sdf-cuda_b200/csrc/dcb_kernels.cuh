@@ -279,8 +279,11 @@ struct OursParams {
     uint32_t* heavy;                // cells with many spheres (a warp each)
     unsigned int* heavy_count;
     long long nt;                   // triangles
-    unsigned long long* mkeys;
     unsigned long long* mkeys_sorted;
+    uint32_t* tcode;                // triangles' 30-bit Morton codes and indices, then sorted
+    uint32_t* tidx;
+    uint32_t* tcode_sorted;
+    uint32_t* tidx_sorted;
     int2* child;                    // internal nodes: children (< 0: ~leaf)
     int* parent;                    // [2 nt]: internal nodes, then leaves at nt - 1 + leaf
     float4* bmin;

@@ -367,9 +367,17 @@ __global__ void __launch_bounds__(128) k_ours_tris(OursParams P) {
                 const unsigned long long b = (unsigned long long)fmin(1023.0, u * 1024.0);
                 code |= expand_bits10(b) << (2 - d);
             }
-            P.mkeys[t] = (code << 32) | (unsigned long long)t;
+            P.tcode[t] = (uint32_t)code;
+            P.tidx[t] = (uint32_t)t;
         }
     }
+}
+
+// Unique sorted keys (Morton code << 32 | triangle): the pairs were sorted stably by code, so
+// equal codes keep ascending triangle order.
+__global__ void k_bvh_keys(OursParams P) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < P.nt; i += (long long)gridDim.x * blockDim.x)
+        P.mkeys_sorted[i] = ((unsigned long long)P.tcode_sorted[i] << 32) | P.tidx_sorted[i];
 }
 
 // Radix tree over the sorted keys (Karras, "Maximizing parallelism in the construction of
@@ -913,13 +921,16 @@ inline size_t al(size_t x) { return (x + 255) & ~size_t(255); }
 size_t ours_workspace_bytes(long long nv, long long nq, long long npts, size_t* cub_bytes) {
     const long long nt = 2 * nq;
     size_t tb1 = 0, tb2 = 0;
-    cub::DeviceRadixSort::SortKeys(nullptr, tb1, (unsigned long long*)nullptr, (unsigned long long*)nullptr,
+    cub::DeviceRadixSort::SortPairs(nullptr, tb1, (uint32_t*)nullptr, (uint32_t*)nullptr, (uint32_t*)nullptr,
+                                    (uint32_t*)nullptr, (int)std::max(1LL, nt));
+    size_t tb0 = 0;
+    cub::DeviceRadixSort::SortKeys(nullptr, tb0, (unsigned long long*)nullptr, (unsigned long long*)nullptr,
                                    (int)std::max(1LL, nt));
     cub::DeviceRadixSort::SortPairs(nullptr, tb2, (unsigned long long*)nullptr, (unsigned long long*)nullptr,
                                     (uint32_t*)nullptr, (uint32_t*)nullptr, (int)std::max(1LL, npts));
     size_t tb3 = 0;
     cub::DeviceRadixSort::SortKeys(nullptr, tb3, (uint32_t*)nullptr, (uint32_t*)nullptr, (int)std::max(1LL, npts));
-    *cub_bytes = std::max(tb1, std::max(tb2, tb3));
+    *cub_bytes = std::max(std::max(tb0, tb1), std::max(tb2, tb3));
     size_t b = 0;
     b += al(sizeof(OursCell) * nv) + al(sizeof(double) * 3 * nv);            // cells, Vm
     b += al(sizeof(int4) * nq) + al(sizeof(double) * 3 * nq);               // quads, gsum
@@ -929,7 +940,8 @@ size_t ours_workspace_bytes(long long nv, long long nq, long long npts, size_t* 
     b += al(sizeof(uint32_t) * (nv + 1));                                    // cells with many spheres
     b += al(sizeof(uint32_t) * npts);                                        // selected points, sorted
     b += al(sizeof(int) * npts);                                             // last closest triangle per point
-    b += 2 * al(sizeof(unsigned long long) * nt) + al(sizeof(int2) * nt) + al(sizeof(int) * 2 * nt);
+    b += al(sizeof(unsigned long long) * nt) + al(sizeof(int2) * nt) + al(sizeof(int) * 2 * nt);
+    b += 4 * al(sizeof(uint32_t) * nt);                                      // triangle codes / indices
     b += 2 * al(sizeof(float4) * 2 * nt) + al(sizeof(unsigned int) * nt) + al(sizeof(double) * 9 * nt);
     b += al(sizeof(uint32_t) * (scan_partials_len(nv + 1) + 1)) + al(64);    // scan partials, counters
     b += al(*cub_bytes);
@@ -958,8 +970,11 @@ cudaError_t ours_run(OursRun& R, cudaStream_t s) {
     P.cell_fill = (unsigned int*)take(sizeof(unsigned int) * (nv + 1));
     P.cell_spheres = (uint32_t*)take(sizeof(uint32_t) * npts);
     P.heavy = (uint32_t*)take(sizeof(uint32_t) * (nv + 1));
-    P.mkeys = (unsigned long long*)take(sizeof(unsigned long long) * nt);
     P.mkeys_sorted = (unsigned long long*)take(sizeof(unsigned long long) * nt);
+    P.tcode = (uint32_t*)take(sizeof(uint32_t) * nt);
+    P.tidx = (uint32_t*)take(sizeof(uint32_t) * nt);
+    P.tcode_sorted = (uint32_t*)take(sizeof(uint32_t) * nt);
+    P.tidx_sorted = (uint32_t*)take(sizeof(uint32_t) * nt);
     P.child = (int2*)take(sizeof(int2) * nt);
     P.parent = (int*)take(sizeof(int) * 2 * nt);
     P.bmin = (float4*)take(sizeof(float4) * 2 * nt);
@@ -990,12 +1005,20 @@ cudaError_t ours_run(OursRun& R, cudaStream_t s) {
     const long long bounded = std::min<long long>(R.batch_size, npts);
     const long long nfill = nband < bounded ? std::min(bounded - nband, nrest) : 0;
     P.nsel = nband + nfill;
-    OURS_TRY(cudaMemcpyAsync(sel, band, sizeof(uint32_t) * nband, cudaMemcpyDeviceToDevice, s));
+    // the near-surface points never change: Morton-ordered once (a warp's queries then cover
+    // a compact block of the grid); a random fill is ordered again every outer iteration
+    if (nband > 0) {
+        k_ours_point_keys<<<grid_for(nband, 256, sms), 256, 0, s>>>(P, band, nband, fk);
+        size_t tb4 = R.cub_bytes;
+        OURS_TRY(cub::DeviceRadixSort::SortPairs(cub_temp, tb4, fk, fk2, band, sel_sorted, (int)nband, 0, 63, s));
+    }
     for (int it = 0; it < R.outer_iters; ++it) {
         if (nq > 0) {
             k_ours_tris<<<grid_for(nq, 128, sms), 128, 0, s>>>(P);
             size_t tb = R.cub_bytes;
-            OURS_TRY(cub::DeviceRadixSort::SortKeys(cub_temp, tb, P.mkeys, P.mkeys_sorted, (int)nt, 0, 64, s));
+            OURS_TRY(cub::DeviceRadixSort::SortPairs(cub_temp, tb, P.tcode, P.tcode_sorted, P.tidx, P.tidx_sorted,
+                                                     (int)nt, 0, 30, s));
+            k_bvh_keys<<<grid_for(nt, 256, sms), 256, 0, s>>>(P);
             OURS_TRY(cudaMemsetAsync(P.flags, 0, sizeof(unsigned int) * nt, s));
             if (nt > 1) k_bvh_tree<<<grid_for(nt - 1, 128, sms), 128, 0, s>>>(P);
             else OURS_TRY(cudaMemsetAsync(P.parent, 0xff, sizeof(int) * 2, s));
@@ -1004,12 +1027,11 @@ cudaError_t ours_run(OursRun& R, cudaStream_t s) {
                 k_ours_fill_keys<<<grid_for(nrest, 256, sms), 256, 0, s>>>(rest, nrest, R.seed, it, fk);
                 size_t tb2 = R.cub_bytes;
                 OURS_TRY(cub::DeviceRadixSort::SortPairs(cub_temp, tb2, fk, fk2, rest, fv2, (int)nrest, 0, 64, s));
-                OURS_TRY(cudaMemcpyAsync(sel + nband, fv2, sizeof(uint32_t) * nfill, cudaMemcpyDeviceToDevice, s));
+                k_ours_point_keys<<<grid_for(nfill, 256, sms), 256, 0, s>>>(P, fv2, nfill, fk);
+                size_t tb3 = R.cub_bytes;
+                OURS_TRY(cub::DeviceRadixSort::SortPairs(cub_temp, tb3, fk, fk2, fv2, sel_sorted + nband, (int)nfill,
+                                                         0, 63, s));
             }
-            // query in Morton order: a warp's points form a compact block of the grid
-            k_ours_point_keys<<<grid_for(P.nsel, 256, sms), 256, 0, s>>>(P, sel, P.nsel, fk);
-            size_t tb3 = R.cub_bytes;
-            OURS_TRY(cub::DeviceRadixSort::SortPairs(cub_temp, tb3, fk, fk2, sel, sel_sorted, (int)P.nsel, 0, 63, s));
             OURS_TRY(cudaMemsetAsync(P.cell_count, 0, sizeof(unsigned int) * (nv + 1), s));
             OURS_TRY(cudaMemsetAsync(P.cell_fill, 0, sizeof(unsigned int) * (nv + 1), s));
             OURS_TRY(cudaMemsetAsync(P.heavy_count, 0, sizeof(unsigned int), s));
