@@ -214,7 +214,7 @@ template <typename T> void jacobi(T a[3][3], T V[3][3]) {
         const double diag = val(a[0][0]) * val(a[0][0]) + val(a[1][1]) * val(a[1][1]) + val(a[2][2]) * val(a[2][2]);
         const double doff = dnorm2(a[0][1]) + dnorm2(a[0][2]) + dnorm2(a[1][2]);
         const double dall = doff + dnorm2(a[0][0]) + dnorm2(a[1][1]) + dnorm2(a[2][2]);
-        if ((off <= 1e-36 * diag || off == 0.0) && doff <= 1e-30 * dall) break;
+        if ((off <= 1e-30 * diag || off == 0.0) && doff <= 1e-30 * dall) break;
         for (int p = 0; p < 2; ++p) {
             for (int q = p + 1; q < 3; ++q) {
                 const T apq = a[p][q];

@@ -152,12 +152,15 @@ int edge_idx_from_points(int ci, int cj, int ck, int i0, int j0, int k0, int i1,
 
 // Cyclic Jacobi eigen-decomposition of a symmetric 3x3 matrix (Golub & Van Loan 8.5).
 // On return a[][] holds eigenvalues on its diagonal and V's columns are eigenvectors.
+// Stops when the off-diagonal mass is below 1e-30 of the diagonal's (off-diagonals ~1e-15
+// relative, the level of Eigen's 2*eps per-pair test): a stricter bound sits under the
+// rounding noise a rotation leaves in a rank-1 matrix, which then never converges.
 void jacobi_eig3(double a[3][3], double V[3][3]) {
     for (int r = 0; r < 3; ++r) for (int c = 0; c < 3; ++c) V[r][c] = (r == c) ? 1.0 : 0.0;
     for (int sweep = 0; sweep < 64; ++sweep) {
         double off = a[0][1] * a[0][1] + a[0][2] * a[0][2] + a[1][2] * a[1][2];
         double diag = a[0][0] * a[0][0] + a[1][1] * a[1][1] + a[2][2] * a[2][2];
-        if (off <= 1e-36 * diag || off == 0.0) break;
+        if (off <= 1e-30 * diag || off == 0.0) break;
         for (int p = 0; p < 2; ++p) {
             for (int q = p + 1; q < 3; ++q) {
                 double apq = a[p][q];

@@ -133,8 +133,11 @@ __device__ inline void jacobi3(double a[3][3], double V[3][3]) {
     for (int sweep = 0; sweep < 64; ++sweep) {
         const double off = a[0][1] * a[0][1] + a[0][2] * a[0][2] + a[1][2] * a[1][2];
         const double diag = a[0][0] * a[0][0] + a[1][1] * a[1][1] + a[2][2] * a[2][2];
-        if (off <= 1e-36 * diag || off == 0.0) break;
+        if (off <= 1e-30 * diag || off == 0.0) break;
+        // unrolled: a and V stay in registers (the order of the rotations is unchanged)
+#pragma unroll
         for (int p = 0; p < 2; ++p) {
+#pragma unroll
             for (int q = p + 1; q < 3; ++q) {
                 const double apq = a[p][q];
                 if (apq == 0.0) continue;
@@ -161,6 +164,30 @@ __device__ inline void jacobi3(double a[3][3], double V[3][3]) {
     }
 }
 
+// Solve of Cell.cpp:318-361 for summed rows (A^T A, A^T b, sum of the m Hermite points):
+// the Jacobi eigen-decomposition and the pseudo-inverse truncated at thr, about the centroid.
+__device__ inline void solve_about_centroid(const double ATA[3][3], const double ATb[3], double c[3], int m,
+                                            double thr, double out[3]) {
+    for (int d = 0; d < 3; ++d) c[d] /= double(m);
+    double A[3][3], V[3][3];
+    for (int r = 0; r < 3; ++r) for (int s = 0; s < 3; ++s) A[r][s] = ATA[r][s];
+    jacobi3(A, V);
+    const double lam[3] = {A[0][0], A[1][1], A[2][2]};
+    double rhs[3];
+    for (int r = 0; r < 3; ++r) rhs[r] = ATb[r] - (ATA[r][0] * c[0] + ATA[r][1] * c[1] + ATA[r][2] * c[2]);
+    double x[3] = {c[0], c[1], c[2]};
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        const double sv = fabs(lam[q]);
+        if (sv > thr) {
+            const double proj = V[0][q] * rhs[0] + V[1][q] * rhs[1] + V[2][q] * rhs[2];
+            const double coef = proj / sv;
+            for (int d = 0; d < 3; ++d) x[d] += V[d][q] * coef;
+        }
+    }
+    out[0] = x[0]; out[1] = x[1]; out[2] = x[2];
+}
+
 // FP64 vertex of active cell (i,j,k), by one thread: Hermite samples with their averaged
 // normals in edge order (the CPU's std::map order), A^T A, A^T b and the centroid summed in
 // that order, then the Jacobi eigen-decomposition and the truncated pseudo-inverse about the
@@ -183,23 +210,7 @@ __device__ inline void cell_vertex_thread(const GridDesc& g, int i, int j, int k
         for (int d = 0; d < 3; ++d) c[d] += p[d];
         ++m;
     }
-    for (int d = 0; d < 3; ++d) c[d] /= double(m);
-    double A[3][3], V[3][3];
-    for (int r = 0; r < 3; ++r) for (int s = 0; s < 3; ++s) A[r][s] = ATA[r][s];
-    jacobi3(A, V);
-    const double lam[3] = {A[0][0], A[1][1], A[2][2]};
-    double rhs[3];
-    for (int r = 0; r < 3; ++r) rhs[r] = ATb[r] - (ATA[r][0] * c[0] + ATA[r][1] * c[1] + ATA[r][2] * c[2]);
-    double x[3] = {c[0], c[1], c[2]};
-    for (int q = 0; q < 3; ++q) {
-        const double sv = fabs(lam[q]);
-        if (sv > thr) {
-            const double proj = V[0][q] * rhs[0] + V[1][q] * rhs[1] + V[2][q] * rhs[2];
-            const double coef = proj / sv;
-            for (int d = 0; d < 3; ++d) x[d] += V[d][q] * coef;
-        }
-    }
-    out[0] = x[0]; out[1] = x[1]; out[2] = x[2];
+    solve_about_centroid(ATA, ATb, c, m, thr, out);
 }
 
 // gradientAt (contouring.cpp:141-207).

@@ -6,125 +6,25 @@
 //
 // Per cell: the Hermite samples (with the three neighbours' own samples of an averaged edge),
 // then A^T A, A^T b and the centroid summed in edge order (the CPU's std::map order), the
-// Jacobi eigen-decomposition and the truncated pseudo-inverse; a warp per cell (samples in
-// parallel, lane 0 sums and solves) when cells are few, a thread per cell when many.
+// Jacobi eigen-decomposition and the truncated pseudo-inverse; a lane per (cell, crossing
+// edge) and a lane per solve when cells are few, a thread per cell when many.
 #include "dcb_f64.cuh"
 
 namespace dcb {
 
 namespace f64 {
 
-// One (edge, cell) task of the 4-cell averaging: cell q around edge e of the centre cell
-// (q = 0 owner at the edge's minimum endpoint, 1 = -d1, 2 = -d2, 3 = both).
-struct Task64 {
-    double n[3];
-    double p[3];
-    int flags;   // bit0 valid sample, bit1 cell active, bit2 edge inside, bit3 own cell
-};
-
-__device__ void run_task(const GridDesc& g, const Cell64& C, int i, int j, int k, int T, Task64& R) {
-    R.flags = 0;
-    R.n[0] = R.n[1] = R.n[2] = 0.0;
-    R.p[0] = R.p[1] = R.p[2] = 0.0;
-    const int e = T >> 2, q = T & 3;
-    const int a = edge_a(e), b = edge_b(e);
-    if (C.cs[a] * C.cs[b] > 0.0) return;                 // no Hermite sample on this edge
-    const int Pa[3] = {i + corner_dx(a), j + corner_dy(a), k + corner_dz(a)};
-    const int Pb[3] = {i + corner_dx(b), j + corner_dy(b), k + corner_dz(b)};
-    int Pm[3], PM[3];
-    for (int d = 0; d < 3; ++d) { Pm[d] = min(Pa[d], Pb[d]); PM[d] = max(Pa[d], Pb[d]); }
-    const bool in0 = Pm[0] > 0 && Pm[0] < g.nx - 1 && Pm[1] > 0 && Pm[1] < g.ny - 1 && Pm[2] > 0 && Pm[2] < g.nz - 1;
-    const bool in1 = PM[0] > 0 && PM[0] < g.nx - 1 && PM[1] > 0 && PM[1] < g.ny - 1 && PM[2] > 0 && PM[2] < g.nz - 1;
-    const int axis = Pa[0] != Pb[0] ? 0 : (Pa[1] != Pb[1] ? 1 : 2);
-    const int d1 = axis == 0 ? 1 : 0;
-    const int d2 = axis == 2 ? 1 : 2;
-    int cc[3] = {Pm[0], Pm[1], Pm[2]};
-    if (q & 1) cc[d1] -= 1;
-    if (q & 2) cc[d2] -= 1;
-    const bool own = cc[0] == i && cc[1] == j && cc[2] == k;
-    if (in0 || in1) R.flags |= 4;
-    if (own) {
-        hermite(C, e, R.p, R.n);
-        R.flags |= 1 | 2 | 8;
-        return;
-    }
-    if (!(in0 || in1)) return;                            // neighbours only matter when averaged
-    Cell64 X;
-    load_cell(g, cc[0], cc[1], cc[2], X);
-    if (!active(X)) return;
-    R.flags |= 2;
-    const int ex = local_edge(axis, Pm[d1] - cc[d1], Pm[d2] - cc[d2]);
-    if (hermite(X, ex, R.p, R.n)) R.flags |= 1;
-}
-
 __device__ __forceinline__ double shfl_d(double v, int src) { return __shfl_sync(0xffffffffu, v, src); }
 
-// FP64 vertex of active cell (i,j,k), computed by the whole warp; valid in lane 0.
-__device__ void cell_vertex_warp(const GridDesc& g, int i, int j, int k, double thr, double out[3]) {
-    const int lane = threadIdx.x & 31;
-    Cell64 C;
-    load_cell(g, i, j, k, C);
-    // 48 tasks (12 edges x 4 cells): lane L runs tasks L and L + 32.
-    Task64 t0, t1;
-    run_task(g, C, i, j, k, lane, t0);
-    if (lane < 16) run_task(g, C, i, j, k, lane + 32, t1);
-    else t1.flags = 0, t1.n[0] = t1.n[1] = t1.n[2] = 0.0, t1.p[0] = t1.p[1] = t1.p[2] = 0.0;
-    // Lane e (< 12) gathers the four tasks of edge e: task 4e+q lives in lane (4e+q) & 31,
-    // slot (4e+q) >> 5.
-    double nq[4][3], po[3] = {0, 0, 0}, no[3] = {0, 0, 0};
-    int fq[4];
-    for (int q = 0; q < 4; ++q) {
-        const int T = 4 * lane + q;
-        const int src = T & 31;
-        const bool hi = T >= 32;
-        double a0[3], a1[3], b0[3], b1[3];
-        for (int d = 0; d < 3; ++d) {
-            a0[d] = shfl_d(t0.n[d], src); a1[d] = shfl_d(t1.n[d], src);
-            b0[d] = shfl_d(t0.p[d], src); b1[d] = shfl_d(t1.p[d], src);
-        }
-        const int f0 = __shfl_sync(0xffffffffu, t0.flags, src), f1 = __shfl_sync(0xffffffffu, t1.flags, src);
-        fq[q] = hi ? f1 : f0;
-        for (int d = 0; d < 3; ++d) nq[q][d] = hi ? a1[d] : a0[d];
-        if (fq[q] & 8) {
-            for (int d = 0; d < 3; ++d) { no[d] = nq[q][d]; po[d] = hi ? b1[d] : b0[d]; }
-        }
-    }
-    bool has = false;
-    double p[3] = {0, 0, 0}, n[3] = {0, 0, 0}, b = 0.0;
-    if (lane < 12) {
-        int own_q = -1;
-        for (int q = 0; q < 4; ++q) if (fq[q] & 8) own_q = q;
-        has = own_q >= 0;
-        if (has) {
-            p[0] = po[0]; p[1] = po[1]; p[2] = po[2];
-            n[0] = no[0]; n[1] = no[1]; n[2] = no[2];
-            // averaging (hermite_update.cpp:334-438): inside, all four cells active
-            bool all = (fq[0] & 4) != 0;
-            for (int q = 0; q < 4; ++q) all = all && (fq[q] & 3) == 3;
-            if (all) {
-                double acc[3] = {0.0, 0.0, 0.0};
-                for (int q = 0; q < 4; ++q) {
-                    if (sqrt(sq3(nq[q])) > 0) { acc[0] += nq[q][0]; acc[1] += nq[q][1]; acc[2] += nq[q][2]; }
-                }
-                normalize3(acc);
-                n[0] = acc[0]; n[1] = acc[1]; n[2] = acc[2];
-            }
-            // Cell::update row (Cell.cpp:298-311), independent per row: normalise, b = n.p
-            if (sqrt(sq3(n)) > 0.0) normalize3(n);
-            b = n[0] * p[0] + n[1] * p[1] + n[2] * p[2];
-        }
-    }
-    const uint32_t mask = __ballot_sync(0xffffffffu, has);
+// One cell's rows summed in edge order (the CPU's std::map order), then the solve.
+__device__ void solve_rows(const double (*rows)[8], uint32_t mask, double thr, double out[3]) {
     double ATA[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, ATb[3] = {0, 0, 0}, c[3] = {0, 0, 0};
     int m = 0;
-    for (int e = 0; e < 12; ++e) {           // edge order = the CPU's std::map order
-        double pe[3], ne[3];
-        for (int d = 0; d < 3; ++d) {
-            pe[d] = shfl_d(p[d], e);
-            ne[d] = shfl_d(n[d], e);
-        }
-        const double bb = shfl_d(b, e);
+    for (int e = 0; e < 12; ++e) {
         if (!(mask & (1u << e))) continue;
+        const double* R = rows[e];
+        const double pe[3] = {R[0], R[1], R[2]}, ne[3] = {R[3], R[4], R[5]};
+        const double bb = R[6];
         for (int r = 0; r < 3; ++r) {
             for (int s = 0; s < 3; ++s) ATA[r][s] += ne[r] * ne[s];
             ATb[r] += ne[r] * bb;
@@ -132,24 +32,7 @@ __device__ void cell_vertex_warp(const GridDesc& g, int i, int j, int k, double 
         for (int d = 0; d < 3; ++d) c[d] += pe[d];
         ++m;
     }
-    if (lane != 0) return;
-    for (int d = 0; d < 3; ++d) c[d] /= double(m);
-    double A[3][3], V[3][3];
-    for (int r = 0; r < 3; ++r) for (int s = 0; s < 3; ++s) A[r][s] = ATA[r][s];
-    jacobi3(A, V);
-    const double lam[3] = {A[0][0], A[1][1], A[2][2]};
-    double rhs[3];
-    for (int r = 0; r < 3; ++r) rhs[r] = ATb[r] - (ATA[r][0] * c[0] + ATA[r][1] * c[1] + ATA[r][2] * c[2]);
-    double x[3] = {c[0], c[1], c[2]};
-    for (int q = 0; q < 3; ++q) {
-        const double sv = fabs(lam[q]);
-        if (sv > thr) {
-            const double proj = V[0][q] * rhs[0] + V[1][q] * rhs[1] + V[2][q] * rhs[2];
-            const double coef = proj / sv;
-            for (int d = 0; d < 3; ++d) x[d] += V[d][q] * coef;
-        }
-    }
-    out[0] = x[0]; out[1] = x[1]; out[2] = x[2];
+    solve_about_centroid(ATA, ATb, c, m, thr, out);
 }
 
 // ---- adjoint of the vertex map -----------------------------------------------------------
@@ -304,23 +187,76 @@ __device__ __forceinline__ void store64(const Vertex64Params& P, uint32_t r, uns
     }
 }
 
-// Listed cells' FP64 vertices: Vf[rank] (float) and/or V64[t] (double). With at most one cell
-// per warp of the launch, a warp shares each cell's 48 samples (short latency); with more,
-// a thread takes a whole cell (every lane busy). Both give the same bits.
-__global__ void __launch_bounds__(128)
+// Listed cells' FP64 vertices: Vf[rank] (float) and/or V64[t] (double). The launch holds as
+// many warps as fit on the GPU at once. With up to kGroupMax cells per warp, the warp's lanes
+// take its cells' crossing edges, one (cell, edge) each: the Hermite sample with its averaged
+// normal and the normalised row, into shared memory; then a lane per cell sums the rows in
+// edge order and solves. With more cells, a thread takes a whole cell. Both give the bits
+// of the CPU's double arithmetic.
+constexpr int kGroupMax = 8;
+constexpr int kV64Threads = 128;
+
+__global__ void __launch_bounds__(kV64Threads)
 k_vertex_fp64(Vertex64Params P) {
+    __shared__ double s_rows[kV64Threads / 32][kGroupMax][12][8];
+    __shared__ uint32_t s_mask[kV64Threads / 32][kGroupMax];
+    __shared__ uint8_t s_pair[kV64Threads / 32][kGroupMax * 12];
     const unsigned int n = min(*P.count, P.cap);
     const unsigned int warps = (gridDim.x * blockDim.x) >> 5;
-    if (n <= warps) {
-        const int lane = threadIdx.x & 31;
-        for (unsigned int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < n; t += warps) {
-            const uint32_t r = P.cells[t];
+    const unsigned int G = (n + warps - 1) / warps;
+    if (G <= (unsigned)kGroupMax) {
+        const int lane = threadIdx.x & 31, wb = threadIdx.x >> 5;
+        const unsigned int t0 = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * G;
+        if (t0 >= n) return;                                  // warp-uniform
+        const unsigned int cnt = min(G, n - t0);
+        // lane q < cnt: crossing edges of cell q (Cell.cpp:185: no sample when fa * fb > 0)
+        uint32_t emask = 0;
+        if ((unsigned)lane < cnt) {
+            const uint32_t r = P.cells[t0 + lane];
             int i, j, k;
             unpack_cell(P.list[r], i, j, k);
             const GridDesc g = P.B.slots[slot_of_rank(P.B, r)].g;
+            double cs[8];
+#pragma unroll
+            for (int c = 0; c < 8; ++c)
+                cs[c] = (double)__ldg(g.v + pidx(g, i + corner_dx(c), j + corner_dy(c), k + corner_dz(c)));
+#pragma unroll
+            for (int e = 0; e < 12; ++e)
+                if (!(cs[edge_a(e)] * cs[edge_b(e)] > 0.0)) emask |= 1u << e;
+            s_mask[wb][lane] = emask;
+        }
+        unsigned int off = __popc(emask);
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned int v = __shfl_up_sync(0xffffffffu, off, o);
+            if (lane >= o) off += v;
+        }
+        const unsigned int total = __shfl_sync(0xffffffffu, off, 31);
+        off -= __popc(emask);
+        for (uint32_t m = emask; m; m &= m - 1) s_pair[wb][off++] = (uint8_t)((lane << 4) | (__ffs(m) - 1));
+        __syncwarp();
+        for (unsigned int pr = lane; pr < total; pr += 32) {
+            const int q = s_pair[wb][pr] >> 4, e = s_pair[wb][pr] & 15;
+            const uint32_t r = P.cells[t0 + q];
+            int i, j, k;
+            unpack_cell(P.list[r], i, j, k);
+            const GridDesc g = P.B.slots[slot_of_rank(P.B, r)].g;
+            f64::Cell64 C;
+            f64::load_cell(g, i, j, k, C);
+            double p[3], nn[3];
+            f64::edge_sample(g, C, i, j, k, e, p, nn);
+            // Cell::update row (Cell.cpp:298-311): normalise, b = n.p
+            if (sqrt(f64::sq3(nn)) > 0.0) f64::normalize3(nn);
+            double* R = s_rows[wb][q][e];
+            R[0] = p[0]; R[1] = p[1]; R[2] = p[2];
+            R[3] = nn[0]; R[4] = nn[1]; R[5] = nn[2];
+            R[6] = nn[0] * p[0] + nn[1] * p[1] + nn[2] * p[2];
+        }
+        __syncwarp();
+        if ((unsigned)lane < cnt) {
             double x[3];
-            f64::cell_vertex_warp(g, i, j, k, P.thr, x);
-            if (lane == 0) store64(P, r, t, x);
+            f64::solve_rows(s_rows[wb][lane], s_mask[wb][lane], P.thr, x);
+            store64(P, P.cells[t0 + lane], t0 + lane, x);
         }
         return;
     }
@@ -337,10 +273,17 @@ k_vertex_fp64(Vertex64Params P) {
 
 cudaError_t launch_vertex_fp64(const Vertex64Params& P, long long max_items, int num_sms, cudaStream_t s) {
     if (max_items <= 0) return cudaSuccess;
-    long long blocks = (max_items + 127) / 128;
-    const long long cap = (long long)num_sms * 16;     // warp mode up to 9,472 cells
+    static int resident = 0;                           // blocks of k_vertex_fp64 per SM at once
+    if (resident == 0) {
+        int b = 0;
+        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_vertex_fp64, kV64Threads, 0);
+        if (e != cudaSuccess) return e;
+        resident = b > 0 ? b : 1;
+    }
+    long long blocks = (max_items + kV64Threads - 1) / kV64Threads;
+    const long long cap = (long long)num_sms * resident;
     if (blocks > cap) blocks = cap;
-    k_vertex_fp64<<<(unsigned)blocks, 128, 0, s>>>(P);
+    k_vertex_fp64<<<(unsigned)blocks, kV64Threads, 0, s>>>(P);
     return cudaGetLastError();
 }
 
