@@ -23,7 +23,7 @@
 extern "C" {
 #endif
 
-#define DCB_ABI_VERSION 2
+#define DCB_ABI_VERSION 3
 
 enum dcb_status {
     DCB_OK = 0,
@@ -51,7 +51,21 @@ typedef struct {
 
 enum dcb_method {
     DCB_METHOD_DUAL_CONTOURING = 1,   /* ContouringMethod::DualContouring (contouring.h:21-25) */
-    DCB_METHOD_OURS = 2               /* outer/inner vertex refinement (contouring.cpp:1255-1328) */
+    DCB_METHOD_OURS = 2,              /* outer/inner vertex refinement (contouring.cpp:1255-1328) */
+    DCB_METHOD_SPARSE = 3,            /* CudaSparseDualContouringBackend (include/dc_cuda.h:37-53):
+                                         brick culling, near-zero cells, thin edges, float QEF
+                                         clamped into the cell (src/cuda/dc_cuda_sparse.cu)     */
+    DCB_METHOD_SPARSE_MVDC = 4        /* CudaSparseMvdcDualContouringBackend (dc_cuda.h:55-62): the
+                                         same with up to two vertices per cell                 */
+};
+
+/* Normal of a crossing edge's sample on the sparse backends (NormalComputationMode,
+ * include/dc_cuda.h:5-9). PRECOMPUTED behaves as TRILINEAR: the reference passes no
+ * precomputed gradients to its kernels (src/cuda/dc_cuda_sparse.cu:1306-1333). */
+enum dcb_normal_mode {
+    DCB_NORMAL_TRILINEAR = 0,         /* FiniteDifference: trilinear gradient at the sample */
+    DCB_NORMAL_EDGE_GRADIENT = 1,     /* EdgeGradient: lerp of the end points' central differences */
+    DCB_NORMAL_PRECOMPUTED = 2        /* PrecomputedGradient */
 };
 
 /* Mirrors ContouringOptions (include/contouring.h:27-41) plus the B200 precision knobs. */
@@ -77,6 +91,9 @@ typedef struct {
     double new_hermite_normal_weight; /* default 0.2 */
     uint64_t seed;                /* random fill of the sphere batch (the reference draws
                                      from std::random_device; here it is seeded)          */
+    /* DCB_METHOD_SPARSE / _MVDC only (CudaSparseDualContouringBackend's constructor): */
+    int brick_size;               /* default 8 (dc_cli.cpp:217) */
+    int normal_mode;              /* dcb_normal_mode, default DCB_NORMAL_TRILINEAR */
 } dcb_opts;
 
 /* Fill `o` with the reference defaults (contouring.h:27-41) and the B200 knobs. */
@@ -102,6 +119,18 @@ typedef struct {
     int64_t escalated_fp64_cells;   /* == qef_fallback_count */
     int64_t winding_fp64_faces;     /* faces whose orientation was re-decided in FP64 */
     int64_t rank_hist[4];           /* retained-rank histogram of the QEF solves */
+    /* sparse backends (DualContouringStats, include/dc_backend.h:44-78); qef_fallback_count
+     * then counts QEF solves that fell back to the centroid and clamp_count the vertices
+     * clamped into their cell */
+    int64_t total_bricks;
+    int64_t active_bricks;
+    int64_t invalid_count;
+    int64_t ambiguous_cells;
+    int64_t multi_vertex_cells;
+    int64_t one_vertex_cells;
+    int64_t two_vertex_cells;
+    int64_t split_rejection_count;
+    int64_t faces_skipped;          /* faces_skipped_due_to_missing_cluster */
 } dcb_stats;
 
 /* Device-resident mesh; pointers are owned by the handle and stay valid until the next

@@ -3,7 +3,8 @@
 The oracle is the FP64 C++ restatement in ``oracle/dc_oracle.cpp`` of the reference's
 ``CpuDualContouringBackend::extract`` (src/cpp/dc_backend.cpp:51-125), and the float
 restatement in ``oracle/mts_oracle.cpp`` of its mesh -> SDF conversion
-(src/cuda/mesh_to_sdf_cuda.cu:740-1009), and ``oracle/dc_adjoint_oracle.cpp``: the per-cell
+(src/cuda/mesh_to_sdf_cuda.cu:740-1009), and ``oracle/sparse_oracle.cpp``: the float restatement of the reference's sparse (brick) and
+multi-vertex GPU backends (src/cuda/dc_cuda_sparse.cu), and ``oracle/dc_adjoint_oracle.cpp``: the per-cell
 FP64 vertex as a template run with double (for finite differences) and with dual numbers
 (the FP64 reference Jacobian of each vertex with respect to its 4x4x4 stencil).  Only ``tests/``,
 ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline / reference legs import this
@@ -20,6 +21,7 @@ _DC_LIB = os.path.join(_HERE, "_build", "libdc_oracle.so")
 _MTS_LIB = os.path.join(_HERE, "_build", "libmts_oracle.so")
 _ADJ_LIB = os.path.join(_HERE, "_build", "libdc_adjoint_oracle.so")
 _OURS_LIB = os.path.join(_HERE, "_build", "libours_oracle.so")
+_SPARSE_LIB = os.path.join(_HERE, "_build", "libsparse_oracle.so")
 _libs = {}
 
 
@@ -324,3 +326,95 @@ def ours(values, dims, spacing, origin, outer_iters=100, inner_iters=100, mu=0.1
                      float(origin[0]), float(origin[1]), float(origin[2]), vals.ctypes.data, ctypes.byref(o),
                      int(threads), ctypes.byref(st))
     return _collect(lib, h, st)
+
+
+SPARSE_STATS = ("total_bricks", "active_bricks", "active_cells", "qef_fallbacks", "clamps", "invalid",
+                "ambiguous_cells", "multi_vertex_cells", "one_vertex_cells", "two_vertex_cells",
+                "split_rejections", "faces_skipped")
+
+
+def _sparse():
+    lib = _load(_SPARSE_LIB)
+    if not getattr(lib, "_typed", False):
+        lib.sdo_extract.restype = ctypes.c_void_p
+        lib.sdo_extract.argtypes = [ctypes.c_void_p] + [ctypes.c_int] * 3 + [ctypes.c_float] * 6 + [ctypes.c_int] * 4
+        for f in ("sdo_num_vertices", "sdo_num_faces", "sdo_num_cells"):
+            getattr(lib, f).restype = ctypes.c_int64
+            getattr(lib, f).argtypes = [ctypes.c_void_p]
+        lib.sdo_copy.restype = None
+        lib.sdo_copy.argtypes = [ctypes.c_void_p] * 7
+        lib.sdo_free.restype = None
+        lib.sdo_free.argtypes = [ctypes.c_void_p]
+        lib._typed = True
+    return lib
+
+
+def sparse_extract(values, dims, spacing, origin, brick_size=8, mvdc=False, normal_mode=0, threads=0):
+    """The reference's sparse brick backend (mvdc=False) or its multi-vertex variant
+    (mvdc=True), restated in float. Returns V (float32), vertex normals N (float32, the
+    multi-vertex variant's per-vertex normals), quads F (int32), the active cells' linear
+    indices, each active cell's first vertex, and the counters of SPARSE_STATS."""
+    lib = _sparse()
+    v = np.ascontiguousarray(values, dtype=np.float32).reshape(-1)
+    nx, ny, nz = (int(d) for d in dims)
+    assert v.size == nx * ny * nz
+    h = lib.sdo_extract(v.ctypes.data, nx, ny, nz, *(float(x) for x in spacing), *(float(x) for x in origin),
+                        int(brick_size), int(bool(mvdc)), int(normal_mode), int(threads))
+    if not h:
+        raise ValueError("sparse oracle rejected the grid")
+    try:
+        nv, nf, nc = lib.sdo_num_vertices(h), lib.sdo_num_faces(h), lib.sdo_num_cells(h)
+        V = np.empty((nv, 3), np.float32)
+        N = np.empty((nv, 3), np.float32)
+        F = np.empty((nf, 4), np.int32)
+        cells = np.empty(nc, np.int64)
+        vstart = np.empty(nc, np.int32)
+        st = np.zeros(len(SPARSE_STATS), np.int64)
+        lib.sdo_copy(h, V.ctypes.data, N.ctypes.data, F.ctypes.data, cells.ctypes.data, vstart.ctypes.data,
+                     st.ctypes.data)
+    finally:
+        lib.sdo_free(h)
+    return {"V": V, "N": N, "F": F, "cells": cells, "vstart": vstart, "stats": dict(zip(SPARSE_STATS, st.tolist()))}
+
+
+def ref_sparse(d_values_ptr, dims, spacing, origin, brick_size=8, normal_mode=0, mvdc=False, exact=True):
+    """The reference's own sparse CUDA backend (src/cuda/dc_cuda_sparse.cu), built from its
+    source into ``oracle/_ref/`` (``make -C oracle ref``): ``exact`` selects the build without
+    FMA contraction (the parity pin), otherwise the build as shipped (the speed bar). Runs on
+    the current CUDA device on a device grid; returns V, F, the counters of SPARSE_STATS plus
+    vertex and face counts, and the reference's own stage times (total, marking+compaction,
+    QEF, faces; ms). Returns None when the library was not built or the grid is refused."""
+    name = "libref_sparse_exact.so" if exact else "libref_sparse.so"
+    path = os.path.join(_HERE, "_ref", name)
+    if not os.path.exists(path):
+        return None
+    if path not in _libs:
+        lib = ctypes.CDLL(path)
+        lib.refsparse_run.restype = ctypes.c_void_p
+        lib.refsparse_run.argtypes = [ctypes.c_int] * 3 + [ctypes.c_float] * 6 + [ctypes.c_void_p] + [ctypes.c_int] * 3
+        for f in ("refsparse_num_vertices", "refsparse_num_faces"):
+            getattr(lib, f).restype = ctypes.c_int64
+            getattr(lib, f).argtypes = [ctypes.c_void_p]
+        lib.refsparse_copy.restype = None
+        lib.refsparse_copy.argtypes = [ctypes.c_void_p] * 5
+        lib.refsparse_free.restype = None
+        lib.refsparse_free.argtypes = [ctypes.c_void_p]
+        _libs[path] = lib
+    lib = _libs[path]
+    nx, ny, nz = (int(d) for d in dims)
+    h = lib.refsparse_run(nx, ny, nz, *(float(x) for x in spacing), *(float(x) for x in origin),
+                          ctypes.c_void_p(int(d_values_ptr)), int(brick_size), int(normal_mode), int(bool(mvdc)))
+    if not h:
+        return None
+    try:
+        nv, nf = lib.refsparse_num_vertices(h), lib.refsparse_num_faces(h)
+        V = np.empty((nv, 3), np.float32)
+        F = np.empty((nf, 4), np.int32)
+        st = np.zeros(16, np.int64)
+        times = np.zeros(4, np.float64)
+        lib.refsparse_copy(h, V.ctypes.data, F.ctypes.data, st.ctypes.data, times.ctypes.data)
+    finally:
+        lib.refsparse_free(h)
+    stats = dict(zip(SPARSE_STATS, st[:12].tolist()))
+    stats.update(vertex_count=int(st[12]), face_count=int(st[13]))
+    return {"V": V, "F": F, "stats": stats, "times": times.tolist()}

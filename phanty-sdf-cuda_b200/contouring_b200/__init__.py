@@ -2,11 +2,14 @@
 
 Public names mirror the reference module ``_contouring_cpp_module`` (src/cpp/bindings.cpp):
 ``DenseSdfGrid``, ``DenseSdfGridDevice``, ``DualContouringMesh``, ``DualContouringStats``,
-``ContouringOptions``, ``ContouringMethod``; the new backend is ``B200DualContouringBackend``.
+``ContouringOptions``, ``ContouringMethod``, ``NormalComputationMode``; the new backends are
+``B200DualContouringBackend`` and, for the reference's sparse CUDA backends,
+``B200SparseDualContouringBackend`` / ``B200SparseMvdcDualContouringBackend``.
 """
-from .backend import (B200DualContouringBackend, ContouringMethod, ContouringOptions, DcbError,
+from .backend import (B200DualContouringBackend, B200SparseDualContouringBackend,
+                      B200SparseMvdcDualContouringBackend, ContouringMethod, ContouringOptions, DcbError,
                       DenseSdfGrid, DenseSdfGridDevice, DualContouringMesh, DualContouringStats,
-                      MeshSdfStats, mesh_to_sdf_cuda, mesh_to_sdf_tensor)
+                      MeshSdfStats, NormalComputationMode, mesh_to_sdf_cuda, mesh_to_sdf_tensor)
 from . import _lib
 
 
@@ -17,6 +20,7 @@ def __getattr__(name):
         return getattr(autograd, name)
     raise AttributeError(name)
 
-__all__ = ["B200DualContouringBackend", "ContouringMethod", "ContouringOptions", "DcbError",
+__all__ = ["B200DualContouringBackend", "B200SparseDualContouringBackend", "B200SparseMvdcDualContouringBackend",
+           "NormalComputationMode", "ContouringMethod", "ContouringOptions", "DcbError",
            "DenseSdfGrid", "DenseSdfGridDevice", "DualContouringMesh", "DualContouringStats",
            "MeshSdfStats", "mesh_to_sdf_cuda", "mesh_to_sdf_tensor", "dual_contour", "DualContourFunction"]

@@ -20,6 +20,8 @@ DCB_ERR_INTERNAL = -7
 
 DCB_METHOD_DUAL_CONTOURING = 1
 DCB_METHOD_OURS = 2
+DCB_METHOD_SPARSE = 3
+DCB_METHOD_SPARSE_MVDC = 4
 
 # Every symbol include/dcb.h declares (checked by the CPU test suite).
 EXPORTED = (
@@ -45,7 +47,8 @@ class DcbOpts(ctypes.Structure):
                 ("fp64_threshold_band", ctypes.c_double), ("emit_triangles", ctypes.c_int),
                 ("force_fp64", ctypes.c_int), ("hermite_update", ctypes.c_int), ("batch_size", ctypes.c_int),
                 ("new_hermite_pos_weight", ctypes.c_double), ("new_face_pos_weight", ctypes.c_double),
-                ("new_hermite_normal_weight", ctypes.c_double), ("seed", ctypes.c_uint64)]
+                ("new_hermite_normal_weight", ctypes.c_double), ("seed", ctypes.c_uint64),
+                ("brick_size", ctypes.c_int), ("normal_mode", ctypes.c_int)]
 
 
 class DcbStats(ctypes.Structure):
@@ -57,7 +60,12 @@ class DcbStats(ctypes.Structure):
                 ("face_emission_ms", ctypes.c_float), ("download_ms", ctypes.c_float),
                 ("total_ms", ctypes.c_float), ("qef_fallback_count", ctypes.c_int64),
                 ("clamp_count", ctypes.c_int64), ("escalated_fp64_cells", ctypes.c_int64),
-                ("winding_fp64_faces", ctypes.c_int64), ("rank_hist", ctypes.c_int64 * 4)]
+                ("winding_fp64_faces", ctypes.c_int64), ("rank_hist", ctypes.c_int64 * 4),
+                ("total_bricks", ctypes.c_int64), ("active_bricks", ctypes.c_int64),
+                ("invalid_count", ctypes.c_int64), ("ambiguous_cells", ctypes.c_int64),
+                ("multi_vertex_cells", ctypes.c_int64), ("one_vertex_cells", ctypes.c_int64),
+                ("two_vertex_cells", ctypes.c_int64), ("split_rejection_count", ctypes.c_int64),
+                ("faces_skipped", ctypes.c_int64)]
 
 
 class DcbMeshDev(ctypes.Structure):

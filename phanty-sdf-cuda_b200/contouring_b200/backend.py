@@ -25,6 +25,13 @@ class ContouringMethod(enum.IntEnum):
     Ours = 2
 
 
+class NormalComputationMode(enum.IntEnum):
+    """NormalComputationMode (include/dc_cuda.h:5-9) of the sparse backends."""
+    FiniteDifference = 0
+    EdgeGradient = 1
+    PrecomputedGradient = 2
+
+
 class ContouringOptions:
     """ContouringOptions (include/contouring.h:27-41) plus the B200 precision knobs."""
 
@@ -53,6 +60,11 @@ class ContouringOptions:
         self.emit_triangles = False
         self.force_fp64 = False
         self.seed = 0x5eed
+        # the sparse backends (set by B200SparseDualContouringBackend): 0 dense, 1 sparse,
+        # 2 sparse with up to two vertices per cell
+        self.sparse = 0
+        self.brick_size = 8
+        self.normal_mode = NormalComputationMode.FiniteDifference
 
     def to_c(self):
         o = _lib.default_opts()
@@ -75,6 +87,10 @@ class ContouringOptions:
         o.new_face_pos_weight = float(self.new_face_pos_weight)
         o.new_hermite_normal_weight = float(self.new_hermite_normal_weight)
         o.seed = int(self.seed)
+        o.brick_size = int(self.brick_size)
+        o.normal_mode = int(self.normal_mode)
+        if self.sparse:
+            o.method = _lib.DCB_METHOD_SPARSE_MVDC if int(self.sparse) == 2 else _lib.DCB_METHOD_SPARSE
         return o
 
 
@@ -151,8 +167,11 @@ class DualContouringStats:
         for f in ("nx", "ny", "nz", "total_cells", "active_cells", "vertex_count", "face_count",
                   "upload_ms", "marking_ms", "compaction_ms", "qef_ms", "face_emission_ms",
                   "download_ms", "total_ms", "qef_fallback_count", "clamp_count",
-                  "escalated_fp64_cells", "winding_fp64_faces"):
+                  "escalated_fp64_cells", "winding_fp64_faces", "total_bricks", "active_bricks",
+                  "invalid_count", "ambiguous_cells", "multi_vertex_cells", "one_vertex_cells",
+                  "two_vertex_cells", "split_rejection_count"):
             setattr(s, f, getattr(st, f))
+        s.faces_skipped_due_to_missing_cluster = st.faces_skipped
         s.active_cell_marking_ms = st.marking_ms
         s.rank_hist = list(st.rank_hist)
         return s
@@ -352,6 +371,43 @@ class B200DualContouringBackend:
                                         ctypes.c_void_p(out.data_ptr()), int(bool(accumulate)),
                                         ctypes.c_void_p(s)), self._h)
         return out
+
+
+class B200SparseDualContouringBackend(B200DualContouringBackend):
+    """Drop-in for ``CudaSparseDualContouringBackend(brick_size, normal_mode, chunk_size,
+    multi_vertex_cells)`` (include/dc_cuda.h:37-53, src/cpp/bindings.cpp:229-249): brick
+    culling, near-zero cells, thin edges, a float QEF clamped into the cell; with
+    ``multi_vertex_cells`` up to two vertices per cell. ``chunk_size`` is accepted and, as in
+    the reference's kernels, unused. ``extract`` / ``extract_device`` / ``extract_tensor``
+    behave as on the dense backend; a backward pass and batches are dense-only."""
+
+    def __init__(self, brick_size=8, normal_mode=NormalComputationMode.FiniteDifference, chunk_size=0,
+                 multi_vertex_cells=False, device=0):
+        super().__init__(device)
+        self.brick_size = brick_size
+        self.normal_mode = normal_mode
+        self.chunk_size = chunk_size
+        self.multi_vertex_cells = multi_vertex_cells
+
+    @property
+    def options(self):
+        o = self._options
+        o.sparse = 2 if self.multi_vertex_cells else 1
+        o.brick_size = int(self.brick_size)
+        o.normal_mode = int(self.normal_mode)
+        return o
+
+    @options.setter
+    def options(self, value):
+        self._options = value
+
+
+class B200SparseMvdcDualContouringBackend(B200SparseDualContouringBackend):
+    """Drop-in for ``CudaSparseMvdcDualContouringBackend(brick_size, normal_mode, chunk_size)``
+    (include/dc_cuda.h:55-62): the sparse backend with up to two vertices per cell."""
+
+    def __init__(self, brick_size=8, normal_mode=NormalComputationMode.FiniteDifference, chunk_size=0, device=0):
+        super().__init__(brick_size, normal_mode, chunk_size, True, device)
 
 
 class MeshSdfStats:

@@ -185,6 +185,21 @@ def thin_gap(res=32):
     return torch.from_numpy(np.minimum(d1, d2).reshape(-1).astype(np.float32)), (res,) * 3, sp, org
 
 
+def thin_shell(res=48, radius=0.3, half_width=0.3, seed=0):
+    """A spherical shell thinner than a cell, |r - radius| - half_width * h (h the spacing,
+    half_width < 0.5): where the shell falls between two grid points both are positive, small
+    and have opposed gradients — the sparse backends' thin edges, and cells whose samples
+    split into two vertices. A seeded shift of the centre (within a cell) varies the cut."""
+    lo, hi = -0.5, 0.5
+    dims, sp, org = _grid_params(res, lo, hi)
+    c = np.random.default_rng(seed).uniform(-0.5, 0.5, 3) * sp[0]
+    ax = _axis(res, lo, sp[0], "cpu").numpy().astype(np.float64)
+    Z, Y, X = np.meshgrid(ax, ax, ax, indexing="ij")
+    r = np.sqrt((X - c[0]) ** 2 + (Y - c[1]) ** 2 + (Z - c[2]) ** 2)
+    v = np.abs(r - radius) - half_width * sp[0]
+    return torch.from_numpy(v.reshape(-1).astype(np.float32)), dims, sp, org
+
+
 def constant(res, value):
     """Constant grid (dc_tests.cpp:171-215 use +1 and -1 on 16^3)."""
     _, sp, org = _cli_axes(res)

@@ -58,6 +58,12 @@ struct dcb_context {
     DevBuf grid, bits, super, list, seg_count, seg_start, counters, V, vclass, fmask, col_count, col_fill,
         col_start, partials, esc_list, hard_list, hard_data, stage_quad, stage_key, faces, wind_items,
         v64_index, v64_cells, V64, tris, tri_items, adj_rows, adj_owners, ours_ws;
+    // sparse backends
+    DevBuf sp_words, sp_brick, sp_vcount, sp_vstart, sp_vtmp, sp_ntmp, sp_N, sp_vcell, sp_fcount, sp_fstart,
+        sp_counters;
+    void* h_sp_counters = nullptr;    // pinned copy of the sparse counters
+    int last_kind = 0;                // last extraction: 0 dense dual contouring, 1 sparse
+    int cells_per_vertex = 0;         // 1: the vertex -> cell list is `sp_vcell` (two vertices per cell)
     // mesh -> SDF workspace
     DevBuf m_verts, m_faces, m_out, m_tris, m_bin_count, m_bin_start, m_bin_fill, m_bin_scratch, m_bin_tris,
         m_bin_active, m_active_list, m_axis_start, m_far, m_ext, m_tmp, m_partials, m_counters;
@@ -331,6 +337,8 @@ int run_batch(dcb_context* h, const dcb_grid* in, int n, const dcb_opts* o, cuda
     h->cy = L.slots[0].g.cy;
     h->cz = L.slots[0].g.cz;
     h->batch_n = n;
+    h->last_kind = 0;
+    h->cells_per_vertex = 0;
     h->batch_cx.resize(n); h->batch_cy.resize(n);
     h->vert_offsets.assign(n + 1, 0);
     h->face_offsets.assign(n + 1, 0);
@@ -559,6 +567,173 @@ int run_ours(dcb_context* h, const dcb_grid* in, const dcb_opts* o, cudaStream_t
     return DCB_OK;
 }
 
+// The sparse (brick) backends (src/cuda/dc_cuda_sparse.cu:1171-1415) on one device grid:
+// point words -> bricks -> active-cell bits, scan + rank expansion, vertices (and, for the
+// multi-vertex variant, their scan and placement), face counts, scan, faces. Two host
+// read-backs: the active-cell count and the vertex and face totals.
+int run_sparse(dcb_context* h, const dcb_grid* in, const dcb_opts* o, cudaStream_t s, dcb_stats* st) {
+    if (o->emit_triangles) return fail(h, DCB_ERR_NOT_SUPPORTED, "the sparse backends emit quads only");
+    if (o->brick_size < 1 || o->brick_size > 4096) return fail(h, DCB_ERR_INVALID_ARGUMENT, "brick_size must be in [1, 4096]");
+    if (o->normal_mode < 0 || o->normal_mode > 2) return fail(h, DCB_ERR_INVALID_ARGUMENT, "unknown normal_mode");
+    if ((double)in->nx * in->ny * in->nz >= 2147483647.0)
+        return fail(h, DCB_ERR_TOO_LARGE, "the sparse backends index points with 32-bit ints (as the reference)");
+    const bool mvdc = o->method == DCB_METHOD_SPARSE_MVDC;
+    GridSlot S{};
+    GridDesc& g = S.g;
+    g.nx = in->nx; g.ny = in->ny; g.nz = in->nz;
+    g.cx = g.nx - 1; g.cy = g.ny - 1; g.cz = g.nz - 1;
+    g.W = ((g.cx + 31) / 32 + 7) / 8 * 8;
+    g.W8 = g.W / 8;
+    g.vx = in->vx; g.vy = in->vy; g.vz = in->vz;
+    g.ox = in->ox; g.oy = in->oy; g.oz = in->oz;
+    g.v = in->values;
+    S.tw = 32;
+    S.nxt = (g.W + 31) / 32;
+    SparseParams P{};
+    P.g = g;
+    P.bs = o->brick_size;
+    P.nbx = (g.cx + P.bs - 1) / P.bs; P.nby = (g.cy + P.bs - 1) / P.bs; P.nbz = (g.cz + P.bs - 1) / P.bs;
+    P.Wp = (g.nx + 31) / 32;
+    P.nxt = S.nxt;
+    P.mvdc = mvdc ? 1 : 0;
+    P.normal_mode = o->normal_mode;
+    P.close = 0.45f * g.vx;
+    const long long prow = (long long)g.ny * g.nz, crow = (long long)g.cy * g.cz;
+    const long long nb = (long long)P.nbx * P.nby * P.nbz, nseg = crow * S.nxt;
+    DCB_TRY(h, ensure(h->sp_words, sizeof(uint32_t) * 3 * prow * P.Wp), "alloc point words");
+    DCB_TRY(h, ensure(h->sp_brick, nb), "alloc brick flags");
+    DCB_TRY(h, ensure(h->bits, sizeof(uint32_t) * crow * g.W), "alloc bits");
+    DCB_TRY(h, ensure(h->super, sizeof(uint32_t) * crow * g.W8), "alloc ranks");
+    DCB_TRY(h, ensure(h->seg_count, sizeof(uint32_t) * nseg), "alloc segment counts");
+    DCB_TRY(h, ensure(h->seg_start, sizeof(uint32_t) * nseg), "alloc segment starts");
+    DCB_TRY(h, ensure(h->sp_counters, sizeof(unsigned long long) * kScSlots), "alloc counters");
+    if (!h->h_sp_counters) DCB_TRY(h, cudaMallocHost(&h->h_sp_counters, sizeof(unsigned long long) * kScSlots), "alloc pinned counters");
+    unsigned long long* dcn = as<unsigned long long>(h->sp_counters);
+    unsigned long long* hcn = reinterpret_cast<unsigned long long*>(h->h_sp_counters);
+    P.pn = as<uint32_t>(h->sp_words);
+    P.pp = P.pn + prow * P.Wp;
+    P.pc = P.pp + prow * P.Wp;
+    P.brick = as<uint8_t>(h->sp_brick);
+    P.bits = as<uint32_t>(h->bits);
+    P.super = as<uint32_t>(h->super);
+    P.seg_count = as<uint32_t>(h->seg_count);
+    P.counters = dcn;
+
+    // 1) point words, bricks, active-cell bits; scan -> the active count
+    DCB_TRY(h, cudaMemsetAsync(dcn, 0, sizeof(unsigned long long) * kScSlots, s), "memset counters");
+    DCB_TRY(h, launch_sparse_mark(P, h->num_sms, s), "launch sparse mark");
+    DCB_TRY(h, cudaEventRecord(h->ev[6], s), "event");
+    long long plen = std::max(1LL, scan_partials_len(nseg));
+    DCB_TRY(h, ensure(h->partials, sizeof(uint32_t) * plen), "alloc scan");
+    DCB_TRY(h, launch_scan(P.seg_count, nseg, as<uint32_t>(h->partials), as<uint32_t>(h->seg_start),
+                           dcn + kScActiveCells, s), "launch segment scan");
+    DCB_TRY(h, cudaEventRecord(h->ev[2], s), "event");
+    DCB_TRY(h, cudaMemcpyAsync(hcn, dcn, sizeof(unsigned long long) * kScSlots, cudaMemcpyDeviceToHost, s), "read counts");
+    DCB_TRY(h, cudaStreamSynchronize(s), "sparse mark");
+    const long long na = (long long)hcn[kScActiveCells];
+    if (na >= (mvdc ? 0x3fffffffLL : 0x7fffffffLL)) return fail(h, DCB_ERR_TOO_LARGE, "more than 2^31-1 vertices");
+
+    h->last_kind = 1;
+    h->cells_per_vertex = mvdc ? 1 : 0;
+    h->nv = 0; h->nf = 0; h->vpf = 4;
+    h->cx = g.cx; h->cy = g.cy; h->cz = g.cz;
+    h->batch_n = 1;
+    h->vert_offsets.assign(2, 0);
+    h->face_offsets.assign(2, 0);
+    if (st) {
+        st->nx = g.nx; st->ny = g.ny; st->nz = g.nz;
+        st->total_cells = (long long)g.cx * crow; st->active_cells = na;
+        st->total_bricks = nb;
+    }
+    long long nverts = 0, nf = 0;
+    if (na > 0) {
+        // 2) ranks + list, vertices
+        DCB_TRY(h, ensure(h->list, sizeof(uint64_t) * na), "alloc active list");
+        DCB_TRY(h, ensure(h->V, sizeof(float) * 3 * (mvdc ? 2 * na : na)), "alloc vertices");
+        DCB_TRY(h, ensure(h->sp_fcount, sizeof(uint32_t) * na), "alloc face counts");
+        DCB_TRY(h, ensure(h->sp_fstart, sizeof(uint32_t) * na), "alloc face starts");
+        plen = std::max(plen, scan_partials_len(na));
+        DCB_TRY(h, ensure(h->partials, sizeof(uint32_t) * plen), "alloc scan");
+        ExpandParams xp{};
+        xp.B.s0 = S; xp.B.n = 1;
+        xp.nseg = nseg; xp.bits = P.bits; xp.seg_count = P.seg_count; xp.seg_start = as<uint32_t>(h->seg_start);
+        xp.super = P.super; xp.list = as<uint64_t>(h->list); xp.cell_slot = nullptr;
+        DCB_TRY(h, launch_expand(xp, h->num_sms, s), "launch expand");
+        P.list = xp.list;
+        P.nactive = na;
+        P.V = as<float>(h->V);
+        if (mvdc) {
+            DCB_TRY(h, ensure(h->sp_vcount, sizeof(uint32_t) * na), "alloc vertex counts");
+            DCB_TRY(h, ensure(h->sp_vstart, sizeof(uint32_t) * na), "alloc vertex starts");
+            DCB_TRY(h, ensure(h->sp_vtmp, sizeof(float) * 6 * na), "alloc vertex staging");
+            DCB_TRY(h, ensure(h->sp_ntmp, sizeof(float) * 6 * na), "alloc normal staging");
+            DCB_TRY(h, ensure(h->sp_N, sizeof(float) * 6 * na), "alloc vertex normals");
+            DCB_TRY(h, ensure(h->sp_vcell, sizeof(uint64_t) * 2 * na), "alloc vertex cells");
+            P.vcount = as<uint32_t>(h->sp_vcount); P.vstart = as<uint32_t>(h->sp_vstart);
+            P.vtmp = as<float>(h->sp_vtmp); P.ntmp = as<float>(h->sp_ntmp);
+            P.N = as<float>(h->sp_N); P.vcell = as<uint64_t>(h->sp_vcell);
+        }
+        DCB_TRY(h, launch_sparse_vertices(P, h->num_sms, s), "launch sparse vertices");
+        if (mvdc) {
+            DCB_TRY(h, launch_scan(P.vcount, na, as<uint32_t>(h->partials), as<uint32_t>(h->sp_vstart),
+                                   dcn + kScVertices, s), "launch vertex scan");
+            DCB_TRY(h, launch_sparse_place(P, h->num_sms, s), "launch vertex placement");
+        }
+        DCB_TRY(h, cudaEventRecord(h->ev[3], s), "event");
+        // 3) faces: counts, scan, emission
+        P.fcount = as<uint32_t>(h->sp_fcount);
+        P.fstart = as<uint32_t>(h->sp_fstart);
+        DCB_TRY(h, launch_sparse_faces(P, false, h->num_sms, s), "launch face count");
+        DCB_TRY(h, launch_scan(P.fcount, na, as<uint32_t>(h->partials), as<uint32_t>(h->sp_fstart),
+                               dcn + kScFaces, s), "launch face scan");
+        DCB_TRY(h, cudaMemcpyAsync(hcn, dcn, sizeof(unsigned long long) * kScSlots, cudaMemcpyDeviceToHost, s), "read totals");
+        DCB_TRY(h, cudaStreamSynchronize(s), "sparse vertices");
+        nverts = mvdc ? (long long)hcn[kScVertices] : na;
+        nf = (long long)hcn[kScFaces];
+        if (nf >= 0x7fffffffLL) return fail(h, DCB_ERR_TOO_LARGE, "more than 2^31-1 faces");
+        DCB_TRY(h, ensure(h->faces, sizeof(int4) * std::max(1LL, nf)), "alloc faces");
+        P.faces = as<int4>(h->faces);
+        DCB_TRY(h, launch_sparse_faces(P, true, h->num_sms, s), "launch face emission");
+    } else {
+        DCB_TRY(h, cudaEventRecord(h->ev[3], s), "event");
+    }
+    DCB_TRY(h, cudaEventRecord(h->ev[4], s), "event");
+    DCB_TRY(h, cudaMemcpyAsync(hcn, dcn, sizeof(unsigned long long) * kScSlots, cudaMemcpyDeviceToHost, s), "read counters");
+    DCB_TRY(h, cudaStreamSynchronize(s), "sparse faces");
+    h->nv = nverts;
+    h->nf = nf;
+    h->vert_offsets[1] = nverts;
+    h->face_offsets[1] = nf;
+    if (st) {
+        st->vertex_count = nverts;
+        st->face_count = nf;
+        st->active_bricks = (int64_t)hcn[kScActiveBricks];
+        st->qef_fallback_count = (int64_t)hcn[kScFallback];
+        st->clamp_count = (int64_t)hcn[kScClamp];
+        st->invalid_count = (int64_t)hcn[kScInvalid];
+        st->ambiguous_cells = (int64_t)hcn[kScAmbiguous];
+        st->multi_vertex_cells = (int64_t)hcn[kScMulti];
+        st->one_vertex_cells = (int64_t)hcn[kScOne];
+        st->two_vertex_cells = (int64_t)hcn[kScTwo];
+        st->split_rejection_count = (int64_t)hcn[kScSplitReject];
+        st->faces_skipped = (int64_t)hcn[kScSkipped];
+    }
+    return DCB_OK;
+}
+
+// The extraction a method names, on a device grid.
+int run_method(dcb_context* h, const dcb_grid* in, const dcb_opts* o, cudaStream_t s, dcb_stats* st) {
+    if (o->method == DCB_METHOD_SPARSE || o->method == DCB_METHOD_SPARSE_MVDC) return run_sparse(h, in, o, s, st);
+    h->last_kind = 0;
+    h->cells_per_vertex = 0;
+    return o->method == DCB_METHOD_OURS ? run_ours(h, in, o, s, st) : run_pipeline(h, in, o, s, st);
+}
+
+bool known_method(int m) {
+    return m == DCB_METHOD_DUAL_CONTOURING || m == DCB_METHOD_OURS || m == DCB_METHOD_SPARSE ||
+           m == DCB_METHOD_SPARSE_MVDC;
+}
+
 void fill_times(dcb_context* h, dcb_stats* st, bool upload) {
     if (!st) return;
     st->upload_ms = upload ? elapsed(h->ev[0], h->ev[1]) : 0.f;
@@ -695,6 +870,8 @@ void dcb_default_opts(dcb_opts* o) {
     o->new_face_pos_weight = 0.2;
     o->new_hermite_normal_weight = 0.2;
     o->seed = 0x5eed;
+    o->brick_size = 8;
+    o->normal_mode = DCB_NORMAL_TRILINEAR;
 }
 
 int dcb_abi_version(void) { return DCB_ABI_VERSION; }
@@ -743,10 +920,13 @@ int dcb_destroy(dcb_handle h) {
                       &h->tris, &h->tri_items, &h->m_verts, &h->m_faces, &h->m_out, &h->m_tris,
                       &h->m_bin_count, &h->m_bin_start, &h->m_bin_fill, &h->m_bin_scratch, &h->m_bin_tris,
                       &h->m_bin_active, &h->m_active_list, &h->m_axis_start, &h->m_far, &h->m_ext, &h->m_tmp,
-                      &h->m_partials, &h->m_counters, &h->table, &h->cell_slot, &h->adj_rows, &h->adj_owners, &h->ours_ws};
+                      &h->m_partials, &h->m_counters, &h->table, &h->cell_slot, &h->adj_rows, &h->adj_owners, &h->ours_ws,
+                      &h->sp_words, &h->sp_brick, &h->sp_vcount, &h->sp_vstart, &h->sp_vtmp, &h->sp_ntmp,
+                      &h->sp_N, &h->sp_vcell, &h->sp_fcount, &h->sp_fstart, &h->sp_counters};
     for (DevBuf* b : bufs) if (b->p) cudaFree(b->p);
     if (h->h_counters) cudaFreeHost(h->h_counters);
     if (h->h_sdf_counters) cudaFreeHost(h->h_sdf_counters);
+    if (h->h_sp_counters) cudaFreeHost(h->h_sp_counters);
     if (h->h_table) cudaFreeHost(h->h_table);
     if (h->h_offsets) cudaFreeHost(h->h_offsets);
     if (h->hV) cudaFreeHost(h->hV);
@@ -763,15 +943,14 @@ int dcb_extract_device(dcb_handle h, const dcb_grid* grid, const dcb_opts* opts,
     dcb_opts def;
     dcb_default_opts(&def);
     const dcb_opts* o = opts ? opts : &def;
-    if (o->method != DCB_METHOD_DUAL_CONTOURING && o->method != DCB_METHOD_OURS)
-        return fail(h, DCB_ERR_NOT_SUPPORTED, "unknown method");
+    if (!known_method(o->method)) return fail(h, DCB_ERR_NOT_SUPPORTED, "unknown method");
     if (!(o->svd_threshold >= 0.0)) return fail(h, DCB_ERR_INVALID_ARGUMENT, "svd_threshold must be >= 0");
     if (cudaSetDevice(h->device) != cudaSuccess) { cudaGetLastError(); return fail(h, DCB_ERR_CUDA, "set device"); }
     cudaStream_t s = reinterpret_cast<cudaStream_t>(cuda_stream);
     if (stats) std::memset(stats, 0, sizeof(*stats));
     DCB_TRY(h, cudaEventRecord(h->ev[0], s), "event");
     DCB_TRY(h, cudaEventRecord(h->ev[1], s), "event");
-    rc = o->method == DCB_METHOD_OURS ? run_ours(h, grid, o, s, stats) : run_pipeline(h, grid, o, s, stats);
+    rc = run_method(h, grid, o, s, stats);
     if (rc != DCB_OK) return rc;
     fill_times(h, stats, false);
     if (stats) stats->total_ms = elapsed(h->ev[1], h->ev[4]);
@@ -781,7 +960,7 @@ int dcb_extract_device(dcb_handle h, const dcb_grid* grid, const dcb_opts* opts,
         out->verts_per_face = h->vpf;
         out->vertices = as<float>(h->V);
         out->faces = face_ptr(h);
-        out->cell_coords = as<uint64_t>(h->list);
+        out->cell_coords = h->cells_per_vertex ? as<uint64_t>(h->sp_vcell) : as<uint64_t>(h->list);
     }
     return DCB_OK;
 }
@@ -829,8 +1008,7 @@ int dcb_extract_host(dcb_handle h, const dcb_grid* grid, const dcb_opts* opts, d
     dcb_opts def;
     dcb_default_opts(&def);
     const dcb_opts* o = opts ? opts : &def;
-    if (o->method != DCB_METHOD_DUAL_CONTOURING && o->method != DCB_METHOD_OURS)
-        return fail(h, DCB_ERR_NOT_SUPPORTED, "unknown method");
+    if (!known_method(o->method)) return fail(h, DCB_ERR_NOT_SUPPORTED, "unknown method");
     if (!(o->svd_threshold >= 0.0)) return fail(h, DCB_ERR_INVALID_ARGUMENT, "svd_threshold must be >= 0");
     cudaStream_t s = reinterpret_cast<cudaStream_t>(cuda_stream);
     if (stats) std::memset(stats, 0, sizeof(*stats));
@@ -841,7 +1019,7 @@ int dcb_extract_host(dcb_handle h, const dcb_grid* grid, const dcb_opts* opts, d
     DCB_TRY(h, cudaEventRecord(h->ev[1], s), "event");
     dcb_grid dg = *grid;
     dg.values = as<float>(h->grid);
-    rc = o->method == DCB_METHOD_OURS ? run_ours(h, &dg, o, s, stats) : run_pipeline(h, &dg, o, s, stats);
+    rc = run_method(h, &dg, o, s, stats);
     if (rc != DCB_OK) return rc;
     DCB_TRY(h, ensure_host(h->hV, h->hV_bytes, sizeof(float) * 3 * h->nv), "alloc host vertices");
     DCB_TRY(h, ensure_host(h->hF, h->hF_bytes, sizeof(int32_t) * h->vpf * h->nf), "alloc host faces");
@@ -889,7 +1067,8 @@ int dcb_copy_cells_to_host(dcb_handle h, int64_t* cell_linear_index, void* cuda_
     cudaStream_t s = reinterpret_cast<cudaStream_t>(cuda_stream);
     if (cudaSetDevice(h->device) != cudaSuccess) { cudaGetLastError(); return fail(h, DCB_ERR_CUDA, "set device"); }
     uint64_t* packed = reinterpret_cast<uint64_t*>(cell_linear_index);
-    DCB_TRY(h, cudaMemcpyAsync(packed, h->list.p, sizeof(uint64_t) * h->nv, cudaMemcpyDeviceToHost, s), "copy cells");
+    DCB_TRY(h, cudaMemcpyAsync(packed, h->cells_per_vertex ? h->sp_vcell.p : h->list.p, sizeof(uint64_t) * h->nv,
+                               cudaMemcpyDeviceToHost, s), "copy cells");
     DCB_TRY(h, cudaStreamSynchronize(s), "copy cells");
     int b = 0;
     for (int64_t r = 0; r < h->nv; ++r) {
@@ -963,7 +1142,7 @@ int dcb_backward(dcb_handle h, const dcb_grid* grid, const dcb_opts* opts, const
     const dcb_opts* o = opts ? opts : &def;
     if (o->method != DCB_METHOD_DUAL_CONTOURING) return fail(h, DCB_ERR_NOT_SUPPORTED, "the adjoint covers dual contouring only");
     if (!(o->svd_threshold >= 0.0)) return fail(h, DCB_ERR_INVALID_ARGUMENT, "svd_threshold must be >= 0");
-    if (h->batch_n != 1 || h->cx != grid->nx - 1 || h->cy != grid->ny - 1 || h->cz != grid->nz - 1)
+    if (h->last_kind != 0 || h->batch_n != 1 || h->cx != grid->nx - 1 || h->cy != grid->ny - 1 || h->cz != grid->nz - 1)
         return fail(h, DCB_ERR_INVALID_ARGUMENT, "backward needs the grid of the last single-grid extraction");
     if (!dL_dgrid || (h->nv > 0 && !dL_dvertices)) return fail(h, DCB_ERR_INVALID_ARGUMENT, "null gradient array");
     if (cudaSetDevice(h->device) != cudaSuccess) { cudaGetLastError(); return fail(h, DCB_ERR_CUDA, "set device"); }

@@ -343,4 +343,52 @@ cudaError_t launch_sdf_masks(const SdfParams& P, int num_sms, cudaStream_t s);
 cudaError_t launch_sdf_flood(const SdfParams& P, int* changed, int num_sms, cudaStream_t s);
 cudaError_t launch_sdf_finish(const SdfParams& P, unsigned long long* filled, float* tmp, int num_sms, cudaStream_t s);
 
+// ---- sparse (brick) backends ------------------------------------------------------------
+
+// SparseParams::counters slots: the reference's DualContouringStats counters of the sparse
+// backends, then the scan totals.
+enum SparseCounter {
+    kScTotalBricks = 0, kScActiveBricks, kScActiveCells, kScFallback, kScClamp, kScInvalid, kScAmbiguous,
+    kScMulti, kScOne, kScTwo, kScSplitReject, kScSkipped,
+    kScCount,                      // counters kept per block in the kernels
+    kScVertices = kScCount,        // total vertices (multi-vertex scan)
+    kScFaces,                      // total faces (face scan)
+    kScSlots = 16
+};
+
+struct SparseParams {
+    GridDesc g;                    // W, W8: the dense path's bitmap layout
+    int bs;                        // brick size (cells)
+    int nbx, nby, nbz;             // bricks per axis
+    int Wp;                        // point words per point row (32 points a word)
+    int nxt;                       // cell-word segments of 32 words per cell row
+    int mvdc;                      // up to two vertices per cell
+    int normal_mode;               // 0 trilinear, 1 edge gradient (2 behaves as 0)
+    float close;                   // 0.45f * vx: near-zero cells and thin edges
+    uint32_t* pn;                  // [ny*nz][Wp] point words: value < 0
+    uint32_t* pp;                  //   value > 0
+    uint32_t* pc;                  //   |value| <= close
+    uint8_t* brick;                // [nbx*nby*nbz] active flags
+    uint32_t* bits;                // [cy*cz][W] active cells
+    uint32_t* super;               // [cy*cz][W8] ranks (after the rank expansion)
+    uint32_t* seg_count;           // [cy*cz][nxt]
+    const uint64_t* list;          // [nactive] packed active cells, ascending
+    long long nactive;
+    uint32_t* vcount;              // multi-vertex: [nactive] vertices of the cell (1 or 2)
+    const uint32_t* vstart;        // multi-vertex: [nactive] first vertex (scan of vcount)
+    float* vtmp;                   // multi-vertex: [nactive][2][3] vertices before placing
+    float* ntmp;                   // multi-vertex: [nactive][2][3] vertex normals
+    float* V;                      // [vertices][3]
+    float* N;                      // multi-vertex: [vertices][3]
+    uint64_t* vcell;               // multi-vertex: [vertices] packed cell of each vertex
+    uint32_t* fcount;              // [nactive] faces of the cell
+    const uint32_t* fstart;        // [nactive] first face (scan of fcount)
+    int4* faces;
+    unsigned long long* counters;  // [kScSlots], indexed by SparseCounter
+};
+cudaError_t launch_sparse_mark(const SparseParams& P, int num_sms, cudaStream_t s);
+cudaError_t launch_sparse_vertices(const SparseParams& P, int num_sms, cudaStream_t s);
+cudaError_t launch_sparse_place(const SparseParams& P, int num_sms, cudaStream_t s);
+cudaError_t launch_sparse_faces(const SparseParams& P, bool emit, int num_sms, cudaStream_t s);
+
 }  // namespace dcb
