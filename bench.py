@@ -466,6 +466,94 @@ def run_refcuda_workload(args):
     return 0
 
 
+class _StdoutToStderr:
+    """Sends file descriptor 1 to stderr for the duration (the reference's sparse backend
+    prints a memory estimate on every call; the bench's stdout carries JSON lines only)."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        os.dup2(2, 1)
+
+    def __exit__(self, *a):
+        sys.stdout.flush()
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+
+
+def run_sparse_workload(args):
+    """The sparse backends (the reference's CudaSparseDualContouringBackend and its
+    multi-vertex variant, dc_cli's default GPU backends) on the device-resident CSG grid
+    (1024^3 unless --res): this engine's device time (CUDA events) and device grid -> host
+    mesh wall clock, against the reference's own sparse CUDA code as shipped (built from its
+    source into oracle/_ref/) on the same GPU, same grid, same brick size (8): wall clock from
+    the device grid to the host mesh, and its own stage timers. One line per variant."""
+    import numpy as np
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O          # only its ref_sparse: the reference's own CUDA code, the comparator
+    from contouring_b200 import B200SparseDualContouringBackend, DenseSdfGridDevice
+    torch.cuda.set_device(0)
+    res = args.res
+    vals, dims, sp, org = make_grid(res, torch.device("cuda", 0))
+    torch.cuda.synchronize()
+    ncell = (dims[0] - 1) * (dims[1] - 1) * (dims[2] - 1)
+    g = DenseSdfGridDevice(*dims, *sp, *org, d_values=vals)
+
+    def wall(fn, steps, warmup):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(steps):
+            t0 = time.perf_counter()
+            fn()
+            torch.cuda.synchronize()
+            ts.append((time.perf_counter() - t0) * 1e3)
+        return statistics.median(ts)
+
+    for mvdc in (False, True):
+        be = B200SparseDualContouringBackend(multi_vertex_cells=mvdc)
+        ms_dev = _timed(lambda: be.extract_tensor_ptr(g), args.steps, args.warmup)
+        ms_host = wall(lambda: be.extract_device(g), args.steps, args.warmup)
+        mesh, st = be.extract_device(g)
+        ref = {}
+        ref_res = []
+
+        def ref_call():
+            with _StdoutToStderr():
+                r = O.ref_sparse(vals.data_ptr(), dims, sp, org, mvdc=mvdc, exact=False)
+            if r is None:
+                raise RuntimeError("reference sparse backend unavailable")
+            ref_res.append(r)
+        try:
+            ms_ref = wall(ref_call, max(1, min(args.steps, 5)), min(args.warmup, 2))
+            r = ref_res[-1]
+            ours_f = mesh.faces.reshape(-1, 4)
+            same_shape = len(r["V"]) * 3 == len(mesh.vertices) and r["F"].shape == ours_f.shape
+            differing = int(np.any(r["F"] != ours_f, axis=1).sum()) if same_shape else None
+            ref = {"ms_per_step": round(ms_ref, 3), "mcells_per_s": round(ncell / (ms_ref / 1e3) / 1e6, 1),
+                   "own_total_ms": round(r["times"][0], 3),
+                   "own_stage_kernels_ms": round(sum(r["times"][1:]), 3),
+                   "vertices": int(len(r["V"])), "quads": int(len(r["F"])),
+                   "quads_differing_from_ours": differing}
+            extra = {"speedup_vs_reference_cuda": round(ms_ref / ms_host, 2),
+                     "device_speedup_vs_reference_cuda_stages": round(sum(r["times"][1:]) / ms_dev, 2)}
+        except (RuntimeError, OSError) as e:
+            ref = {"unavailable": str(e)}
+            extra = {}
+        name = "sparse_mvdc" if mvdc else "sparse"
+        _side_line("dc_%s_mcells_per_s" % name, ncell / (ms_dev / 1e3) / 1e6, "Mcells/s", ms_dev, args,
+                   {"workload": "csg%d_%s_brick8" % (res, name), "grid": list(dims)},
+                   device_grid_to_host_mesh_ms=round(ms_host, 3), vertices=st.vertex_count, quads=st.face_count,
+                   active_cells=st.active_cells, active_bricks=st.active_bricks, two_vertex_cells=st.two_vertex_cells,
+                   stage_ms={"mark": round(st.marking_ms, 4), "scan": round(st.compaction_ms, 4),
+                             "vertices": round(st.qef_ms, 4), "faces": round(st.face_emission_ms, 4)},
+                   reference_cuda=ref, **extra)
+        be.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -477,10 +565,11 @@ def main():
     ap.add_argument("--ref-zslab", type=int, default=96, help="point planes per CPU sample (over 8 slabs)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-sequential", action="store_true", help="batch256: skip the one-by-one comparison")
-    ap.add_argument("--workload", default="csg1024", choices=["csg1024", "batch256", "adjoint128", "ours128", "mesh512", "refcuda512"],
+    ap.add_argument("--workload", default="csg1024", choices=["csg1024", "batch256", "adjoint128", "ours128", "mesh512", "refcuda512", "sparse1024"],
                     help="side workloads (not the headline): batch256 = 256 uneven CSG grids batched vs one "
                          "by one; adjoint128 = forward + adjoint; ours128 = the full refinement; mesh512 = "
-                         "mesh_to_sdf; refcuda512 = the reference's CUDA backend vs this engine at 512^3")
+                         "mesh_to_sdf; refcuda512 = the reference's CUDA backend vs this engine at 512^3; "
+                         "sparse1024 = the sparse and multi-vertex backends vs the reference's at --res")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -500,6 +589,8 @@ def main():
         return run_mesh_workload(args)
     if args.workload == "refcuda512":
         return run_refcuda_workload(args)
+    if args.workload == "sparse1024":
+        return run_sparse_workload(args)
 
     import numpy as np
     import torch

@@ -60,7 +60,7 @@ struct dcb_context {
         v64_index, v64_cells, V64, tris, tri_items, adj_rows, adj_owners, ours_ws;
     // sparse backends
     DevBuf sp_words, sp_brick, sp_vcount, sp_vstart, sp_vtmp, sp_ntmp, sp_N, sp_vcell, sp_fcount, sp_fstart,
-        sp_counters;
+        sp_stage, sp_counters;
     void* h_sp_counters = nullptr;    // pinned copy of the sparse counters
     int last_kind = 0;                // last extraction: 0 dense dual contouring, 1 sparse
     int cells_per_vertex = 0;         // 1: the vertex -> cell list is `sp_vcell` (two vertices per cell)
@@ -569,8 +569,8 @@ int run_ours(dcb_context* h, const dcb_grid* in, const dcb_opts* o, cudaStream_t
 
 // The sparse (brick) backends (src/cuda/dc_cuda_sparse.cu:1171-1415) on one device grid:
 // point words -> bricks -> active-cell bits, scan + rank expansion, vertices (and, for the
-// multi-vertex variant, their scan and placement), face counts, scan, faces. Two host
-// read-backs: the active-cell count and the vertex and face totals.
+// multi-vertex variant, their scan and placement), faces into per-cell slots, scan,
+// compaction. Two host read-backs: the active-cell count and the vertex and face totals.
 int run_sparse(dcb_context* h, const dcb_grid* in, const dcb_opts* o, cudaStream_t s, dcb_stats* st) {
     if (o->emit_triangles) return fail(h, DCB_ERR_NOT_SUPPORTED, "the sparse backends emit quads only");
     if (o->brick_size < 1 || o->brick_size > 4096) return fail(h, DCB_ERR_INVALID_ARGUMENT, "brick_size must be in [1, 4096]");
@@ -652,6 +652,7 @@ int run_sparse(dcb_context* h, const dcb_grid* in, const dcb_opts* o, cudaStream
         DCB_TRY(h, ensure(h->V, sizeof(float) * 3 * (mvdc ? 2 * na : na)), "alloc vertices");
         DCB_TRY(h, ensure(h->sp_fcount, sizeof(uint32_t) * na), "alloc face counts");
         DCB_TRY(h, ensure(h->sp_fstart, sizeof(uint32_t) * na), "alloc face starts");
+        DCB_TRY(h, ensure(h->sp_stage, sizeof(int4) * 6 * na), "alloc face staging");
         plen = std::max(plen, scan_partials_len(na));
         DCB_TRY(h, ensure(h->partials, sizeof(uint32_t) * plen), "alloc scan");
         ExpandParams xp{};
@@ -680,10 +681,11 @@ int run_sparse(dcb_context* h, const dcb_grid* in, const dcb_opts* o, cudaStream
             DCB_TRY(h, launch_sparse_place(P, h->num_sms, s), "launch vertex placement");
         }
         DCB_TRY(h, cudaEventRecord(h->ev[3], s), "event");
-        // 3) faces: counts, scan, emission
+        // 3) faces: per-cell staging with counts, scan, compaction
         P.fcount = as<uint32_t>(h->sp_fcount);
         P.fstart = as<uint32_t>(h->sp_fstart);
-        DCB_TRY(h, launch_sparse_faces(P, false, h->num_sms, s), "launch face count");
+        P.stage = as<int4>(h->sp_stage);
+        DCB_TRY(h, launch_sparse_faces(P, h->num_sms, s), "launch faces");
         DCB_TRY(h, launch_scan(P.fcount, na, as<uint32_t>(h->partials), as<uint32_t>(h->sp_fstart),
                                dcn + kScFaces, s), "launch face scan");
         DCB_TRY(h, cudaMemcpyAsync(hcn, dcn, sizeof(unsigned long long) * kScSlots, cudaMemcpyDeviceToHost, s), "read totals");
@@ -693,7 +695,7 @@ int run_sparse(dcb_context* h, const dcb_grid* in, const dcb_opts* o, cudaStream
         if (nf >= 0x7fffffffLL) return fail(h, DCB_ERR_TOO_LARGE, "more than 2^31-1 faces");
         DCB_TRY(h, ensure(h->faces, sizeof(int4) * std::max(1LL, nf)), "alloc faces");
         P.faces = as<int4>(h->faces);
-        DCB_TRY(h, launch_sparse_faces(P, true, h->num_sms, s), "launch face emission");
+        DCB_TRY(h, launch_sparse_compact(P, h->num_sms, s), "launch face compaction");
     } else {
         DCB_TRY(h, cudaEventRecord(h->ev[3], s), "event");
     }
@@ -922,7 +924,7 @@ int dcb_destroy(dcb_handle h) {
                       &h->m_bin_active, &h->m_active_list, &h->m_axis_start, &h->m_far, &h->m_ext, &h->m_tmp,
                       &h->m_partials, &h->m_counters, &h->table, &h->cell_slot, &h->adj_rows, &h->adj_owners, &h->ours_ws,
                       &h->sp_words, &h->sp_brick, &h->sp_vcount, &h->sp_vstart, &h->sp_vtmp, &h->sp_ntmp,
-                      &h->sp_N, &h->sp_vcell, &h->sp_fcount, &h->sp_fstart, &h->sp_counters};
+                      &h->sp_N, &h->sp_vcell, &h->sp_fcount, &h->sp_fstart, &h->sp_stage, &h->sp_counters};
     for (DevBuf* b : bufs) if (b->p) cudaFree(b->p);
     if (h->h_counters) cudaFreeHost(h->h_counters);
     if (h->h_sdf_counters) cudaFreeHost(h->h_sdf_counters);

@@ -383,12 +383,14 @@ struct SparseParams {
     uint64_t* vcell;               // multi-vertex: [vertices] packed cell of each vertex
     uint32_t* fcount;              // [nactive] faces of the cell
     const uint32_t* fstart;        // [nactive] first face (scan of fcount)
+    int4* stage;                   // [nactive][6] faces of each cell before the scan
     int4* faces;
     unsigned long long* counters;  // [kScSlots], indexed by SparseCounter
 };
 cudaError_t launch_sparse_mark(const SparseParams& P, int num_sms, cudaStream_t s);
 cudaError_t launch_sparse_vertices(const SparseParams& P, int num_sms, cudaStream_t s);
 cudaError_t launch_sparse_place(const SparseParams& P, int num_sms, cudaStream_t s);
-cudaError_t launch_sparse_faces(const SparseParams& P, bool emit, int num_sms, cudaStream_t s);
+cudaError_t launch_sparse_faces(const SparseParams& P, int num_sms, cudaStream_t s);
+cudaError_t launch_sparse_compact(const SparseParams& P, int num_sms, cudaStream_t s);
 
 }  // namespace dcb

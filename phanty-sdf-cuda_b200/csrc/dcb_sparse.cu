@@ -201,7 +201,11 @@ __device__ int face_vertex(const SparseParams& P, int i, int j, int k, float3 gn
 // ---- marking ----------------------------------------------------------------------------
 
 // Negative / positive / near-zero bit words of every point row (32 points a word), a warp
-// per 32 consecutive words of a row: one coalesced 128-byte load and three ballots per word.
+// per 32 consecutive words of a row. VEC4 (rows 16-byte aligned, nx % 4 == 0): lane l loads
+// points 4l..4l+3 of each 128-point chunk as one float4, builds the three nibbles and an
+// 8-lane shuffle-OR forms each word; otherwise one coalesced scalar load and three ballots
+// per word.
+template <bool VEC4>
 __global__ void __launch_bounds__(256) k_sparse_points(const __grid_constant__ SparseParams P) {
     const GridDesc& g = P.g;
     const int lane = threadIdx.x & 31;
@@ -213,15 +217,51 @@ __global__ void __launch_bounds__(256) k_sparse_points(const __grid_constant__ S
         const int w0 = (int)(c - row * cpr) * 32;
         const float* src = g.v + row * g.nx;
         uint32_t mn = 0, mp = 0, mc = 0;
+        if (VEC4) {
+            float4 v[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const int x = w0 * 32 + 128 * q + 4 * lane;
+                v[q] = x < g.nx ? __ldg(reinterpret_cast<const float4*>(src + x)) : make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const bool in = w0 * 32 + 128 * q + 4 * lane < g.nx;
+                const float e[4] = {v[q].x, v[q].y, v[q].z, v[q].w};
+                uint32_t n = 0, p = 0, z = 0;
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    n |= (e[u] < 0.f ? 1u : 0u) << u;
+                    p |= (e[u] > 0.f ? 1u : 0u) << u;
+                    z |= (fabsf(e[u]) <= P.close ? 1u : 0u) << u;
+                }
+                if (!in) n = p = z = 0;
+                const int sh = 4 * (lane & 7);
+                n <<= sh; p <<= sh; z <<= sh;
+#pragma unroll
+                for (int o = 1; o < 8; o <<= 1) {
+                    n |= __shfl_xor_sync(0xffffffffu, n, o);
+                    p |= __shfl_xor_sync(0xffffffffu, p, o);
+                    z |= __shfl_xor_sync(0xffffffffu, z, o);
+                }
+                // word 4q + (l >> 3) is complete in lanes 8*(l >> 3)..; lane L keeps word L
+                const int src_lane = 8 * (lane & 3);
+                const uint32_t tn = __shfl_sync(0xffffffffu, n, src_lane);
+                const uint32_t tp = __shfl_sync(0xffffffffu, p, src_lane);
+                const uint32_t tz = __shfl_sync(0xffffffffu, z, src_lane);
+                if ((lane >> 2) == q) { mn = tn; mp = tp; mc = tz; }
+            }
+        } else {
 #pragma unroll 8
-        for (int u = 0; u < 32; ++u) {
-            const int x = (w0 + u) * 32 + lane;
-            const bool in = x < g.nx;
-            const float v = in ? __ldg(src + x) : 0.f;
-            const uint32_t bn = __ballot_sync(0xffffffffu, in && v < 0.f);
-            const uint32_t bp = __ballot_sync(0xffffffffu, in && v > 0.f);
-            const uint32_t bc = __ballot_sync(0xffffffffu, in && fabsf(v) <= P.close);
-            if (lane == u) { mn = bn; mp = bp; mc = bc; }
+            for (int u = 0; u < 32; ++u) {
+                const int x = (w0 + u) * 32 + lane;
+                const bool in = x < g.nx;
+                const float v = in ? __ldg(src + x) : 0.f;
+                const uint32_t bn = __ballot_sync(0xffffffffu, in && v < 0.f);
+                const uint32_t bp = __ballot_sync(0xffffffffu, in && v > 0.f);
+                const uint32_t bc = __ballot_sync(0xffffffffu, in && fabsf(v) <= P.close);
+                if (lane == u) { mn = bn; mp = bp; mc = bc; }
+            }
         }
         if (w0 + lane < P.Wp) {
             const long long o = row * P.Wp + w0 + lane;
@@ -230,31 +270,47 @@ __global__ void __launch_bounds__(256) k_sparse_points(const __grid_constant__ S
     }
 }
 
-// Brick flags from the point words (:271-308).
-__global__ void __launch_bounds__(256) k_sparse_bricks(const __grid_constant__ SparseParams P) {
+// Brick flags from the point words (:271-308): a block per row of bricks (by, bz). Its threads
+// OR the point words of the brick row's (s+1)^2 point rows, word by word (coalesced), into
+// shared memory; then a thread per brick tests its x-range of points in those words.
+constexpr int kBrickThreads = 128;
+constexpr int kMaxPointWords = 2048;           // nx <= 65536
+
+__global__ void __launch_bounds__(kBrickThreads) k_sparse_bricks(const __grid_constant__ SparseParams P) {
     const GridDesc& g = P.g;
+    __shared__ uint32_t s_n[kMaxPointWords], s_p[kMaxPointWords];
     __shared__ unsigned int s_active;
     if (threadIdx.x == 0) s_active = 0;
-    __syncthreads();
-    const long long nb = (long long)P.nbx * P.nby * P.nbz;
-    for (long long b = (long long)blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += (long long)gridDim.x * blockDim.x) {
-        const int bx = (int)(b % P.nbx), by = (int)((b / P.nbx) % P.nby), bz = (int)(b / ((long long)P.nbx * P.nby));
-        const int i0 = bx * P.bs, j0 = by * P.bs, k0 = bz * P.bs;
-        const int i1 = min(i0 + P.bs + 1, g.nx), j1 = min(j0 + P.bs + 1, g.ny), k1 = min(k0 + P.bs + 1, g.nz);
-        const int w0 = i0 >> 5, w1 = (i1 - 1) >> 5;
-        bool neg = false, pos = false;
-        for (int k = k0; k < k1 && !(neg && pos); ++k)
-            for (int j = j0; j < j1 && !(neg && pos); ++j) {
-                const long long row = ((long long)j + (long long)g.ny * k) * P.Wp;
-                for (int w = w0; w <= w1; ++w) {
-                    const uint32_t m = range_bits(max(i0 - 32 * w, 0), min(i1 - 32 * w, 32));
-                    neg |= (__ldg(P.pn + row + w) & m) != 0u;
-                    pos |= (__ldg(P.pp + row + w) & m) != 0u;
+    const long long nrow = (long long)P.nby * P.nbz;
+    for (long long br = blockIdx.x; br < nrow; br += gridDim.x) {
+        const int by = (int)(br % P.nby), bz = (int)(br / P.nby);
+        const int j0 = by * P.bs, k0 = bz * P.bs;
+        const int j1 = min(j0 + P.bs + 1, g.ny), k1 = min(k0 + P.bs + 1, g.nz);
+        __syncthreads();
+        for (int w = threadIdx.x; w < P.Wp; w += blockDim.x) {
+            uint32_t n = 0, p = 0;
+            for (int k = k0; k < k1; ++k)
+                for (int j = j0; j < j1; ++j) {
+                    const long long o = ((long long)j + (long long)g.ny * k) * P.Wp + w;
+                    n |= __ldg(P.pn + o);
+                    p |= __ldg(P.pp + o);
                 }
+            s_n[w] = n;
+            s_p[w] = p;
+        }
+        __syncthreads();
+        for (int bx = threadIdx.x; bx < P.nbx; bx += blockDim.x) {
+            const int i0 = bx * P.bs, i1 = min(i0 + P.bs + 1, g.nx);
+            bool neg = false, pos = false;
+            for (int w = i0 >> 5; w <= (i1 - 1) >> 5; ++w) {
+                const uint32_t m = range_bits(max(i0 - 32 * w, 0), min(i1 - 32 * w, 32));
+                neg |= (s_n[w] & m) != 0u;
+                pos |= (s_p[w] & m) != 0u;
             }
-        const bool act = neg && pos;
-        P.brick[b] = act ? 1 : 0;
-        if (act) atomicAdd(&s_active, 1u);
+            const bool act = neg && pos;
+            P.brick[bx + (long long)P.nbx * br] = act ? 1 : 0;
+            if (act) atomicAdd(&s_active, 1u);
+        }
     }
     __syncthreads();
     if (threadIdx.x == 0 && s_active) atomicAdd(P.counters + kScActiveBricks, (unsigned long long)s_active);
@@ -447,32 +503,40 @@ __global__ void __launch_bounds__(256) k_sparse_place(const __grid_constant__ Sp
 
 // ---- faces ----------------------------------------------------------------------------------
 
-// A thread per active cell: its faces counted (EMIT = false) or written at the cell's scanned
-// offset (EMIT = true), in the reference's order (:853-1102).
-template <bool EMIT>
+// A thread per active cell: its faces in the reference's order (:853-1102) into the cell's six
+// staging slots (three axes, a thin edge's reversed quad beside its own) and their count;
+// k_sparse_compact moves them to their scanned positions. A cell without faces adds nothing
+// to the skipped-face counter (the reference's emit pass returns for it, :954).
 __global__ void __launch_bounds__(128) k_sparse_faces(const __grid_constant__ SparseParams P) {
     __shared__ unsigned int s_skipped;
-    if (EMIT && threadIdx.x == 0) s_skipped = 0;
-    if (EMIT) __syncthreads();
+    if (threadIdx.x == 0) s_skipped = 0;
+    __syncthreads();
     const GridDesc& g = P.g;
     for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < P.nactive;
          r += (long long)gridDim.x * blockDim.x) {
         int i, j, k;
         unpack_cell(P.list[r], i, j, k);
-        uint32_t count = 0;
-        uint32_t out = EMIT ? P.fstart[r] : 0u;
-        if (EMIT && P.fcount[r] == 0u) continue;
+        uint32_t count = 0, skipped = 0;
+        int4* const out = P.stage + 6 * r;
+        const float s0 = sval(g, i, j, k);
+        float3 g0 = f3(0.f, 0.f, 0.f);
+        bool have_g0 = false;
 #pragma unroll 1
         for (int axis = 0; axis < 3; ++axis) {
             if (axis == 0 && !(j >= 1 && k >= 1)) continue;
             if (axis == 1 && !(i >= 1 && k >= 1 && j < g.ny - 1)) continue;
             if (axis == 2 && !(i >= 1 && j >= 1 && k < g.nz - 1)) continue;
             const int i1 = i + (axis == 0), j1 = j + (axis == 1), k1 = k + (axis == 2);
-            const float s0 = sval(g, i, j, k), s1 = sval(g, i1, j1, k1);
+            const float s1 = sval(g, i1, j1, k1);
             const bool crossing = s0 * s1 < 0.0f;
-            const bool thin = !crossing && thin_edge(P, s0, s1, i, j, k, i1, j1, k1);
+            bool thin = false;
+            if (!crossing && !(s0 * s1 <= 0.0f) && !(fabsf(s0) > P.close || fabsf(s1) > P.close)) {
+                if (!have_g0) { g0 = sgrad(g, i, j, k); have_g0 = true; }
+                thin = dot3(g0, sgrad(g, i1, j1, k1)) < -0.3f;
+            }
             if (!crossing && !thin) continue;
-            const float3 gn = add3(sgrad(g, i, j, k), sgrad(g, i1, j1, k1));
+            if (!have_g0) { g0 = sgrad(g, i, j, k); have_g0 = true; }
+            const float3 gn = add3(g0, sgrad(g, i1, j1, k1));
             int v0, v1, v2, v3;
             if (axis == 0) {
                 v0 = face_vertex(P, i, j - 1, k - 1, gn); v1 = face_vertex(P, i, j, k - 1, gn);
@@ -485,10 +549,9 @@ __global__ void __launch_bounds__(128) k_sparse_faces(const __grid_constant__ Sp
                 v2 = face_vertex(P, i, j, k, gn); v3 = face_vertex(P, i - 1, j, k, gn);
             }
             if (v0 < 0 || v1 < 0 || v2 < 0 || v3 < 0) {
-                if (EMIT && P.mvdc) atomicAdd(&s_skipped, 1u);
+                if (P.mvdc) ++skipped;
                 continue;
             }
-            if (!EMIT) { count += thin ? 2u : 1u; continue; }
             auto vtx = [&](int v) {
                 return f3(__ldg(P.V + 3 * (size_t)v), __ldg(P.V + 3 * (size_t)v + 1), __ldg(P.V + 3 * (size_t)v + 2));
             };
@@ -496,14 +559,22 @@ __global__ void __launch_bounds__(128) k_sparse_faces(const __grid_constant__ Sp
             float3 qn = cross3(sub3(pb, pa), sub3(pd, pa));
             if (dot3(qn, qn) < 1e-12f) qn = cross3(sub3(pc, pa), sub3(pd, pa));
             if (dot3(gn, gn) > 0.0f && dot3(qn, qn) > 0.0f && dot3(qn, gn) < 0.0f) { const int t = v1; v1 = v3; v3 = t; }
-            P.faces[out++] = make_int4(v0, v1, v2, v3);
-            if (thin) P.faces[out++] = make_int4(v0, v3, v2, v1);
+            out[count++] = make_int4(v0, v1, v2, v3);
+            if (thin) out[count++] = make_int4(v0, v3, v2, v1);
         }
-        if (!EMIT) P.fcount[r] = count;
+        P.fcount[r] = count;
+        if (count && skipped) atomicAdd(&s_skipped, skipped);
     }
-    if (EMIT) {
-        __syncthreads();
-        if (threadIdx.x == 0 && s_skipped) atomicAdd(P.counters + kScSkipped, (unsigned long long)s_skipped);
+    __syncthreads();
+    if (threadIdx.x == 0 && s_skipped) atomicAdd(P.counters + kScSkipped, (unsigned long long)s_skipped);
+}
+
+// Each cell's staged faces to their scanned positions.
+__global__ void __launch_bounds__(256) k_sparse_compact(const __grid_constant__ SparseParams P) {
+    for (long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x; r < P.nactive;
+         r += (long long)gridDim.x * blockDim.x) {
+        const uint32_t c = P.fcount[r], st = P.fstart[r];
+        for (uint32_t q = 0; q < c; ++q) P.faces[st + q] = P.stage[6 * r + q];
     }
 }
 
@@ -520,9 +591,11 @@ unsigned blocks_for(long long items, int threads, int num_sms, int per_sm) {
 
 cudaError_t launch_sparse_mark(const SparseParams& P, int num_sms, cudaStream_t s) {
     const long long chunks = (long long)P.g.ny * P.g.nz * ((P.Wp + 31) / 32);
-    k_sparse_points<<<blocks_for(chunks * 32, 256, num_sms, 16), 256, 0, s>>>(P);
-    const long long nb = (long long)P.nbx * P.nby * P.nbz;
-    k_sparse_bricks<<<blocks_for(nb, 256, num_sms, 8), 256, 0, s>>>(P);
+    const bool vec4 = P.g.nx % 4 == 0 && (reinterpret_cast<uintptr_t>(P.g.v) % 16) == 0;
+    if (vec4) k_sparse_points<true><<<blocks_for(chunks * 32, 256, num_sms, 16), 256, 0, s>>>(P);
+    else      k_sparse_points<false><<<blocks_for(chunks * 32, 256, num_sms, 16), 256, 0, s>>>(P);
+    const long long nrow = (long long)P.nby * P.nbz;
+    k_sparse_bricks<<<(unsigned)std::min<long long>(nrow, (long long)num_sms * 16), kBrickThreads, 0, s>>>(P);
     const long long nseg = (long long)P.g.cy * P.g.cz * P.nxt;
     k_sparse_cells<<<blocks_for(nseg * 32, 256, num_sms, 16), 256, 0, s>>>(P);
     return cudaGetLastError();
@@ -540,10 +613,15 @@ cudaError_t launch_sparse_place(const SparseParams& P, int num_sms, cudaStream_t
     return cudaGetLastError();
 }
 
-cudaError_t launch_sparse_faces(const SparseParams& P, bool emit, int num_sms, cudaStream_t s) {
+cudaError_t launch_sparse_faces(const SparseParams& P, int num_sms, cudaStream_t s) {
     if (P.nactive <= 0) return cudaSuccess;
-    if (emit) k_sparse_faces<true><<<blocks_for(P.nactive, 128, num_sms, 16), 128, 0, s>>>(P);
-    else      k_sparse_faces<false><<<blocks_for(P.nactive, 128, num_sms, 16), 128, 0, s>>>(P);
+    k_sparse_faces<<<blocks_for(P.nactive, 128, num_sms, 16), 128, 0, s>>>(P);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sparse_compact(const SparseParams& P, int num_sms, cudaStream_t s) {
+    if (P.nactive <= 0) return cudaSuccess;
+    k_sparse_compact<<<blocks_for(P.nactive, 256, num_sms, 8), 256, 0, s>>>(P);
     return cudaGetLastError();
 }
 
