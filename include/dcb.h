@@ -200,6 +200,23 @@ int dcb_copy_cells_to_host(dcb_handle h, int64_t* cell_linear_index, void* cuda_
 int dcb_mark_active_cells_noalloc(const dcb_grid* grid, int64_t* cells, int64_t capacity,
                                   int64_t* count, void* cuda_stream);
 
+/* ---- files either side of the extraction (src/cpp/dc_cli.cpp:17-47) -------------------- */
+
+/* Replaces dc_cli's write_obj (dc_cli.cpp:17-29): "v x y z" lines (6 significant digits, the
+ * C++ stream default) then "f ..." lines with 1-based indices, verts_per_face 4 (quads) or 3.
+ * Host arrays. threads <= 0: all hardware threads format slices in parallel. */
+int dcb_write_obj(const char* path, const float* vertices, int64_t num_vertices, const int32_t* faces,
+                  int64_t num_faces, int verts_per_face, int threads);
+
+/* Replaces dc_cli's read_sdf (dc_cli.cpp:31-47): int32 nx, ny, nz, float32 vx, vy, vz, ox, oy,
+ * oz, then nx*ny*nz float32 values. With values == NULL only the header is read (to size the
+ * caller's buffer, e.g. pinned host memory for an upload); otherwise `capacity` floats are
+ * available and header->values is set to `values`. */
+int dcb_read_sdf(const char* path, dcb_grid* header, float* values, int64_t capacity);
+
+/* The inverse of dcb_read_sdf (host values). */
+int dcb_write_sdf(const char* path, const dcb_grid* grid);
+
 /* ---- batches of grids ------------------------------------------------------------------- */
 
 /* The meshes of a batch, concatenated grid by grid in device memory. Grid b's vertices are

@@ -30,7 +30,7 @@ EXPORTED = (
     "dcb_copy_mesh_to_host", "dcb_copy_mesh_device", "dcb_copy_cells_to_host",
     "dcb_mark_active_cells_noalloc", "dcb_mesh_to_sdf_device", "dcb_mesh_to_sdf_host",
     "dcb_extract_batch_device", "dcb_backward", "dcb_autotune_mark",
-)
+    "dcb_write_obj", "dcb_read_sdf", "dcb_write_sdf")
 
 
 class DcbGrid(ctypes.Structure):
@@ -123,6 +123,13 @@ def lib():
     L.dcb_status_string.restype = ctypes.c_char_p
     L.dcb_last_error.argtypes = [ctypes.c_void_p]
     L.dcb_last_error.restype = ctypes.c_char_p
+    L.dcb_write_obj.argtypes = [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64,
+                                ctypes.c_int, ctypes.c_int]
+    L.dcb_write_obj.restype = ctypes.c_int
+    L.dcb_read_sdf.argtypes = [ctypes.c_char_p, P(DcbGrid), ctypes.c_void_p, ctypes.c_int64]
+    L.dcb_read_sdf.restype = ctypes.c_int
+    L.dcb_write_sdf.argtypes = [ctypes.c_char_p, P(DcbGrid)]
+    L.dcb_write_sdf.restype = ctypes.c_int
     L.dcb_create.argtypes = [P(ctypes.c_void_p), ctypes.c_int]
     L.dcb_create.restype = ctypes.c_int
     L.dcb_destroy.argtypes = [ctypes.c_void_p]

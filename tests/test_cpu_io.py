@@ -1,0 +1,72 @@
+"""The CLI file formats (src/cpp/dc_cli.cpp:17-47) on the C ABI's native reader and writers:
+the binary `.sdf` layout byte for byte, round trips, and the OBJ text line for line against
+the reference writer's formatting (the C++ stream default: 6 significant digits, i.e. %g),
+on one thread and on many."""
+import struct
+
+import numpy as np
+import pytest
+
+
+def _grid(seed=0, dims=(7, 5, 6)):
+    from contouring_b200 import DenseSdfGrid
+    rng = np.random.default_rng(seed)
+    v = rng.normal(size=int(np.prod(dims))).astype(np.float32)
+    return DenseSdfGrid(*dims, 0.125, 0.25, 0.5, -1.0, -0.75, 0.3, values=v)
+
+
+def test_sdf_layout_and_round_trip(tmp_path):
+    from contouring_b200 import io
+    g = _grid()
+    p = tmp_path / "g.sdf"
+    io.write_sdf(p, g)
+    raw = p.read_bytes()
+    want = struct.pack("<3i6f", g.nx, g.ny, g.nz, g.vx, g.vy, g.vz, g.ox, g.oy, g.oz) + g.values.tobytes()
+    assert raw == want
+    h = io.read_sdf(p)
+    assert (h.nx, h.ny, h.nz) == (g.nx, g.ny, g.nz)
+    assert (h.vx, h.vy, h.vz, h.ox, h.oy, h.oz) == tuple(float(np.float32(x)) for x in (g.vx, g.vy, g.vz, g.ox, g.oy, g.oz))
+    assert np.array_equal(h.values, g.values)
+
+
+def test_sdf_errors(tmp_path):
+    import ctypes
+    from contouring_b200 import DcbError, _lib, io
+    with pytest.raises(DcbError):
+        io.read_sdf(tmp_path / "missing.sdf")
+    p = tmp_path / "short.sdf"
+    p.write_bytes(struct.pack("<3i6f", 4, 4, 4, 1, 1, 1, 0, 0, 0) + b"\0" * 8)
+    with pytest.raises(DcbError):
+        io.read_sdf(p)
+    io.write_sdf(p, _grid())
+    h = _lib.DcbGrid()
+    buf = np.empty(10, np.float32)
+    assert _lib.lib().dcb_read_sdf(bytes(p), ctypes.byref(h), buf.ctypes.data, 10) == _lib.DCB_ERR_TOO_LARGE
+
+
+def _obj_text(V, F):
+    lines = ["v %g %g %g" % tuple(float(x) for x in v) for v in V]
+    lines += ["f " + " ".join(str(int(i) + 1) for i in f) for f in F]
+    return "\n".join(lines) + "\n"
+
+
+@pytest.mark.parametrize("threads", [1, 0])
+@pytest.mark.parametrize("vpf", [4, 3])
+def test_obj_text(tmp_path, threads, vpf):
+    from contouring_b200 import io
+    rng = np.random.default_rng(3)
+    V = (rng.normal(size=(70000, 3)) * 10.0 ** rng.integers(-8, 6, size=(70000, 1))).astype(np.float32)
+    V[:5] = [[0, -0.0, 1e-30], [1e7, -1e-7, 123456.7], [np.float32(0.1), 1 / 3, 2 / 3], [1, 2, 3], [-0.5, 0.25, 7e20]]
+    F = rng.integers(0, len(V), size=(50000, vpf)).astype(np.int32)
+    p = tmp_path / "m.obj"
+    io.write_obj(p, V, F, verts_per_face=vpf, threads=threads)
+    assert p.read_text() == _obj_text(V, F)
+
+
+def test_obj_from_mesh_and_empty(tmp_path):
+    from contouring_b200 import DualContouringMesh, io
+    m = DualContouringMesh(np.array([0, 0, 0, 1, 0, 0, 1, 1, 0, 0, 1, 0], np.float32), np.array([0, 1, 2, 3], np.int32))
+    io.write_obj(tmp_path / "q.obj", m)
+    assert (tmp_path / "q.obj").read_text() == "v 0 0 0\nv 1 0 0\nv 1 1 0\nv 0 1 0\nf 1 2 3 4\n"
+    io.write_obj(tmp_path / "e.obj", DualContouringMesh())
+    assert (tmp_path / "e.obj").read_text() == ""
