@@ -638,7 +638,8 @@ def main():
     host = torch.empty(vals.numel(), dtype=torch.float32, pin_memory=True)
     host.copy_(vals.cpu())
     hgrid = DenseSdfGrid(*dims, *spacing, *origin, values=host.numpy())
-    mesh, _ = be.extract(hgrid)
+    for _ in range(args.warmup):             # steady state of the pinned output buffers too
+        mesh, _ = be.extract(hgrid)
     torch.cuda.synchronize()
     barrier()
     t0 = time.perf_counter()
@@ -691,7 +692,9 @@ def main():
                          "faces": round(stats.face_emission_ms, 4)},
             "escalated_fp64_cells": stats.escalated_fp64_cells, "winding_fp64_faces": stats.winding_fp64_faces,
             "e2e": {"value": round(e2e_value, 2) if e2e_value else None, "unit": "Mcells/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h, "ms_per_step": round(e2e_s * 1e3, 2)},
+                    "d2h_bytes_per_step": d2h, "ms_per_step": round(e2e_s * 1e3, 2),
+                    "last_step_upload_ms": round(est.upload_ms, 2) if args.e2e_steps > 0 else None,
+                    "last_step_download_ms": round(est.download_ms, 2) if args.e2e_steps > 0 else None},
             "gpu_launches": KERNELS_PER_STEP * args.steps,
             "clocks": clk.summary(),
             "cpu_baseline": cpu,

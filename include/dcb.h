@@ -171,6 +171,13 @@ int dcb_extract_device(dcb_handle h, const dcb_grid* grid, const dcb_opts* opts,
 int dcb_extract_host(dcb_handle h, const dcb_grid* grid, const dcb_opts* opts,
                      dcb_mesh_host* out, dcb_stats* stats, void* cuda_stream);
 
+/* dcb_extract_host without the download: grid->values is a host pointer (pinned for full
+ * bandwidth), the mesh stays in the handle's device buffers as with dcb_extract_device. The
+ * caller then sizes its own host arrays (e.g. pinned) from `out` and calls
+ * dcb_copy_mesh_to_host: one device-to-host copy, no staging through the handle. */
+int dcb_extract_upload(dcb_handle h, const dcb_grid* grid, const dcb_opts* opts,
+                       dcb_mesh_dev* out, dcb_stats* stats, void* cuda_stream);
+
 /* Copy the last mesh of `h` into caller-owned host arrays (3*V floats, vpf*F ints). */
 int dcb_copy_mesh_to_host(dcb_handle h, float* vertices, int32_t* faces, void* cuda_stream);
 

@@ -30,7 +30,7 @@ EXPORTED = (
     "dcb_copy_mesh_to_host", "dcb_copy_mesh_device", "dcb_copy_cells_to_host",
     "dcb_mark_active_cells_noalloc", "dcb_mesh_to_sdf_device", "dcb_mesh_to_sdf_host",
     "dcb_extract_batch_device", "dcb_backward", "dcb_autotune_mark",
-    "dcb_write_obj", "dcb_read_sdf", "dcb_write_sdf")
+    "dcb_write_obj", "dcb_read_sdf", "dcb_write_sdf", "dcb_extract_upload")
 
 
 class DcbGrid(ctypes.Structure):
@@ -138,6 +138,8 @@ def lib():
     L.dcb_extract_device.restype = ctypes.c_int
     L.dcb_extract_host.argtypes = [ctypes.c_void_p, P(DcbGrid), P(DcbOpts), P(DcbMeshHost), P(DcbStats), ctypes.c_void_p]
     L.dcb_extract_host.restype = ctypes.c_int
+    L.dcb_extract_upload.argtypes = [ctypes.c_void_p, P(DcbGrid), P(DcbOpts), P(DcbMeshDev), P(DcbStats), ctypes.c_void_p]
+    L.dcb_extract_upload.restype = ctypes.c_int
     L.dcb_copy_mesh_to_host.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
     L.dcb_copy_mesh_to_host.restype = ctypes.c_int
     L.dcb_copy_mesh_device.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]

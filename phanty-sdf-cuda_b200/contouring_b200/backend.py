@@ -11,6 +11,7 @@ terminating the process (the reference exits on CUDA errors: src/cuda/dc_cuda.cu
 """
 import ctypes
 import enum
+import time
 
 import numpy as np
 
@@ -183,6 +184,20 @@ class DualContouringStats:
         return d
 
 
+def _host_array(n, dtype):
+    """A host array for a mesh download: page-locked (torch's caching host allocator, so the
+    copy runs at full DMA speed and repeated calls reuse blocks) when torch with CUDA is
+    present, else ordinary memory."""
+    try:
+        import torch
+        if torch.cuda.is_available():
+            tdt = torch.float32 if dtype == np.float32 else torch.int32
+            return torch.empty(max(n, 0), dtype=tdt, pin_memory=True).numpy()
+    except ImportError:
+        pass
+    return np.empty(n, dtype)
+
+
 def _current_stream():
     try:
         import torch
@@ -231,14 +246,24 @@ class B200DualContouringBackend:
             raise DcbError(_lib.DCB_ERR_INVALID_ARGUMENT, "values has %d entries, expected nx*ny*nz" % vals.size)
         gc = self._grid_c(grid, vals.ctypes.data)
         st = _lib.DcbStats()
-        mh = _lib.DcbMeshHost()
+        md = _lib.DcbMeshDev()
         s = _current_stream() if stream is None else stream
-        _lib.check(self._L.dcb_extract_host(self._h, ctypes.byref(gc), ctypes.byref(self.options.to_c()),
-                                            ctypes.byref(mh), ctypes.byref(st), ctypes.c_void_p(s)), self._h)
-        self._last_nv = mh.vertex_count
-        self._last_vpf = mh.verts_per_face
+        # upload + extraction; the mesh is then read once, straight into the returned arrays
+        _lib.check(self._L.dcb_extract_upload(self._h, ctypes.byref(gc), ctypes.byref(self.options.to_c()),
+                                              ctypes.byref(md), ctypes.byref(st), ctypes.c_void_p(s)), self._h)
+        self._last_nv = md.vertex_count
+        self._last_vpf = md.verts_per_face
         self._generation += 1
-        return self._host_mesh(mh), DualContouringStats.from_c(st)
+        nv, nf, vpf = md.vertex_count, md.face_count, md.verts_per_face
+        V = _host_array(3 * nv, np.float32)
+        F = _host_array(vpf * nf, np.int32)
+        t0 = time.perf_counter()
+        _lib.check(self._L.dcb_copy_mesh_to_host(self._h, V.ctypes.data if nv else None,
+                                                 F.ctypes.data if nf else None, ctypes.c_void_p(s)), self._h)
+        stats = DualContouringStats.from_c(st)
+        stats.download_ms = (time.perf_counter() - t0) * 1e3
+        stats.total_ms += stats.download_ms
+        return DualContouringMesh(V, F), stats
 
     @staticmethod
     def _host_mesh(mh):

@@ -1044,6 +1044,40 @@ int dcb_extract_host(dcb_handle h, const dcb_grid* grid, const dcb_opts* opts, d
     return DCB_OK;
 }
 
+int dcb_extract_upload(dcb_handle h, const dcb_grid* grid, const dcb_opts* opts, dcb_mesh_dev* out,
+                       dcb_stats* stats, void* cuda_stream) {
+    int rc = validate(h, grid);
+    if (rc != DCB_OK) return rc;
+    if (cudaSetDevice(h->device) != cudaSuccess) { cudaGetLastError(); return fail(h, DCB_ERR_CUDA, "set device"); }
+    dcb_opts def;
+    dcb_default_opts(&def);
+    const dcb_opts* o = opts ? opts : &def;
+    if (!known_method(o->method)) return fail(h, DCB_ERR_NOT_SUPPORTED, "unknown method");
+    if (!(o->svd_threshold >= 0.0)) return fail(h, DCB_ERR_INVALID_ARGUMENT, "svd_threshold must be >= 0");
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(cuda_stream);
+    if (stats) std::memset(stats, 0, sizeof(*stats));
+    const size_t npts = (size_t)grid->nx * grid->ny * grid->nz;
+    DCB_TRY(h, ensure(h->grid, sizeof(float) * npts), "alloc grid");
+    DCB_TRY(h, cudaEventRecord(h->ev[0], s), "event");
+    DCB_TRY(h, cudaMemcpyAsync(h->grid.p, grid->values, sizeof(float) * npts, cudaMemcpyHostToDevice, s), "upload grid");
+    DCB_TRY(h, cudaEventRecord(h->ev[1], s), "event");
+    dcb_grid dg = *grid;
+    dg.values = as<float>(h->grid);
+    rc = run_method(h, &dg, o, s, stats);
+    if (rc != DCB_OK) return rc;
+    fill_times(h, stats, true);
+    if (stats) stats->total_ms = elapsed(h->ev[0], h->ev[4]);
+    if (out) {
+        out->vertex_count = h->nv;
+        out->face_count = h->nf;
+        out->verts_per_face = h->vpf;
+        out->vertices = as<float>(h->V);
+        out->faces = face_ptr(h);
+        out->cell_coords = h->cells_per_vertex ? as<uint64_t>(h->sp_vcell) : as<uint64_t>(h->list);
+    }
+    return DCB_OK;
+}
+
 int dcb_copy_mesh_to_host(dcb_handle h, float* vertices, int32_t* faces, void* cuda_stream) {
     if (!h) return DCB_ERR_INVALID_ARGUMENT;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(cuda_stream);
