@@ -392,6 +392,35 @@ def run_mesh_workload(args):
                {"workload": "icospheres32_mesh_to_sdf512", "grid": list(dims), "triangles": len(F)},
                stage_ms={"bins": round(st.bins_ms, 4), "band": round(st.band_ms, 4), "sign": round(st.sign_ms, 4),
                          "relax": round(st.relax_ms, 4)}, **extra)
+    # voxelize-first (dc_cli --voxelize-first, voxel_res = grid resolution by default)
+    vres = dims[0]
+    msv = _timed(lambda: mesh_to_sdf_tensor(be, Vd, Fd, dims, org, sp, out=out, voxelize_first=True, voxel_res=vres),
+                 args.steps, args.warmup)
+    _, stv = mesh_to_sdf_tensor(be, Vd, Fd, dims, org, sp, out=out, voxelize_first=True, voxel_res=vres)
+    extra = {}
+    if os.path.exists(ref_path):
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import numpy as np
+        import oracle as O        # only its ref_mesh_to_sdf: the reference's own CUDA code, the comparator
+        ts = []
+        r = None
+        for q in range(min(args.warmup, 2) + min(args.steps, 3)):
+            r = O.ref_mesh_to_sdf(V, F, dims, org, sp, voxelize_first=True, voxel_res=vres, exact=False)
+            if r is None:
+                break
+            if q >= min(args.warmup, 2):
+                ts.append(r[1])
+        if r is not None:
+            ours = out.cpu().numpy()
+            ms_ref = statistics.median(ts)
+            extra["reference_cuda"] = {"ms_per_step": round(ms_ref, 3),
+                                       "sign_agreement": float(np.mean(np.sign(ours) == np.sign(r[0]))),
+                                       "speedup": round(ms_ref / msv, 2)}
+    _side_line("mesh_to_sdf_voxelized_mpoints_per_s", npts / (msv / 1e3) / 1e6, "Mpoints/s", msv, args,
+               {"workload": "icospheres32_mesh_to_sdf512_voxelize_first", "grid": list(dims), "triangles": len(F),
+                "voxel_res": vres},
+               stage_ms={"bins": round(stv.bins_ms, 4), "band": round(stv.band_ms, 4),
+                         "voxel_solid_and_sign": round(stv.sign_ms, 4)}, voxel_flood_passes=stv.flood_passes, **extra)
     be.close()
     return 0
 

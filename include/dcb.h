@@ -288,6 +288,20 @@ int dcb_mesh_to_sdf_host(dcb_handle h, const float* vertices, int64_t num_vertic
                          int64_t num_faces, int nx, int ny, int nz, float ox, float oy, float oz, float vx,
                          float vy, float vz, float* out_values, dcb_sdf_stats* stats, void* cuda_stream);
 
+/* The two calls above with the reference's remaining arguments of compute_mesh_sdf[_device]_cuda
+ * (include/mesh_to_sdf.h; dc_cli's --voxelize-first / --voxel-res): voxelize_first != 0 takes
+ * the sign of the points beyond the band from a voxel solid of voxel_res^3 voxels (clamped to
+ * [32, 2048]; mesh_to_sdf_cuda.cu:458-577, 764-832) instead of the exterior flood and the
+ * relaxation. voxelize_first = 0 is the plain conversion (voxel_res unused). */
+int dcb_mesh_to_sdf_device_ex(dcb_handle h, const float* vertices, int64_t num_vertices, const int32_t* faces,
+                              int64_t num_faces, int nx, int ny, int nz, float ox, float oy, float oz, float vx,
+                              float vy, float vz, int voxelize_first, int voxel_res, float* out_values,
+                              dcb_sdf_stats* stats, void* cuda_stream);
+int dcb_mesh_to_sdf_host_ex(dcb_handle h, const float* vertices, int64_t num_vertices, const int32_t* faces,
+                            int64_t num_faces, int nx, int ny, int nz, float ox, float oy, float oz, float vx,
+                            float vy, float vz, int voxelize_first, int voxel_res, float* out_values,
+                            dcb_sdf_stats* stats, void* cuda_stream);
+
 /* ---- adjoint of the vertices ------------------------------------------------------------ */
 
 /* Gradient of a loss with respect to the grid values, given its gradient with respect to the

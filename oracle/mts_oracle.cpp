@@ -16,6 +16,13 @@
 //   sign fill       init_exterior_border / propagate_exterior_signs /
 //                   resolve_interior_cavities (:362-428)
 //   eikonal         4 Jacobi passes of eikonal_relaxation_kernel (:430-456)
+// With voxelize_first (mts_compute_voxelized; the `if` branch at :764-832): a voxel_res^3
+// solid — every voxel corner within 0.866 * (largest voxel side) of a triangle is shell
+// (rasterize_triangles_to_voxels_kernel, :458-501), the shell dilated by one voxel
+// (dilate_voxel_shell_kernel, :503-526), the exterior flooded from the border through the
+// other voxels to its fixpoint (:528-575; the reference stops after 3*voxel_res in-place
+// passes), the rest solid — gives the points beyond the band -10 inside, +10 outside
+// (apply_solid_voxel_sign_mask_kernel, :660-690), with no flood and no relaxation of the grid.
 // All arithmetic is float, evaluated as the source writes it (no contraction: compile with
 // -ffp-contract=off). Definitions where the reference's GPU execution is not deterministic:
 //   * the triangles of a bin are visited in ascending triangle index (the reference fills
@@ -337,6 +344,98 @@ int mts_compute(const float* V, int64_t nv, const int* F, int64_t nf, int nx, in
         st->bin_entries = (int64_t)B.tris.size();
         st->band_points = band;
         st->exterior_filled = filled;
+    }
+    return 0;
+}
+
+
+// The conversion with voxelize_first (see the header); solid (optional, voxel_res^3 bytes,
+// clamped resolution) receives the voxel solid.
+int mts_compute_voxelized(const float* V, int64_t nv, const int* F, int64_t nf, int nx, int ny, int nz, float ox,
+                          float oy, float oz, float vx, float vy, float vz, int voxel_res, int threads, float* out,
+                          mts_stats* st, uint8_t* solid) {
+    (void)nv;
+    if (nx < 1 || ny < 1 || nz < 1 || !V || !F || !out) return -1;
+    Mesh m{V, F, nf};
+    const int vr = std::max(32, std::min(2048, voxel_res));
+    const float vox_x = ((float)nx * vx) / (float)vr, vox_y = ((float)ny * vy) / (float)vr;
+    const float vox_z = ((float)nz * vz) / (float)vr;
+    const int64_t NV = (int64_t)vr * vr * vr;
+    std::vector<uint8_t> shell(NV, 0);
+    const float mvd = std::fmax(vox_x, std::fmax(vox_y, vox_z)) * 0.8660254f;
+    const float lim = mvd * mvd;
+    for (int64_t f = 0; f < nf; ++f) {
+        const F3 a = m.vtx((int)f, 0), b = m.vtx((int)f, 1), c = m.vtx((int)f, 2);
+        const float mnx = std::fmin(a.x, std::fmin(b.x, c.x)), mny = std::fmin(a.y, std::fmin(b.y, c.y));
+        const float mnz = std::fmin(a.z, std::fmin(b.z, c.z)), mxx = std::fmax(a.x, std::fmax(b.x, c.x));
+        const float mxy = std::fmax(a.y, std::fmax(b.y, c.y)), mxz = std::fmax(a.z, std::fmax(b.z, c.z));
+        const int x0 = bin_coord(mnx, ox, vox_x, vr), x1 = bin_coord(mxx, ox, vox_x, vr);
+        const int y0 = bin_coord(mny, oy, vox_y, vr), y1 = bin_coord(mxy, oy, vox_y, vr);
+        const int z0 = bin_coord(mnz, oz, vox_z, vr), z1 = bin_coord(mxz, oz, vox_z, vr);
+        for (int bz = z0; bz <= z1; ++bz)
+            for (int by = y0; by <= y1; ++by)
+                for (int bx = x0; bx <= x1; ++bx) {
+                    F3 closest;
+                    const F3 q = mk(ox + (float)bx * vox_x, oy + (float)by * vox_y, oz + (float)bz * vox_z);
+                    if (point_triangle(q, a, b, c, closest) <= lim) shell[bx + (int64_t)vr * (by + (int64_t)vr * bz)] = 1;
+                }
+    }
+    std::vector<uint8_t> dil(NV, 0);
+#pragma omp parallel for schedule(static) num_threads(nthreads(threads))
+    for (int64_t q = 0; q < NV; ++q) {
+        const int ix = (int)(q % vr), iy = (int)((q / vr) % vr), iz = (int)(q / ((int64_t)vr * vr));
+        uint8_t d = 0;
+        for (int z = std::max(0, iz - 1); z <= std::min(vr - 1, iz + 1) && !d; ++z)
+            for (int y = std::max(0, iy - 1); y <= std::min(vr - 1, iy + 1) && !d; ++y)
+                for (int x = std::max(0, ix - 1); x <= std::min(vr - 1, ix + 1); ++x)
+                    if (shell[x + (int64_t)vr * (y + (int64_t)vr * z)]) { d = 1; break; }
+        dil[q] = d;
+    }
+    std::vector<uint8_t> ext(NV, 0);
+    std::vector<int64_t> stack;
+    for (int64_t q = 0; q < NV; ++q) {
+        const int ix = (int)(q % vr), iy = (int)((q / vr) % vr), iz = (int)(q / ((int64_t)vr * vr));
+        const bool border = ix == 0 || ix == vr - 1 || iy == 0 || iy == vr - 1 || iz == 0 || iz == vr - 1;
+        if (border && !dil[q]) { ext[q] = 1; stack.push_back(q); }
+    }
+    const int64_t vplane = (int64_t)vr * vr;
+    while (!stack.empty()) {
+        const int64_t q = stack.back();
+        stack.pop_back();
+        const int ix = (int)(q % vr), iy = (int)((q / vr) % vr), iz = (int)(q / vplane);
+        const int64_t nb[6] = {ix > 0 ? q - 1 : -1, ix < vr - 1 ? q + 1 : -1, iy > 0 ? q - vr : -1,
+                               iy < vr - 1 ? q + vr : -1, iz > 0 ? q - vplane : -1, iz < vr - 1 ? q + vplane : -1};
+        for (int t = 0; t < 6; ++t) {
+            const int64_t r = nb[t];
+            if (r < 0 || ext[r] || dil[r]) continue;
+            ext[r] = 1;
+            stack.push_back(r);
+        }
+    }
+    if (solid)
+        for (int64_t q = 0; q < NV; ++q) solid[q] = ext[q] ? 0 : 1;
+    Bins B;
+    build_bins(m, nx, ny, nz, ox, oy, oz, vx, vy, vz, B);
+    const int64_t N = (int64_t)nx * ny * nz;
+    const int64_t plane = (int64_t)nx * ny;
+#pragma omp parallel for schedule(dynamic, 4096) num_threads(nthreads(threads))
+    for (int64_t q = 0; q < N; ++q) out[q] = band_value(m, B, nx, ny, ox, oy, oz, vx, vy, vz, q);
+    int64_t band = 0, outside = 0;
+    for (int64_t q = 0; q < N; ++q) {
+        if (out[q] != kFar) { ++band; continue; }
+        const int ix = (int)(q % nx), iy = (int)((q / nx) % ny), iz = (int)(q / plane);
+        const int bx = bin_coord(ox + (float)ix * vx, ox, vox_x, vr);
+        const int by = bin_coord(oy + (float)iy * vy, oy, vox_y, vr);
+        const int bz = bin_coord(oz + (float)iz * vz, oz, vox_z, vr);
+        const bool exterior = ext[bx + (int64_t)vr * (by + (int64_t)vr * bz)] != 0;
+        out[q] = exterior ? 10.0f : -10.0f;
+        outside += exterior ? 1 : 0;
+    }
+    if (st) {
+        st->num_bins = (int64_t)B.gx * B.gy * B.gz;
+        st->bin_entries = (int64_t)B.tris.size();
+        st->band_points = band;
+        st->exterior_filled = outside;
     }
     return 0;
 }

@@ -171,6 +171,9 @@ def _mts():
         lib.mts_compute.restype = ctypes.c_int
         lib.mts_band_values.argtypes = common + [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_void_p]
         lib.mts_band_values.restype = ctypes.c_int
+        lib.mts_compute_voxelized.argtypes = common + [ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                                       ctypes.POINTER(_MtsStats), ctypes.c_void_p]
+        lib.mts_compute_voxelized.restype = ctypes.c_int
         lib._typed = True
     return lib
 
@@ -195,6 +198,27 @@ def mesh_to_sdf(V, F, dims, origin, spacing, threads=0):
     if rc != 0:
         raise ValueError("oracle rejected the input")
     return out, {k: getattr(st, k) for k, _ in _MtsStats._fields_}
+
+
+def mesh_to_sdf_voxelized(V, F, dims, origin, spacing, voxel_res=256, threads=0, return_solid=False):
+    """The conversion with voxelize_first: far points signed by a voxel_res^3 solid. Returns
+    (float32 values, stats), plus the solid (uint8, (vres, vres, vres) z-major) if asked."""
+    V, F = _mesh_args(V, F)
+    nx, ny, nz = (int(d) for d in dims)
+    out = np.empty(nx * ny * nz, np.float32)
+    st = _MtsStats()
+    vr = max(32, min(2048, int(voxel_res)))
+    solid = np.empty(vr ** 3, np.uint8) if return_solid else None
+    rc = _mts().mts_compute_voxelized(V.ctypes.data, len(V), F.ctypes.data, len(F), nx, ny, nz,
+                                      *[float(x) for x in origin], *[float(x) for x in spacing], int(voxel_res),
+                                      int(threads), out.ctypes.data, ctypes.byref(st),
+                                      solid.ctypes.data if return_solid else None)
+    if rc != 0:
+        raise ValueError("oracle rejected the input")
+    stats = {k: getattr(st, k) for k, _ in _MtsStats._fields_}
+    if return_solid:
+        return out, stats, solid.reshape(vr, vr, vr)
+    return out, stats
 
 
 def mesh_band_values(V, F, dims, origin, spacing, idx, threads=0):
@@ -418,3 +442,32 @@ def ref_sparse(d_values_ptr, dims, spacing, origin, brick_size=8, normal_mode=0,
     stats = dict(zip(SPARSE_STATS, st[:12].tolist()))
     stats.update(vertex_count=int(st[12]), face_count=int(st[13]))
     return {"V": V, "F": F, "stats": stats, "times": times.tolist()}
+
+
+def ref_mesh_to_sdf(V, F, dims, origin, spacing, voxelize_first=False, voxel_res=256, exact=True):
+    """The reference's own CUDA mesh -> SDF conversion (compute_mesh_sdf_device_cuda,
+    src/cuda/mesh_to_sdf_cuda.cu:740-1009) from ``oracle/_ref/`` (``make -C oracle ref``):
+    ``exact`` selects the build without FMA contraction. Host arrays in; returns (float32
+    values, its own milliseconds), or None when the library was not built."""
+    name = "libref_dc_cuda_exact.so" if exact else "libref_dc_cuda.so"
+    path = os.path.join(_HERE, "_ref", name)
+    if not os.path.exists(path):
+        return None
+    key = path + ":sdf"
+    if key not in _libs:
+        lib = ctypes.CDLL(path)
+        lib.refsdf_compute_ex.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int] + \
+            [ctypes.c_int] * 3 + [ctypes.c_float] * 6 + [ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]
+        lib.refsdf_compute_ex.restype = ctypes.c_int
+        _libs[key] = lib
+    lib = _libs[key]
+    V, F = _mesh_args(V, F)
+    nx, ny, nz = (int(d) for d in dims)
+    out = np.empty(nx * ny * nz, np.float32)
+    ms = ctypes.c_float()
+    rc = lib.refsdf_compute_ex(V.ctypes.data, len(V), F.ctypes.data, len(F), nx, ny, nz,
+                               *[float(x) for x in origin], *[float(x) for x in spacing],
+                               1 if voxelize_first else 0, int(voxel_res), ctypes.byref(ms), out.ctypes.data)
+    if rc != 0:
+        return None
+    return out, ms.value

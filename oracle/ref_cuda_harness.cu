@@ -1,6 +1,7 @@
 // ref_cuda_harness.cu — TEST INFRASTRUCTURE ONLY: a C entry point around the reference's own
 // CUDA dense backend (CudaDualContouringBackend::extract_device, src/cuda/dc_cuda.cu:652-847,
-// compiled from the reference's source by oracle/Makefile's `ref` target into oracle/_ref/).
+// compiled from the reference's source by oracle/Makefile's `ref` target into oracle/_ref/,
+// as shipped and, for parity checks, without FMA contraction).
 // It is a same-GPU speed bar for bench.py's refcuda512 workload and nothing else: its
 // vertices differ from the CPU backend's (no normal averaging, clamping into the cell).
 //
@@ -55,6 +56,22 @@ extern "C" int refsdf_compute(const float* vertices, int num_vertices, const int
     float t = 0.f;
     DenseSdfGridDevice g = compute_mesh_sdf_device_cuda(vertices, num_vertices, faces, num_faces, nx, ny, nz, ox, oy,
                                                         oz, vx, vy, vz, &t, false, 256);
+    if (ms) *ms = t;
+    if (out_host)
+        cudaMemcpy(out_host, g.d_values, sizeof(float) * (size_t)nx * ny * nz, cudaMemcpyDeviceToHost);
+    free_mesh_sdf_device_cuda(g);
+    return 0;
+}
+
+// The same with the reference's voxelize_first / voxel_res arguments (mesh_to_sdf_cuda.cu:764-832).
+extern "C" int refsdf_compute_ex(const float* vertices, int num_vertices, const int* faces, int num_faces, int nx,
+                                 int ny, int nz, float ox, float oy, float oz, float vx, float vy, float vz,
+                                 int voxelize_first, int voxel_res, float* ms, float* out_host) {
+    if (nx < 2 || ny < 2 || nz < 2 || !vertices || !faces) return -1;
+    if ((long long)nx * ny * nz >= 0x7fffffffLL) return -2;
+    float t = 0.f;
+    DenseSdfGridDevice g = compute_mesh_sdf_device_cuda(vertices, num_vertices, faces, num_faces, nx, ny, nz, ox, oy,
+                                                        oz, vx, vy, vz, &t, voxelize_first != 0, voxel_res);
     if (ms) *ms = t;
     if (out_host)
         cudaMemcpy(out_host, g.d_values, sizeof(float) * (size_t)nx * ny * nz, cudaMemcpyDeviceToHost);

@@ -30,7 +30,8 @@ EXPORTED = (
     "dcb_copy_mesh_to_host", "dcb_copy_mesh_device", "dcb_copy_cells_to_host",
     "dcb_mark_active_cells_noalloc", "dcb_mesh_to_sdf_device", "dcb_mesh_to_sdf_host",
     "dcb_extract_batch_device", "dcb_backward", "dcb_autotune_mark",
-    "dcb_write_obj", "dcb_read_sdf", "dcb_write_sdf", "dcb_extract_upload")
+    "dcb_write_obj", "dcb_read_sdf", "dcb_write_sdf", "dcb_extract_upload", "dcb_mesh_to_sdf_device_ex",
+    "dcb_mesh_to_sdf_host_ex")
 
 
 class DcbGrid(ctypes.Structure):
@@ -162,6 +163,10 @@ def lib():
         [ctypes.c_int] * 3 + [ctypes.c_float] * 6 + [ctypes.c_void_p, P(DcbSdfStats), ctypes.c_void_p]
     for name in ("dcb_mesh_to_sdf_device", "dcb_mesh_to_sdf_host"):
         getattr(L, name).argtypes = sdf_args
+        getattr(L, name).restype = ctypes.c_int
+    sdf_ex_args = sdf_args[:14] + [ctypes.c_int, ctypes.c_int] + sdf_args[14:]   # after the 6 floats
+    for name in ("dcb_mesh_to_sdf_device_ex", "dcb_mesh_to_sdf_host_ex"):
+        getattr(L, name).argtypes = sdf_ex_args
         getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L

@@ -446,19 +446,23 @@ class MeshSdfStats:
         return {name: getattr(self, name) for name, _ in _lib.DcbSdfStats._fields_}
 
 
-def _sdf_call(backend, fn, Vp, nv, Fp, nf, dims, origin, spacing, outp, stream):
+def _sdf_call(backend, fn, Vp, nv, Fp, nf, dims, origin, spacing, outp, stream, voxelize_first, voxel_res):
     st = _lib.DcbSdfStats()
     s = _current_stream() if stream is None else stream
     _lib.check(fn(backend._h, ctypes.c_void_p(Vp), int(nv), ctypes.c_void_p(Fp), int(nf),
                   *[int(d) for d in dims], *[float(o) for o in origin], *[float(v) for v in spacing],
+                  1 if voxelize_first else 0, int(voxel_res),
                   ctypes.c_void_p(outp), ctypes.byref(st), ctypes.c_void_p(s)), backend._h)
     return MeshSdfStats(st)
 
 
-def mesh_to_sdf_tensor(backend, vertices, faces, dims, origin, spacing, out=None, stream=None):
+def mesh_to_sdf_tensor(backend, vertices, faces, dims, origin, spacing, out=None, stream=None,
+                       voxelize_first=False, voxel_res=256):
     """``compute_mesh_sdf_device_cuda`` (src/cuda/mesh_to_sdf_cuda.cu:740-1009) on CUDA tensors:
     float32 (n,3) vertices and int32 (m,3) triangles in, a float32 CUDA tensor of nx*ny*nz
-    signed distances (x fastest) out, with the conversion's stats."""
+    signed distances (x fastest) out, with the conversion's stats. ``voxelize_first`` /
+    ``voxel_res`` as in the reference: the points beyond the band take their sign from a
+    voxel_res^3 solid."""
     import torch
     V = vertices.to(torch.float32).contiguous()
     F = faces.to(torch.int32).contiguous()
@@ -469,17 +473,18 @@ def mesh_to_sdf_tensor(backend, vertices, faces, dims, origin, spacing, out=None
         out = torch.empty(n, dtype=torch.float32, device=V.device)
     elif out.numel() != n or out.dtype != torch.float32 or not out.is_cuda or not out.is_contiguous():
         raise DcbError(_lib.DCB_ERR_INVALID_ARGUMENT, "out must be a contiguous float32 CUDA tensor of nx*ny*nz")
-    st = _sdf_call(backend, backend._L.dcb_mesh_to_sdf_device, V.data_ptr(), V.shape[0], F.data_ptr(), F.shape[0],
-                   dims, origin, spacing, out.data_ptr(), stream)
+    st = _sdf_call(backend, backend._L.dcb_mesh_to_sdf_device_ex, V.data_ptr(), V.shape[0], F.data_ptr(),
+                   F.shape[0], dims, origin, spacing, out.data_ptr(), stream, voxelize_first, voxel_res)
     return out, st
 
 
-def mesh_to_sdf_cuda(backend, vertices, faces, nx, ny, nz, ox, oy, oz, vx, vy, vz):
+def mesh_to_sdf_cuda(backend, vertices, faces, nx, ny, nz, ox, oy, oz, vx, vy, vz, voxelize_first=False,
+                     voxel_res=256):
     """The reference module's ``mesh_to_sdf_cuda`` (src/cpp/bindings.cpp:270-276): host arrays in,
     ``(DenseSdfGrid, milliseconds)`` out."""
     V = np.ascontiguousarray(np.asarray(vertices, np.float32).reshape(-1, 3))
     F = np.ascontiguousarray(np.asarray(faces, np.int32).reshape(-1, 3))
     out = np.empty(int(nx) * int(ny) * int(nz), np.float32)
-    st = _sdf_call(backend, backend._L.dcb_mesh_to_sdf_host, V.ctypes.data, len(V), F.ctypes.data, len(F),
-                   (nx, ny, nz), (ox, oy, oz), (vx, vy, vz), out.ctypes.data, None)
+    st = _sdf_call(backend, backend._L.dcb_mesh_to_sdf_host_ex, V.ctypes.data, len(V), F.ctypes.data, len(F),
+                   (nx, ny, nz), (ox, oy, oz), (vx, vy, vz), out.ctypes.data, None, voxelize_first, voxel_res)
     return DenseSdfGrid(nx, ny, nz, vx, vy, vz, ox, oy, oz, values=out), st.total_ms

@@ -66,7 +66,7 @@ struct dcb_context {
     int cells_per_vertex = 0;         // 1: the vertex -> cell list is `sp_vcell` (two vertices per cell)
     // mesh -> SDF workspace
     DevBuf m_verts, m_faces, m_out, m_tris, m_bin_count, m_bin_start, m_bin_fill, m_bin_scratch, m_bin_tris,
-        m_bin_active, m_active_list, m_axis_start, m_far, m_ext, m_tmp, m_partials, m_counters;
+        m_bin_active, m_active_list, m_axis_start, m_far, m_ext, m_tmp, m_partials, m_counters, m_vox;
     void* h_sdf_counters = nullptr;   // pinned SdfCounters
     void* h_counters = nullptr;       // pinned Counters
     void* hV = nullptr; size_t hV_bytes = 0;
@@ -758,8 +758,8 @@ bool finite_pos_spacing(float v) { return std::isfinite(v) && v > 0.f; }
 
 // The mesh -> SDF pipeline on device arrays; out has nx*ny*nz floats.
 int run_mesh_sdf(dcb_context* h, const float* d_verts, int64_t nv, const int32_t* d_faces, int64_t nf, int nx,
-                 int ny, int nz, float ox, float oy, float oz, float vx, float vy, float vz, float* out,
-                 dcb_sdf_stats* st, cudaStream_t s) {
+                 int ny, int nz, float ox, float oy, float oz, float vx, float vy, float vz, int voxelize_first,
+                 int voxel_res, float* out, dcb_sdf_stats* st, cudaStream_t s) {
     if (nx < 1 || ny < 1 || nz < 1) return fail(h, DCB_ERR_INVALID_ARGUMENT, "grid needs at least 1 point per axis");
     if (nv < 0 || nf < 0 || (nf > 0 && (!d_verts || !d_faces)) || !out)
         return fail(h, DCB_ERR_INVALID_ARGUMENT, "null mesh or output array");
@@ -817,19 +817,49 @@ int run_mesh_sdf(dcb_context* h, const float* d_verts, int64_t nv, const int32_t
     DCB_TRY(h, cudaEventRecord(ev[1], s), "event");
     DCB_TRY(h, launch_sdf_band(P, h->num_sms, s), "launch band");
     DCB_TRY(h, cudaEventRecord(ev[2], s), "event");
-    DCB_TRY(h, launch_sdf_masks(P, h->num_sms, s), "launch masks");
     int64_t passes = 0;
-    for (;;) {
-        DCB_TRY(h, cudaMemsetAsync(&dc->changed, 0, sizeof(int), s), "memset");
-        DCB_TRY(h, launch_sdf_flood(P, &dc->changed, h->num_sms, s), "launch flood");
-        DCB_TRY(h, cudaMemcpyAsync(&hc->changed, &dc->changed, sizeof(int), cudaMemcpyDeviceToHost, s), "read flag");
-        DCB_TRY(h, cudaStreamSynchronize(s), "flood");
-        ++passes;
-        if (!hc->changed) break;
-        if (passes > 1000000) return fail(h, DCB_ERR_INTERNAL, "exterior flood did not converge");
+    if (!voxelize_first) {
+        DCB_TRY(h, launch_sdf_masks(P, h->num_sms, s), "launch masks");
+        for (;;) {
+            DCB_TRY(h, cudaMemsetAsync(&dc->changed, 0, sizeof(int), s), "memset");
+            DCB_TRY(h, launch_sdf_flood(P, &dc->changed, h->num_sms, s), "launch flood");
+            DCB_TRY(h, cudaMemcpyAsync(&hc->changed, &dc->changed, sizeof(int), cudaMemcpyDeviceToHost, s), "read flag");
+            DCB_TRY(h, cudaStreamSynchronize(s), "flood");
+            ++passes;
+            if (!hc->changed) break;
+            if (passes > 1000000) return fail(h, DCB_ERR_INTERNAL, "exterior flood did not converge");
+        }
+        DCB_TRY(h, cudaEventRecord(ev[3], s), "event");
+        DCB_TRY(h, launch_sdf_finish(P, &dc->exterior, as<float>(h->m_tmp), h->num_sms, s), "launch finish");
+    } else {
+        // the voxel solid (:764-808): shell, dilation, exterior flood to its fixpoint; then the
+        // far grid points take their sign from it (:826-832); no relaxation in this branch
+        const int vr = std::max(32, std::min(2048, voxel_res));
+        P.vres = vr;
+        P.Wv = (vr + 31) / 32;
+        P.vox_vx = ((float)nx * vx) / (float)vr;
+        P.vox_vy = ((float)ny * vy) / (float)vr;
+        P.vox_vz = ((float)nz * vz) / (float)vr;
+        const size_t vwords = (size_t)vr * vr * P.Wv;
+        DCB_TRY(h, ensure(h->m_vox, sizeof(uint32_t) * 3 * vwords), "alloc voxels");
+        P.vshell = as<uint32_t>(h->m_vox);
+        P.vfar = P.vshell + vwords;
+        P.vext = P.vfar + vwords;
+        DCB_TRY(h, cudaMemsetAsync(P.vshell, 0, sizeof(uint32_t) * vwords, s), "memset");
+        DCB_TRY(h, launch_vox_raster(P, h->num_sms, s), "launch voxel raster");
+        DCB_TRY(h, launch_vox_dilate(P, h->num_sms, s), "launch voxel dilation");
+        for (;;) {
+            DCB_TRY(h, cudaMemsetAsync(&dc->changed, 0, sizeof(int), s), "memset");
+            DCB_TRY(h, launch_vox_flood(P, &dc->changed, h->num_sms, s), "launch voxel flood");
+            DCB_TRY(h, cudaMemcpyAsync(&hc->changed, &dc->changed, sizeof(int), cudaMemcpyDeviceToHost, s), "read flag");
+            DCB_TRY(h, cudaStreamSynchronize(s), "voxel flood");
+            ++passes;
+            if (!hc->changed) break;
+            if (passes > 1000000) return fail(h, DCB_ERR_INTERNAL, "voxel flood did not converge");
+        }
+        DCB_TRY(h, cudaEventRecord(ev[3], s), "event");
+        DCB_TRY(h, launch_vox_sign(P, &dc->exterior, h->num_sms, s), "launch voxel sign");
     }
-    DCB_TRY(h, cudaEventRecord(ev[3], s), "event");
-    DCB_TRY(h, launch_sdf_finish(P, &dc->exterior, as<float>(h->m_tmp), h->num_sms, s), "launch finish");
     DCB_TRY(h, cudaEventRecord(ev[4], s), "event");
     DCB_TRY(h, cudaMemcpyAsync(hc, dc, sizeof(SdfCounters), cudaMemcpyDeviceToHost, s), "read counters");
     DCB_TRY(h, cudaStreamSynchronize(s), "mesh to sdf");
@@ -842,7 +872,8 @@ int run_mesh_sdf(dcb_context* h, const float* d_verts, int64_t nv, const int32_t
         st->bins_ms = elapsed(ev[0], ev[1]);
         st->band_ms = elapsed(ev[1], ev[2]);
         st->sign_ms = elapsed(ev[2], ev[3]);
-        st->relax_ms = elapsed(ev[3], ev[4]);
+        st->relax_ms = voxelize_first ? 0.f : elapsed(ev[3], ev[4]);
+        st->sign_ms += voxelize_first ? elapsed(ev[3], ev[4]) : 0.f;
         st->total_ms = elapsed(ev[0], ev[4]);
     }
     return DCB_OK;
@@ -922,7 +953,7 @@ int dcb_destroy(dcb_handle h) {
                       &h->tris, &h->tri_items, &h->m_verts, &h->m_faces, &h->m_out, &h->m_tris,
                       &h->m_bin_count, &h->m_bin_start, &h->m_bin_fill, &h->m_bin_scratch, &h->m_bin_tris,
                       &h->m_bin_active, &h->m_active_list, &h->m_axis_start, &h->m_far, &h->m_ext, &h->m_tmp,
-                      &h->m_partials, &h->m_counters, &h->table, &h->cell_slot, &h->adj_rows, &h->adj_owners, &h->ours_ws,
+                      &h->m_partials, &h->m_counters, &h->m_vox, &h->table, &h->cell_slot, &h->adj_rows, &h->adj_owners, &h->ours_ws,
                       &h->sp_words, &h->sp_brick, &h->sp_vcount, &h->sp_vstart, &h->sp_vtmp, &h->sp_ntmp,
                       &h->sp_N, &h->sp_vcell, &h->sp_fcount, &h->sp_fstart, &h->sp_stage, &h->sp_counters};
     for (DevBuf* b : bufs) if (b->p) cudaFree(b->p);
@@ -1208,19 +1239,35 @@ int dcb_backward(dcb_handle h, const dcb_grid* grid, const dcb_opts* opts, const
     return DCB_OK;
 }
 
-int dcb_mesh_to_sdf_device(dcb_handle h, const float* vertices, int64_t num_vertices, const int32_t* faces,
-                           int64_t num_faces, int nx, int ny, int nz, float ox, float oy, float oz, float vx,
-                           float vy, float vz, float* out_values, dcb_sdf_stats* stats, void* cuda_stream) {
+int dcb_mesh_to_sdf_device_ex(dcb_handle h, const float* vertices, int64_t num_vertices, const int32_t* faces,
+                              int64_t num_faces, int nx, int ny, int nz, float ox, float oy, float oz, float vx,
+                              float vy, float vz, int voxelize_first, int voxel_res, float* out_values,
+                              dcb_sdf_stats* stats, void* cuda_stream) {
     if (!h) return DCB_ERR_INVALID_ARGUMENT;
     if (cudaSetDevice(h->device) != cudaSuccess) { cudaGetLastError(); return fail(h, DCB_ERR_CUDA, "set device"); }
     if (stats) std::memset(stats, 0, sizeof(*stats));
-    return run_mesh_sdf(h, vertices, num_vertices, faces, num_faces, nx, ny, nz, ox, oy, oz, vx, vy, vz, out_values,
-                        stats, reinterpret_cast<cudaStream_t>(cuda_stream));
+    return run_mesh_sdf(h, vertices, num_vertices, faces, num_faces, nx, ny, nz, ox, oy, oz, vx, vy, vz,
+                        voxelize_first, voxel_res, out_values, stats, reinterpret_cast<cudaStream_t>(cuda_stream));
+}
+
+int dcb_mesh_to_sdf_device(dcb_handle h, const float* vertices, int64_t num_vertices, const int32_t* faces,
+                           int64_t num_faces, int nx, int ny, int nz, float ox, float oy, float oz, float vx,
+                           float vy, float vz, float* out_values, dcb_sdf_stats* stats, void* cuda_stream) {
+    return dcb_mesh_to_sdf_device_ex(h, vertices, num_vertices, faces, num_faces, nx, ny, nz, ox, oy, oz, vx, vy, vz,
+                                     0, 256, out_values, stats, cuda_stream);
 }
 
 int dcb_mesh_to_sdf_host(dcb_handle h, const float* vertices, int64_t num_vertices, const int32_t* faces,
                          int64_t num_faces, int nx, int ny, int nz, float ox, float oy, float oz, float vx,
                          float vy, float vz, float* out_values, dcb_sdf_stats* stats, void* cuda_stream) {
+    return dcb_mesh_to_sdf_host_ex(h, vertices, num_vertices, faces, num_faces, nx, ny, nz, ox, oy, oz, vx, vy, vz,
+                                   0, 256, out_values, stats, cuda_stream);
+}
+
+int dcb_mesh_to_sdf_host_ex(dcb_handle h, const float* vertices, int64_t num_vertices, const int32_t* faces,
+                            int64_t num_faces, int nx, int ny, int nz, float ox, float oy, float oz, float vx,
+                            float vy, float vz, int voxelize_first, int voxel_res, float* out_values,
+                            dcb_sdf_stats* stats, void* cuda_stream) {
     if (!h) return DCB_ERR_INVALID_ARGUMENT;
     if (!out_values || num_vertices < 0 || num_faces < 0 || (num_faces > 0 && (!vertices || !faces)))
         return fail(h, DCB_ERR_INVALID_ARGUMENT, "null mesh or output array");
@@ -1237,7 +1284,7 @@ int dcb_mesh_to_sdf_host(dcb_handle h, const float* vertices, int64_t num_vertic
     if (num_faces)
         DCB_TRY(h, cudaMemcpyAsync(h->m_faces.p, faces, sizeof(int32_t) * 3 * num_faces, cudaMemcpyHostToDevice, s), "upload faces");
     const int rc = run_mesh_sdf(h, as<float>(h->m_verts), num_vertices, as<int32_t>(h->m_faces), num_faces, nx, ny, nz,
-                                ox, oy, oz, vx, vy, vz, as<float>(h->m_out), stats, s);
+                                ox, oy, oz, vx, vy, vz, voxelize_first, voxel_res, as<float>(h->m_out), stats, s);
     if (rc != DCB_OK) return rc;
     DCB_TRY(h, cudaMemcpyAsync(out_values, h->m_out.p, sizeof(float) * npts, cudaMemcpyDeviceToHost, s), "download values");
     DCB_TRY(h, cudaStreamSynchronize(s), "download values");

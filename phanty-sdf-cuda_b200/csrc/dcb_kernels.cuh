@@ -333,6 +333,13 @@ struct SdfParams {
     uint32_t* far;                 // [nz*ny][W] bits: value is far
     uint32_t* ext;                 // [nz*ny][W] bits: exterior
     int* err;
+    // voxelize-first (mesh_to_sdf_cuda.cu:458-577, :764-832)
+    int vres;                      // voxels per axis
+    int Wv;                        // 32-voxel words per voxel row
+    float vox_vx, vox_vy, vox_vz;  // voxel size (n*v)/vres
+    uint32_t* vshell;              // [vres*vres][Wv] rasterised shell
+    uint32_t* vfar;                // [vres*vres][Wv] outside the dilated shell (flood passes through)
+    uint32_t* vext;                // [vres*vres][Wv] exterior (flood result)
 };
 void sdf_bin_geometry(SdfParams& P);
 size_t sdf_tri_record_bytes();     // bytes of one triangle record in SdfParams::tris
@@ -342,6 +349,11 @@ cudaError_t launch_sdf_band(const SdfParams& P, int num_sms, cudaStream_t s);
 cudaError_t launch_sdf_masks(const SdfParams& P, int num_sms, cudaStream_t s);
 cudaError_t launch_sdf_flood(const SdfParams& P, int* changed, int num_sms, cudaStream_t s);
 cudaError_t launch_sdf_finish(const SdfParams& P, unsigned long long* filled, float* tmp, int num_sms, cudaStream_t s);
+cudaError_t launch_vox_raster(const SdfParams& P, int num_sms, cudaStream_t s);
+cudaError_t launch_vox_dilate(const SdfParams& P, int num_sms, cudaStream_t s);
+// the exterior flood of the voxel grid (k_flood on vfar / vext)
+cudaError_t launch_vox_flood(const SdfParams& P, int* changed, int num_sms, cudaStream_t s);
+cudaError_t launch_vox_sign(const SdfParams& P, unsigned long long* filled, int num_sms, cudaStream_t s);
 
 // ---- sparse (brick) backends ------------------------------------------------------------
 

@@ -627,6 +627,91 @@ __global__ void __launch_bounds__(256) k_relax(SdfParams P, const float* __restr
     }
 }
 
+// ---- voxelize-first (compute_mesh_sdf_device_cuda with voxelize_first, :764-832) -------------
+
+// A thread per triangle: every voxel corner of the triangle's voxel box whose squared distance
+// to the triangle is within (0.866 * largest voxel side)^2 joins the shell (:458-501).
+__global__ void __launch_bounds__(256) k_vox_raster(SdfParams P) {
+    const int vr = P.vres;
+    const float mvd = fmaxf(P.vox_vx, fmaxf(P.vox_vy, P.vox_vz)) * 0.8660254f;
+    const float lim = mvd * mvd;
+    for (long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x; f < P.nf; f += (long long)gridDim.x * blockDim.x) {
+        float3 a, b, c;
+        if (!load_tri(P, f, a, b, c)) continue;
+        const float mnx = fminf(a.x, fminf(b.x, c.x)), mny = fminf(a.y, fminf(b.y, c.y)), mnz = fminf(a.z, fminf(b.z, c.z));
+        const float mxx = fmaxf(a.x, fmaxf(b.x, c.x)), mxy = fmaxf(a.y, fmaxf(b.y, c.y)), mxz = fmaxf(a.z, fmaxf(b.z, c.z));
+        const int bx0 = bin_coord(mnx, P.ox, P.vox_vx, vr), bx1 = bin_coord(mxx, P.ox, P.vox_vx, vr);
+        const int by0 = bin_coord(mny, P.oy, P.vox_vy, vr), by1 = bin_coord(mxy, P.oy, P.vox_vy, vr);
+        const int bz0 = bin_coord(mnz, P.oz, P.vox_vz, vr), bz1 = bin_coord(mxz, P.oz, P.vox_vz, vr);
+        for (int bz = bz0; bz <= bz1; ++bz)
+            for (int by = by0; by <= by1; ++by)
+                for (int bx = bx0; bx <= bx1; ++bx) {
+                    const float3 q = f3(P.ox + (float)bx * P.vox_vx, P.oy + (float)by * P.vox_vy, P.oz + (float)bz * P.vox_vz);
+                    float3 closest;
+                    if (point_triangle(q, a, b, c, closest) <= lim)
+                        atomicOr(P.vshell + ((long long)bz * vr + by) * P.Wv + (bx >> 5), 1u << (bx & 31));
+                }
+    }
+}
+
+// The shell dilated by one voxel (27-neighbourhood, :503-526), then the flood's inputs: the
+// voxels outside the dilated shell pass the exterior flood, and those of them on the border
+// seed it (init_voxel_exterior_kernel, :561-575). A thread per 32-voxel word.
+__global__ void __launch_bounds__(256) k_vox_dilate(SdfParams P) {
+    const int vr = P.vres;
+    const long long words = (long long)vr * vr * P.Wv;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < words;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const int w = (int)(idx % P.Wv);
+        const long long row = idx / P.Wv;
+        const int y = (int)(row % vr), z = (int)(row / vr);
+        uint32_t dil = 0;
+        for (int zz = max(0, z - 1); zz <= min(vr - 1, z + 1); ++zz)
+            for (int yy = max(0, y - 1); yy <= min(vr - 1, y + 1); ++yy) {
+                const uint32_t* src = P.vshell + ((long long)zz * vr + yy) * P.Wv;
+                const uint32_t cur = src[w];
+                const uint32_t prev = w > 0 ? src[w - 1] : 0u, next = w + 1 < P.Wv ? src[w + 1] : 0u;
+                dil |= cur | (cur << 1) | (cur >> 1) | (prev >> 31) | (next << 31);
+            }
+        const int valid_bits = min(32, vr - 32 * w);
+        const uint32_t valid = valid_bits >= 32 ? 0xffffffffu : ((1u << valid_bits) - 1u);
+        const uint32_t pass = ~dil & valid;
+        uint32_t border;
+        if (y == 0 || y == vr - 1 || z == 0 || z == vr - 1) {
+            border = valid;
+        } else {
+            border = 0;
+            if (w == 0) border |= 1u;
+            if ((vr - 1) >> 5 == w) border |= 1u << ((vr - 1) & 31);
+        }
+        P.vfar[idx] = pass;
+        P.vext[idx] = pass & border;
+    }
+}
+
+// Far grid points -> -10 inside the solid voxels (not exterior), +10 elsewhere
+// (apply_solid_voxel_sign_mask_kernel, :660-690); block per x row.
+__global__ void __launch_bounds__(256) k_vox_sign(SdfParams P, unsigned long long* filled) {
+    const long long rows = (long long)P.ny * P.nz;
+    const int vr = P.vres;
+    unsigned long long cnt = 0;
+    for (long long row = blockIdx.x; row < rows; row += gridDim.x) {
+        const int iy = (int)(row % P.ny), iz = (int)(row / P.ny);
+        float* r = P.out + row * P.nx;
+        const float py = P.oy + (float)iy * P.vy, pz = P.oz + (float)iz * P.vz;
+        const int vby = bin_coord(py, P.oy, P.vox_vy, vr), vbz = bin_coord(pz, P.oz, P.vox_vz, vr);
+        const uint32_t* e = P.vext + ((long long)vbz * vr + vby) * P.Wv;
+        for (int ix = threadIdx.x; ix < P.nx; ix += blockDim.x) {
+            if (r[ix] != kFar) continue;
+            const int vbx = bin_coord(P.ox + (float)ix * P.vx, P.ox, P.vox_vx, vr);
+            const bool exterior = (e[vbx >> 5] >> (vbx & 31)) & 1u;
+            r[ix] = exterior ? 10.0f : -10.0f;
+            cnt += exterior ? 1 : 0;
+        }
+    }
+    if (cnt) atomicAdd(filled, cnt);
+}
+
 unsigned grid_for(long long items, int per_block, int num_sms, int per_sm) {
     long long b = (items + per_block - 1) / per_block;
     const long long cap = (long long)num_sms * per_sm;
@@ -693,6 +778,32 @@ cudaError_t launch_sdf_finish(const SdfParams& P, unsigned long long* filled, fl
         if (it % 2 == 0) k_relax<<<g, 256, 0, s>>>(P, P.out, tmp);
         else             k_relax<<<g, 256, 0, s>>>(P, tmp, P.out);
     }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_vox_raster(const SdfParams& P, int num_sms, cudaStream_t s) {
+    if (P.nf <= 0) return cudaSuccess;
+    k_vox_raster<<<grid_for(P.nf, 256, num_sms, 16), 256, 0, s>>>(P);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_vox_dilate(const SdfParams& P, int num_sms, cudaStream_t s) {
+    k_vox_dilate<<<grid_for((long long)P.vres * P.vres * P.Wv, 256, num_sms, 16), 256, 0, s>>>(P);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_vox_flood(const SdfParams& P, int* changed, int num_sms, cudaStream_t s) {
+    SdfParams V = P;
+    V.W = P.Wv;
+    V.nx = P.vres; V.ny = P.vres; V.nz = P.vres;
+    V.far = P.vfar;
+    V.ext = P.vext;
+    return launch_sdf_flood(V, changed, num_sms, s);
+}
+
+cudaError_t launch_vox_sign(const SdfParams& P, unsigned long long* filled, int num_sms, cudaStream_t s) {
+    const long long rows = (long long)P.ny * P.nz;
+    k_vox_sign<<<grid_for(rows, 1, num_sms, 8), 256, 0, s>>>(P, filled);
     return cudaGetLastError();
 }
 
