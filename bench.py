@@ -243,6 +243,23 @@ def run_batch_workload(args):
         e1.record(stream)
         torch.cuda.synchronize()
         ms_seq = e0.elapsed_time(e1) / reps
+    # the same batch captured in a CUDA graph and replayed (no host synchronisation inside)
+    side = torch.cuda.Stream()
+    with torch.cuda.stream(side):
+        be.batch_graph_create(grids, headroom=0.25)
+        for _ in range(args.warmup):
+            be.batch_graph_launch()
+        torch.cuda.synchronize()
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g0.record(side)
+        for _ in range(args.steps):
+            be.batch_graph_launch()
+        g1.record(side)
+        _, gst = be.batch_graph_finish()
+    torch.cuda.synchronize()
+    ms_graph = g0.elapsed_time(g1) / args.steps
+    same_graph = gst.vertex_count == st.vertex_count and gst.face_count == st.face_count
+    be.batch_graph_destroy()
     line = {
         "metric": "dc_extract_mcells_per_s", "value": round(ncell / (ms_batch / 1e3) / 1e6, 2), "unit": "Mcells/s",
         "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_batch, 4),
@@ -255,6 +272,9 @@ def run_batch_workload(args):
         "mark_tiles": {"waves": waves, "narrow_tile_max_cells": narrow, "autotune_mark_ms": round(tune_ms, 4)},
         "sequential_plain_ms": round(ms_seq, 3) if ms_seq else None,
         "batched_speedup": round(ms_seq / ms_batch, 2) if ms_seq else None,
+        "graph": {"ms_per_step": round(ms_graph, 4), "mcells_per_s": round(ncell / (ms_graph / 1e3) / 1e6, 2),
+                  "same_counts_as_eager": bool(same_graph),
+                  "speedup_vs_sequential": round(ms_seq / ms_graph, 2) if ms_seq else None},
     }
     print(json.dumps(line), flush=True)
     be.close()

@@ -250,6 +250,27 @@ typedef struct {
 int dcb_extract_batch_device(dcb_handle h, const dcb_grid* grids, int n, const dcb_opts* opts,
                              dcb_batch_mesh* out, dcb_stats* stats, void* cuda_stream);
 
+/* ---- a batch pipeline captured in a CUDA graph -------------------------------------------- */
+
+/* Captures the whole batched extraction of `grids` (device grids whose pointers, sizes and
+ * spacing stay fixed; their values may change between launches) into a CUDA graph kept in
+ * the handle. An eager run first sizes the buffers: capacity = active cells * (1 + headroom)
+ * + 1024. The graph has no host synchronisation inside: the kernels read the active count
+ * from device memory; counters and offsets are copied to pinned host memory as the graph's
+ * last nodes. cuda_stream must not be the legacy default stream. The graph holds pointers into
+ * the handle's workspace: any other extraction, backward or autotune call on the handle
+ * invalidates it (launch then returns DCB_ERR_INVALID_ARGUMENT). */
+int dcb_batch_graph_create(dcb_handle h, const dcb_grid* grids, int n, const dcb_opts* opts, double headroom,
+                           void* cuda_stream);
+/* Enqueues one replay on the stream (returns at once). */
+int dcb_batch_graph_launch(dcb_handle h, void* cuda_stream);
+/* Waits for the stream and publishes the last replay's mesh as dcb_extract_batch_device does;
+ * DCB_ERR_TOO_LARGE when the grids had more active cells than the capacity (nothing was
+ * extracted: recreate the graph). */
+int dcb_batch_graph_finish(dcb_handle h, dcb_batch_mesh* out, dcb_stats* stats, void* cuda_stream);
+int dcb_batch_graph_destroy(dcb_handle h);
+
+
 /* Tile autotuner for the mark kernel (no counterpart in the reference): times the mark
  * launches of these device grids (one batch) for every combination of CTAs per resident
  * slot (waves 1, 2, 4, 8) and x-tile width (256-cell tiles for grids at most 0, 256, 512 or

@@ -31,7 +31,8 @@ EXPORTED = (
     "dcb_mark_active_cells_noalloc", "dcb_mesh_to_sdf_device", "dcb_mesh_to_sdf_host",
     "dcb_extract_batch_device", "dcb_backward", "dcb_autotune_mark",
     "dcb_write_obj", "dcb_read_sdf", "dcb_write_sdf", "dcb_extract_upload", "dcb_mesh_to_sdf_device_ex",
-    "dcb_mesh_to_sdf_host_ex")
+    "dcb_mesh_to_sdf_host_ex", "dcb_batch_graph_create", "dcb_batch_graph_launch", "dcb_batch_graph_finish",
+    "dcb_batch_graph_destroy")
 
 
 class DcbGrid(ctypes.Structure):
@@ -139,6 +140,15 @@ def lib():
     L.dcb_extract_device.restype = ctypes.c_int
     L.dcb_extract_host.argtypes = [ctypes.c_void_p, P(DcbGrid), P(DcbOpts), P(DcbMeshHost), P(DcbStats), ctypes.c_void_p]
     L.dcb_extract_host.restype = ctypes.c_int
+    L.dcb_batch_graph_create.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, P(DcbOpts), ctypes.c_double,
+                                         ctypes.c_void_p]
+    L.dcb_batch_graph_create.restype = ctypes.c_int
+    L.dcb_batch_graph_launch.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+    L.dcb_batch_graph_launch.restype = ctypes.c_int
+    L.dcb_batch_graph_finish.argtypes = [ctypes.c_void_p, P(DcbBatchMesh), P(DcbStats), ctypes.c_void_p]
+    L.dcb_batch_graph_finish.restype = ctypes.c_int
+    L.dcb_batch_graph_destroy.argtypes = [ctypes.c_void_p]
+    L.dcb_batch_graph_destroy.restype = ctypes.c_int
     L.dcb_extract_upload.argtypes = [ctypes.c_void_p, P(DcbGrid), P(DcbOpts), P(DcbMeshDev), P(DcbStats), ctypes.c_void_p]
     L.dcb_extract_upload.restype = ctypes.c_int
     L.dcb_copy_mesh_to_host.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]

@@ -308,6 +308,45 @@ class B200DualContouringBackend:
         self._generation += 1
         return md.vertices, md.faces, DualContouringStats.from_c(st)
 
+    def _grid_array(self, grids):
+        arr = (_lib.DcbGrid * len(grids))()
+        for b, (values, dims, spacing, origin) in enumerate(grids):
+            d = DenseSdfGridDevice(*dims, *spacing, *origin, d_values=values)
+            arr[b] = self._grid_c(d, d.pointer())
+        return arr
+
+    def batch_graph_create(self, grids, headroom=0.25, stream=None):
+        """Capture the batched extraction of these device grids into a CUDA graph kept in the
+        handle (their pointers and sizes stay fixed; the values may change between replays).
+        Needs a stream other than the legacy default one (e.g. inside ``torch.cuda.stream``)."""
+        s = _current_stream() if stream is None else stream
+        _lib.check(self._L.dcb_batch_graph_create(self._h, self._grid_array(grids), len(grids),
+                                                  ctypes.byref(self.options.to_c()), float(headroom),
+                                                  ctypes.c_void_p(s)), self._h)
+        self._graph_grids = grids          # the graph reads these tensors' memory
+        self._generation += 1
+
+    def batch_graph_launch(self, stream=None):
+        """Enqueue one replay of the captured batch (returns at once)."""
+        s = _current_stream() if stream is None else stream
+        _lib.check(self._L.dcb_batch_graph_launch(self._h, ctypes.c_void_p(s)), self._h)
+
+    def batch_graph_finish(self, stream=None):
+        """Wait for the replays and publish the last one's mesh like ``extract_batch_ptr``."""
+        st = _lib.DcbStats()
+        out = _lib.DcbBatchMesh()
+        s = _current_stream() if stream is None else stream
+        _lib.check(self._L.dcb_batch_graph_finish(self._h, ctypes.byref(out), ctypes.byref(st), ctypes.c_void_p(s)),
+                   self._h)
+        self._last_nv = out.vertex_count
+        self._last_vpf = out.verts_per_face
+        self._generation += 1
+        return out, DualContouringStats.from_c(st)
+
+    def batch_graph_destroy(self):
+        _lib.check(self._L.dcb_batch_graph_destroy(self._h), self._h)
+        self._graph_grids = None
+
     def extract_batch_ptr(self, grids, stream=None):
         """Batched extraction into the handle's device buffers (valid until the next call);
         returns the raw ``DcbBatchMesh`` and the batch's stats."""
@@ -344,20 +383,27 @@ class B200DualContouringBackend:
         """Batched extraction of ``grids`` = [(CUDA float32 values, dims, spacing, origin)] in one
         pass of the pipeline. Returns ``[(V (nv,3) float32, F (nf,vpf) int32)]`` CUDA tensors per
         grid (faces index their own grid's vertices) and the batch's totals as stats."""
-        import torch
-        n = len(grids)
         s = _current_stream() if stream is None else stream
         out, stats = self.extract_batch_ptr(grids, s)
+        return self._batch_meshes(out, len(grids), grids[0][0].device, s), stats
+
+    def batch_graph_meshes(self, stream=None):
+        """``batch_graph_finish`` with the per-grid tensors of ``extract_batch``."""
+        s = _current_stream() if stream is None else stream
+        out, stats = self.batch_graph_finish(s)
+        grids = self._graph_grids
+        return self._batch_meshes(out, len(grids), grids[0][0].device, s), stats
+
+    def _batch_meshes(self, out, n, dev, s):
+        import torch
         vpf = out.verts_per_face
-        dev = grids[0][0].device
         V = torch.empty((out.vertex_count, 3), dtype=torch.float32, device=dev)
         F = torch.empty((out.face_count, vpf), dtype=torch.int32, device=dev)
         _lib.check(self._L.dcb_copy_mesh_device(self._h, V.data_ptr() if V.numel() else None,
                                                 F.data_ptr() if F.numel() else None, ctypes.c_void_p(s)), self._h)
         vo = [out.vertex_offset[b] for b in range(n + 1)]
         fo = [out.face_offset[b] for b in range(n + 1)]
-        meshes = [(V[vo[b]:vo[b + 1]], F[fo[b]:fo[b + 1]]) for b in range(n)]
-        return meshes, stats
+        return [(V[vo[b]:vo[b + 1]], F[fo[b]:fo[b + 1]]) for b in range(n)]
 
     def extract_tensor(self, values, dims, spacing, origin):
         """torch convenience: CUDA float32 grid in, ``(V (nv,3) float32, F (nf,4) int32,

@@ -63,6 +63,10 @@ struct dcb_context {
         sp_stage, sp_counters;
     void* h_sp_counters = nullptr;    // pinned copy of the sparse counters
     int last_kind = 0;                // last extraction: 0 dense dual contouring, 1 sparse
+    // a captured batch graph (dcb_batch_graph_*): it holds pointers into this workspace, so
+    // every call that may reallocate or rewrite the workspace bumps `gen` and invalidates it
+    unsigned long long gen = 0;
+    struct BatchGraphState* bg = nullptr;
     int cells_per_vertex = 0;         // 1: the vertex -> cell list is `sp_vcell` (two vertices per cell)
     // mesh -> SDF workspace
     DevBuf m_verts, m_faces, m_out, m_tris, m_bin_count, m_bin_start, m_bin_fill, m_bin_scratch, m_bin_tris,
@@ -231,6 +235,31 @@ struct TableView {
 
 size_t align_up(size_t x) { return (x + 255) & ~size_t(255); }
 
+}  // namespace
+
+// A captured batch pipeline (dcb_batch_graph_create): the graph, its layout and options, and
+// the capacity its buffers were sized for.
+struct BatchGraphState {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    BatchLayout L;
+    TableView T;
+    dcb_opts o;
+    long long cap = 0;
+    int n = 0;
+    unsigned long long gen = 0;
+};
+
+namespace {
+
+void destroy_graph(dcb_context* h) {
+    if (!h->bg) return;
+    if (h->bg->exec) cudaGraphExecDestroy(h->bg->exec);
+    if (h->bg->graph) cudaGraphDestroy(h->bg->graph);
+    delete h->bg;
+    h->bg = nullptr;
+}
+
 int upload_table(dcb_context* h, const BatchLayout& L, cudaStream_t s, TableView& T) {
     const int n = (int)L.slots.size();
     const size_t o_slots = 0;
@@ -287,11 +316,10 @@ int launch_marks(dcb_context* h, const BatchLayout& L, const TableView& T, cudaS
 // Runs the pipeline on n device-resident grids as one batch (a single extraction is n = 1);
 // ev[1] must already be recorded. Vertices are numbered over the whole batch while running;
 // for n > 1 the faces are rebased to their own grid's vertices at the end.
-int run_batch(dcb_context* h, const dcb_grid* in, int n, const dcb_opts* o, cudaStream_t s, dcb_stats* st) {
-    BatchLayout L;
+// Layout, table upload and the buffers whose sizes do not depend on the active count.
+int batch_prepare(dcb_context* h, const dcb_grid* in, int n, cudaStream_t s, BatchLayout& L, TableView& T) {
     int rc = layout_batch(h, in, n, L);
     if (rc != DCB_OK) return rc;
-    TableView T;
     rc = upload_table(h, L, s, T);
     if (rc != DCB_OK) return rc;
     const long long nseg = L.nseg, ncol = L.ncol;
@@ -308,28 +336,59 @@ int run_batch(dcb_context* h, const dcb_grid* in, int n, const dcb_opts* o, cuda
     DCB_TRY(h, ensure(h->partials, sizeof(uint32_t) * std::max(1LL, plen)), "alloc scan");
     if (!h->h_counters) DCB_TRY(h, cudaMallocHost(&h->h_counters, sizeof(Counters)), "alloc pinned counters");
     DCB_TRY(h, ensure_host(h->h_offsets, h->h_offsets_bytes, 2 * sizeof(unsigned long long) * (n + 1)), "alloc pinned offsets");
-    unsigned long long* h_vert_off = reinterpret_cast<unsigned long long*>(h->h_offsets);
-    unsigned long long* h_face_off = h_vert_off + (n + 1);
 
+
+    return DCB_OK;
+}
+
+// The buffers for up to `cap` active cells.
+int batch_alloc(dcb_context* h, int n, long long cap, const dcb_opts* o, TableView& T) {
+    DCB_TRY(h, ensure(h->list, sizeof(uint64_t) * cap), "alloc active list");
+    DCB_TRY(h, ensure(h->V, sizeof(float) * 3 * cap), "alloc vertices");
+    DCB_TRY(h, ensure(h->fmask, cap), "alloc face masks");
+    DCB_TRY(h, ensure(h->vclass, cap), "alloc vertex classes");
+    DCB_TRY(h, ensure(h->esc_list, sizeof(uint32_t) * cap), "alloc escalation list");
+    DCB_TRY(h, ensure(h->hard_list, sizeof(uint32_t) * cap), "alloc hard list");
+    DCB_TRY(h, ensure(h->hard_data, sizeof(float4) * 3 * cap), "alloc hard data");
+    DCB_TRY(h, ensure(h->stage_quad, sizeof(int4) * 3 * cap), "alloc face staging");
+    DCB_TRY(h, ensure(h->stage_key, sizeof(uint2) * 3 * cap), "alloc face keys");
+    DCB_TRY(h, ensure(h->faces, sizeof(int4) * 3 * cap), "alloc faces");
+    DCB_TRY(h, ensure(h->v64_index, sizeof(int) * cap), "alloc fp64 index");
+    if (n > 1) {
+        DCB_TRY(h, ensure(h->cell_slot, sizeof(uint32_t) * cap), "alloc vertex grids");
+        T.B.cell_slot = as<uint32_t>(h->cell_slot);
+    }
+    // Exact upper bounds: at most 3 faces per owner cell, one FP64 vertex per cell.
+    const long long wind_cap = std::min(0x7fffffffLL, 3 * cap);
+    const long long v64_cap = cap;
+    DCB_TRY(h, ensure(h->wind_items, sizeof(uint4) * wind_cap), "alloc winding list");
+    DCB_TRY(h, ensure(h->v64_cells, sizeof(uint32_t) * v64_cap), "alloc fp64 cells");
+    DCB_TRY(h, ensure(h->V64, sizeof(double) * 3 * v64_cap), "alloc fp64 vertices");
+    if (o->emit_triangles) {
+        DCB_TRY(h, ensure(h->tris, sizeof(int) * 6 * 3 * cap), "alloc triangles");
+        DCB_TRY(h, ensure(h->tri_items, sizeof(uint32_t) * wind_cap), "alloc triangle list");
+    }
+    return DCB_OK;
+}
+
+// The mark launches, the segment scan (total active count into the counters) and the
+// first vertex of every grid.
+int batch_mark(dcb_context* h, const BatchLayout& L, const TableView& T, cudaStream_t s, bool events) {
     Counters* dc = as<Counters>(h->counters);
-    Counters* hc = reinterpret_cast<Counters*>(h->h_counters);
-
-    // 1) mark: active bits + per-segment counts; scan -> segment starts and the total.
     DCB_TRY(h, cudaMemsetAsync(h->counters.p, 0, sizeof(Counters), s), "memset counters");
-    rc = launch_marks(h, L, T, s);
+    int rc = launch_marks(h, L, T, s);
     if (rc != DCB_OK) return rc;
-    DCB_TRY(h, cudaEventRecord(h->ev[6], s), "event");
-    DCB_TRY(h, launch_scan(as<uint32_t>(h->seg_count), nseg, as<uint32_t>(h->partials), as<uint32_t>(h->seg_start),
+    if (events) DCB_TRY(h, cudaEventRecord(h->ev[6], s), "event");
+    DCB_TRY(h, launch_scan(as<uint32_t>(h->seg_count), L.nseg, as<uint32_t>(h->partials), as<uint32_t>(h->seg_start),
                            &dc->total_active, s), "launch segment scan");
     DCB_TRY(h, launch_vert_offsets(T.B, as<uint32_t>(h->seg_start), &dc->total_active, T.vert_off, s), "vertex offsets");
-    DCB_TRY(h, cudaEventRecord(h->ev[2], s), "event");
-    DCB_TRY(h, cudaMemcpyAsync(hc, dc, sizeof(Counters), cudaMemcpyDeviceToHost, s), "read count");
-    DCB_TRY(h, cudaMemcpyAsync(h_vert_off, T.vert_off, sizeof(unsigned long long) * (n + 1), cudaMemcpyDeviceToHost, s),
-            "read vertex offsets");
-    DCB_TRY(h, cudaStreamSynchronize(s), "mark");
-    const long long nv = (long long)hc->total_active;
-    if (nv >= 0x7fffffffLL) return fail(h, DCB_ERR_TOO_LARGE, "more than 2^31-1 vertices");
+    if (events) DCB_TRY(h, cudaEventRecord(h->ev[2], s), "event");
+    return DCB_OK;
+}
 
+// Handle state of a batch with nv vertices (the per-grid first vertices are in h_offsets).
+void batch_state(dcb_context* h, const BatchLayout& L, int n, const dcb_opts* o, long long nv) {
+    const unsigned long long* h_vert_off = reinterpret_cast<const unsigned long long*>(h->h_offsets);
     h->nv = nv;
     h->nf = 0;
     h->vpf = o->emit_triangles ? 3 : 4;
@@ -344,40 +403,21 @@ int run_batch(dcb_context* h, const dcb_grid* in, int n, const dcb_opts* o, cuda
     h->face_offsets.assign(n + 1, 0);
     for (int b = 0; b < n; ++b) { h->batch_cx[b] = L.slots[b].g.cx; h->batch_cy[b] = L.slots[b].g.cy; }
     for (int b = 0; b <= n; ++b) h->vert_offsets[b] = (int64_t)h_vert_off[b];
-    if (st) {
-        st->nx = L.slots[0].g.nx; st->ny = L.slots[0].g.ny; st->nz = L.slots[0].g.nz;
-        st->total_cells = L.ncell; st->active_cells = nv; st->vertex_count = nv;
-    }
-    if (nv == 0) {
-        DCB_TRY(h, cudaEventRecord(h->ev[3], s), "event");
-        DCB_TRY(h, cudaEventRecord(h->ev[4], s), "event");
-        return DCB_OK;
-    }
+}
 
-    DCB_TRY(h, ensure(h->list, sizeof(uint64_t) * nv), "alloc active list");
-    DCB_TRY(h, ensure(h->V, sizeof(float) * 3 * nv), "alloc vertices");
-    DCB_TRY(h, ensure(h->fmask, nv), "alloc face masks");
-    DCB_TRY(h, ensure(h->vclass, nv), "alloc vertex classes");
-    DCB_TRY(h, ensure(h->esc_list, sizeof(uint32_t) * nv), "alloc escalation list");
-    DCB_TRY(h, ensure(h->hard_list, sizeof(uint32_t) * nv), "alloc hard list");
-    DCB_TRY(h, ensure(h->hard_data, sizeof(float4) * 3 * nv), "alloc hard data");
-    DCB_TRY(h, ensure(h->stage_quad, sizeof(int4) * 3 * nv), "alloc face staging");
-    DCB_TRY(h, ensure(h->stage_key, sizeof(uint2) * 3 * nv), "alloc face keys");
-    DCB_TRY(h, ensure(h->faces, sizeof(int4) * 3 * nv), "alloc faces");
-    DCB_TRY(h, ensure(h->v64_index, sizeof(int) * nv), "alloc fp64 index");
-    if (n > 1) {
-        DCB_TRY(h, ensure(h->cell_slot, sizeof(uint32_t) * nv), "alloc vertex grids");
-        T.B.cell_slot = as<uint32_t>(h->cell_slot);
-    }
-    // Exact upper bounds: at most 3 faces per owner cell, one FP64 vertex per cell.
-    const long long wind_cap = std::min(0x7fffffffLL, 3 * nv);
-    const long long v64_cap = nv;
-    DCB_TRY(h, ensure(h->wind_items, sizeof(uint4) * wind_cap), "alloc winding list");
-    DCB_TRY(h, ensure(h->v64_cells, sizeof(uint32_t) * v64_cap), "alloc fp64 cells");
-    DCB_TRY(h, ensure(h->V64, sizeof(double) * 3 * v64_cap), "alloc fp64 vertices");
+// Everything after the mark for up to `cap` active cells: ranks and list, vertices, faces.
+// With `live` (a device count, as in a captured graph) the kernels take the active count from
+// there, bounded by cap; otherwise it is cap.
+int batch_rest(dcb_context* h, const BatchLayout& L, TableView& T, const dcb_opts* o, cudaStream_t s, long long cap,
+               const unsigned long long* live, bool events) {
+    const int n = (int)L.slots.size();
+    const long long nseg = L.nseg, ncol = L.ncol;
+    Counters* dc = as<Counters>(h->counters);
+    const long long wind_cap = std::min(0x7fffffffLL, 3 * cap);
+    const long long v64_cap = cap;
     DCB_TRY(h, cudaMemsetAsync(h->col_count.p, 0, sizeof(uint32_t) * ncol, s), "memset");
     DCB_TRY(h, cudaMemsetAsync(h->col_fill.p, 0, sizeof(uint32_t) * ncol, s), "memset");
-    DCB_TRY(h, cudaMemsetAsync(h->v64_index.p, 0xff, sizeof(int) * nv, s), "memset");
+    DCB_TRY(h, cudaMemsetAsync(h->v64_index.p, 0xff, sizeof(int) * cap, s), "memset");
 
     // 2) ranks + list, QEF with fused edge normals (rank-1 fast path, Jacobi list, FP64).
     ExpandParams xp;
@@ -385,9 +425,10 @@ int run_batch(dcb_context* h, const dcb_grid* in, int n, const dcb_opts* o, cuda
     xp.seg_start = as<uint32_t>(h->seg_start); xp.super = as<uint32_t>(h->super); xp.list = as<uint64_t>(h->list);
     xp.cell_slot = n > 1 ? as<uint32_t>(h->cell_slot) : nullptr;
     xp.B.cell_slot = nullptr;                      // expand finds grids by segment
+    xp.list_cap = cap;
     DCB_TRY(h, launch_expand(xp, h->num_sms, s), "launch expand");
     QefParams qp;
-    qp.B = T.B; qp.list = xp.list; qp.nactive = nv; qp.V = as<float>(h->V); qp.vclass = as<uint8_t>(h->vclass);
+    qp.B = T.B; qp.list = xp.list; qp.nactive = cap; qp.live = live; qp.V = as<float>(h->V); qp.vclass = as<uint8_t>(h->vclass);
     qp.fmask = as<uint8_t>(h->fmask); qp.col_count = as<uint32_t>(h->col_count);
     qp.esc_list = as<uint32_t>(h->esc_list); qp.esc_count = &dc->esc_count;
     qp.hard_list = as<uint32_t>(h->hard_list); qp.hard_data = as<float4>(h->hard_data); qp.hard_count = &dc->hard_count;
@@ -395,12 +436,12 @@ int run_batch(dcb_context* h, const dcb_grid* in, int n, const dcb_opts* o, cuda
     qp.thr = (float)o->svd_threshold; qp.band = (float)o->fp64_threshold_band;
     qp.cond_max = (float)std::min(o->fp64_escalation_cond, 3.0e38); qp.force64 = o->force_fp64;
     DCB_TRY(h, launch_cell_qef(qp, h->num_sms, s), "launch qef");
-    DCB_TRY(h, launch_cell_jacobi(qp, nv, h->num_sms, s), "launch jacobi");
+    DCB_TRY(h, launch_cell_jacobi(qp, cap, h->num_sms, s), "launch jacobi");
     Vertex64Params v64;
-    v64.B = T.B; v64.list = xp.list; v64.cells = qp.esc_list; v64.count = &dc->esc_count; v64.cap = (unsigned int)nv;
+    v64.B = T.B; v64.list = xp.list; v64.cells = qp.esc_list; v64.count = &dc->esc_count; v64.cap = (unsigned int)cap;
     v64.Vf = qp.V; v64.vclass = qp.vclass; v64.V64 = nullptr; v64.thr = o->svd_threshold;
-    DCB_TRY(h, launch_vertex_fp64(v64, nv, h->num_sms, s), "launch vertex fp64");
-    DCB_TRY(h, cudaEventRecord(h->ev[3], s), "event");
+    DCB_TRY(h, launch_vertex_fp64(v64, cap, h->num_sms, s), "launch vertex fp64");
+    if (events) DCB_TRY(h, cudaEventRecord(h->ev[3], s), "event");
 
     // 3) faces: column scan, scatter with FP32 winding, FP64 re-decisions, in-column order.
     DCB_TRY(h, launch_scan(as<uint32_t>(h->col_count), ncol, as<uint32_t>(h->partials),
@@ -408,7 +449,7 @@ int run_batch(dcb_context* h, const dcb_grid* in, int n, const dcb_opts* o, cuda
     if (n > 1)
         DCB_TRY(h, launch_face_offsets(T.B, as<uint32_t>(h->col_start), &dc->face_total, T.face_off, s), "face offsets");
     FaceParams fp;
-    fp.B = T.B; fp.list = xp.list; fp.nactive = nv; fp.fmask = qp.fmask; fp.V = qp.V; fp.vclass = qp.vclass;
+    fp.B = T.B; fp.list = xp.list; fp.nactive = cap; fp.live = live; fp.fmask = qp.fmask; fp.V = qp.V; fp.vclass = qp.vclass;
     fp.bits = xp.bits; fp.super = xp.super;
     fp.col_start = as<uint32_t>(h->col_start); fp.col_count = as<uint32_t>(h->col_count);
     fp.col_fill = as<uint32_t>(h->col_fill);
@@ -429,12 +470,10 @@ int run_batch(dcb_context* h, const dcb_grid* in, int n, const dcb_opts* o, cuda
     wp.quads = fp.stage_quad; wp.v64_index = fp.v64_index; wp.V64 = w64.V64; wp.err = &dc->err;
     DCB_TRY(h, launch_winding_fp64(wp, wind_cap, h->num_sms, s), "launch winding fp64");
     DCB_TRY(h, launch_face_order(fp.stage_quad, fp.stage_key, fp.col_start, fp.col_count, &dc->face_total,
-                                 as<int4>(h->faces), 3 * nv, h->num_sms, s), "launch face order");
+                                 as<int4>(h->faces), 3 * cap, h->num_sms, s), "launch face order");
     if (o->emit_triangles) {
         // 4) quads -> triangles; FP64 vertices for the quads FP32 cannot orient (the winding
         // pass's FP64 vertices are recomputed too: same values, and few).
-        DCB_TRY(h, ensure(h->tris, sizeof(int) * 6 * 3 * nv), "alloc triangles");
-        DCB_TRY(h, ensure(h->tri_items, sizeof(uint32_t) * wind_cap), "alloc triangle list");
         TriParams tp;
         tp.B = T.B;
         tp.quads = as<int4>(h->faces); tp.nquads = &dc->face_total; tp.V = qp.V; tp.vclass = qp.vclass;
@@ -442,7 +481,7 @@ int run_batch(dcb_context* h, const dcb_grid* in, int n, const dcb_opts* o, cuda
         tp.item_count = &dc->tri_count; tp.item_cap = (unsigned int)wind_cap;
         tp.v64_index = fp.v64_index; tp.v64_cells = fp.v64_cells; tp.v64_count = fp.v64_count;
         tp.v64_cap = fp.v64_cap; tp.err = &dc->err;
-        DCB_TRY(h, launch_triangulate(tp, 3 * nv, h->num_sms, s), "launch triangulate");
+        DCB_TRY(h, launch_triangulate(tp, 3 * cap, h->num_sms, s), "launch triangulate");
         DCB_TRY(h, launch_vertex_fp64(w64, v64_cap, h->num_sms, s), "launch fp64 vertices for triangles");
         Tri64Params t64;
         t64.quads = tp.quads; t64.items = tp.items; t64.count = tp.item_count; t64.cap = tp.item_cap;
@@ -452,15 +491,19 @@ int run_batch(dcb_context* h, const dcb_grid* in, int n, const dcb_opts* o, cuda
     if (n > 1) {
         // 5) faces refer to vertices of their own grid
         if (o->emit_triangles)
-            DCB_TRY(h, launch_localize_faces(T.vert_off, T.face_off, n, as<int>(h->tris), 3, 6 * nv, h->num_sms, s), "localize");
+            DCB_TRY(h, launch_localize_faces(T.vert_off, T.face_off, n, as<int>(h->tris), 3, 6 * cap, h->num_sms, s), "localize");
         else
-            DCB_TRY(h, launch_localize_faces(T.vert_off, T.face_off, n, as<int>(h->faces), 4, 3 * nv, h->num_sms, s), "localize");
-        DCB_TRY(h, cudaMemcpyAsync(h_face_off, T.face_off, sizeof(unsigned long long) * (n + 1),
+            DCB_TRY(h, launch_localize_faces(T.vert_off, T.face_off, n, as<int>(h->faces), 4, 3 * cap, h->num_sms, s), "localize");
+        DCB_TRY(h, cudaMemcpyAsync(reinterpret_cast<unsigned long long*>(h->h_offsets) + (n + 1), T.face_off, sizeof(unsigned long long) * (n + 1),
                                    cudaMemcpyDeviceToHost, s), "read face offsets");
     }
-    DCB_TRY(h, cudaEventRecord(h->ev[4], s), "event");
-    DCB_TRY(h, cudaMemcpyAsync(hc, dc, sizeof(Counters), cudaMemcpyDeviceToHost, s), "read counters");
-    DCB_TRY(h, cudaStreamSynchronize(s), "pipeline");
+    return DCB_OK;
+}
+
+// After the last copy of the counters has arrived: errors, face counts and offsets, stats.
+int batch_finish(dcb_context* h, int n, const dcb_opts* o, dcb_stats* st) {
+    const Counters* hc = reinterpret_cast<const Counters*>(h->h_counters);
+    const unsigned long long* h_face_off = reinterpret_cast<const unsigned long long*>(h->h_offsets) + (n + 1);
     if (hc->err) {
         return fail(h, hc->err == kErrTimeout ? DCB_ERR_TIMEOUT : DCB_ERR_INTERNAL,
                     hc->err == kErrOverflow ? "FP64 work list overflow" : "device error flag set");
@@ -479,6 +522,46 @@ int run_batch(dcb_context* h, const dcb_grid* in, int n, const dcb_opts* o, cuda
         st->clamp_count = 0;
     }
     return DCB_OK;
+}
+
+int run_batch(dcb_context* h, const dcb_grid* in, int n, const dcb_opts* o, cudaStream_t s, dcb_stats* st) {
+    ++h->gen;
+    BatchLayout L;
+    TableView T;
+    int rc = batch_prepare(h, in, n, s, L, T);
+    if (rc != DCB_OK) return rc;
+    Counters* dc = as<Counters>(h->counters);
+    Counters* hc = reinterpret_cast<Counters*>(h->h_counters);
+    unsigned long long* h_vert_off = reinterpret_cast<unsigned long long*>(h->h_offsets);
+
+    // 1) mark: active bits + per-segment counts; scan -> segment starts and the total.
+    rc = batch_mark(h, L, T, s, true);
+    if (rc != DCB_OK) return rc;
+    DCB_TRY(h, cudaMemcpyAsync(hc, dc, sizeof(Counters), cudaMemcpyDeviceToHost, s), "read count");
+    DCB_TRY(h, cudaMemcpyAsync(h_vert_off, T.vert_off, sizeof(unsigned long long) * (n + 1), cudaMemcpyDeviceToHost, s),
+            "read vertex offsets");
+    DCB_TRY(h, cudaStreamSynchronize(s), "mark");
+    const long long nv = (long long)hc->total_active;
+    if (nv >= 0x7fffffffLL) return fail(h, DCB_ERR_TOO_LARGE, "more than 2^31-1 vertices");
+    batch_state(h, L, n, o, nv);
+    if (st) {
+        st->nx = L.slots[0].g.nx; st->ny = L.slots[0].g.ny; st->nz = L.slots[0].g.nz;
+        st->total_cells = L.ncell; st->active_cells = nv; st->vertex_count = nv;
+    }
+    if (nv == 0) {
+        DCB_TRY(h, cudaEventRecord(h->ev[3], s), "event");
+        DCB_TRY(h, cudaEventRecord(h->ev[4], s), "event");
+        return DCB_OK;
+    }
+    rc = batch_alloc(h, n, nv, o, T);
+    if (rc != DCB_OK) return rc;
+    // 2) ranks + list, vertices, faces
+    rc = batch_rest(h, L, T, o, s, nv, nullptr, true);
+    if (rc != DCB_OK) return rc;
+    DCB_TRY(h, cudaEventRecord(h->ev[4], s), "event");
+    DCB_TRY(h, cudaMemcpyAsync(hc, dc, sizeof(Counters), cudaMemcpyDeviceToHost, s), "read counters");
+    DCB_TRY(h, cudaStreamSynchronize(s), "pipeline");
+    return batch_finish(h, n, o, st);
 }
 
 int run_pipeline(dcb_context* h, const dcb_grid* in, const dcb_opts* o, cudaStream_t s, dcb_stats* st) {
@@ -572,6 +655,7 @@ int run_ours(dcb_context* h, const dcb_grid* in, const dcb_opts* o, cudaStream_t
 // multi-vertex variant, their scan and placement), faces into per-cell slots, scan,
 // compaction. Two host read-backs: the active-cell count and the vertex and face totals.
 int run_sparse(dcb_context* h, const dcb_grid* in, const dcb_opts* o, cudaStream_t s, dcb_stats* st) {
+    ++h->gen;
     if (o->emit_triangles) return fail(h, DCB_ERR_NOT_SUPPORTED, "the sparse backends emit quads only");
     if (o->brick_size < 1 || o->brick_size > 4096) return fail(h, DCB_ERR_INVALID_ARGUMENT, "brick_size must be in [1, 4096]");
     if (o->normal_mode < 0 || o->normal_mode > 2) return fail(h, DCB_ERR_INVALID_ARGUMENT, "unknown normal_mode");
@@ -960,6 +1044,7 @@ int dcb_destroy(dcb_handle h) {
     if (h->h_counters) cudaFreeHost(h->h_counters);
     if (h->h_sdf_counters) cudaFreeHost(h->h_sdf_counters);
     if (h->h_sp_counters) cudaFreeHost(h->h_sp_counters);
+    destroy_graph(h);
     if (h->h_table) cudaFreeHost(h->h_table);
     if (h->h_offsets) cudaFreeHost(h->h_offsets);
     if (h->hV) cudaFreeHost(h->hV);
@@ -1075,6 +1160,115 @@ int dcb_extract_host(dcb_handle h, const dcb_grid* grid, const dcb_opts* opts, d
     return DCB_OK;
 }
 
+int dcb_batch_graph_create(dcb_handle h, const dcb_grid* grids, int n, const dcb_opts* opts, double headroom,
+                           void* cuda_stream) {
+    if (!h) return DCB_ERR_INVALID_ARGUMENT;
+    if (!grids || n < 1) return fail(h, DCB_ERR_INVALID_ARGUMENT, "empty batch");
+    for (int b = 0; b < n; ++b) {
+        const int rc = validate(h, grids + b);
+        if (rc != DCB_OK) return rc;
+    }
+    dcb_opts def;
+    dcb_default_opts(&def);
+    const dcb_opts* o = opts ? opts : &def;
+    if (o->method != DCB_METHOD_DUAL_CONTOURING) return fail(h, DCB_ERR_NOT_SUPPORTED, "batches run dual contouring only");
+    if (!(o->svd_threshold >= 0.0)) return fail(h, DCB_ERR_INVALID_ARGUMENT, "svd_threshold must be >= 0");
+    if (!(headroom >= 0.0) || headroom > 100.0) return fail(h, DCB_ERR_INVALID_ARGUMENT, "headroom must be in [0, 100]");
+    if (cudaSetDevice(h->device) != cudaSuccess) { cudaGetLastError(); return fail(h, DCB_ERR_CUDA, "set device"); }
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(cuda_stream);
+    if (s == 0) return fail(h, DCB_ERR_INVALID_ARGUMENT, "capture needs a stream other than the legacy default stream");
+    destroy_graph(h);
+    // an eager run sizes the capacity and leaves every size-independent buffer in place
+    DCB_TRY(h, cudaEventRecord(h->ev[1], s), "event");
+    int rc = run_batch(h, grids, n, o, s, nullptr);
+    if (rc != DCB_OK) return rc;
+    long long cap = (long long)((double)h->nv * (1.0 + headroom)) + 1024;
+    cap = std::min(cap, 0x7ffffffeLL);
+    BatchGraphState* g = new BatchGraphState();
+    g->n = n; g->o = *o; g->cap = cap;
+    rc = batch_prepare(h, grids, n, s, g->L, g->T);
+    if (rc == DCB_OK) rc = batch_alloc(h, n, cap, o, g->T);
+    if (rc == DCB_OK) {
+        cudaError_t e = cudaStreamSynchronize(s);            // table upload done before the capture
+        if (e != cudaSuccess) rc = cuda_fail(h, e, "prepare graph");
+    }
+    if (rc != DCB_OK) { delete g; return rc; }
+    Counters* dc = as<Counters>(h->counters);
+    cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) { delete g; return cuda_fail(h, e, "begin capture"); }
+    rc = batch_mark(h, g->L, g->T, s, false);
+    if (rc == DCB_OK) rc = batch_rest(h, g->L, g->T, o, s, cap, &dc->total_active, false);
+    if (rc == DCB_OK) {
+        e = cudaMemcpyAsync(h->h_counters, dc, sizeof(Counters), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(h->h_offsets, g->T.vert_off, sizeof(unsigned long long) * (n + 1),
+                                cudaMemcpyDeviceToHost, s);
+        if (e != cudaSuccess) rc = cuda_fail(h, e, "capture read-back");
+    }
+    const cudaError_t ee = cudaStreamEndCapture(s, &g->graph);
+    if (rc == DCB_OK && ee != cudaSuccess) rc = cuda_fail(h, ee, "end capture");
+    if (rc == DCB_OK) {
+        e = cudaGraphInstantiate(&g->exec, g->graph, 0);
+        if (e != cudaSuccess) rc = cuda_fail(h, e, "instantiate graph");
+    }
+    if (rc != DCB_OK) {
+        cudaGetLastError();
+        if (g->graph) cudaGraphDestroy(g->graph);
+        delete g;
+        return rc;
+    }
+    g->gen = h->gen;
+    h->bg = g;
+    return DCB_OK;
+}
+
+int dcb_batch_graph_launch(dcb_handle h, void* cuda_stream) {
+    if (!h) return DCB_ERR_INVALID_ARGUMENT;
+    if (!h->bg) return fail(h, DCB_ERR_INVALID_ARGUMENT, "no batch graph: call dcb_batch_graph_create");
+    if (h->bg->gen != h->gen)
+        return fail(h, DCB_ERR_INVALID_ARGUMENT, "the handle was used for another call since the graph was captured");
+    if (cudaSetDevice(h->device) != cudaSuccess) { cudaGetLastError(); return fail(h, DCB_ERR_CUDA, "set device"); }
+    DCB_TRY(h, cudaGraphLaunch(h->bg->exec, reinterpret_cast<cudaStream_t>(cuda_stream)), "launch graph");
+    return DCB_OK;
+}
+
+int dcb_batch_graph_finish(dcb_handle h, dcb_batch_mesh* out, dcb_stats* stats, void* cuda_stream) {
+    if (!h) return DCB_ERR_INVALID_ARGUMENT;
+    if (!h->bg) return fail(h, DCB_ERR_INVALID_ARGUMENT, "no batch graph: call dcb_batch_graph_create");
+    if (cudaSetDevice(h->device) != cudaSuccess) { cudaGetLastError(); return fail(h, DCB_ERR_CUDA, "set device"); }
+    DCB_TRY(h, cudaStreamSynchronize(reinterpret_cast<cudaStream_t>(cuda_stream)), "graph");
+    BatchGraphState* g = h->bg;
+    const Counters* hc = reinterpret_cast<const Counters*>(h->h_counters);
+    const long long nv = (long long)hc->total_active;
+    if (nv > g->cap)
+        return fail(h, DCB_ERR_TOO_LARGE, "the grids now have more active cells than the graph was built for; "
+                                          "recreate it");
+    if (stats) std::memset(stats, 0, sizeof(*stats));
+    batch_state(h, g->L, g->n, &g->o, nv);
+    if (stats) {
+        stats->nx = g->L.slots[0].g.nx; stats->ny = g->L.slots[0].g.ny; stats->nz = g->L.slots[0].g.nz;
+        stats->total_cells = g->L.ncell; stats->active_cells = nv; stats->vertex_count = nv;
+    }
+    const int rc = batch_finish(h, g->n, &g->o, stats);
+    if (rc != DCB_OK) return rc;
+    if (out) {
+        out->vertex_count = h->nv;
+        out->face_count = h->nf;
+        out->verts_per_face = h->vpf;
+        out->vertices = as<float>(h->V);
+        out->faces = face_ptr(h);
+        out->vertex_offset = h->vert_offsets.data();
+        out->face_offset = h->face_offsets.data();
+    }
+    return DCB_OK;
+}
+
+int dcb_batch_graph_destroy(dcb_handle h) {
+    if (!h) return DCB_ERR_INVALID_ARGUMENT;
+    destroy_graph(h);
+    return DCB_OK;
+}
+
 int dcb_extract_upload(dcb_handle h, const dcb_grid* grid, const dcb_opts* opts, dcb_mesh_dev* out,
                        dcb_stats* stats, void* cuda_stream) {
     int rc = validate(h, grid);
@@ -1150,6 +1344,7 @@ int dcb_copy_cells_to_host(dcb_handle h, int64_t* cell_linear_index, void* cuda_
 
 int dcb_autotune_mark(dcb_handle h, const dcb_grid* grids, int n, int* waves_out, int* narrow_cells_out,
                       float* best_ms_out, void* cuda_stream) {
+    if (h) ++h->gen;                        // reuses the extraction workspace
     if (!h) return DCB_ERR_INVALID_ARGUMENT;
     if (!grids || n < 1) return fail(h, DCB_ERR_INVALID_ARGUMENT, "empty batch");
     for (int b = 0; b < n; ++b) {
@@ -1212,6 +1407,7 @@ int dcb_backward(dcb_handle h, const dcb_grid* grid, const dcb_opts* opts, const
     if (h->last_kind != 0 || h->batch_n != 1 || h->cx != grid->nx - 1 || h->cy != grid->ny - 1 || h->cz != grid->nz - 1)
         return fail(h, DCB_ERR_INVALID_ARGUMENT, "backward needs the grid of the last single-grid extraction");
     if (!dL_dgrid || (h->nv > 0 && !dL_dvertices)) return fail(h, DCB_ERR_INVALID_ARGUMENT, "null gradient array");
+    ++h->gen;
     if (cudaSetDevice(h->device) != cudaSuccess) { cudaGetLastError(); return fail(h, DCB_ERR_CUDA, "set device"); }
     cudaStream_t s = reinterpret_cast<cudaStream_t>(cuda_stream);
     const size_t npts = (size_t)grid->nx * grid->ny * grid->nz;

@@ -234,14 +234,17 @@ k_face_scatter(const __grid_constant__ FaceParams P) {
     __shared__ uint8_t s_item[kFaceThreads / 32][96];
     const int lane = threadIdx.x & 31, wb = threadIdx.x >> 5;
     const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x - lane); base < P.nactive;
+    // a captured graph whose live count exceeds the capacity it was built for does nothing
+    // (the host reports the overflow after the replay)
+    const long long nact = P.live ? ((long long)*P.live > P.nactive ? 0 : (long long)*P.live) : P.nactive;
+    for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x - lane); base < nact;
          base += stride) {                                                // warp-uniform
         const long long rr = base + lane;
         uint32_t fm = 0;
         int gi = 0, i = 0, j = 0, k = 0;
         float3 g0 = make_float3(0.f, 0.f, 0.f);
         uint32_t r_k1 = 0xffffffffu, r_j1 = 0xffffffffu, r_jk = 0xffffffffu;
-        if (rr < P.nactive) fm = P.fmask[rr];
+        if (rr < nact) fm = P.fmask[rr];
         if (fm) {
             gi = ONE ? 0 : slot_of_rank(P.B, (unsigned long long)rr);
             const GridSlot& S = slot_ref<ONE>(P.B, gi);

@@ -86,6 +86,7 @@ struct ExpandParams {
     uint32_t* super;               // all grids' super ranks
     uint64_t* list;                // [active] packed cells, grid-local coordinates
     uint32_t* cell_slot;           // [active] grid of every vertex (batches only; may be null)
+    long long list_cap;            // entries of list / cell_slot; <= 0: sized for every active cell
 };
 cudaError_t launch_expand(const ExpandParams& P, int num_sms, cudaStream_t s);
 
@@ -106,7 +107,9 @@ enum VertexClass : uint8_t { kVcRank1 = 0, kVcJacobi = 1, kVcFp64 = 2 };
 struct QefParams {
     BatchTable B;
     const uint64_t* list;
-    long long nactive;
+    long long nactive;             // active cells (capacity when live is set)
+    const unsigned long long* live; // device count of active cells (a captured graph; above
+                                    // nactive, nothing is processed), or null
     float* V;
     uint8_t* vclass;                // [active] VertexClass
     uint8_t* fmask;                 // bit a: cell owns a face on its min-corner edge a
@@ -157,7 +160,9 @@ long long scan_partials_len(long long n);
 struct FaceParams {
     BatchTable B;
     const uint64_t* list;
-    long long nactive;
+    long long nactive;             // active cells (capacity when live is set)
+    const unsigned long long* live; // device count of active cells (a captured graph; above
+                                    // nactive, nothing is processed), or null
     const uint8_t* fmask;
     const float* V;
     const uint8_t* vclass;

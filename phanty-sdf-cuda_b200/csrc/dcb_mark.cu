@@ -195,8 +195,10 @@ k_expand_ranks(const __grid_constant__ ExpandParams P) {
                     while (m) {
                         const int bb = __ffs(m) - 1;
                         m &= m - 1;
-                        P.list[rank] = pack_cell(32 * w + bb, j, k);
-                        if (!ONE && P.cell_slot) P.cell_slot[rank] = (uint32_t)my_slot;
+                        if (P.list_cap <= 0 || (long long)rank < P.list_cap) {
+                            P.list[rank] = pack_cell(32 * w + bb, j, k);
+                            if (!ONE && P.cell_slot) P.cell_slot[rank] = (uint32_t)my_slot;
+                        }
                         ++rank;
                     }
                 }
@@ -242,6 +244,7 @@ k_expand_ranks(const __grid_constant__ ExpandParams P) {
                 const uint32_t word = __shfl_sync(0xffffffffu, act, lo);
                 const uint32_t before = __shfl_sync(0xffffffffu, incl - c, lo);
                 if (idx >= n) continue;
+                if (P.list_cap > 0 && (long long)seg_first + idx >= P.list_cap) continue;
                 const uint32_t r = idx - before;               // r-th set bit of the word
                 int pos = 0;
 #pragma unroll

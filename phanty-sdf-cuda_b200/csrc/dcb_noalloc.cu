@@ -169,6 +169,7 @@ extern "C" int dcb_mark_active_cells_noalloc(const dcb_grid* grid, int64_t* cell
     xp.B = B; xp.nseg = nseg; xp.cell_slot = nullptr; xp.bits = mp.bits; xp.seg_count = mp.seg_count; xp.seg_start = seg_start;
     xp.super = reinterpret_cast<uint32_t*>(sb + off_super);
     xp.list = reinterpret_cast<uint64_t*>(cells);
+    xp.list_cap = capacity;
     if (launch_expand(xp, sms, s) != cudaSuccess) { cudaGetLastError(); return DCB_ERR_CUDA; }
     long long blocks = ((long long)n + 255) / 256;
     if (blocks > (long long)sms * 16) blocks = (long long)sms * 16;

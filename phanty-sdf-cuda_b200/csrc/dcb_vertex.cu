@@ -249,7 +249,10 @@ k_cell_qef(const __grid_constant__ QefParams P) {
     const int tid = threadIdx.x;
     if (tid == 0) s_hist = 0;
     __syncthreads();
-    for (long long r = (long long)blockIdx.x * blockDim.x + tid; r < P.nactive;
+    // a captured graph whose live count exceeds the capacity it was built for does nothing
+    // (the host reports the overflow after the replay)
+    const long long nact = P.live ? ((long long)*P.live > P.nactive ? 0 : (long long)*P.live) : P.nactive;
+    for (long long r = (long long)blockIdx.x * blockDim.x + tid; r < nact;
          r += (long long)gridDim.x * blockDim.x) {
         const GridSlot& S = slot_ref<ONE>(P.B, ONE ? 0 : slot_of_rank(P.B, (unsigned long long)r));
         const GridDesc& g = S.g;

@@ -94,3 +94,58 @@ def test_autotune_keeps_the_results(backend):
     for (Va, Fa), (Vb, Fb) in zip(before, after):
         assert torch.equal(Va, Vb) and torch.equal(Fa, Fb)
     print("autotuned mark tiling: %d waves, 256-cell tiles up to %d cells wide, %.3f ms" % (waves, narrow, ms))
+
+
+# ---- the batch captured in a CUDA graph (dcb_batch_graph_*) -----------------------------------
+
+def _same(meshes_a, meshes_b):
+    assert len(meshes_a) == len(meshes_b)
+    for (Va, Fa), (Vb, Fb) in zip(meshes_a, meshes_b):
+        assert np.array_equal(Va.cpu().numpy(), Vb.cpu().numpy())
+        assert np.array_equal(Fa.cpu().numpy(), Fb.cpu().numpy())
+
+
+def test_graph_replays_equal_eager_batches(backend):
+    """The captured pipeline gives the eager batch's meshes bit for bit, replay after replay,
+    and follows new values written into the same grid buffers."""
+    import torch
+    grids = _mixed()
+    side = torch.cuda.Stream()
+    with torch.cuda.stream(side):
+        eager, st = backend.extract_batch(grids)
+        eager = [(V.clone(), F.clone()) for V, F in eager]
+        backend.batch_graph_create(grids, headroom=0.5)
+        for _ in range(3):
+            backend.batch_graph_launch()
+        got, gst = backend.batch_graph_meshes()
+        _same(got, eager)
+        assert gst.vertex_count == st.vertex_count and gst.face_count == st.face_count
+        # new values in the same buffers (fewer active cells: a smaller sphere)
+        from contouring_b200 import synth
+        v, d, sp, o = synth.sphere(48, 0.2)
+        grids[3][0].copy_(v.cuda())
+        backend.batch_graph_launch()
+        got2, _ = backend.batch_graph_meshes()
+        ref, _ = backend.extract_batch(grids)            # an eager call: invalidates the graph
+        _same(got2, ref)
+        from contouring_b200 import DcbError
+        with pytest.raises(DcbError):
+            backend.batch_graph_launch()
+        backend.batch_graph_destroy()
+    torch.cuda.synchronize()
+
+
+def test_graph_capacity_overflow_is_reported(backend):
+    import torch
+    from contouring_b200 import DcbError, synth
+    grids = [(synth.sphere(40, 0.2)[0].cuda(), (40, 40, 40), synth.sphere(40, 0.2)[2], synth.sphere(40, 0.2)[3])]
+    side = torch.cuda.Stream()
+    with torch.cuda.stream(side):
+        backend.batch_graph_create(grids, headroom=0.0)          # capacity = active cells + 1024
+        noise = synth.noise((40, 40, 40), seed=3)[0]            # far more active cells
+        grids[0][0].copy_(noise.cuda())
+        backend.batch_graph_launch()
+        with pytest.raises(DcbError):
+            backend.batch_graph_finish()
+        backend.batch_graph_destroy()
+    torch.cuda.synchronize()
