@@ -344,6 +344,43 @@ const char* dcb_status_string(int status);
 const char* dcb_last_error(dcb_handle h);
 
 /* Version of the ABI compiled into the library. */
+/* ---- mesh post-pass. Replaces postprocess_mesh (include/dc_backend.h:28;
+ * src/cpp/dc_backend.cpp:217-558, its vertex weld merge_vertices_in_place :127-215): weld
+ * vertices on a grid of 1e-5 box diagonals, drop faces left with < 3 distinct vertices, keep
+ * only the largest face component (remove_floaters), fill boundary loops of 3..4096 vertices
+ * with rings and a fan (close_holes), number vertices by first use and weld again (close_holes).
+ * The result has the reference's vertices, faces and order, bit for bit. Quads in and out (4
+ * int32 indices per face; a filled triangle repeats its last index). With neither flag, or an
+ * empty mesh, the input is returned unchanged (out points at it). */
+typedef struct {
+    int64_t welded_vertices;      /* after the first weld */
+    int64_t welded_faces;
+    int64_t components;           /* face components (remove_floaters), else 0 */
+    int64_t kept_faces;           /* faces of the kept component */
+    int64_t boundary_edges;       /* edge uses that bound the mesh (one use; with both flags, also
+                                     every use of a non-manifold edge) */
+    int64_t loops_found;          /* loops the boundary walks closed */
+    int64_t loops_filled;         /* of them, those with 3..4096 vertices */
+    int64_t fill_vertices;        /* vertices and faces the fill added */
+    int64_t fill_faces;
+    int64_t vertex_count;         /* the result */
+    int64_t face_count;
+    float total_ms;
+} dcb_post_stats;
+
+/* vertices/faces are device pointers (e.g. the handle's own last mesh, quads only). The result
+ * lives in buffers of the handle until the next post-pass call or dcb_destroy. */
+int dcb_postprocess_device(dcb_handle h, const float* vertices, int64_t num_vertices, const int32_t* faces,
+                           int64_t num_faces, int close_holes, int remove_floaters, dcb_mesh_dev* out,
+                           dcb_post_stats* stats, void* cuda_stream);
+/* The same from host arrays (uploaded on the stream); read the result with dcb_copy_post_mesh. */
+int dcb_postprocess_host(dcb_handle h, const float* vertices, int64_t num_vertices, const int32_t* faces,
+                         int64_t num_faces, int close_holes, int remove_floaters, dcb_mesh_dev* out,
+                         dcb_post_stats* stats, void* cuda_stream);
+/* Copy the last post-pass result into caller-owned arrays (3*V floats, 4*F ints): host arrays
+ * when to_host is non-zero (returns after the copy), device arrays otherwise. */
+int dcb_copy_post_mesh(dcb_handle h, float* vertices, int32_t* faces, int to_host, void* cuda_stream);
+
 int dcb_abi_version(void);
 
 #ifdef __cplusplus

@@ -22,6 +22,7 @@ _MTS_LIB = os.path.join(_HERE, "_build", "libmts_oracle.so")
 _ADJ_LIB = os.path.join(_HERE, "_build", "libdc_adjoint_oracle.so")
 _OURS_LIB = os.path.join(_HERE, "_build", "libours_oracle.so")
 _SPARSE_LIB = os.path.join(_HERE, "_build", "libsparse_oracle.so")
+_POST_LIB = os.path.join(_HERE, "_build", "libpost_oracle.so")
 _libs = {}
 
 
@@ -471,3 +472,63 @@ def ref_mesh_to_sdf(V, F, dims, origin, spacing, voxelize_first=False, voxel_res
     if rc != 0:
         return None
     return out, ms.value
+
+
+# ---- mesh post-pass: oracle/post_oracle.cpp restates postprocess_mesh (src/cpp/dc_backend.cpp:127-558)
+POST_STATS = ("welded_vertices", "welded_faces", "components", "kept_faces", "boundary_edges", "loops_found",
+              "loops_filled", "fill_vertices", "fill_faces", "vertex_count", "face_count")
+
+
+def _post_lib(path, prefix):
+    lib = _load(path)
+    if not getattr(lib, "_post_typed", False):
+        run = getattr(lib, prefix + "_run")
+        run.restype = ctypes.c_void_p
+        run.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, ctypes.c_int]
+        for name in ("_num_vertices", "_num_faces"):
+            f = getattr(lib, prefix + name)
+            f.restype = ctypes.c_int64
+            f.argtypes = [ctypes.c_void_p]
+        getattr(lib, prefix + "_free").argtypes = [ctypes.c_void_p]
+        lib._post_typed = True
+    return lib
+
+
+def _post_call(lib, prefix, V, F, close_holes, remove_floaters, with_stats):
+    V = np.ascontiguousarray(V, dtype=np.float32).reshape(-1, 3)
+    F = np.ascontiguousarray(F, dtype=np.int32).reshape(-1, 4)
+    h = getattr(lib, prefix + "_run")(V.ctypes.data if V.size else None, V.shape[0],
+                                     F.ctypes.data if F.size else None, F.shape[0], int(close_holes), int(remove_floaters))
+    if not h:
+        raise ValueError("invalid mesh")
+    try:
+        nv, nf = getattr(lib, prefix + "_num_vertices")(h), getattr(lib, prefix + "_num_faces")(h)
+        Vo = np.empty((nv, 3), np.float32)
+        Fo = np.empty((nf, 4), np.int32)
+        if with_stats:
+            st = np.zeros(len(POST_STATS), np.int64)
+            lib.ppo_copy(ctypes.c_void_p(h), Vo.ctypes.data_as(ctypes.c_void_p), Fo.ctypes.data_as(ctypes.c_void_p),
+                         st.ctypes.data_as(ctypes.c_void_p))
+            return Vo, Fo, dict(zip(POST_STATS, st.tolist()))
+        lib.refpost_copy(ctypes.c_void_p(h), Vo.ctypes.data_as(ctypes.c_void_p), Fo.ctypes.data_as(ctypes.c_void_p))
+        return Vo, Fo
+    finally:
+        getattr(lib, prefix + "_free")(ctypes.c_void_p(h))
+
+
+def postprocess_mesh(V, F, close_holes=True, remove_floaters=True):
+    """The oracle's post-pass: (vertices, quads, stats dict) for quads in."""
+    if not os.path.exists(_POST_LIB):
+        build()
+    return _post_call(_post_lib(_POST_LIB, "ppo"), "ppo", V, F, close_holes, remove_floaters, True)
+
+
+_REF_POST_LIB = os.path.join(_HERE, "_ref", "libref_post.so")
+
+
+def ref_postprocess_mesh(V, F, close_holes=True, remove_floaters=True):
+    """The reference's own postprocess_mesh compiled from its source (oracle/_ref/libref_post.so,
+    `make -C oracle ref`); None when that library was not built."""
+    if not os.path.exists(_REF_POST_LIB):
+        return None
+    return _post_call(_post_lib(_REF_POST_LIB, "refpost"), "refpost", V, F, close_holes, remove_floaters, False)

@@ -9,7 +9,8 @@ Public names mirror the reference module ``_contouring_cpp_module`` (src/cpp/bin
 from .backend import (B200DualContouringBackend, B200SparseDualContouringBackend,
                       B200SparseMvdcDualContouringBackend, ContouringMethod, ContouringOptions, DcbError,
                       DenseSdfGrid, DenseSdfGridDevice, DualContouringMesh, DualContouringStats,
-                      MeshSdfStats, NormalComputationMode, mesh_to_sdf_cuda, mesh_to_sdf_tensor)
+                      MeshSdfStats, NormalComputationMode, PostprocessStats, mesh_to_sdf_cuda, mesh_to_sdf_tensor,
+                      postprocess_mesh, postprocess_mesh_tensor)
 from . import _lib
 
 
@@ -23,4 +24,5 @@ def __getattr__(name):
 __all__ = ["B200DualContouringBackend", "B200SparseDualContouringBackend", "B200SparseMvdcDualContouringBackend",
            "NormalComputationMode", "ContouringMethod", "ContouringOptions", "DcbError",
            "DenseSdfGrid", "DenseSdfGridDevice", "DualContouringMesh", "DualContouringStats",
-           "MeshSdfStats", "mesh_to_sdf_cuda", "mesh_to_sdf_tensor", "dual_contour", "DualContourFunction"]
+           "MeshSdfStats", "mesh_to_sdf_cuda", "mesh_to_sdf_tensor", "dual_contour", "DualContourFunction",
+           "PostprocessStats", "postprocess_mesh", "postprocess_mesh_tensor"]

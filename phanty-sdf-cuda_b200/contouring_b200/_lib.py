@@ -32,7 +32,7 @@ EXPORTED = (
     "dcb_extract_batch_device", "dcb_backward", "dcb_autotune_mark",
     "dcb_write_obj", "dcb_read_sdf", "dcb_write_sdf", "dcb_extract_upload", "dcb_mesh_to_sdf_device_ex",
     "dcb_mesh_to_sdf_host_ex", "dcb_batch_graph_create", "dcb_batch_graph_launch", "dcb_batch_graph_finish",
-    "dcb_batch_graph_destroy")
+    "dcb_batch_graph_destroy", "dcb_postprocess_device", "dcb_postprocess_host", "dcb_copy_post_mesh")
 
 
 class DcbGrid(ctypes.Structure):
@@ -94,6 +94,12 @@ class DcbSdfStats(ctypes.Structure):
                 ("flood_passes", ctypes.c_int64), ("exterior_points", ctypes.c_int64),
                 ("bins_ms", ctypes.c_float), ("band_ms", ctypes.c_float), ("sign_ms", ctypes.c_float),
                 ("relax_ms", ctypes.c_float), ("total_ms", ctypes.c_float)]
+
+
+class DcbPostStats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int64) for n in (
+        "welded_vertices", "welded_faces", "components", "kept_faces", "boundary_edges", "loops_found",
+        "loops_filled", "fill_vertices", "fill_faces", "vertex_count", "face_count")] + [("total_ms", ctypes.c_float)]
 
 
 class DcbError(RuntimeError):
@@ -178,6 +184,13 @@ def lib():
     for name in ("dcb_mesh_to_sdf_device_ex", "dcb_mesh_to_sdf_host_ex"):
         getattr(L, name).argtypes = sdf_ex_args
         getattr(L, name).restype = ctypes.c_int
+    post_args = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int,
+                 ctypes.c_int, P(DcbMeshDev), P(DcbPostStats), ctypes.c_void_p]
+    for name in ("dcb_postprocess_device", "dcb_postprocess_host"):
+        getattr(L, name).argtypes = post_args
+        getattr(L, name).restype = ctypes.c_int
+    L.dcb_copy_post_mesh.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+    L.dcb_copy_post_mesh.restype = ctypes.c_int
     _lib = L
     return L
 

@@ -534,3 +534,75 @@ def mesh_to_sdf_cuda(backend, vertices, faces, nx, ny, nz, ox, oy, oz, vx, vy, v
     st = _sdf_call(backend, backend._L.dcb_mesh_to_sdf_host_ex, V.ctypes.data, len(V), F.ctypes.data, len(F),
                    (nx, ny, nz), (ox, oy, oz), (vx, vy, vz), out.ctypes.data, None, voxelize_first, voxel_res)
     return DenseSdfGrid(nx, ny, nz, vx, vy, vz, ox, oy, oz, values=out), st.total_ms
+
+
+class PostprocessStats:
+    """Counters of one mesh post-pass (``dcb_post_stats``)."""
+
+    def __init__(self, st):
+        for name, _ in _lib.DcbPostStats._fields_:
+            setattr(self, name, getattr(st, name))
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in _lib.DcbPostStats._fields_}
+
+
+_default_backends = {}
+
+
+def _default_backend(device=0):
+    if device not in _default_backends:
+        _default_backends[device] = B200DualContouringBackend(device=device)
+    return _default_backends[device]
+
+
+def postprocess_mesh_tensor(backend, vertices, faces, close_holes, remove_floaters, stream=None):
+    """``postprocess_mesh`` (src/cpp/dc_backend.cpp:217-558) on CUDA tensors: float32 (n,3)
+    vertices and int32 (m,4) quads in (e.g. the tensors of ``extract_tensor``); new tensors of
+    the result and its ``PostprocessStats`` out."""
+    import torch
+    V = vertices.to(torch.float32).contiguous()
+    F = faces.to(torch.int32).contiguous()
+    if not (V.is_cuda and F.is_cuda):
+        raise DcbError(_lib.DCB_ERR_INVALID_ARGUMENT, "vertices and faces must be CUDA tensors")
+    if F.dim() != 2 or F.shape[1] != 4 or (V.numel() and (V.dim() != 2 or V.shape[1] != 3)):
+        raise DcbError(_lib.DCB_ERR_INVALID_ARGUMENT, "expected (n,3) vertices and (m,4) quads")
+    s = _current_stream() if stream is None else stream
+    md = _lib.DcbMeshDev()
+    st = _lib.DcbPostStats()
+    L = backend._L
+    _lib.check(L.dcb_postprocess_device(backend._h, V.data_ptr() if V.numel() else None, V.shape[0],
+                                        F.data_ptr() if F.numel() else None, F.shape[0], int(bool(close_holes)),
+                                        int(bool(remove_floaters)), ctypes.byref(md), ctypes.byref(st),
+                                        ctypes.c_void_p(s)), backend._h)
+    Vo = torch.empty((md.vertex_count, 3), dtype=torch.float32, device=V.device)
+    Fo = torch.empty((md.face_count, 4), dtype=torch.int32, device=V.device)
+    _lib.check(L.dcb_copy_post_mesh(backend._h, Vo.data_ptr() if Vo.numel() else None,
+                                    Fo.data_ptr() if Fo.numel() else None, 0, ctypes.c_void_p(s)), backend._h)
+    return Vo, Fo, PostprocessStats(st)
+
+
+def postprocess_mesh(mesh, close_holes, remove_floaters, backend=None, stream=None):
+    """The reference module's ``postprocess_mesh(mesh, close_holes, remove_floaters)``
+    (src/cpp/bindings.cpp:145): a ``DualContouringMesh`` of quads in, the post-processed
+    ``DualContouringMesh`` out (flat arrays, as ``extract`` returns them), computed on the GPU.
+    The stats of the call are left in ``backend.last_postprocess_stats``."""
+    backend = backend if backend is not None else _default_backend()
+    V = np.ascontiguousarray(np.asarray(mesh.vertices, np.float32).reshape(-1))
+    F = np.ascontiguousarray(np.asarray(mesh.faces, np.int32).reshape(-1))
+    if V.size % 3 or F.size % 4:
+        raise DcbError(_lib.DCB_ERR_INVALID_ARGUMENT, "expected xyz vertices and quads (4 indices per face)")
+    s = _current_stream() if stream is None else stream
+    md = _lib.DcbMeshDev()
+    st = _lib.DcbPostStats()
+    L = backend._L
+    _lib.check(L.dcb_postprocess_host(backend._h, V.ctypes.data if V.size else None, V.size // 3,
+                                      F.ctypes.data if F.size else None, F.size // 4, int(bool(close_holes)),
+                                      int(bool(remove_floaters)), ctypes.byref(md), ctypes.byref(st),
+                                      ctypes.c_void_p(s)), backend._h)
+    Vo = _host_array(3 * md.vertex_count, np.float32)
+    Fo = _host_array(4 * md.face_count, np.int32)
+    _lib.check(L.dcb_copy_post_mesh(backend._h, Vo.ctypes.data if Vo.size else None, Fo.ctypes.data if Fo.size else None,
+                                    1, ctypes.c_void_p(s)), backend._h)
+    backend.last_postprocess_stats = PostprocessStats(st)
+    return DualContouringMesh(Vo, Fo)

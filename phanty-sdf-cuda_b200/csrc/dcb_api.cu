@@ -90,6 +90,12 @@ struct dcb_context {
     int batch_n = 1;
     std::vector<int> batch_cx, batch_cy;
     std::vector<int64_t> vert_offsets, face_offsets;
+    // mesh post-pass: workspace, uploaded host input, the last result
+    PostWork post;
+    DevBuf pp_in_V, pp_in_F;
+    const float* pp_V = nullptr;
+    const int32_t* pp_F = nullptr;
+    int64_t pp_nv = 0, pp_nf = 0;
 };
 
 namespace {
@@ -1045,6 +1051,9 @@ int dcb_destroy(dcb_handle h) {
     if (h->h_sdf_counters) cudaFreeHost(h->h_sdf_counters);
     if (h->h_sp_counters) cudaFreeHost(h->h_sp_counters);
     destroy_graph(h);
+    post_release(h->post);
+    if (h->pp_in_V.p) cudaFree(h->pp_in_V.p);
+    if (h->pp_in_F.p) cudaFree(h->pp_in_F.p);
     if (h->h_table) cudaFreeHost(h->h_table);
     if (h->h_offsets) cudaFreeHost(h->h_offsets);
     if (h->hV) cudaFreeHost(h->hV);
@@ -1484,6 +1493,83 @@ int dcb_mesh_to_sdf_host_ex(dcb_handle h, const float* vertices, int64_t num_ver
     if (rc != DCB_OK) return rc;
     DCB_TRY(h, cudaMemcpyAsync(out_values, h->m_out.p, sizeof(float) * npts, cudaMemcpyDeviceToHost, s), "download values");
     DCB_TRY(h, cudaStreamSynchronize(s), "download values");
+    return DCB_OK;
+}
+
+int dcb_postprocess_device(dcb_handle h, const float* vertices, int64_t num_vertices, const int32_t* faces,
+                           int64_t num_faces, int close_holes, int remove_floaters, dcb_mesh_dev* out,
+                           dcb_post_stats* stats, void* cuda_stream) {
+    if (!h) return DCB_ERR_INVALID_ARGUMENT;
+    if (stats) std::memset(stats, 0, sizeof(*stats));
+    if (out) std::memset(out, 0, sizeof(*out));
+    h->pp_V = nullptr; h->pp_F = nullptr; h->pp_nv = 0; h->pp_nf = 0;
+    if (num_vertices < 0 || num_faces < 0 || (num_vertices > 0 && !vertices) || (num_faces > 0 && !faces))
+        return fail(h, DCB_ERR_INVALID_ARGUMENT, "null mesh arrays or negative counts");
+    if (num_vertices >= 0x7fffffffLL || num_faces >= (1LL << 29))
+        return fail(h, DCB_ERR_TOO_LARGE, "post-pass limits: < 2^31 vertices, < 2^29 quads");
+    if (cudaSetDevice(h->device) != cudaSuccess) { cudaGetLastError(); return fail(h, DCB_ERR_CUDA, "set device"); }
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(cuda_stream);
+    DCB_TRY(h, cudaEventRecord(h->ev[0], s), "event");
+    PostRun R;
+    R.V = vertices; R.nv = num_vertices; R.F = faces; R.nf = num_faces;
+    R.close_holes = close_holes != 0; R.remove_floaters = remove_floaters != 0; R.num_sms = h->num_sms;
+    const cudaError_t e = post_run(h->post, R, s);
+    if (e != cudaSuccess) return cuda_fail(h, e, R.what ? R.what : "post-pass");
+    if (R.err & 1) return fail(h, DCB_ERR_INVALID_ARGUMENT, "face index out of range");
+    if (R.err & 2) return fail(h, DCB_ERR_INVALID_ARGUMENT, "non-finite vertex coordinate");
+    if (R.err & 4) return fail(h, DCB_ERR_NOT_SUPPORTED, "vertices too close together for the weld step");
+    if (R.err & 16) return fail(h, DCB_ERR_NOT_SUPPORTED, "a hole fill did not converge within 8192 rings");
+    if (R.err) return fail(h, DCB_ERR_INTERNAL, "post-pass consistency check failed");
+    if (R.too_large) return fail(h, DCB_ERR_TOO_LARGE, "filled mesh exceeds the index limits");
+    DCB_TRY(h, cudaEventRecord(h->ev[4], s), "event");
+    DCB_TRY(h, cudaEventSynchronize(h->ev[4]), "post-pass");
+    h->pp_V = R.out_V; h->pp_F = R.out_F; h->pp_nv = R.nv_out; h->pp_nf = R.nf_out;
+    if (stats) {
+        int64_t* st = &stats->welded_vertices;
+        for (int i = 0; i < kPostNumStats; ++i) st[i] = R.stats[i];
+        stats->total_ms = elapsed(h->ev[0], h->ev[4]);
+    }
+    if (out) {
+        out->vertex_count = R.nv_out;
+        out->face_count = R.nf_out;
+        out->verts_per_face = 4;
+        out->vertices = const_cast<float*>(R.out_V);
+        out->faces = const_cast<int32_t*>(R.out_F);
+        out->cell_coords = nullptr;
+    }
+    return DCB_OK;
+}
+
+int dcb_postprocess_host(dcb_handle h, const float* vertices, int64_t num_vertices, const int32_t* faces,
+                         int64_t num_faces, int close_holes, int remove_floaters, dcb_mesh_dev* out,
+                         dcb_post_stats* stats, void* cuda_stream) {
+    if (!h) return DCB_ERR_INVALID_ARGUMENT;
+    if (num_vertices < 0 || num_faces < 0 || (num_vertices > 0 && !vertices) || (num_faces > 0 && !faces))
+        return fail(h, DCB_ERR_INVALID_ARGUMENT, "null mesh arrays or negative counts");
+    if (num_vertices >= 0x7fffffffLL || num_faces >= (1LL << 29))
+        return fail(h, DCB_ERR_TOO_LARGE, "post-pass limits: < 2^31 vertices, < 2^29 quads");
+    if (cudaSetDevice(h->device) != cudaSuccess) { cudaGetLastError(); return fail(h, DCB_ERR_CUDA, "set device"); }
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(cuda_stream);
+    DCB_TRY(h, ensure(h->pp_in_V, sizeof(float) * 3 * (size_t)std::max<int64_t>(1, num_vertices)), "alloc vertices");
+    DCB_TRY(h, ensure(h->pp_in_F, sizeof(int32_t) * 4 * (size_t)std::max<int64_t>(1, num_faces)), "alloc faces");
+    if (num_vertices)
+        DCB_TRY(h, cudaMemcpyAsync(h->pp_in_V.p, vertices, sizeof(float) * 3 * num_vertices, cudaMemcpyHostToDevice, s), "upload vertices");
+    if (num_faces)
+        DCB_TRY(h, cudaMemcpyAsync(h->pp_in_F.p, faces, sizeof(int32_t) * 4 * num_faces, cudaMemcpyHostToDevice, s), "upload faces");
+    return dcb_postprocess_device(h, as<float>(h->pp_in_V), num_vertices, as<int32_t>(h->pp_in_F), num_faces,
+                                  close_holes, remove_floaters, out, stats, cuda_stream);
+}
+
+int dcb_copy_post_mesh(dcb_handle h, float* vertices, int32_t* faces, int to_host, void* cuda_stream) {
+    if (!h) return DCB_ERR_INVALID_ARGUMENT;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(cuda_stream);
+    if (cudaSetDevice(h->device) != cudaSuccess) { cudaGetLastError(); return fail(h, DCB_ERR_CUDA, "set device"); }
+    const cudaMemcpyKind kind = to_host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    if (vertices && h->pp_nv)
+        DCB_TRY(h, cudaMemcpyAsync(vertices, h->pp_V, sizeof(float) * 3 * h->pp_nv, kind, s), "copy vertices");
+    if (faces && h->pp_nf)
+        DCB_TRY(h, cudaMemcpyAsync(faces, h->pp_F, sizeof(int32_t) * 4 * h->pp_nf, kind, s), "copy faces");
+    if (to_host) DCB_TRY(h, cudaStreamSynchronize(s), "copy mesh");
     return DCB_OK;
 }
 

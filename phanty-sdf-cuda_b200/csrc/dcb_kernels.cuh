@@ -410,4 +410,47 @@ cudaError_t launch_sparse_place(const SparseParams& P, int num_sms, cudaStream_t
 cudaError_t launch_sparse_faces(const SparseParams& P, int num_sms, cudaStream_t s);
 cudaError_t launch_sparse_compact(const SparseParams& P, int num_sms, cudaStream_t s);
 
+// ---- mesh post-pass (dcb_post.cu): postprocess_mesh, src/cpp/dc_backend.cpp:127-558
+struct PostBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+enum PostStatIndex {
+    kPostWeldedVertices, kPostWeldedFaces, kPostComponents, kPostKeptFaces, kPostBoundaryEdges, kPostLoopsFound,
+    kPostLoopsFilled, kPostFillVertices, kPostFillFaces, kPostVertexCount, kPostFaceCount, kPostNumStats
+};
+
+// Device workspace of the post-pass; kept by the handle between calls (buffers only grow).
+struct PostWork {
+    PostBuf count, key, key2, val, val2, u0, u1, u2, u3, ft, flag8, cub;
+    PostBuf Vw, Fw, kept, parent, csize, bnd;
+    PostBuf deg, bot, top, pos, vparent, skey, sdeg, shead, soff, sgid, stack, lverts, lflag, lkey, llen;
+    PostBuf lpos, lorder, lkey2, nvl, nfl, vb, fb, fillV, fillF;
+    PostBuf first, fflag, slot, V1, F1, outV, outF;
+    void* hcount = nullptr;             // page-locked copy of the device counters
+};
+
+struct PostRun {
+    // in: a quad mesh on the device
+    const float* V = nullptr;
+    long long nv = 0;
+    const int32_t* F = nullptr;
+    long long nf = 0;
+    int close_holes = 0, remove_floaters = 0;
+    int num_sms = 148;
+    // out: the result (the workspace's buffers, or the input when nothing is to be done)
+    const float* out_V = nullptr;
+    const int32_t* out_F = nullptr;
+    long long nv_out = 0, nf_out = 0;
+    long long stats[kPostNumStats] = {};
+    int err = 0;                        // device-side findings: 1 face index out of range, 2 non-finite vertex,
+                                        // 4 weld key out of range, 8 walk guard, 16 fill did not converge
+    int too_large = 0;
+    const char* what = nullptr;         // the failing CUDA call
+};
+
+cudaError_t post_run(PostWork& W, PostRun& R, cudaStream_t s);
+void post_release(PostWork& W);
+
 }  // namespace dcb

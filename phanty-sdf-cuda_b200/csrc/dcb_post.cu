@@ -1,0 +1,1048 @@
+// dcb_post.cu — the mesh post-pass on the GPU: vertex weld, floater removal and hole closing of
+// a quad mesh. The semantics are the reference's postprocess_mesh and merge_vertices_in_place
+// (src/cpp/dc_backend.cpp:127-558): the same vertices, faces and order, bit for bit.
+//
+// Stages, on one stream, with a few host reads of counts between them (sizes of what follows):
+//   weld     bounding box by ordered-integer atomics; the quantisation step in the reference's
+//            float expression order (one thread); a 51-bit grid-point key per vertex (17 bits per
+//            axis relative to the box's low corner: the box spans at most ~1e5 steps); a stable
+//            radix sort; the first vertex of each key represents it; representatives numbered by
+//            a scan in index order; faces remapped, those with < 3 distinct indices dropped with
+//            the order kept (dc_backend.cpp:127-215).
+//   edges    the 4 edge uses of every face keyed by (min, max) vertex and radix sorted; a run of
+//            one use is a boundary edge, a run of two joins its faces in a union-find whose roots
+//            are the smallest face index (dc_backend.cpp:231-310).
+//   keep     the component with the most faces, the one with the smallest first face on ties
+//            (the reference numbers components by their first face: dc_backend.cpp:312-361).
+//   holes    boundary edges of the kept faces sorted by (from, to), so each vertex's outgoing
+//            edges are in the order the reference pushes them and are taken from the back. Walks
+//            (dc_backend.cpp:468-503) are sequential inside a weakly connected component of the
+//            boundary graph — one thread each, start vertices in ascending order — and
+//            independent across components; the loops they close are put in the reference's
+//            global order by (start vertex, sequence). Filling (dc_backend.cpp:376-466): a block
+//            per loop, ring by ring, the running sums in the reference's order by one thread per
+//            coordinate and the rest in parallel; run once for sizes and once to write.
+//   renumber vertices by first use in the face list (dc_backend.cpp:537-550): atomicMin of the
+//            first position of every vertex, a scan over first uses.
+//   weld     again on the result when holes are closed (dc_backend.cpp:552-554).
+//
+// Compiled with --fmad=false: every float expression is rounded as written, like the
+// reference's x86-64 build.
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
+#include <cub/device/device_select.cuh>
+#include <thrust/iterator/counting_iterator.h>
+#include "dcb_kernels.cuh"
+
+namespace dcb {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kMaxLoop = 4096;          // loops longer than this are not filled (dc_backend.cpp:487, 497)
+constexpr int kMaxRings = 8192;         // a fill that has not converged by then is reported
+constexpr int kFillThreads = 256;
+constexpr int kKeyBits = 17;            // per axis in the weld key
+
+enum PostErr { kPostBadIndex = 1, kPostNonFinite = 2, kPostWeldSpan = 4, kPostWalkGuard = 8, kPostRingGuard = 16 };
+
+struct PostCounters {
+    unsigned int box[6];                // ordered bits: min x, y, z; max x, y, z
+    int err;
+    int pad;
+    float inv;                          // 1 / weld step
+    int pad2;
+    long long qlo[3];                   // grid point of the box's low corner
+    unsigned long long nvw;             // welded vertices (groups)
+    unsigned long long nsel;            // selection counts (faces kept by the weld, by the component)
+    unsigned long long nb;              // boundary uses
+    unsigned long long ncomp;           // face components
+    unsigned long long best;            // size << 32 | ~root of the largest component
+    unsigned long long nbk;             // boundary edges of kept faces
+    unsigned long long nstarts;         // vertices with outgoing boundary edges
+    unsigned long long loops_found;
+    unsigned long long nloops;          // loops of 3..4096 vertices
+    unsigned long long fill_v, fill_f;
+    unsigned long long nout;            // vertices after renumbering
+};
+
+inline unsigned grid_for(long long n, int threads, int num_sms) {
+    const long long blocks = (n + threads - 1) / threads;
+    return (unsigned)std::max(1LL, std::min(blocks, (long long)num_sms * 16));
+}
+
+__device__ __forceinline__ unsigned int ordered(float x) {
+    const unsigned int b = __float_as_uint(x);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ float unordered(unsigned int o) {
+    return __uint_as_float((o & 0x80000000u) ? (o & 0x7fffffffu) : ~o);
+}
+
+// ---- union-find with roots = smallest member; finds halve the path as they go (the
+// intermediate pointer jumping of Jaiganesh & Burtscher, "A high-performance connected
+// components implementation for GPUs", HPDC 2018). Parents only ever point to smaller indices.
+__device__ __forceinline__ int uf_find(int* parent, int x) {
+    volatile int* p = parent;
+    int cur = p[x];
+    if (cur != x) {
+        int prev = x, next;
+        while (cur > (next = p[cur])) {
+            p[prev] = next;
+            prev = cur;
+            cur = next;
+        }
+    }
+    return cur;
+}
+
+__device__ void uf_unite(int* parent, int a, int b, int* err) {
+    int ra = uf_find(parent, a), rb = uf_find(parent, b);
+    for (int guard = 0; ra != rb; ++guard) {
+        if (guard > (1 << 24)) { atomicOr(err, kPostWalkGuard); return; }
+        if (ra < rb) { const int t = ra; ra = rb; rb = t; }
+        const int old = atomicCAS(&parent[ra], ra, rb);
+        if (old == ra) return;
+        ra = old;   // ra was linked meanwhile: continue from its new parent
+    }
+}
+
+__global__ void k_iota(int* a, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        a[i] = (int)i;
+}
+
+// After all unions: every parent becomes its root. The walk up only reads (a path-halving
+// write here could replace a root that another thread just stored with an intermediate
+// ancestor); the only writes are roots.
+__global__ void k_flatten(int* parent, long long n) {
+    volatile int* p = parent;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        int x = (int)i, up;
+        while ((up = p[x]) != x) x = up;   // indices strictly decrease towards the root
+        p[i] = x;
+    }
+}
+
+// ---------------------------------------------------------------- weld
+__global__ void k_post_reset(PostCounters* C) {
+    if (threadIdx.x == 0) {
+        for (int a = 0; a < 3; ++a) { C->box[a] = 0xffffffffu; C->box[3 + a] = 0u; }
+        C->nvw = 0; C->nsel = 0;
+    }
+}
+
+__global__ void k_bbox(const float* __restrict__ V, long long nv, PostCounters* C) {
+    unsigned int lo[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu}, hi[3] = {0u, 0u, 0u};
+    bool bad = false;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nv; i += (long long)gridDim.x * blockDim.x)
+        for (int a = 0; a < 3; ++a) {
+            const float x = V[3 * i + a];
+            bad |= !isfinite(x);
+            const unsigned int o = ordered(x);
+            lo[a] = min(lo[a], o);
+            hi[a] = max(hi[a], o);
+        }
+    for (int a = 0; a < 3; ++a)
+        for (int d = 16; d > 0; d >>= 1) {
+            lo[a] = min(lo[a], __shfl_xor_sync(0xffffffffu, lo[a], d));
+            hi[a] = max(hi[a], __shfl_xor_sync(0xffffffffu, hi[a], d));
+        }
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(&C->err, kPostNonFinite);
+    if ((threadIdx.x & 31) == 0)
+        for (int a = 0; a < 3; ++a) { atomicMin(&C->box[a], lo[a]); atomicMax(&C->box[3 + a], hi[a]); }
+}
+
+// The weld step: eps = |box diagonal| * 1e-5 (1e-5 for a point), in the reference's order.
+__global__ void k_weld_params(PostCounters* C) {
+    if (threadIdx.x != 0) return;
+    float lo[3], hi[3];
+    for (int a = 0; a < 3; ++a) { lo[a] = unordered(C->box[a]); hi[a] = unordered(C->box[3 + a]); }
+    const float ex = hi[0] - lo[0], ey = hi[1] - lo[1], ez = hi[2] - lo[2];
+    const float diag = sqrtf(ex * ex + ey * ey + ez * ez);
+    const float eps = diag > 0.0f ? diag * 1e-5f : 1e-5f;
+    const float inv = 1.0f / eps;
+    C->inv = inv;
+    for (int a = 0; a < 3; ++a) C->qlo[a] = (long long)roundf(lo[a] * inv);
+}
+
+__global__ void k_weld_keys(const float* __restrict__ V, long long nv, PostCounters* C,
+                            unsigned long long* key, int* idx) {
+    const float inv = C->inv;
+    const long long q0 = C->qlo[0], q1 = C->qlo[1], q2 = C->qlo[2];
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nv; i += (long long)gridDim.x * blockDim.x) {
+        const long long d0 = (long long)roundf(V[3 * i] * inv) - q0;
+        const long long d1 = (long long)roundf(V[3 * i + 1] * inv) - q1;
+        const long long d2 = (long long)roundf(V[3 * i + 2] * inv) - q2;
+        const long long lim = 1LL << kKeyBits;
+        if (d0 < 0 || d0 >= lim || d1 < 0 || d1 >= lim || d2 < 0 || d2 >= lim) atomicOr(&C->err, kPostWeldSpan);
+        key[i] = ((unsigned long long)(d0 & (lim - 1))) | ((unsigned long long)(d1 & (lim - 1)) << kKeyBits) |
+                 ((unsigned long long)(d2 & (lim - 1)) << (2 * kKeyBits));
+        idx[i] = (int)i;
+    }
+}
+
+// head[p]: sorted position p starts a key; rep[i]: vertex i is the first of its key.
+__global__ void k_weld_heads(const unsigned long long* __restrict__ skey, const int* __restrict__ sidx, long long n,
+                             unsigned int* head, unsigned int* rep) {
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+        const unsigned int h = (p == 0 || skey[p] != skey[p - 1]) ? 1u : 0u;
+        head[p] = h;
+        rep[sidx[p]] = h;
+    }
+}
+
+// group g (1-based inclusive scan of heads) -> new index of its representative; welded vertices.
+__global__ void k_weld_groups(const int* __restrict__ sidx, const unsigned int* __restrict__ head,
+                              const unsigned int* __restrict__ gid, const unsigned int* __restrict__ newid,
+                              const float* __restrict__ V, long long n, unsigned int* grp, float* Vw, PostCounters* C) {
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+        if (p == n - 1) C->nvw = gid[p];
+        if (!head[p]) continue;
+        const int i = sidx[p];
+        const unsigned int nid = newid[i];
+        grp[gid[p] - 1] = nid;
+        Vw[3 * (long long)nid] = V[3 * (long long)i];
+        Vw[3 * (long long)nid + 1] = V[3 * (long long)i + 1];
+        Vw[3 * (long long)nid + 2] = V[3 * (long long)i + 2];
+    }
+}
+
+__global__ void k_weld_remap(const int* __restrict__ sidx, const unsigned int* __restrict__ gid,
+                             const unsigned int* __restrict__ grp, long long n, int* remap) {
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x)
+        remap[sidx[p]] = (int)grp[gid[p] - 1];
+}
+
+__global__ void k_weld_faces(const int32_t* __restrict__ F, long long nf, long long nv, const int* __restrict__ remap,
+                             int4* Ft, unsigned char* keep, PostCounters* C) {
+    for (long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x; f < nf; f += (long long)gridDim.x * blockDim.x) {
+        int c[4];
+        bool ok = true;
+        for (int k = 0; k < 4; ++k) {
+            const int32_t v = F[4 * f + k];
+            ok = ok && v >= 0 && v < nv;
+            c[k] = v;
+        }
+        if (!ok) { atomicOr(&C->err, kPostBadIndex); keep[f] = 0; continue; }
+        int distinct = 0;
+        for (int k = 0; k < 4; ++k) {
+            c[k] = remap[c[k]];
+            bool seen = false;
+            for (int j = 0; j < k; ++j) seen = seen || c[j] == c[k];
+            distinct += !seen;
+        }
+        Ft[f] = make_int4(c[0], c[1], c[2], c[3]);
+        keep[f] = distinct >= 3 ? 1 : 0;
+    }
+}
+
+// ---------------------------------------------------------------- edges and components
+__device__ __forceinline__ int corner(const int4& q, int e) {
+    return e == 0 ? q.x : e == 1 ? q.y : e == 2 ? q.z : q.w;
+}
+
+__global__ void k_edge_uses(const int4* __restrict__ Fw, long long nf, int b, unsigned long long* key, int* val) {
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < 4 * nf; t += (long long)gridDim.x * blockDim.x) {
+        const long long f = t >> 2;
+        const int e = (int)(t & 3);
+        const int4 q = Fw[f];
+        const int u = corner(q, e), v = corner(q, (e + 1) & 3);
+        key[t] = u == v ? ~0ull : ((unsigned long long)min(u, v) << b) | (unsigned long long)max(u, v);
+        val[t] = (int)t;
+    }
+}
+
+struct EdgeRunParams {
+    const unsigned long long* key;
+    const int* val;
+    long long n;
+    unsigned long long invalid;         // the sentinel within the sorted bits
+    const int4* Fw;
+    int close, remove;
+    int* parent;
+    int4* bnd;                          // (from, to, face, 0)
+    PostCounters* C;
+};
+
+__device__ __forceinline__ void push_boundary(const EdgeRunParams& P, int use) {
+    const int f = use >> 2, e = use & 3;
+    const int4 q = P.Fw[f];
+    const unsigned long long at = atomicAdd(&P.C->nb, 1ull);
+    P.bnd[at] = make_int4(corner(q, e), corner(q, (e + 1) & 3), f, 0);
+}
+
+__global__ void k_edge_runs(EdgeRunParams P) {
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < P.n; p += (long long)gridDim.x * blockDim.x) {
+        const unsigned long long k = P.key[p];
+        if ((k & P.invalid) == P.invalid) continue;
+        if (p > 0 && P.key[p - 1] == k) continue;
+        long long q = p + 1;
+        while (q < P.n && P.key[q] == k) ++q;
+        const long long c = q - p;
+        if (c == 1) {
+            push_boundary(P, P.val[p]);
+        } else if (c == 2) {
+            if (P.remove) uf_unite(P.parent, P.val[p] >> 2, P.val[p + 1] >> 2, &P.C->err);
+        } else if (P.close && P.remove) {
+            for (long long x = p; x < q; ++x) push_boundary(P, P.val[x]);
+        }
+    }
+}
+
+__global__ void k_comp_size(const int* __restrict__ root, long long n, unsigned int* size) {
+    for (long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x; f < n; f += (long long)gridDim.x * blockDim.x)
+        atomicAdd(&size[root[f]], 1u);
+}
+
+__global__ void k_comp_pick(const int* __restrict__ root, const unsigned int* __restrict__ size, long long n, PostCounters* C) {
+    for (long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x; f < n; f += (long long)gridDim.x * blockDim.x) {
+        if (root[f] != f) continue;
+        atomicAdd(&C->ncomp, 1ull);
+        atomicMax(&C->best, ((unsigned long long)size[f] << 32) | (0xffffffffull - (unsigned long long)f));
+    }
+}
+
+__global__ void k_keep_flags(const int* __restrict__ root, long long n, const PostCounters* C, unsigned char* keep) {
+    const int L = (int)(0xffffffffull - (C->best & 0xffffffffull));
+    for (long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x; f < n; f += (long long)gridDim.x * blockDim.x)
+        keep[f] = root[f] == L ? 1 : 0;
+}
+
+// ---------------------------------------------------------------- holes
+__global__ void k_bnd_keys(const int4* __restrict__ bnd, long long nb, const int* __restrict__ root, int remove, int b,
+                           unsigned long long* key, unsigned int* deg, PostCounters* C) {
+    const int L = remove ? (int)(0xffffffffull - (C->best & 0xffffffffull)) : 0;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nb; t += (long long)gridDim.x * blockDim.x) {
+        const int4 e = bnd[t];
+        if (remove && root[e.z] != L) { key[t] = ~0ull; continue; }
+        key[t] = ((unsigned long long)e.x << b) | (unsigned long long)e.y;
+        atomicAdd(&deg[e.x], 1u);
+        atomicAdd(&C->nbk, 1ull);
+    }
+}
+
+__global__ void k_bnd_unite(const unsigned long long* __restrict__ key, long long n, int b, int* parent, PostCounters* C) {
+    const unsigned long long m = (1ull << b) - 1;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+        uf_unite(parent, (int)(key[t] >> b), (int)(key[t] & m), &C->err);
+}
+
+__global__ void k_start_keys(const unsigned int* __restrict__ deg, const int* __restrict__ root, long long nv, int b,
+                             unsigned long long* key, PostCounters* C) {
+    for (long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x; u < nv; u += (long long)gridDim.x * blockDim.x) {
+        if (!deg[u]) continue;
+        key[atomicAdd(&C->nstarts, 1ull)] = ((unsigned long long)root[u] << b) | (unsigned long long)u;
+    }
+}
+
+// Per sorted start: its out-degree (for the region offsets) and whether it opens a component.
+__global__ void k_start_info(const unsigned long long* __restrict__ skey, long long n, int b,
+                             const unsigned int* __restrict__ deg, unsigned long long* sdeg, unsigned int* shead) {
+    const unsigned long long m = (1ull << b) - 1;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+        sdeg[p] = deg[skey[p] & m];
+        shead[p] = (p == 0 || (skey[p] >> b) != (skey[p - 1] >> b)) ? 1u : 0u;
+    }
+}
+
+struct WalkParams {
+    const unsigned long long* skey;     // sorted starts: root << b | vertex
+    long long nstarts;
+    const unsigned int* shead;
+    const unsigned long long* soff;     // exclusive scan of the starts' out-degrees
+    const unsigned int* sgid;           // inclusive scan of shead
+    int b;
+    const unsigned long long* adj;      // sorted boundary keys: from << b | to
+    const unsigned int* bot;            // first adjacency entry of every vertex
+    unsigned int* top;                  // one past its last unused entry
+    int* pos;                           // position on the current path, -1 when off it
+    int* stack;                         // per component: out-degree sum + 1 entries
+    int* lverts;                        // per component: out-degree sum entries
+    unsigned char* lflag;               // a recorded loop starts here
+    unsigned long long* lkey;           // its order: start vertex << 32 | sequence
+    int* llen;
+    PostCounters* C;
+};
+
+// One thread per boundary component: the reference's walks (dc_backend.cpp:468-503) over the
+// component's start vertices in ascending order. Every step consumes one edge, so a walk ends
+// after at most the component's edge count steps.
+__global__ void k_walk(WalkParams P) {
+    for (long long p0 = blockIdx.x * (long long)blockDim.x + threadIdx.x; p0 < P.nstarts;
+         p0 += (long long)gridDim.x * blockDim.x) {
+        if (!P.shead[p0]) continue;
+        const unsigned long long m = (1ull << P.b) - 1;
+        const unsigned long long root = P.skey[p0] >> P.b;
+        long long p1 = p0 + 1;
+        while (p1 < P.nstarts && (P.skey[p1] >> P.b) == root) ++p1;
+        const unsigned long long base = P.soff[p0];
+        int* stk = P.stack + base + (P.sgid[p0] - 1);
+        long long w = 0;               // written loop vertices
+        unsigned long long found = 0, recorded = 0;
+        long long guard = 0;
+        for (long long p = p0; p < p1; ++p) {
+            const int s = (int)(P.skey[p] & m);
+            unsigned int seq = 0;
+            while (P.top[s] > P.bot[s]) {
+                int len = 1;
+                stk[0] = s;
+                P.pos[s] = 0;
+                int at = s;
+                bool closed = false;
+                while (P.top[at] > P.bot[at]) {
+                    if (++guard > (1LL << 31)) { atomicOr(&P.C->err, kPostWalkGuard); return; }
+                    const unsigned int t = --P.top[at];
+                    const int next = (int)(P.adj[t] & m);
+                    if (next == s) { closed = true; break; }
+                    const int hit = P.pos[next];
+                    if (hit >= 0) {
+                        const int L = len - hit;
+                        ++found;
+                        if (L >= 3 && L <= kMaxLoop) {
+                            const long long o = (long long)base + w;
+                            for (int i = 0; i < L; ++i) P.lverts[o + i] = stk[len - 1 - i];
+                            P.lflag[o] = 1;
+                            P.lkey[o] = ((unsigned long long)s << 32) | seq++;
+                            P.llen[o] = L;
+                            w += L;
+                            ++recorded;
+                        }
+                        for (int i = hit; i < len; ++i) P.pos[stk[i]] = -1;
+                        len = hit;
+                    }
+                    stk[len] = next;
+                    P.pos[next] = len;
+                    ++len;
+                    at = next;
+                }
+                if (closed) {
+                    ++found;
+                    if (len >= 3 && len <= kMaxLoop) {
+                        const long long o = (long long)base + w;
+                        for (int i = 0; i < len; ++i) P.lverts[o + i] = stk[len - 1 - i];
+                        P.lflag[o] = 1;
+                        P.lkey[o] = ((unsigned long long)s << 32) | seq++;
+                        P.llen[o] = len;
+                        w += len;
+                        ++recorded;
+                    }
+                }
+                for (int i = 0; i < len; ++i) P.pos[stk[i]] = -1;
+            }
+        }
+        atomicAdd(&P.C->loops_found, found);
+        atomicAdd(&P.C->nloops, recorded);
+    }
+}
+
+__global__ void k_tops(const unsigned int* __restrict__ bot, const unsigned int* __restrict__ deg, long long n,
+                       unsigned int* top) {
+    for (long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x; u < n; u += (long long)gridDim.x * blockDim.x)
+        top[u] = bot[u] + deg[u];
+}
+
+__global__ void k_gather_keys(const int* __restrict__ lpos, const unsigned long long* __restrict__ lkey, long long n,
+                              unsigned long long* key) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        key[i] = lkey[lpos[i]];
+}
+
+struct FillParams {
+    const int* lorder;                  // loop start positions in fill order
+    long long nloops;
+    const int* lverts;
+    const int* llen;
+    const float* Vw;                    // welded vertices (loop vertices are among them)
+    long long nvw;
+    unsigned long long* nvl;            // sizes pass: new vertices and faces per loop
+    unsigned long long* nfl;
+    const unsigned long long* vb;       // write pass: exclusive scans of the sizes
+    const unsigned long long* fb;
+    float* fillV;                       // new vertices (global index nvw + local)
+    int4* fillF;                        // new faces
+    PostCounters* C;
+};
+
+// One loop per block: rings towards the centroid (dc_backend.cpp:376-466). Shared memory holds
+// two rings (x, y, z arrays) and one scratch array of kMaxLoop floats each.
+template <bool WRITE>
+__global__ void __launch_bounds__(kFillThreads) k_fill(FillParams P) {
+    extern __shared__ float sh[];
+    float* ax = sh;                      // current ring
+    float* ay = ax + kMaxLoop;
+    float* az = ay + kMaxLoop;
+    float* bx = az + kMaxLoop;           // next ring
+    float* by = bx + kMaxLoop;
+    float* bz = by + kMaxLoop;
+    float* sd = bz + kMaxLoop;
+    __shared__ float s_step, s_c[3], s_far;
+    const int tid = threadIdx.x;
+    for (long long li = blockIdx.x; li < P.nloops; li += gridDim.x) {
+        const int at = P.lorder[li];
+        const int n = P.llen[at];
+        const int* idx = P.lverts + at;
+        for (int k = tid; k < n; k += blockDim.x) {
+            const long long v = idx[k];
+            ax[k] = P.Vw[3 * v]; ay[k] = P.Vw[3 * v + 1]; az[k] = P.Vw[3 * v + 2];
+        }
+        __syncthreads();
+        for (int k = tid; k < n; k += blockDim.x) {
+            const int k1 = k + 1 == n ? 0 : k + 1;
+            const float dx = ax[k1] - ax[k], dy = ay[k1] - ay[k], dz = az[k1] - az[k];
+            sd[k] = sqrtf(dx * dx + dy * dy + dz * dz);
+        }
+        __syncthreads();
+        if (tid == 0) {
+            float step = 0.0f;
+            for (int k = 0; k < n; ++k) step += sd[k];
+            step /= (float)n;
+            if (step <= 0.0001f) step = 1.0f;
+            s_step = step;
+        }
+        __syncthreads();
+        const float step = s_step;
+        const long long vbase = WRITE ? P.nvw + (long long)P.vb[li] : 0;
+        const long long fbase = WRITE ? (long long)P.fb[li] : 0;
+        int rings = 0;
+        for (;;) {
+            // centroid of the current ring: one sequential sum per coordinate, in loop order
+            if (tid < 3) {
+                const float* a = tid == 0 ? ax : tid == 1 ? ay : az;
+                float c = 0.0f;
+                for (int k = 0; k < n; ++k) c += a[k];
+                s_c[tid] = c / (float)n;
+            }
+            if (tid == 0) s_far = 0.0f;
+            __syncthreads();
+            const float cx = s_c[0], cy = s_c[1], cz = s_c[2];
+            if (n <= 4) break;
+            float far = 0.0f;
+            for (int k = tid; k < n; k += blockDim.x) {
+                const float dx = cx - ax[k], dy = cy - ay[k], dz = cz - az[k];
+                far = fmaxf(far, sqrtf(dx * dx + dy * dy + dz * dz));
+            }
+            for (int d = 16; d > 0; d >>= 1) far = fmaxf(far, __shfl_xor_sync(0xffffffffu, far, d));
+            if ((tid & 31) == 0) atomicMax(reinterpret_cast<int*>(&s_far), __float_as_int(far));   // far >= 0
+            __syncthreads();
+            if (s_far <= 1.25f * step) break;
+            if (rings >= kMaxRings) {
+                if (tid == 0) atomicOr(&P.C->err, kPostRingGuard);
+                break;
+            }
+            ++rings;
+            for (int k = tid; k < n; k += blockDim.x) {
+                const float px = ax[k], py = ay[k], pz = az[k];
+                float dx = cx - px, dy = cy - py, dz = cz - pz;
+                const float d = sqrtf(dx * dx + dy * dy + dz * dz);
+                const float move = d > step ? step : d * 0.5f;
+                if (d > 0.0001f) { dx /= d; dy /= d; dz /= d; }
+                else { dx = 0.0f; dy = 0.0f; dz = 0.0f; }
+                bx[k] = px + dx * move; by[k] = py + dy * move; bz[k] = pz + dz * move;
+                if (WRITE) {
+                    const long long g = vbase - P.nvw + (long long)(rings - 1) * n + k;
+                    P.fillV[3 * g] = bx[k]; P.fillV[3 * g + 1] = by[k]; P.fillV[3 * g + 2] = bz[k];
+                    const int k1 = k + 1 == n ? 0 : k + 1;
+                    const long long prev = rings == 1 ? -1 : vbase + (long long)(rings - 2) * n;
+                    const int o0 = prev < 0 ? idx[k] : (int)(prev + k), o1 = prev < 0 ? idx[k1] : (int)(prev + k1);
+                    const int i0 = (int)(vbase + (long long)(rings - 1) * n + k), i1 = (int)(vbase + (long long)(rings - 1) * n + k1);
+                    P.fillF[fbase + (long long)(rings - 1) * n + k] = make_int4(o0, o1, i1, i0);
+                }
+            }
+            __syncthreads();
+            float* t;
+            t = ax; ax = bx; bx = t;
+            t = ay; ay = by; by = t;
+            t = az; az = bz; bz = t;
+        }
+        // the rest: a triangle, a quad or a fan around the centroid of the last ring
+        if (WRITE) {
+            const long long cur = rings == 0 ? -1 : vbase + (long long)(rings - 1) * n;
+            auto ring_index = [&](int k) { return cur < 0 ? idx[k] : (int)(cur + k); };
+            const long long f0 = fbase + (long long)rings * n;
+            if (n == 3) {
+                if (tid == 0) P.fillF[f0] = make_int4(ring_index(0), ring_index(1), ring_index(2), ring_index(2));
+            } else if (n == 4) {
+                if (tid == 0) P.fillF[f0] = make_int4(ring_index(0), ring_index(1), ring_index(2), ring_index(3));
+            } else {
+                const int center = (int)(vbase + (long long)rings * n);
+                if (tid == 0) {
+                    const long long g = center - P.nvw;
+                    P.fillV[3 * g] = s_c[0]; P.fillV[3 * g + 1] = s_c[1]; P.fillV[3 * g + 2] = s_c[2];
+                }
+                for (int k = tid; k < n; k += blockDim.x)
+                    P.fillF[f0 + k] = make_int4(ring_index(k), ring_index(k + 1 == n ? 0 : k + 1), center, center);
+            }
+        } else if (tid == 0) {
+            P.nvl[li] = (unsigned long long)rings * n + (n > 4 ? 1 : 0);
+            P.nfl[li] = (unsigned long long)rings * n + (n > 4 ? n : 1);
+        }
+        __syncthreads();
+        ax = sh; ay = ax + kMaxLoop; az = ay + kMaxLoop; bx = az + kMaxLoop; by = bx + kMaxLoop; bz = by + kMaxLoop;
+    }
+}
+
+__global__ void k_fill_totals(const unsigned long long* vb, const unsigned long long* nvl, const unsigned long long* fb,
+                              const unsigned long long* nfl, long long n, PostCounters* C) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        C->fill_v = n ? vb[n - 1] + nvl[n - 1] : 0;
+        C->fill_f = n ? fb[n - 1] + nfl[n - 1] : 0;
+    }
+}
+
+// ---------------------------------------------------------------- renumber by first use
+struct FaceList {                        // kept faces, then the fill's faces
+    const int4* kept;
+    long long nkept;
+    const int4* fill;
+    __device__ __forceinline__ int at(long long p) const {
+        const long long f = p >> 2;
+        const int4 q = f < nkept ? kept[f] : fill[f - nkept];
+        return corner(q, (int)(p & 3));
+    }
+};
+
+__global__ void k_first_use(FaceList A, long long n, unsigned int* first) {
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x)
+        atomicMin(&first[A.at(p)], (unsigned int)p);
+}
+
+__global__ void k_first_flags(FaceList A, long long n, const unsigned int* __restrict__ first, unsigned int* flag) {
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x)
+        flag[p] = first[A.at(p)] == (unsigned int)p ? 1u : 0u;
+}
+
+__global__ void k_renumber(FaceList A, long long n, const unsigned int* __restrict__ first,
+                           const unsigned int* __restrict__ flag, const unsigned int* __restrict__ slot,
+                           const float* __restrict__ Vw, long long nvw, const float* __restrict__ fillV,
+                           float* outV, int32_t* outF, PostCounters* C) {
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+        const int v = A.at(p);
+        outF[p] = (int32_t)slot[first[v]];
+        if (flag[p]) {
+            const float* src = v < nvw ? Vw + 3 * (long long)v : fillV + 3 * ((long long)v - nvw);
+            const long long o = 3 * (long long)slot[p];
+            outV[o] = src[0]; outV[o + 1] = src[1]; outV[o + 2] = src[2];
+        }
+        if (p == n - 1) C->nout = slot[p] + flag[p];
+    }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- host side
+namespace {
+
+cudaError_t grow(PostBuf& b, size_t bytes) {
+    if (bytes <= b.bytes && b.p) return cudaSuccess;
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.bytes = 0;
+    const size_t want = std::max<size_t>(256, (bytes + 255) & ~(size_t)255);
+    cudaError_t e = cudaMalloc(&b.p, want);
+    if (e != cudaSuccess) { cudaGetLastError(); return e; }
+    b.bytes = want;
+    return cudaSuccess;
+}
+
+template <class T> T* as(PostBuf& b) { return reinterpret_cast<T*>(b.p); }
+
+int bits_for(long long n) {   // bits to hold 0..n-1
+    int b = 1;
+    while (b < 31 && (1LL << b) < n) ++b;
+    return b;
+}
+
+#define PP_TRY(x) do { cudaError_t e_ = (x); if (e_ != cudaSuccess) { R.what = #x; return e_; } } while (0)
+
+cudaError_t read_counters(PostWork& W, PostRun& R, cudaStream_t s) {
+    PP_TRY(cudaMemcpyAsync(W.hcount, W.count.p, sizeof(PostCounters), cudaMemcpyDeviceToHost, s));
+    PP_TRY(cudaStreamSynchronize(s));
+    return cudaSuccess;
+}
+
+const PostCounters& host_counters(const PostWork& W) { return *reinterpret_cast<const PostCounters*>(W.hcount); }
+
+// Weld V (nv) / F (nf quads) into Vout / Fout. Returns the welded counts.
+cudaError_t weld(PostWork& W, PostRun& R, const float* V, long long nv, const int32_t* F, long long nf, PostBuf& Vout,
+                 PostBuf& Fout, long long& nvw, long long& nfw, int sms, cudaStream_t s) {
+    PostCounters* C = as<PostCounters>(W.count);
+    PP_TRY(grow(W.key, sizeof(unsigned long long) * nv));
+    PP_TRY(grow(W.key2, sizeof(unsigned long long) * nv));
+    PP_TRY(grow(W.val, sizeof(int) * nv));
+    PP_TRY(grow(W.val2, sizeof(int) * nv));
+    PP_TRY(grow(W.u0, sizeof(unsigned int) * nv));
+    PP_TRY(grow(W.u1, sizeof(unsigned int) * nv));
+    PP_TRY(grow(W.u2, sizeof(unsigned int) * nv));
+    PP_TRY(grow(W.u3, sizeof(unsigned int) * nv));
+    PP_TRY(grow(W.ft, sizeof(int4) * nf));
+    PP_TRY(grow(W.flag8, nf));
+    PP_TRY(grow(Vout, sizeof(float) * 3 * nv));
+    PP_TRY(grow(Fout, sizeof(int4) * nf));
+    size_t t0 = 0, t1 = 0, t2 = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, t0, (unsigned long long*)nullptr, (unsigned long long*)nullptr, (int*)nullptr,
+                                    (int*)nullptr, (int)nv, 0, 3 * kKeyBits, s);
+    cub::DeviceScan::ExclusiveSum(nullptr, t1, (unsigned int*)nullptr, (unsigned int*)nullptr, (int)nv, s);
+    cub::DeviceSelect::Flagged(nullptr, t2, (int4*)nullptr, (unsigned char*)nullptr, (int4*)nullptr,
+                               (unsigned long long*)nullptr, (int)nf, s);
+    const size_t tb = std::max(t0, std::max(t1, t2));
+    PP_TRY(grow(W.cub, tb));
+    const unsigned g = grid_for(nv, kThreads, sms);
+    k_post_reset<<<1, 32, 0, s>>>(C);
+    k_bbox<<<g, kThreads, 0, s>>>(V, nv, C);
+    k_weld_params<<<1, 32, 0, s>>>(C);
+    k_weld_keys<<<g, kThreads, 0, s>>>(V, nv, C, as<unsigned long long>(W.key), as<int>(W.val));
+    PP_TRY(cudaGetLastError());
+    size_t tt = W.cub.bytes;
+    PP_TRY(cub::DeviceRadixSort::SortPairs(W.cub.p, tt, as<unsigned long long>(W.key), as<unsigned long long>(W.key2),
+                                           as<int>(W.val), as<int>(W.val2), (int)nv, 0, 3 * kKeyBits, s));
+    k_weld_heads<<<g, kThreads, 0, s>>>(as<unsigned long long>(W.key2), as<int>(W.val2), nv, as<unsigned int>(W.u0),
+                                        as<unsigned int>(W.u1));
+    tt = W.cub.bytes;
+    PP_TRY(cub::DeviceScan::ExclusiveSum(W.cub.p, tt, as<unsigned int>(W.u1), as<unsigned int>(W.u2), (int)nv, s));
+    tt = W.cub.bytes;
+    PP_TRY(cub::DeviceScan::InclusiveSum(W.cub.p, tt, as<unsigned int>(W.u0), as<unsigned int>(W.u3), (int)nv, s));
+    // u0 head, u3 group (1-based), u2 new index of representatives; u1 -> group's new index
+    k_weld_groups<<<g, kThreads, 0, s>>>(as<int>(W.val2), as<unsigned int>(W.u0), as<unsigned int>(W.u3),
+                                         as<unsigned int>(W.u2), V, nv, as<unsigned int>(W.u1), as<float>(Vout), C);
+    k_weld_remap<<<g, kThreads, 0, s>>>(as<int>(W.val2), as<unsigned int>(W.u3), as<unsigned int>(W.u1), nv,
+                                        as<int>(W.val));
+    k_weld_faces<<<grid_for(nf, kThreads, sms), kThreads, 0, s>>>(F, nf, nv, as<int>(W.val), as<int4>(W.ft),
+                                                                   as<unsigned char>(W.flag8), C);
+    PP_TRY(cudaGetLastError());
+    tt = W.cub.bytes;
+    PP_TRY(cub::DeviceSelect::Flagged(W.cub.p, tt, as<int4>(W.ft), as<unsigned char>(W.flag8), as<int4>(Fout),
+                                      &C->nsel, (int)nf, s));
+    cudaError_t e = read_counters(W, R, s);
+    if (e != cudaSuccess) return e;
+    nvw = (long long)host_counters(W).nvw;
+    nfw = (long long)host_counters(W).nsel;
+    return cudaSuccess;
+}
+
+}  // namespace
+
+void post_release(PostWork& W) {
+    PostBuf* all[] = {&W.count, &W.key, &W.key2, &W.val, &W.val2, &W.u0, &W.u1, &W.u2, &W.u3, &W.ft, &W.flag8, &W.cub,
+                      &W.Vw, &W.Fw, &W.kept, &W.parent, &W.csize, &W.bnd, &W.deg, &W.bot, &W.top, &W.pos, &W.vparent,
+                      &W.skey, &W.sdeg, &W.shead, &W.soff, &W.sgid, &W.stack, &W.lverts, &W.lflag, &W.lkey, &W.llen,
+                      &W.lpos, &W.lorder, &W.lkey2, &W.nvl, &W.nfl, &W.vb, &W.fb, &W.fillV, &W.fillF, &W.first,
+                      &W.fflag, &W.slot, &W.V1, &W.F1, &W.outV, &W.outF};
+    for (PostBuf* b : all) {
+        if (b->p) cudaFree(b->p);
+        b->p = nullptr;
+        b->bytes = 0;
+    }
+    if (W.hcount) cudaFreeHost(W.hcount);
+    W.hcount = nullptr;
+}
+
+cudaError_t post_run(PostWork& W, PostRun& R, cudaStream_t s) {
+    std::memset(R.stats, 0, sizeof(R.stats));
+    R.err = 0;
+    R.out_V = nullptr;
+    R.out_F = nullptr;
+    R.nv_out = R.nf_out = 0;
+    const long long nv = R.nv, nf = R.nf;
+    const int sms = R.num_sms;
+    if (!W.hcount) PP_TRY(cudaMallocHost(&W.hcount, sizeof(PostCounters)));
+    PP_TRY(grow(W.count, sizeof(PostCounters)));
+    PP_TRY(cudaMemsetAsync(W.count.p, 0, sizeof(PostCounters), s));
+    PostCounters* C = as<PostCounters>(W.count);
+    auto passthrough = [&]() {
+        R.out_V = R.V;
+        R.out_F = R.F;
+        R.nv_out = nv;
+        R.nf_out = nf;
+        R.stats[kPostVertexCount] = nv;
+        R.stats[kPostFaceCount] = nf;
+        return cudaSuccess;
+    };
+    if (nv == 0 || nf == 0 || (!R.close_holes && !R.remove_floaters)) return passthrough();
+
+    long long nvw = 0, nfw = 0;
+    cudaError_t e = weld(W, R, R.V, nv, R.F, nf, W.Vw, W.Fw, nvw, nfw, sms, s);
+    if (e != cudaSuccess) return e;
+    R.err = host_counters(W).err;
+    if (R.err) return cudaSuccess;
+    R.stats[kPostWeldedVertices] = nvw;
+    R.stats[kPostWeldedFaces] = nfw;
+    if (nvw == 0 || nfw == 0) return passthrough();
+
+    // edges: uses sorted by undirected key; runs -> boundary edges and face unions
+    const int b = bits_for(nvw);
+    const long long ne = 4 * nfw;
+    const unsigned long long inval = (b >= 32) ? ~0ull : ((1ull << (2 * b)) - 1);
+    PP_TRY(grow(W.key, sizeof(unsigned long long) * ne));
+    PP_TRY(grow(W.key2, sizeof(unsigned long long) * ne));
+    PP_TRY(grow(W.val, sizeof(int) * ne));
+    PP_TRY(grow(W.val2, sizeof(int) * ne));
+    PP_TRY(grow(W.bnd, sizeof(int4) * ne));
+    PP_TRY(grow(W.parent, sizeof(int) * nfw));
+    PP_TRY(grow(W.csize, sizeof(unsigned int) * nfw));
+    PP_TRY(grow(W.kept, sizeof(int4) * nfw));
+    PP_TRY(grow(W.flag8, nfw));
+    {
+        size_t t0 = 0, t1 = 0;
+        cub::DeviceRadixSort::SortPairs(nullptr, t0, (unsigned long long*)nullptr, (unsigned long long*)nullptr,
+                                        (int*)nullptr, (int*)nullptr, (int)ne, 0, 2 * b, s);
+        cub::DeviceSelect::Flagged(nullptr, t1, (int4*)nullptr, (unsigned char*)nullptr, (int4*)nullptr,
+                                   (unsigned long long*)nullptr, (int)nfw, s);
+        PP_TRY(grow(W.cub, std::max(t0, t1)));
+    }
+    const int4* Fw = as<int4>(W.Fw);
+    k_edge_uses<<<grid_for(ne, kThreads, sms), kThreads, 0, s>>>(Fw, nfw, b, as<unsigned long long>(W.key), as<int>(W.val));
+    size_t tt = W.cub.bytes;
+    PP_TRY(cub::DeviceRadixSort::SortPairs(W.cub.p, tt, as<unsigned long long>(W.key), as<unsigned long long>(W.key2),
+                                           as<int>(W.val), as<int>(W.val2), (int)ne, 0, 2 * b, s));
+    if (R.remove_floaters) {
+        k_iota<<<grid_for(nfw, kThreads, sms), kThreads, 0, s>>>(as<int>(W.parent), nfw);
+        PP_TRY(cudaMemsetAsync(W.csize.p, 0, sizeof(unsigned int) * nfw, s));
+    }
+    EdgeRunParams ep;
+    ep.key = as<unsigned long long>(W.key2); ep.val = as<int>(W.val2); ep.n = ne; ep.invalid = inval; ep.Fw = Fw;
+    ep.close = R.close_holes; ep.remove = R.remove_floaters; ep.parent = as<int>(W.parent); ep.bnd = as<int4>(W.bnd);
+    ep.C = C;
+    k_edge_runs<<<grid_for(ne, kThreads, sms), kThreads, 0, s>>>(ep);
+    PP_TRY(cudaGetLastError());
+    long long nkept = nfw;
+    const int4* kept = Fw;
+    if (R.remove_floaters) {
+        k_flatten<<<grid_for(nfw, kThreads, sms), kThreads, 0, s>>>(as<int>(W.parent), nfw);
+        k_comp_size<<<grid_for(nfw, kThreads, sms), kThreads, 0, s>>>(as<int>(W.parent), nfw, as<unsigned int>(W.csize));
+        k_comp_pick<<<grid_for(nfw, kThreads, sms), kThreads, 0, s>>>(as<int>(W.parent), as<unsigned int>(W.csize), nfw, C);
+        k_keep_flags<<<grid_for(nfw, kThreads, sms), kThreads, 0, s>>>(as<int>(W.parent), nfw, C, as<unsigned char>(W.flag8));
+        PP_TRY(cudaGetLastError());
+        PP_TRY(cudaMemsetAsync(&C->nsel, 0, sizeof(unsigned long long), s));
+        tt = W.cub.bytes;
+        PP_TRY(cub::DeviceSelect::Flagged(W.cub.p, tt, Fw, as<unsigned char>(W.flag8), as<int4>(W.kept), &C->nsel,
+                                          (int)nfw, s));
+        kept = as<int4>(W.kept);
+    }
+    e = read_counters(W, R, s);
+    if (e != cudaSuccess) return e;
+    {
+        const PostCounters& h = host_counters(W);
+        R.err = h.err;
+        if (R.err) return cudaSuccess;
+        if (R.remove_floaters) nkept = (long long)h.nsel;
+        R.stats[kPostComponents] = R.remove_floaters ? (long long)h.ncomp : 0;
+        R.stats[kPostKeptFaces] = nkept;
+        R.stats[kPostBoundaryEdges] = (long long)h.nb;
+    }
+    const long long nb = (long long)host_counters(W).nb;
+
+    // holes
+    long long nloops = 0, fill_v = 0, fill_f = 0;
+    if (R.close_holes && nb > 0) {
+        PP_TRY(grow(W.deg, sizeof(unsigned int) * nvw));
+        PP_TRY(grow(W.bot, sizeof(unsigned int) * nvw));
+        PP_TRY(grow(W.top, sizeof(unsigned int) * nvw));
+        PP_TRY(grow(W.pos, sizeof(int) * nvw));
+        PP_TRY(grow(W.vparent, sizeof(int) * nvw));
+        PP_TRY(cudaMemsetAsync(W.deg.p, 0, sizeof(unsigned int) * nvw, s));
+        PP_TRY(cudaMemsetAsync(W.pos.p, 0xff, sizeof(int) * nvw, s));
+        k_bnd_keys<<<grid_for(nb, kThreads, sms), kThreads, 0, s>>>(as<int4>(W.bnd), nb, as<int>(W.parent),
+                                                                     R.remove_floaters, b, as<unsigned long long>(W.key),
+                                                                     as<unsigned int>(W.deg), C);
+        size_t t0 = 0, t1 = 0;
+        cub::DeviceRadixSort::SortKeys(nullptr, t0, (unsigned long long*)nullptr, (unsigned long long*)nullptr, (int)nb,
+                                       0, 2 * b, s);
+        cub::DeviceScan::ExclusiveSum(nullptr, t1, (unsigned int*)nullptr, (unsigned int*)nullptr, (int)nvw, s);
+        PP_TRY(grow(W.cub, std::max(t0, t1)));
+        tt = W.cub.bytes;
+        PP_TRY(cub::DeviceRadixSort::SortKeys(W.cub.p, tt, as<unsigned long long>(W.key), as<unsigned long long>(W.key2),
+                                              (int)nb, 0, 2 * b, s));
+        tt = W.cub.bytes;
+        PP_TRY(cub::DeviceScan::ExclusiveSum(W.cub.p, tt, as<unsigned int>(W.deg), as<unsigned int>(W.bot), (int)nvw, s));
+        e = read_counters(W, R, s);
+        if (e != cudaSuccess) return e;
+        const long long nbk = (long long)host_counters(W).nbk;
+        if (nbk > 0) {
+            // top = bot + deg; weak components of the boundary graph
+            k_iota<<<grid_for(nvw, kThreads, sms), kThreads, 0, s>>>(as<int>(W.vparent), nvw);
+            k_bnd_unite<<<grid_for(nbk, kThreads, sms), kThreads, 0, s>>>(as<unsigned long long>(W.key2), nbk, b,
+                                                                           as<int>(W.vparent), C);
+            k_flatten<<<grid_for(nvw, kThreads, sms), kThreads, 0, s>>>(as<int>(W.vparent), nvw);
+            PP_TRY(grow(W.skey, sizeof(unsigned long long) * nvw));
+            PP_TRY(grow(W.lkey2, sizeof(unsigned long long) * std::max(nvw, nbk)));
+            k_start_keys<<<grid_for(nvw, kThreads, sms), kThreads, 0, s>>>(as<unsigned int>(W.deg), as<int>(W.vparent),
+                                                                            nvw, b, as<unsigned long long>(W.skey), C);
+            PP_TRY(cudaGetLastError());
+            e = read_counters(W, R, s);
+            if (e != cudaSuccess) return e;
+            const long long ns = (long long)host_counters(W).nstarts;
+            {
+                size_t ta = 0, tb2 = 0, tc = 0;
+                cub::DeviceRadixSort::SortKeys(nullptr, ta, (unsigned long long*)nullptr, (unsigned long long*)nullptr,
+                                               (int)ns, 0, 2 * b, s);
+                cub::DeviceScan::ExclusiveSum(nullptr, tb2, (unsigned long long*)nullptr, (unsigned long long*)nullptr,
+                                              (int)ns, s);
+                cub::DeviceScan::InclusiveSum(nullptr, tc, (unsigned int*)nullptr, (unsigned int*)nullptr, (int)ns, s);
+                PP_TRY(grow(W.cub, std::max(ta, std::max(tb2, tc))));
+            }
+            tt = W.cub.bytes;
+            PP_TRY(cub::DeviceRadixSort::SortKeys(W.cub.p, tt, as<unsigned long long>(W.skey),
+                                                  as<unsigned long long>(W.lkey2), (int)ns, 0, 2 * b, s));
+            PP_TRY(grow(W.sdeg, sizeof(unsigned long long) * ns));
+            PP_TRY(grow(W.shead, sizeof(unsigned int) * ns));
+            PP_TRY(grow(W.soff, sizeof(unsigned long long) * ns));
+            PP_TRY(grow(W.sgid, sizeof(unsigned int) * ns));
+            k_start_info<<<grid_for(ns, kThreads, sms), kThreads, 0, s>>>(as<unsigned long long>(W.lkey2), ns, b,
+                                                                          as<unsigned int>(W.deg),
+                                                                          as<unsigned long long>(W.sdeg),
+                                                                          as<unsigned int>(W.shead));
+            tt = W.cub.bytes;
+            PP_TRY(cub::DeviceScan::ExclusiveSum(W.cub.p, tt, as<unsigned long long>(W.sdeg), as<unsigned long long>(W.soff),
+                                                 (int)ns, s));
+            tt = W.cub.bytes;
+            PP_TRY(cub::DeviceScan::InclusiveSum(W.cub.p, tt, as<unsigned int>(W.shead), as<unsigned int>(W.sgid), (int)ns, s));
+            k_tops<<<grid_for(nvw, kThreads, sms), kThreads, 0, s>>>(as<unsigned int>(W.bot), as<unsigned int>(W.deg), nvw,
+                                                                     as<unsigned int>(W.top));
+            PP_TRY(grow(W.stack, sizeof(int) * (nbk + ns + 1)));
+            PP_TRY(grow(W.lverts, sizeof(int) * nbk));
+            PP_TRY(grow(W.lflag, nbk));
+            PP_TRY(grow(W.lkey, sizeof(unsigned long long) * nbk));
+            PP_TRY(grow(W.llen, sizeof(int) * nbk));
+            PP_TRY(cudaMemsetAsync(W.lflag.p, 0, nbk, s));
+            WalkParams wp;
+            wp.skey = as<unsigned long long>(W.lkey2); wp.nstarts = ns; wp.shead = as<unsigned int>(W.shead);
+            wp.soff = as<unsigned long long>(W.soff); wp.sgid = as<unsigned int>(W.sgid); wp.b = b;
+            wp.adj = as<unsigned long long>(W.key2); wp.bot = as<unsigned int>(W.bot); wp.top = as<unsigned int>(W.top);
+            wp.pos = as<int>(W.pos); wp.stack = as<int>(W.stack); wp.lverts = as<int>(W.lverts);
+            wp.lflag = as<unsigned char>(W.lflag); wp.lkey = as<unsigned long long>(W.lkey); wp.llen = as<int>(W.llen);
+            wp.C = C;
+            k_walk<<<grid_for(ns, 64, sms), 64, 0, s>>>(wp);
+            PP_TRY(cudaGetLastError());
+            // the recorded loops in fill order
+            PP_TRY(grow(W.lpos, sizeof(int) * nbk));
+            PP_TRY(grow(W.lorder, sizeof(int) * nbk));
+            {
+                size_t ta = 0;
+                cub::DeviceSelect::Flagged(nullptr, ta, thrust::counting_iterator<int>(0), (unsigned char*)nullptr,
+                                           (int*)nullptr, (unsigned long long*)nullptr, (int)nbk, s);
+                PP_TRY(grow(W.cub, ta));
+            }
+            PP_TRY(cudaMemsetAsync(&C->nsel, 0, sizeof(unsigned long long), s));
+            tt = W.cub.bytes;
+            PP_TRY(cub::DeviceSelect::Flagged(W.cub.p, tt, thrust::counting_iterator<int>(0), as<unsigned char>(W.lflag),
+                                              as<int>(W.lpos), &C->nsel, (int)nbk, s));
+            e = read_counters(W, R, s);
+            if (e != cudaSuccess) return e;
+            R.err = host_counters(W).err;
+            if (R.err) return cudaSuccess;
+            nloops = (long long)host_counters(W).nloops;
+            R.stats[kPostLoopsFound] = (long long)host_counters(W).loops_found;
+            R.stats[kPostLoopsFilled] = nloops;
+        }
+    }
+    if (nloops > 0) {
+        PP_TRY(grow(W.key, sizeof(unsigned long long) * nloops));
+        k_gather_keys<<<grid_for(nloops, kThreads, sms), kThreads, 0, s>>>(as<int>(W.lpos), as<unsigned long long>(W.lkey),
+                                                                            nloops, as<unsigned long long>(W.key));
+        {
+            size_t ta = 0, tb2 = 0;
+            cub::DeviceRadixSort::SortPairs(nullptr, ta, (unsigned long long*)nullptr, (unsigned long long*)nullptr,
+                                            (int*)nullptr, (int*)nullptr, (int)nloops, 0, 64, s);
+            cub::DeviceScan::ExclusiveSum(nullptr, tb2, (unsigned long long*)nullptr, (unsigned long long*)nullptr,
+                                          (int)nloops, s);
+            PP_TRY(grow(W.cub, std::max(ta, tb2)));
+        }
+        PP_TRY(grow(W.lkey2, sizeof(unsigned long long) * nloops));
+        tt = W.cub.bytes;
+        PP_TRY(cub::DeviceRadixSort::SortPairs(W.cub.p, tt, as<unsigned long long>(W.key), as<unsigned long long>(W.lkey2),
+                                               as<int>(W.lpos), as<int>(W.lorder), (int)nloops, 0, 64, s));
+        PP_TRY(grow(W.nvl, sizeof(unsigned long long) * nloops));
+        PP_TRY(grow(W.nfl, sizeof(unsigned long long) * nloops));
+        PP_TRY(grow(W.vb, sizeof(unsigned long long) * nloops));
+        PP_TRY(grow(W.fb, sizeof(unsigned long long) * nloops));
+        FillParams fp;
+        fp.lorder = as<int>(W.lorder); fp.nloops = nloops; fp.lverts = as<int>(W.lverts); fp.llen = as<int>(W.llen);
+        fp.Vw = as<float>(W.Vw); fp.nvw = nvw; fp.nvl = as<unsigned long long>(W.nvl); fp.nfl = as<unsigned long long>(W.nfl);
+        fp.vb = as<unsigned long long>(W.vb); fp.fb = as<unsigned long long>(W.fb); fp.fillV = nullptr; fp.fillF = nullptr;
+        fp.C = C;
+        const size_t smem = sizeof(float) * 7 * kMaxLoop;
+        PP_TRY(cudaFuncSetAttribute(k_fill<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        PP_TRY(cudaFuncSetAttribute(k_fill<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        const unsigned fg = (unsigned)std::min<long long>(nloops, (long long)sms * 2);
+        k_fill<false><<<fg, kFillThreads, smem, s>>>(fp);
+        PP_TRY(cudaGetLastError());
+        tt = W.cub.bytes;
+        PP_TRY(cub::DeviceScan::ExclusiveSum(W.cub.p, tt, as<unsigned long long>(W.nvl), as<unsigned long long>(W.vb),
+                                             (int)nloops, s));
+        tt = W.cub.bytes;
+        PP_TRY(cub::DeviceScan::ExclusiveSum(W.cub.p, tt, as<unsigned long long>(W.nfl), as<unsigned long long>(W.fb),
+                                             (int)nloops, s));
+        k_fill_totals<<<1, 32, 0, s>>>(as<unsigned long long>(W.vb), as<unsigned long long>(W.nvl),
+                                       as<unsigned long long>(W.fb), as<unsigned long long>(W.nfl), nloops, C);
+        e = read_counters(W, R, s);
+        if (e != cudaSuccess) return e;
+        R.err = host_counters(W).err;
+        if (R.err) return cudaSuccess;
+        fill_v = (long long)host_counters(W).fill_v;
+        fill_f = (long long)host_counters(W).fill_f;
+        if (nvw + fill_v >= 0x7fffffffLL || 4 * (nkept + fill_f) >= 0x7fffffffLL) {   // int item counts
+            R.too_large = 1;
+            return cudaSuccess;
+        }
+        PP_TRY(grow(W.fillV, sizeof(float) * 3 * std::max(1LL, fill_v)));
+        PP_TRY(grow(W.fillF, sizeof(int4) * std::max(1LL, fill_f)));
+        fp.fillV = as<float>(W.fillV);
+        fp.fillF = as<int4>(W.fillF);
+        k_fill<true><<<fg, kFillThreads, smem, s>>>(fp);
+        PP_TRY(cudaGetLastError());
+        R.stats[kPostFillVertices] = fill_v;
+        R.stats[kPostFillFaces] = fill_f;
+    }
+
+    // renumber by first use
+    const long long nall = nvw + fill_v;
+    const long long nA = 4 * (nkept + fill_f);
+    PP_TRY(grow(W.first, sizeof(unsigned int) * nall));
+    PP_TRY(grow(W.fflag, sizeof(unsigned int) * nA));
+    PP_TRY(grow(W.slot, sizeof(unsigned int) * nA));
+    PostBuf& dstV = R.close_holes ? W.V1 : W.outV;
+    PostBuf& dstF = R.close_holes ? W.F1 : W.outF;
+    PP_TRY(grow(dstV, sizeof(float) * 3 * nall));
+    PP_TRY(grow(dstF, sizeof(int32_t) * nA));
+    {
+        size_t ta = 0;
+        cub::DeviceScan::ExclusiveSum(nullptr, ta, (unsigned int*)nullptr, (unsigned int*)nullptr, (int)nA, s);
+        PP_TRY(grow(W.cub, ta));
+    }
+    FaceList A;
+    A.kept = kept; A.nkept = nkept; A.fill = as<int4>(W.fillF);
+    PP_TRY(cudaMemsetAsync(W.first.p, 0xff, sizeof(unsigned int) * nall, s));
+    k_first_use<<<grid_for(nA, kThreads, sms), kThreads, 0, s>>>(A, nA, as<unsigned int>(W.first));
+    k_first_flags<<<grid_for(nA, kThreads, sms), kThreads, 0, s>>>(A, nA, as<unsigned int>(W.first), as<unsigned int>(W.fflag));
+    tt = W.cub.bytes;
+    PP_TRY(cub::DeviceScan::ExclusiveSum(W.cub.p, tt, as<unsigned int>(W.fflag), as<unsigned int>(W.slot), (int)nA, s));
+    k_renumber<<<grid_for(nA, kThreads, sms), kThreads, 0, s>>>(A, nA, as<unsigned int>(W.first), as<unsigned int>(W.fflag),
+                                                                 as<unsigned int>(W.slot), as<float>(W.Vw), nvw,
+                                                                 as<float>(W.fillV), as<float>(dstV), as<int32_t>(dstF), C);
+    PP_TRY(cudaGetLastError());
+    e = read_counters(W, R, s);
+    if (e != cudaSuccess) return e;
+    long long nvo = (long long)host_counters(W).nout, nfo = nA / 4;
+    if (R.close_holes) {
+        long long nv2 = 0, nf2 = 0;
+        e = weld(W, R, as<float>(W.V1), nvo, as<int32_t>(W.F1), nfo, W.outV, W.outF, nv2, nf2, sms, s);
+        if (e != cudaSuccess) return e;
+        R.err = host_counters(W).err;
+        if (R.err) return cudaSuccess;
+        nvo = nv2;
+        nfo = nf2;
+    }
+    R.out_V = as<float>(W.outV);
+    R.out_F = as<int32_t>(W.outF);
+    R.nv_out = nvo;
+    R.nf_out = nfo;
+    R.stats[kPostVertexCount] = nvo;
+    R.stats[kPostFaceCount] = nfo;
+    return cudaSuccess;
+}
+
+}  // namespace dcb
