@@ -603,6 +603,76 @@ def run_sparse_workload(args):
     return 0
 
 
+def run_post_workload(args):
+    """The mesh post-pass (postprocess_mesh, src/cpp/dc_backend.cpp:217-558, dc_cli's
+    --close-holes / --remove-floaters) on meshes this engine extracts at --res (1024^3 unless
+    given): the CSG scene (floaters, grid-cut holes) and a sphere larger than the grid (six
+    large holes, each filled ring by ring). Device time per call (CUDA events; the call reads
+    counts back to size its outputs), host mesh -> host mesh wall clock, and the reference's own
+    postprocess_mesh (built from its source into oracle/_ref/; the oracle's restatement when
+    absent) on the same host mesh, once, with the GPU output compared to it bit for bit."""
+    import numpy as np
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O          # the reference's own CPU post-pass: the comparator
+    from contouring_b200 import B200DualContouringBackend, DualContouringMesh, postprocess_mesh, postprocess_mesh_tensor
+    from contouring_b200 import synth
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    res = args.res
+    scenes = [("csg%d" % res, lambda: make_grid(res, dev))]
+
+    def cut_sphere():
+        dims, sp, org = synth._grid_params(res, -0.5, 0.5)
+        vals = synth._eval_slabs(dims, sp, org, lambda q: (q - torch.tensor([0.05, 0.0, 0.0], device=q.device)).norm(dim=-1) - 0.6, dev)
+        return vals, dims, sp, org
+    scenes.append(("cut_sphere%d" % res, cut_sphere))
+    be = B200DualContouringBackend(device=0)
+    for name, make in scenes:
+        vals, dims, sp, org = make()
+        V, F, _ = be.extract_tensor(vals, dims, sp, org)
+        del vals
+        torch.cuda.synchronize()
+        ms_dev = _timed(lambda: postprocess_mesh_tensor(be, V, F, True, True), args.steps, args.warmup)
+        Vo, Fo, st = postprocess_mesh_tensor(be, V, F, True, True)
+        Vh = V.cpu().numpy()
+        Fh = F.cpu().numpy()
+        mesh = DualContouringMesh(Vh.reshape(-1), Fh.reshape(-1))
+        walls = []
+        for i in range(max(1, min(args.e2e_steps, 3)) + 1):
+            t0 = time.perf_counter()
+            out = postprocess_mesh(mesh, True, True, backend=be)
+            if i:
+                walls.append((time.perf_counter() - t0) * 1e3)
+        ms_e2e = statistics.median(walls)
+        t0 = time.perf_counter()
+        r = O.ref_postprocess_mesh(Vh, Fh, True, True)
+        kind = "reference"
+        if r is None:
+            r = O.postprocess_mesh(Vh, Fh, True, True)[:2]
+            kind = "port"
+        ms_ref = (time.perf_counter() - t0) * 1e3
+        identical = (r[0].shape == tuple(Vo.shape) and r[1].shape == tuple(Fo.shape)
+                     and bool(np.array_equal(r[0].view(np.uint32), Vo.cpu().numpy().view(np.uint32)))
+                     and bool(np.array_equal(r[1], Fo.cpu().numpy())))
+        nf = int(F.shape[0])
+        h2d = int(Vh.nbytes + Fh.nbytes)
+        d2h = int(np.asarray(out.vertices).nbytes + np.asarray(out.faces).nbytes)
+        _side_line("post_mquads_per_s", nf / (ms_dev / 1e3) / 1e6, "Mquads/s", ms_dev, args,
+                   {"workload": "postprocess_%s_close_holes_remove_floaters" % name, "grid": list(dims),
+                    "input_vertices": int(V.shape[0]), "input_quads": nf},
+                   stats=st.as_dict(),
+                   e2e={"value": round(nf / (ms_e2e / 1e3) / 1e6, 3), "unit": "Mquads/s", "ms_per_step": round(ms_e2e, 3),
+                        "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+                   cpu_baseline={"value": round(nf / (ms_ref / 1e3) / 1e6, 3), "unit": "Mquads/s", "cores": 1,
+                                 "kind": kind, "sample": "the whole mesh, once", "ms": round(ms_ref, 1)},
+                   identical_to_reference=identical,
+                   speedup_e2e_vs_reference=round(ms_ref / ms_e2e, 2))
+        del V, F, Vo, Fo
+    be.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -614,11 +684,13 @@ def main():
     ap.add_argument("--ref-zslab", type=int, default=96, help="point planes per CPU sample (over 8 slabs)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-sequential", action="store_true", help="batch256: skip the one-by-one comparison")
-    ap.add_argument("--workload", default="csg1024", choices=["csg1024", "batch256", "adjoint128", "ours128", "mesh512", "refcuda512", "sparse1024"],
+    ap.add_argument("--workload", default="csg1024", choices=["csg1024", "batch256", "adjoint128", "ours128", "mesh512", "refcuda512", "sparse1024",
+                             "post1024"],
                     help="side workloads (not the headline): batch256 = 256 uneven CSG grids batched vs one "
                          "by one; adjoint128 = forward + adjoint; ours128 = the full refinement; mesh512 = "
                          "mesh_to_sdf; refcuda512 = the reference's CUDA backend vs this engine at 512^3; "
-                         "sparse1024 = the sparse and multi-vertex backends vs the reference's at --res")
+                         "sparse1024 = the sparse and multi-vertex backends vs the reference's at --res; "
+                         "post1024 = the mesh post-pass on meshes extracted at --res vs the reference's")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -640,6 +712,8 @@ def main():
         return run_refcuda_workload(args)
     if args.workload == "sparse1024":
         return run_sparse_workload(args)
+    if args.workload == "post1024":
+        return run_post_workload(args)
 
     import numpy as np
     import torch

@@ -100,13 +100,15 @@ __device__ __forceinline__ int uf_find(int* parent, int x) {
 }
 
 __device__ void uf_unite(int* parent, int a, int b, int* err) {
-    int ra = uf_find(parent, a), rb = uf_find(parent, b);
-    for (int guard = 0; ra != rb; ++guard) {
+    int ra = a, rb = b;
+    for (int guard = 0;; ++guard) {
         if (guard > (1 << 24)) { atomicOr(err, kPostWalkGuard); return; }
+        ra = uf_find(parent, ra);
+        rb = uf_find(parent, rb);
+        if (ra == rb) return;
         if (ra < rb) { const int t = ra; ra = rb; rb = t; }
-        const int old = atomicCAS(&parent[ra], ra, rb);
-        if (old == ra) return;
-        ra = old;   // ra was linked meanwhile: continue from its new parent
+        if (atomicCAS(&parent[ra], ra, rb) == ra) return;
+        // ra was linked meanwhile: both roots are found again from where they are
     }
 }
 
@@ -152,8 +154,14 @@ __global__ void k_bbox(const float* __restrict__ V, long long nv, PostCounters* 
             hi[a] = max(hi[a], __shfl_xor_sync(0xffffffffu, hi[a], d));
         }
     if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(&C->err, kPostNonFinite);
+    __shared__ unsigned int s_box[6];
+    if (threadIdx.x < 6) s_box[threadIdx.x] = threadIdx.x < 3 ? 0xffffffffu : 0u;
+    __syncthreads();
     if ((threadIdx.x & 31) == 0)
-        for (int a = 0; a < 3; ++a) { atomicMin(&C->box[a], lo[a]); atomicMax(&C->box[3 + a], hi[a]); }
+        for (int a = 0; a < 3; ++a) { atomicMin(&s_box[a], lo[a]); atomicMax(&s_box[3 + a], hi[a]); }
+    __syncthreads();
+    if (threadIdx.x < 3) atomicMin(&C->box[threadIdx.x], s_box[threadIdx.x]);
+    else if (threadIdx.x < 6) atomicMax(&C->box[threadIdx.x], s_box[threadIdx.x]);
 }
 
 // The weld step: eps = |box diagonal| * 1e-5 (1e-5 for a point), in the reference's order.
@@ -293,9 +301,36 @@ __global__ void k_edge_runs(EdgeRunParams P) {
     }
 }
 
+// Faces per root. Components are large: each thread counts runs of one root and adds a run
+// when the root changes; the last runs are added once per distinct root in the warp.
+// Before the unions: every face of a two-use edge points at the smaller face of the pair (the
+// smallest such neighbour wins). Each link is an edge of the face graph and points to a smaller
+// index, so this is already a valid union-find forest, and most of it is flat.
+__global__ void k_first_links(EdgeRunParams P) {
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < P.n; p += (long long)gridDim.x * blockDim.x) {
+        const unsigned long long k = P.key[p];
+        if ((k & P.invalid) == P.invalid || (p > 0 && P.key[p - 1] == k)) continue;
+        if (p + 1 >= P.n || P.key[p + 1] != k || (p + 2 < P.n && P.key[p + 2] == k)) continue;
+        const int a = P.val[p] >> 2, b = P.val[p + 1] >> 2;
+        if (a != b) atomicMin(&P.parent[max(a, b)], min(a, b));
+    }
+}
+
 __global__ void k_comp_size(const int* __restrict__ root, long long n, unsigned int* size) {
-    for (long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x; f < n; f += (long long)gridDim.x * blockDim.x)
-        atomicAdd(&size[root[f]], 1u);
+    int cur = -1;
+    unsigned int run = 0;
+    for (long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x; f < n; f += (long long)gridDim.x * blockDim.x) {
+        const int r = root[f];
+        if (r != cur) {
+            if (run) atomicAdd(&size[cur], run);
+            cur = r;
+            run = 0;
+        }
+        ++run;
+    }
+    const unsigned int peers = __match_any_sync(0xffffffffu, cur);
+    const unsigned int total = __reduce_add_sync(peers, run);
+    if (run && cur >= 0 && (threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&size[cur], total);
 }
 
 __global__ void k_comp_pick(const int* __restrict__ root, const unsigned int* __restrict__ size, long long n, PostCounters* C) {
@@ -359,6 +394,7 @@ struct WalkParams {
     const unsigned long long* adj;      // sorted boundary keys: from << b | to
     const unsigned int* bot;            // first adjacency entry of every vertex
     unsigned int* top;                  // one past its last unused entry
+    const int* succ;                    // the target of a vertex's only edge, else -1
     int* pos;                           // position on the current path, -1 when off it
     int* stack;                         // per component: out-degree sum + 1 entries
     int* lverts;                        // per component: out-degree sum entries
@@ -396,7 +432,8 @@ __global__ void k_walk(WalkParams P) {
                 while (P.top[at] > P.bot[at]) {
                     if (++guard > (1LL << 31)) { atomicOr(&P.C->err, kPostWalkGuard); return; }
                     const unsigned int t = --P.top[at];
-                    const int next = (int)(P.adj[t] & m);
+                    const int only = P.succ[at];
+                    const int next = only >= 0 ? only : (int)(P.adj[t] & m);
                     if (next == s) { closed = true; break; }
                     const int hit = P.pos[next];
                     if (hit >= 0) {
@@ -439,10 +476,15 @@ __global__ void k_walk(WalkParams P) {
     }
 }
 
-__global__ void k_tops(const unsigned int* __restrict__ bot, const unsigned int* __restrict__ deg, long long n,
-                       unsigned int* top) {
-    for (long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x; u < n; u += (long long)gridDim.x * blockDim.x)
+// One past every vertex's last outgoing edge, and its successor when it has exactly one (the
+// walk then needs one dependent load per step instead of two).
+__global__ void k_tops(const unsigned int* __restrict__ bot, const unsigned int* __restrict__ deg,
+                       const unsigned long long* __restrict__ adj, int b, long long n, unsigned int* top, int* succ) {
+    const unsigned long long m = (1ull << b) - 1;
+    for (long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x; u < n; u += (long long)gridDim.x * blockDim.x) {
         top[u] = bot[u] + deg[u];
+        succ[u] = deg[u] == 1 ? (int)(adj[bot[u]] & m) : -1;
+    }
 }
 
 __global__ void k_gather_keys(const int* __restrict__ lpos, const unsigned long long* __restrict__ lkey, long long n,
@@ -466,6 +508,30 @@ struct FillParams {
     int4* fillF;                        // new faces
     PostCounters* C;
 };
+
+// ((a[0] + a[1]) + a[2]) + ... in float, as a sequential loop rounds it: the additions stay in
+// order, one dependent chain; the shared-memory loads of the next eight are issued before the
+// eight additions of the current ones, so the chain does not wait on them (a is 16-byte aligned).
+__device__ __forceinline__ float ordered_sum(const float* a, int n) {
+    float c = 0.0f;
+    int k = 0;
+    if (n >= 16) {
+        float4 u = *reinterpret_cast<const float4*>(a);
+        float4 v = *reinterpret_cast<const float4*>(a + 4);
+        for (k = 8; k + 8 <= n; k += 8) {
+            const float4 u2 = *reinterpret_cast<const float4*>(a + k);
+            const float4 v2 = *reinterpret_cast<const float4*>(a + k + 4);
+            c += u.x; c += u.y; c += u.z; c += u.w;
+            c += v.x; c += v.y; c += v.z; c += v.w;
+            u = u2;
+            v = v2;
+        }
+        c += u.x; c += u.y; c += u.z; c += u.w;
+        c += v.x; c += v.y; c += v.z; c += v.w;
+    }
+    for (; k < n; ++k) c += a[k];
+    return c;
+}
 
 // One loop per block: rings towards the centroid (dc_backend.cpp:376-466). Shared memory holds
 // two rings (x, y, z arrays) and one scratch array of kMaxLoop floats each.
@@ -497,8 +563,7 @@ __global__ void __launch_bounds__(kFillThreads) k_fill(FillParams P) {
         }
         __syncthreads();
         if (tid == 0) {
-            float step = 0.0f;
-            for (int k = 0; k < n; ++k) step += sd[k];
+            float step = ordered_sum(sd, n);
             step /= (float)n;
             if (step <= 0.0001f) step = 1.0f;
             s_step = step;
@@ -510,12 +575,7 @@ __global__ void __launch_bounds__(kFillThreads) k_fill(FillParams P) {
         int rings = 0;
         for (;;) {
             // centroid of the current ring: one sequential sum per coordinate, in loop order
-            if (tid < 3) {
-                const float* a = tid == 0 ? ax : tid == 1 ? ay : az;
-                float c = 0.0f;
-                for (int k = 0; k < n; ++k) c += a[k];
-                s_c[tid] = c / (float)n;
-            }
+            if (tid < 3) s_c[tid] = ordered_sum(tid == 0 ? ax : tid == 1 ? ay : az, n) / (float)n;
             if (tid == 0) s_far = 0.0f;
             __syncthreads();
             const float cx = s_c[0], cy = s_c[1], cz = s_c[2];
@@ -730,7 +790,7 @@ void post_release(PostWork& W) {
                       &W.Vw, &W.Fw, &W.kept, &W.parent, &W.csize, &W.bnd, &W.deg, &W.bot, &W.top, &W.pos, &W.vparent,
                       &W.skey, &W.sdeg, &W.shead, &W.soff, &W.sgid, &W.stack, &W.lverts, &W.lflag, &W.lkey, &W.llen,
                       &W.lpos, &W.lorder, &W.lkey2, &W.nvl, &W.nfl, &W.vb, &W.fb, &W.fillV, &W.fillF, &W.first,
-                      &W.fflag, &W.slot, &W.V1, &W.F1, &W.outV, &W.outF};
+                      &W.fflag, &W.slot, &W.V1, &W.F1, &W.outV, &W.outF, &W.succ};
     for (PostBuf* b : all) {
         if (b->p) cudaFree(b->p);
         b->p = nullptr;
@@ -806,6 +866,7 @@ cudaError_t post_run(PostWork& W, PostRun& R, cudaStream_t s) {
     ep.key = as<unsigned long long>(W.key2); ep.val = as<int>(W.val2); ep.n = ne; ep.invalid = inval; ep.Fw = Fw;
     ep.close = R.close_holes; ep.remove = R.remove_floaters; ep.parent = as<int>(W.parent); ep.bnd = as<int4>(W.bnd);
     ep.C = C;
+    if (R.remove_floaters) k_first_links<<<grid_for(ne, kThreads, sms), kThreads, 0, s>>>(ep);
     k_edge_runs<<<grid_for(ne, kThreads, sms), kThreads, 0, s>>>(ep);
     PP_TRY(cudaGetLastError());
     long long nkept = nfw;
@@ -900,8 +961,10 @@ cudaError_t post_run(PostWork& W, PostRun& R, cudaStream_t s) {
                                                  (int)ns, s));
             tt = W.cub.bytes;
             PP_TRY(cub::DeviceScan::InclusiveSum(W.cub.p, tt, as<unsigned int>(W.shead), as<unsigned int>(W.sgid), (int)ns, s));
-            k_tops<<<grid_for(nvw, kThreads, sms), kThreads, 0, s>>>(as<unsigned int>(W.bot), as<unsigned int>(W.deg), nvw,
-                                                                     as<unsigned int>(W.top));
+            PP_TRY(grow(W.succ, sizeof(int) * nvw));
+            k_tops<<<grid_for(nvw, kThreads, sms), kThreads, 0, s>>>(as<unsigned int>(W.bot), as<unsigned int>(W.deg),
+                                                                     as<unsigned long long>(W.key2), b, nvw,
+                                                                     as<unsigned int>(W.top), as<int>(W.succ));
             PP_TRY(grow(W.stack, sizeof(int) * (nbk + ns + 1)));
             PP_TRY(grow(W.lverts, sizeof(int) * nbk));
             PP_TRY(grow(W.lflag, nbk));
@@ -912,6 +975,7 @@ cudaError_t post_run(PostWork& W, PostRun& R, cudaStream_t s) {
             wp.skey = as<unsigned long long>(W.lkey2); wp.nstarts = ns; wp.shead = as<unsigned int>(W.shead);
             wp.soff = as<unsigned long long>(W.soff); wp.sgid = as<unsigned int>(W.sgid); wp.b = b;
             wp.adj = as<unsigned long long>(W.key2); wp.bot = as<unsigned int>(W.bot); wp.top = as<unsigned int>(W.top);
+            wp.succ = as<int>(W.succ);
             wp.pos = as<int>(W.pos); wp.stack = as<int>(W.stack); wp.lverts = as<int>(W.lverts);
             wp.lflag = as<unsigned char>(W.lflag); wp.lkey = as<unsigned long long>(W.lkey); wp.llen = as<int>(W.llen);
             wp.C = C;
