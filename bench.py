@@ -34,7 +34,7 @@ KERNELS_PER_STEP = 16
 # profiles/k_mark_zmarch_csg512.md (dram__bytes_read.sum + dram__bytes_write.sum divided by
 # the grid points of that capture; the kernel streams the grid once, so traffic scales with
 # the number of points). None = not measured.
-MARK_TRAFFIC_BYTES_PER_POINT = (554.966272e6 + 19.405056e6) / 512 ** 3
+MARK_TRAFFIC_BYTES_PER_POINT = (563.814656e6 + 18.4768e6) / 512 ** 3
 
 
 def max_over_ranks(local, dist, device):

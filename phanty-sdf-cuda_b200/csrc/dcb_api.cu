@@ -77,7 +77,7 @@ struct dcb_context {
     void* hF = nullptr; size_t hF_bytes = 0;
     int64_t nv = 0, nf = 0;           // vertices; output faces (quads or triangles)
     int vpf = 4;                      // output vertices per face
-    int mark_ctas[2] = {0, 0};        // resident mark CTAs per SM (scalar, float4 loads)
+    int mark_ctas[2] = {0, 0};        // resident mark CTAs per SM: batch, single grid
     // mark tiling (dcb_autotune_mark): CTAs per resident mark slot, and the widest grid
     // (cells along x) that marches 256-cell x-tiles instead of 1024-cell ones
     int tune_waves = 4;
@@ -170,9 +170,9 @@ float elapsed(cudaEvent_t a, cudaEvent_t b) {
 struct BatchLayout {
     std::vector<GridSlot> slots;
     std::vector<long long> seg_off, col_off;          // n + 1
-    // mark launches: index vec4 + 2 * narrow (scalar/float4 loads x 1024/256-cell tiles)
-    std::vector<int> tile_slot[4];                    // grids of each mark launch
-    std::vector<long long> tile_off[4];               // their first tiles (+ total)
+    // mark launches: index 1 for 256-cell x-tiles, 0 for 1024-cell ones
+    std::vector<int> tile_slot[2];                    // grids of each mark launch
+    std::vector<long long> tile_off[2];               // their first tiles (+ total)
     long long bits = 0, super = 0, nseg = 0, ncol = 0, ncell = 0;
     float hmax = 0.f;
 };
@@ -181,7 +181,7 @@ int layout_batch(dcb_context* h, const dcb_grid* in, int n, BatchLayout& L) {
     L.slots.resize(n);
     L.seg_off.assign(n + 1, 0);
     L.col_off.assign(n + 1, 0);
-    for (int v = 0; v < 4; ++v) { L.tile_slot[v].clear(); L.tile_off[v].assign(1, 0); }
+    for (int v = 0; v < 2; ++v) { L.tile_slot[v].clear(); L.tile_off[v].assign(1, 0); }
     for (int b = 0; b < n; ++b) {
         GridSlot& S = L.slots[b];
         GridDesc& g = S.g;
@@ -193,7 +193,6 @@ int layout_batch(dcb_context* h, const dcb_grid* in, int n, BatchLayout& L) {
         g.ox = in[b].ox; g.oy = in[b].oy; g.oz = in[b].oz;
         g.v = in[b].values;
         const long long rows = (long long)g.cy * g.cz;
-        S.vec4 = (g.nx % 4 == 0 && (reinterpret_cast<uintptr_t>(g.v) % 16) == 0) ? 1 : 0;
         // grids at most 256 cells wide march 256-cell x-tiles (less idle width)
         S.tw = g.cx <= h->tune_narrow_cells ? mark_narrow_tile_words() : mark_tile_words();
         S.nxt = (g.cx + 32 * S.tw - 1) / (32 * S.tw);
@@ -201,8 +200,8 @@ int layout_batch(dcb_context* h, const dcb_grid* in, int n, BatchLayout& L) {
         S.nrb = (g.cy + S.R - 1) / S.R;
         // About four CTAs per resident slot, each marching 8..64 planes (a single long wave
         // measured slower at 1024^3: 0.887 vs 0.848 ms).
-        if (h->mark_ctas[S.vec4] == 0) h->mark_ctas[S.vec4] = mark_ctas_per_sm(S.vec4);
-        const long long slots = (long long)h->num_sms * h->mark_ctas[S.vec4] * h->tune_waves;
+        if (h->mark_ctas[n == 1] == 0) h->mark_ctas[n == 1] = mark_ctas_per_sm(n == 1);
+        const long long slots = (long long)h->num_sms * h->mark_ctas[n == 1] * h->tune_waves;
         S.KZ = (int)std::max(8LL, std::min(64LL, (g.cz * S.nxt * (long long)S.nrb + slots - 1) / slots));
         S.nzc = (g.cz + S.KZ - 1) / S.KZ;
         S.bits_off = L.bits;
@@ -216,7 +215,7 @@ int layout_batch(dcb_context* h, const dcb_grid* in, int n, BatchLayout& L) {
         L.nseg += rows * S.nxt;
         L.ncol += 3LL * g.cx * g.cy;
         L.ncell += (long long)g.cx * rows;
-        const int grp = S.vec4 + 2 * (S.tw == mark_narrow_tile_words() ? 1 : 0);
+        const int grp = S.tw == mark_narrow_tile_words() ? 1 : 0;
         L.tile_slot[grp].push_back(b);
         L.tile_off[grp].push_back(L.tile_off[grp].back() + (long long)S.nxt * S.nrb * S.nzc);
         S.hmax = std::max(std::fabs(g.vx), std::max(std::fabs(g.vy), std::fabs(g.vz)));
@@ -224,7 +223,7 @@ int layout_batch(dcb_context* h, const dcb_grid* in, int n, BatchLayout& L) {
     }
     L.seg_off[n] = L.nseg;
     L.col_off[n] = L.ncol;
-    for (int v = 0; v < 4; ++v)
+    for (int v = 0; v < 2; ++v)
         if (L.tile_off[v].back() > 0x7fffffffLL) return fail(h, DCB_ERR_TOO_LARGE, "grid too large for the tiling");
     if (L.nseg >= 0xffffffffLL || L.ncol >= 0xffffffffLL) return fail(h, DCB_ERR_TOO_LARGE, "batch too large");
     return DCB_OK;
@@ -235,8 +234,8 @@ struct TableView {
     BatchTable B;
     unsigned long long* vert_off;
     unsigned long long* face_off;
-    const int* tile_slot[4];
-    const long long* tile_off[4];
+    const int* tile_slot[2];
+    const long long* tile_off[2];
 };
 
 size_t align_up(size_t x) { return (x + 255) & ~size_t(255); }
@@ -273,10 +272,10 @@ int upload_table(dcb_context* h, const BatchLayout& L, cudaStream_t s, TableView
     const size_t o_col = align_up(o_seg + sizeof(long long) * (n + 1));
     const size_t o_vert = align_up(o_col + sizeof(long long) * (n + 1));
     const size_t o_face = align_up(o_vert + sizeof(unsigned long long) * (n + 1));
-    size_t o_ts[4], o_to[4];
+    size_t o_ts[2], o_to[2];
     size_t at = align_up(o_face + sizeof(unsigned long long) * (n + 1));
-    for (int v = 0; v < 4; ++v) { o_ts[v] = at; at = align_up(at + sizeof(int) * L.tile_slot[v].size() + 1); }
-    for (int v = 0; v < 4; ++v) { o_to[v] = at; at = align_up(at + sizeof(long long) * L.tile_off[v].size()); }
+    for (int v = 0; v < 2; ++v) { o_ts[v] = at; at = align_up(at + sizeof(int) * L.tile_slot[v].size() + 1); }
+    for (int v = 0; v < 2; ++v) { o_to[v] = at; at = align_up(at + sizeof(long long) * L.tile_off[v].size()); }
     const size_t total = at;
     DCB_TRY(h, ensure(h->table, total), "alloc batch table");
     DCB_TRY(h, ensure_host(h->h_table, h->h_table_bytes, total), "alloc pinned batch table");
@@ -284,7 +283,7 @@ int upload_table(dcb_context* h, const BatchLayout& L, cudaStream_t s, TableView
     std::memcpy(hb + o_slots, L.slots.data(), sizeof(GridSlot) * n);
     std::memcpy(hb + o_seg, L.seg_off.data(), sizeof(long long) * (n + 1));
     std::memcpy(hb + o_col, L.col_off.data(), sizeof(long long) * (n + 1));
-    for (int v = 0; v < 4; ++v) {
+    for (int v = 0; v < 2; ++v) {
         std::memcpy(hb + o_ts[v], L.tile_slot[v].data(), sizeof(int) * L.tile_slot[v].size());
         std::memcpy(hb + o_to[v], L.tile_off[v].data(), sizeof(long long) * L.tile_off[v].size());
     }
@@ -299,7 +298,7 @@ int upload_table(dcb_context* h, const BatchLayout& L, cudaStream_t s, TableView
     T.face_off = reinterpret_cast<unsigned long long*>(db + o_face);
     T.B.vert_off = T.vert_off;
     T.B.cell_slot = nullptr;
-    for (int v = 0; v < 4; ++v) {
+    for (int v = 0; v < 2; ++v) {
         T.tile_slot[v] = reinterpret_cast<const int*>(db + o_ts[v]);
         T.tile_off[v] = reinterpret_cast<const long long*>(db + o_to[v]);
     }
@@ -308,13 +307,13 @@ int upload_table(dcb_context* h, const BatchLayout& L, cudaStream_t s, TableView
 
 // The mark launches of a batch (one per group of grids with the same load width and tile).
 int launch_marks(dcb_context* h, const BatchLayout& L, const TableView& T, cudaStream_t s) {
-    for (int v = 0; v < 4; ++v) {
+    for (int v = 0; v < 2; ++v) {
         if (L.tile_slot[v].empty()) continue;
         MarkParams mp;
         mp.B = T.B; mp.tile_slot = T.tile_slot[v]; mp.tile_off = T.tile_off[v];
         mp.m = (int)L.tile_slot[v].size(); mp.ntiles = L.tile_off[v].back();
         mp.bits = as<uint32_t>(h->bits); mp.seg_count = as<uint32_t>(h->seg_count);
-        DCB_TRY(h, launch_mark(mp, v & 1, (v & 2) ? mark_narrow_tile_words() : mark_tile_words(), s), "launch mark");
+        DCB_TRY(h, launch_mark(mp, v ? mark_narrow_tile_words() : mark_tile_words(), s), "launch mark");
     }
     return DCB_OK;
 }

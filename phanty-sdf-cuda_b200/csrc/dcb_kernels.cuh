@@ -20,7 +20,6 @@ struct GridSlot {
     int nxt;                       // mark: x-tiles of 1024 cells per row
     int nrb;                       // mark: row blocks
     int nzc;                       // mark: z-chunks
-    int vec4;                      // rows are 16-byte aligned and nx % 4 == 0
     int tw;                        // mark: cell words per x-tile (32, or 8 for narrow grids)
     float hmax;                    // largest cell width of the grid (world units)
 };
@@ -71,10 +70,10 @@ struct MarkParams {
     uint32_t* bits;                // all grids' active bits
     uint32_t* seg_count;           // all grids' segment counts
 };
-cudaError_t launch_mark(const MarkParams& P, int vec4, int tw, cudaStream_t s);
+cudaError_t launch_mark(const MarkParams& P, int tw, cudaStream_t s);
 int mark_tile_words();
 int mark_narrow_tile_words();
-int mark_ctas_per_sm(int vec4);   // resident CTAs of the mark kernel per SM
+int mark_ctas_per_sm(bool one);   // resident CTAs of the mark kernel per SM (single grid / batch)
 int mark_max_rows();
 
 struct ExpandParams {

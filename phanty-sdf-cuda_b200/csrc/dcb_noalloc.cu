@@ -109,8 +109,6 @@ extern "C" int dcb_mark_active_cells_noalloc(const dcb_grid* grid, int64_t* cell
     slot.nrb = (g.cy + slot.R - 1) / slot.R;
     slot.KZ = (int)std::max(8LL, std::min(64LL, ((long long)g.cz * nxt * slot.nrb + (long long)sms * 12 - 1) / ((long long)sms * 12)));
     slot.nzc = (g.cz + slot.KZ - 1) / slot.KZ;
-    const uintptr_t vaddr = reinterpret_cast<uintptr_t>(g.v);
-    slot.vec4 = (g.nx % 4 == 0 && (vaddr % 16) == 0) ? 1 : 0;
     const long long ntiles = (long long)nxt * slot.nrb * slot.nzc;
     if (ntiles > 0x7fffffffLL) return DCB_ERR_TOO_LARGE;
     Table ht;
@@ -149,7 +147,7 @@ extern "C" int dcb_mark_active_cells_noalloc(const dcb_grid* grid, int64_t* cell
     mp.B = B; mp.tile_slot = dt->tile_slot; mp.tile_off = dt->tile_off; mp.m = 1; mp.ntiles = ntiles;
     mp.bits = reinterpret_cast<uint32_t*>(sb + off_bits);
     mp.seg_count = reinterpret_cast<uint32_t*>(sb + off_count);
-    if (launch_mark(mp, slot.vec4, slot.tw, s) != cudaSuccess) { cudaGetLastError(); return DCB_ERR_CUDA; }
+    if (launch_mark(mp, slot.tw, s) != cudaSuccess) { cudaGetLastError(); return DCB_ERR_CUDA; }
     uint32_t* seg_start = reinterpret_cast<uint32_t*>(sb + off_start);
     if (launch_scan(mp.seg_count, nseg, reinterpret_cast<uint32_t*>(sb + off_part), seg_start, total, s) != cudaSuccess) {
         cudaGetLastError();
