@@ -426,7 +426,7 @@ struct PostWork {
     PostBuf Vw, Fw, kept, parent, csize, bnd;
     PostBuf deg, bot, top, pos, vparent, skey, sdeg, shead, soff, sgid, stack, lverts, lflag, lkey, llen;
     PostBuf lpos, lorder, lkey2, nvl, nfl, vb, fb, fillV, fillF;
-    PostBuf first, fflag, slot, V1, F1, outV, outF, succ;
+    PostBuf first, fflag, slot, V1, F1, outV, outF, succ, indeg, cbad, clen, cbase, crank, jflags;
     void* hcount = nullptr;             // page-locked copy of the device counters
 };
 

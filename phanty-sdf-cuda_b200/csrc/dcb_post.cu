@@ -46,6 +46,7 @@ constexpr int kMaxLoop = 4096;          // loops longer than this are not filled
 constexpr int kMaxRings = 8192;         // a fill that has not converged by then is reported
 constexpr int kFillThreads = 256;
 constexpr int kKeyBits = 17;            // per axis in the weld key
+constexpr int kRankRounds = 32;         // pointer-jumping rounds: enough for cycles of 2^31 vertices
 
 enum PostErr { kPostBadIndex = 1, kPostNonFinite = 2, kPostWeldSpan = 4, kPostWalkGuard = 8, kPostRingGuard = 16 };
 
@@ -366,6 +367,104 @@ __global__ void k_bnd_unite(const unsigned long long* __restrict__ key, long lon
         uf_unite(parent, (int)(key[t] >> b), (int)(key[t] & m), &C->err);
 }
 
+// ---- boundary components that are simple cycles (every vertex one edge out, one in): the
+// reference's walk from the component's smallest vertex s just follows the cycle back to s, so
+// the loop is the cycle from s. Each vertex's place on it comes from list ranking (pointer
+// jumping on (distance, next) pairs), in parallel, instead of a sequential walk.
+__global__ void k_cycle_indeg(const unsigned long long* __restrict__ key, long long n, int b,
+                              const unsigned int* __restrict__ deg, const int* __restrict__ root, unsigned int* indeg,
+                              unsigned int* bad) {
+    const unsigned long long m = (1ull << b) - 1;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const unsigned int v = (unsigned int)(key[t] & m);
+        atomicAdd(&indeg[v], 1u);
+        if (!deg[v]) atomicOr(&bad[root[v]], 1u);    // a sink: the walk ends there
+    }
+}
+
+// Over the vertices with outgoing edges (the sorted starts): bad[root] when one lacks exactly
+// one edge in and one out (sinks were marked with the in-degrees); len[root]: vertex count.
+__global__ void k_cycle_marks(const unsigned long long* __restrict__ skey, long long ns, int b,
+                              const unsigned int* __restrict__ deg, const unsigned int* __restrict__ indeg,
+                              const int* __restrict__ root, unsigned int* bad, unsigned int* len) {
+    const unsigned long long m = (1ull << b) - 1;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < ns; p += (long long)gridDim.x * blockDim.x) {
+        const unsigned int u = (unsigned int)(skey[p] & m);
+        if (deg[u] != 1 || indeg[u] != 1) atomicOr(&bad[root[u]], 1u);
+        atomicAdd(&len[root[u]], 1u);
+    }
+}
+
+// (distance to the cycle's last vertex before s, next vertex or -1) packed as dist << 32 | next.
+__global__ void k_cycle_rank_init(const unsigned long long* __restrict__ skey, long long ns, int b,
+                                  const unsigned int* __restrict__ bad, const int* __restrict__ root,
+                                  const int* __restrict__ succ, unsigned long long* rank) {
+    const unsigned long long m = (1ull << b) - 1;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < ns; p += (long long)gridDim.x * blockDim.x) {
+        const unsigned int u = (unsigned int)(skey[p] & m);
+        if (bad[root[u]]) continue;
+        const int nx = succ[u];
+        rank[u] = nx == root[u] ? 0xffffffffull : ((1ull << 32) | (unsigned int)nx);
+    }
+}
+
+// One round of pointer jumping in place; a pair is read and written as one 64-bit word, so
+// (distance, next) always stays consistent. changed[r] records whether round r moved
+// anything; a round after one that moved nothing returns at once.
+__global__ void k_cycle_rank_jump(const unsigned long long* __restrict__ skey, long long ns, int b,
+                                  const unsigned int* __restrict__ bad, const int* __restrict__ root,
+                                  unsigned long long* rank, int* changed, int r) {
+    if (r > 0 && !changed[r - 1]) return;
+    const unsigned long long m = (1ull << b) - 1;
+    volatile unsigned long long* R = rank;
+    bool moved = false;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < ns; p += (long long)gridDim.x * blockDim.x) {
+        const unsigned int u = (unsigned int)(skey[p] & m);
+        if (bad[root[u]]) continue;
+        const unsigned long long me = R[u];
+        const unsigned int nx = (unsigned int)me;
+        if (nx == 0xffffffffu) continue;
+        const unsigned long long there = R[nx];
+        R[u] = (((me >> 32) + (there >> 32)) << 32) | (there & 0xffffffffull);
+        moved = true;
+    }
+    if (__any_sync(0xffffffffu, moved) && (threadIdx.x & 31) == 0) changed[r] = 1;
+}
+
+// The loop region of every component: base[root] = its first entry (the starts' scan).
+__global__ void k_cycle_bases(const unsigned long long* __restrict__ skey, const unsigned int* __restrict__ shead,
+                              const unsigned long long* __restrict__ soff, long long n, int b, unsigned long long* base) {
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x)
+        if (shead[p]) base[skey[p] >> b] = soff[p];
+}
+
+// Every cycle vertex writes itself into the reversed loop; s records the loop.
+__global__ void k_cycle_emit(const unsigned long long* __restrict__ skey, long long ns, int b,
+                             const unsigned int* __restrict__ bad, const int* __restrict__ root,
+                             const unsigned int* __restrict__ len, const unsigned long long* __restrict__ rank,
+                             const unsigned long long* __restrict__ base, int* lverts, unsigned char* lflag,
+                             unsigned long long* lkey, int* llen, PostCounters* C) {
+    const unsigned long long m = (1ull << b) - 1;
+    for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < ns; p += (long long)gridDim.x * blockDim.x) {
+        const unsigned int u = (unsigned int)(skey[p] & m);
+        const int s = root[u];
+        if (bad[s]) continue;
+        const unsigned int L = len[s];
+        const bool keep = L >= 3 && L <= (unsigned int)kMaxLoop;
+        const unsigned long long o = base[s];
+        if (keep) lverts[o + (rank[u] >> 32)] = (int)u;
+        if ((int)u == s) {
+            atomicAdd(&C->loops_found, 1ull);
+            if (keep) {
+                lflag[o] = 1;
+                lkey[o] = (unsigned long long)s << 32;
+                llen[o] = (int)L;
+                atomicAdd(&C->nloops, 1ull);
+            }
+        }
+    }
+}
+
 __global__ void k_start_keys(const unsigned int* __restrict__ deg, const int* __restrict__ root, long long nv, int b,
                              unsigned long long* key, PostCounters* C) {
     for (long long u = blockIdx.x * (long long)blockDim.x + threadIdx.x; u < nv; u += (long long)gridDim.x * blockDim.x) {
@@ -395,6 +494,7 @@ struct WalkParams {
     const unsigned int* bot;            // first adjacency entry of every vertex
     unsigned int* top;                  // one past its last unused entry
     const int* succ;                    // the target of a vertex's only edge, else -1
+    const unsigned int* cbad;           // per root: the component is not a simple cycle
     int* pos;                           // position on the current path, -1 when off it
     int* stack;                         // per component: out-degree sum + 1 entries
     int* lverts;                        // per component: out-degree sum entries
@@ -413,6 +513,7 @@ __global__ void k_walk(WalkParams P) {
         if (!P.shead[p0]) continue;
         const unsigned long long m = (1ull << P.b) - 1;
         const unsigned long long root = P.skey[p0] >> P.b;
+        if (!P.cbad[root]) continue;   // a simple cycle: placed by the ranking kernels
         long long p1 = p0 + 1;
         while (p1 < P.nstarts && (P.skey[p1] >> P.b) == root) ++p1;
         const unsigned long long base = P.soff[p0];
@@ -790,7 +891,8 @@ void post_release(PostWork& W) {
                       &W.Vw, &W.Fw, &W.kept, &W.parent, &W.csize, &W.bnd, &W.deg, &W.bot, &W.top, &W.pos, &W.vparent,
                       &W.skey, &W.sdeg, &W.shead, &W.soff, &W.sgid, &W.stack, &W.lverts, &W.lflag, &W.lkey, &W.llen,
                       &W.lpos, &W.lorder, &W.lkey2, &W.nvl, &W.nfl, &W.vb, &W.fb, &W.fillV, &W.fillF, &W.first,
-                      &W.fflag, &W.slot, &W.V1, &W.F1, &W.outV, &W.outF, &W.succ};
+                      &W.fflag, &W.slot, &W.V1, &W.F1, &W.outV, &W.outF, &W.succ, &W.indeg, &W.cbad, &W.clen,
+                      &W.cbase, &W.crank, &W.jflags};
     for (PostBuf* b : all) {
         if (b->p) cudaFree(b->p);
         b->p = nullptr;
@@ -965,17 +1067,55 @@ cudaError_t post_run(PostWork& W, PostRun& R, cudaStream_t s) {
             k_tops<<<grid_for(nvw, kThreads, sms), kThreads, 0, s>>>(as<unsigned int>(W.bot), as<unsigned int>(W.deg),
                                                                      as<unsigned long long>(W.key2), b, nvw,
                                                                      as<unsigned int>(W.top), as<int>(W.succ));
+            // simple cycles: degrees, marks, ranks
+            PP_TRY(grow(W.indeg, sizeof(unsigned int) * nvw));
+            PP_TRY(grow(W.cbad, sizeof(unsigned int) * nvw));
+            PP_TRY(grow(W.clen, sizeof(unsigned int) * nvw));
+            PP_TRY(grow(W.cbase, sizeof(unsigned long long) * nvw));
+            PP_TRY(grow(W.crank, sizeof(unsigned long long) * nvw));
+            PP_TRY(grow(W.jflags, sizeof(int) * kRankRounds));
+            PP_TRY(cudaMemsetAsync(W.indeg.p, 0, sizeof(unsigned int) * nvw, s));
+            PP_TRY(cudaMemsetAsync(W.cbad.p, 0, sizeof(unsigned int) * nvw, s));
+            PP_TRY(cudaMemsetAsync(W.clen.p, 0, sizeof(unsigned int) * nvw, s));
+            PP_TRY(cudaMemsetAsync(W.jflags.p, 0, sizeof(int) * kRankRounds, s));
+            const unsigned long long* starts = as<unsigned long long>(W.lkey2);
+            k_cycle_indeg<<<grid_for(nbk, kThreads, sms), kThreads, 0, s>>>(as<unsigned long long>(W.key2), nbk, b,
+                                                                             as<unsigned int>(W.deg), as<int>(W.vparent),
+                                                                             as<unsigned int>(W.indeg), as<unsigned int>(W.cbad));
+            k_cycle_marks<<<grid_for(ns, kThreads, sms), kThreads, 0, s>>>(starts, ns, b, as<unsigned int>(W.deg),
+                                                                            as<unsigned int>(W.indeg), as<int>(W.vparent),
+                                                                            as<unsigned int>(W.cbad), as<unsigned int>(W.clen));
+            k_cycle_rank_init<<<grid_for(ns, kThreads, sms), kThreads, 0, s>>>(starts, ns, b, as<unsigned int>(W.cbad),
+                                                                                as<int>(W.vparent), as<int>(W.succ),
+                                                                                as<unsigned long long>(W.crank));
+            for (int r = 0; r < kRankRounds; ++r)
+                k_cycle_rank_jump<<<grid_for(ns, kThreads, sms), kThreads, 0, s>>>(starts, ns, b, as<unsigned int>(W.cbad),
+                                                                                    as<int>(W.vparent),
+                                                                                    as<unsigned long long>(W.crank),
+                                                                                    as<int>(W.jflags), r);
+            k_cycle_bases<<<grid_for(ns, kThreads, sms), kThreads, 0, s>>>(as<unsigned long long>(W.lkey2),
+                                                                            as<unsigned int>(W.shead),
+                                                                            as<unsigned long long>(W.soff), ns, b,
+                                                                            as<unsigned long long>(W.cbase));
+            PP_TRY(cudaGetLastError());
             PP_TRY(grow(W.stack, sizeof(int) * (nbk + ns + 1)));
             PP_TRY(grow(W.lverts, sizeof(int) * nbk));
             PP_TRY(grow(W.lflag, nbk));
             PP_TRY(grow(W.lkey, sizeof(unsigned long long) * nbk));
             PP_TRY(grow(W.llen, sizeof(int) * nbk));
             PP_TRY(cudaMemsetAsync(W.lflag.p, 0, nbk, s));
+            k_cycle_emit<<<grid_for(ns, kThreads, sms), kThreads, 0, s>>>(starts, ns, b, as<unsigned int>(W.cbad),
+                                                                           as<int>(W.vparent), as<unsigned int>(W.clen),
+                                                                           as<unsigned long long>(W.crank),
+                                                                           as<unsigned long long>(W.cbase), as<int>(W.lverts),
+                                                                           as<unsigned char>(W.lflag),
+                                                                           as<unsigned long long>(W.lkey), as<int>(W.llen), C);
             WalkParams wp;
             wp.skey = as<unsigned long long>(W.lkey2); wp.nstarts = ns; wp.shead = as<unsigned int>(W.shead);
             wp.soff = as<unsigned long long>(W.soff); wp.sgid = as<unsigned int>(W.sgid); wp.b = b;
             wp.adj = as<unsigned long long>(W.key2); wp.bot = as<unsigned int>(W.bot); wp.top = as<unsigned int>(W.top);
             wp.succ = as<int>(W.succ);
+            wp.cbad = as<unsigned int>(W.cbad);
             wp.pos = as<int>(W.pos); wp.stack = as<int>(W.stack); wp.lverts = as<int>(W.lverts);
             wp.lflag = as<unsigned char>(W.lflag); wp.lkey = as<unsigned long long>(W.lkey); wp.llen = as<int>(W.llen);
             wp.C = C;
