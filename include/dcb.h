@@ -224,6 +224,19 @@ int dcb_read_sdf(const char* path, dcb_grid* header, float* values, int64_t capa
 /* The inverse of dcb_read_sdf (host values). */
 int dcb_write_sdf(const char* path, const dcb_grid* grid);
 
+/* Replaces the OBJ reading of dc_cli's read_obj_to_sdf (dc_cli.cpp:121-158): "v" lines, "f"
+ * lines with 1-based or negative indices (the leading integer of "v/vt/vn" tokens), polygons
+ * fanned into triangles. Sets *num_vertices and *num_triangles; with vertices and triangles
+ * NULL that is all, otherwise both arrays must hold the counts (DCB_ERR_TOO_LARGE if not).
+ * A file without vertices or faces, or with an index out of range, is DCB_ERR_INVALID_ARGUMENT. */
+int dcb_read_obj(const char* path, float* vertices, int64_t vertex_capacity, int32_t* triangles,
+                 int64_t triangle_capacity, int64_t* num_vertices, int64_t* num_triangles);
+
+/* The grid read_obj_to_sdf puts around a mesh (dc_cli.cpp:160-184): res points per axis over
+ * the bounding box grown by 8% of its diagonal on every side (0.1 for a single point);
+ * grid->values is set to NULL. The mesh -> SDF call then fills it (dcb_mesh_to_sdf_*_ex). */
+int dcb_obj_grid(const float* vertices, int64_t num_vertices, int res, dcb_grid* grid);
+
 /* ---- batches of grids ------------------------------------------------------------------- */
 
 /* The meshes of a batch, concatenated grid by grid in device memory. Grid b's vertices are

@@ -32,7 +32,8 @@ EXPORTED = (
     "dcb_extract_batch_device", "dcb_backward", "dcb_autotune_mark",
     "dcb_write_obj", "dcb_read_sdf", "dcb_write_sdf", "dcb_extract_upload", "dcb_mesh_to_sdf_device_ex",
     "dcb_mesh_to_sdf_host_ex", "dcb_batch_graph_create", "dcb_batch_graph_launch", "dcb_batch_graph_finish",
-    "dcb_batch_graph_destroy", "dcb_postprocess_device", "dcb_postprocess_host", "dcb_copy_post_mesh")
+    "dcb_batch_graph_destroy", "dcb_postprocess_device", "dcb_postprocess_host", "dcb_copy_post_mesh",
+    "dcb_read_obj", "dcb_obj_grid")
 
 
 class DcbGrid(ctypes.Structure):
@@ -138,6 +139,11 @@ def lib():
     L.dcb_read_sdf.restype = ctypes.c_int
     L.dcb_write_sdf.argtypes = [ctypes.c_char_p, P(DcbGrid)]
     L.dcb_write_sdf.restype = ctypes.c_int
+    L.dcb_read_obj.argtypes = [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64,
+                               P(ctypes.c_int64), P(ctypes.c_int64)]
+    L.dcb_read_obj.restype = ctypes.c_int
+    L.dcb_obj_grid.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_int, P(DcbGrid)]
+    L.dcb_obj_grid.restype = ctypes.c_int
     L.dcb_create.argtypes = [P(ctypes.c_void_p), ctypes.c_int]
     L.dcb_create.restype = ctypes.c_int
     L.dcb_destroy.argtypes = [ctypes.c_void_p]

@@ -1,7 +1,9 @@
 """The reference CLI's file formats (src/cpp/dc_cli.cpp:17-47) on the C ABI's native readers and
 writers: the binary ``.sdf`` grid and the OBJ mesh.
 
-``read_sdf`` returns a :class:`DenseSdfGrid` like the reference's ``read_sdf``; ``read_sdf_tensor``
+``read_sdf`` returns a :class:`DenseSdfGrid` like the reference's ``read_sdf``; ``read_obj`` /
+``obj_grid`` / ``read_obj_to_sdf`` are the CLI's OBJ -> SDF ingestion (dc_cli.cpp:121-203) with the
+conversion on the GPU; ``read_sdf_tensor``
 reads straight into pinned host memory and uploads it to a CUDA tensor for ``extract_tensor``
 (the torch path of ``extract_device``, src/cpp/bindings.cpp:223-227); ``write_obj`` formats the
 mesh in parallel slices with the reference's text (6 significant digits, 1-based indices)."""
@@ -77,3 +79,34 @@ def _host(a):
     if hasattr(a, "detach"):
         return a.detach().cpu().numpy()
     return np.asarray(a)
+
+
+def read_obj(path):
+    """The OBJ reading of ``read_obj_to_sdf`` (dc_cli.cpp:121-158): float32 vertices (N, 3) and
+    int32 triangles (M, 3) (polygons fanned from their first vertex)."""
+    L = _lib.lib()
+    nv, nt = ctypes.c_int64(), ctypes.c_int64()
+    _lib.check(L.dcb_read_obj(_path(path), None, 0, None, 0, ctypes.byref(nv), ctypes.byref(nt)))
+    V = np.empty((nv.value, 3), np.float32)
+    T = np.empty((nt.value, 3), np.int32)
+    _lib.check(L.dcb_read_obj(_path(path), V.ctypes.data, nv.value, T.ctypes.data, nt.value,
+                              ctypes.byref(nv), ctypes.byref(nt)))
+    return V, T
+
+
+def obj_grid(vertices, res):
+    """(dims, spacing, origin) of the grid ``read_obj_to_sdf`` puts around a mesh
+    (dc_cli.cpp:160-184): the bounding box grown by 8% of its diagonal, res points per axis."""
+    V = np.ascontiguousarray(_host(vertices), dtype=np.float32).reshape(-1)
+    g = _lib.DcbGrid()
+    _lib.check(_lib.lib().dcb_obj_grid(V.ctypes.data if V.size else None, V.size // 3, int(res), ctypes.byref(g)))
+    return (g.nx, g.ny, g.nz), (g.vx, g.vy, g.vz), (g.ox, g.oy, g.oz)
+
+
+def read_obj_to_sdf(backend, path, res, voxelize_first=False, voxel_res=256):
+    """``read_obj_to_sdf`` (dc_cli.cpp:121-203): the OBJ's signed distance grid, computed on the
+    GPU; returns ``(DenseSdfGrid, milliseconds of the conversion)``."""
+    from .backend import mesh_to_sdf_cuda
+    V, T = read_obj(path)
+    dims, sp, org = obj_grid(V, res)
+    return mesh_to_sdf_cuda(backend, V, T, *dims, *org, *sp, voxelize_first=voxelize_first, voxel_res=voxel_res)

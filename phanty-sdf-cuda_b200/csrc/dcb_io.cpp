@@ -5,8 +5,16 @@
 //
 // The OBJ text is formatted in parallel slices (one buffer per thread, written in order), so
 // a 10-million-vertex mesh does not serialise on one formatting loop.
+//
+// OBJ input follows the CLI's read_obj_to_sdf (dc_cli.cpp:121-203): "v " lines with three
+// floats, "f " lines whose tokens (split at blanks and tabs) give 1-based or negative
+// (relative) vertex indices by their leading integer ("7/2/5" is vertex 7), polygons fanned
+// into triangles from their first vertex; the grid around the mesh is its bounding box grown
+// by 8% of the box diagonal on every side, in the reference's float arithmetic.
+#include <cmath>
 #include <cstdint>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <thread>
@@ -36,9 +44,107 @@ void format_range(std::string& out, const float* V, int64_t v0, int64_t v1, cons
     }
 }
 
+struct ObjData {
+    std::vector<float> V;
+    std::vector<int32_t> T;     // triangles
+};
+
+// Parses the whole file; false when it cannot be read. Indices are not range-checked here.
+bool parse_obj(const char* path, ObjData& D) {
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return false;
+    std::string text;
+    char chunk[1 << 16];
+    size_t got;
+    while ((got = std::fread(chunk, 1, sizeof(chunk), f)) > 0) text.append(chunk, got);
+    std::fclose(f);
+    std::string line;
+    std::vector<int32_t> poly;
+    size_t at = 0;
+    while (at < text.size()) {
+        size_t end = text.find('\n', at);
+        if (end == std::string::npos) end = text.size();
+        line.assign(text, at, end - at);
+        at = end + 1;
+        if (line.size() < 2 || line[1] != ' ') continue;
+        if (line[0] == 'v') {
+            // three floats, each after optional white space; the line counts only if all parse
+            const char* p = line.c_str() + 2;
+            char* e = nullptr;
+            float xyz[3];
+            int k = 0;
+            for (; k < 3; ++k) {
+                xyz[k] = std::strtof(p, &e);
+                if (e == p) break;
+                p = e;
+            }
+            if (k == 3) D.V.insert(D.V.end(), xyz, xyz + 3);
+        } else if (line[0] == 'f') {
+            poly.clear();
+            const char* p = line.c_str() + 2;
+            while (*p) {
+                while (*p == ' ' || *p == '\t') ++p;
+                if (!*p) break;
+                int idx = (int)std::strtol(p, nullptr, 10);
+                if (idx != 0) {
+                    if (idx < 0) idx = (int)(D.V.size() / 3) + idx + 1;
+                    poly.push_back(idx - 1);
+                }
+                while (*p && *p != ' ' && *p != '\t') ++p;
+            }
+            for (size_t k = 1; k + 1 < poly.size(); ++k) {
+                D.T.push_back(poly[0]);
+                D.T.push_back(poly[k]);
+                D.T.push_back(poly[k + 1]);
+            }
+        }
+    }
+    return true;
+}
+
 }  // namespace
 
 extern "C" {
+
+int dcb_read_obj(const char* path, float* vertices, int64_t vertex_capacity, int32_t* triangles,
+                 int64_t triangle_capacity, int64_t* num_vertices, int64_t* num_triangles) {
+    if (!path || !num_vertices || !num_triangles) return DCB_ERR_INVALID_ARGUMENT;
+    ObjData D;
+    if (!parse_obj(path, D)) return DCB_ERR_INVALID_ARGUMENT;
+    const int64_t nv = (int64_t)D.V.size() / 3, nt = (int64_t)D.T.size() / 3;
+    *num_vertices = nv;
+    *num_triangles = nt;
+    if (nv == 0 || nt == 0) return DCB_ERR_INVALID_ARGUMENT;   // read_obj_to_sdf fails on such files
+    for (int32_t v : D.T)
+        if (v < 0 || v >= nv) return DCB_ERR_INVALID_ARGUMENT;
+    if (!vertices && !triangles) return DCB_OK;                  // counts only
+    if (!vertices || !triangles || vertex_capacity < nv || triangle_capacity < nt) return DCB_ERR_TOO_LARGE;
+    std::memcpy(vertices, D.V.data(), sizeof(float) * D.V.size());
+    std::memcpy(triangles, D.T.data(), sizeof(int32_t) * D.T.size());
+    return DCB_OK;
+}
+
+int dcb_obj_grid(const float* vertices, int64_t num_vertices, int res, dcb_grid* grid) {
+    if (!vertices || num_vertices < 1 || res < 2 || !grid) return DCB_ERR_INVALID_ARGUMENT;
+    float lo[3] = {vertices[0], vertices[1], vertices[2]}, hi[3] = {vertices[0], vertices[1], vertices[2]};
+    for (int64_t i = 0; i < num_vertices; ++i)
+        for (int a = 0; a < 3; ++a) {
+            const float x = vertices[3 * i + a];
+            if (x < lo[a]) lo[a] = x;
+            if (x > hi[a]) hi[a] = x;
+        }
+    const float diag = std::sqrt((hi[0] - lo[0]) * (hi[0] - lo[0]) + (hi[1] - lo[1]) * (hi[1] - lo[1]) +
+                                 (hi[2] - lo[2]) * (hi[2] - lo[2]));
+    const float pad = diag > 0.0f ? diag * 0.08f : 0.1f;
+    for (int a = 0; a < 3; ++a) { lo[a] -= pad; hi[a] += pad; }
+    grid->nx = grid->ny = grid->nz = res;
+    grid->ox = lo[0]; grid->oy = lo[1]; grid->oz = lo[2];
+    grid->vx = (hi[0] - lo[0]) / (res - 1);
+    grid->vy = (hi[1] - lo[1]) / (res - 1);
+    grid->vz = (hi[2] - lo[2]) / (res - 1);
+    grid->values = nullptr;
+    return DCB_OK;
+}
 
 int dcb_write_obj(const char* path, const float* vertices, int64_t num_vertices, const int32_t* faces,
                   int64_t num_faces, int verts_per_face, int threads) {

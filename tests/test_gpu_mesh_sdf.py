@@ -248,3 +248,27 @@ def test_voxelized_against_reference(backend, name, vres):
     print("%s vres %d: identical values %.6f, same sign %.6f, largest relative difference %.3g" % (
         name, vres, same, signs, rel.max()))
     assert signs == 1.0 and same >= 0.99 and rel.max() <= 2e-5
+
+
+@pytest.mark.parametrize("voxelize_first", [False, True])
+def test_obj_to_sdf_ingestion(backend, tmp_path, voxelize_first):
+    """dc_cli's read_obj_to_sdf (dc_cli.cpp:121-203): OBJ file -> padded grid -> SDF on the GPU,
+    equal to the oracle's conversion of the same triangles on the same grid."""
+    import oracle as O
+    from contouring_b200 import io as dio
+    from contouring_b200 import synth
+    V, F = synth.icosphere(3)
+    V = (V * np.float32(0.7) + np.float32([0.1, -0.2, 0.05])).astype(np.float32)
+    path = tmp_path / "ico.obj"
+    dio.write_obj(path, V, F, verts_per_face=3)
+    grid, ms = dio.read_obj_to_sdf(backend, path, 40, voxelize_first=voxelize_first, voxel_res=64)
+    Vr, Tr = dio.read_obj(path)
+    dims, sp, org = dio.obj_grid(Vr, 40)
+    if voxelize_first:
+        ref = O.mesh_to_sdf_voxelized(Vr, Tr, dims, org, sp, voxel_res=64)[0]
+    else:
+        ref = O.mesh_to_sdf(Vr, Tr, dims, org, sp)[0]
+    got = np.asarray(grid.values, np.float32)
+    assert (grid.nx, grid.ny, grid.nz) == dims and ms >= 0
+    assert np.array_equal(np.sign(got), np.sign(ref))
+    assert np.abs(got.astype(np.float64) - ref).max() <= DIST_TOL
