@@ -427,6 +427,9 @@ struct PostWork {
     PostBuf deg, bot, top, pos, vparent, skey, sdeg, shead, soff, sgid, stack, lverts, lflag, lkey, llen;
     PostBuf lpos, lorder, lkey2, nvl, nfl, vb, fb, fillV, fillF;
     PostBuf first, fflag, slot, V1, F1, outV, outF, succ, indeg, cbad, clen, cbase, crank, jflags;
+    PostBuf fscratch, frings, fcenters;
+    unsigned long long fill_scap = 1ull << 23;   // ring vertices the fill scratch holds (grows)
+    unsigned long long fill_rcap = 1ull << 20;   // ring records
     void* hcount = nullptr;             // page-locked copy of the device counters
 };
 

@@ -68,6 +68,10 @@ struct PostCounters {
     unsigned long long nloops;          // loops of 3..4096 vertices
     unsigned long long fill_v, fill_f;
     unsigned long long nout;            // vertices after renumbering
+    unsigned long long cursor;          // ring vertices reserved in the fill scratch
+    unsigned long long nrings;          // ring records written
+    int fill_overflow;                  // the scratch or the record list was too small
+    int pad3;
 };
 
 inline unsigned grid_for(long long n, int threads, int num_sms) {
@@ -607,6 +611,12 @@ struct FillParams {
     const unsigned long long* fb;
     float* fillV;                       // new vertices (global index nvw + local)
     int4* fillF;                        // new faces
+    // sizes pass: ring positions kept in a scratch area (null: not kept)
+    float* scratch;                     // 3 floats per ring vertex
+    unsigned long long scap;            // its capacity in vertices
+    longlong2* rings;                   // per ring: (loop << 32 | ring number, scratch offset)
+    unsigned long long rcap;
+    float* centers;                     // per loop: the centroid of its last ring (the fan's centre)
     PostCounters* C;
 };
 
@@ -647,6 +657,8 @@ __global__ void __launch_bounds__(kFillThreads) k_fill(FillParams P) {
     float* bz = by + kMaxLoop;
     float* sd = bz + kMaxLoop;
     __shared__ float s_step, s_c[3], s_far;
+    __shared__ unsigned long long s_base;
+    __shared__ int s_fits;
     const int tid = threadIdx.x;
     for (long long li = blockIdx.x; li < P.nloops; li += gridDim.x) {
         const int at = P.lorder[li];
@@ -695,6 +707,18 @@ __global__ void __launch_bounds__(kFillThreads) k_fill(FillParams P) {
                 break;
             }
             ++rings;
+            if (!WRITE && P.scratch) {
+                // room for this ring in the scratch area, and its record; bounds-checked
+                if (tid == 0) {
+                    const unsigned long long base = atomicAdd(&P.C->cursor, (unsigned long long)n);
+                    const unsigned long long rec = atomicAdd(&P.C->nrings, 1ull);
+                    s_fits = base + n <= P.scap && rec < P.rcap;
+                    s_base = base;
+                    if (s_fits) P.rings[rec] = make_longlong2(((long long)li << 32) | rings, (long long)base);
+                    else atomicOr(&P.C->fill_overflow, 1);
+                }
+                __syncthreads();
+            }
             for (int k = tid; k < n; k += blockDim.x) {
                 const float px = ax[k], py = ay[k], pz = az[k];
                 float dx = cx - px, dy = cy - py, dz = cz - pz;
@@ -703,6 +727,10 @@ __global__ void __launch_bounds__(kFillThreads) k_fill(FillParams P) {
                 if (d > 0.0001f) { dx /= d; dy /= d; dz /= d; }
                 else { dx = 0.0f; dy = 0.0f; dz = 0.0f; }
                 bx[k] = px + dx * move; by[k] = py + dy * move; bz[k] = pz + dz * move;
+                if (!WRITE && P.scratch && s_fits) {
+                    float* q = P.scratch + 3 * (s_base + k);
+                    q[0] = bx[k]; q[1] = by[k]; q[2] = bz[k];
+                }
                 if (WRITE) {
                     const long long g = vbase - P.nvw + (long long)(rings - 1) * n + k;
                     P.fillV[3 * g] = bx[k]; P.fillV[3 * g + 1] = by[k]; P.fillV[3 * g + 2] = bz[k];
@@ -740,6 +768,7 @@ __global__ void __launch_bounds__(kFillThreads) k_fill(FillParams P) {
         } else if (tid == 0) {
             P.nvl[li] = (unsigned long long)rings * n + (n > 4 ? 1 : 0);
             P.nfl[li] = (unsigned long long)rings * n + (n > 4 ? n : 1);
+            if (P.centers) { P.centers[3 * li] = s_c[0]; P.centers[3 * li + 1] = s_c[1]; P.centers[3 * li + 2] = s_c[2]; }
         }
         __syncthreads();
         ax = sh; ay = ax + kMaxLoop; az = ay + kMaxLoop; bx = az + kMaxLoop; by = bx + kMaxLoop; bz = by + kMaxLoop;
@@ -751,6 +780,58 @@ __global__ void k_fill_totals(const unsigned long long* vb, const unsigned long 
     if (threadIdx.x == 0 && blockIdx.x == 0) {
         C->fill_v = n ? vb[n - 1] + nvl[n - 1] : 0;
         C->fill_f = n ? fb[n - 1] + nfl[n - 1] : 0;
+    }
+}
+
+// The kept rings moved from the scratch area to their places: ring j of loop li is vertices
+// vb[li] + (j-1)*n .. + n of the fill.
+__global__ void k_fill_copy(const longlong2* __restrict__ rings, long long nrings, const int* __restrict__ lorder,
+                            const int* __restrict__ llen, const unsigned long long* __restrict__ vb,
+                            const float* __restrict__ scratch, float* fillV) {
+    for (long long r = blockIdx.x; r < nrings; r += gridDim.x) {
+        const longlong2 rec = rings[r];
+        const long long li = rec.x >> 32, j = rec.x & 0xffffffffLL;
+        const int n = llen[lorder[li]];
+        const unsigned long long dst = vb[li] + (unsigned long long)(j - 1) * n;
+        for (int k = threadIdx.x; k < 3 * n; k += blockDim.x) fillV[3 * dst + k] = scratch[3 * (unsigned long long)rec.y + k];
+    }
+}
+
+// The fill's faces from the sizes alone (no positions needed): ring j's quads join ring j-1
+// (the loop itself for j = 1) to ring j; then the triangle, quad or fan of the last ring, whose
+// fan centre comes from the sizes pass.
+__global__ void k_fill_faces(FillParams P) {
+    for (long long li = blockIdx.x; li < P.nloops; li += gridDim.x) {
+        const int at = P.lorder[li];
+        const int n = P.llen[at];
+        const int* idx = P.lverts + at;
+        const long long rings = (long long)((P.nvl[li] - (n > 4 ? 1 : 0)) / (unsigned long long)n);
+        const long long vbase = P.nvw + (long long)P.vb[li], fbase = (long long)P.fb[li];
+        for (long long t = threadIdx.x; t < rings * n; t += blockDim.x) {
+            const long long j = t / n + 1;
+            const int k = (int)(t - (j - 1) * n), k1 = k + 1 == n ? 0 : k + 1;
+            const long long prev = j == 1 ? -1 : vbase + (j - 2) * n;
+            const int o0 = prev < 0 ? idx[k] : (int)(prev + k), o1 = prev < 0 ? idx[k1] : (int)(prev + k1);
+            const int i0 = (int)(vbase + (j - 1) * n + k), i1 = (int)(vbase + (j - 1) * n + k1);
+            P.fillF[fbase + t] = make_int4(o0, o1, i1, i0);
+        }
+        const long long cur = rings == 0 ? -1 : vbase + (rings - 1) * n;
+        auto ring_index = [&](int k) { return cur < 0 ? idx[k] : (int)(cur + k); };
+        const long long f0 = fbase + rings * n;
+        if (n == 3) {
+            if (threadIdx.x == 0) P.fillF[f0] = make_int4(ring_index(0), ring_index(1), ring_index(2), ring_index(2));
+        } else if (n == 4) {
+            if (threadIdx.x == 0) P.fillF[f0] = make_int4(ring_index(0), ring_index(1), ring_index(2), ring_index(3));
+        } else {
+            const int center = (int)(vbase + rings * n);
+            if (threadIdx.x == 0) {
+                const long long g = center - P.nvw;
+                P.fillV[3 * g] = P.centers[3 * li]; P.fillV[3 * g + 1] = P.centers[3 * li + 1];
+                P.fillV[3 * g + 2] = P.centers[3 * li + 2];
+            }
+            for (int k = threadIdx.x; k < n; k += blockDim.x)
+                P.fillF[f0 + k] = make_int4(ring_index(k), ring_index(k + 1 == n ? 0 : k + 1), center, center);
+        }
     }
 }
 
@@ -892,7 +973,7 @@ void post_release(PostWork& W) {
                       &W.skey, &W.sdeg, &W.shead, &W.soff, &W.sgid, &W.stack, &W.lverts, &W.lflag, &W.lkey, &W.llen,
                       &W.lpos, &W.lorder, &W.lkey2, &W.nvl, &W.nfl, &W.vb, &W.fb, &W.fillV, &W.fillF, &W.first,
                       &W.fflag, &W.slot, &W.V1, &W.F1, &W.outV, &W.outF, &W.succ, &W.indeg, &W.cbad, &W.clen,
-                      &W.cbase, &W.crank, &W.jflags};
+                      &W.cbase, &W.crank, &W.jflags, &W.fscratch, &W.frings, &W.fcenters};
     for (PostBuf* b : all) {
         if (b->p) cudaFree(b->p);
         b->p = nullptr;
@@ -1168,6 +1249,14 @@ cudaError_t post_run(PostWork& W, PostRun& R, cudaStream_t s) {
         fp.Vw = as<float>(W.Vw); fp.nvw = nvw; fp.nvl = as<unsigned long long>(W.nvl); fp.nfl = as<unsigned long long>(W.nfl);
         fp.vb = as<unsigned long long>(W.vb); fp.fb = as<unsigned long long>(W.fb); fp.fillV = nullptr; fp.fillF = nullptr;
         fp.C = C;
+        // ring positions kept by the sizes pass (the capacity grows to what the last call needed)
+        PP_TRY(grow(W.fscratch, sizeof(float) * 3 * W.fill_scap));
+        PP_TRY(grow(W.frings, sizeof(longlong2) * W.fill_rcap));
+        PP_TRY(grow(W.fcenters, sizeof(float) * 3 * nloops));
+        fp.scratch = as<float>(W.fscratch); fp.scap = W.fill_scap;
+        fp.rings = as<longlong2>(W.frings); fp.rcap = W.fill_rcap;
+        fp.centers = as<float>(W.fcenters);
+        PP_TRY(cudaMemsetAsync(&C->cursor, 0, 2 * sizeof(unsigned long long) + 2 * sizeof(int), s));
         const size_t smem = sizeof(float) * 7 * kMaxLoop;
         PP_TRY(cudaFuncSetAttribute(k_fill<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         PP_TRY(cudaFuncSetAttribute(k_fill<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -1196,7 +1285,21 @@ cudaError_t post_run(PostWork& W, PostRun& R, cudaStream_t s) {
         PP_TRY(grow(W.fillF, sizeof(int4) * std::max(1LL, fill_f)));
         fp.fillV = as<float>(W.fillV);
         fp.fillF = as<int4>(W.fillF);
-        k_fill<true><<<fg, kFillThreads, smem, s>>>(fp);
+        const PostCounters& hc = host_counters(W);
+        if (!hc.fill_overflow) {
+            const long long nr = (long long)hc.nrings;
+            if (nr > 0)
+                k_fill_copy<<<(unsigned)std::min<long long>(nr, (long long)sms * 8), kThreads, 0, s>>>(
+                    fp.rings, nr, fp.lorder, fp.llen, fp.vb, fp.scratch, fp.fillV);
+            k_fill_faces<<<(unsigned)std::min<long long>(nloops, (long long)sms * 8), kThreads, 0, s>>>(fp);
+        } else {
+            // the kept positions did not fit: recompute the rings while writing them, and let
+            // the next call keep them
+            W.fill_scap = std::max<unsigned long long>(W.fill_scap, hc.cursor);
+            W.fill_rcap = std::max<unsigned long long>(W.fill_rcap, hc.nrings);
+            fp.scratch = nullptr;
+            k_fill<true><<<fg, kFillThreads, smem, s>>>(fp);
+        }
         PP_TRY(cudaGetLastError());
         R.stats[kPostFillVertices] = fill_v;
         R.stats[kPostFillFaces] = fill_f;
