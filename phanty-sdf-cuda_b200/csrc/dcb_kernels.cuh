@@ -447,7 +447,7 @@ struct PostRun {
     long long nv_out = 0, nf_out = 0;
     long long stats[kPostNumStats] = {};
     int err = 0;                        // device-side findings: 1 face index out of range, 2 non-finite vertex,
-                                        // 4 weld key out of range, 8 walk guard, 16 fill did not converge
+                                        // 4 weld key out of range, 8 a bounded loop gave up, 16 fill did not converge
     int too_large = 0;
     const char* what = nullptr;         // the failing CUDA call
 };

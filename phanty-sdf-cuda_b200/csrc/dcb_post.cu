@@ -48,7 +48,10 @@ constexpr int kFillThreads = 256;
 constexpr int kKeyBits = 17;            // per axis in the weld key
 constexpr int kRankRounds = 32;         // pointer-jumping rounds: enough for cycles of 2^31 vertices
 
-enum PostErr { kPostBadIndex = 1, kPostNonFinite = 2, kPostWeldSpan = 4, kPostWalkGuard = 8, kPostRingGuard = 16 };
+// Device-side findings (PostRun::err): a face index out of range, a non-finite vertex, a weld
+// key beyond 17 bits, a bounded loop that gave up (union retries, walk steps), a hole fill that
+// had not converged after kMaxRings rings.
+enum PostErr { kPostBadIndex = 1, kPostNonFinite = 2, kPostWeldSpan = 4, kPostLoopGuard = 8, kPostRingGuard = 16 };
 
 struct PostCounters {
     unsigned int box[6];                // ordered bits: min x, y, z; max x, y, z
@@ -107,7 +110,7 @@ __device__ __forceinline__ int uf_find(int* parent, int x) {
 __device__ void uf_unite(int* parent, int a, int b, int* err) {
     int ra = a, rb = b;
     for (int guard = 0;; ++guard) {
-        if (guard > (1 << 24)) { atomicOr(err, kPostWalkGuard); return; }
+        if (guard > (1 << 24)) { atomicOr(err, kPostLoopGuard); return; }
         ra = uf_find(parent, ra);
         rb = uf_find(parent, rb);
         if (ra == rb) return;
@@ -535,7 +538,7 @@ __global__ void k_walk(WalkParams P) {
                 int at = s;
                 bool closed = false;
                 while (P.top[at] > P.bot[at]) {
-                    if (++guard > (1LL << 31)) { atomicOr(&P.C->err, kPostWalkGuard); return; }
+                    if (++guard > (1LL << 31)) { atomicOr(&P.C->err, kPostLoopGuard); return; }
                     const unsigned int t = --P.top[at];
                     const int only = P.succ[at];
                     const int next = only >= 0 ? only : (int)(P.adj[t] & m);
