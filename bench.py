@@ -639,7 +639,9 @@ def run_post_workload(args):
         Fh = F.cpu().numpy()
         mesh = DualContouringMesh(Vh.reshape(-1), Fh.reshape(-1))
         walls = []
+        out = None
         for i in range(max(1, min(args.e2e_steps, 3)) + 1):
+            out = None      # the previous result's page-locked arrays go back to the host cache
             t0 = time.perf_counter()
             out = postprocess_mesh(mesh, True, True, backend=be)
             if i:
