@@ -23,7 +23,10 @@
 extern "C" {
 #endif
 
-#define DCB_ABI_VERSION 3
+/* 4 adds, without changing earlier layouts: the batch CUDA-graph calls, the mesh post-pass
+ * (dcb_postprocess_*, dcb_copy_post_mesh, dcb_post_stats) and the OBJ reader (dcb_read_obj,
+ * dcb_obj_grid). */
+#define DCB_ABI_VERSION 4
 
 enum dcb_status {
     DCB_OK = 0,

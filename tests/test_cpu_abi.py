@@ -38,7 +38,7 @@ def test_library_exports_every_declared_symbol():
 def test_abi_utilities():
     from contouring_b200 import _lib
     L = _lib.lib()
-    assert L.dcb_abi_version() >= 1
+    assert L.dcb_abi_version() >= 4
     for code in range(0, -8, -1):
         assert L.dcb_status_string(code)
     assert L.dcb_status_string(-99) == b"unknown status"
