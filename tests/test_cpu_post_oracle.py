@@ -74,3 +74,27 @@ def test_stats_describe_the_scene():
     V, F = S.floaters(32)
     _, Fo, st = O.postprocess_mesh(V, F, 0, 1)
     assert st["components"] == 3 and st["kept_faces"] == Fo.shape[0] < F.shape[0]
+
+
+def _random_mesh(seed):
+    """A small messy quad mesh: lattice vertices (so many coincide or lie within the weld step),
+    random quads (some degenerate, many sharing edges in odd ways), plus a clean patch."""
+    rng = np.random.default_rng(seed)
+    n = int(rng.integers(8, 60))
+    lattice = rng.integers(0, 5, size=(n, 3)).astype(np.float32) * np.float32(0.25)
+    jitter = (rng.random((n, 3)).astype(np.float32) - np.float32(0.5)) * np.float32(2e-6)
+    V = lattice + np.where(rng.random((n, 1)) < 0.3, jitter, np.float32(0))
+    F = rng.integers(0, n, size=(int(rng.integers(4, 80)), 4)).astype(np.int32)
+    Vp, Fp = S.figure_eight()
+    return np.concatenate([V, Vp + np.float32(3)]).astype(np.float32), np.concatenate([F, Fp + n]).astype(np.int32)
+
+
+@pytest.mark.parametrize("seed", range(40))
+def test_oracle_matches_reference_on_random_meshes(seed):
+    import oracle as O
+    V, F = _random_mesh(seed)
+    for close, remove in S.FLAGS:
+        r = O.ref_postprocess_mesh(V, F, close, remove)
+        if r is None:
+            pytest.skip("oracle/_ref/libref_post.so was not built (make -C oracle ref)")
+        assert _same(O.postprocess_mesh(V, F, close, remove), r), (seed, close, remove)

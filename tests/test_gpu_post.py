@@ -115,3 +115,13 @@ def test_invalid_meshes_are_refused(backend):
     # the handle stays usable
     m = postprocess_mesh(DualContouringMesh(V, F), True, True, backend=backend)
     assert len(m.faces) // 4 == 144
+
+
+@pytest.mark.parametrize("seed", range(40))
+def test_random_messy_meshes_match_oracle(backend, seed):
+    """Lattice vertices (many coincide), random and degenerate quads, tangled boundaries."""
+    import oracle as O
+    from test_cpu_post_oracle import _random_mesh
+    V, F = _random_mesh(seed)
+    for close, remove in S.FLAGS:
+        check_same(run_gpu(backend, V, F, close, remove), O.postprocess_mesh(V, F, close, remove), (seed, close, remove))
