@@ -60,7 +60,8 @@ def test_struct_layouts_match_the_header():
     from contouring_b200 import _lib
     structs = {"dcb_grid": _lib.DcbGrid, "dcb_opts": _lib.DcbOpts, "dcb_stats": _lib.DcbStats,
                "dcb_mesh_dev": _lib.DcbMeshDev, "dcb_mesh_host": _lib.DcbMeshHost,
-               "dcb_sdf_stats": _lib.DcbSdfStats, "dcb_batch_mesh": _lib.DcbBatchMesh}
+               "dcb_sdf_stats": _lib.DcbSdfStats, "dcb_batch_mesh": _lib.DcbBatchMesh,
+               "dcb_post_stats": _lib.DcbPostStats}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "dcb.h"', "int main(void) {"]
     for cname, py in structs.items():
         lines.append('printf("%s %%zu\\n", sizeof(%s));' % (cname, cname))
@@ -87,6 +88,18 @@ def test_null_arguments_are_rejected_without_a_device():
     assert L.dcb_mark_active_cells_noalloc(None, None, 0, ctypes.byref(cnt), None) == _lib.DCB_ERR_INVALID_ARGUMENT
     assert L.dcb_create(None, 0) == _lib.DCB_ERR_INVALID_ARGUMENT
     assert L.dcb_destroy(None) in (_lib.DCB_OK, _lib.DCB_ERR_INVALID_ARGUMENT)
+    # the mesh post-pass and the OBJ entry points
+    assert L.dcb_postprocess_device(None, None, 0, None, 0, 1, 1, None, None, None) == _lib.DCB_ERR_INVALID_ARGUMENT
+    assert L.dcb_postprocess_host(None, None, 0, None, 0, 1, 1, None, None, None) == _lib.DCB_ERR_INVALID_ARGUMENT
+    assert L.dcb_copy_post_mesh(None, None, None, 1, None) == _lib.DCB_ERR_INVALID_ARGUMENT
+    g = _lib.DcbGrid()
+    V = np.zeros((2, 3), np.float32)
+    assert L.dcb_obj_grid(None, 0, 8, ctypes.byref(g)) == _lib.DCB_ERR_INVALID_ARGUMENT
+    assert L.dcb_obj_grid(V.ctypes.data, 2, 1, ctypes.byref(g)) == _lib.DCB_ERR_INVALID_ARGUMENT
+    assert L.dcb_obj_grid(V.ctypes.data, 2, 8, None) == _lib.DCB_ERR_INVALID_ARGUMENT
+    nv, nt = ctypes.c_int64(), ctypes.c_int64()
+    assert L.dcb_read_obj(None, None, 0, None, 0, ctypes.byref(nv), ctypes.byref(nt)) == _lib.DCB_ERR_INVALID_ARGUMENT
+    assert L.dcb_batch_graph_launch(None, None) == _lib.DCB_ERR_INVALID_ARGUMENT
 
 
 def test_no_device_fails_loudly():
