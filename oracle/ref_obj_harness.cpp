@@ -1,0 +1,67 @@
+// ref_obj_harness.cpp — TEST INFRASTRUCTURE ONLY: runs the reference CLI's own OBJ -> SDF
+// ingestion, read_obj_to_sdf (src/cpp/dc_cli.cpp:121-203), on a file and records what it hands
+// to the mesh -> SDF conversion: the parsed vertices and triangles and the padded grid. The
+// CLI source is compiled into this translation unit where it lies (its function is file-static;
+// its main is renamed and never called); compute_mesh_sdf_cuda is replaced by the recorder
+// below. Built by oracle/Makefile's `ref` target into oracle/_ref/ref_obj_to_sdf, with
+// src/cpp/dc_backend.cpp (headers of ref_stubs/ first, as for ref_post_harness.cpp).
+//
+//   ref_obj_to_sdf <file.obj> <res> <record.bin>
+//   record: int64 nv, int64 nt, float32 vertices[3 nv], int32 triangles[3 nt],
+//           int32 nx, ny, nz, float32 ox, oy, oz, vx, vy, vz
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <fstream>
+#include <iostream>
+#include <memory>
+#include <string>
+#include <vector>
+
+#define DC_ENABLE_CUDA 1
+#define main reference_cli_main
+#include "dc_cli.cpp"
+#undef main
+
+// dc_backend.cpp is linked for DenseSdfGrid's virtual sample(); the two functions it calls
+// from the contouring library (declared by ref_stubs/) are never reached.
+#include "Cell.h"
+#include "contouring.h"
+void contouring(const Eigen::VectorXd&, const Eigen::MatrixXd&, int, int, int, double, Eigen::MatrixXd&,
+                Eigen::MatrixXi&, const ContouringOptions&) {
+    std::abort();
+}
+std::vector<Cell>* getGeneratedCells() { return nullptr; }
+
+static FILE* g_record = nullptr;
+
+DenseSdfGrid compute_mesh_sdf_cuda(const float* vertices, int num_vertices, const int* faces, int num_faces, int nx,
+                                   int ny, int nz, float ox, float oy, float oz, float vx, float vy, float vz, float*,
+                                   bool, int) {
+    const int64_t counts[2] = {num_vertices, num_faces};
+    const int32_t dims[3] = {nx, ny, nz};
+    const float geo[6] = {ox, oy, oz, vx, vy, vz};
+    std::fwrite(counts, sizeof(int64_t), 2, g_record);
+    std::fwrite(vertices, sizeof(float), 3 * (size_t)num_vertices, g_record);
+    std::fwrite(faces, sizeof(int32_t), 3 * (size_t)num_faces, g_record);
+    std::fwrite(dims, sizeof(int32_t), 3, g_record);
+    std::fwrite(geo, sizeof(float), 6, g_record);
+    DenseSdfGrid g;
+    g.nx = nx; g.ny = ny; g.nz = nz;
+    g.ox = ox; g.oy = oy; g.oz = oz;
+    g.vx = vx; g.vy = vy; g.vz = vz;
+    return g;
+}
+
+int main(int argc, char** argv) {
+    if (argc != 4) return 2;
+    g_record = std::fopen(argv[3], "wb");
+    if (!g_record) return 2;
+    DenseSdfGrid grid;
+    const bool ok = read_obj_to_sdf(argv[1], std::atoi(argv[2]), grid);
+    std::fclose(g_record);
+    return ok ? 0 : 1;
+}

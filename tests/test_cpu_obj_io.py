@@ -100,3 +100,49 @@ def test_obj_errors(tmp_path):
     p.write_text("v 0 0 0\nv 1 0 0\nv 0 1 0\nf 1 2 4\n")
     with pytest.raises(DcbError):
         dio.read_obj(p)
+
+
+def _reference_record(path, res):
+    """The reference CLI's own read_obj_to_sdf run on `path` (oracle/_ref/ref_obj_to_sdf, built
+    from dc_cli.cpp by `make -C oracle ref`): what it hands to the conversion. None when the
+    harness was not built."""
+    import os
+    import subprocess
+    exe = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref", "ref_obj_to_sdf")
+    if not os.path.exists(exe):
+        return None
+    rec = str(path) + ".rec"
+    subprocess.run([exe, str(path), str(res), rec], check=True)
+    raw = open(rec, "rb").read()
+    nv, nt = np.frombuffer(raw[:16], np.int64)
+    at = 16
+    V = np.frombuffer(raw[at:at + 12 * nv], np.float32).reshape(-1, 3)
+    at += 12 * nv
+    T = np.frombuffer(raw[at:at + 12 * nt], np.int32).reshape(-1, 3)
+    at += 12 * nt
+    dims = tuple(int(x) for x in np.frombuffer(raw[at:at + 12], np.int32))
+    geo = np.frombuffer(raw[at + 12:at + 36], np.float32)
+    return V, T, dims, geo[:3], geo[3:]
+
+
+@pytest.mark.parametrize("res", [16, 97])
+def test_ingestion_matches_the_reference_cli(tmp_path, res):
+    from contouring_b200 import synth
+    files = []
+    p = tmp_path / "edge.obj"
+    p.write_bytes(TEXT.encode())
+    files.append(p)
+    V, F = synth.icosphere(2)
+    q = tmp_path / "ico.obj"
+    dio.write_obj(q, (V * np.float32(3.7) + np.float32([1.0, -2.0, 0.5])).astype(np.float32), F, verts_per_face=3)
+    files.append(q)
+    for path in files:
+        ref = _reference_record(path, res)
+        if ref is None:
+            pytest.skip("oracle/_ref/ref_obj_to_sdf was not built (make -C oracle ref)")
+        Vr, Tr, dims_r, org_r, sp_r = ref
+        Vo, To = dio.read_obj(path)
+        dims, sp, org = dio.obj_grid(Vo, res)
+        assert np.array_equal(Vo.view(np.uint32), Vr.view(np.uint32)) and np.array_equal(To, Tr), path
+        assert dims == dims_r
+        assert np.array_equal(np.array(org, np.float32), org_r) and np.array_equal(np.array(sp, np.float32), sp_r)
