@@ -2,10 +2,15 @@
 the binary `.sdf` layout byte for byte, round trips, and the OBJ text line for line against
 the reference writer's formatting (the C++ stream default: 6 significant digits, i.e. %g),
 on one thread and on many."""
+import os
 import struct
+import subprocess
 
 import numpy as np
 import pytest
+
+from contouring_b200 import DenseSdfGrid
+from contouring_b200 import io as dio
 
 
 def _grid(seed=0, dims=(7, 5, 6)):
@@ -70,3 +75,45 @@ def test_obj_from_mesh_and_empty(tmp_path):
     assert (tmp_path / "q.obj").read_text() == "v 0 0 0\nv 1 0 0\nv 1 1 0\nv 0 1 0\nf 1 2 3 4\n"
     io.write_obj(tmp_path / "e.obj", DualContouringMesh())
     assert (tmp_path / "e.obj").read_text() == ""
+
+
+def _cli_harness():
+    """oracle/_ref/ref_obj_to_sdf: the reference CLI's own file functions (dc_cli.cpp:17-47),
+    compiled from dc_cli.cpp by `make -C oracle ref`; None when not built."""
+    exe = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref", "ref_obj_to_sdf")
+    return exe if os.path.exists(exe) else None
+
+
+def test_obj_text_identical_to_the_reference_cli_writer(tmp_path):
+    exe = _cli_harness()
+    if exe is None:
+        pytest.skip("oracle/_ref/ref_obj_to_sdf was not built (make -C oracle ref)")
+    rng = np.random.default_rng(5)
+    V = (rng.standard_normal((2000, 3)) * np.array([1e-6, 1.0, 3e5])).astype(np.float32)
+    V[:20] = np.array([0.0, -0.0, 1e-38, -1e-45, 123456789.0, 1e20, 0.1, 2.5e-5, 7.0, -3.25] * 6, np.float32).reshape(20, 3)
+    F = rng.integers(0, 2000, size=(1500, 4)).astype(np.int32)
+    mesh_bin = tmp_path / "mesh.bin"
+    with open(mesh_bin, "wb") as f:
+        f.write(np.array([2000, 1500], np.int64).tobytes() + V.tobytes() + F.tobytes())
+    subprocess.run([exe, "write_obj", str(mesh_bin), str(tmp_path / "ref.obj")], check=True)
+    for threads in (1, 7):
+        dio.write_obj(tmp_path / "ours.obj", V, F, verts_per_face=4, threads=threads)
+        assert (tmp_path / "ours.obj").read_bytes() == (tmp_path / "ref.obj").read_bytes()
+
+
+def test_sdf_reader_identical_to_the_reference_cli_reader(tmp_path):
+    exe = _cli_harness()
+    if exe is None:
+        pytest.skip("oracle/_ref/ref_obj_to_sdf was not built (make -C oracle ref)")
+    rng = np.random.default_rng(6)
+    vals = rng.standard_normal(7 * 5 * 3).astype(np.float32)
+    g = DenseSdfGrid(7, 5, 3, 0.5, 0.25, 0.125, -1.0, 2.0, 3.5, values=vals)
+    path = tmp_path / "g.sdf"
+    dio.write_sdf(path, g)
+    subprocess.run([exe, "read_sdf", str(path), str(tmp_path / "rec.bin")], check=True)
+    raw = (tmp_path / "rec.bin").read_bytes()
+    ours = dio.read_sdf(path)
+    assert tuple(np.frombuffer(raw[:12], np.int32)) == (ours.nx, ours.ny, ours.nz)
+    assert np.array_equal(np.frombuffer(raw[12:36], np.float32),
+                          np.array([ours.vx, ours.vy, ours.vz, ours.ox, ours.oy, ours.oz], np.float32))
+    assert np.array_equal(np.frombuffer(raw[36:], np.float32), np.asarray(ours.values))

@@ -112,7 +112,7 @@ def _reference_record(path, res):
     if not os.path.exists(exe):
         return None
     rec = str(path) + ".rec"
-    subprocess.run([exe, str(path), str(res), rec], check=True)
+    subprocess.run([exe, "obj2sdf", str(path), str(res), rec], check=True)
     raw = open(rec, "rb").read()
     nv, nt = np.frombuffer(raw[:16], np.int64)
     at = 16
