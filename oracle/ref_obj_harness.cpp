@@ -13,6 +13,8 @@
 //   ref_obj_to_sdf write_obj <mesh.bin> <out.obj>   mesh: int64 nv, nf, float32 V[3 nv], int32 F[4 nf]
 //   ref_obj_to_sdf read_sdf <in.sdf> <record.bin>   record: int32 nx, ny, nz, float32 vx, vy, vz,
 //                                                   ox, oy, oz, values
+// and its analytic test grids (dc_cli.cpp:49-118), written in the .sdf layout:
+//   ref_obj_to_sdf generate <sphere|box|plane> <res> <out.sdf>
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -92,6 +94,25 @@ int main(int argc, char** argv) {
         DenseSdfGrid grid;
         if (!read_sdf(argv[2], grid)) return 1;
         FILE* f = std::fopen(argv[3], "wb");
+        if (!f) return 2;
+        const int32_t dims[3] = {grid.nx, grid.ny, grid.nz};
+        const float geo[6] = {grid.vx, grid.vy, grid.vz, grid.ox, grid.oy, grid.oz};
+        std::fwrite(dims, sizeof(int32_t), 3, f);
+        std::fwrite(geo, sizeof(float), 6, f);
+        std::fwrite(grid.values.data(), sizeof(float), grid.values.size(), f);
+        std::fclose(f);
+        return 0;
+    }
+    if (mode == "generate" && argc == 5) {
+        DenseSdfGrid grid;
+        const std::string shape = argv[2];
+        const int res = std::atoi(argv[3]);
+        if (res < 2) return 2;
+        if (shape == "sphere") generate_sphere(grid, res);
+        else if (shape == "box") generate_box(grid, res);
+        else if (shape == "plane") generate_plane(grid, res);
+        else return 2;
+        FILE* f = std::fopen(argv[4], "wb");
         if (!f) return 2;
         const int32_t dims[3] = {grid.nx, grid.ny, grid.nz};
         const float geo[6] = {grid.vx, grid.vy, grid.vz, grid.ox, grid.oy, grid.oz};

@@ -117,3 +117,21 @@ def test_sdf_reader_identical_to_the_reference_cli_reader(tmp_path):
     assert np.array_equal(np.frombuffer(raw[12:36], np.float32),
                           np.array([ours.vx, ours.vy, ours.vz, ours.ox, ours.oy, ours.oz], np.float32))
     assert np.array_equal(np.frombuffer(raw[36:], np.float32), np.asarray(ours.values))
+
+
+@pytest.mark.parametrize("shape", ["sphere", "box", "plane"])
+@pytest.mark.parametrize("res", [9, 24, 33])
+def test_cli_test_grids_identical_to_the_reference_generators(tmp_path, shape, res):
+    """synth.cli_sphere / cli_box / cli_plane against the CLI's own generate_* (dc_cli.cpp:49-118)."""
+    from contouring_b200 import synth
+    exe = _cli_harness()
+    if exe is None:
+        pytest.skip("oracle/_ref/ref_obj_to_sdf was not built (make -C oracle ref)")
+    out = tmp_path / ("%s.sdf" % shape)
+    subprocess.run([exe, "generate", shape, str(res), str(out)], check=True)
+    ref = dio.read_sdf(out)
+    vals, dims, sp, org = getattr(synth, "cli_" + shape)(res)
+    assert dims == (ref.nx, ref.ny, ref.nz)
+    assert np.array_equal(np.array(sp, np.float32), np.array([ref.vx, ref.vy, ref.vz], np.float32))
+    assert np.array_equal(np.array(org, np.float32), np.array([ref.ox, ref.oy, ref.oz], np.float32))
+    assert np.array_equal(np.asarray(vals.numpy()).view(np.uint32), np.asarray(ref.values).view(np.uint32))
