@@ -30,10 +30,10 @@ sys.path.insert(0, os.path.join(ROOT, "phanty-sdf-cuda_b200"))
 # edge normals, QEF, Jacobi list, FP64 vertices, 3 column-scan passes, face scatter,
 # FP64 vertices for windings, FP64 windings, face order.
 KERNELS_PER_STEP = 16
-# DRAM traffic of k_mark_zmarch per grid point, from the ncu capture summarised in
-# profiles/k_mark_zmarch_csg512.md (dram__bytes_read.sum + dram__bytes_write.sum divided by
-# the grid points of that capture; the kernel streams the grid once, so traffic scales with
-# the number of points). None = not measured.
+# DRAM traffic of k_mark_zmarch per grid point, from a single-kernel ncu capture of the 512^3
+# CSG workload (dram__bytes_read.sum + dram__bytes_write.sum divided by the grid points of
+# that capture; the kernel streams the grid once, so traffic scales with the number of
+# points). None = not measured.
 MARK_TRAFFIC_BYTES_PER_POINT = (563.814656e6 + 18.4768e6) / 512 ** 3
 
 

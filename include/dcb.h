@@ -203,10 +203,11 @@ int dcb_copy_cells_to_host(dcb_handle h, int64_t* cell_linear_index, void* cuda_
  * when capacity is too small, and DCB_ERR_TOO_LARGE when the grid's scratch exceeds the
  * fixed 16 MiB scratch array (a 450^3 grid fits; the bound is checked on every call).
  * Scratch lives in one file-scope device array shared by all calls on a device and kept
- * between calls: calls whose work overlaps on the GPU race. The first call on a device
- * resolves the array's address (cudaGetSymbolAddress); make that first call before any
- * stream capture. Runs on the current device and the given stream and returns after the
- * result is complete. */
+ * between calls: calls whose work overlaps on the GPU race. Every call looks the array's
+ * address up in the current context (cudaGetSymbolAddress, no allocation); the first call on
+ * a device may also load the library's device code, so make it before any stream capture.
+ * Runs on the current device and the given stream and returns after the result is
+ * complete. */
 int dcb_mark_active_cells_noalloc(const dcb_grid* grid, int64_t* cells, int64_t capacity,
                                   int64_t* count, void* cuda_stream);
 

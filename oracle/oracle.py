@@ -445,6 +445,43 @@ def ref_sparse(d_values_ptr, dims, spacing, origin, brick_size=8, normal_mode=0,
     return {"V": V, "F": F, "stats": stats, "times": times.tolist()}
 
 
+def ref_dense_mesh(d_values_ptr, dims, spacing, origin, exact=True):
+    """The reference's own dense CUDA backend (CudaDualContouringBackend::extract_device,
+    src/cuda/dc_cuda.cu:652-847) from ``oracle/_ref/`` (``make -C oracle ref``) on a device grid
+    of the current CUDA device: returns its vertices (float32, nv x 3) and quads (int32, nf x 4)
+    in its own order, or None when the library was not built or the grid exceeds its 32-bit
+    indices. Its active-cell numbering and its unordered quad set follow the CPU semantics; its
+    vertex positions (clamped into the cell, no normal averaging), quad order and winding do
+    not."""
+    name = "libref_dc_cuda_exact.so" if exact else "libref_dc_cuda.so"
+    path = os.path.join(_HERE, "_ref", name)
+    if not os.path.exists(path):
+        return None
+    key = path + ":dense"
+    if key not in _libs:
+        lib = ctypes.CDLL(path)
+        lib.refdc_extract_mesh.argtypes = [ctypes.c_int] * 3 + [ctypes.c_float] * 6 + \
+            [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64,
+             ctypes.c_void_p, ctypes.c_void_p]
+        lib.refdc_extract_mesh.restype = ctypes.c_int
+        _libs[key] = lib
+    lib = _libs[key]
+    nx, ny, nz = (int(d) for d in dims)
+    nv, nf = ctypes.c_int64(0), ctypes.c_int64(0)
+    args = [nx, ny, nz, *(float(x) for x in spacing), *(float(x) for x in origin), ctypes.c_void_p(int(d_values_ptr))]
+    rc = lib.refdc_extract_mesh(*args, None, 0, None, 0, ctypes.byref(nv), ctypes.byref(nf))
+    if rc == -3:
+        V = np.empty((nv.value, 3), np.float32)
+        F = np.empty((nf.value, 4), np.int32)
+        rc = lib.refdc_extract_mesh(*args, V.ctypes.data, nv.value, F.ctypes.data, nf.value,
+                                    ctypes.byref(nv), ctypes.byref(nf))
+    elif rc == 0:
+        V, F = np.empty((0, 3), np.float32), np.empty((0, 4), np.int32)
+    if rc != 0:
+        return None
+    return V, F
+
+
 def ref_mesh_to_sdf(V, F, dims, origin, spacing, voxelize_first=False, voxel_res=256, exact=True):
     """The reference's own CUDA mesh -> SDF conversion (compute_mesh_sdf_device_cuda,
     src/cuda/mesh_to_sdf_cuda.cu:740-1009) from ``oracle/_ref/`` (``make -C oracle ref``):

@@ -94,16 +94,4 @@ enum DeviceError : int { kErrNone = 0, kErrTimeout = 1, kErrInternal = 2, kErrOv
 
 __device__ __forceinline__ void set_error(int* flag, int code) { atomicCAS(flag, 0, code); }
 
-// Bounded spin iterations for cross-CTA waits (~ tens of milliseconds with backoff).
-constexpr long long kSpinLimit = 1ll << 22;
-
-__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p) {
-    unsigned long long v;
-    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-    return v;
-}
-__device__ __forceinline__ void st_relaxed_u64(unsigned long long* p, unsigned long long v) {
-    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" :: "l"(p), "l"(v) : "memory");
-}
-
 }  // namespace dcb

@@ -8,55 +8,36 @@
 // __device__ array of fixed size. The caller passes the grid and the output buffer.
 //
 // The array's name is only a host-side stand-in in host code; its device address is
-// obtained with cudaGetSymbolAddress once per device (on that device's first call, with
-// the device current) and passed to the kernels. All calls on a device share the array and
-// it keeps the last call's contents, so the counters are cleared at the start of each call
-// and two calls whose work overlaps on the GPU race on it.
+// looked up with cudaGetSymbolAddress on every call, with the caller's device and context
+// current, and passed to the kernels. Nothing is cached between calls, so a device reset or
+// another context on the same device never sees a stale address. The very first call on a
+// device may load the library's device code (lazy module loading), so make it before any
+// stream capture. All calls on a device share the array and it keeps the last call's
+// contents, so the counter is cleared at the start of each call and two calls whose work
+// overlaps on the GPU race on it.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
-#include <mutex>
 #include "dcb_kernels.cuh"
 #include "../../include/dcb.h"
 
 namespace dcb {
 
 constexpr size_t kNoAllocScratchBytes = 16u << 20;   // 16 MiB, held by every device that loads the library
-constexpr int kNoAllocMaxDevices = 64;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
 namespace {
 
-std::mutex g_setup_mutex;
-void* g_scratch_ptr[kNoAllocMaxDevices] = {};
-
-// Device address of the scratch array on `device` (which must be current), resolved once.
-cudaError_t scratch_address(int device, void** out) {
-    std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_ptr[device]) {
-        void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess) return e;
-        g_scratch_ptr[device] = p;
-    }
-    *out = g_scratch_ptr[device];
-    return cudaSuccess;
+// Device address of the scratch array in the current context. Looked up on every call: the
+// lookup allocates nothing, and an address kept from an earlier call could belong to a
+// context that has since been reset or to another context on the same device.
+cudaError_t scratch_address(void** out) {
+    *out = nullptr;
+    return cudaGetSymbolAddress(out, g_noalloc_scratch);
 }
 
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
-
-// The grid as a batch of one: its slot and offset tables (see dcb_kernels.cuh).
-struct Table {
-    GridSlot slot;
-    long long seg_off[2];
-    long long col_off[2];
-    unsigned long long vert_off[2];
-    long long tile_off[2];
-    int tile_slot[2];
-};
-
-__global__ void k_store_table(Table* dst, Table src) { *dst = src; }
 
 // Packed (i | j<<21 | k<<42) -> linear index i + cx*(j + cy*k), in place.
 __global__ void k_packed_to_linear(uint64_t* cells, long long n, int cx, int cy) {
@@ -80,7 +61,6 @@ extern "C" int dcb_mark_active_cells_noalloc(const dcb_grid* grid, int64_t* cell
     if (grid->nx > 65536 || grid->ny > (1 << 21) || grid->nz > (1 << 21)) return DCB_ERR_TOO_LARGE;
     int device = 0;
     if (cudaGetDevice(&device) != cudaSuccess) { cudaGetLastError(); return DCB_ERR_CUDA; }
-    if (device < 0 || device >= kNoAllocMaxDevices) return DCB_ERR_NOT_SUPPORTED;
     cudaStream_t s = reinterpret_cast<cudaStream_t>(cuda_stream);
 
     GridDesc g;
@@ -98,7 +78,8 @@ extern "C" int dcb_mark_active_cells_noalloc(const dcb_grid* grid, int64_t* cell
 
     int sms = 148;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) { cudaGetLastError(); return DCB_ERR_CUDA; }
-    // The grid as a batch of one: its slot and offset tables also live in the scratch array.
+    // The grid as a batch of one. A single grid's kernels take its slot from the launch
+    // parameters (BatchTable::s0) and read no device-side table, so none is stored.
     GridSlot slot;
     slot.g = g;
     slot.bits_off = 0; slot.super_off = 0; slot.seg_off = 0; slot.col_off = 0;
@@ -111,16 +92,10 @@ extern "C" int dcb_mark_active_cells_noalloc(const dcb_grid* grid, int64_t* cell
     slot.nzc = (g.cz + slot.KZ - 1) / slot.KZ;
     const long long ntiles = (long long)nxt * slot.nrb * slot.nzc;
     if (ntiles > 0x7fffffffLL) return DCB_ERR_TOO_LARGE;
-    Table ht;
-    std::memset(&ht, 0, sizeof(ht));
-    ht.slot = slot;
-    ht.seg_off[1] = nseg;
-    ht.tile_off[1] = ntiles;
 
-    // Scratch layout, each part 256-byte aligned: table | total | bits | super | seg_count |
+    // Scratch layout, each part 256-byte aligned: total | bits | super | seg_count |
     // seg_start | scan partials. Grids that need more than the array are rejected.
-    const size_t off_table = 0;
-    const size_t off_total = align256(off_table + sizeof(Table));
+    const size_t off_total = 0;
     const size_t off_bits = align256(off_total + sizeof(unsigned long long));
     const size_t off_super = align256(off_bits + sizeof(uint32_t) * (size_t)rows * g.W);
     const size_t off_count = align256(off_super + sizeof(uint32_t) * (size_t)rows * g.W8);
@@ -130,21 +105,18 @@ extern "C" int dcb_mark_active_cells_noalloc(const dcb_grid* grid, int64_t* cell
     if (need > kNoAllocScratchBytes) return DCB_ERR_TOO_LARGE;
 
     void* base = nullptr;
-    if (scratch_address(device, &base) != cudaSuccess) { cudaGetLastError(); return DCB_ERR_CUDA; }
+    if (scratch_address(&base) != cudaSuccess) { cudaGetLastError(); return DCB_ERR_CUDA; }
     unsigned char* sb = static_cast<unsigned char*>(base);
     unsigned long long* total = reinterpret_cast<unsigned long long*>(sb + off_total);
-    Table* dt = reinterpret_cast<Table*>(sb + off_table);
 
-    // The array keeps the previous call's contents: write this call's table (a one-thread
-    // kernel takes it by value) and clear the counter this call reads.
-    k_store_table<<<1, 1, 0, s>>>(dt, ht);
-    if (cudaGetLastError() != cudaSuccess) return DCB_ERR_CUDA;
+    // The array keeps the previous call's contents: clear the counter this call reads (the
+    // bits, counts and starts are all overwritten before they are read).
     if (cudaMemsetAsync(total, 0, sizeof(unsigned long long), s) != cudaSuccess) { cudaGetLastError(); return DCB_ERR_CUDA; }
 
     BatchTable B;
-    B.s0 = slot; B.slots = &dt->slot; B.n = 1; B.cell_slot = nullptr; B.seg_off = dt->seg_off; B.col_off = dt->col_off; B.vert_off = dt->vert_off;
+    B.s0 = slot; B.slots = nullptr; B.n = 1; B.cell_slot = nullptr; B.seg_off = nullptr; B.col_off = nullptr; B.vert_off = nullptr;
     MarkParams mp;
-    mp.B = B; mp.tile_slot = dt->tile_slot; mp.tile_off = dt->tile_off; mp.m = 1; mp.ntiles = ntiles;
+    mp.B = B; mp.tile_slot = nullptr; mp.tile_off = nullptr; mp.m = 1; mp.ntiles = ntiles;
     mp.bits = reinterpret_cast<uint32_t*>(sb + off_bits);
     mp.seg_count = reinterpret_cast<uint32_t*>(sb + off_count);
     if (launch_mark(mp, slot.tw, s) != cudaSuccess) { cudaGetLastError(); return DCB_ERR_CUDA; }

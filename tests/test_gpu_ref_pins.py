@@ -1,0 +1,139 @@
+"""Pins of the B200 engine to the reference's OWN code (compiled from its sources into
+oracle/_ref/ by `make -C oracle ref`), on top of the FP64 restatement the other parity tests
+use.
+
+1. Dense dual contouring, topology: the reference's dense CUDA backend
+   (CudaDualContouringBackend::extract_device, src/cuda/dc_cuda.cu:652-847) marks a cell
+   active on strict corner signs like the CPU backend (mark_active_cells_kernel :241-281 vs
+   Cell.cpp:57-77), numbers vertices by ascending cell index (thrust::copy_if :701-712) and
+   emits a quad for every interior edge with a strict sign change whose four cells are active,
+   from the same four cells as the CPU loops (count/emit_faces_kernel :425-605 vs
+   contouring.cpp:607-729). So the vertex count, the cell each reference vertex is clamped
+   into (:409-420) and the unordered quad set must equal this engine's. The reference's
+   vertex positions (no normal averaging, clamped), quad order and winding are not CPU
+   semantics and are not compared. Its 32-bit edge indices cap the grids at 1024x1024x~680.
+2. Mesh -> SDF without voxelisation (compute_mesh_sdf_device_cuda, src/cuda/mesh_to_sdf_cuda.cu:
+   863-951): the whole output grid, with the tie tolerance of the voxelised pin (its bins are
+   filled by atomics, so its order among near-tied triangles varies from run to run).
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def backend():
+    from contouring_b200 import B200DualContouringBackend
+    b = B200DualContouringBackend(0)
+    yield b
+    b.close()
+
+
+def _dense_cases():
+    from contouring_b200 import synth
+    return {
+        # dc_tests.cpp cases (src/cpp/dc_tests.cpp:14-215)
+        "sphere32": lambda: synth.cli_sphere(32),
+        "box32": lambda: synth.cli_box(32),
+        "plane16": lambda: synth.cli_plane(16),
+        "thin_gap32": lambda: synth.thin_gap(32),
+        "empty16": lambda: synth.constant(16, 1.0),
+        "full16": lambda: synth.constant(16, -1.0),
+        # the small config (128^3 sphere r = 0.35) and dc_cli's own sphere generator grid
+        "sphere128_r035": lambda: synth.sphere(128, 0.35),
+        "cli_sphere128": lambda: synth.cli_sphere(128),
+        "csg96": lambda: synth.csg(96, seed=0),
+        "csg128_seed3": lambda: synth.csg(128, seed=3),
+        "rbf_sphere64": lambda: synth.rbf_sphere(64),
+        # exact zeros: neither sign, so they decide activity and faces only through the others
+        "noise_zeros17x23x9": lambda: synth.noise((17, 23, 9), seed=2, zero_frac=0.3),
+        "noise_zeros_half": lambda: synth.noise((24, 19, 21), seed=3, zero_frac=0.5),
+        "ternary": lambda: synth.ternary((21, 22, 23), seed=4),
+        "plane17_zero_layer": lambda: synth.cli_plane(17),
+        "sphere_zero_shell": lambda: synth.sphere_with_zero_shell(40),
+        "noise_ragged": lambda: synth.noise((33, 7, 41), seed=9),
+    }
+
+
+def _canonical_quads(F):
+    """Quads as sorted 4-tuples of vertex indices, rows sorted: the unordered, unoriented set."""
+    Q = np.sort(np.asarray(F, np.int64).reshape(-1, 4), axis=1)
+    if len(Q) == 0:
+        return Q
+    return Q[np.lexsort(Q.T[::-1])]
+
+
+def _check_dense(backend, case, name):
+    import torch
+    import oracle as O
+    from contouring_b200 import DenseSdfGridDevice
+    vals, dims, sp, org = case
+    dvals = vals.cuda() if not vals.is_cuda else vals
+    r = O.ref_dense_mesh(dvals.data_ptr(), dims, sp, org, exact=True)
+    if r is None:
+        pytest.skip("oracle/_ref/libref_dc_cuda_exact.so was not built")
+    rV, rF = r
+    _, _, st = backend.extract_tensor_ptr(DenseSdfGridDevice(*dims, *sp, *org, d_values=dvals))
+    cells = backend.active_cells()
+    mesh, _ = backend.extract_device(DenseSdfGridDevice(*dims, *sp, *org, d_values=dvals))
+    F = mesh.faces.reshape(-1, 4)
+    torch.cuda.synchronize()
+    assert st.vertex_count == len(rV) == len(cells), "%s: %d vertices, reference %d" % (name, st.vertex_count, len(rV))
+    assert len(F) == len(rF), "%s: %d quads, reference %d" % (name, len(F), len(rF))
+    # each reference vertex lies in (is clamped into) the box of this engine's cell of the same
+    # index: the two active-cell lists are the same list
+    if len(cells):
+        cx, cy = dims[0] - 1, dims[1] - 1
+        ijk = np.stack([cells % cx, (cells // cx) % cy, cells // (cx * cy)], axis=1)
+        o = np.asarray(org, np.float64)
+        h = np.asarray(sp, np.float64)
+        lo = o + ijk * h
+        hi = lo + h
+        tol = 4 * np.finfo(np.float32).eps * (np.abs(o) + np.asarray(dims) * np.abs(h)).max()
+        rv = rV.astype(np.float64)
+        ok = ((rv >= lo - tol) & (rv <= hi + tol)).all(axis=1) | ~np.isfinite(rv).all(axis=1)
+        assert ok.all(), "%s: %d reference vertices outside their cell" % (name, int((~ok).sum()))
+    assert np.array_equal(_canonical_quads(F), _canonical_quads(rF)), "%s: quad sets differ" % name
+    print("%s: %d active cells, %d quads identical to the reference's dense CUDA topology" % (name, len(cells), len(F)))
+
+
+@pytest.mark.parametrize("name", list(_dense_cases().keys()))
+def test_dense_topology_matches_reference_cuda(backend, name):
+    _check_dense(backend, _dense_cases()[name](), name)
+
+
+def test_dense_topology_matches_reference_cuda_csg512(backend):
+    """The sharp-feature CSG scene at 512^3 (the largest cube the reference's int indices allow
+    comfortably): ~1.5M active cells and quads."""
+    from contouring_b200 import synth
+    _check_dense(backend, synth.csg(512, seed=0, device="cuda"), "csg512")
+
+
+def _sdf_scenes():
+    from test_gpu_mesh_sdf import _scene
+    return _scene
+
+
+# no_faces is left out: the reference launches zero-sized grids on an empty mesh
+SDF_CASES = ["spheres4_48", "spheres6_ragged", "sphere_s3_64", "coarse_bins_16", "degenerate_and_duplicates",
+             "open_patch"]
+
+
+@pytest.mark.parametrize("name", SDF_CASES)
+def test_plain_mesh_to_sdf_matches_reference(backend, name):
+    import torch
+    import oracle as O
+    from contouring_b200 import mesh_to_sdf_tensor
+    V, F, (dims, sp, org) = _sdf_scenes()(name)
+    r = O.ref_mesh_to_sdf(V, F, dims, org, sp, voxelize_first=False, exact=True)
+    if r is None:
+        pytest.skip("oracle/_ref/libref_dc_cuda_exact.so was not built")
+    out, _ = mesh_to_sdf_tensor(backend, torch.from_numpy(V).cuda(), torch.from_numpy(F).cuda(), dims, org, sp)
+    got = out.cpu().numpy()
+    ref = r[0]
+    same = np.mean(got.view(np.uint32) == ref.view(np.uint32))
+    signs = np.mean(np.sign(got) == np.sign(ref))
+    rel = np.abs(got.astype(np.float64) - ref) / np.maximum(np.abs(ref.astype(np.float64)), 1e-30)
+    print("%s: identical values %.6f, same sign %.6f, largest relative difference %.3g" % (name, same, signs, rel.max()))
+    assert signs == 1.0 and same >= 0.99 and rel.max() <= 2e-5
