@@ -26,7 +26,7 @@ extern "C" {
 /* 4 adds, without changing earlier layouts: the batch CUDA-graph calls, the mesh post-pass
  * (dcb_postprocess_*, dcb_copy_post_mesh, dcb_post_stats) and the OBJ reader (dcb_read_obj,
  * dcb_obj_grid). */
-#define DCB_ABI_VERSION 4
+#define DCB_ABI_VERSION 5
 
 enum dcb_status {
     DCB_OK = 0,
@@ -134,6 +134,18 @@ typedef struct {
     int64_t two_vertex_cells;
     int64_t split_rejection_count;
     int64_t faces_skipped;          /* faces_skipped_due_to_missing_cluster */
+    /* the remaining DualContouringStats fields: active cells are marked and compacted in one
+     * pass (the brick times are 0, the cell times equal marking_ms / compaction_ms); faces
+     * are counted (inside the vertex stage for dual contouring), their counts scanned, then
+     * filled; bad_qef_count is always 0, as in the reference, which never increments it */
+    float active_brick_marking_ms;
+    float active_brick_compaction_ms;
+    float active_cell_marking_ms;
+    float active_cell_compaction_ms;
+    float face_count_ms;
+    float face_prefix_sum_ms;
+    float face_fill_ms;
+    int64_t bad_qef_count;
 } dcb_stats;
 
 /* Device-resident mesh; pointers are owned by the handle and stay valid until the next

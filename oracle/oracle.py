@@ -445,6 +445,40 @@ def ref_sparse(d_values_ptr, dims, spacing, origin, brick_size=8, normal_mode=0,
     return {"V": V, "F": F, "stats": stats, "times": times.tolist()}
 
 
+def ref_cpu_extract(values, dims, spacing, origin, timeout=600):
+    """The reference's OWN CPU dual contouring backend (CpuDualContouringBackend::extract,
+    src/cpp/dc_backend.cpp:51-125), compiled from its sources into oracle/_ref/ref_cpu_dc
+    (``make -C oracle ref``) with stand-in Eigen headers (JacobiSVD restated). Host float32
+    values in; returns (V float32 nv x 3, F int32 nf x 4, active_cells), or None when the
+    program was not built. Single-threaded and about 2-3 KB per cell, like the reference:
+    keep grids small (<= ~96^3)."""
+    import subprocess
+    import tempfile
+    exe = os.path.join(_HERE, "_ref", "ref_cpu_dc")
+    if not os.path.exists(exe):
+        return None
+    v = np.ascontiguousarray(np.asarray(values, np.float32).reshape(-1))
+    nx, ny, nz = (int(d) for d in dims)
+    with tempfile.TemporaryDirectory() as td:
+        gp, op = os.path.join(td, "g.sdf"), os.path.join(td, "o.bin")
+        with open(gp, "wb") as f:
+            f.write(np.array([nx, ny, nz], np.int32).tobytes())
+            f.write(np.array(list(spacing) + list(origin), np.float32).tobytes())
+            f.write(v.tobytes())
+        r = subprocess.run([exe, gp, op], capture_output=True, timeout=timeout)
+        if r.returncode != 0:
+            raise RuntimeError("ref_cpu_dc failed (%d): %s" % (r.returncode, r.stderr.decode()[-500:]))
+        buf = open(op, "rb").read()
+    nv, nf, vpf = np.frombuffer(buf, np.int64, 3, 0)
+    pos = 24
+    V = np.frombuffer(buf, np.float32, 3 * int(nv), pos).reshape(-1, 3).copy()
+    pos += 12 * int(nv)
+    F = np.frombuffer(buf, np.int32, int(vpf * nf), pos).reshape(-1, int(vpf)).copy()
+    pos += 4 * int(vpf * nf)
+    active = int(np.frombuffer(buf, np.int64, 1, pos)[0])
+    return V, F, active
+
+
 def ref_dense_mesh(d_values_ptr, dims, spacing, origin, exact=True):
     """The reference's own dense CUDA backend (CudaDualContouringBackend::extract_device,
     src/cuda/dc_cuda.cu:652-847) from ``oracle/_ref/`` (``make -C oracle ref``) on a device grid

@@ -68,7 +68,11 @@ class DcbStats(ctypes.Structure):
                 ("invalid_count", ctypes.c_int64), ("ambiguous_cells", ctypes.c_int64),
                 ("multi_vertex_cells", ctypes.c_int64), ("one_vertex_cells", ctypes.c_int64),
                 ("two_vertex_cells", ctypes.c_int64), ("split_rejection_count", ctypes.c_int64),
-                ("faces_skipped", ctypes.c_int64)]
+                ("faces_skipped", ctypes.c_int64),
+                ("active_brick_marking_ms", ctypes.c_float), ("active_brick_compaction_ms", ctypes.c_float),
+                ("active_cell_marking_ms", ctypes.c_float), ("active_cell_compaction_ms", ctypes.c_float),
+                ("face_count_ms", ctypes.c_float), ("face_prefix_sum_ms", ctypes.c_float),
+                ("face_fill_ms", ctypes.c_float), ("bad_qef_count", ctypes.c_int64)]
 
 
 class DcbMeshDev(ctypes.Structure):

@@ -170,10 +170,11 @@ class DualContouringStats:
                   "download_ms", "total_ms", "qef_fallback_count", "clamp_count",
                   "escalated_fp64_cells", "winding_fp64_faces", "total_bricks", "active_bricks",
                   "invalid_count", "ambiguous_cells", "multi_vertex_cells", "one_vertex_cells",
-                  "two_vertex_cells", "split_rejection_count"):
+                  "two_vertex_cells", "split_rejection_count", "active_brick_marking_ms",
+                  "active_brick_compaction_ms", "active_cell_marking_ms", "active_cell_compaction_ms",
+                  "face_count_ms", "face_prefix_sum_ms", "face_fill_ms", "bad_qef_count"):
             setattr(s, f, getattr(st, f))
         s.faces_skipped_due_to_missing_cluster = st.faces_skipped
-        s.active_cell_marking_ms = st.marking_ms
         s.rank_hist = list(st.rank_hist)
         return s
 

@@ -39,6 +39,8 @@ struct Counters {
     unsigned int tri_count;           // quads whose triangle orientation goes to FP64
     unsigned long long rank_hist[4];
     unsigned long long face_total;
+    unsigned int band_chunk;          // tile band kernel: next chunk
+    unsigned int face_staged;         // tile band kernel: staged faces
 };
 
 struct DevBuf {
@@ -54,10 +56,11 @@ struct dcb_context {
     int device = 0;
     int num_sms = 148;
     std::string last_error;
-    cudaEvent_t ev[8] = {};
+    cudaEvent_t ev[10] = {};
+    bool substage_events = false;     // ev[8] / ev[9] hold the face sub-stages of the last call
     DevBuf grid, bits, super, list, seg_count, seg_start, counters, V, vclass, fmask, col_count, col_fill,
         col_start, partials, esc_list, hard_list, hard_data, stage_quad, stage_key, faces, wind_items,
-        v64_index, v64_cells, V64, tris, tri_items, adj_rows, adj_owners, ours_ws;
+        v64_index, v64_cells, V64, tris, tri_items, adj_rows, adj_owners, ours_ws, face_grad;
     // sparse backends
     DevBuf sp_words, sp_brick, sp_vcount, sp_vstart, sp_vtmp, sp_ntmp, sp_N, sp_vcell, sp_fcount, sp_fstart,
         sp_stage, sp_counters;
@@ -359,6 +362,7 @@ int batch_alloc(dcb_context* h, int n, long long cap, const dcb_opts* o, TableVi
     DCB_TRY(h, ensure(h->stage_key, sizeof(uint2) * 3 * cap), "alloc face keys");
     DCB_TRY(h, ensure(h->faces, sizeof(int4) * 3 * cap), "alloc faces");
     DCB_TRY(h, ensure(h->v64_index, sizeof(int) * cap), "alloc fp64 index");
+    if (n == 1) DCB_TRY(h, ensure(h->face_grad, sizeof(float4) * 3 * cap), "alloc staged face gradients");
     if (n > 1) {
         DCB_TRY(h, ensure(h->cell_slot, sizeof(uint32_t) * cap), "alloc vertex grids");
         T.B.cell_slot = as<uint32_t>(h->cell_slot);
@@ -432,6 +436,9 @@ int batch_rest(dcb_context* h, const BatchLayout& L, TableView& T, const dcb_opt
     xp.B.cell_slot = nullptr;                      // expand finds grids by segment
     xp.list_cap = cap;
     DCB_TRY(h, launch_expand(xp, h->num_sms, s), "launch expand");
+    // A single grid outside a captured graph runs the tile band kernel (vertices and staged
+    // faces from shared-memory stencils); batches run the per-cell kernels.
+    const bool band = n == 1 && live == nullptr;
     QefParams qp;
     qp.B = T.B; qp.list = xp.list; qp.nactive = cap; qp.live = live; qp.V = as<float>(h->V); qp.vclass = as<uint8_t>(h->vclass);
     qp.fmask = as<uint8_t>(h->fmask); qp.col_count = as<uint32_t>(h->col_count);
@@ -440,17 +447,44 @@ int batch_rest(dcb_context* h, const BatchLayout& L, TableView& T, const dcb_opt
     qp.rank_hist = dc->rank_hist;
     qp.thr = (float)o->svd_threshold; qp.band = (float)o->fp64_threshold_band;
     qp.cond_max = (float)std::min(o->fp64_escalation_cond, 3.0e38); qp.force64 = o->force_fp64;
-    DCB_TRY(h, launch_cell_qef(qp, h->num_sms, s), "launch qef");
+    if (band) {
+        const GridSlot& S = L.slots[0];
+        BandParams bp;
+        bp.S = S;
+        bp.bits = xp.bits; bp.super = xp.super;
+        bp.nxc = ((S.g.cx + 31) / 32 + 31) / 32;
+        bp.nyb = (S.g.cy + band_tile_rows() - 1) / band_tile_rows();
+        bp.nzb = (S.g.cz + band_tile_planes() - 1) / band_tile_planes();
+        bp.nchunks = (long long)bp.nxc * bp.nyb * bp.nzb;
+        bp.chunk_next = &dc->band_chunk;
+        bp.V = qp.V; bp.vclass = qp.vclass; bp.col_count = qp.col_count;
+        bp.esc_list = qp.esc_list; bp.esc_count = qp.esc_count;
+        bp.hard_list = qp.hard_list; bp.hard_data = qp.hard_data; bp.hard_count = qp.hard_count;
+        bp.rank_hist = qp.rank_hist;
+        bp.face_cells = as<int4>(h->faces); bp.face_grad = as<float4>(h->face_grad);
+        bp.face_count = &dc->face_staged; bp.face_cap = (unsigned long long)(3 * cap); bp.nv = cap;
+        bp.err = &dc->err;
+        bp.thr = qp.thr; bp.band = qp.band; bp.force64 = qp.force64;
+        DCB_TRY(h, launch_band(bp, h->num_sms, s), "launch band");
+    } else {
+        DCB_TRY(h, launch_cell_qef(qp, h->num_sms, s), "launch qef");
+    }
     DCB_TRY(h, launch_cell_jacobi(qp, cap, h->num_sms, s), "launch jacobi");
     Vertex64Params v64;
     v64.B = T.B; v64.list = xp.list; v64.cells = qp.esc_list; v64.count = &dc->esc_count; v64.cap = (unsigned int)cap;
     v64.Vf = qp.V; v64.vclass = qp.vclass; v64.V64 = nullptr; v64.thr = o->svd_threshold;
     DCB_TRY(h, launch_vertex_fp64(v64, cap, h->num_sms, s), "launch vertex fp64");
     if (events) DCB_TRY(h, cudaEventRecord(h->ev[3], s), "event");
+    // the faces were counted per column by the vertex kernels
+    if (events) DCB_TRY(h, cudaEventRecord(h->ev[8], s), "event");
 
     // 3) faces: column scan, scatter with FP32 winding, FP64 re-decisions, in-column order.
     DCB_TRY(h, launch_scan(as<uint32_t>(h->col_count), ncol, as<uint32_t>(h->partials),
                            as<uint32_t>(h->col_start), &dc->face_total, s), "launch scan");
+    if (events) {
+        DCB_TRY(h, cudaEventRecord(h->ev[9], s), "event");
+        h->substage_events = true;
+    }
     if (n > 1)
         DCB_TRY(h, launch_face_offsets(T.B, as<uint32_t>(h->col_start), &dc->face_total, T.face_off, s), "face offsets");
     FaceParams fp;
@@ -465,7 +499,21 @@ int batch_rest(dcb_context* h, const BatchLayout& L, TableView& T, const dcb_opt
     fp.v64_count = &dc->v64_count; fp.v64_cap = (unsigned long long)v64_cap;
     fp.err = &dc->err;
     fp.hmax = L.hmax;
-    DCB_TRY(h, launch_face_scatter(fp, h->num_sms, s), "launch face scatter");
+    if (band) {
+        FacePlaceParams pp;
+        pp.S = L.slots[0]; pp.list = xp.list;
+        pp.face_cells = as<int4>(h->faces); pp.face_grad = as<float4>(h->face_grad);
+        pp.face_count = &dc->face_staged; pp.face_cap = (unsigned long long)(3 * cap); pp.nv = cap;
+        pp.V = qp.V; pp.vclass = qp.vclass;
+        pp.col_start = fp.col_start; pp.col_fill = fp.col_fill;
+        pp.stage_quad = fp.stage_quad; pp.stage_key = fp.stage_key;
+        pp.wind_items = fp.wind_items; pp.wind_count = fp.wind_count; pp.wind_cap = fp.wind_cap;
+        pp.v64_index = fp.v64_index; pp.v64_cells = fp.v64_cells; pp.v64_count = fp.v64_count;
+        pp.v64_cap = fp.v64_cap; pp.err = fp.err;
+        DCB_TRY(h, launch_face_place(pp, 3 * cap, h->num_sms, s), "launch face placement");
+    } else {
+        DCB_TRY(h, launch_face_scatter(fp, h->num_sms, s), "launch face scatter");
+    }
     Vertex64Params w64;
     w64.B = T.B; w64.list = xp.list; w64.cells = fp.v64_cells; w64.count = fp.v64_count; w64.cap = (unsigned int)v64_cap;
     w64.Vf = nullptr; w64.vclass = nullptr; w64.V64 = as<double>(h->V64); w64.thr = o->svd_threshold;
@@ -775,8 +823,11 @@ int run_sparse(dcb_context* h, const dcb_grid* in, const dcb_opts* o, cudaStream
         P.fstart = as<uint32_t>(h->sp_fstart);
         P.stage = as<int4>(h->sp_stage);
         DCB_TRY(h, launch_sparse_faces(P, h->num_sms, s), "launch faces");
+        DCB_TRY(h, cudaEventRecord(h->ev[8], s), "event");
         DCB_TRY(h, launch_scan(P.fcount, na, as<uint32_t>(h->partials), as<uint32_t>(h->sp_fstart),
                                dcn + kScFaces, s), "launch face scan");
+        DCB_TRY(h, cudaEventRecord(h->ev[9], s), "event");
+        h->substage_events = true;
         DCB_TRY(h, cudaMemcpyAsync(hcn, dcn, sizeof(unsigned long long) * kScSlots, cudaMemcpyDeviceToHost, s), "read totals");
         DCB_TRY(h, cudaStreamSynchronize(s), "sparse vertices");
         nverts = mvdc ? (long long)hcn[kScVertices] : na;
@@ -814,6 +865,7 @@ int run_sparse(dcb_context* h, const dcb_grid* in, const dcb_opts* o, cudaStream
 
 // The extraction a method names, on a device grid.
 int run_method(dcb_context* h, const dcb_grid* in, const dcb_opts* o, cudaStream_t s, dcb_stats* st) {
+    h->substage_events = false;
     if (o->method == DCB_METHOD_SPARSE || o->method == DCB_METHOD_SPARSE_MVDC) return run_sparse(h, in, o, s, st);
     h->last_kind = 0;
     h->cells_per_vertex = 0;
@@ -832,6 +884,20 @@ void fill_times(dcb_context* h, dcb_stats* st, bool upload) {
     st->compaction_ms = elapsed(h->ev[6], h->ev[2]);    // segment scan
     st->qef_ms = elapsed(h->ev[2], h->ev[3]);
     st->face_emission_ms = elapsed(h->ev[3], h->ev[4]);
+    // DualContouringStats' finer stage times (include/dc_backend.h:44-78, filled by the
+    // reference's sparse backend, dc_cuda_sparse.cu:1458-1467): active cells are marked and
+    // compacted in one pass over the grid (no separate brick stage); faces are counted, their
+    // counts scanned, then filled.
+    st->active_brick_marking_ms = 0.f;
+    st->active_brick_compaction_ms = 0.f;
+    st->active_cell_marking_ms = st->marking_ms;
+    st->active_cell_compaction_ms = st->compaction_ms;
+    st->face_count_ms = h->substage_events ? elapsed(h->ev[3], h->ev[8]) : 0.f;
+    st->face_prefix_sum_ms = h->substage_events ? elapsed(h->ev[8], h->ev[9]) : 0.f;
+    st->face_fill_ms = h->substage_events ? elapsed(h->ev[9], h->ev[4]) : 0.f;
+    // the reference declares and reports bad_qef_count but never increments it
+    // (dc_cuda_sparse.cu:41, 1481)
+    st->bad_qef_count = 0;
 }
 
 struct SdfCounters {
@@ -1039,7 +1105,7 @@ int dcb_destroy(dcb_handle h) {
                       &h->V, &h->vclass, &h->fmask, &h->col_count, &h->col_fill, &h->col_start,
                       &h->partials, &h->esc_list, &h->hard_list, &h->hard_data, &h->stage_quad,
                       &h->stage_key, &h->faces, &h->wind_items, &h->v64_index, &h->v64_cells, &h->V64,
-                      &h->tris, &h->tri_items, &h->m_verts, &h->m_faces, &h->m_out, &h->m_tris,
+                      &h->tris, &h->tri_items, &h->face_grad, &h->m_verts, &h->m_faces, &h->m_out, &h->m_tris,
                       &h->m_bin_count, &h->m_bin_start, &h->m_bin_fill, &h->m_bin_scratch, &h->m_bin_tris,
                       &h->m_bin_active, &h->m_active_list, &h->m_axis_start, &h->m_far, &h->m_ext, &h->m_tmp,
                       &h->m_partials, &h->m_counters, &h->m_vox, &h->table, &h->cell_slot, &h->adj_rows, &h->adj_owners, &h->ours_ws,

@@ -296,6 +296,70 @@ cudaError_t launch_face_scatter(const FaceParams& P, int num_sms, cudaStream_t s
     return cudaGetLastError();
 }
 
+// ---- placement of the faces staged by the tile band kernel -------------------------------
+
+// Thread per staged face (its four cells' ranks in the CPU corner order and the summed
+// gradientAt of its edge's endpoints): the FP32 winding test with its error bound, exactly
+// as emit_face decides it, and the face's slot in its column; uncertain faces are listed for
+// the FP64 re-decision.
+__global__ void __launch_bounds__(256)
+k_face_place(const __grid_constant__ FacePlaceParams P) {
+    const GridDesc& g = P.S.g;
+    const long long cxcy = (long long)g.cx * g.cy;
+    const long long nf = min((long long)*P.face_count, (long long)P.face_cap);
+    for (long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x; f < nf;
+         f += (long long)gridDim.x * blockDim.x) {
+        const int4 q = P.face_cells[f];
+        const float4 gg = P.face_grad[f];
+        const uint32_t col = __float_as_uint(gg.w);
+        const int axis = (int)(col / (uint32_t)cxcy);
+        const uint32_t r0 = (uint32_t)q.x, r1 = (uint32_t)q.y, r2 = (uint32_t)q.z, r3 = (uint32_t)q.w;
+        if ((long long)max(max(r0, r1), max(r2, r3)) >= P.nv || axis > 2) { set_error(P.err, kErrInternal); continue; }
+        const uint64_t pk = __ldg(reinterpret_cast<const unsigned long long*>(P.list) + r2);
+        const uint32_t k = (uint32_t)(pk >> 42);
+        const float3 gn = make_float3(gg.x, gg.y, gg.z);
+        const float3 pa = ldv(P.V, r0), pb = ldv(P.V, r1), pc = ldv(P.V, r2), pd = ldv(P.V, r3);
+        const float dv = quad_vertex_bound(P.vclass, r0, r1, r2, r3, pa, pb, pc, pd, P.S.hmax);
+        const float3 ba = sub3(pb, pa), da = sub3(pd, pa), ca = sub3(pc, pa);
+        float3 qn = cross3(ba, da);
+        float qn2 = dot3(qn, qn);
+        const float lb = sqrtf(dot3(ba, ba)), ld = sqrtf(dot3(da, da)), lc = sqrtf(dot3(ca, ca));
+        float dq = 2.f * dv * (lb + ld + 2.f * dv);
+        const float qnl0 = sqrtf(qn2);
+        const bool near_fallback = (qnl0 - dq) < 1e-12f && (qnl0 + dq) >= 1e-12f;
+        if (qn2 < 1e-24f) { qn = cross3(ca, da); qn2 = dot3(qn, qn); dq = 2.f * dv * (lc + ld + 2.f * dv); }
+        const float gn2 = dot3(gn, gn);
+        const float d = dot3(qn, gn);
+        const float qnl = sqrtf(qn2), gnl = sqrtf(gn2);
+        const bool uncertain = near_fallback || gn2 < 1e-4f ||
+                               fabsf(d) <= 4.f * dq * gnl + 1e-5f * qnl * gnl;
+        const bool swap = !uncertain && gn2 > 0.f && qn2 > 0.f && d < 0.f;
+        const uint32_t slot = P.col_start[col] + atomicAdd(&P.col_fill[col], 1u);
+        if ((unsigned long long)slot >= P.face_cap) { set_error(P.err, kErrInternal); continue; }
+        P.stage_quad[slot] = swap ? make_int4((int)r0, (int)r3, (int)r2, (int)r1)
+                                  : make_int4((int)r0, (int)r1, (int)r2, (int)r3);
+        P.stage_key[slot] = make_uint2(k, col);
+        if (uncertain) {
+            const unsigned int w = atomicAdd(P.wind_count, 1u);
+            if (w < P.wind_cap) P.wind_items[w] = make_uint4(slot, (uint32_t)axis, (uint32_t)pk, (uint32_t)(pk >> 32));
+            else set_error(P.err, kErrOverflow);
+            const uint32_t rq[4] = {r0, r1, r2, r3};
+#pragma unroll
+            for (int t = 0; t < 4; ++t)
+                request_fp64_vertex(P.v64_index, P.v64_cells, P.v64_count, P.v64_cap, P.err, rq[t]);
+        }
+    }
+}
+
+cudaError_t launch_face_place(const FacePlaceParams& P, long long max_faces, int num_sms, cudaStream_t s) {
+    if (max_faces <= 0) return cudaSuccess;
+    long long blocks = (max_faces + 255) / 256;
+    const long long cap = (long long)num_sms * 16;
+    if (blocks > cap) blocks = cap;
+    k_face_place<<<(unsigned)blocks, 256, 0, s>>>(P);
+    return cudaGetLastError();
+}
+
 // ---- in-column ordering ----------------------------------------------------------------
 
 __global__ void __launch_bounds__(256)

@@ -206,6 +206,65 @@ struct TriParams {
 };
 cudaError_t launch_triangulate(const TriParams& P, long long max_quads, int num_sms, cudaStream_t s);
 
+// ---- tile band kernel (dcb_band.cu), single grids ----
+// Work unit: a chunk of up to 32 x-adjacent tiles of 32 x 4 x 4 cells (one active-bit word
+// per cell row), handed out by an atomic counter.
+struct BandParams {
+    GridSlot S;                    // the grid
+    const uint32_t* bits;          // its active bits and super-word ranks
+    const uint32_t* super;
+    int nxc, nyb, nzb;             // chunks along x (32 words each), row blocks, plane blocks
+    long long nchunks;
+    unsigned int* chunk_next;      // chunk counter, zero before the launch
+    float* V;
+    uint8_t* vclass;
+    uint32_t* col_count;           // [3][cx*cy]: a*cx*cy + i*cy + j
+    uint32_t* esc_list;
+    unsigned int* esc_count;
+    uint32_t* hard_list;
+    float4* hard_data;
+    unsigned int* hard_count;
+    unsigned long long* rank_hist;
+    int4* face_cells;              // staged faces: ranks of the four cells, CPU corner order
+    float4* face_grad;             // staged faces: gradientAt(p0) + gradientAt(p1), column in w
+    unsigned int* face_count;
+    unsigned long long face_cap;
+    long long nv;                  // active cells (vertex ranks are below it)
+    int* err;
+    float thr;
+    float band;
+    int force64;
+};
+cudaError_t launch_band(const BandParams& P, int num_sms, cudaStream_t s);
+int band_tile_rows();
+int band_tile_planes();
+
+// Staged faces -> FP32 winding decision and their slot in the column order (dcb_band.cu).
+struct FacePlaceParams {
+    GridSlot S;
+    const uint64_t* list;
+    const int4* face_cells;
+    const float4* face_grad;
+    const unsigned int* face_count;
+    unsigned long long face_cap;   // staged face entries (and stage_quad / stage_key entries)
+    long long nv;                  // vertices
+    const float* V;
+    const uint8_t* vclass;
+    const uint32_t* col_start;
+    uint32_t* col_fill;
+    int4* stage_quad;
+    uint2* stage_key;              // {k, column}
+    uint4* wind_items;             // {slot, axis, packed lo, packed hi}
+    unsigned int* wind_count;
+    unsigned long long wind_cap;
+    int* v64_index;
+    uint32_t* v64_cells;
+    unsigned int* v64_count;
+    unsigned long long v64_cap;
+    int* err;
+};
+cudaError_t launch_face_place(const FacePlaceParams& P, long long max_faces, int num_sms, cudaStream_t s);
+
 struct Tri64Params {
     const int4* quads;
     const uint32_t* items;

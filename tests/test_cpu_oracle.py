@@ -63,6 +63,20 @@ def test_oracle_matches_golden(path):
     assert np.abs(r["V"] - g["V"]).max(initial=0.0) <= 1e-12
 
 
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLDEN, "dc_*.npz"))),
+                         ids=lambda p: os.path.basename(p)[3:-4])
+def test_oracle_matches_reference_cpu_golden(path):
+    """The committed output of the reference's OWN CPU backend (compiled from its sources,
+    tests/golden/make_golden.py): identical quads (order and winding) and vertex count, and
+    every vertex the float rounding of the oracle's FP64 vertex."""
+    g = np.load(path)
+    r = O.dc_extract(g["values"], tuple(g["dims"]), tuple(g["spacing"]), tuple(g["origin"]), threads=0)
+    assert np.array_equal(r["F"], g["ref_F"])
+    assert len(r["V"]) == len(g["ref_V"]) == int(g["ref_active"])
+    tol = np.maximum(1.2e-7 * np.abs(r["V"]), 1e-9 * g["spacing"].astype(np.float64))
+    assert np.all(np.abs(g["ref_V"].astype(np.float64) - r["V"]) <= tol)
+
+
 def test_golden_fixtures_present():
     assert len(glob.glob(os.path.join(GOLDEN, "dc_*.npz"))) >= 6
 

@@ -130,6 +130,11 @@ def test_engine_matches_golden(backend, path):
     V = mesh.vertices.reshape(-1, 3).astype(np.float64)
     if len(V):
         assert (np.abs(V - g["V"]) / g["spacing"].astype(np.float64)).max() <= VERTEX_TOL
+    # the reference's own CPU backend's output on the same grid (compiled from its sources)
+    assert np.array_equal(mesh.faces.reshape(-1, 4), g["ref_F"])
+    assert stats.vertex_count == len(g["ref_V"]) == int(g["ref_active"])
+    if len(V):
+        assert (np.abs(V - g["ref_V"]) / g["spacing"].astype(np.float64)).max() <= VERTEX_TOL
 
 
 @pytest.mark.parametrize("name", ["sphere32", "csg96", "noise_zeros17x23x9", "ternary", "sphere_zero_shell"])
