@@ -35,6 +35,12 @@ KERNELS_PER_STEP = 16
 # that capture; the kernel streams the grid once, so traffic scales with the number of
 # points). None = not measured.
 MARK_TRAFFIC_BYTES_PER_POINT = (563.814656e6 + 18.4768e6) / 512 ** 3
+# DRAM traffic of a whole extraction (every kernel of one step), as grid-proportional bytes per
+# point plus band-proportional bytes per active cell, from single-kernel-list ncu captures
+# (dram__bytes_read.sum + dram__bytes_write.sum summed over the step's launches). None = not
+# measured.
+PIPELINE_TRAFFIC_BYTES_PER_POINT = None
+PIPELINE_TRAFFIC_BYTES_PER_ACTIVE = None
 
 
 def max_over_ranks(local, dist, device):
@@ -144,20 +150,104 @@ def grid_axes(dims, spacing, origin):
             for a in range(3)]
 
 
-def cpu_sample(slabs, dims, spacing, origin, threads):
+def cpu_sample(slabs, dims, spacing, origin, threads, keep=False):
     """Time the CPU oracle on z-slabs of the grid: ``slabs`` = [((k0, k1), float32 values of
-    planes k0..k1-1)]. Returns (Mcells/s, seconds, cells)."""
+    planes k0..k1-1)]. Returns (Mcells/s, seconds, cells[, per-slab results when keep])."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     nx, ny, _ = dims
     ax = grid_axes(dims, spacing, origin)
-    dt, cells = 0.0, 0
+    dt, cells, kept = 0.0, 0, []
     for (k0, k1), v in slabs:
         t0 = time.perf_counter()
-        O.dc_extract_positions(v, (nx, ny, k1 - k0), ax[0], ax[1], ax[2][k0:k1], threads=threads)
+        r = O.dc_extract_positions(v, (nx, ny, k1 - k0), ax[0], ax[1], ax[2][k0:k1], threads=threads)
         dt += time.perf_counter() - t0
         cells += (nx - 1) * (ny - 1) * (k1 - k0 - 1)
+        if keep:
+            kept.append(r)
+    if keep:
+        return cells / dt / 1e6, dt, cells, kept
     return cells / dt / 1e6, dt, cells
+
+
+# Cells closer than this to a slab's z faces depend on planes outside the slab.
+SLAB_MARGIN = 3
+
+
+def slab_vertex_error(slabs, kept, dims, spacing, V, cells):
+    """Max and RMS difference, in cell widths, between the engine's vertices and the FP64
+    oracle's on the slabs of the CPU sample: every active cell at least SLAB_MARGIN planes
+    inside its slab (the slabs span the whole grid in x and y, so no other cell depends on
+    data outside). Also checks that those cells are the same active cells."""
+    import numpy as np
+    nx, ny, _ = dims
+    cx, cy = nx - 1, ny - 1
+    h = np.asarray(spacing, np.float64)
+    errs = []
+    for ((k0, k1), _), r in zip(slabs, kept):
+        lk = r["cells"] // (cx * cy)
+        inner = (lk >= SLAB_MARGIN) & (lk < (k1 - k0 - 1) - SLAB_MARGIN)
+        glob = r["cells"][inner] + k0 * cx * cy
+        gidx = np.searchsorted(cells, glob)
+        if len(glob) and not np.array_equal(cells[np.minimum(gidx, len(cells) - 1)], glob):
+            raise RuntimeError("engine and oracle active cells differ in slab %s" % ((k0, k1),))
+        errs.append((np.abs(V[gidx].astype(np.float64) - r["V"][inner]) / h).ravel())
+    e = np.concatenate(errs) if errs else np.zeros(0)
+    return {"max_cell_widths": float(e.max()) if e.size else 0.0,
+            "rms_cell_widths": float(np.sqrt(np.mean(e * e))) if e.size else 0.0,
+            "vertices_compared": int(e.size // 3),
+            "against": "FP64 oracle on the CPU-sample slabs (cells >= %d planes inside)" % SLAB_MARGIN}
+
+
+REF_CPU_DC = os.path.join(ROOT, "oracle", "_ref", "ref_cpu_dc")
+REF_CUBE = 40          # points per side of each sub-cube the reference CPU backend runs on
+
+
+def cube_origins(res, n):
+    """n sub-cube corners spread over the grid: the cubes straddle the scene's surface-rich
+    middle third in z and are spaced evenly in x and y."""
+    import numpy as np
+    rng = np.random.default_rng(11)
+    lo, hi = res // 6, res - res // 6 - REF_CUBE
+    return [tuple(int(x) for x in rng.integers(lo, hi, 3)) for _ in range(n)]
+
+
+def ref_cpu_cubes(values_of_cube, origins, spacing, origin, workdir):
+    """Write the sub-cube grids for the reference's own CPU backend (oracle/_ref/ref_cpu_dc):
+    values_of_cube(i0, j0, k0) -> float32 REF_CUBE^3 values (x fastest). Returns the file paths
+    and the cell count."""
+    import numpy as np
+    paths = []
+    for q, (i0, j0, k0) in enumerate(origins):
+        v = values_of_cube(i0, j0, k0)
+        o = [float(np.float32(np.float32(origin[a]) + np.float32((i0, j0, k0)[a]) * np.float32(spacing[a])))
+             for a in range(3)]
+        path = os.path.join(workdir, "cube%d.sdf" % q)
+        with open(path, "wb") as f:
+            f.write(np.array([REF_CUBE] * 3, np.int32).tobytes())
+            f.write(np.array(list(spacing) + o, np.float32).tobytes())
+            f.write(np.ascontiguousarray(v, np.float32).tobytes())
+        paths.append(path)
+    return paths, len(origins) * (REF_CUBE - 1) ** 3
+
+
+def ref_cpu_run(paths, workdir):
+    """One step of the reference CPU arm: the reference's own (single-threaded) CPU backend on
+    every sub-cube at once, one process per cube. Returns wall seconds."""
+    import subprocess
+    t0 = time.perf_counter()
+    procs = [subprocess.Popen([REF_CPU_DC, p, os.path.join(workdir, "out%d.bin" % q)],
+                              stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL) for q, p in enumerate(paths)]
+    rcs = [p.wait() for p in procs]
+    dt = time.perf_counter() - t0
+    if any(rcs):
+        raise RuntimeError("ref_cpu_dc failed: %s" % rcs)
+    return dt
+
+
+def _ref_sample_text(n, res, cells):
+    return ("%d sub-cubes of %d^3 points inside the %d^3 CSG grid (%d cells), the reference's own CPU "
+            "backend (compiled from its sources) on each, one process per cube" % (n, REF_CUBE, res, cells))
 
 
 def _sample_text(dims, ranges, cells, res):
@@ -167,14 +257,49 @@ def _sample_text(dims, ranges, cells, res):
 
 
 def run_reference(args, rank, world):
-    """CPU reference arm: the oracle port with all host threads on a bounded, evenly spread
-    sample of the same grid per step."""
+    """CPU reference arm: the reference's own CPU backend (CpuDualContouringBackend::extract,
+    compiled from its sources into oracle/_ref/ref_cpu_dc) on a bounded sample of the same grid,
+    one process per host core; where that program was not built, the oracle port with all host
+    threads on evenly spread z-slabs."""
     import numpy as np
     from contouring_b200 import synth
     if rank != 0:
         return 0
     threads = os.cpu_count() or 1
     dims = (args.res,) * 3
+    if os.path.exists(REF_CPU_DC):
+        import tempfile
+        ncube = max(1, min(threads, 16))
+        origins = cube_origins(args.res, ncube)
+        spacing = origin = None
+
+        def cube(i0, j0, k0):
+            nonlocal spacing, origin
+            v, _, spacing, origin = synth.csg(args.res, seed=0, device="cpu", planes=(k0, k0 + REF_CUBE))
+            return v.numpy().reshape(REF_CUBE, args.res, args.res)[:, j0:j0 + REF_CUBE, i0:i0 + REF_CUBE].copy()
+
+        with tempfile.TemporaryDirectory() as td:
+            cubes = [cube(*o) for o in origins]
+            paths, cells = ref_cpu_cubes(lambda i0, j0, k0: cubes[origins.index((i0, j0, k0))], origins,
+                                         spacing, origin, td)
+            for _ in range(args.warmup):
+                ref_cpu_run(paths, td)
+            secs = [ref_cpu_run(paths, td) for _ in range(args.steps)]
+        dt = float(np.median(secs))
+        value = cells / dt / 1e6
+        sample = _ref_sample_text(ncube, args.res, cells)
+        line = {
+            "metric": "dc_extract_mcells_per_s", "value": round(value, 4), "unit": "Mcells/s",
+            "impl": "reference", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(1000 * dt, 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "csg%d_dense_dc" % args.res, "grid": list(dims), "sample": sample},
+            "cpu_baseline": {"value": round(value, 4), "unit": "Mcells/s", "cores": ncube,
+                             "kind": "reference", "sample": sample},
+            "e2e": {"value": round(value, 4), "unit": "Mcells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line), flush=True)
+        return 0
     ranges = slab_ranges(args.res, args.ref_zslab)
     slabs = []
     for r in ranges:
@@ -782,19 +907,65 @@ def main():
     mark_bytes = 4.0 * npts                       # algorithmic: every grid value read once
     achieved = mark_bytes / (mark_avg_ms / 1e3) / 1e9
     nv, nf = stats.vertex_count, stats.face_count
+    # whole extraction: grid read once, vertices and quads written once
     pipe_bytes = 4.0 * npts + 12.0 * nv + 16.0 * nf
     pipe_gbs = pipe_bytes / (ms_step / 1e3) / 1e9
     traffic = (MARK_TRAFFIC_BYTES_PER_POINT * npts) if MARK_TRAFFIC_BYTES_PER_POINT else None
+    pipe_traffic = None
+    if PIPELINE_TRAFFIC_BYTES_PER_POINT and PIPELINE_TRAFFIC_BYTES_PER_ACTIVE:
+        pipe_traffic = PIPELINE_TRAFFIC_BYTES_PER_POINT * npts + PIPELINE_TRAFFIC_BYTES_PER_ACTIVE * nv
+    # stage times of the last timed extraction (CUDA events inside the library)
+    band_bytes = 12.0 * nv                         # vertices written (stencils come from L2 / HBM re-reads)
+    face_bytes = 16.0 * nf
+    kernels = [
+        {"stage": "mark (k_mark_zmarch)", "ms": round(stats.marking_ms, 4), "algorithmic_bytes": mark_bytes,
+         "achieved_gbs": round(mark_bytes / (stats.marking_ms / 1e3) / 1e9, 1) if stats.marking_ms else None,
+         "frac": round(mark_bytes / (stats.marking_ms / 1e3) / 1e9 / peak, 4) if stats.marking_ms else None},
+        {"stage": "segment scan", "ms": round(stats.compaction_ms, 4)},
+        {"stage": "vertices (k_expand_ranks, k_band, k_cell_jacobi, k_vertex_fp64)", "ms": round(stats.qef_ms, 4),
+         "algorithmic_bytes": band_bytes},
+        {"stage": "faces (column scan, k_face_place, FP64 windings, k_face_order)",
+         "ms": round(stats.face_emission_ms, 4), "algorithmic_bytes": face_bytes,
+         "sub_ms": {"count": round(stats.face_count_ms, 4), "prefix_sum": round(stats.face_prefix_sum_ms, 4),
+                    "fill": round(stats.face_fill_ms, 4)}},
+    ]
 
     cpu = None
+    vertex_error = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         ranges = slab_ranges(dims[2], args.ref_zslab)
         plane = dims[0] * dims[1]
         slabs = [(r, vals[r[0] * plane:r[1] * plane].cpu().numpy()) for r in ranges]
-        rate, dt, cells = cpu_sample(slabs, dims, spacing, origin, threads)
+        rate, dt, cells, kept = cpu_sample(slabs, dims, spacing, origin, threads, keep=True)
+        # one host thread, as the reference CPU backend runs, on the first slab
+        rate1, dt1, cells1 = cpu_sample(slabs[:1], dims, spacing, origin, 1)
         cpu = {"value": round(rate, 3), "unit": "Mcells/s", "cores": threads, "kind": "port",
-               "sample": _sample_text(dims, ranges, cells, args.res) + ", %.1f s" % dt}
+               "sample": _sample_text(dims, ranges, cells, args.res) + ", %.1f s" % dt,
+               "single_thread": {"value": round(rate1, 3), "unit": "Mcells/s", "cores": 1,
+                                 "sample": "the first of those slabs (%d cells), %.1f s" % (cells1, dt1)}}
+        if os.path.exists(REF_CPU_DC):
+            # the reference's own CPU backend (compiled from its sources), one process per cube
+            import tempfile
+            ncube = max(1, min(threads, 16))
+            origins = cube_origins(args.res, ncube)
+            vz = vals.view(dims[2], dims[1], dims[0])
+
+            def cube(i0, j0, k0):
+                return vz[k0:k0 + REF_CUBE, j0:j0 + REF_CUBE, i0:i0 + REF_CUBE].cpu().numpy()
+
+            with tempfile.TemporaryDirectory() as td:
+                paths, rcells = ref_cpu_cubes(cube, origins, spacing, origin, td)
+                ref_cpu_run(paths, td)
+                rdt = ref_cpu_run(paths, td)
+            port = dict(cpu)
+            cpu = {"value": round(rcells / rdt / 1e6, 4), "unit": "Mcells/s", "cores": ncube, "kind": "reference",
+                   "sample": _ref_sample_text(ncube, args.res, rcells) + ", %.1f s" % rdt, "port": port}
+        # vertex error of this run against the FP64 oracle on the same slabs
+        Vt, _, _ = be.extract_tensor(vals, dims, spacing, origin)
+        vertex_error = slab_vertex_error(slabs, kept, dims, spacing, Vt.cpu().numpy().reshape(-1, 3),
+                                         be.active_cells())
+        del Vt
 
     if rank == 0:
         line = {
@@ -806,15 +977,21 @@ def main():
                        "cells": ncell, "vertices": nv, "quads": nf,
                        "l2": "input (%.2f GB) larger than L2; no flush needed" % (4 * npts / 1e9),
                        "parallelism": "replicas: one independent grid per rank"},
-            "roofline": {"bound": "hbm", "kernel": "k_mark_zmarch", "achieved": round(achieved, 1),
-                         "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                         "traffic": traffic, "peak_source": peak_kind,
-                         "algorithmic_bytes": mark_bytes, "avg_launch_ms": round(mark_avg_ms, 4)},
-            "pipeline_roofline": {"algorithmic_bytes": pipe_bytes, "achieved": round(pipe_gbs, 1),
-                                  "frac": round(pipe_gbs / peak, 4), "unit": "GB/s"},
+            # the whole extraction (every kernel of a step) against the measured copy bandwidth
+            "roofline": {"bound": "hbm", "kernel": "whole extraction (%d launches)" % KERNELS_PER_STEP,
+                         "achieved": round(pipe_gbs, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(pipe_gbs / peak, 4), "traffic": pipe_traffic, "peak_source": peak_kind,
+                         "algorithmic_bytes": pipe_bytes, "avg_launch_ms": round(ms_step, 4)},
+            # the grid scan alone (the one kernel that streams the 4 GB grid)
+            "mark_roofline": {"bound": "hbm", "kernel": "k_mark_zmarch", "achieved": round(achieved, 1),
+                              "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                              "traffic": traffic, "peak_source": peak_kind,
+                              "algorithmic_bytes": mark_bytes, "avg_launch_ms": round(mark_avg_ms, 4)},
+            "kernels": kernels,
             "stage_ms": {"mark": round(stats.marking_ms, 4), "scan": round(stats.compaction_ms, 4),
                          "qef": round(stats.qef_ms, 4),
                          "faces": round(stats.face_emission_ms, 4)},
+            "vertex_error": vertex_error,
             "escalated_fp64_cells": stats.escalated_fp64_cells, "winding_fp64_faces": stats.winding_fp64_faces,
             "e2e": {"value": round(e2e_value, 2) if e2e_value else None, "unit": "Mcells/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ms_per_step": round(e2e_s * 1e3, 2),

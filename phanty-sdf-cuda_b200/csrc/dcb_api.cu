@@ -435,10 +435,11 @@ int batch_rest(dcb_context* h, const BatchLayout& L, TableView& T, const dcb_opt
     xp.cell_slot = n > 1 ? as<uint32_t>(h->cell_slot) : nullptr;
     xp.B.cell_slot = nullptr;                      // expand finds grids by segment
     xp.list_cap = cap;
-    DCB_TRY(h, launch_expand(xp, h->num_sms, s), "launch expand");
-    // A single grid outside a captured graph runs the tile band kernel (vertices and staged
-    // faces from shared-memory stencils); batches run the per-cell kernels.
+    // A single grid outside a captured graph runs the tile band kernel (ranks, the active-cell
+    // list, vertices and staged faces from shared-memory stencils); batches run the rank
+    // expansion and the per-cell kernels.
     const bool band = n == 1 && live == nullptr;
+    if (!band) DCB_TRY(h, launch_expand(xp, h->num_sms, s), "launch expand");
     QefParams qp;
     qp.B = T.B; qp.list = xp.list; qp.nactive = cap; qp.live = live; qp.V = as<float>(h->V); qp.vclass = as<uint8_t>(h->vclass);
     qp.fmask = as<uint8_t>(h->fmask); qp.col_count = as<uint32_t>(h->col_count);
@@ -451,7 +452,7 @@ int batch_rest(dcb_context* h, const BatchLayout& L, TableView& T, const dcb_opt
         const GridSlot& S = L.slots[0];
         BandParams bp;
         bp.S = S;
-        bp.bits = xp.bits; bp.super = xp.super;
+        bp.bits = xp.bits; bp.seg_start = xp.seg_start; bp.super = xp.super; bp.list = xp.list;
         bp.nxc = ((S.g.cx + 31) / 32 + 31) / 32;
         bp.nyb = (S.g.cy + band_tile_rows() - 1) / band_tile_rows();
         bp.nzb = (S.g.cz + band_tile_planes() - 1) / band_tile_planes();

@@ -16,7 +16,10 @@
 // the bit words (lane per word), and for each such tile:
 //   1. stages the 35 x 7 x 7 grid points around it (every 4x4x4 stencil of its cells) in
 //      shared memory, with the tile's and the surrounding rows' active words and the global
-//      rank of each word's first active cell (super-word rank + popcounts);
+//      rank of each word's first active cell (the mark segment's first rank + popcounts of
+//      the segment's earlier words, a warp scan over the chunk's words; the chunk also writes
+//      the super-word ranks of its rows and, per cell, the packed active-cell list, so no
+//      separate rank expansion runs);
 //   2. lists, row by row with ballots, the crossing edges of the tile's active cells;
 //   3. computes, a thread per listed edge, the edge's averaged normal ONCE (four trilinear
 //      gradients, each an edge difference plus two bilinear differences of the staged
@@ -60,6 +63,8 @@ struct BandSmem {
     uint16_t cells[kTileCells];        // active tile cells: (kk * 4 + jj) << 5 | bit
     uint32_t word[kTZ + 1][kTY + 1];   // active word of cell rows (y0-1+a, z0-1+b) -> [b][a]
     uint32_t rank0[kTZ + 1][kTY + 1];  // global rank of that word's first active cell
+    uint32_t cw[kTZ + 1][kTY + 1][32]; // the chunk's words of those rows, [..][x-word in chunk]
+    uint32_t cr[kTZ + 1][kTY + 1][32]; // global rank of each such word's first active cell
     uint32_t tiles;                    // active tiles of the chunk
     unsigned int chunk;
     unsigned int hist;
@@ -235,6 +240,36 @@ k_band(const __grid_constant__ BandParams P) {
             __syncthreads();
         }
         uint32_t tiles = s.tiles;
+        if (tiles) {
+            // words and first ranks of the chunk's rows and the rows below / behind them: lane =
+            // word; a segment's earlier words are summed by a scan of width tw (the mark's
+            // segment, 32 or 8 words, aligned with the chunk)
+            const int w = xc * 32 + lane;
+            const int tw = P.S.tw;
+            for (int q = warp; q < (kTY + 1) * (kTZ + 1); q += kBandThreads / 32) {
+                const int a = q % (kTY + 1), cc = q / (kTY + 1);
+                const int y = y0 - 1 + a, z = z0 - 1 + cc;
+                const bool row_ok = y >= 0 && y < g.cy && z >= 0 && z < g.cz;
+                const long long row = (long long)y + (long long)g.cy * z;
+                const uint32_t word = (row_ok && w < nwx) ? __ldg(P.bits + row * g.W + w) : 0u;
+                const uint32_t cnt = __popc(word);
+                uint32_t incl = cnt;
+                for (int o = 1; o < tw; o <<= 1) {
+                    const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o, tw);
+                    if ((lane & (tw - 1)) >= o) incl += t;
+                }
+                uint32_t start = 0;
+                if (row_ok && w < nwx && ((lane & (tw - 1)) == 0 || word))
+                    start = __ldg(P.seg_start + row * P.S.nxt + w / tw);
+                start = __shfl_sync(0xffffffffu, start, lane & ~(tw - 1), 32);
+                const uint32_t r0 = start + incl - cnt;
+                s.cw[cc][a][lane] = word;
+                s.cr[cc][a][lane] = r0;
+                // the chunk's own rows: rank of the first active cell of each 8-word super word
+                if (row_ok && a >= 1 && cc >= 1 && w < g.W && (w & 7) == 0) P.super[row * g.W8 + (w >> 3)] = r0;
+            }
+            __syncthreads();
+        }
         while (tiles) {
             const int tb = __ffs(tiles) - 1;
             tiles &= tiles - 1;
@@ -265,24 +300,8 @@ k_band(const __grid_constant__ BandParams P) {
                 s.rw[2][q] = 1.f / (pos_axis(g.oz, g.vz, z + 1) - pos_axis(g.oz, g.vz, z));
             } else if (tid >= 64 && tid < 64 + (kTY + 1) * (kTZ + 1)) {
                 const int q = tid - 64, a = q % (kTY + 1), cc = q / (kTY + 1);
-                const int y = y0 - 1 + a, z = z0 - 1 + cc;
-                uint32_t word = 0, r0 = 0;
-                if (y >= 0 && y < g.cy && z >= 0 && z < g.cz) {
-                    const long long row = (long long)y + (long long)g.cy * z;
-                    word = __ldg(P.bits + row * g.W + w);
-                    if (word) {
-                        const int sw = w >> 3;
-                        r0 = __ldg(P.super + row * g.W8 + sw);
-                        const uint4* p = reinterpret_cast<const uint4*>(P.bits + row * g.W + 8 * sw);
-                        const uint4 u0 = __ldg(p), u1 = __ldg(p + 1);
-                        const uint32_t ws[8] = {u0.x, u0.y, u0.z, u0.w, u1.x, u1.y, u1.z, u1.w};
-                        const int wl = w & 7;
-#pragma unroll
-                        for (int q8 = 0; q8 < 8; ++q8) if (q8 < wl) r0 += __popc(ws[q8]);
-                    }
-                }
-                s.word[cc][a] = word;
-                s.rank0[cc][a] = r0;
+                s.word[cc][a] = s.cw[cc][a][tb];
+                s.rank0[cc][a] = s.cr[cc][a][tb];
             }
             __syncthreads();
             // 3) edge rows: crossing edges (Hermite test) of the tile's active cells; then the
@@ -365,6 +384,7 @@ k_band(const __grid_constant__ BandParams P) {
                 const int i = x0 + b, j = y0 + jj, k = z0 + kk;
                 const uint32_t r = rank_in(s, jj + 1, kk + 1, b);
                 if ((long long)r >= P.nv) { set_error(P.err, kErrInternal); continue; }
+                P.list[r] = pack_cell(i, j, k);
                 float c[8];
 #pragma unroll
                 for (int q = 0; q < 8; ++q) c[q] = sval(s, b + corner_dx(q), jj + corner_dy(q), kk + corner_dz(q));

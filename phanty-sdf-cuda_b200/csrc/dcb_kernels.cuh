@@ -211,8 +211,10 @@ cudaError_t launch_triangulate(const TriParams& P, long long max_quads, int num_
 // per cell row), handed out by an atomic counter.
 struct BandParams {
     GridSlot S;                    // the grid
-    const uint32_t* bits;          // its active bits and super-word ranks
-    const uint32_t* super;
+    const uint32_t* bits;          // its active bits (mark)
+    const uint32_t* seg_start;     // first global rank of every mark segment (scan)
+    uint32_t* super;               // written: rank of the first active cell of every 256-cell word
+    uint64_t* list;                // written: packed cell of every rank
     int nxc, nyb, nzb;             // chunks along x (32 words each), row blocks, plane blocks
     long long nchunks;
     unsigned int* chunk_next;      // chunk counter, zero before the launch
