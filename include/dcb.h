@@ -223,6 +223,13 @@ int dcb_copy_cells_to_host(dcb_handle h, int64_t* cell_linear_index, void* cuda_
 int dcb_mark_active_cells_noalloc(const dcb_grid* grid, int64_t* cells, int64_t capacity,
                                   int64_t* count, void* cuda_stream);
 
+/* Test hook (no counterpart in the reference; the host-side failure injection of a forced
+ * allocation failure): after `allowed` more device or page-locked host allocations, every
+ * allocation the library attempts fails as cudaMalloc does when the device is out of memory,
+ * so entry points return DCB_ERR_OUT_OF_MEMORY; allowed < 0 turns the hook off. Process-wide,
+ * for tests; a handle stays usable after such a failure. Returns DCB_OK. */
+int dcb_debug_fail_allocations(int64_t allowed);
+
 /* ---- files either side of the extraction (src/cpp/dc_cli.cpp:17-47) -------------------- */
 
 /* Replaces dc_cli's write_obj (dc_cli.cpp:17-29): "v x y z" lines (6 significant digits, the

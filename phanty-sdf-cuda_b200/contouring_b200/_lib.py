@@ -33,7 +33,7 @@ EXPORTED = (
     "dcb_write_obj", "dcb_read_sdf", "dcb_write_sdf", "dcb_extract_upload", "dcb_mesh_to_sdf_device_ex",
     "dcb_mesh_to_sdf_host_ex", "dcb_batch_graph_create", "dcb_batch_graph_launch", "dcb_batch_graph_finish",
     "dcb_batch_graph_destroy", "dcb_postprocess_device", "dcb_postprocess_host", "dcb_copy_post_mesh",
-    "dcb_read_obj", "dcb_obj_grid")
+    "dcb_read_obj", "dcb_obj_grid", "dcb_debug_fail_allocations")
 
 
 class DcbGrid(ctypes.Structure):
@@ -173,6 +173,8 @@ def lib():
     L.dcb_copy_mesh_device.restype = ctypes.c_int
     L.dcb_copy_cells_to_host.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
     L.dcb_copy_cells_to_host.restype = ctypes.c_int
+    L.dcb_debug_fail_allocations.argtypes = [ctypes.c_int64]
+    L.dcb_debug_fail_allocations.restype = ctypes.c_int
     L.dcb_mark_active_cells_noalloc.argtypes = [P(DcbGrid), ctypes.c_void_p, ctypes.c_int64,
                                                 P(ctypes.c_int64), ctypes.c_void_p]
     L.dcb_mark_active_cells_noalloc.restype = ctypes.c_int

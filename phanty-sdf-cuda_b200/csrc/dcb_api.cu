@@ -22,6 +22,7 @@
 #include <cmath>
 #include <string>
 #include <algorithm>
+#include <atomic>
 #include <vector>
 #include "dcb_kernels.cuh"
 #include "../../include/dcb.h"
@@ -101,6 +102,33 @@ struct dcb_context {
     int64_t pp_nv = 0, pp_nf = 0;
 };
 
+namespace dcb {
+
+// dcb_debug_fail_allocations: < 0 off; otherwise the number of allocations still allowed before
+// every further one fails.
+std::atomic<long long> g_alloc_budget{-1};
+
+static bool allocation_refused() {
+    long long b = g_alloc_budget.load();
+    while (b >= 0) {
+        if (b == 0) return true;
+        if (g_alloc_budget.compare_exchange_weak(b, b - 1)) return false;
+    }
+    return false;
+}
+
+cudaError_t dev_malloc(void** p, size_t bytes) {
+    if (allocation_refused()) { *p = nullptr; return cudaErrorMemoryAllocation; }
+    return cudaMalloc(p, bytes);
+}
+
+cudaError_t host_malloc(void** p, size_t bytes) {
+    if (allocation_refused()) { *p = nullptr; return cudaErrorMemoryAllocation; }
+    return cudaMallocHost(p, bytes);
+}
+
+}  // namespace dcb
+
 namespace {
 
 int fail(dcb_context* h, int code, const std::string& msg) {
@@ -125,7 +153,7 @@ cudaError_t ensure(DevBuf& b, size_t bytes) {
     if (b.bytes >= bytes) return cudaSuccess;
     if (b.p) { cudaFree(b.p); b.p = nullptr; b.bytes = 0; }
     const size_t want = bytes + bytes / 8;   // headroom for slowly growing workloads
-    cudaError_t e = cudaMalloc(&b.p, want);
+    cudaError_t e = dev_malloc(&b.p, want);
     if (e != cudaSuccess) { cudaGetLastError(); return e; }
     b.bytes = want;
     return cudaSuccess;
@@ -136,7 +164,7 @@ cudaError_t ensure_host(void*& p, size_t& have, size_t bytes) {
     if (have >= bytes) return cudaSuccess;
     if (p) { cudaFreeHost(p); p = nullptr; have = 0; }
     const size_t want = bytes + bytes / 8;
-    cudaError_t e = cudaMallocHost(&p, want);
+    cudaError_t e = host_malloc(&p, want);
     if (e != cudaSuccess) { cudaGetLastError(); return e; }
     have = want;
     return cudaSuccess;
@@ -173,10 +201,11 @@ float elapsed(cudaEvent_t a, cudaEvent_t b) {
 struct BatchLayout {
     std::vector<GridSlot> slots;
     std::vector<long long> seg_off, col_off;          // n + 1
+    std::vector<long long> chunk_off;                 // n + 1: first tile-band chunk of each grid
     // mark launches: index 1 for 256-cell x-tiles, 0 for 1024-cell ones
     std::vector<int> tile_slot[2];                    // grids of each mark launch
     std::vector<long long> tile_off[2];               // their first tiles (+ total)
-    long long bits = 0, super = 0, nseg = 0, ncol = 0, ncell = 0;
+    long long bits = 0, super = 0, nseg = 0, ncol = 0, ncell = 0, nchunk = 0;
     float hmax = 0.f;
 };
 
@@ -184,6 +213,7 @@ int layout_batch(dcb_context* h, const dcb_grid* in, int n, BatchLayout& L) {
     L.slots.resize(n);
     L.seg_off.assign(n + 1, 0);
     L.col_off.assign(n + 1, 0);
+    L.chunk_off.assign(n + 1, 0);
     for (int v = 0; v < 2; ++v) { L.tile_slot[v].clear(); L.tile_off[v].assign(1, 0); }
     for (int b = 0; b < n; ++b) {
         GridSlot& S = L.slots[b];
@@ -213,6 +243,8 @@ int layout_batch(dcb_context* h, const dcb_grid* in, int n, BatchLayout& L) {
         S.col_off = L.ncol;
         L.seg_off[b] = L.nseg;
         L.col_off[b] = L.ncol;
+        L.chunk_off[b] = L.nchunk;
+        L.nchunk += band_chunk_count(g.nx, g.ny, g.nz);
         L.bits += rows * g.W;
         L.super += rows * g.W8;
         L.nseg += rows * S.nxt;
@@ -226,6 +258,8 @@ int layout_batch(dcb_context* h, const dcb_grid* in, int n, BatchLayout& L) {
     }
     L.seg_off[n] = L.nseg;
     L.col_off[n] = L.ncol;
+    L.chunk_off[n] = L.nchunk;
+    if (L.nchunk >= 0xffffffffLL) return fail(h, DCB_ERR_TOO_LARGE, "batch too large for the tile band kernel");
     for (int v = 0; v < 2; ++v)
         if (L.tile_off[v].back() > 0x7fffffffLL) return fail(h, DCB_ERR_TOO_LARGE, "grid too large for the tiling");
     if (L.nseg >= 0xffffffffLL || L.ncol >= 0xffffffffLL) return fail(h, DCB_ERR_TOO_LARGE, "batch too large");
@@ -275,8 +309,9 @@ int upload_table(dcb_context* h, const BatchLayout& L, cudaStream_t s, TableView
     const size_t o_col = align_up(o_seg + sizeof(long long) * (n + 1));
     const size_t o_vert = align_up(o_col + sizeof(long long) * (n + 1));
     const size_t o_face = align_up(o_vert + sizeof(unsigned long long) * (n + 1));
+    const size_t o_chunk = align_up(o_face + sizeof(unsigned long long) * (n + 1));
     size_t o_ts[2], o_to[2];
-    size_t at = align_up(o_face + sizeof(unsigned long long) * (n + 1));
+    size_t at = align_up(o_chunk + sizeof(long long) * (n + 1));
     for (int v = 0; v < 2; ++v) { o_ts[v] = at; at = align_up(at + sizeof(int) * L.tile_slot[v].size() + 1); }
     for (int v = 0; v < 2; ++v) { o_to[v] = at; at = align_up(at + sizeof(long long) * L.tile_off[v].size()); }
     const size_t total = at;
@@ -286,6 +321,7 @@ int upload_table(dcb_context* h, const BatchLayout& L, cudaStream_t s, TableView
     std::memcpy(hb + o_slots, L.slots.data(), sizeof(GridSlot) * n);
     std::memcpy(hb + o_seg, L.seg_off.data(), sizeof(long long) * (n + 1));
     std::memcpy(hb + o_col, L.col_off.data(), sizeof(long long) * (n + 1));
+    std::memcpy(hb + o_chunk, L.chunk_off.data(), sizeof(long long) * (n + 1));
     for (int v = 0; v < 2; ++v) {
         std::memcpy(hb + o_ts[v], L.tile_slot[v].data(), sizeof(int) * L.tile_slot[v].size());
         std::memcpy(hb + o_to[v], L.tile_off[v].data(), sizeof(long long) * L.tile_off[v].size());
@@ -297,6 +333,7 @@ int upload_table(dcb_context* h, const BatchLayout& L, cudaStream_t s, TableView
     T.B.n = n;
     T.B.seg_off = reinterpret_cast<const long long*>(db + o_seg);
     T.B.col_off = reinterpret_cast<const long long*>(db + o_col);
+    T.B.chunk_off = reinterpret_cast<const long long*>(db + o_chunk);
     T.vert_off = reinterpret_cast<unsigned long long*>(db + o_vert);
     T.face_off = reinterpret_cast<unsigned long long*>(db + o_face);
     T.B.vert_off = T.vert_off;
@@ -342,7 +379,7 @@ int batch_prepare(dcb_context* h, const dcb_grid* in, int n, cudaStream_t s, Bat
     DCB_TRY(h, ensure(h->col_start, sizeof(uint32_t) * ncol), "alloc column starts");
     const long long plen = std::max(scan_partials_len(ncol), scan_partials_len(nseg));
     DCB_TRY(h, ensure(h->partials, sizeof(uint32_t) * std::max(1LL, plen)), "alloc scan");
-    if (!h->h_counters) DCB_TRY(h, cudaMallocHost(&h->h_counters, sizeof(Counters)), "alloc pinned counters");
+    if (!h->h_counters) DCB_TRY(h, host_malloc(&h->h_counters, sizeof(Counters)), "alloc pinned counters");
     DCB_TRY(h, ensure_host(h->h_offsets, h->h_offsets_bytes, 2 * sizeof(unsigned long long) * (n + 1)), "alloc pinned offsets");
 
 
@@ -362,7 +399,7 @@ int batch_alloc(dcb_context* h, int n, long long cap, const dcb_opts* o, TableVi
     DCB_TRY(h, ensure(h->stage_key, sizeof(uint2) * 3 * cap), "alloc face keys");
     DCB_TRY(h, ensure(h->faces, sizeof(int4) * 3 * cap), "alloc faces");
     DCB_TRY(h, ensure(h->v64_index, sizeof(int) * cap), "alloc fp64 index");
-    if (n == 1) DCB_TRY(h, ensure(h->face_grad, sizeof(float4) * 3 * cap), "alloc staged face gradients");
+    DCB_TRY(h, ensure(h->face_grad, sizeof(float4) * 3 * cap), "alloc staged face gradients");
     if (n > 1) {
         DCB_TRY(h, ensure(h->cell_slot, sizeof(uint32_t) * cap), "alloc vertex grids");
         T.B.cell_slot = as<uint32_t>(h->cell_slot);
@@ -435,35 +472,31 @@ int batch_rest(dcb_context* h, const BatchLayout& L, TableView& T, const dcb_opt
     xp.cell_slot = n > 1 ? as<uint32_t>(h->cell_slot) : nullptr;
     xp.B.cell_slot = nullptr;                      // expand finds grids by segment
     xp.list_cap = cap;
-    // A single grid outside a captured graph runs the tile band kernel (ranks, the active-cell
-    // list, vertices and staged faces from shared-memory stencils); batches run the rank
-    // expansion and the per-cell kernels.
-    const bool band = n == 1 && live == nullptr;
-    if (!band) DCB_TRY(h, launch_expand(xp, h->num_sms, s), "launch expand");
+    // The tile band kernel: ranks, the active-cell list, vertices and staged faces from
+    // shared-memory stencils, over the tiles of every grid of the batch.
+    const bool band = true;
     QefParams qp;
     qp.B = T.B; qp.list = xp.list; qp.nactive = cap; qp.live = live; qp.V = as<float>(h->V); qp.vclass = as<uint8_t>(h->vclass);
     qp.fmask = as<uint8_t>(h->fmask); qp.col_count = as<uint32_t>(h->col_count);
     qp.esc_list = as<uint32_t>(h->esc_list); qp.esc_count = &dc->esc_count;
     qp.hard_list = as<uint32_t>(h->hard_list); qp.hard_data = as<float4>(h->hard_data); qp.hard_count = &dc->hard_count;
     qp.rank_hist = dc->rank_hist;
+    qp.err = &dc->err;
     qp.thr = (float)o->svd_threshold; qp.band = (float)o->fp64_threshold_band;
     qp.cond_max = (float)std::min(o->fp64_escalation_cond, 3.0e38); qp.force64 = o->force_fp64;
     if (band) {
-        const GridSlot& S = L.slots[0];
         BandParams bp;
-        bp.S = S;
+        bp.B = T.B;
         bp.bits = xp.bits; bp.seg_start = xp.seg_start; bp.super = xp.super; bp.list = xp.list;
-        bp.nxc = ((S.g.cx + 31) / 32 + 31) / 32;
-        bp.nyb = (S.g.cy + band_tile_rows() - 1) / band_tile_rows();
-        bp.nzb = (S.g.cz + band_tile_planes() - 1) / band_tile_planes();
-        bp.nchunks = (long long)bp.nxc * bp.nyb * bp.nzb;
+        bp.cell_slot = xp.cell_slot;
+        bp.nchunks = L.nchunk;
         bp.chunk_next = &dc->band_chunk;
         bp.V = qp.V; bp.vclass = qp.vclass; bp.col_count = qp.col_count;
         bp.esc_list = qp.esc_list; bp.esc_count = qp.esc_count;
         bp.hard_list = qp.hard_list; bp.hard_data = qp.hard_data; bp.hard_count = qp.hard_count;
         bp.rank_hist = qp.rank_hist;
         bp.face_cells = as<int4>(h->faces); bp.face_grad = as<float4>(h->face_grad);
-        bp.face_count = &dc->face_staged; bp.face_cap = (unsigned long long)(3 * cap); bp.nv = cap;
+        bp.face_count = &dc->face_staged; bp.face_cap = (unsigned long long)(3 * cap); bp.nv = cap; bp.live = live;
         bp.err = &dc->err;
         bp.thr = qp.thr; bp.band = qp.band; bp.force64 = qp.force64;
         DCB_TRY(h, launch_band(bp, h->num_sms, s), "launch band");
@@ -502,7 +535,7 @@ int batch_rest(dcb_context* h, const BatchLayout& L, TableView& T, const dcb_opt
     fp.hmax = L.hmax;
     if (band) {
         FacePlaceParams pp;
-        pp.S = L.slots[0]; pp.list = xp.list;
+        pp.B = T.B; pp.list = xp.list;
         pp.face_cells = as<int4>(h->faces); pp.face_grad = as<float4>(h->face_grad);
         pp.face_count = &dc->face_staged; pp.face_cap = (unsigned long long)(3 * cap); pp.nv = cap;
         pp.V = qp.V; pp.vclass = qp.vclass;
@@ -558,6 +591,10 @@ int batch_rest(dcb_context* h, const BatchLayout& L, TableView& T, const dcb_opt
 int batch_finish(dcb_context* h, int n, const dcb_opts* o, dcb_stats* st) {
     const Counters* hc = reinterpret_cast<const Counters*>(h->h_counters);
     const unsigned long long* h_face_off = reinterpret_cast<const unsigned long long*>(h->h_offsets) + (n + 1);
+    if (hc->err == kErrNonFinite)
+        return fail(h, DCB_ERR_INVALID_ARGUMENT,
+                    "an infinite grid value at a quad edge's interpolation end: the reference CPU backend "
+                    "cannot find that edge's Hermite sample and exits (contouring.cpp:590-594)");
     if (hc->err) {
         return fail(h, hc->err == kErrTimeout ? DCB_ERR_TIMEOUT : DCB_ERR_INTERNAL,
                     hc->err == kErrOverflow ? "FP64 work list overflow" : "device error flag set");
@@ -745,7 +782,7 @@ int run_sparse(dcb_context* h, const dcb_grid* in, const dcb_opts* o, cudaStream
     DCB_TRY(h, ensure(h->seg_count, sizeof(uint32_t) * nseg), "alloc segment counts");
     DCB_TRY(h, ensure(h->seg_start, sizeof(uint32_t) * nseg), "alloc segment starts");
     DCB_TRY(h, ensure(h->sp_counters, sizeof(unsigned long long) * kScSlots), "alloc counters");
-    if (!h->h_sp_counters) DCB_TRY(h, cudaMallocHost(&h->h_sp_counters, sizeof(unsigned long long) * kScSlots), "alloc pinned counters");
+    if (!h->h_sp_counters) DCB_TRY(h, host_malloc(&h->h_sp_counters, sizeof(unsigned long long) * kScSlots), "alloc pinned counters");
     unsigned long long* dcn = as<unsigned long long>(h->sp_counters);
     unsigned long long* hcn = reinterpret_cast<unsigned long long*>(h->h_sp_counters);
     P.pn = as<uint32_t>(h->sp_words);
@@ -943,7 +980,7 @@ int run_mesh_sdf(dcb_context* h, const float* d_verts, int64_t nv, const int32_t
     DCB_TRY(h, ensure(h->m_ext, sizeof(uint32_t) * rows * P.W), "alloc masks");
     DCB_TRY(h, ensure(h->m_tmp, sizeof(float) * (size_t)nx * ny * nz), "alloc relaxation buffer");
     DCB_TRY(h, ensure(h->m_counters, sizeof(SdfCounters)), "alloc counters");
-    if (!h->h_sdf_counters) DCB_TRY(h, cudaMallocHost(&h->h_sdf_counters, sizeof(SdfCounters)), "alloc pinned counters");
+    if (!h->h_sdf_counters) DCB_TRY(h, host_malloc(&h->h_sdf_counters, sizeof(SdfCounters)), "alloc pinned counters");
     SdfCounters* dc = as<SdfCounters>(h->m_counters);
     SdfCounters* hc = reinterpret_cast<SdfCounters*>(h->h_sdf_counters);
     P.tris = as<float>(h->m_tris);
@@ -1061,6 +1098,11 @@ void dcb_default_opts(dcb_opts* o) {
     o->seed = 0x5eed;
     o->brick_size = 8;
     o->normal_mode = DCB_NORMAL_TRILINEAR;
+}
+
+int dcb_debug_fail_allocations(int64_t allowed) {
+    g_alloc_budget.store(allowed < 0 ? -1 : (long long)allowed);
+    return DCB_OK;
 }
 
 int dcb_abi_version(void) { return DCB_ABI_VERSION; }

@@ -201,25 +201,43 @@ __device__ __forceinline__ unsigned int reserve_slots(unsigned int* counter, uns
     return grp.shfl(base, 0) + pre;
 }
 
+// Chunks of one grid: along x (32 words of 32 cells), row blocks, plane blocks.
+__host__ __device__ inline void band_chunks(const GridDesc& g, int& nxc, int& nyb, int& nzb) {
+    nxc = ((g.cx + 31) / 32 + 31) / 32;
+    nyb = (g.cy + kTY - 1) / kTY;
+    nzb = (g.cz + kTZ - 1) / kTZ;
+}
+
+template <bool ONE>
 __global__ void __launch_bounds__(kBandThreads, 4)
 k_band(const __grid_constant__ BandParams P) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     BandSmem& s = *reinterpret_cast<BandSmem*>(smem_raw);
-    const GridDesc& g = P.S.g;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const long long cxcy = (long long)g.cx * g.cy;
-    const int nwx = (g.cx + 31) >> 5;                 // words holding cells, per row
+    // a captured graph whose live count exceeds the capacity it was built for does nothing
+    // (the host reports the overflow after the replay)
+    if (P.live && *P.live > (unsigned long long)P.nv) return;
     if (tid == 0) s.hist = 0;
 
     for (;;) {
         __syncthreads();
         if (tid == 0) s.chunk = atomicAdd(P.chunk_next, 1u);
         __syncthreads();
-        const long long c = s.chunk;
-        if (c >= P.nchunks) break;
-        const int xc = (int)(c % P.nxc);
-        const int jb = (int)((c / P.nxc) % P.nyb);
-        const int kb = (int)(c / ((long long)P.nxc * P.nyb));
+        const long long cg_ = s.chunk;
+        if (cg_ >= P.nchunks) break;
+        // the chunk's grid (batches: the grids' chunks are concatenated)
+        const int gi = ONE ? 0 : slot_search(P.B.chunk_off, P.B.n, cg_);
+        const GridSlot& S = slot_ref<ONE>(P.B, gi);
+        const GridDesc& g = S.g;
+        const long long c = ONE ? cg_ : cg_ - P.B.chunk_off[gi];
+        const uint32_t* const bits = P.bits + S.bits_off;
+        const long long cxcy = (long long)g.cx * g.cy;
+        const int nwx = (g.cx + 31) >> 5;                 // words holding cells, per row
+        int nxc, nyb, nzb;
+        band_chunks(g, nxc, nyb, nzb);
+        const int xc = (int)(c % nxc);
+        const int jb = (int)((c / nxc) % nyb);
+        const int kb = (int)(c / ((long long)nxc * nyb));
         const int y0 = jb * kTY, z0 = kb * kTZ;
         // 1) active tiles of the chunk: lane = word, warps split the 16 cell rows
         {
@@ -230,7 +248,7 @@ k_band(const __grid_constant__ BandParams P) {
                 for (int q = 0; q < 4; ++q) {
                     const int rr = warp * 4 + q;
                     const int y = y0 + (rr & 3), z = z0 + (rr >> 2);
-                    if (y < g.cy && z < g.cz) any |= __ldg(P.bits + ((long long)y + (long long)g.cy * z) * g.W + w);
+                    if (y < g.cy && z < g.cz) any |= __ldg(bits + ((long long)y + (long long)g.cy * z) * g.W + w);
                 }
             }
             const uint32_t m = __ballot_sync(0xffffffffu, any != 0);
@@ -245,13 +263,13 @@ k_band(const __grid_constant__ BandParams P) {
             // word; a segment's earlier words are summed by a scan of width tw (the mark's
             // segment, 32 or 8 words, aligned with the chunk)
             const int w = xc * 32 + lane;
-            const int tw = P.S.tw;
+            const int tw = S.tw;
             for (int q = warp; q < (kTY + 1) * (kTZ + 1); q += kBandThreads / 32) {
                 const int a = q % (kTY + 1), cc = q / (kTY + 1);
                 const int y = y0 - 1 + a, z = z0 - 1 + cc;
                 const bool row_ok = y >= 0 && y < g.cy && z >= 0 && z < g.cz;
                 const long long row = (long long)y + (long long)g.cy * z;
-                const uint32_t word = (row_ok && w < nwx) ? __ldg(P.bits + row * g.W + w) : 0u;
+                const uint32_t word = (row_ok && w < nwx) ? __ldg(bits + row * g.W + w) : 0u;
                 const uint32_t cnt = __popc(word);
                 uint32_t incl = cnt;
                 for (int o = 1; o < tw; o <<= 1) {
@@ -259,14 +277,13 @@ k_band(const __grid_constant__ BandParams P) {
                     if ((lane & (tw - 1)) >= o) incl += t;
                 }
                 uint32_t start = 0;
-                if (row_ok && w < nwx && ((lane & (tw - 1)) == 0 || word))
-                    start = __ldg(P.seg_start + row * P.S.nxt + w / tw);
+                if (row_ok && w < nwx && (lane & (tw - 1)) == 0) start = __ldg(P.seg_start + S.seg_off + row * S.nxt + w / tw);
                 start = __shfl_sync(0xffffffffu, start, lane & ~(tw - 1), 32);
                 const uint32_t r0 = start + incl - cnt;
                 s.cw[cc][a][lane] = word;
                 s.cr[cc][a][lane] = r0;
                 // the chunk's own rows: rank of the first active cell of each 8-word super word
-                if (row_ok && a >= 1 && cc >= 1 && w < g.W && (w & 7) == 0) P.super[row * g.W8 + (w >> 3)] = r0;
+                if (row_ok && a >= 1 && cc >= 1 && w < g.W && (w & 7) == 0) P.super[S.super_off + row * g.W8 + (w >> 3)] = r0;
             }
             __syncthreads();
         }
@@ -385,6 +402,7 @@ k_band(const __grid_constant__ BandParams P) {
                 const uint32_t r = rank_in(s, jj + 1, kk + 1, b);
                 if ((long long)r >= P.nv) { set_error(P.err, kErrInternal); continue; }
                 P.list[r] = pack_cell(i, j, k);
+                if (!ONE && P.cell_slot) P.cell_slot[r] = (uint32_t)gi;
                 float c[8];
 #pragma unroll
                 for (int q = 0; q < 8; ++q) c[q] = sval(s, b + corner_dx(q), jj + corner_dy(q), kk + corner_dz(q));
@@ -468,6 +486,11 @@ k_band(const __grid_constant__ BandParams P) {
                 const bool fx = j >= 1 && k >= 1 && strict_change(c[0], c[1]);
                 const bool fyy = i >= 1 && k >= 1 && strict_change(c[0], c[3]);
                 const bool fzz = i >= 1 && j >= 1 && strict_change(c[0], c[4]);
+                // the reference looks each quad's Hermite normal up in the cell at (i, j-1, k-1),
+                // (i-1, j, k-1) or (i-1, j-1, k); its sample interpolates from (i+1, j, k) for an
+                // X edge and from (i, j, k) for Y and Z edges: infinite there, the sample is NaN
+                // and the reference exits (contouring.cpp:560-594, 607-729)
+                if ((fx && isinf(c[1])) || ((fyy || fzz) && isinf(c[0]))) set_error(P.err, kErrNonFinite);
                 const unsigned int nfc = (unsigned int)fx + (unsigned int)fyy + (unsigned int)fzz;
                 unsigned int f = reserve_slots(P.face_count, nfc);
                 if (nfc) {
@@ -483,7 +506,7 @@ k_band(const __grid_constant__ BandParams P) {
                         else if (axis == 1) { r1 = rank_in(s, jj + 1, kk, b); r0 = r1 - 1u; r3 = r - 1u; }
                         else { r1 = rank_in(s, jj, kk + 1, b); r0 = r1 - 1u; r3 = r - 1u; }
                         const float3 g1 = gradient_at(s, g, x0, y0, z0, i + (axis == 0), j + (axis == 1), k + (axis == 2));
-                        const long long col = axis * cxcy + (long long)i * g.cy + j;
+                        const long long col = S.col_off + axis * cxcy + (long long)i * g.cy + j;
                         atomicAdd(&P.col_count[col], 1u);
                         if (f < P.face_cap) {
                             P.face_cells[f] = make_int4((int)r0, (int)r1, (int)r, (int)r3);
@@ -501,25 +524,31 @@ k_band(const __grid_constant__ BandParams P) {
     if (tid == 0 && s.hist) atomicAdd(P.rank_hist + 1, (unsigned long long)s.hist);
 }
 
-cudaError_t launch_band(const BandParams& P, int num_sms, cudaStream_t s) {
-    if (P.nchunks <= 0) return cudaSuccess;
-    static bool attr_set = false;
+template <bool ONE>
+cudaError_t launch_band_t(const BandParams& P, int num_sms, cudaStream_t s) {
     const int bytes = (int)sizeof(BandSmem);
-    if (!attr_set) {
-        const cudaError_t e = cudaFuncSetAttribute(k_band, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-        if (e != cudaSuccess) return e;
-        attr_set = true;
-    }
+    cudaError_t e = cudaFuncSetAttribute(k_band<ONE>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e != cudaSuccess) return e;
     int per_sm = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_band, kBandThreads, bytes);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_band<ONE>, kBandThreads, bytes);
     if (e != cudaSuccess) return e;
     long long blocks = (long long)num_sms * (per_sm > 0 ? per_sm : 1);
     if (blocks > P.nchunks) blocks = P.nchunks;
-    k_band<<<(unsigned)blocks, kBandThreads, bytes, s>>>(P);
+    k_band<ONE><<<(unsigned)blocks, kBandThreads, bytes, s>>>(P);
     return cudaGetLastError();
 }
 
-int band_tile_rows() { return kTY; }
-int band_tile_planes() { return kTZ; }
+cudaError_t launch_band(const BandParams& P, int num_sms, cudaStream_t s) {
+    if (P.nchunks <= 0) return cudaSuccess;
+    return P.B.n == 1 ? launch_band_t<true>(P, num_sms, s) : launch_band_t<false>(P, num_sms, s);
+}
+
+long long band_chunk_count(int nx, int ny, int nz) {
+    GridDesc g{};
+    g.cx = nx - 1; g.cy = ny - 1; g.cz = nz - 1;
+    int nxc, nyb, nzb;
+    band_chunks(g, nxc, nyb, nzb);
+    return (long long)nxc * nyb * nzb;
+}
 
 }  // namespace dcb

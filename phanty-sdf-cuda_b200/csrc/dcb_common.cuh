@@ -90,7 +90,11 @@ __device__ __forceinline__ bool hermite_crossing(float a, float b) {
 }
 
 // Error flags written by kernels (first error wins).
-enum DeviceError : int { kErrNone = 0, kErrTimeout = 1, kErrInternal = 2, kErrOverflow = 3, kErrInvalid = 4 };
+// kErrNonFinite: a quad's edge whose Hermite sample the reference CPU backend cannot find
+// again (an infinite value at the end its representative cell interpolates from gives a NaN
+// sample), where that backend exits (src/cpp/contouring.cpp:590-594).
+enum DeviceError : int { kErrNone = 0, kErrTimeout = 1, kErrInternal = 2, kErrOverflow = 3, kErrInvalid = 4,
+                         kErrNonFinite = 5 };
 
 __device__ __forceinline__ void set_error(int* flag, int code) { atomicCAS(flag, 0, code); }
 

@@ -302,24 +302,26 @@ cudaError_t launch_face_scatter(const FaceParams& P, int num_sms, cudaStream_t s
 // gradientAt of its edge's endpoints): the FP32 winding test with its error bound, exactly
 // as emit_face decides it, and the face's slot in its column; uncertain faces are listed for
 // the FP64 re-decision.
+template <bool ONE>
 __global__ void __launch_bounds__(256)
 k_face_place(const __grid_constant__ FacePlaceParams P) {
-    const GridDesc& g = P.S.g;
-    const long long cxcy = (long long)g.cx * g.cy;
     const long long nf = min((long long)*P.face_count, (long long)P.face_cap);
     for (long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x; f < nf;
          f += (long long)gridDim.x * blockDim.x) {
         const int4 q = P.face_cells[f];
         const float4 gg = P.face_grad[f];
-        const uint32_t col = __float_as_uint(gg.w);
-        const int axis = (int)(col / (uint32_t)cxcy);
+        const uint32_t col = __float_as_uint(gg.w);               // column of the whole batch
+        const int gi = ONE ? 0 : slot_of_column(P.B, (long long)col);
+        const GridSlot& S = slot_ref<ONE>(P.B, gi);
+        const long long cxcy = (long long)S.g.cx * S.g.cy;
+        const int axis = (int)(((long long)col - S.col_off) / cxcy);
         const uint32_t r0 = (uint32_t)q.x, r1 = (uint32_t)q.y, r2 = (uint32_t)q.z, r3 = (uint32_t)q.w;
         if ((long long)max(max(r0, r1), max(r2, r3)) >= P.nv || axis > 2) { set_error(P.err, kErrInternal); continue; }
         const uint64_t pk = __ldg(reinterpret_cast<const unsigned long long*>(P.list) + r2);
         const uint32_t k = (uint32_t)(pk >> 42);
         const float3 gn = make_float3(gg.x, gg.y, gg.z);
         const float3 pa = ldv(P.V, r0), pb = ldv(P.V, r1), pc = ldv(P.V, r2), pd = ldv(P.V, r3);
-        const float dv = quad_vertex_bound(P.vclass, r0, r1, r2, r3, pa, pb, pc, pd, P.S.hmax);
+        const float dv = quad_vertex_bound(P.vclass, r0, r1, r2, r3, pa, pb, pc, pd, S.hmax);
         const float3 ba = sub3(pb, pa), da = sub3(pd, pa), ca = sub3(pc, pa);
         float3 qn = cross3(ba, da);
         float qn2 = dot3(qn, qn);
@@ -341,7 +343,7 @@ k_face_place(const __grid_constant__ FacePlaceParams P) {
         P.stage_key[slot] = make_uint2(k, col);
         if (uncertain) {
             const unsigned int w = atomicAdd(P.wind_count, 1u);
-            if (w < P.wind_cap) P.wind_items[w] = make_uint4(slot, (uint32_t)axis, (uint32_t)pk, (uint32_t)(pk >> 32));
+            if (w < P.wind_cap) P.wind_items[w] = make_uint4(slot, (uint32_t)axis | ((uint32_t)gi << 2), (uint32_t)pk, (uint32_t)(pk >> 32));
             else set_error(P.err, kErrOverflow);
             const uint32_t rq[4] = {r0, r1, r2, r3};
 #pragma unroll
@@ -356,7 +358,8 @@ cudaError_t launch_face_place(const FacePlaceParams& P, long long max_faces, int
     long long blocks = (max_faces + 255) / 256;
     const long long cap = (long long)num_sms * 16;
     if (blocks > cap) blocks = cap;
-    k_face_place<<<(unsigned)blocks, 256, 0, s>>>(P);
+    if (P.B.n == 1) k_face_place<true><<<(unsigned)blocks, 256, 0, s>>>(P);
+    else            k_face_place<false><<<(unsigned)blocks, 256, 0, s>>>(P);
     return cudaGetLastError();
 }
 

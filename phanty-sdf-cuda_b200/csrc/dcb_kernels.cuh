@@ -32,6 +32,7 @@ struct BatchTable {
     const long long* col_off;              // [n+1] first face column per grid
     const unsigned long long* vert_off;    // [n+1] first vertex rank per grid (after the scan)
     const uint32_t* cell_slot;             // [active] grid of every vertex rank (n > 1, after expand)
+    const long long* chunk_off;            // [n+1] first tile-band chunk per grid
 };
 
 // Largest index b in [0, n) with offs[b] <= x (offsets ascending, offs[0] = 0).
@@ -60,6 +61,11 @@ __device__ __forceinline__ int slot_of_segment(const BatchTable& B, long long s)
 __device__ __forceinline__ int slot_of_column(const BatchTable& B, long long c) {
     return B.n == 1 ? 0 : slot_search(B.col_off, B.n, c);
 }
+
+// Device and pinned-host allocations of the library go through these two (dcb_api.cu); the test
+// hook dcb_debug_fail_allocations makes them fail as if the device were out of memory.
+cudaError_t dev_malloc(void** p, size_t bytes);
+cudaError_t host_malloc(void** p, size_t bytes);
 
 struct MarkParams {
     BatchTable B;
@@ -119,6 +125,7 @@ struct QefParams {
     float4* hard_data;              // [3 per hard cell]: A^T A (6), A^T b (3), centroid (3)
     unsigned int* hard_count;
     unsigned long long* rank_hist;  // [4]
+    int* err;
     float thr;
     float band;
     float cond_max;
@@ -210,13 +217,13 @@ cudaError_t launch_triangulate(const TriParams& P, long long max_quads, int num_
 // Work unit: a chunk of up to 32 x-adjacent tiles of 32 x 4 x 4 cells (one active-bit word
 // per cell row), handed out by an atomic counter.
 struct BandParams {
-    GridSlot S;                    // the grid
-    const uint32_t* bits;          // its active bits (mark)
+    BatchTable B;                  // the grids (B.chunk_off: first chunk of each)
+    const uint32_t* bits;          // active bits of all grids (mark)
     const uint32_t* seg_start;     // first global rank of every mark segment (scan)
     uint32_t* super;               // written: rank of the first active cell of every 256-cell word
     uint64_t* list;                // written: packed cell of every rank
-    int nxc, nyb, nzb;             // chunks along x (32 words each), row blocks, plane blocks
-    long long nchunks;
+    uint32_t* cell_slot;           // written (batches, may be null): grid of every rank
+    long long nchunks;             // all grids' chunks
     unsigned int* chunk_next;      // chunk counter, zero before the launch
     float* V;
     uint8_t* vclass;
@@ -231,19 +238,20 @@ struct BandParams {
     float4* face_grad;             // staged faces: gradientAt(p0) + gradientAt(p1), column in w
     unsigned int* face_count;
     unsigned long long face_cap;
-    long long nv;                  // active cells (vertex ranks are below it)
+    long long nv;                  // active cells (vertex ranks are below it); capacity with live
+    const unsigned long long* live; // device count of active cells (a captured graph; above nv,
+                                    // nothing is processed), or null
     int* err;
     float thr;
     float band;
     int force64;
 };
 cudaError_t launch_band(const BandParams& P, int num_sms, cudaStream_t s);
-int band_tile_rows();
-int band_tile_planes();
+long long band_chunk_count(int nx, int ny, int nz);   // band kernel work units of one grid
 
 // Staged faces -> FP32 winding decision and their slot in the column order (dcb_band.cu).
 struct FacePlaceParams {
-    GridSlot S;
+    BatchTable B;
     const uint64_t* list;
     const int4* face_cells;
     const float4* face_grad;

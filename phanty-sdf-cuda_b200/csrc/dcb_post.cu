@@ -887,7 +887,7 @@ cudaError_t grow(PostBuf& b, size_t bytes) {
     b.p = nullptr;
     b.bytes = 0;
     const size_t want = std::max<size_t>(256, (bytes + 255) & ~(size_t)255);
-    cudaError_t e = cudaMalloc(&b.p, want);
+    cudaError_t e = dev_malloc(&b.p, want);
     if (e != cudaSuccess) { cudaGetLastError(); return e; }
     b.bytes = want;
     return cudaSuccess;
@@ -994,7 +994,7 @@ cudaError_t post_run(PostWork& W, PostRun& R, cudaStream_t s) {
     R.nv_out = R.nf_out = 0;
     const long long nv = R.nv, nf = R.nf;
     const int sms = R.num_sms;
-    if (!W.hcount) PP_TRY(cudaMallocHost(&W.hcount, sizeof(PostCounters)));
+    if (!W.hcount) PP_TRY(host_malloc(&W.hcount, sizeof(PostCounters)));
     PP_TRY(grow(W.count, sizeof(PostCounters)));
     PP_TRY(cudaMemsetAsync(W.count.p, 0, sizeof(PostCounters), s));
     PostCounters* C = as<PostCounters>(W.count);

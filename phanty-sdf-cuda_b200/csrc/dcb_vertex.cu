@@ -147,6 +147,9 @@ k_cell_qef(const __grid_constant__ QefParams P) {
         if (i >= 1 && j >= 1 && strict_change(c[0], c[4])) {
             fm |= 4; atomicAdd(&col_count[2 * cxcy + (long long)i * g.cy + j], 1u);
         }
+        // an infinite value where the reference's face lookup interpolates from: it exits
+        // (contouring.cpp:560-594); the host reports DCB_ERR_INVALID_ARGUMENT
+        if (((fm & 1) && isinf(c[1])) || ((fm & 6) && isinf(c[0]))) set_error(P.err, kErrNonFinite);
         P.fmask[r] = fm;
 
         // Pass 1: crossing edges and the centroid in local units.
