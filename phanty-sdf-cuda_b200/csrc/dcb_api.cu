@@ -61,7 +61,7 @@ struct dcb_context {
     bool substage_events = false;     // ev[8] / ev[9] hold the face sub-stages of the last call
     DevBuf grid, bits, super, list, seg_count, seg_start, counters, V, vclass, fmask, col_count, col_fill,
         col_start, partials, esc_list, hard_list, hard_data, stage_quad, stage_key, faces, wind_items,
-        v64_index, v64_cells, V64, tris, tri_items, adj_rows, adj_owners, ours_ws, face_grad;
+        v64_index, v64_cells, V64, tris, tri_items, adj_rows, adj_owners, ours_ws, face_grad, tilemap;
     // sparse backends
     DevBuf sp_words, sp_brick, sp_vcount, sp_vstart, sp_vtmp, sp_ntmp, sp_N, sp_vcell, sp_fcount, sp_fstart,
         sp_stage, sp_counters;
@@ -244,6 +244,7 @@ int layout_batch(dcb_context* h, const dcb_grid* in, int n, BatchLayout& L) {
         L.seg_off[b] = L.nseg;
         L.col_off[b] = L.ncol;
         L.chunk_off[b] = L.nchunk;
+        S.chunk_off = L.nchunk;
         L.nchunk += band_chunk_count(g.nx, g.ny, g.nz);
         L.bits += rows * g.W;
         L.super += rows * g.W8;
@@ -353,6 +354,7 @@ int launch_marks(dcb_context* h, const BatchLayout& L, const TableView& T, cudaS
         mp.B = T.B; mp.tile_slot = T.tile_slot[v]; mp.tile_off = T.tile_off[v];
         mp.m = (int)L.tile_slot[v].size(); mp.ntiles = L.tile_off[v].back();
         mp.bits = as<uint32_t>(h->bits); mp.seg_count = as<uint32_t>(h->seg_count);
+        mp.tilemap = as<uint32_t>(h->tilemap);
         DCB_TRY(h, launch_mark(mp, v ? mark_narrow_tile_words() : mark_tile_words(), s), "launch mark");
     }
     return DCB_OK;
@@ -374,6 +376,7 @@ int batch_prepare(dcb_context* h, const dcb_grid* in, int n, cudaStream_t s, Bat
     DCB_TRY(h, ensure(h->seg_count, sizeof(uint32_t) * nseg), "alloc segment counts");
     DCB_TRY(h, ensure(h->seg_start, sizeof(uint32_t) * nseg), "alloc segment starts");
     DCB_TRY(h, ensure(h->counters, sizeof(Counters)), "alloc counters");
+    DCB_TRY(h, ensure(h->tilemap, sizeof(uint32_t) * std::max(1LL, L.nchunk)), "alloc tile map");
     DCB_TRY(h, ensure(h->col_count, sizeof(uint32_t) * ncol), "alloc column counts");
     DCB_TRY(h, ensure(h->col_fill, sizeof(uint32_t) * ncol), "alloc column fill");
     DCB_TRY(h, ensure(h->col_start, sizeof(uint32_t) * ncol), "alloc column starts");
@@ -422,6 +425,7 @@ int batch_alloc(dcb_context* h, int n, long long cap, const dcb_opts* o, TableVi
 int batch_mark(dcb_context* h, const BatchLayout& L, const TableView& T, cudaStream_t s, bool events) {
     Counters* dc = as<Counters>(h->counters);
     DCB_TRY(h, cudaMemsetAsync(h->counters.p, 0, sizeof(Counters), s), "memset counters");
+    DCB_TRY(h, cudaMemsetAsync(h->tilemap.p, 0, sizeof(uint32_t) * std::max(1LL, L.nchunk), s), "memset tile map");
     int rc = launch_marks(h, L, T, s);
     if (rc != DCB_OK) return rc;
     if (events) DCB_TRY(h, cudaEventRecord(h->ev[6], s), "event");
@@ -489,6 +493,7 @@ int batch_rest(dcb_context* h, const BatchLayout& L, TableView& T, const dcb_opt
         bp.B = T.B;
         bp.bits = xp.bits; bp.seg_start = xp.seg_start; bp.super = xp.super; bp.list = xp.list;
         bp.cell_slot = xp.cell_slot;
+        bp.tilemap = as<uint32_t>(h->tilemap);
         bp.nchunks = L.nchunk;
         bp.chunk_next = &dc->band_chunk;
         bp.V = qp.V; bp.vclass = qp.vclass; bp.col_count = qp.col_count;
@@ -1148,7 +1153,7 @@ int dcb_destroy(dcb_handle h) {
                       &h->V, &h->vclass, &h->fmask, &h->col_count, &h->col_fill, &h->col_start,
                       &h->partials, &h->esc_list, &h->hard_list, &h->hard_data, &h->stage_quad,
                       &h->stage_key, &h->faces, &h->wind_items, &h->v64_index, &h->v64_cells, &h->V64,
-                      &h->tris, &h->tri_items, &h->face_grad, &h->m_verts, &h->m_faces, &h->m_out, &h->m_tris,
+                      &h->tris, &h->tri_items, &h->face_grad, &h->tilemap, &h->m_verts, &h->m_faces, &h->m_out, &h->m_tris,
                       &h->m_bin_count, &h->m_bin_start, &h->m_bin_fill, &h->m_bin_scratch, &h->m_bin_tris,
                       &h->m_bin_active, &h->m_active_list, &h->m_axis_start, &h->m_far, &h->m_ext, &h->m_tmp,
                       &h->m_partials, &h->m_counters, &h->m_vox, &h->table, &h->cell_slot, &h->adj_rows, &h->adj_owners, &h->ours_ws,

@@ -12,8 +12,9 @@
 //                     edge with a strict sign change; cell (i,j,k) owns its min-corner edges
 //
 // Work split. A tile is 32 x 4 x 4 cells: one 32-cell active-bit word in each of 16 cell rows.
-// A CTA takes a chunk of up to 32 x-adjacent tiles, finds the tiles with an active cell from
-// the bit words (lane per word), and for each such tile:
+// A CTA takes 32 consecutive chunks of up to 32 x-adjacent tiles each; the mark kernel
+// recorded which tiles of each chunk hold an active cell. For each such chunk the CTA forms the
+// ranks of its rows (below), and for each of its active tiles:
 //   1. stages the 35 x 7 x 7 grid points around it (every 4x4x4 stencil of its cells) in
 //      shared memory, with the tile's and the surrounding rows' active words and the global
 //      rank of each word's first active cell (the mark segment's first rank + popcounts of
@@ -39,7 +40,8 @@ namespace dcb {
 namespace cg = cooperative_groups;
 
 constexpr int kBandThreads = 128;
-constexpr int kTY = 4, kTZ = 4;                 // cell rows and planes per tile
+constexpr int kTY = kBandTileRows, kTZ = kBandTilePlanes;   // cell rows and planes per tile
+constexpr int kChunkGroup = 32;                 // chunks a CTA takes at a time
 constexpr int kSX = 36;                         // staged points per row: x0-1 .. x0+34
 constexpr int kSY = kTY + 3, kSZ = kTZ + 3;     // rows y0-1 .. y0+5, planes z0-1 .. z0+5
 constexpr int kXRows = (kTY + 1) * (kTZ + 1);   // X edges (py, pz): py in [y0, y0+4], pz in [z0, z0+4]
@@ -52,8 +54,13 @@ constexpr int kRows = kERows + kCRows;              // counted rows (edges, then
 constexpr int kMaxEdges = 32 * kXRows + 33 * (kYRows + kZRows);   // 2,120
 constexpr int kTileCells = 32 * kTY * kTZ;
 
+// The staged grid values of one tile, 0 outside the grid.
+struct Vals {
+    float v[kSZ][kSY][kSX];
+};
+
 struct BandSmem {
-    float v[kSZ][kSY][kSX];            // grid values, 0 outside the grid
+    Vals vb[2];                        // this tile's values and the next tile's (in flight)
     float rw[3][kSX];                  // 1 / cell width along x, y, z at index (lo - 1 + q)
     float4 e[kMaxEdges];               // per listed edge: averaged normal, flags in w
     float t[12][kBandThreads];         // per cell thread: lerp parameter of each crossing edge
@@ -65,7 +72,7 @@ struct BandSmem {
     uint32_t rank0[kTZ + 1][kTY + 1];  // global rank of that word's first active cell
     uint32_t cw[kTZ + 1][kTY + 1][32]; // the chunk's words of those rows, [..][x-word in chunk]
     uint32_t cr[kTZ + 1][kTY + 1][32]; // global rank of each such word's first active cell
-    uint32_t tiles;                    // active tiles of the chunk
+    uint32_t gtiles[32];               // active tiles of each chunk of the group
     unsigned int chunk;
     unsigned int hist;
 };
@@ -74,12 +81,42 @@ struct BandSmem {
 constexpr uint32_t kEdgeOwn = 1;   // not averaged: each cell uses its own trilinear normal
 constexpr uint32_t kEdgeIll = 2;   // FP32 cannot be trusted with this normal
 
-__device__ __forceinline__ float sval(const BandSmem& s, int xl, int yl, int zl) {
-    return s.v[zl + 1][yl + 1][xl + 1];   // local coordinates relative to (x0, y0, z0)
+__device__ __forceinline__ float sval(const Vals& V, int xl, int yl, int zl) {
+    return V.v[zl + 1][yl + 1][xl + 1];   // local coordinates relative to (x0, y0, z0)
+}
+
+// One 4-byte asynchronous global -> shared copy (cp.async); an invalid point reads nothing
+// (source size 0) and is zero-filled.
+__device__ __forceinline__ void copy4_async(float* dst, const float* src, const float* any_valid, bool valid) {
+    const unsigned int saddr = (unsigned int)__cvta_generic_to_shared(dst);
+    const int n = valid ? 4 : 0;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(saddr), "l"(valid ? src : any_valid), "r"(n)
+                 : "memory");
+}
+__device__ __forceinline__ void copy_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void copy_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// Start the copies of tile (x0, y0, z0)'s 35 x 7 x 7 points into V: a warp per point row, lane l
+// copying point x0-1+l and lanes 0-3 also x0+31+l. Completes at copy_wait_all + a barrier.
+__device__ __forceinline__ void stage_tile_async(Vals& V, const GridDesc& g, int x0, int y0, int z0, int warp,
+                                                 int lane) {
+    for (int r = warp; r < kSY * kSZ; r += kBandThreads / 32) {
+        const int yl = r % kSY - 1, zl = r / kSY - 1;
+        const int y = y0 + yl, z = z0 + zl;
+        const bool row_in = y >= 0 && y < g.ny && z >= 0 && z < g.nz;
+        const float* row = g.v + (row_in ? ((long long)y + (long long)g.ny * z) * g.nx : 0);
+        const int xa = x0 - 1 + lane;
+        copy4_async(&V.v[zl + 1][yl + 1][lane], row + xa, g.v, row_in && xa >= 0 && xa < g.nx);
+        if (lane < kSX - 32) {
+            const int xb = x0 + 31 + lane;
+            copy4_async(&V.v[zl + 1][yl + 1][32 + lane], row + xb, g.v, row_in && xb < g.nx);
+        }
+    }
+    copy_commit();
 }
 
 // Active test of the cell whose min corner is at local (xl, yl, zl) from the staged points.
-__device__ __forceinline__ bool active_local(const BandSmem& s, int xl, int yl, int zl) {
+__device__ __forceinline__ bool active_local(const Vals& s, int xl, int yl, int zl) {
     bool neg = false, pos = false;
 #pragma unroll
     for (int c = 0; c < 8; ++c) {
@@ -92,7 +129,7 @@ __device__ __forceinline__ bool active_local(const BandSmem& s, int xl, int yl, 
 
 // gradientAt (contouring.cpp:141-207) in FP32 at grid point (x, y, z), neighbours clamped to
 // the grid, from the staged points (orientation tests only, as grid_gradient32).
-__device__ __forceinline__ float3 gradient_at(const BandSmem& s, const GridDesc& g, int x0, int y0, int z0,
+__device__ __forceinline__ float3 gradient_at(const Vals& s, const GridDesc& g, int x0, int y0, int z0,
                                               int x, int y, int z) {
     const int xm = max(x - 1, 0), xp = min(x + 1, g.nx - 1);
     const int ym = max(y - 1, 0), yp = min(y + 1, g.ny - 1);
@@ -119,8 +156,8 @@ __device__ __forceinline__ void edge_row(int q, int& axis, int& yl, int& zl) {
 
 // Averaged normal of the crossing edge with low endpoint at local (xl, yl, zl) along axis, or
 // the kEdgeOwn flag (edge_normal of dcb_vertex.cu, with the stencil in shared memory).
-__device__ float4 edge_record(const BandSmem& s, const GridDesc& g, int x0, int y0, int z0, int axis, int xl,
-                              int yl, int zl) {
+__device__ float4 edge_record(const BandSmem& sm, const Vals& s, const GridDesc& g, int x0, int y0, int z0, int axis,
+                              int xl, int yl, int zl) {
     const int lx = x0 + xl, ly = y0 + yl, lz = z0 + zl;
     const int hx = lx + (axis == 0), hy = ly + (axis == 1), hz = lz + (axis == 2);
     const bool in0 = lx > 0 && lx < g.nx - 1 && ly > 0 && ly < g.ny - 1 && lz > 0 && lz < g.nz - 1;
@@ -145,7 +182,7 @@ __device__ float4 edge_record(const BandSmem& s, const GridDesc& g, int x0, int 
     const float t_lo = lerp_t(s_lo, s_hi);
     const float u_hi = fabsf(s_lo - s_hi) < 1e-6f ? 1.f - lerp_t(s_hi, s_lo) : t_lo;
     const int hxl = xl + (axis == 0), hyl = yl + (axis == 1), hzl = zl + (axis == 2);
-    const float ga = (s_hi - s_lo) * s.rw[axis][(axis == 0 ? xl : axis == 1 ? yl : zl) + 1];
+    const float ga = (s_hi - s_lo) * sm.rw[axis][(axis == 0 ? xl : axis == 1 ? yl : zl) + 1];
     // perpendicular differences at both edge ends: forward (p) and backward (m)
     const float a0p = sval(s, xl + e1x, yl + e1y, zl) - s_lo, a0m = s_lo - sval(s, xl - e1x, yl - e1y, zl);
     const float a1p = sval(s, hxl + e1x, hyl + e1y, hzl) - s_hi, a1m = s_hi - sval(s, hxl - e1x, hyl - e1y, hzl);
@@ -153,8 +190,8 @@ __device__ float4 edge_record(const BandSmem& s, const GridDesc& g, int x0, int 
     const float b1p = sval(s, hxl, hyl + e2y, hzl + e2z) - s_hi, b1m = s_hi - sval(s, hxl, hyl - e2y, hzl - e2z);
     // widths of the cells on either side of the edge along d1 and d2
     const int c1 = d1 == 0 ? xl : yl, c2 = d2 == 1 ? yl : zl;
-    const float rw1p = s.rw[d1][c1 + 1], rw1m = s.rw[d1][c1];
-    const float rw2p = s.rw[d2][c2 + 1], rw2m = s.rw[d2][c2];
+    const float rw1p = sm.rw[d1][c1 + 1], rw1m = sm.rw[d1][c1];
+    const float rw2p = sm.rw[d2][c2 + 1], rw2m = sm.rw[d2][c2];
     const float m1v = fmaxf(fmaxf(fabsf(a0p), fabsf(a1p)) * rw1p, fmaxf(fabsf(a0m), fabsf(a1m)) * rw1m);
     const float m2v = fmaxf(fmaxf(fabsf(b0p), fabsf(b1p)) * rw2p, fmaxf(fabsf(b0m), fabsf(b1m)) * rw2m);
     const float bound2 = kNormalCond2 * (ga * ga + m1v * m1v + m2v * m2v);
@@ -220,11 +257,18 @@ k_band(const __grid_constant__ BandParams P) {
     if (tid == 0) s.hist = 0;
 
     for (;;) {
+        // a group of 32 consecutive chunks; the mark kernel recorded each one's active tiles
         __syncthreads();
-        if (tid == 0) s.chunk = atomicAdd(P.chunk_next, 1u);
+        if (tid == 0) s.chunk = atomicAdd(P.chunk_next, (unsigned int)kChunkGroup);
         __syncthreads();
-        const long long cg_ = s.chunk;
-        if (cg_ >= P.nchunks) break;
+        const long long c0 = s.chunk;
+        if (c0 >= P.nchunks) break;
+        if (warp == 0) s.gtiles[lane] = c0 + lane < P.nchunks ? __ldg(P.tilemap + c0 + lane) : 0u;
+        __syncthreads();
+      for (int q = 0; q < kChunkGroup; ++q) {
+        uint32_t tiles = s.gtiles[q];
+        if (!tiles) continue;                               // uniform: shared memory
+        const long long cg_ = c0 + q;
         // the chunk's grid (batches: the grids' chunks are concatenated)
         const int gi = ONE ? 0 : slot_search(P.B.chunk_off, P.B.n, cg_);
         const GridSlot& S = slot_ref<ONE>(P.B, gi);
@@ -239,46 +283,43 @@ k_band(const __grid_constant__ BandParams P) {
         const int jb = (int)((c / nxc) % nyb);
         const int kb = (int)(c / ((long long)nxc * nyb));
         const int y0 = jb * kTY, z0 = kb * kTZ;
-        // 1) active tiles of the chunk: lane = word, warps split the 16 cell rows
-        {
-            const int w = xc * 32 + lane;
-            uint32_t any = 0;
-            if (w < nwx) {
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const int rr = warp * 4 + q;
-                    const int y = y0 + (rr & 3), z = z0 + (rr >> 2);
-                    if (y < g.cy && z < g.cz) any |= __ldg(bits + ((long long)y + (long long)g.cy * z) * g.W + w);
-                }
-            }
-            const uint32_t m = __ballot_sync(0xffffffffu, any != 0);
-            if (tid == 0) s.tiles = 0;
-            __syncthreads();
-            if (lane == 0 && m) atomicOr(&s.tiles, m);
-            __syncthreads();
-        }
-        uint32_t tiles = s.tiles;
+        __syncthreads();   // the previous chunk's shared data is no longer read
         if (tiles) {
             // words and first ranks of the chunk's rows and the rows below / behind them: lane =
             // word; a segment's earlier words are summed by a scan of width tw (the mark's
             // segment, 32 or 8 words, aligned with the chunk)
             const int w = xc * 32 + lane;
             const int tw = S.tw;
-            for (int q = warp; q < (kTY + 1) * (kTZ + 1); q += kBandThreads / 32) {
+            constexpr int kRankRows = (kTY + 1) * (kTZ + 1);
+            constexpr int kPer = (kRankRows + kBandThreads / 32 - 1) / (kBandThreads / 32);
+            // every row's word and segment start first (all loads in flight), then the scans
+            uint32_t wv[kPer], sv[kPer];
+#pragma unroll
+            for (int it = 0; it < kPer; ++it) {
+                const int q = warp + it * (kBandThreads / 32);
+                const int a = q % (kTY + 1), cc = q / (kTY + 1);
+                const int y = y0 - 1 + a, z = z0 - 1 + cc;
+                const bool row_ok = q < kRankRows && y >= 0 && y < g.cy && z >= 0 && z < g.cz;
+                const long long row = (long long)y + (long long)g.cy * z;
+                wv[it] = (row_ok && w < nwx) ? __ldg(bits + row * g.W + w) : 0u;
+                sv[it] = (row_ok && w < nwx && (lane & (tw - 1)) == 0) ? __ldg(P.seg_start + S.seg_off + row * S.nxt + w / tw) : 0u;
+            }
+#pragma unroll
+            for (int it = 0; it < kPer; ++it) {
+                const int q = warp + it * (kBandThreads / 32);
+                if (q >= kRankRows) break;                       // warp-uniform
                 const int a = q % (kTY + 1), cc = q / (kTY + 1);
                 const int y = y0 - 1 + a, z = z0 - 1 + cc;
                 const bool row_ok = y >= 0 && y < g.cy && z >= 0 && z < g.cz;
                 const long long row = (long long)y + (long long)g.cy * z;
-                const uint32_t word = (row_ok && w < nwx) ? __ldg(bits + row * g.W + w) : 0u;
+                const uint32_t word = wv[it];
                 const uint32_t cnt = __popc(word);
                 uint32_t incl = cnt;
                 for (int o = 1; o < tw; o <<= 1) {
                     const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o, tw);
                     if ((lane & (tw - 1)) >= o) incl += t;
                 }
-                uint32_t start = 0;
-                if (row_ok && w < nwx && (lane & (tw - 1)) == 0) start = __ldg(P.seg_start + S.seg_off + row * S.nxt + w / tw);
-                start = __shfl_sync(0xffffffffu, start, lane & ~(tw - 1), 32);
+                const uint32_t start = __shfl_sync(0xffffffffu, sv[it], lane & ~(tw - 1), 32);
                 const uint32_t r0 = start + incl - cnt;
                 s.cw[cc][a][lane] = word;
                 s.cr[cc][a][lane] = r0;
@@ -287,25 +328,16 @@ k_band(const __grid_constant__ BandParams P) {
             }
             __syncthreads();
         }
+        // the first tile's points; each later tile's are copied while the one before it is solved
+        int cur = 0;
+        if (tiles) stage_tile_async(s.vb[0], g, 32 * (xc * 32 + __ffs(tiles) - 1), y0, z0, warp, lane);
         while (tiles) {
             const int tb = __ffs(tiles) - 1;
             tiles &= tiles - 1;
             const int w = xc * 32 + tb;
             const int x0 = 32 * w;
             __syncthreads();   // the previous tile's shared data is no longer read
-            // 2) stage the points, the reciprocal widths, the words and their first ranks
-            for (int r = warp; r < kSY * kSZ; r += kBandThreads / 32) {
-                const int yl = r % kSY - 1, zl = r / kSY - 1;
-                const int y = y0 + yl, z = z0 + zl;
-                const bool row_in = y >= 0 && y < g.ny && z >= 0 && z < g.nz;
-                const float* row = g.v + ((long long)y + (long long)g.ny * z) * g.nx;
-                const int xa = x0 - 1 + lane;
-                s.v[zl + 1][yl + 1][lane] = (row_in && xa >= 0 && xa < g.nx) ? __ldg(row + xa) : 0.f;
-                if (lane < kSX - 32) {
-                    const int xb = x0 + 31 + lane;
-                    s.v[zl + 1][yl + 1][32 + lane] = (row_in && xb < g.nx) ? __ldg(row + xb) : 0.f;
-                }
-            }
+            // 2) the reciprocal widths, the words and their first ranks; the points arrive
             if (tid < kSX) {
                 const int x = x0 - 1 + tid;
                 s.rw[0][tid] = 1.f / (pos_axis(g.ox, g.vx, x + 1) - pos_axis(g.ox, g.vx, x));
@@ -320,7 +352,11 @@ k_band(const __grid_constant__ BandParams P) {
                 s.word[cc][a] = s.cw[cc][a][tb];
                 s.rank0[cc][a] = s.cr[cc][a][tb];
             }
+            copy_wait_all();
             __syncthreads();
+            const Vals& V = s.vb[cur];
+            if (tiles) stage_tile_async(s.vb[cur ^ 1], g, 32 * (xc * 32 + __ffs(tiles) - 1), y0, z0, warp, lane);
+            cur ^= 1;
             // 3) edge rows: crossing edges (Hermite test) of the tile's active cells; then the
             //    16 cell rows' active counts
             for (int q = warp; q < kERows; q += kBandThreads / 32) {
@@ -336,12 +372,12 @@ k_band(const __grid_constant__ BandParams P) {
                     const unsigned long long A = axis == 1 ? (act(yl, zl - 1) | act(yl, zl)) : (act(yl - 1, zl) | act(yl, zl));
                     cells = A | (A << 1);
                 }
-                const float a0 = sval(s, lane, yl, zl);
-                const float a1 = sval(s, lane + (axis == 0), yl + (axis == 1), zl + (axis == 2));
+                const float a0 = sval(V, lane, yl, zl);
+                const float a1 = sval(V, lane + (axis == 0), yl + (axis == 1), zl + (axis == 2));
                 unsigned long long m = __ballot_sync(0xffffffffu, hermite_crossing(a0, a1));
                 if (axis != 0) {
-                    const float b0 = sval(s, 32, yl, zl);
-                    const float b1 = sval(s, 32, yl + (axis == 1), zl + (axis == 2));
+                    const float b0 = sval(V, 32, yl, zl);
+                    const float b1 = sval(V, 32, yl + (axis == 1), zl + (axis == 2));
                     if (hermite_crossing(b0, b1)) m |= 1ull << 32;
                 }
                 m &= cells;
@@ -390,7 +426,7 @@ k_band(const __grid_constant__ BandParams P) {
                 const uint32_t it = s.list[e];
                 int axis, yl, zl;
                 edge_row((int)(it >> 6), axis, yl, zl);
-                s.e[e] = edge_record(s, g, x0, y0, z0, axis, (int)(it & 63), yl, zl);
+                s.e[e] = edge_record(s, V, g, x0, y0, z0, axis, (int)(it & 63), yl, zl);
             }
             __syncthreads();
             // 5) cells, a thread per active cell
@@ -405,7 +441,7 @@ k_band(const __grid_constant__ BandParams P) {
                 if (!ONE && P.cell_slot) P.cell_slot[r] = (uint32_t)gi;
                 float c[8];
 #pragma unroll
-                for (int q = 0; q < 8; ++q) c[q] = sval(s, b + corner_dx(q), jj + corner_dy(q), kk + corner_dz(q));
+                for (int q = 0; q < 8; ++q) c[q] = sval(V, b + corner_dx(q), jj + corner_dy(q), kk + corner_dz(q));
                 // Pass 1: crossing edges and the centroid in local units.
                 uint32_t hmask = 0;
                 float cu = 0.f, cv = 0.f, cw = 0.f;
@@ -494,7 +530,7 @@ k_band(const __grid_constant__ BandParams P) {
                 const unsigned int nfc = (unsigned int)fx + (unsigned int)fyy + (unsigned int)fzz;
                 unsigned int f = reserve_slots(P.face_count, nfc);
                 if (nfc) {
-                    const float3 g0 = gradient_at(s, g, x0, y0, z0, i, j, k);
+                    const float3 g0 = gradient_at(V, g, x0, y0, z0, i, j, k);
 #pragma unroll
                     for (int axis = 0; axis < 3; ++axis) {
                         const bool has = axis == 0 ? fx : (axis == 1 ? fyy : fzz);
@@ -505,7 +541,7 @@ k_band(const __grid_constant__ BandParams P) {
                         if (axis == 0) { r0 = rank_in(s, jj, kk, b); r1 = rank_in(s, jj + 1, kk, b); r3 = rank_in(s, jj, kk + 1, b); }
                         else if (axis == 1) { r1 = rank_in(s, jj + 1, kk, b); r0 = r1 - 1u; r3 = r - 1u; }
                         else { r1 = rank_in(s, jj, kk + 1, b); r0 = r1 - 1u; r3 = r - 1u; }
-                        const float3 g1 = gradient_at(s, g, x0, y0, z0, i + (axis == 0), j + (axis == 1), k + (axis == 2));
+                        const float3 g1 = gradient_at(V, g, x0, y0, z0, i + (axis == 0), j + (axis == 1), k + (axis == 2));
                         const long long col = S.col_off + axis * cxcy + (long long)i * g.cy + j;
                         atomicAdd(&P.col_count[col], 1u);
                         if (f < P.face_cap) {
@@ -519,6 +555,7 @@ k_band(const __grid_constant__ BandParams P) {
                 }
             }
         }
+      }
     }
     __syncthreads();
     if (tid == 0 && s.hist) atomicAdd(P.rank_hist + 1, (unsigned long long)s.hist);

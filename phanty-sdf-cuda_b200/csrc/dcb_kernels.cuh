@@ -22,6 +22,7 @@ struct GridSlot {
     int nzc;                       // mark: z-chunks
     int tw;                        // mark: cell words per x-tile (32, or 8 for narrow grids)
     float hmax;                    // largest cell width of the grid (world units)
+    long long chunk_off;           // first tile-band chunk (32 words x 4 rows x 4 planes)
 };
 
 struct BatchTable {
@@ -75,6 +76,8 @@ struct MarkParams {
     long long ntiles;
     uint32_t* bits;                // all grids' active bits
     uint32_t* seg_count;           // all grids' segment counts
+    uint32_t* tilemap;             // optional, zeroed before: per band chunk, bit w set when the
+                                   // chunk's 32 x 4 x 4-cell tile of word w has an active cell
 };
 cudaError_t launch_mark(const MarkParams& P, int tw, cudaStream_t s);
 int mark_tile_words();
@@ -213,7 +216,9 @@ struct TriParams {
 };
 cudaError_t launch_triangulate(const TriParams& P, long long max_quads, int num_sms, cudaStream_t s);
 
-// ---- tile band kernel (dcb_band.cu), single grids ----
+// ---- tile band kernel (dcb_band.cu) ----
+// Tile: one 32-cell active-bit word in each of kBandTileRows x kBandTilePlanes cell rows.
+constexpr int kBandTileRows = 4, kBandTilePlanes = 4;
 // Work unit: a chunk of up to 32 x-adjacent tiles of 32 x 4 x 4 cells (one active-bit word
 // per cell row), handed out by an atomic counter.
 struct BandParams {
@@ -223,6 +228,7 @@ struct BandParams {
     uint32_t* super;               // written: rank of the first active cell of every 256-cell word
     uint64_t* list;                // written: packed cell of every rank
     uint32_t* cell_slot;           // written (batches, may be null): grid of every rank
+    const uint32_t* tilemap;       // active tiles of every chunk (mark)
     long long nchunks;             // all grids' chunks
     unsigned int* chunk_next;      // chunk counter, zero before the launch
     float* V;

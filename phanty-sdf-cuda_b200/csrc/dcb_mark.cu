@@ -132,6 +132,19 @@ k_mark_zmarch(const __grid_constant__ MarkParams P) {
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
             if (lane == 0) seg_count[row * nxt + xt] = cnt;
+            if (P.tilemap) {
+                // the band kernel's tiles: 32-cell words x 4 rows x 4 planes, in chunks of 32
+                // words; one OR per row and plane that has an active cell
+                const uint32_t any = __ballot_sync(0xffffffffu, act != 0u) & (word_lane ? 0xffffffffu : 0u);
+                const int j = j0 + r;
+                if (lane == 0 && any) {
+                    const int w0 = xt * TW;                       // first word of this x-tile
+                    const int nwx = (g.cx + 31) >> 5;
+                    const long long nxc = (nwx + 31) / 32, nyb = (g.cy + kBandTileRows - 1) / kBandTileRows;
+                    const long long chunk = S.chunk_off + (w0 >> 5) + nxc * (j / kBandTileRows + nyb * (k / kBandTilePlanes));
+                    atomicOr(P.tilemap + chunk, any << (w0 & 31));
+                }
+            }
         }
         __syncthreads();
     }
