@@ -1,16 +1,16 @@
 // dcb_api.cu — handle, workspace and the C ABI declared in include/dcb.h.
 //
-// Pipeline of one extraction (all on the caller's stream):
-//   k_mark_zmarch    grid -> active bits, per-segment counts           (dcb_mark.cu)
+// Pipeline of one extraction, or of a batch of grids as one (all on the caller's stream):
+//   k_mark_zmarch    grid -> active bits, per-segment counts, active band tiles (dcb_mark.cu)
 //   scan             segment counts -> segment first ranks, total     (dcb_faces.cu)
 //   [host reads the active count: sizes the vertex buffers]
-//   k_expand_ranks   super-word ranks + packed active-cell list        (dcb_mark.cu)
-//   k_cell_qef       Hermite + averaging + QEF (rank-1 certified), face masks, column
-//                    counts; other cells listed                        (dcb_vertex.cu)
+//   k_band           per 32x4x4-cell tile, stencils in shared memory: ranks, super-word
+//                    ranks, the active-cell list, Hermite + averaging + QEF (rank-1
+//                    certified), column counts, staged faces; other cells listed (dcb_band.cu)
 //   k_cell_jacobi    listed cells solved with FP32 Jacobi              (dcb_vertex.cu)
 //   k_vertex_fp64    cells FP32 does not trust, re-solved in FP64      (dcb_vertex64.cu)
 //   scan             column counts -> column starts, face total       (dcb_faces.cu)
-//   k_face_scatter   quads into their columns, FP32 winding           (dcb_faces.cu)
+//   k_face_place     staged faces into their columns, FP32 winding    (dcb_faces.cu)
 //   k_vertex_fp64    FP64 vertices of the cells of uncertain windings  (dcb_vertex64.cu)
 //   k_winding_fp64   uncertain windings re-decided in FP64            (dcb_vertex64.cu)
 //   k_face_order     rank by k inside each column -> final face list  (dcb_faces.cu)
@@ -59,7 +59,7 @@ struct dcb_context {
     std::string last_error;
     cudaEvent_t ev[10] = {};
     bool substage_events = false;     // ev[8] / ev[9] hold the face sub-stages of the last call
-    DevBuf grid, bits, super, list, seg_count, seg_start, counters, V, vclass, fmask, col_count, col_fill,
+    DevBuf grid, bits, super, list, seg_count, seg_start, counters, V, vclass, col_count, col_fill,
         col_start, partials, esc_list, hard_list, hard_data, stage_quad, stage_key, faces, wind_items,
         v64_index, v64_cells, V64, tris, tri_items, adj_rows, adj_owners, ours_ws, face_grad, tilemap;
     // sparse backends
@@ -393,7 +393,6 @@ int batch_prepare(dcb_context* h, const dcb_grid* in, int n, cudaStream_t s, Bat
 int batch_alloc(dcb_context* h, int n, long long cap, const dcb_opts* o, TableView& T) {
     DCB_TRY(h, ensure(h->list, sizeof(uint64_t) * cap), "alloc active list");
     DCB_TRY(h, ensure(h->V, sizeof(float) * 3 * cap), "alloc vertices");
-    DCB_TRY(h, ensure(h->fmask, cap), "alloc face masks");
     DCB_TRY(h, ensure(h->vclass, cap), "alloc vertex classes");
     DCB_TRY(h, ensure(h->esc_list, sizeof(uint32_t) * cap), "alloc escalation list");
     DCB_TRY(h, ensure(h->hard_list, sizeof(uint32_t) * cap), "alloc hard list");
@@ -469,99 +468,75 @@ int batch_rest(dcb_context* h, const BatchLayout& L, TableView& T, const dcb_opt
     DCB_TRY(h, cudaMemsetAsync(h->col_fill.p, 0, sizeof(uint32_t) * ncol, s), "memset");
     DCB_TRY(h, cudaMemsetAsync(h->v64_index.p, 0xff, sizeof(int) * cap, s), "memset");
 
-    // 2) ranks + list, QEF with fused edge normals (rank-1 fast path, Jacobi list, FP64).
-    ExpandParams xp;
-    xp.B = T.B; xp.nseg = nseg; xp.bits = as<uint32_t>(h->bits); xp.seg_count = as<uint32_t>(h->seg_count);
-    xp.seg_start = as<uint32_t>(h->seg_start); xp.super = as<uint32_t>(h->super); xp.list = as<uint64_t>(h->list);
-    xp.cell_slot = n > 1 ? as<uint32_t>(h->cell_slot) : nullptr;
-    xp.B.cell_slot = nullptr;                      // expand finds grids by segment
-    xp.list_cap = cap;
-    // The tile band kernel: ranks, the active-cell list, vertices and staged faces from
-    // shared-memory stencils, over the tiles of every grid of the batch.
-    const bool band = true;
+    // 2) the tile band kernel over the tiles of every grid of the batch: ranks, the active-cell
+    //    list, vertices (rank-1 certified in FP32; Jacobi list; FP64 list) and staged faces
+    //    from shared-memory stencils; then the Jacobi and FP64 vertices.
+    uint32_t* const bits = as<uint32_t>(h->bits);
+    uint64_t* const list = as<uint64_t>(h->list);
     QefParams qp;
-    qp.B = T.B; qp.list = xp.list; qp.nactive = cap; qp.live = live; qp.V = as<float>(h->V); qp.vclass = as<uint8_t>(h->vclass);
-    qp.fmask = as<uint8_t>(h->fmask); qp.col_count = as<uint32_t>(h->col_count);
+    qp.B = T.B; qp.list = list; qp.nactive = cap; qp.live = live; qp.V = as<float>(h->V); qp.vclass = as<uint8_t>(h->vclass);
     qp.esc_list = as<uint32_t>(h->esc_list); qp.esc_count = &dc->esc_count;
     qp.hard_list = as<uint32_t>(h->hard_list); qp.hard_data = as<float4>(h->hard_data); qp.hard_count = &dc->hard_count;
     qp.rank_hist = dc->rank_hist;
     qp.err = &dc->err;
     qp.thr = (float)o->svd_threshold; qp.band = (float)o->fp64_threshold_band;
     qp.cond_max = (float)std::min(o->fp64_escalation_cond, 3.0e38); qp.force64 = o->force_fp64;
-    if (band) {
-        BandParams bp;
-        bp.B = T.B;
-        bp.bits = xp.bits; bp.seg_start = xp.seg_start; bp.super = xp.super; bp.list = xp.list;
-        bp.cell_slot = xp.cell_slot;
-        bp.tilemap = as<uint32_t>(h->tilemap);
-        bp.nchunks = L.nchunk;
-        bp.chunk_next = &dc->band_chunk;
-        bp.V = qp.V; bp.vclass = qp.vclass; bp.col_count = qp.col_count;
-        bp.esc_list = qp.esc_list; bp.esc_count = qp.esc_count;
-        bp.hard_list = qp.hard_list; bp.hard_data = qp.hard_data; bp.hard_count = qp.hard_count;
-        bp.rank_hist = qp.rank_hist;
-        bp.face_cells = as<int4>(h->faces); bp.face_grad = as<float4>(h->face_grad);
-        bp.face_count = &dc->face_staged; bp.face_cap = (unsigned long long)(3 * cap); bp.nv = cap; bp.live = live;
-        bp.err = &dc->err;
-        bp.thr = qp.thr; bp.band = qp.band; bp.force64 = qp.force64;
-        DCB_TRY(h, launch_band(bp, h->num_sms, s), "launch band");
-    } else {
-        DCB_TRY(h, launch_cell_qef(qp, h->num_sms, s), "launch qef");
-    }
+    BandParams bp;
+    bp.B = T.B;
+    bp.bits = bits; bp.seg_start = as<uint32_t>(h->seg_start); bp.super = as<uint32_t>(h->super); bp.list = list;
+    bp.cell_slot = n > 1 ? as<uint32_t>(h->cell_slot) : nullptr;
+    bp.tilemap = as<uint32_t>(h->tilemap);
+    bp.nchunks = L.nchunk;
+    bp.chunk_next = &dc->band_chunk;
+    bp.V = qp.V; bp.vclass = qp.vclass; bp.col_count = as<uint32_t>(h->col_count);
+    bp.esc_list = qp.esc_list; bp.esc_count = qp.esc_count;
+    bp.hard_list = qp.hard_list; bp.hard_data = qp.hard_data; bp.hard_count = qp.hard_count;
+    bp.rank_hist = qp.rank_hist;
+    bp.face_cells = as<int4>(h->faces); bp.face_grad = as<float4>(h->face_grad);
+    bp.face_count = &dc->face_staged; bp.face_cap = (unsigned long long)(3 * cap); bp.nv = cap; bp.live = live;
+    bp.err = &dc->err;
+    bp.thr = qp.thr; bp.band = qp.band; bp.force64 = qp.force64;
+    DCB_TRY(h, launch_band(bp, h->num_sms, s), "launch band");
     DCB_TRY(h, launch_cell_jacobi(qp, cap, h->num_sms, s), "launch jacobi");
     Vertex64Params v64;
-    v64.B = T.B; v64.list = xp.list; v64.cells = qp.esc_list; v64.count = &dc->esc_count; v64.cap = (unsigned int)cap;
+    v64.B = T.B; v64.list = list; v64.cells = qp.esc_list; v64.count = &dc->esc_count; v64.cap = (unsigned int)cap;
     v64.Vf = qp.V; v64.vclass = qp.vclass; v64.V64 = nullptr; v64.thr = o->svd_threshold;
     DCB_TRY(h, launch_vertex_fp64(v64, cap, h->num_sms, s), "launch vertex fp64");
     if (events) DCB_TRY(h, cudaEventRecord(h->ev[3], s), "event");
-    // the faces were counted per column by the vertex kernels
+    // the faces were counted per column by the band kernel
     if (events) DCB_TRY(h, cudaEventRecord(h->ev[8], s), "event");
 
-    // 3) faces: column scan, scatter with FP32 winding, FP64 re-decisions, in-column order.
-    DCB_TRY(h, launch_scan(as<uint32_t>(h->col_count), ncol, as<uint32_t>(h->partials),
-                           as<uint32_t>(h->col_start), &dc->face_total, s), "launch scan");
+    // 3) faces: column scan, placement with the FP32 winding, FP64 re-decisions, in-column order.
+    uint32_t* const col_start = as<uint32_t>(h->col_start);
+    DCB_TRY(h, launch_scan(as<uint32_t>(h->col_count), ncol, as<uint32_t>(h->partials), col_start,
+                           &dc->face_total, s), "launch scan");
     if (events) {
         DCB_TRY(h, cudaEventRecord(h->ev[9], s), "event");
         h->substage_events = true;
     }
     if (n > 1)
-        DCB_TRY(h, launch_face_offsets(T.B, as<uint32_t>(h->col_start), &dc->face_total, T.face_off, s), "face offsets");
-    FaceParams fp;
-    fp.B = T.B; fp.list = xp.list; fp.nactive = cap; fp.live = live; fp.fmask = qp.fmask; fp.V = qp.V; fp.vclass = qp.vclass;
-    fp.bits = xp.bits; fp.super = xp.super;
-    fp.col_start = as<uint32_t>(h->col_start); fp.col_count = as<uint32_t>(h->col_count);
-    fp.col_fill = as<uint32_t>(h->col_fill);
-    fp.stage_quad = as<int4>(h->stage_quad); fp.stage_key = as<uint2>(h->stage_key);
-    fp.wind_items = as<uint4>(h->wind_items); fp.wind_count = &dc->wind_count;
-    fp.wind_cap = (unsigned long long)wind_cap;
-    fp.v64_index = as<int>(h->v64_index); fp.v64_cells = as<uint32_t>(h->v64_cells);
-    fp.v64_count = &dc->v64_count; fp.v64_cap = (unsigned long long)v64_cap;
-    fp.err = &dc->err;
-    fp.hmax = L.hmax;
-    if (band) {
-        FacePlaceParams pp;
-        pp.B = T.B; pp.list = xp.list;
-        pp.face_cells = as<int4>(h->faces); pp.face_grad = as<float4>(h->face_grad);
-        pp.face_count = &dc->face_staged; pp.face_cap = (unsigned long long)(3 * cap); pp.nv = cap;
-        pp.V = qp.V; pp.vclass = qp.vclass;
-        pp.col_start = fp.col_start; pp.col_fill = fp.col_fill;
-        pp.stage_quad = fp.stage_quad; pp.stage_key = fp.stage_key;
-        pp.wind_items = fp.wind_items; pp.wind_count = fp.wind_count; pp.wind_cap = fp.wind_cap;
-        pp.v64_index = fp.v64_index; pp.v64_cells = fp.v64_cells; pp.v64_count = fp.v64_count;
-        pp.v64_cap = fp.v64_cap; pp.err = fp.err;
-        DCB_TRY(h, launch_face_place(pp, 3 * cap, h->num_sms, s), "launch face placement");
-    } else {
-        DCB_TRY(h, launch_face_scatter(fp, h->num_sms, s), "launch face scatter");
-    }
+        DCB_TRY(h, launch_face_offsets(T.B, col_start, &dc->face_total, T.face_off, s), "face offsets");
+    FacePlaceParams pp;
+    pp.B = T.B; pp.list = list;
+    pp.face_cells = as<int4>(h->faces); pp.face_grad = as<float4>(h->face_grad);
+    pp.face_count = &dc->face_staged; pp.face_cap = (unsigned long long)(3 * cap); pp.nv = cap;
+    pp.V = qp.V; pp.vclass = qp.vclass;
+    pp.col_start = col_start; pp.col_fill = as<uint32_t>(h->col_fill);
+    pp.stage_quad = as<int4>(h->stage_quad); pp.stage_key = as<uint2>(h->stage_key);
+    pp.wind_items = as<uint4>(h->wind_items); pp.wind_count = &dc->wind_count; pp.wind_cap = (unsigned long long)wind_cap;
+    pp.v64_index = as<int>(h->v64_index); pp.v64_cells = as<uint32_t>(h->v64_cells);
+    pp.v64_count = &dc->v64_count; pp.v64_cap = (unsigned long long)v64_cap;
+    pp.err = &dc->err;
+    DCB_TRY(h, launch_face_place(pp, 3 * cap, h->num_sms, s), "launch face placement");
     Vertex64Params w64;
-    w64.B = T.B; w64.list = xp.list; w64.cells = fp.v64_cells; w64.count = fp.v64_count; w64.cap = (unsigned int)v64_cap;
+    w64.B = T.B; w64.list = list; w64.cells = pp.v64_cells; w64.count = pp.v64_count; w64.cap = (unsigned int)v64_cap;
     w64.Vf = nullptr; w64.vclass = nullptr; w64.V64 = as<double>(h->V64); w64.thr = o->svd_threshold;
     DCB_TRY(h, launch_vertex_fp64(w64, v64_cap, h->num_sms, s), "launch fp64 vertices for windings");
     Winding64Params wp;
-    wp.B = T.B; wp.items = fp.wind_items; wp.count = fp.wind_count; wp.cap = (unsigned int)wind_cap;
-    wp.quads = fp.stage_quad; wp.v64_index = fp.v64_index; wp.V64 = w64.V64; wp.err = &dc->err;
+    wp.B = T.B; wp.items = pp.wind_items; wp.count = pp.wind_count; wp.cap = (unsigned int)wind_cap;
+    wp.quads = pp.stage_quad; wp.v64_index = pp.v64_index; wp.V64 = w64.V64; wp.err = &dc->err;
     DCB_TRY(h, launch_winding_fp64(wp, wind_cap, h->num_sms, s), "launch winding fp64");
-    DCB_TRY(h, launch_face_order(fp.stage_quad, fp.stage_key, fp.col_start, fp.col_count, &dc->face_total,
+    DCB_TRY(h, launch_face_order(pp.stage_quad, pp.stage_key, col_start, as<uint32_t>(h->col_count), &dc->face_total,
                                  as<int4>(h->faces), 3 * cap, h->num_sms, s), "launch face order");
     if (o->emit_triangles) {
         // 4) quads -> triangles; FP64 vertices for the quads FP32 cannot orient (the winding
@@ -569,15 +544,15 @@ int batch_rest(dcb_context* h, const BatchLayout& L, TableView& T, const dcb_opt
         TriParams tp;
         tp.B = T.B;
         tp.quads = as<int4>(h->faces); tp.nquads = &dc->face_total; tp.V = qp.V; tp.vclass = qp.vclass;
-        tp.hmax = fp.hmax; tp.tris = as<int>(h->tris); tp.items = as<uint32_t>(h->tri_items);
+        tp.hmax = L.hmax; tp.tris = as<int>(h->tris); tp.items = as<uint32_t>(h->tri_items);
         tp.item_count = &dc->tri_count; tp.item_cap = (unsigned int)wind_cap;
-        tp.v64_index = fp.v64_index; tp.v64_cells = fp.v64_cells; tp.v64_count = fp.v64_count;
-        tp.v64_cap = fp.v64_cap; tp.err = &dc->err;
+        tp.v64_index = pp.v64_index; tp.v64_cells = pp.v64_cells; tp.v64_count = pp.v64_count;
+        tp.v64_cap = pp.v64_cap; tp.err = &dc->err;
         DCB_TRY(h, launch_triangulate(tp, 3 * cap, h->num_sms, s), "launch triangulate");
         DCB_TRY(h, launch_vertex_fp64(w64, v64_cap, h->num_sms, s), "launch fp64 vertices for triangles");
         Tri64Params t64;
         t64.quads = tp.quads; t64.items = tp.items; t64.count = tp.item_count; t64.cap = tp.item_cap;
-        t64.v64_index = fp.v64_index; t64.V64 = w64.V64; t64.tris = tp.tris; t64.err = &dc->err;
+        t64.v64_index = pp.v64_index; t64.V64 = w64.V64; t64.tris = tp.tris; t64.err = &dc->err;
         DCB_TRY(h, launch_tri_fp64(t64, wind_cap, h->num_sms, s), "launch triangle fp64");
     }
     if (n > 1) {
@@ -1150,7 +1125,7 @@ int dcb_destroy(dcb_handle h) {
     if (!h) return DCB_ERR_INVALID_ARGUMENT;
     cudaSetDevice(h->device);
     DevBuf* bufs[] = {&h->grid, &h->bits, &h->super, &h->list, &h->seg_count, &h->seg_start, &h->counters,
-                      &h->V, &h->vclass, &h->fmask, &h->col_count, &h->col_fill, &h->col_start,
+                      &h->V, &h->vclass, &h->col_count, &h->col_fill, &h->col_start,
                       &h->partials, &h->esc_list, &h->hard_list, &h->hard_data, &h->stage_quad,
                       &h->stage_key, &h->faces, &h->wind_items, &h->v64_index, &h->v64_cells, &h->V64,
                       &h->tris, &h->tri_items, &h->face_grad, &h->tilemap, &h->m_verts, &h->m_faces, &h->m_out, &h->m_tris,

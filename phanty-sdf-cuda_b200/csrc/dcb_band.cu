@@ -52,6 +52,9 @@ constexpr int kERows = kXRows + kYRows + kZRows;    // 65 edge rows
 constexpr int kCRows = kTY * kTZ;                   // 16 cell rows
 constexpr int kRows = kERows + kCRows;              // counted rows (edges, then cells)
 constexpr int kMaxEdges = 32 * kXRows + 33 * (kYRows + kZRows);   // 2,120
+// Edge records kept in shared memory per tile; a tile with more listed edges (dense sign noise,
+// not surfaces) has the rest recomputed by the cells that need them, with the same function.
+constexpr int kEdgeCap = 512;
 constexpr int kTileCells = 32 * kTY * kTZ;
 
 // The staged grid values of one tile, 0 outside the grid.
@@ -62,7 +65,7 @@ struct Vals {
 struct BandSmem {
     Vals vb[2];                        // this tile's values and the next tile's (in flight)
     float rw[3][kSX];                  // 1 / cell width along x, y, z at index (lo - 1 + q)
-    float4 e[kMaxEdges];               // per listed edge: averaged normal, flags in w
+    float4 e[kEdgeCap];                // per listed edge: averaged normal, flags in w
     float t[12][kBandThreads];         // per cell thread: lerp parameter of each crossing edge
     unsigned long long m[kERows];      // edge rows: crossing edges of active tile cells
     uint32_t off[kRows + 1];           // exclusive prefix of the row counts
@@ -421,7 +424,7 @@ k_band(const __grid_constant__ BandParams P) {
             }
             __syncthreads();
             // 4) edge normals, a thread per listed edge
-            const int nedges = (int)s.off[kERows];
+            const int nedges = min((int)s.off[kERows], kEdgeCap);
             for (int e = tid; e < nedges; e += kBandThreads) {
                 const uint32_t it = s.list[e];
                 int axis, yl, zl;
@@ -486,7 +489,7 @@ k_band(const __grid_constant__ BandParams P) {
                                             : (axis == 1 ? kYBase + zl * kTY + yl : kZBase + zl * (kTY + 1) + yl);
                     const unsigned long long mrow = s.m[q];
                     const int slot = (int)s.off[q] + __popcll(mrow & ((1ull << xb) - 1ull));
-                    const float4 rec = s.e[slot];
+                    const float4 rec = slot < kEdgeCap ? s.e[slot] : edge_record(s, V, g, x0, y0, z0, axis, xb, yl, zl);
                     const uint32_t fl = __float_as_uint(rec.w);
                     float3 n;
                     if (fl & kEdgeOwn) {
@@ -502,6 +505,10 @@ k_band(const __grid_constant__ BandParams P) {
                     kahan_add(R0, Q0, n.x * nb); kahan_add(R1, Q1, n.y * nb); kahan_add(R2, Q2, n.z * nb);
                 }
                 float ox, oy, oz;
+                // A NaN or infinite value anywhere in the normal equations (a non-finite grid value in
+                // the stencil) propagates into the CPU backend's vertex through its SVD factors
+                // (Cell.cpp:324-361); only the FP64 path repeats that, so such cells go there.
+                if (!isfinite(M00 + M01 + M02 + M11 + M12 + M22 + R0 + R1 + R2 + cu + cv + cw)) ill = true;
                 if (ill || P.force64) {
                     // FP32 cannot be trusted: the FP64 path recomputes this cell from the grid.
                     const unsigned int slot = reserve_slots(P.esc_count, 1u);

@@ -120,8 +120,6 @@ struct QefParams {
                                     // nactive, nothing is processed), or null
     float* V;
     uint8_t* vclass;                // [active] VertexClass
-    uint8_t* fmask;                 // bit a: cell owns a face on its min-corner edge a
-    uint32_t* col_count;            // per grid [3][cx*cy]: col_off + a*cx*cy + i*cy + j
     uint32_t* esc_list;
     unsigned int* esc_count;
     uint32_t* hard_list;            // cells not certified rank 1
@@ -134,7 +132,6 @@ struct QefParams {
     float cond_max;
     int force64;
 };
-cudaError_t launch_cell_qef(const QefParams& P, int num_sms, cudaStream_t s);
 cudaError_t launch_cell_jacobi(const QefParams& P, long long max_items, int num_sms, cudaStream_t s);
 
 struct Vertex64Params {
@@ -166,33 +163,6 @@ cudaError_t launch_scan(const uint32_t* in, long long n, uint32_t* partials, uin
                         unsigned long long* grand_total, cudaStream_t s);
 long long scan_partials_len(long long n);
 
-struct FaceParams {
-    BatchTable B;
-    const uint64_t* list;
-    long long nactive;             // active cells (capacity when live is set)
-    const unsigned long long* live; // device count of active cells (a captured graph; above
-                                    // nactive, nothing is processed), or null
-    const uint8_t* fmask;
-    const float* V;
-    const uint8_t* vclass;
-    const uint32_t* bits;
-    const uint32_t* super;
-    const uint32_t* col_start;     // per grid [3][cx*cy] (global column index)
-    const uint32_t* col_count;
-    uint32_t* col_fill;
-    int4* stage_quad;
-    uint2* stage_key;              // {k, column}
-    uint4* wind_items;             // {slot, axis | grid << 2, packed lo, packed hi}
-    unsigned int* wind_count;
-    unsigned long long wind_cap;
-    int* v64_index;                // [rank] -> FP64 vertex slot (-1 none, -2 being claimed)
-    uint32_t* v64_cells;           // cells whose FP64 vertex the windings need
-    unsigned int* v64_count;
-    unsigned long long v64_cap;
-    int* err;
-    float hmax;                    // unused: each grid's slot holds its own cell width
-};
-cudaError_t launch_face_scatter(const FaceParams& P, int num_sms, cudaStream_t s);
 cudaError_t launch_face_order(const int4* stage_quad, const uint2* stage_key, const uint32_t* col_start,
                               const uint32_t* col_count, const unsigned long long* nfaces, int4* faces,
                               long long max_faces, int num_sms, cudaStream_t s);

@@ -78,11 +78,19 @@ def _calls():
             "backward": (dense_be, backward)}
 
 
-def _same(a, b):
+def _same(a, b, rtol=0.0):
     if isinstance(a, (tuple, list)):
-        return len(a) == len(b) and all(_same(x, y) for x, y in zip(a, b))
+        return len(a) == len(b) and all(_same(x, y, rtol) for x, y in zip(a, b))
     a, b = np.asarray(a), np.asarray(b)
-    return a.shape == b.shape and np.array_equal(a, b, equal_nan=a.dtype.kind == "f")
+    if a.shape != b.shape:
+        return False
+    if rtol:
+        return bool(np.allclose(a, b, rtol=rtol, atol=rtol * float(np.abs(b).max(initial=0.0)), equal_nan=True))
+    return np.array_equal(a, b, equal_nan=a.dtype.kind == "f")
+
+
+# d(loss)/d(grid) is accumulated with float atomics: equal up to the order of the additions
+RTOL = {"backward": 1e-5}
 
 
 @pytest.mark.parametrize("name", ["extract_device", "extract_host", "extract_batch", "sparse", "mesh_to_sdf",
@@ -109,11 +117,11 @@ def test_allocation_failure_is_reported_and_recoverable(name):
             finally:
                 _hook(-1)
             if ok:
-                assert _same(got, expect), "%s succeeded after %d allocations with a different result" % (name, k)
+                assert _same(got, expect, RTOL.get(name, 0.0)), "%s succeeded after %d allocations with a different result" % (name, k)
                 break
             failures += 1
             # the handle is still usable and gives the untouched handle's result
-            assert _same(fn(be), expect), "%s: handle unusable after a failure at allocation %d" % (name, k)
+            assert _same(fn(be), expect, RTOL.get(name, 0.0)), "%s: handle unusable after a failure at allocation %d" % (name, k)
         finally:
             _hook(-1)
             be.close()
