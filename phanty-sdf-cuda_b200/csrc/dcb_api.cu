@@ -460,7 +460,7 @@ void batch_state(dcb_context* h, const BatchLayout& L, int n, const dcb_opts* o,
 int batch_rest(dcb_context* h, const BatchLayout& L, TableView& T, const dcb_opts* o, cudaStream_t s, long long cap,
                const unsigned long long* live, bool events) {
     const int n = (int)L.slots.size();
-    const long long nseg = L.nseg, ncol = L.ncol;
+    const long long ncol = L.ncol;
     Counters* dc = as<Counters>(h->counters);
     const long long wind_cap = std::min(0x7fffffffLL, 3 * cap);
     const long long v64_cap = cap;

@@ -1,7 +1,7 @@
-// dcb_band.cu — Hermite samples, 4-cell normal averaging, FP32 QEF and face staging for a
-// single grid, a tile of cells at a time with the tile's stencil in shared memory.
+// dcb_band.cu — Hermite samples, 4-cell normal averaging, FP32 QEF and face staging, a tile of
+// cells at a time with the tile's stencil in shared memory, over every grid of a batch.
 //
-// Semantics are those of k_cell_qef (dcb_vertex.cu), which follows the reference CPU backend:
+// Semantics follow the reference CPU backend:
 //   Hermite samples   Cell::fill_hermite_data (src/cpp/Cell.cpp:162-212), lerp t = fa/(fa-fb
 //                     +1e-16) (:49-52), normalised trilinear gradient (:80-155)
 //   averaging         average_hermite_normals / process_edge (src/cpp/hermite_update.cpp:
@@ -24,9 +24,9 @@
 //   2. lists, row by row with ballots, the crossing edges of the tile's active cells;
 //   3. computes, a thread per listed edge, the edge's averaged normal ONCE (four trilinear
 //      gradients, each an edge difference plus two bilinear differences of the staged
-//      points) — the per-cell kernel recomputes it in each of the four cells;
+//      points), not once per cell that shares it;
 //   4. solves, a thread per active cell, its centred FP32 normal equations (Kahan sums,
-//      rank-1 certificate; other cells to the Jacobi / FP64 lists as in k_cell_qef), writes
+//      rank-1 certificate; other cells to the Jacobi (dcb_vertex.cu) or FP64 list), writes
 //      the vertex at its rank, and stages each face it owns with the ranks of its four cells
 //      and the gradient sum that decides the winding (k_face_place finishes the faces once
 //      every vertex exists).
@@ -131,7 +131,8 @@ __device__ __forceinline__ bool active_local(const Vals& s, int xl, int yl, int 
 }
 
 // gradientAt (contouring.cpp:141-207) in FP32 at grid point (x, y, z), neighbours clamped to
-// the grid, from the staged points (orientation tests only, as grid_gradient32).
+// the grid, from the staged points (orientation tests only: a 2-ulp quotient is far inside the
+// uncertainty margin, and uncertain faces are re-decided in FP64).
 __device__ __forceinline__ float3 gradient_at(const Vals& s, const GridDesc& g, int x0, int y0, int z0,
                                               int x, int y, int z) {
     const int xm = max(x - 1, 0), xp = min(x + 1, g.nx - 1);
@@ -158,7 +159,8 @@ __device__ __forceinline__ void edge_row(int q, int& axis, int& yl, int& zl) {
 }
 
 // Averaged normal of the crossing edge with low endpoint at local (xl, yl, zl) along axis, or
-// the kEdgeOwn flag (edge_normal of dcb_vertex.cu, with the stencil in shared memory).
+// the kEdgeOwn flag. On an edge every trilinear gradient reduces to the edge difference plus
+// two bilinear differences, so the four cells' normals need the edge's 2 x 3 x 3 points.
 __device__ float4 edge_record(const BandSmem& sm, const Vals& s, const GridDesc& g, int x0, int y0, int z0, int axis,
                               int xl, int yl, int zl) {
     const int lx = x0 + xl, ly = y0 + yl, lz = z0 + zl;

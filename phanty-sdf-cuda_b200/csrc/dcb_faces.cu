@@ -103,28 +103,7 @@ cudaError_t launch_scan(const uint32_t* in, long long n, uint32_t* partials, uin
 
 long long scan_partials_len(long long n) { return (n + kScanTile - 1) / kScanTile; }
 
-// ---- face scatter ----------------------------------------------------------------------
-
-constexpr int kFaceThreads = 128;
-
-
-// gradientAt (contouring.cpp:141-207) in FP32 (orientation tests only: a 2-ulp quotient is
-// far inside the uncertainty margin, and uncertain faces are re-decided in FP64).
-__device__ __forceinline__ float3 grid_gradient32(const GridDesc& g, int i, int j, int k) {
-    const int im = max(i - 1, 0), ip = min(i + 1, g.nx - 1);
-    const int jm = max(j - 1, 0), jp = min(j + 1, g.ny - 1);
-    const int km = max(k - 1, 0), kp = min(k + 1, g.nz - 1);
-    float3 o = make_float3(0.f, 0.f, 0.f);
-    const float dx = pos_axis(g.ox, g.vx, ip) - pos_axis(g.ox, g.vx, im);
-    if (fabsf(dx) > 1e-12f) o.x = __fdividef(__ldg(g.v + pidx(g, ip, j, k)) - __ldg(g.v + pidx(g, im, j, k)), dx);
-    const float dy = pos_axis(g.oy, g.vy, jp) - pos_axis(g.oy, g.vy, jm);
-    if (fabsf(dy) > 1e-12f) o.y = __fdividef(__ldg(g.v + pidx(g, i, jp, k)) - __ldg(g.v + pidx(g, i, jm, k)), dy);
-    const float dz = pos_axis(g.oz, g.vz, kp) - pos_axis(g.oz, g.vz, km);
-    if (fabsf(dz) > 1e-12f) o.z = __fdividef(__ldg(g.v + pidx(g, i, j, kp)) - __ldg(g.v + pidx(g, i, j, km)), dz);
-    const float n2 = o.x * o.x + o.y * o.y + o.z * o.z;
-    if (n2 > 0.f) { const float r = rsqrtf(n2); o.x *= r; o.y *= r; o.z *= r; }
-    return o;
-}
+// ---- shared helpers of the face kernels ---------------------------------------------
 
 __device__ __forceinline__ float3 ldv(const float* V, uint32_t r) {
     return make_float3(__ldg(V + 3 * (size_t)r), __ldg(V + 3 * (size_t)r + 1), __ldg(V + 3 * (size_t)r + 2));
