@@ -354,7 +354,8 @@ int launch_marks(dcb_context* h, const BatchLayout& L, const TableView& T, cudaS
         mp.B = T.B; mp.tile_slot = T.tile_slot[v]; mp.tile_off = T.tile_off[v];
         mp.m = (int)L.tile_slot[v].size(); mp.ntiles = L.tile_off[v].back();
         mp.bits = as<uint32_t>(h->bits); mp.seg_count = as<uint32_t>(h->seg_count);
-        mp.tilemap = as<uint32_t>(h->tilemap);
+        // the band kernel's tile map, when the workspace holds one for this layout
+        mp.tilemap = h->tilemap.bytes >= sizeof(uint32_t) * (size_t)L.nchunk ? as<uint32_t>(h->tilemap) : nullptr;
         DCB_TRY(h, launch_mark(mp, v ? mark_narrow_tile_words() : mark_tile_words(), s), "launch mark");
     }
     return DCB_OK;
@@ -1467,6 +1468,7 @@ int dcb_autotune_mark(dcb_handle h, const dcb_grid* grids, int n, int* waves_out
                 if (rc == DCB_OK) {
                     DCB_TRY(h, ensure(h->bits, sizeof(uint32_t) * L.bits), "alloc bits");
                     DCB_TRY(h, ensure(h->seg_count, sizeof(uint32_t) * L.nseg), "alloc segment counts");
+                    DCB_TRY(h, ensure(h->tilemap, sizeof(uint32_t) * std::max(1LL, L.nchunk)), "alloc tile map");
                     float ms[3];
                     for (int r = 0; r < 4 && rc == DCB_OK; ++r) {       // one warm-up, three timed
                         DCB_TRY(h, cudaEventRecord(h->ev[0], s), "event");
