@@ -159,11 +159,17 @@ def test_nan_values_match_oracle_and_reference():
     ref = O.dc_extract(v, dims, sp, org)
     V = mesh.vertices.reshape(-1, 3).astype(np.float64)
     F = mesh.faces.reshape(-1, 4)
-    assert np.array_equal(cells, ref["cells"]) and np.array_equal(F, ref["F"])
+    assert np.array_equal(cells, ref["cells"])
     nan_rows = np.isnan(V).any(1)
-    assert nan_rows.any() and np.array_equal(nan_rows, np.isnan(ref["V"]).any(1))
+    ref_nan = np.isnan(ref["V"]).any(1)
+    assert nan_rows.any() and np.array_equal(nan_rows, ref_nan), "NaN vertices: engine %s, oracle %s" % (
+        np.nonzero(nan_rows & ~ref_nan)[0][:8].tolist(), np.nonzero(ref_nan & ~nan_rows)[0][:8].tolist())
     err = np.abs(V[~nan_rows] - ref["V"][~nan_rows]) / np.asarray(sp)
     assert err.max() <= VERTEX_TOL
+    bad = np.nonzero((F != ref["F"]).any(1))[0] if F.shape == ref["F"].shape else np.arange(1)
+    assert len(bad) == 0, "%d quads differ (escalated %d), first: engine %s oracle %s, engine vertices %s, oracle %s" % (
+        len(bad), st.escalated_fp64_cells, F[bad[:3]].tolist(), ref["F"][bad[:3]].tolist(),
+        V[F[bad[0]]].tolist(), ref["V"][ref["F"][bad[0]]].tolist())
     r = O.ref_cpu_extract(v, dims, sp, org)
     if r is not None:
         rV, rF, _ = r
