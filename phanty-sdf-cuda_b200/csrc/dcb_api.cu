@@ -86,6 +86,7 @@ struct dcb_context {
     // (cells along x) that marches 256-cell x-tiles instead of 1024-cell ones
     int tune_waves = 4;
     int tune_narrow_cells = 256;
+    int tune_band_ctas = 0;           // band kernel: persistent CTAs per SM (0: occupancy limit)
     int cx = 0, cy = 0, cz = 0;
     // batch layout table (device + pinned staging) and the last batch's per-grid offsets
     DevBuf table, cell_slot;
@@ -455,6 +456,47 @@ void batch_state(dcb_context* h, const BatchLayout& L, int n, const dcb_opts* o,
     for (int b = 0; b <= n; ++b) h->vert_offsets[b] = (int64_t)h_vert_off[b];
 }
 
+// The vertex outputs and solve lists of a batch of up to `cap` active cells.
+QefParams qef_params(dcb_context* h, const TableView& T, const dcb_opts* o, long long cap,
+                     const unsigned long long* live) {
+    Counters* dc = as<Counters>(h->counters);
+    QefParams qp;
+    qp.B = T.B; qp.list = as<uint64_t>(h->list); qp.nactive = cap; qp.live = live;
+    qp.V = as<float>(h->V); qp.vclass = as<uint8_t>(h->vclass);
+    qp.esc_list = as<uint32_t>(h->esc_list); qp.esc_count = &dc->esc_count;
+    qp.hard_list = as<uint32_t>(h->hard_list); qp.hard_data = as<float4>(h->hard_data); qp.hard_count = &dc->hard_count;
+    qp.rank_hist = dc->rank_hist;
+    qp.err = &dc->err;
+    qp.thr = (float)o->svd_threshold; qp.band = (float)o->fp64_threshold_band;
+    qp.cond_max = (float)std::min(o->fp64_escalation_cond, 3.0e38); qp.force64 = o->force_fp64;
+    return qp;
+}
+
+// The band kernel's parameters for a batch of up to `cap` active cells (qp: the vertex
+// outputs and lists it shares with the Jacobi pass).
+BandParams band_params(dcb_context* h, const BatchLayout& L, const TableView& T, const QefParams& qp, long long cap,
+                       const unsigned long long* live) {
+    Counters* dc = as<Counters>(h->counters);
+    BandParams bp;
+    bp.B = T.B;
+    bp.bits = as<uint32_t>(h->bits); bp.seg_start = as<uint32_t>(h->seg_start); bp.super = as<uint32_t>(h->super);
+    bp.list = as<uint64_t>(h->list);
+    bp.cell_slot = L.slots.size() > 1 ? as<uint32_t>(h->cell_slot) : nullptr;
+    bp.tilemap = as<uint32_t>(h->tilemap);
+    bp.nchunks = L.nchunk;
+    bp.ctas_per_sm = h->tune_band_ctas;
+    bp.chunk_next = &dc->band_chunk;
+    bp.V = qp.V; bp.vclass = qp.vclass; bp.col_count = as<uint32_t>(h->col_count);
+    bp.esc_list = qp.esc_list; bp.esc_count = qp.esc_count;
+    bp.hard_list = qp.hard_list; bp.hard_data = qp.hard_data; bp.hard_count = qp.hard_count;
+    bp.rank_hist = qp.rank_hist;
+    bp.face_cells = as<int4>(h->faces); bp.face_grad = as<float4>(h->face_grad);
+    bp.face_count = &dc->face_staged; bp.face_cap = (unsigned long long)(3 * cap); bp.nv = cap; bp.live = live;
+    bp.err = &dc->err;
+    bp.thr = qp.thr; bp.band = qp.band; bp.force64 = qp.force64;
+    return bp;
+}
+
 // Everything after the mark for up to `cap` active cells: ranks and list, vertices, faces.
 // With `live` (a device count, as in a captured graph) the kernels take the active count from
 // there, bounded by cap; otherwise it is cap.
@@ -472,31 +514,9 @@ int batch_rest(dcb_context* h, const BatchLayout& L, TableView& T, const dcb_opt
     // 2) the tile band kernel over the tiles of every grid of the batch: ranks, the active-cell
     //    list, vertices (rank-1 certified in FP32; Jacobi list; FP64 list) and staged faces
     //    from shared-memory stencils; then the Jacobi and FP64 vertices.
-    uint32_t* const bits = as<uint32_t>(h->bits);
     uint64_t* const list = as<uint64_t>(h->list);
-    QefParams qp;
-    qp.B = T.B; qp.list = list; qp.nactive = cap; qp.live = live; qp.V = as<float>(h->V); qp.vclass = as<uint8_t>(h->vclass);
-    qp.esc_list = as<uint32_t>(h->esc_list); qp.esc_count = &dc->esc_count;
-    qp.hard_list = as<uint32_t>(h->hard_list); qp.hard_data = as<float4>(h->hard_data); qp.hard_count = &dc->hard_count;
-    qp.rank_hist = dc->rank_hist;
-    qp.err = &dc->err;
-    qp.thr = (float)o->svd_threshold; qp.band = (float)o->fp64_threshold_band;
-    qp.cond_max = (float)std::min(o->fp64_escalation_cond, 3.0e38); qp.force64 = o->force_fp64;
-    BandParams bp;
-    bp.B = T.B;
-    bp.bits = bits; bp.seg_start = as<uint32_t>(h->seg_start); bp.super = as<uint32_t>(h->super); bp.list = list;
-    bp.cell_slot = n > 1 ? as<uint32_t>(h->cell_slot) : nullptr;
-    bp.tilemap = as<uint32_t>(h->tilemap);
-    bp.nchunks = L.nchunk;
-    bp.chunk_next = &dc->band_chunk;
-    bp.V = qp.V; bp.vclass = qp.vclass; bp.col_count = as<uint32_t>(h->col_count);
-    bp.esc_list = qp.esc_list; bp.esc_count = qp.esc_count;
-    bp.hard_list = qp.hard_list; bp.hard_data = qp.hard_data; bp.hard_count = qp.hard_count;
-    bp.rank_hist = qp.rank_hist;
-    bp.face_cells = as<int4>(h->faces); bp.face_grad = as<float4>(h->face_grad);
-    bp.face_count = &dc->face_staged; bp.face_cap = (unsigned long long)(3 * cap); bp.nv = cap; bp.live = live;
-    bp.err = &dc->err;
-    bp.thr = qp.thr; bp.band = qp.band; bp.force64 = qp.force64;
+    const QefParams qp = qef_params(h, T, o, cap, live);
+    const BandParams bp = band_params(h, L, T, qp, cap, live);
     DCB_TRY(h, launch_band(bp, h->num_sms, s), "launch band");
     DCB_TRY(h, launch_cell_jacobi(qp, cap, h->num_sms, s), "launch jacobi");
     Vertex64Params v64;
@@ -1490,6 +1510,63 @@ int dcb_autotune_mark(dcb_handle h, const dcb_grid* grids, int n, int* waves_out
     h->tune_narrow_cells = best_n;
     if (waves_out) *waves_out = best_w;
     if (narrow_cells_out) *narrow_cells_out = best_n;
+    if (best_ms_out) *best_ms_out = best;
+    return DCB_OK;
+}
+
+int dcb_autotune_band(dcb_handle h, const dcb_grid* grids, int n, int* ctas_per_sm_out, float* best_ms_out,
+                      void* cuda_stream) {
+    if (h) ++h->gen;                        // reuses the extraction workspace
+    if (!h) return DCB_ERR_INVALID_ARGUMENT;
+    if (!grids || n < 1) return fail(h, DCB_ERR_INVALID_ARGUMENT, "empty batch");
+    for (int b = 0; b < n; ++b) {
+        const int rc = validate(h, grids + b);
+        if (rc != DCB_OK) return rc;
+    }
+    if (cudaSetDevice(h->device) != cudaSuccess) { cudaGetLastError(); return fail(h, DCB_ERR_CUDA, "set device"); }
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(cuda_stream);
+    BatchLayout L;
+    TableView T;
+    int rc = batch_prepare(h, grids, n, s, L, T);
+    if (rc != DCB_OK) return rc;
+    rc = batch_mark(h, L, T, s, false);
+    if (rc != DCB_OK) return rc;
+    Counters* dc = as<Counters>(h->counters);
+    Counters* hc = reinterpret_cast<Counters*>(h->h_counters);
+    DCB_TRY(h, cudaMemcpyAsync(hc, dc, sizeof(Counters), cudaMemcpyDeviceToHost, s), "read count");
+    DCB_TRY(h, cudaStreamSynchronize(s), "mark");
+    const long long nv = (long long)hc->total_active;
+    const int keep = h->tune_band_ctas;
+    int best_w = keep;
+    float best = 0.f;
+    if (nv > 0 && nv < 0x7fffffffLL) {
+        dcb_opts od;
+        dcb_default_opts(&od);
+        rc = batch_alloc(h, n, nv, &od, T);
+        if (rc != DCB_OK) return rc;
+        const QefParams qp = qef_params(h, T, &od, nv, nullptr);
+        const int maxw = band_max_ctas_per_sm();
+        best = 1e30f;
+        for (int w = 1; w <= maxw; ++w) {
+            h->tune_band_ctas = w;
+            const BandParams bp = band_params(h, L, T, qp, nv, nullptr);
+            float ms[3];
+            for (int r = 0; r < 4; ++r) {                    // one warm-up, three timed
+                // the band kernel's counters (work queue, lists, staged faces) start at zero
+                DCB_TRY(h, cudaMemsetAsync(h->counters.p, 0, sizeof(Counters), s), "memset counters");
+                DCB_TRY(h, cudaEventRecord(h->ev[0], s), "event");
+                const cudaError_t e = launch_band(bp, h->num_sms, s);
+                if (e != cudaSuccess) { h->tune_band_ctas = keep; return cuda_fail(h, e, "launch band"); }
+                DCB_TRY(h, cudaEventRecord(h->ev[1], s), "event");
+                DCB_TRY(h, cudaEventSynchronize(h->ev[1]), "autotune");
+                if (r > 0) ms[r - 1] = elapsed(h->ev[0], h->ev[1]);
+            }
+            std::sort(ms, ms + 3);
+            if (ms[1] < best) { best = ms[1]; best_w = w; }
+        }
+    }
+    h->tune_band_ctas = best_w;
+    if (ctas_per_sm_out) *ctas_per_sm_out = best_w;
     if (best_ms_out) *best_ms_out = best;
     return DCB_OK;
 }

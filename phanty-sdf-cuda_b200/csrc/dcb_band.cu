@@ -578,7 +578,9 @@ cudaError_t launch_band_t(const BandParams& P, int num_sms, cudaStream_t s) {
     int per_sm = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_band<ONE>, kBandThreads, bytes);
     if (e != cudaSuccess) return e;
-    long long blocks = (long long)num_sms * (per_sm > 0 ? per_sm : 1);
+    if (per_sm < 1) per_sm = 1;
+    if (P.ctas_per_sm > 0 && P.ctas_per_sm < per_sm) per_sm = P.ctas_per_sm;
+    long long blocks = (long long)num_sms * per_sm;
     if (blocks > P.nchunks) blocks = P.nchunks;
     k_band<ONE><<<(unsigned)blocks, kBandThreads, bytes, s>>>(P);
     return cudaGetLastError();
@@ -587,6 +589,20 @@ cudaError_t launch_band_t(const BandParams& P, int num_sms, cudaStream_t s) {
 cudaError_t launch_band(const BandParams& P, int num_sms, cudaStream_t s) {
     if (P.nchunks <= 0) return cudaSuccess;
     return P.B.n == 1 ? launch_band_t<true>(P, num_sms, s) : launch_band_t<false>(P, num_sms, s);
+}
+
+int band_max_ctas_per_sm() {
+    const int bytes = (int)sizeof(BandSmem);
+    if (cudaFuncSetAttribute(k_band<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return 1;
+    }
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_band<true>, kBandThreads, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return 1;
+    }
+    return per_sm > 0 ? per_sm : 1;
 }
 
 long long band_chunk_count(int nx, int ny, int nz) {

@@ -200,6 +200,7 @@ struct BandParams {
     uint32_t* cell_slot;           // written (batches, may be null): grid of every rank
     const uint32_t* tilemap;       // active tiles of every chunk (mark)
     long long nchunks;             // all grids' chunks
+    int ctas_per_sm;               // persistent CTAs per SM (<= the occupancy limit; 0: the limit)
     unsigned int* chunk_next;      // chunk counter, zero before the launch
     float* V;
     uint8_t* vclass;
@@ -223,6 +224,7 @@ struct BandParams {
     int force64;
 };
 cudaError_t launch_band(const BandParams& P, int num_sms, cudaStream_t s);
+int band_max_ctas_per_sm();                           // occupancy limit of the band kernel
 long long band_chunk_count(int nx, int ny, int nz);   // band kernel work units of one grid
 
 // Staged faces -> FP32 winding decision and their slot in the column order (dcb_band.cu).
