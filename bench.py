@@ -340,7 +340,6 @@ def run_batch_workload(args):
     be = B200DualContouringBackend(0)
     ncell = sum((d[0] - 1) * (d[1] - 1) * (d[2] - 1) for _, d, _, _ in grids)
     waves, narrow, tune_ms = be.autotune_mark(grids)         # tile shapes for this batch
-    band_ctas, band_ms = be.autotune_band(grids)              # band kernel width for this batch
     stream = torch.cuda.current_stream()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     for _ in range(args.warmup):
@@ -396,7 +395,6 @@ def run_batch_workload(args):
                      "qef": round(st.qef_ms, 4), "faces": round(st.face_emission_ms, 4)},
         "escalated_fp64_cells": st.escalated_fp64_cells, "winding_fp64_faces": st.winding_fp64_faces,
         "mark_tiles": {"waves": waves, "narrow_tile_max_cells": narrow, "autotune_mark_ms": round(tune_ms, 4)},
-        "band_kernel": {"ctas_per_sm": band_ctas, "autotune_band_ms": round(band_ms, 4)},
         "sequential_plain_ms": round(ms_seq, 3) if ms_seq else None,
         "batched_speedup": round(ms_seq / ms_batch, 2) if ms_seq else None,
         "graph": {"ms_per_step": round(ms_graph, 4), "mcells_per_s": round(ncell / (ms_graph / 1e3) / 1e6, 2),
@@ -924,9 +922,9 @@ def main():
          "achieved_gbs": round(mark_bytes / (stats.marking_ms / 1e3) / 1e9, 1) if stats.marking_ms else None,
          "frac": round(mark_bytes / (stats.marking_ms / 1e3) / 1e9 / peak, 4) if stats.marking_ms else None},
         {"stage": "segment scan", "ms": round(stats.compaction_ms, 4)},
-        {"stage": "vertices (k_expand_ranks, k_band, k_cell_jacobi, k_vertex_fp64)", "ms": round(stats.qef_ms, 4),
+        {"stage": "vertices (k_expand_ranks, k_cell_qef, k_cell_jacobi, k_vertex_fp64)", "ms": round(stats.qef_ms, 4),
          "algorithmic_bytes": band_bytes},
-        {"stage": "faces (column scan, k_face_place, FP64 windings, k_face_order)",
+        {"stage": "faces (column scan, k_face_scatter, FP64 windings, k_face_order)",
          "ms": round(stats.face_emission_ms, 4), "algorithmic_bytes": face_bytes,
          "sub_ms": {"count": round(stats.face_count_ms, 4), "prefix_sum": round(stats.face_prefix_sum_ms, 4),
                     "fill": round(stats.face_fill_ms, 4)}},

@@ -316,15 +316,6 @@ int dcb_batch_graph_destroy(dcb_handle h);
 int dcb_autotune_mark(dcb_handle h, const dcb_grid* grids, int n, int* waves_out, int* narrow_cells_out,
                       float* best_ms_out, void* cuda_stream);
 
-/* Autotuner of the band kernel (the Hermite / QEF / face-staging pass over 32x4x4-cell tiles):
- * marks the batch, then times the kernel with 1 .. (occupancy limit) persistent CTAs per SM
- * and keeps the fastest width in the handle for later extractions. No counterpart in the
- * reference (its kernels have fixed launch shapes). Results of an extraction do not depend on
- * the width. The chosen CTAs per SM and the median band time (ms; 0 when the batch has no
- * active cell) are returned through the optional pointers. */
-int dcb_autotune_band(dcb_handle h, const dcb_grid* grids, int n, int* ctas_per_sm_out, float* best_ms_out,
-                      void* cuda_stream);
-
 /* ---- mesh -> signed distance grid ------------------------------------------------------ */
 
 typedef struct {

@@ -380,21 +380,6 @@ class B200DualContouringBackend:
                                              ctypes.c_void_p(s)), self._h)
         return w.value, nc.value, ms.value
 
-    def autotune_band(self, grids, stream=None):
-        """Time the band kernel (Hermite, QEF and face staging over 32x4x4-cell tiles) on ``grids``
-        with 1 .. its occupancy limit of persistent CTAs per SM and keep the fastest for this
-        backend; returns (ctas_per_sm, ms)."""
-        n = len(grids)
-        arr = (_lib.DcbGrid * n)()
-        for b, (values, dims, spacing, origin) in enumerate(grids):
-            d = DenseSdfGridDevice(*dims, *spacing, *origin, d_values=values)
-            arr[b] = self._grid_c(d, d.pointer())
-        w, ms = ctypes.c_int(), ctypes.c_float()
-        s = _current_stream() if stream is None else stream
-        _lib.check(self._L.dcb_autotune_band(self._h, arr, n, ctypes.byref(w), ctypes.byref(ms), ctypes.c_void_p(s)),
-                   self._h)
-        return w.value, ms.value
-
     def extract_batch(self, grids, stream=None):
         """Batched extraction of ``grids`` = [(CUDA float32 values, dims, spacing, origin)] in one
         pass of the pipeline. Returns ``[(V (nv,3) float32, F (nf,vpf) int32)]`` CUDA tensors per

@@ -1,16 +1,17 @@
 // dcb_api.cu — handle, workspace and the C ABI declared in include/dcb.h.
 //
-// Pipeline of one extraction, or of a batch of grids as one (all on the caller's stream):
-//   k_mark_zmarch    grid -> active bits, per-segment counts, active band tiles (dcb_mark.cu)
+// Pipeline of one extraction (all on the caller's stream):
+//   k_mark_zmarch    grid -> active bits, per-segment counts, a flag for non-finite
+//                    values                                            (dcb_mark.cu)
 //   scan             segment counts -> segment first ranks, total     (dcb_faces.cu)
 //   [host reads the active count: sizes the vertex buffers]
-//   k_band           per 32x4x4-cell tile, stencils in shared memory: ranks, super-word
-//                    ranks, the active-cell list, Hermite + averaging + QEF (rank-1
-//                    certified), column counts, staged faces; other cells listed (dcb_band.cu)
+//   k_expand_ranks   super-word ranks + packed active-cell list        (dcb_mark.cu)
+//   k_cell_qef       Hermite + averaging + QEF (rank-1 certified), face masks, column
+//                    counts; other cells listed                        (dcb_vertex.cu)
 //   k_cell_jacobi    listed cells solved with FP32 Jacobi              (dcb_vertex.cu)
 //   k_vertex_fp64    cells FP32 does not trust, re-solved in FP64      (dcb_vertex64.cu)
 //   scan             column counts -> column starts, face total       (dcb_faces.cu)
-//   k_face_place     staged faces into their columns, FP32 winding    (dcb_faces.cu)
+//   k_face_scatter   quads into their columns, FP32 winding           (dcb_faces.cu)
 //   k_vertex_fp64    FP64 vertices of the cells of uncertain windings  (dcb_vertex64.cu)
 //   k_winding_fp64   uncertain windings re-decided in FP64            (dcb_vertex64.cu)
 //   k_face_order     rank by k inside each column -> final face list  (dcb_faces.cu)
@@ -40,8 +41,7 @@ struct Counters {
     unsigned int tri_count;           // quads whose triangle orientation goes to FP64
     unsigned long long rank_hist[4];
     unsigned long long face_total;
-    unsigned int band_chunk;          // tile band kernel: next chunk
-    unsigned int face_staged;         // tile band kernel: staged faces
+    int nonfinite;                    // the mark met a NaN or infinite grid value
 };
 
 struct DevBuf {
@@ -59,9 +59,9 @@ struct dcb_context {
     std::string last_error;
     cudaEvent_t ev[10] = {};
     bool substage_events = false;     // ev[8] / ev[9] hold the face sub-stages of the last call
-    DevBuf grid, bits, super, list, seg_count, seg_start, counters, V, vclass, col_count, col_fill,
+    DevBuf grid, bits, super, list, seg_count, seg_start, counters, V, vclass, fmask, col_count, col_fill,
         col_start, partials, esc_list, hard_list, hard_data, stage_quad, stage_key, faces, wind_items,
-        v64_index, v64_cells, V64, tris, tri_items, adj_rows, adj_owners, ours_ws, face_grad, tilemap;
+        v64_index, v64_cells, V64, tris, tri_items, adj_rows, adj_owners, ours_ws;
     // sparse backends
     DevBuf sp_words, sp_brick, sp_vcount, sp_vstart, sp_vtmp, sp_ntmp, sp_N, sp_vcell, sp_fcount, sp_fstart,
         sp_stage, sp_counters;
@@ -86,7 +86,6 @@ struct dcb_context {
     // (cells along x) that marches 256-cell x-tiles instead of 1024-cell ones
     int tune_waves = 4;
     int tune_narrow_cells = 256;
-    int tune_band_ctas = 0;           // band kernel: persistent CTAs per SM (0: occupancy limit)
     int cx = 0, cy = 0, cz = 0;
     // batch layout table (device + pinned staging) and the last batch's per-grid offsets
     DevBuf table, cell_slot;
@@ -202,11 +201,10 @@ float elapsed(cudaEvent_t a, cudaEvent_t b) {
 struct BatchLayout {
     std::vector<GridSlot> slots;
     std::vector<long long> seg_off, col_off;          // n + 1
-    std::vector<long long> chunk_off;                 // n + 1: first tile-band chunk of each grid
     // mark launches: index 1 for 256-cell x-tiles, 0 for 1024-cell ones
     std::vector<int> tile_slot[2];                    // grids of each mark launch
     std::vector<long long> tile_off[2];               // their first tiles (+ total)
-    long long bits = 0, super = 0, nseg = 0, ncol = 0, ncell = 0, nchunk = 0;
+    long long bits = 0, super = 0, nseg = 0, ncol = 0, ncell = 0;
     float hmax = 0.f;
 };
 
@@ -214,7 +212,6 @@ int layout_batch(dcb_context* h, const dcb_grid* in, int n, BatchLayout& L) {
     L.slots.resize(n);
     L.seg_off.assign(n + 1, 0);
     L.col_off.assign(n + 1, 0);
-    L.chunk_off.assign(n + 1, 0);
     for (int v = 0; v < 2; ++v) { L.tile_slot[v].clear(); L.tile_off[v].assign(1, 0); }
     for (int b = 0; b < n; ++b) {
         GridSlot& S = L.slots[b];
@@ -244,9 +241,6 @@ int layout_batch(dcb_context* h, const dcb_grid* in, int n, BatchLayout& L) {
         S.col_off = L.ncol;
         L.seg_off[b] = L.nseg;
         L.col_off[b] = L.ncol;
-        L.chunk_off[b] = L.nchunk;
-        S.chunk_off = L.nchunk;
-        L.nchunk += band_chunk_count(g.nx, g.ny, g.nz);
         L.bits += rows * g.W;
         L.super += rows * g.W8;
         L.nseg += rows * S.nxt;
@@ -260,8 +254,6 @@ int layout_batch(dcb_context* h, const dcb_grid* in, int n, BatchLayout& L) {
     }
     L.seg_off[n] = L.nseg;
     L.col_off[n] = L.ncol;
-    L.chunk_off[n] = L.nchunk;
-    if (L.nchunk >= 0xffffffffLL) return fail(h, DCB_ERR_TOO_LARGE, "batch too large for the tile band kernel");
     for (int v = 0; v < 2; ++v)
         if (L.tile_off[v].back() > 0x7fffffffLL) return fail(h, DCB_ERR_TOO_LARGE, "grid too large for the tiling");
     if (L.nseg >= 0xffffffffLL || L.ncol >= 0xffffffffLL) return fail(h, DCB_ERR_TOO_LARGE, "batch too large");
@@ -311,9 +303,8 @@ int upload_table(dcb_context* h, const BatchLayout& L, cudaStream_t s, TableView
     const size_t o_col = align_up(o_seg + sizeof(long long) * (n + 1));
     const size_t o_vert = align_up(o_col + sizeof(long long) * (n + 1));
     const size_t o_face = align_up(o_vert + sizeof(unsigned long long) * (n + 1));
-    const size_t o_chunk = align_up(o_face + sizeof(unsigned long long) * (n + 1));
     size_t o_ts[2], o_to[2];
-    size_t at = align_up(o_chunk + sizeof(long long) * (n + 1));
+    size_t at = align_up(o_face + sizeof(unsigned long long) * (n + 1));
     for (int v = 0; v < 2; ++v) { o_ts[v] = at; at = align_up(at + sizeof(int) * L.tile_slot[v].size() + 1); }
     for (int v = 0; v < 2; ++v) { o_to[v] = at; at = align_up(at + sizeof(long long) * L.tile_off[v].size()); }
     const size_t total = at;
@@ -323,7 +314,6 @@ int upload_table(dcb_context* h, const BatchLayout& L, cudaStream_t s, TableView
     std::memcpy(hb + o_slots, L.slots.data(), sizeof(GridSlot) * n);
     std::memcpy(hb + o_seg, L.seg_off.data(), sizeof(long long) * (n + 1));
     std::memcpy(hb + o_col, L.col_off.data(), sizeof(long long) * (n + 1));
-    std::memcpy(hb + o_chunk, L.chunk_off.data(), sizeof(long long) * (n + 1));
     for (int v = 0; v < 2; ++v) {
         std::memcpy(hb + o_ts[v], L.tile_slot[v].data(), sizeof(int) * L.tile_slot[v].size());
         std::memcpy(hb + o_to[v], L.tile_off[v].data(), sizeof(long long) * L.tile_off[v].size());
@@ -335,7 +325,6 @@ int upload_table(dcb_context* h, const BatchLayout& L, cudaStream_t s, TableView
     T.B.n = n;
     T.B.seg_off = reinterpret_cast<const long long*>(db + o_seg);
     T.B.col_off = reinterpret_cast<const long long*>(db + o_col);
-    T.B.chunk_off = reinterpret_cast<const long long*>(db + o_chunk);
     T.vert_off = reinterpret_cast<unsigned long long*>(db + o_vert);
     T.face_off = reinterpret_cast<unsigned long long*>(db + o_face);
     T.B.vert_off = T.vert_off;
@@ -355,8 +344,7 @@ int launch_marks(dcb_context* h, const BatchLayout& L, const TableView& T, cudaS
         mp.B = T.B; mp.tile_slot = T.tile_slot[v]; mp.tile_off = T.tile_off[v];
         mp.m = (int)L.tile_slot[v].size(); mp.ntiles = L.tile_off[v].back();
         mp.bits = as<uint32_t>(h->bits); mp.seg_count = as<uint32_t>(h->seg_count);
-        // the band kernel's tile map, when the workspace holds one for this layout
-        mp.tilemap = h->tilemap.bytes >= sizeof(uint32_t) * (size_t)L.nchunk ? as<uint32_t>(h->tilemap) : nullptr;
+        mp.nonfinite = h->counters.p ? &as<Counters>(h->counters)->nonfinite : nullptr;
         DCB_TRY(h, launch_mark(mp, v ? mark_narrow_tile_words() : mark_tile_words(), s), "launch mark");
     }
     return DCB_OK;
@@ -378,7 +366,6 @@ int batch_prepare(dcb_context* h, const dcb_grid* in, int n, cudaStream_t s, Bat
     DCB_TRY(h, ensure(h->seg_count, sizeof(uint32_t) * nseg), "alloc segment counts");
     DCB_TRY(h, ensure(h->seg_start, sizeof(uint32_t) * nseg), "alloc segment starts");
     DCB_TRY(h, ensure(h->counters, sizeof(Counters)), "alloc counters");
-    DCB_TRY(h, ensure(h->tilemap, sizeof(uint32_t) * std::max(1LL, L.nchunk)), "alloc tile map");
     DCB_TRY(h, ensure(h->col_count, sizeof(uint32_t) * ncol), "alloc column counts");
     DCB_TRY(h, ensure(h->col_fill, sizeof(uint32_t) * ncol), "alloc column fill");
     DCB_TRY(h, ensure(h->col_start, sizeof(uint32_t) * ncol), "alloc column starts");
@@ -395,6 +382,7 @@ int batch_prepare(dcb_context* h, const dcb_grid* in, int n, cudaStream_t s, Bat
 int batch_alloc(dcb_context* h, int n, long long cap, const dcb_opts* o, TableView& T) {
     DCB_TRY(h, ensure(h->list, sizeof(uint64_t) * cap), "alloc active list");
     DCB_TRY(h, ensure(h->V, sizeof(float) * 3 * cap), "alloc vertices");
+    DCB_TRY(h, ensure(h->fmask, cap), "alloc face masks");
     DCB_TRY(h, ensure(h->vclass, cap), "alloc vertex classes");
     DCB_TRY(h, ensure(h->esc_list, sizeof(uint32_t) * cap), "alloc escalation list");
     DCB_TRY(h, ensure(h->hard_list, sizeof(uint32_t) * cap), "alloc hard list");
@@ -403,7 +391,6 @@ int batch_alloc(dcb_context* h, int n, long long cap, const dcb_opts* o, TableVi
     DCB_TRY(h, ensure(h->stage_key, sizeof(uint2) * 3 * cap), "alloc face keys");
     DCB_TRY(h, ensure(h->faces, sizeof(int4) * 3 * cap), "alloc faces");
     DCB_TRY(h, ensure(h->v64_index, sizeof(int) * cap), "alloc fp64 index");
-    DCB_TRY(h, ensure(h->face_grad, sizeof(float4) * 3 * cap), "alloc staged face gradients");
     if (n > 1) {
         DCB_TRY(h, ensure(h->cell_slot, sizeof(uint32_t) * cap), "alloc vertex grids");
         T.B.cell_slot = as<uint32_t>(h->cell_slot);
@@ -426,7 +413,6 @@ int batch_alloc(dcb_context* h, int n, long long cap, const dcb_opts* o, TableVi
 int batch_mark(dcb_context* h, const BatchLayout& L, const TableView& T, cudaStream_t s, bool events) {
     Counters* dc = as<Counters>(h->counters);
     DCB_TRY(h, cudaMemsetAsync(h->counters.p, 0, sizeof(Counters), s), "memset counters");
-    DCB_TRY(h, cudaMemsetAsync(h->tilemap.p, 0, sizeof(uint32_t) * std::max(1LL, L.nchunk), s), "memset tile map");
     int rc = launch_marks(h, L, T, s);
     if (rc != DCB_OK) return rc;
     if (events) DCB_TRY(h, cudaEventRecord(h->ev[6], s), "event");
@@ -456,54 +442,13 @@ void batch_state(dcb_context* h, const BatchLayout& L, int n, const dcb_opts* o,
     for (int b = 0; b <= n; ++b) h->vert_offsets[b] = (int64_t)h_vert_off[b];
 }
 
-// The vertex outputs and solve lists of a batch of up to `cap` active cells.
-QefParams qef_params(dcb_context* h, const TableView& T, const dcb_opts* o, long long cap,
-                     const unsigned long long* live) {
-    Counters* dc = as<Counters>(h->counters);
-    QefParams qp;
-    qp.B = T.B; qp.list = as<uint64_t>(h->list); qp.nactive = cap; qp.live = live;
-    qp.V = as<float>(h->V); qp.vclass = as<uint8_t>(h->vclass);
-    qp.esc_list = as<uint32_t>(h->esc_list); qp.esc_count = &dc->esc_count;
-    qp.hard_list = as<uint32_t>(h->hard_list); qp.hard_data = as<float4>(h->hard_data); qp.hard_count = &dc->hard_count;
-    qp.rank_hist = dc->rank_hist;
-    qp.err = &dc->err;
-    qp.thr = (float)o->svd_threshold; qp.band = (float)o->fp64_threshold_band;
-    qp.cond_max = (float)std::min(o->fp64_escalation_cond, 3.0e38); qp.force64 = o->force_fp64;
-    return qp;
-}
-
-// The band kernel's parameters for a batch of up to `cap` active cells (qp: the vertex
-// outputs and lists it shares with the Jacobi pass).
-BandParams band_params(dcb_context* h, const BatchLayout& L, const TableView& T, const QefParams& qp, long long cap,
-                       const unsigned long long* live) {
-    Counters* dc = as<Counters>(h->counters);
-    BandParams bp;
-    bp.B = T.B;
-    bp.bits = as<uint32_t>(h->bits); bp.seg_start = as<uint32_t>(h->seg_start); bp.super = as<uint32_t>(h->super);
-    bp.list = as<uint64_t>(h->list);
-    bp.cell_slot = L.slots.size() > 1 ? as<uint32_t>(h->cell_slot) : nullptr;
-    bp.tilemap = as<uint32_t>(h->tilemap);
-    bp.nchunks = L.nchunk;
-    bp.ctas_per_sm = h->tune_band_ctas;
-    bp.chunk_next = &dc->band_chunk;
-    bp.V = qp.V; bp.vclass = qp.vclass; bp.col_count = as<uint32_t>(h->col_count);
-    bp.esc_list = qp.esc_list; bp.esc_count = qp.esc_count;
-    bp.hard_list = qp.hard_list; bp.hard_data = qp.hard_data; bp.hard_count = qp.hard_count;
-    bp.rank_hist = qp.rank_hist;
-    bp.face_cells = as<int4>(h->faces); bp.face_grad = as<float4>(h->face_grad);
-    bp.face_count = &dc->face_staged; bp.face_cap = (unsigned long long)(3 * cap); bp.nv = cap; bp.live = live;
-    bp.err = &dc->err;
-    bp.thr = qp.thr; bp.band = qp.band; bp.force64 = qp.force64;
-    return bp;
-}
-
 // Everything after the mark for up to `cap` active cells: ranks and list, vertices, faces.
 // With `live` (a device count, as in a captured graph) the kernels take the active count from
 // there, bounded by cap; otherwise it is cap.
 int batch_rest(dcb_context* h, const BatchLayout& L, TableView& T, const dcb_opts* o, cudaStream_t s, long long cap,
                const unsigned long long* live, bool events) {
     const int n = (int)L.slots.size();
-    const long long ncol = L.ncol;
+    const long long nseg = L.nseg, ncol = L.ncol;
     Counters* dc = as<Counters>(h->counters);
     const long long wind_cap = std::min(0x7fffffffLL, 3 * cap);
     const long long v64_cap = cap;
@@ -511,53 +456,65 @@ int batch_rest(dcb_context* h, const BatchLayout& L, TableView& T, const dcb_opt
     DCB_TRY(h, cudaMemsetAsync(h->col_fill.p, 0, sizeof(uint32_t) * ncol, s), "memset");
     DCB_TRY(h, cudaMemsetAsync(h->v64_index.p, 0xff, sizeof(int) * cap, s), "memset");
 
-    // 2) the tile band kernel over the tiles of every grid of the batch: ranks, the active-cell
-    //    list, vertices (rank-1 certified in FP32; Jacobi list; FP64 list) and staged faces
-    //    from shared-memory stencils; then the Jacobi and FP64 vertices.
-    uint64_t* const list = as<uint64_t>(h->list);
-    const QefParams qp = qef_params(h, T, o, cap, live);
-    const BandParams bp = band_params(h, L, T, qp, cap, live);
-    DCB_TRY(h, launch_band(bp, h->num_sms, s), "launch band");
+    // 2) ranks + list, QEF with fused edge normals (rank-1 fast path, Jacobi list, FP64).
+    ExpandParams xp;
+    xp.B = T.B; xp.nseg = nseg; xp.bits = as<uint32_t>(h->bits); xp.seg_count = as<uint32_t>(h->seg_count);
+    xp.seg_start = as<uint32_t>(h->seg_start); xp.super = as<uint32_t>(h->super); xp.list = as<uint64_t>(h->list);
+    xp.cell_slot = n > 1 ? as<uint32_t>(h->cell_slot) : nullptr;
+    xp.B.cell_slot = nullptr;                      // expand finds grids by segment
+    xp.list_cap = cap;
+    DCB_TRY(h, launch_expand(xp, h->num_sms, s), "launch expand");
+    QefParams qp;
+    qp.B = T.B; qp.list = xp.list; qp.nactive = cap; qp.live = live; qp.V = as<float>(h->V); qp.vclass = as<uint8_t>(h->vclass);
+    qp.fmask = as<uint8_t>(h->fmask); qp.col_count = as<uint32_t>(h->col_count);
+    qp.esc_list = as<uint32_t>(h->esc_list); qp.esc_count = &dc->esc_count;
+    qp.hard_list = as<uint32_t>(h->hard_list); qp.hard_data = as<float4>(h->hard_data); qp.hard_count = &dc->hard_count;
+    qp.rank_hist = dc->rank_hist;
+    qp.err = &dc->err;
+    qp.nonfinite = &dc->nonfinite;
+    qp.thr = (float)o->svd_threshold; qp.band = (float)o->fp64_threshold_band;
+    qp.cond_max = (float)std::min(o->fp64_escalation_cond, 3.0e38); qp.force64 = o->force_fp64;
+    DCB_TRY(h, launch_cell_qef(qp, h->num_sms, s), "launch qef");
     DCB_TRY(h, launch_cell_jacobi(qp, cap, h->num_sms, s), "launch jacobi");
     Vertex64Params v64;
-    v64.B = T.B; v64.list = list; v64.cells = qp.esc_list; v64.count = &dc->esc_count; v64.cap = (unsigned int)cap;
+    v64.B = T.B; v64.list = xp.list; v64.cells = qp.esc_list; v64.count = &dc->esc_count; v64.cap = (unsigned int)cap;
     v64.Vf = qp.V; v64.vclass = qp.vclass; v64.V64 = nullptr; v64.thr = o->svd_threshold;
     DCB_TRY(h, launch_vertex_fp64(v64, cap, h->num_sms, s), "launch vertex fp64");
     if (events) DCB_TRY(h, cudaEventRecord(h->ev[3], s), "event");
-    // the faces were counted per column by the band kernel
+    // the faces were counted per column by k_cell_qef
     if (events) DCB_TRY(h, cudaEventRecord(h->ev[8], s), "event");
 
-    // 3) faces: column scan, placement with the FP32 winding, FP64 re-decisions, in-column order.
-    uint32_t* const col_start = as<uint32_t>(h->col_start);
-    DCB_TRY(h, launch_scan(as<uint32_t>(h->col_count), ncol, as<uint32_t>(h->partials), col_start,
-                           &dc->face_total, s), "launch scan");
+    // 3) faces: column scan, scatter with FP32 winding, FP64 re-decisions, in-column order.
+    DCB_TRY(h, launch_scan(as<uint32_t>(h->col_count), ncol, as<uint32_t>(h->partials),
+                           as<uint32_t>(h->col_start), &dc->face_total, s), "launch scan");
     if (events) {
         DCB_TRY(h, cudaEventRecord(h->ev[9], s), "event");
         h->substage_events = true;
     }
     if (n > 1)
-        DCB_TRY(h, launch_face_offsets(T.B, col_start, &dc->face_total, T.face_off, s), "face offsets");
-    FacePlaceParams pp;
-    pp.B = T.B; pp.list = list;
-    pp.face_cells = as<int4>(h->faces); pp.face_grad = as<float4>(h->face_grad);
-    pp.face_count = &dc->face_staged; pp.face_cap = (unsigned long long)(3 * cap); pp.nv = cap;
-    pp.V = qp.V; pp.vclass = qp.vclass;
-    pp.col_start = col_start; pp.col_fill = as<uint32_t>(h->col_fill);
-    pp.stage_quad = as<int4>(h->stage_quad); pp.stage_key = as<uint2>(h->stage_key);
-    pp.wind_items = as<uint4>(h->wind_items); pp.wind_count = &dc->wind_count; pp.wind_cap = (unsigned long long)wind_cap;
-    pp.v64_index = as<int>(h->v64_index); pp.v64_cells = as<uint32_t>(h->v64_cells);
-    pp.v64_count = &dc->v64_count; pp.v64_cap = (unsigned long long)v64_cap;
-    pp.err = &dc->err;
-    DCB_TRY(h, launch_face_place(pp, 3 * cap, h->num_sms, s), "launch face placement");
+        DCB_TRY(h, launch_face_offsets(T.B, as<uint32_t>(h->col_start), &dc->face_total, T.face_off, s), "face offsets");
+    FaceParams fp;
+    fp.B = T.B; fp.list = xp.list; fp.nactive = cap; fp.live = live; fp.fmask = qp.fmask; fp.V = qp.V; fp.vclass = qp.vclass;
+    fp.bits = xp.bits; fp.super = xp.super;
+    fp.col_start = as<uint32_t>(h->col_start); fp.col_count = as<uint32_t>(h->col_count);
+    fp.col_fill = as<uint32_t>(h->col_fill);
+    fp.stage_quad = as<int4>(h->stage_quad); fp.stage_key = as<uint2>(h->stage_key);
+    fp.wind_items = as<uint4>(h->wind_items); fp.wind_count = &dc->wind_count;
+    fp.wind_cap = (unsigned long long)wind_cap;
+    fp.v64_index = as<int>(h->v64_index); fp.v64_cells = as<uint32_t>(h->v64_cells);
+    fp.v64_count = &dc->v64_count; fp.v64_cap = (unsigned long long)v64_cap;
+    fp.err = &dc->err;
+    fp.hmax = L.hmax;
+    DCB_TRY(h, launch_face_scatter(fp, h->num_sms, s), "launch face scatter");
     Vertex64Params w64;
-    w64.B = T.B; w64.list = list; w64.cells = pp.v64_cells; w64.count = pp.v64_count; w64.cap = (unsigned int)v64_cap;
+    w64.B = T.B; w64.list = xp.list; w64.cells = fp.v64_cells; w64.count = fp.v64_count; w64.cap = (unsigned int)v64_cap;
     w64.Vf = nullptr; w64.vclass = nullptr; w64.V64 = as<double>(h->V64); w64.thr = o->svd_threshold;
     DCB_TRY(h, launch_vertex_fp64(w64, v64_cap, h->num_sms, s), "launch fp64 vertices for windings");
     Winding64Params wp;
-    wp.B = T.B; wp.items = pp.wind_items; wp.count = pp.wind_count; wp.cap = (unsigned int)wind_cap;
-    wp.quads = pp.stage_quad; wp.v64_index = pp.v64_index; wp.V64 = w64.V64; wp.err = &dc->err;
+    wp.B = T.B; wp.items = fp.wind_items; wp.count = fp.wind_count; wp.cap = (unsigned int)wind_cap;
+    wp.quads = fp.stage_quad; wp.v64_index = fp.v64_index; wp.V64 = w64.V64; wp.err = &dc->err;
     DCB_TRY(h, launch_winding_fp64(wp, wind_cap, h->num_sms, s), "launch winding fp64");
-    DCB_TRY(h, launch_face_order(pp.stage_quad, pp.stage_key, col_start, as<uint32_t>(h->col_count), &dc->face_total,
+    DCB_TRY(h, launch_face_order(fp.stage_quad, fp.stage_key, fp.col_start, fp.col_count, &dc->face_total,
                                  as<int4>(h->faces), 3 * cap, h->num_sms, s), "launch face order");
     if (o->emit_triangles) {
         // 4) quads -> triangles; FP64 vertices for the quads FP32 cannot orient (the winding
@@ -565,15 +522,15 @@ int batch_rest(dcb_context* h, const BatchLayout& L, TableView& T, const dcb_opt
         TriParams tp;
         tp.B = T.B;
         tp.quads = as<int4>(h->faces); tp.nquads = &dc->face_total; tp.V = qp.V; tp.vclass = qp.vclass;
-        tp.hmax = L.hmax; tp.tris = as<int>(h->tris); tp.items = as<uint32_t>(h->tri_items);
+        tp.hmax = fp.hmax; tp.tris = as<int>(h->tris); tp.items = as<uint32_t>(h->tri_items);
         tp.item_count = &dc->tri_count; tp.item_cap = (unsigned int)wind_cap;
-        tp.v64_index = pp.v64_index; tp.v64_cells = pp.v64_cells; tp.v64_count = pp.v64_count;
-        tp.v64_cap = pp.v64_cap; tp.err = &dc->err;
+        tp.v64_index = fp.v64_index; tp.v64_cells = fp.v64_cells; tp.v64_count = fp.v64_count;
+        tp.v64_cap = fp.v64_cap; tp.err = &dc->err;
         DCB_TRY(h, launch_triangulate(tp, 3 * cap, h->num_sms, s), "launch triangulate");
         DCB_TRY(h, launch_vertex_fp64(w64, v64_cap, h->num_sms, s), "launch fp64 vertices for triangles");
         Tri64Params t64;
         t64.quads = tp.quads; t64.items = tp.items; t64.count = tp.item_count; t64.cap = tp.item_cap;
-        t64.v64_index = pp.v64_index; t64.V64 = w64.V64; t64.tris = tp.tris; t64.err = &dc->err;
+        t64.v64_index = fp.v64_index; t64.V64 = w64.V64; t64.tris = tp.tris; t64.err = &dc->err;
         DCB_TRY(h, launch_tri_fp64(t64, wind_cap, h->num_sms, s), "launch triangle fp64");
     }
     if (n > 1) {
@@ -1146,10 +1103,10 @@ int dcb_destroy(dcb_handle h) {
     if (!h) return DCB_ERR_INVALID_ARGUMENT;
     cudaSetDevice(h->device);
     DevBuf* bufs[] = {&h->grid, &h->bits, &h->super, &h->list, &h->seg_count, &h->seg_start, &h->counters,
-                      &h->V, &h->vclass, &h->col_count, &h->col_fill, &h->col_start,
+                      &h->V, &h->vclass, &h->fmask, &h->col_count, &h->col_fill, &h->col_start,
                       &h->partials, &h->esc_list, &h->hard_list, &h->hard_data, &h->stage_quad,
                       &h->stage_key, &h->faces, &h->wind_items, &h->v64_index, &h->v64_cells, &h->V64,
-                      &h->tris, &h->tri_items, &h->face_grad, &h->tilemap, &h->m_verts, &h->m_faces, &h->m_out, &h->m_tris,
+                      &h->tris, &h->tri_items, &h->m_verts, &h->m_faces, &h->m_out, &h->m_tris,
                       &h->m_bin_count, &h->m_bin_start, &h->m_bin_fill, &h->m_bin_scratch, &h->m_bin_tris,
                       &h->m_bin_active, &h->m_active_list, &h->m_axis_start, &h->m_far, &h->m_ext, &h->m_tmp,
                       &h->m_partials, &h->m_counters, &h->m_vox, &h->table, &h->cell_slot, &h->adj_rows, &h->adj_owners, &h->ours_ws,
@@ -1488,7 +1445,6 @@ int dcb_autotune_mark(dcb_handle h, const dcb_grid* grids, int n, int* waves_out
                 if (rc == DCB_OK) {
                     DCB_TRY(h, ensure(h->bits, sizeof(uint32_t) * L.bits), "alloc bits");
                     DCB_TRY(h, ensure(h->seg_count, sizeof(uint32_t) * L.nseg), "alloc segment counts");
-                    DCB_TRY(h, ensure(h->tilemap, sizeof(uint32_t) * std::max(1LL, L.nchunk)), "alloc tile map");
                     float ms[3];
                     for (int r = 0; r < 4 && rc == DCB_OK; ++r) {       // one warm-up, three timed
                         DCB_TRY(h, cudaEventRecord(h->ev[0], s), "event");
@@ -1510,63 +1466,6 @@ int dcb_autotune_mark(dcb_handle h, const dcb_grid* grids, int n, int* waves_out
     h->tune_narrow_cells = best_n;
     if (waves_out) *waves_out = best_w;
     if (narrow_cells_out) *narrow_cells_out = best_n;
-    if (best_ms_out) *best_ms_out = best;
-    return DCB_OK;
-}
-
-int dcb_autotune_band(dcb_handle h, const dcb_grid* grids, int n, int* ctas_per_sm_out, float* best_ms_out,
-                      void* cuda_stream) {
-    if (h) ++h->gen;                        // reuses the extraction workspace
-    if (!h) return DCB_ERR_INVALID_ARGUMENT;
-    if (!grids || n < 1) return fail(h, DCB_ERR_INVALID_ARGUMENT, "empty batch");
-    for (int b = 0; b < n; ++b) {
-        const int rc = validate(h, grids + b);
-        if (rc != DCB_OK) return rc;
-    }
-    if (cudaSetDevice(h->device) != cudaSuccess) { cudaGetLastError(); return fail(h, DCB_ERR_CUDA, "set device"); }
-    cudaStream_t s = reinterpret_cast<cudaStream_t>(cuda_stream);
-    BatchLayout L;
-    TableView T;
-    int rc = batch_prepare(h, grids, n, s, L, T);
-    if (rc != DCB_OK) return rc;
-    rc = batch_mark(h, L, T, s, false);
-    if (rc != DCB_OK) return rc;
-    Counters* dc = as<Counters>(h->counters);
-    Counters* hc = reinterpret_cast<Counters*>(h->h_counters);
-    DCB_TRY(h, cudaMemcpyAsync(hc, dc, sizeof(Counters), cudaMemcpyDeviceToHost, s), "read count");
-    DCB_TRY(h, cudaStreamSynchronize(s), "mark");
-    const long long nv = (long long)hc->total_active;
-    const int keep = h->tune_band_ctas;
-    int best_w = keep;
-    float best = 0.f;
-    if (nv > 0 && nv < 0x7fffffffLL) {
-        dcb_opts od;
-        dcb_default_opts(&od);
-        rc = batch_alloc(h, n, nv, &od, T);
-        if (rc != DCB_OK) return rc;
-        const QefParams qp = qef_params(h, T, &od, nv, nullptr);
-        const int maxw = band_max_ctas_per_sm();
-        best = 1e30f;
-        for (int w = 1; w <= maxw; ++w) {
-            h->tune_band_ctas = w;
-            const BandParams bp = band_params(h, L, T, qp, nv, nullptr);
-            float ms[3];
-            for (int r = 0; r < 4; ++r) {                    // one warm-up, three timed
-                // the band kernel's counters (work queue, lists, staged faces) start at zero
-                DCB_TRY(h, cudaMemsetAsync(h->counters.p, 0, sizeof(Counters), s), "memset counters");
-                DCB_TRY(h, cudaEventRecord(h->ev[0], s), "event");
-                const cudaError_t e = launch_band(bp, h->num_sms, s);
-                if (e != cudaSuccess) { h->tune_band_ctas = keep; return cuda_fail(h, e, "launch band"); }
-                DCB_TRY(h, cudaEventRecord(h->ev[1], s), "event");
-                DCB_TRY(h, cudaEventSynchronize(h->ev[1]), "autotune");
-                if (r > 0) ms[r - 1] = elapsed(h->ev[0], h->ev[1]);
-            }
-            std::sort(ms, ms + 3);
-            if (ms[1] < best) { best = ms[1]; best_w = w; }
-        }
-    }
-    h->tune_band_ctas = best_w;
-    if (ctas_per_sm_out) *ctas_per_sm_out = best_w;
     if (best_ms_out) *best_ms_out = best;
     return DCB_OK;
 }

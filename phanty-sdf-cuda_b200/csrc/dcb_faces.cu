@@ -103,7 +103,28 @@ cudaError_t launch_scan(const uint32_t* in, long long n, uint32_t* partials, uin
 
 long long scan_partials_len(long long n) { return (n + kScanTile - 1) / kScanTile; }
 
-// ---- shared helpers of the face kernels ---------------------------------------------
+// ---- face scatter ----------------------------------------------------------------------
+
+constexpr int kFaceThreads = 128;
+
+
+// gradientAt (contouring.cpp:141-207) in FP32 (orientation tests only: a 2-ulp quotient is
+// far inside the uncertainty margin, and uncertain faces are re-decided in FP64).
+__device__ __forceinline__ float3 grid_gradient32(const GridDesc& g, int i, int j, int k) {
+    const int im = max(i - 1, 0), ip = min(i + 1, g.nx - 1);
+    const int jm = max(j - 1, 0), jp = min(j + 1, g.ny - 1);
+    const int km = max(k - 1, 0), kp = min(k + 1, g.nz - 1);
+    float3 o = make_float3(0.f, 0.f, 0.f);
+    const float dx = pos_axis(g.ox, g.vx, ip) - pos_axis(g.ox, g.vx, im);
+    if (fabsf(dx) > 1e-12f) o.x = __fdividef(__ldg(g.v + pidx(g, ip, j, k)) - __ldg(g.v + pidx(g, im, j, k)), dx);
+    const float dy = pos_axis(g.oy, g.vy, jp) - pos_axis(g.oy, g.vy, jm);
+    if (fabsf(dy) > 1e-12f) o.y = __fdividef(__ldg(g.v + pidx(g, i, jp, k)) - __ldg(g.v + pidx(g, i, jm, k)), dy);
+    const float dz = pos_axis(g.oz, g.vz, kp) - pos_axis(g.oz, g.vz, km);
+    if (fabsf(dz) > 1e-12f) o.z = __fdividef(__ldg(g.v + pidx(g, i, j, kp)) - __ldg(g.v + pidx(g, i, j, km)), dz);
+    const float n2 = o.x * o.x + o.y * o.y + o.z * o.z;
+    if (n2 > 0.f) { const float r = rsqrtf(n2); o.x *= r; o.y *= r; o.z *= r; }
+    return o;
+}
 
 __device__ __forceinline__ float3 ldv(const float* V, uint32_t r) {
     return make_float3(__ldg(V + 3 * (size_t)r), __ldg(V + 3 * (size_t)r + 1), __ldg(V + 3 * (size_t)r + 2));
@@ -145,70 +166,133 @@ __device__ __forceinline__ void request_fp64_vertex(int* v64_index, uint32_t* v6
     }
 }
 
-// ---- placement of the faces staged by the tile band kernel -------------------------------
-
-// Thread per staged face (its four cells' ranks in the CPU corner order and the summed
-// gradientAt of its edge's endpoints): the FP32 winding test with its error bound, exactly
-// as emit_face decides it, and the face's slot in its column; uncertain faces are listed for
-// the FP64 re-decision.
+// One face of cell (i,j,k) (rank r) along `axis`: its four cells' ranks, the FP32 winding test
+// with its error bound, the staging slot in its column, and for an uncertain face the FP64
+// work items.
 template <bool ONE>
-__global__ void __launch_bounds__(256)
-k_face_place(const __grid_constant__ FacePlaceParams P) {
-    const long long nf = min((long long)*P.face_count, (long long)P.face_cap);
-    for (long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x; f < nf;
-         f += (long long)gridDim.x * blockDim.x) {
-        const int4 q = P.face_cells[f];
-        const float4 gg = P.face_grad[f];
-        const uint32_t col = __float_as_uint(gg.w);               // column of the whole batch
-        const int gi = ONE ? 0 : slot_of_column(P.B, (long long)col);
-        const GridSlot& S = slot_ref<ONE>(P.B, gi);
-        const long long cxcy = (long long)S.g.cx * S.g.cy;
-        const int axis = (int)(((long long)col - S.col_off) / cxcy);
-        const uint32_t r0 = (uint32_t)q.x, r1 = (uint32_t)q.y, r2 = (uint32_t)q.z, r3 = (uint32_t)q.w;
-        if ((long long)max(max(r0, r1), max(r2, r3)) >= P.nv || axis > 2) { set_error(P.err, kErrInternal); continue; }
-        const uint64_t pk = __ldg(reinterpret_cast<const unsigned long long*>(P.list) + r2);
-        const uint32_t k = (uint32_t)(pk >> 42);
-        const float3 gn = make_float3(gg.x, gg.y, gg.z);
-        const float3 pa = ldv(P.V, r0), pb = ldv(P.V, r1), pc = ldv(P.V, r2), pd = ldv(P.V, r3);
-        const float dv = quad_vertex_bound(P.vclass, r0, r1, r2, r3, pa, pb, pc, pd, S.hmax);
-        const float3 ba = sub3(pb, pa), da = sub3(pd, pa), ca = sub3(pc, pa);
-        float3 qn = cross3(ba, da);
-        float qn2 = dot3(qn, qn);
-        const float lb = sqrtf(dot3(ba, ba)), ld = sqrtf(dot3(da, da)), lc = sqrtf(dot3(ca, ca));
-        float dq = 2.f * dv * (lb + ld + 2.f * dv);
-        const float qnl0 = sqrtf(qn2);
-        const bool near_fallback = (qnl0 - dq) < 1e-12f && (qnl0 + dq) >= 1e-12f;
-        if (qn2 < 1e-24f) { qn = cross3(ca, da); qn2 = dot3(qn, qn); dq = 2.f * dv * (lc + ld + 2.f * dv); }
-        const float gn2 = dot3(gn, gn);
-        const float d = dot3(qn, gn);
-        const float qnl = sqrtf(qn2), gnl = sqrtf(gn2);
-        const bool uncertain = near_fallback || gn2 < 1e-4f ||
-                               fabsf(d) <= 4.f * dq * gnl + 1e-5f * qnl * gnl;
-        const bool swap = !uncertain && gn2 > 0.f && qn2 > 0.f && d < 0.f;
-        const uint32_t slot = P.col_start[col] + atomicAdd(&P.col_fill[col], 1u);
-        if ((unsigned long long)slot >= P.face_cap) { set_error(P.err, kErrInternal); continue; }
-        P.stage_quad[slot] = swap ? make_int4((int)r0, (int)r3, (int)r2, (int)r1)
-                                  : make_int4((int)r0, (int)r1, (int)r2, (int)r3);
-        P.stage_key[slot] = make_uint2(k, col);
-        if (uncertain) {
-            const unsigned int w = atomicAdd(P.wind_count, 1u);
-            if (w < P.wind_cap) P.wind_items[w] = make_uint4(slot, (uint32_t)axis | ((uint32_t)gi << 2), (uint32_t)pk, (uint32_t)(pk >> 32));
-            else set_error(P.err, kErrOverflow);
-            const uint32_t rq[4] = {r0, r1, r2, r3};
-#pragma unroll
-            for (int t = 0; t < 4; ++t)
-                request_fp64_vertex(P.v64_index, P.v64_cells, P.v64_count, P.v64_cap, P.err, rq[t]);
+__device__ __forceinline__ void emit_face(const FaceParams& P, int gi, int i, int j, int k, uint32_t r, int axis,
+                                          float3 g0, uint32_t r_k1, uint32_t r_j1, uint32_t r_jk) {
+    const GridSlot& S = slot_ref<ONE>(P.B, gi);
+    const GridDesc& g = S.g;
+    const long long cxcy = (long long)g.cx * g.cy;
+    uint32_t r0, r1, r3;
+    if (axis == 0) { r0 = r_jk; r1 = r_k1; r3 = r_j1; }                // (i,j-1,k-1) (i,j,k-1) (i,j-1,k)
+    else if (axis == 1) { r0 = r_k1 - 1u; r1 = r_k1; r3 = r - 1u; }    // (i-1,j,k-1) (i,j,k-1) (i-1,j,k)
+    else { r0 = r_j1 - 1u; r1 = r_j1; r3 = r - 1u; }                   // (i-1,j-1,k) (i,j-1,k) (i-1,j,k)
+    const uint32_t r2 = r;
+    const float3 g1 = grid_gradient32(g, i + (axis == 0), j + (axis == 1), k + (axis == 2));
+    const float3 gn = make_float3(g0.x + g1.x, g0.y + g1.y, g0.z + g1.z);
+    const float3 pa = ldv(P.V, r0), pb = ldv(P.V, r1), pc = ldv(P.V, r2), pd = ldv(P.V, r3);
+    const float dv = quad_vertex_bound(P.vclass, r0, r1, r2, r3, pa, pb, pc, pd, S.hmax);
+    const float3 ba = sub3(pb, pa), da = sub3(pd, pa), ca = sub3(pc, pa);
+    float3 qn = cross3(ba, da);
+    float qn2 = dot3(qn, qn);
+    // |qn| error bound of the FP32 cross product from the vertex bounds
+    const float lb = sqrtf(dot3(ba, ba)), ld = sqrtf(dot3(da, da)), lc = sqrtf(dot3(ca, ca));
+    float dq = 2.f * dv * (lb + ld + 2.f * dv);
+    // The reference switches to the other diagonal below |qn|^2 = 1e-24 (absolute):
+    // decide in FP64 whenever the bound straddles that switch.
+    const float qnl0 = sqrtf(qn2);
+    const bool near_fallback = (qnl0 - dq) < 1e-12f && (qnl0 + dq) >= 1e-12f;
+    if (qn2 < 1e-24f) { qn = cross3(ca, da); qn2 = dot3(qn, qn); dq = 2.f * dv * (lc + ld + 2.f * dv); }
+    const float gn2 = dot3(gn, gn);
+    const float d = dot3(qn, gn);
+    const float qnl = sqrtf(qn2), gnl = sqrtf(gn2);
+    // gradient sum: FP32 quotients and normalisation, ~1e-6 relative
+    const bool uncertain = near_fallback || gn2 < 1e-4f ||
+                           fabsf(d) <= 4.f * dq * gnl + 1e-5f * qnl * gnl;
+    bool swap = !uncertain && gn2 > 0.f && qn2 > 0.f && d < 0.f;
+    const long long col = S.col_off + axis * cxcy + (long long)i * g.cy + j;
+    const uint32_t slot = P.col_start[col] + atomicAdd(&P.col_fill[col], 1u);
+    P.stage_quad[slot] = swap ? make_int4((int)r0, (int)r3, (int)r2, (int)r1)
+                              : make_int4((int)r0, (int)r1, (int)r2, (int)r3);
+    P.stage_key[slot] = make_uint2((uint32_t)k, (uint32_t)col);
+    if (uncertain) {
+        const unsigned int w = atomicAdd(P.wind_count, 1u);
+        if (w < P.wind_cap) {
+            const uint64_t pk = pack_cell(i, j, k);
+            P.wind_items[w] = make_uint4(slot, (uint32_t)axis | ((uint32_t)gi << 2), (uint32_t)pk, (uint32_t)(pk >> 32));
+        } else {
+            set_error(P.err, kErrOverflow);
         }
+        // request the FP64 vertex of each of the four cells once
+        const uint32_t rq[4] = {r0, r1, r2, r3};
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            request_fp64_vertex(P.v64_index, P.v64_cells, P.v64_count, P.v64_cap, P.err, rq[q]);
     }
 }
 
-cudaError_t launch_face_place(const FacePlaceParams& P, long long max_faces, int num_sms, cudaStream_t s) {
-    if (max_faces <= 0) return cudaSuccess;
-    long long blocks = (max_faces + 255) / 256;
+// A warp takes 32 consecutive active cells. Each lane reads its cell's face mask (the cell's
+// min-corner edges with a strict sign change, contouring.cpp:609-729) and, when it owns a
+// face, the cell's gradient and the ranks of the face neighbours; then the warp's faces
+// (about one per cell) are dealt out a lane each, the owner's data passed by shuffle, so
+// the per-face work runs with the lanes full.
+template <bool ONE>
+__global__ void __launch_bounds__(kFaceThreads)
+k_face_scatter(const __grid_constant__ FaceParams P) {
+    __shared__ uint8_t s_item[kFaceThreads / 32][96];
+    const int lane = threadIdx.x & 31, wb = threadIdx.x >> 5;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    // a captured graph whose live count exceeds the capacity it was built for does nothing
+    // (the host reports the overflow after the replay)
+    const long long nact = P.live ? ((long long)*P.live > P.nactive ? 0 : (long long)*P.live) : P.nactive;
+    for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x - lane); base < nact;
+         base += stride) {                                                // warp-uniform
+        const long long rr = base + lane;
+        uint32_t fm = 0;
+        int gi = 0, i = 0, j = 0, k = 0;
+        float3 g0 = make_float3(0.f, 0.f, 0.f);
+        uint32_t r_k1 = 0xffffffffu, r_j1 = 0xffffffffu, r_jk = 0xffffffffu;
+        if (rr < nact) fm = P.fmask[rr];
+        if (fm) {
+            gi = ONE ? 0 : slot_of_rank(P.B, (unsigned long long)rr);
+            const GridSlot& S = slot_ref<ONE>(P.B, gi);
+            const uint32_t* const bits = P.bits + S.bits_off;
+            const uint32_t* const super = P.super + S.super_off;
+            unpack_cell(P.list[rr], i, j, k);
+            g0 = grid_gradient32(S.g, i, j, k);
+            // All four cells of a face are active, so a cell's x-1 neighbour in a face is the
+            // previous active cell in linear order (rank - 1).
+            if (fm & 3) r_k1 = cell_rank(bits, super, S.g, i, j, k - 1);
+            if (fm & 5) r_j1 = cell_rank(bits, super, S.g, i, j - 1, k);
+            if (fm & 1) r_jk = cell_rank(bits, super, S.g, i, j - 1, k - 1);
+        }
+        const uint32_t cnt = __popc(fm);
+        uint32_t off = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(0xffffffffu, off, o);
+            if (lane >= o) off += v;
+        }
+        const uint32_t total = __shfl_sync(0xffffffffu, off, 31);
+        off -= cnt;
+        for (uint32_t m = fm; m; m &= m - 1) s_item[wb][off++] = (uint8_t)((lane << 2) | (__ffs(m) - 1));
+        __syncwarp();
+        for (uint32_t t0 = 0; t0 < total; t0 += 32) {                     // warp-uniform
+            const uint32_t t = t0 + lane;
+            const uint32_t it = t < total ? s_item[wb][t] : 0u;
+            const int src = (int)(it >> 2), axis = (int)(it & 3);
+            const int fi = __shfl_sync(0xffffffffu, i, src), fj = __shfl_sync(0xffffffffu, j, src);
+            const int fk = __shfl_sync(0xffffffffu, k, src), fg = __shfl_sync(0xffffffffu, gi, src);
+            const float3 f0 = make_float3(__shfl_sync(0xffffffffu, g0.x, src), __shfl_sync(0xffffffffu, g0.y, src),
+                                          __shfl_sync(0xffffffffu, g0.z, src));
+            const uint32_t fk1 = __shfl_sync(0xffffffffu, r_k1, src), fj1 = __shfl_sync(0xffffffffu, r_j1, src);
+            const uint32_t fjk = __shfl_sync(0xffffffffu, r_jk, src);
+            if (t < total)
+                emit_face<ONE>(P, fg, fi, fj, fk, (uint32_t)(base + src), axis, f0, fk1, fj1, fjk);
+        }
+        __syncwarp();
+    }
+}
+
+cudaError_t launch_face_scatter(const FaceParams& P, int num_sms, cudaStream_t s) {
+    if (P.nactive <= 0) return cudaSuccess;
+    long long blocks = (P.nactive + kFaceThreads - 1) / kFaceThreads;
     const long long cap = (long long)num_sms * 16;
     if (blocks > cap) blocks = cap;
-    if (P.B.n == 1) k_face_place<true><<<(unsigned)blocks, 256, 0, s>>>(P);
-    else            k_face_place<false><<<(unsigned)blocks, 256, 0, s>>>(P);
+    if (P.B.n == 1) k_face_scatter<true><<<(unsigned)blocks, kFaceThreads, 0, s>>>(P);
+    else            k_face_scatter<false><<<(unsigned)blocks, kFaceThreads, 0, s>>>(P);
     return cudaGetLastError();
 }
 

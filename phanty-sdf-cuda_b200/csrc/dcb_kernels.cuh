@@ -22,7 +22,6 @@ struct GridSlot {
     int nzc;                       // mark: z-chunks
     int tw;                        // mark: cell words per x-tile (32, or 8 for narrow grids)
     float hmax;                    // largest cell width of the grid (world units)
-    long long chunk_off;           // first tile-band chunk (32 words x 4 rows x 4 planes)
 };
 
 struct BatchTable {
@@ -33,7 +32,6 @@ struct BatchTable {
     const long long* col_off;              // [n+1] first face column per grid
     const unsigned long long* vert_off;    // [n+1] first vertex rank per grid (after the scan)
     const uint32_t* cell_slot;             // [active] grid of every vertex rank (n > 1, after expand)
-    const long long* chunk_off;            // [n+1] first tile-band chunk per grid
 };
 
 // Largest index b in [0, n) with offs[b] <= x (offsets ascending, offs[0] = 0).
@@ -76,8 +74,7 @@ struct MarkParams {
     long long ntiles;
     uint32_t* bits;                // all grids' active bits
     uint32_t* seg_count;           // all grids' segment counts
-    uint32_t* tilemap;             // optional, zeroed before: per band chunk, bit w set when the
-                                   // chunk's 32 x 4 x 4-cell tile of word w has an active cell
+    int* nonfinite;                // optional: set to 1 when a grid value is NaN or infinite
 };
 cudaError_t launch_mark(const MarkParams& P, int tw, cudaStream_t s);
 int mark_tile_words();
@@ -120,6 +117,8 @@ struct QefParams {
                                     // nactive, nothing is processed), or null
     float* V;
     uint8_t* vclass;                // [active] VertexClass
+    uint8_t* fmask;                 // bit a: cell owns a face on its min-corner edge a
+    uint32_t* col_count;            // per grid [3][cx*cy]: col_off + a*cx*cy + i*cy + j
     uint32_t* esc_list;
     unsigned int* esc_count;
     uint32_t* hard_list;            // cells not certified rank 1
@@ -127,11 +126,14 @@ struct QefParams {
     unsigned int* hard_count;
     unsigned long long* rank_hist;  // [4]
     int* err;
+    const int* nonfinite;           // device flag: the grid holds NaN or infinite values; every
+                                    // cell then takes the FP64 path (may be null)
     float thr;
     float band;
     float cond_max;
     int force64;
 };
+cudaError_t launch_cell_qef(const QefParams& P, int num_sms, cudaStream_t s);
 cudaError_t launch_cell_jacobi(const QefParams& P, long long max_items, int num_sms, cudaStream_t s);
 
 struct Vertex64Params {
@@ -163,6 +165,33 @@ cudaError_t launch_scan(const uint32_t* in, long long n, uint32_t* partials, uin
                         unsigned long long* grand_total, cudaStream_t s);
 long long scan_partials_len(long long n);
 
+struct FaceParams {
+    BatchTable B;
+    const uint64_t* list;
+    long long nactive;             // active cells (capacity when live is set)
+    const unsigned long long* live; // device count of active cells (a captured graph; above
+                                    // nactive, nothing is processed), or null
+    const uint8_t* fmask;
+    const float* V;
+    const uint8_t* vclass;
+    const uint32_t* bits;
+    const uint32_t* super;
+    const uint32_t* col_start;     // per grid [3][cx*cy] (global column index)
+    const uint32_t* col_count;
+    uint32_t* col_fill;
+    int4* stage_quad;
+    uint2* stage_key;              // {k, column}
+    uint4* wind_items;             // {slot, axis | grid << 2, packed lo, packed hi}
+    unsigned int* wind_count;
+    unsigned long long wind_cap;
+    int* v64_index;                // [rank] -> FP64 vertex slot (-1 none, -2 being claimed)
+    uint32_t* v64_cells;           // cells whose FP64 vertex the windings need
+    unsigned int* v64_count;
+    unsigned long long v64_cap;
+    int* err;
+    float hmax;                    // unused: each grid's slot holds its own cell width
+};
+cudaError_t launch_face_scatter(const FaceParams& P, int num_sms, cudaStream_t s);
 cudaError_t launch_face_order(const int4* stage_quad, const uint2* stage_key, const uint32_t* col_start,
                               const uint32_t* col_count, const unsigned long long* nfaces, int4* faces,
                               long long max_faces, int num_sms, cudaStream_t s);
@@ -185,73 +214,6 @@ struct TriParams {
     int* err;
 };
 cudaError_t launch_triangulate(const TriParams& P, long long max_quads, int num_sms, cudaStream_t s);
-
-// ---- tile band kernel (dcb_band.cu) ----
-// Tile: one 32-cell active-bit word in each of kBandTileRows x kBandTilePlanes cell rows.
-constexpr int kBandTileRows = 4, kBandTilePlanes = 4;
-// Work unit: a chunk of up to 32 x-adjacent tiles of 32 x 4 x 4 cells (one active-bit word
-// per cell row), handed out by an atomic counter.
-struct BandParams {
-    BatchTable B;                  // the grids (B.chunk_off: first chunk of each)
-    const uint32_t* bits;          // active bits of all grids (mark)
-    const uint32_t* seg_start;     // first global rank of every mark segment (scan)
-    uint32_t* super;               // written: rank of the first active cell of every 256-cell word
-    uint64_t* list;                // written: packed cell of every rank
-    uint32_t* cell_slot;           // written (batches, may be null): grid of every rank
-    const uint32_t* tilemap;       // active tiles of every chunk (mark)
-    long long nchunks;             // all grids' chunks
-    int ctas_per_sm;               // persistent CTAs per SM (<= the occupancy limit; 0: the limit)
-    unsigned int* chunk_next;      // chunk counter, zero before the launch
-    float* V;
-    uint8_t* vclass;
-    uint32_t* col_count;           // [3][cx*cy]: a*cx*cy + i*cy + j
-    uint32_t* esc_list;
-    unsigned int* esc_count;
-    uint32_t* hard_list;
-    float4* hard_data;
-    unsigned int* hard_count;
-    unsigned long long* rank_hist;
-    int4* face_cells;              // staged faces: ranks of the four cells, CPU corner order
-    float4* face_grad;             // staged faces: gradientAt(p0) + gradientAt(p1), column in w
-    unsigned int* face_count;
-    unsigned long long face_cap;
-    long long nv;                  // active cells (vertex ranks are below it); capacity with live
-    const unsigned long long* live; // device count of active cells (a captured graph; above nv,
-                                    // nothing is processed), or null
-    int* err;
-    float thr;
-    float band;
-    int force64;
-};
-cudaError_t launch_band(const BandParams& P, int num_sms, cudaStream_t s);
-int band_max_ctas_per_sm();                           // occupancy limit of the band kernel
-long long band_chunk_count(int nx, int ny, int nz);   // band kernel work units of one grid
-
-// Staged faces -> FP32 winding decision and their slot in the column order (dcb_band.cu).
-struct FacePlaceParams {
-    BatchTable B;
-    const uint64_t* list;
-    const int4* face_cells;
-    const float4* face_grad;
-    const unsigned int* face_count;
-    unsigned long long face_cap;   // staged face entries (and stage_quad / stage_key entries)
-    long long nv;                  // vertices
-    const float* V;
-    const uint8_t* vclass;
-    const uint32_t* col_start;
-    uint32_t* col_fill;
-    int4* stage_quad;
-    uint2* stage_key;              // {k, column}
-    uint4* wind_items;             // {slot, axis, packed lo, packed hi}
-    unsigned int* wind_count;
-    unsigned long long wind_cap;
-    int* v64_index;
-    uint32_t* v64_cells;
-    unsigned int* v64_count;
-    unsigned long long v64_cap;
-    int* err;
-};
-cudaError_t launch_face_place(const FacePlaceParams& P, long long max_faces, int num_sms, cudaStream_t s);
 
 struct Tri64Params {
     const int4* quads;

@@ -57,7 +57,7 @@ __device__ __forceinline__ void load_row(const float* __restrict__ row, int x0, 
 
 // Negative / positive bit words of the loaded segment (word q covers points x0+32q..+31).
 template <int TW>
-__device__ __forceinline__ void row_words(const RowRegs<TW>& R, int lane, uint32_t* nw, uint32_t* pw) {
+__device__ __forceinline__ void row_words(const RowRegs<TW>& R, int lane, uint32_t* nw, uint32_t* pw, bool& bad) {
     constexpr int kPtWords = Tile<TW>::kPtWords;
 #pragma unroll
     for (int c = 0; c < Tile<TW>::kChunks; ++c) {
@@ -66,6 +66,7 @@ __device__ __forceinline__ void row_words(const RowRegs<TW>& R, int lane, uint32
         for (int s = 0; s < 4; ++s) {
             const int w = 4 * c + s;
             if (w >= kPtWords) break;
+            bad |= !(fabsf(q[s]) <= 3.402823466e38f);           // NaN or infinite
             const uint32_t n = __ballot_sync(0xffffffffu, q[s] < 0.f);
             const uint32_t p = __ballot_sync(0xffffffffu, q[s] > 0.f);
             if (lane == 0) { nw[w] = n; pw[w] = p; }
@@ -101,9 +102,10 @@ k_mark_zmarch(const __grid_constant__ MarkParams P) {
     const int64_t plane = (int64_t)g.nx * g.ny;
 
     RowRegs<TW> cur;
+    bool bad = false;                          // a NaN or infinite value among this lane's points
     if (loader) {
         load_row<TW>(base + (int64_t)kb * plane, x0, g.nx, lane, cur);
-        row_words<TW>(cur, lane, s_nw[kb & 1][warp], s_pw[kb & 1][warp]);
+        row_words<TW>(cur, lane, s_nw[kb & 1][warp], s_pw[kb & 1][warp], bad);
         load_row<TW>(base + (int64_t)(kb + 1) * plane, x0, g.nx, lane, cur);
     }
     const bool word_lane = TW == 32 || lane < TW;   // lanes beyond the tile's words idle
@@ -115,7 +117,7 @@ k_mark_zmarch(const __grid_constant__ MarkParams P) {
     for (int k = kb; k < ke; ++k) {
         const int p1 = (k + 1) & 1, p0 = k & 1;
         if (loader) {
-            row_words<TW>(cur, lane, s_nw[p1][warp], s_pw[p1][warp]);
+            row_words<TW>(cur, lane, s_nw[p1][warp], s_pw[p1][warp], bad);
             if (k + 2 <= ke) load_row<TW>(base + (int64_t)(k + 2) * plane, x0, g.nx, lane, cur);
         }
         __syncthreads();
@@ -132,22 +134,11 @@ k_mark_zmarch(const __grid_constant__ MarkParams P) {
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
             if (lane == 0) seg_count[row * nxt + xt] = cnt;
-            if (P.tilemap) {
-                // the band kernel's tiles: 32-cell words x 4 rows x 4 planes, in chunks of 32
-                // words; one OR per row and plane that has an active cell
-                const uint32_t any = __ballot_sync(0xffffffffu, act != 0u) & (word_lane ? 0xffffffffu : 0u);
-                const int j = j0 + r;
-                if (lane == 0 && any) {
-                    const int w0 = xt * TW;                       // first word of this x-tile
-                    const int nwx = (g.cx + 31) >> 5;
-                    const long long nxc = (nwx + 31) / 32, nyb = (g.cy + kBandTileRows - 1) / kBandTileRows;
-                    const long long chunk = S.chunk_off + (w0 >> 5) + nxc * (j / kBandTileRows + nyb * (k / kBandTilePlanes));
-                    atomicOr(P.tilemap + chunk, any << (w0 & 31));
-                }
-            }
         }
         __syncthreads();
     }
+    // the host learns that the grid holds non-finite values (their cells take the FP64 path)
+    if (__syncthreads_or(bad) && threadIdx.x == 0 && P.nonfinite) atomicOr(P.nonfinite, 1);
 }
 
 // Segments with at most this many active cells are expanded by one lane.

@@ -116,7 +116,7 @@ extern "C" int dcb_mark_active_cells_noalloc(const dcb_grid* grid, int64_t* cell
     BatchTable B;
     B.s0 = slot; B.slots = nullptr; B.n = 1; B.cell_slot = nullptr; B.seg_off = nullptr; B.col_off = nullptr; B.vert_off = nullptr;
     MarkParams mp;
-    mp.B = B; mp.tile_slot = nullptr; mp.tile_off = nullptr; mp.m = 1; mp.ntiles = ntiles; mp.tilemap = nullptr;
+    mp.B = B; mp.tile_slot = nullptr; mp.tile_off = nullptr; mp.m = 1; mp.ntiles = ntiles; mp.nonfinite = nullptr;
     mp.bits = reinterpret_cast<uint32_t*>(sb + off_bits);
     mp.seg_count = reinterpret_cast<uint32_t*>(sb + off_count);
     if (launch_mark(mp, slot.tw, s) != cudaSuccess) { cudaGetLastError(); return DCB_ERR_CUDA; }

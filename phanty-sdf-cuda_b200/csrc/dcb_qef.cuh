@@ -1,4 +1,5 @@
-// dcb_qef.cuh — device helpers of the FP32 vertex kernels (dcb_band.cu, dcb_vertex.cu): Hermite interpolation and
+// dcb_qef.cuh — device helpers of the FP32 vertex kernels (k_cell_qef and k_cell_jacobi of
+// dcb_vertex.cu): Hermite interpolation and
 // trilinear normals (src/cpp/Cell.cpp:49-155), cell widths as the reference forms positions
 // (src/cpp/dc_backend.cpp:63-65), compensated sums and the rank-1 certified QEF solve.
 #pragma once
@@ -10,6 +11,9 @@ namespace dcb {
 // FP32 rounding can move by ~1e-5; such cells are re-solved in FP64.
 constexpr float kNormalCond2 = 1e-4f;
 
+__device__ __forceinline__ float ldv(const GridDesc& g, int i, int j, int k) {
+    return __ldg(g.v + pidx(g, i, j, k));
+}
 __device__ __forceinline__ float width_axis(const GridDesc& g, int axis, int idx) {
     if (axis == 0) return pos_axis(g.ox, g.vx, idx + 1) - pos_axis(g.ox, g.vx, idx);
     if (axis == 1) return pos_axis(g.oy, g.vy, idx + 1) - pos_axis(g.oy, g.vy, idx);
@@ -29,6 +33,23 @@ __device__ __forceinline__ float lerp_t(float fa, float fb) {
     if (fabsf(d) < 1e-6f) return (float)((double)fa / ((double)fa - (double)fb + 1e-16));
     return __fdividef(fa, d);   // |t| <= 1 here: the 2-ulp quotient is far inside the FP32 budget
 }
+__device__ __forceinline__ bool active_at(const GridDesc& g, int i, int j, int k) {
+    bool neg = false, pos = false;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        const float v = ldv(g, i + corner_dx(c), j + corner_dy(c), k + corner_dz(c));
+        neg |= v < 0.f;
+        pos |= v > 0.f;
+    }
+    return neg && pos;
+}
+__device__ __forceinline__ int3 add3(int3 a, int axis, int d) {
+    if (axis == 0) a.x += d; else if (axis == 1) a.y += d; else a.z += d;
+    return a;
+}
+__device__ __forceinline__ int comp(int3 a, int axis) { return axis == 0 ? a.x : (axis == 1 ? a.y : a.z); }
+__device__ __forceinline__ float ldp(const GridDesc& g, int3 p) { return ldv(g, p.x, p.y, p.z); }
+
 __device__ __forceinline__ void kahan_add(float& s, float& c, float x) {
     const float y = x - c;
     const float t = s + y;
@@ -79,6 +100,33 @@ __host__ __device__ constexpr uint32_t edge_geo(int e) {
 }
 static __constant__ uint32_t c_edge_geo[12] = {edge_geo(0), edge_geo(1), edge_geo(2), edge_geo(3), edge_geo(4), edge_geo(5),
                                         edge_geo(6), edge_geo(7), edge_geo(8), edge_geo(9), edge_geo(10), edge_geo(11)};
+
+// Widths (and reciprocals) of the cells i-1, i, i+1 along each axis, exact float
+// differences of the float grid positions (the CPU forms positions the same way).
+struct Widths {
+    float w[3][3];   // [axis][offset+1]
+    float r[3][3];
+};
+__device__ __forceinline__ void cell_widths(const GridDesc& g, int i, int j, int k, Widths& W) {
+    const int idx[3] = {i, j, k};
+    const float o[3] = {g.ox, g.oy, g.oz}, v[3] = {g.vx, g.vy, g.vz};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        float pm = pos_axis(o[a], v[a], idx[a] - 1), p0 = pos_axis(o[a], v[a], idx[a]);
+        float p1 = pos_axis(o[a], v[a], idx[a] + 1), p2 = pos_axis(o[a], v[a], idx[a] + 2);
+        W.w[a][0] = p0 - pm; W.w[a][1] = p1 - p0; W.w[a][2] = p2 - p1;
+#pragma unroll
+        for (int q = 0; q < 3; ++q) W.r[a][q] = 1.f / W.w[a][q];
+    }
+}
+
+// W.r[a][q] for runtime a, q with literal array indices only (keeps W in registers).
+__device__ __forceinline__ float pick_r(const Widths& W, int a, int q) {
+    const float r0 = q == 0 ? W.r[0][0] : (q == 1 ? W.r[0][1] : W.r[0][2]);
+    const float r1 = q == 0 ? W.r[1][0] : (q == 1 ? W.r[1][1] : W.r[1][2]);
+    const float r2 = q == 0 ? W.r[2][0] : (q == 1 ? W.r[2][1] : W.r[2][2]);
+    return a == 0 ? r0 : (a == 1 ? r1 : r2);
+}
 
 // Local -> world: one double combination per axis, one float rounding.
 __device__ __forceinline__ void store_vertex(float* __restrict__ V, const GridDesc& g, long long r, int i, int j, int k,

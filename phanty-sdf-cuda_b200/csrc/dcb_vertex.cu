@@ -1,14 +1,248 @@
-// dcb_vertex.cu — the FP32 cyclic-Jacobi solve of the cells whose normal equations the band
-// kernel (dcb_band.cu) could not certify as rank 1.
+// dcb_vertex.cu — Hermite estimate, 4-cell normal averaging and QEF solve in FP32, plus
+// the face mask of each cell's three min-corner edges.
 //
-// Semantics: Cell::update / solve_quadratic_system (src/cpp/Cell.cpp:284-361): the truncated
-// pseudo-inverse of A^T A (singular values <= svd_threshold dropped) about the centroid. A cell
-// whose retained spectrum is ill-conditioned, or has an eigenvalue within a relative band of
-// the threshold (the rank decision is ambiguous in FP32), is listed for the FP64 path
-// (dcb_vertex64.cu), which repeats the CPU arithmetic.
+// Semantics follow the reference CPU backend:
+//   Hermite samples   Cell::fill_hermite_data (src/cpp/Cell.cpp:162-212): every edge with
+//                     fa*fb <= 0, t = fa/(fa - fb + 1e-16), normal = normalised trilinear
+//                     gradient of the cell at the sample (Cell.cpp:80-155)
+//   averaging         average_hermite_normals / process_edge (src/cpp/hermite_update.cpp:
+//                     171-438): a grid edge with an endpoint strictly inside the grid whose
+//                     four cells are all active gets n = normalize(sum of the four cells' own
+//                     non-zero normals), summed owner, -dir1, -dir2, diagonal; the owner is the
+//                     cell at the edge's minimum endpoint
+//   QEF               Cell::update / solve_quadratic_system (Cell.cpp:284-361): A^T A, A^T b,
+//                     pinv truncating singular values <= svd_threshold, about the centroid
+//   faces             extract_mesh_from_cells (src/cpp/contouring.cpp:607-729): a face per
+//                     edge with s0*s1 < 0; cell (i,j,k) owns its three min-corner edges.
+// The reference GPU kernel clamps vertices, skips the averaging and uses another lerp
+// epsilon (src/cuda/dc_cuda.cu:283-423); none of that is reproduced.
+//
+// Work split:
+//   k_cell_qef       one thread per active cell. Each lane walks only its own crossing
+//                    edges. On an edge every trilinear gradient reduces to the edge difference
+//                    plus two bilinear differences, so the four cells' normals of an averaged
+//                    edge need 10 grid values; every cell sharing the edge recomputes the same
+//                    average (no storage, no neighbour lookups). Hermite positions are kept in
+//                    cell-local units, the centred normal equations are summed with Kahan
+//                    compensation, and the cell is solved at once when its spectrum is
+//                    provably rank 1 (power iteration + trace test); every other cell is
+//                    appended to a compact list. The kernel also emits the face mask of the
+//                    cell's three min-corner edges and the per-column face counts.
+//   k_cell_jacobi    the listed cells: cyclic Jacobi in FP32.
+// FP32 is not trusted when an eigenvalue sits within a relative band of the threshold,
+// when the retained condition exceeds the limit, or when a normal's direction is decided
+// by cancellation (gradient tiny against its terms, or four normals nearly cancelling);
+// such cells go to the FP64 path (dcb_vertex64.cu), which repeats the CPU arithmetic.
 #include "dcb_qef.cuh"
 
 namespace dcb {
+
+// Hermite normal of one crossing edge: the 4-cell average when the edge is in the averaging
+// set, else the cell's own trilinear normal at its sample. The average is a function of
+// the edge alone, so every cell sharing the edge computes the same value.
+// lo: global low endpoint; o1/o2: offset (0/1) of the low endpoint from the cell along d1/d2.
+__device__ float3 edge_normal(const GridDesc& g, int3 lo, int axis, int o1, int o2, float s_lo, float s_hi,
+                              float t_lo, float pu, float pv, float pw, const float cc[8],
+                              const Widths& W, bool& ill) {
+    const int3 hi = add3(lo, axis, 1);
+    const bool in0 = lo.x > 0 && lo.x < g.nx - 1 && lo.y > 0 && lo.y < g.ny - 1 && lo.z > 0 && lo.z < g.nz - 1;
+    const bool in1 = hi.x > 0 && hi.x < g.nx - 1 && hi.y > 0 && hi.y < g.ny - 1 && hi.z > 0 && hi.z < g.nz - 1;
+    const int d1 = axis == 0 ? 1 : 0;
+    const int d2 = axis == 2 ? 1 : 2;
+    bool avg = in0 || in1;
+    if (avg && !strict_change(s_lo, s_hi)) {
+        // zero endpoint: the four cells are not automatically active
+        for (int q = 0; q < 4 && avg; ++q) {
+            int3 c = lo;
+            if (q & 1) c = add3(c, d1, -1);
+            if (q & 2) c = add3(c, d2, -1);
+            avg = active_at(g, c.x, c.y, c.z);
+        }
+    }
+    if (!avg) return normalized(own_gradient(cc, pu, pv, pw, W.r[0][1], W.r[1][1], W.r[2][1], ill));
+    // Along-edge sample of each cell in its own EDGE_PAIRS orientation: X edges start at
+    // local x=1 when local y=1, Y edges at local y=1 when local x=0, Z edges at z=0. A cell
+    // starting at the high end samples at 1 - t_hi, which equals t_lo unless |s_lo - s_hi| is
+    // tiny (both t are then formed in double, exactly as the CPU forms them).
+    const float u_hi = fabsf(s_lo - s_hi) < 1e-6f ? 1.f - lerp_t(s_hi, s_lo) : t_lo;
+    const int64_t st1 = d1 == 0 ? 1 : (int64_t)g.nx;
+    const int64_t st2 = d2 == 1 ? (int64_t)g.nx : (int64_t)g.nx * g.ny;
+    const float* plo = g.v + pidx(g, lo.x, lo.y, lo.z);
+    const float* phi = g.v + pidx(g, hi.x, hi.y, hi.z);
+    const float ga = (s_hi - s_lo) * pick_r(W, axis, 1);
+    // perpendicular differences at both edge ends: forward (m=0) and backward (m=1)
+    const float a0p = __ldg(plo + st1) - s_lo, a0m = s_lo - __ldg(plo - st1);
+    const float a1p = __ldg(phi + st1) - s_hi, a1m = s_hi - __ldg(phi - st1);
+    const float b0p = __ldg(plo + st2) - s_lo, b0m = s_lo - __ldg(plo - st2);
+    const float b1p = __ldg(phi + st2) - s_hi, b1m = s_hi - __ldg(phi - st2);
+    // widths of the cells on either side of the edge: the cell index along d is
+    // (cell coordinate + o) for m = 0 and one less for m = 1
+    const float rw1p = pick_r(W, d1, 1 + o1), rw1m = pick_r(W, d1, o1);
+    const float rw2p = pick_r(W, d2, 1 + o2), rw2m = pick_r(W, d2, o2);
+    // one cancellation bound per edge (>= each cell's own bound)
+    const float m1v = fmaxf(fmaxf(fabsf(a0p), fabsf(a1p)) * rw1p, fmaxf(fabsf(a0m), fabsf(a1m)) * rw1m);
+    const float m2v = fmaxf(fmaxf(fabsf(b0p), fabsf(b1p)) * rw2p, fmaxf(fabsf(b0m), fabsf(b1m)) * rw2m);
+    const float bound2 = kNormalCond2 * (ga * ga + m1v * m1v + m2v * m2v);
+    float3 acc = make_float3(0.f, 0.f, 0.f);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int m1 = q & 1, m2 = q >> 1;
+        const bool start_high = (axis == 0) ? (m1 == 1) : (axis == 1) ? (m1 == 0) : false;
+        const float u = start_high ? u_hi : t_lo;
+        const float e1lo = m1 ? a0m : a0p, e1hi = m1 ? a1m : a1p;
+        const float e2lo = m2 ? b0m : b0p, e2hi = m2 ? b1m : b1p;
+        const float g1 = (e1lo + u * (e1hi - e1lo)) * (m1 ? rw1m : rw1p);
+        const float g2 = (e2lo + u * (e2hi - e2lo)) * (m2 ? rw2m : rw2p);
+        float3 gv;
+        if (axis == 0) gv = make_float3(ga, g1, g2);
+        else if (axis == 1) gv = make_float3(g1, ga, g2);
+        else gv = make_float3(g1, g2, ga);
+        const float gn2 = gv.x * gv.x + gv.y * gv.y + gv.z * gv.z;
+        if (gn2 <= bound2) ill = true;
+        if (gn2 > 0.f) {
+            const float rn = rsqrtf(gn2);
+            acc.x += gv.x * rn; acc.y += gv.y * rn; acc.z += gv.z * rn;
+        }
+    }
+    if (acc.x * acc.x + acc.y * acc.y + acc.z * acc.z < 1e-4f) ill = true;
+    return normalized(acc);
+}
+
+// ---- k_cell_qef -------------------------------------------------------------------------
+
+template <bool ONE>
+__global__ void __launch_bounds__(128, 5)
+k_cell_qef(const __grid_constant__ QefParams P) {
+    __shared__ unsigned int s_hist;
+    __shared__ float s_c[8][128];    // per-thread corner values (dynamically indexed)
+    __shared__ float s_t[12][128];   // per-thread lerp parameter of each crossing edge
+    const int tid = threadIdx.x;
+    if (tid == 0) s_hist = 0;
+    __syncthreads();
+    // a captured graph whose live count exceeds the capacity it was built for does nothing
+    // (the host reports the overflow after the replay)
+    const long long nact = P.live ? ((long long)*P.live > P.nactive ? 0 : (long long)*P.live) : P.nactive;
+    for (long long r = (long long)blockIdx.x * blockDim.x + tid; r < nact;
+         r += (long long)gridDim.x * blockDim.x) {
+        const GridSlot& S = slot_ref<ONE>(P.B, ONE ? 0 : slot_of_rank(P.B, (unsigned long long)r));
+        const GridDesc& g = S.g;
+        const long long cxcy = (long long)g.cx * g.cy;
+        uint32_t* const col_count = P.col_count + S.col_off;
+        int i, j, k;
+        unpack_cell(P.list[r], i, j, k);
+        float c[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            c[q] = ldv(g, i + corner_dx(q), j + corner_dy(q), k + corner_dz(q));
+            s_c[q][tid] = c[q];
+        }
+        // Faces owned by this cell: its min-corner X, Y, Z edges (contouring.cpp:609-729).
+        uint8_t fm = 0;
+        if (j >= 1 && k >= 1 && strict_change(c[0], c[1])) {
+            fm |= 1; atomicAdd(&col_count[0 * cxcy + (long long)i * g.cy + j], 1u);
+        }
+        if (i >= 1 && k >= 1 && strict_change(c[0], c[3])) {
+            fm |= 2; atomicAdd(&col_count[1 * cxcy + (long long)i * g.cy + j], 1u);
+        }
+        if (i >= 1 && j >= 1 && strict_change(c[0], c[4])) {
+            fm |= 4; atomicAdd(&col_count[2 * cxcy + (long long)i * g.cy + j], 1u);
+        }
+        // an infinite value where the reference's face lookup interpolates from: it exits
+        // (contouring.cpp:560-594); the host reports DCB_ERR_INVALID_ARGUMENT
+        if (((fm & 1) && isinf(c[1])) || ((fm & 6) && isinf(c[0]))) set_error(P.err, kErrNonFinite);
+        P.fmask[r] = fm;
+
+        // Pass 1: crossing edges and the centroid in local units.
+        uint32_t hmask = 0;
+        float cu = 0.f, cv = 0.f, cw = 0.f;
+#pragma unroll
+        for (int e = 0; e < 12; ++e) {
+            const int a = edge_a(e), b = edge_b(e);
+            if (!hermite_crossing(c[a], c[b])) continue;
+            hmask |= 1u << e;
+            const float t = lerp_t(c[a], c[b]);
+            s_t[e][tid] = t;
+            float pu = (float)corner_dx(a), pv = (float)corner_dy(a), pw = (float)corner_dz(a);
+            if (corner_dx(a) != corner_dx(b)) pu = corner_dx(a) ? 1.f - t : t;
+            if (corner_dy(a) != corner_dy(b)) pv = corner_dy(a) ? 1.f - t : t;
+            if (corner_dz(a) != corner_dz(b)) pw = corner_dz(a) ? 1.f - t : t;
+            cu += pu; cv += pv; cw += pw;
+        }
+        const float invm = 1.f / (float)__popc(hmask);
+        cu *= invm; cv *= invm; cw *= invm;
+        Widths W;
+        cell_widths(g, i, j, k, W);
+        const float fy = W.w[1][1] * W.r[0][1], fz = W.w[2][1] * W.r[0][1];
+
+        // Pass 2: each lane walks its own crossing edges (warp iterations = max count).
+        float M00 = 0, M01 = 0, M02 = 0, M11 = 0, M12 = 0, M22 = 0, R0 = 0, R1 = 0, R2 = 0;
+        float K00 = 0, K01 = 0, K02 = 0, K11 = 0, K12 = 0, K22 = 0, Q0 = 0, Q1 = 0, Q2 = 0;
+        bool ill = false;
+        uint32_t rem = hmask;
+        while (rem) {
+            const int e = __ffs(rem) - 1;
+            rem &= rem - 1;
+            const uint32_t geo = c_edge_geo[e];
+            const int axis = geo & 3;
+            const int lox = (geo >> 2) & 1, loy = (geo >> 3) & 1, loz = (geo >> 4) & 1;
+            const bool own_low = (geo >> 5) & 1;
+            const float s_lo = s_c[(geo >> 6) & 7][tid], s_hi = s_c[(geo >> 9) & 7][tid];
+            // this cell's own sample (pass 1): t in its own orientation
+            const float t = s_t[e][tid];
+            const float along = own_low ? t : 1.f - t;
+            const float t_lo = own_low ? t : lerp_t(s_lo, s_hi);
+            const float pu = axis == 0 ? along : (float)lox;
+            const float pv = axis == 1 ? along : (float)loy;
+            const float pw = axis == 2 ? along : (float)loz;
+            const int o1 = axis == 0 ? loy : lox, o2 = axis == 2 ? loy : loz;
+            const float3 n = edge_normal(g, make_int3(i + lox, j + loy, k + loz), axis, o1, o2, s_lo, s_hi, t_lo,
+                                         pu, pv, pw, c, W, ill);
+            const float qx = pu - cu, qy = (pv - cv) * fy, qz = (pw - cw) * fz;
+            const float nb = n.x * qx + n.y * qy + n.z * qz;
+            kahan_add(M00, K00, n.x * n.x); kahan_add(M01, K01, n.x * n.y); kahan_add(M02, K02, n.x * n.z);
+            kahan_add(M11, K11, n.y * n.y); kahan_add(M12, K12, n.y * n.z); kahan_add(M22, K22, n.z * n.z);
+            kahan_add(R0, Q0, n.x * nb); kahan_add(R1, Q1, n.y * nb); kahan_add(R2, Q2, n.z * nb);
+        }
+
+        // A NaN or infinite value in the normal equations, or anywhere in the grid (the CPU
+        // backend's trilinear normals then see it through zero-weighted corners, Cell.cpp:80-155,
+        // and its SVD factors carry it into the vertex, Cell.cpp:324-361): only the FP64 path
+        // repeats that arithmetic, so such cells go there.
+        if (!isfinite(M00 + M01 + M02 + M11 + M12 + M22 + R0 + R1 + R2 + cu + cv + cw) || (P.nonfinite && *P.nonfinite))
+            ill = true;
+        if (ill || P.force64) {
+            // FP32 cannot be trusted: the FP64 path recomputes this cell from the grid.
+            const unsigned int slot = atomicAdd(P.esc_count, 1u);
+            P.esc_list[slot] = (uint32_t)r;
+            store_vertex(P.V, g, r, i, j, k, cu, cv, cw);
+            continue;
+        }
+        float ox, oy, oz;
+        if (qef_rank1(M00, M01, M02, M11, M12, M22, R0, R1, R2, P.thr, P.band, ox, oy, oz)) {
+            store_vertex(P.V, g, r, i, j, k, cu + ox, cv + oy / fy, cw + oz / fz);
+            P.vclass[r] = kVcRank1;
+            atomicAdd(&s_hist, 1u);
+        } else {
+            const unsigned int slot = atomicAdd(P.hard_count, 1u);
+            P.hard_list[slot] = (uint32_t)r;
+            P.hard_data[3 * (size_t)slot + 0] = make_float4(M00, M01, M02, M11);
+            P.hard_data[3 * (size_t)slot + 1] = make_float4(M12, M22, R0, R1);
+            P.hard_data[3 * (size_t)slot + 2] = make_float4(R2, cu, cv, cw);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && s_hist) atomicAdd(P.rank_hist + 1, (unsigned long long)s_hist);
+}
+
+cudaError_t launch_cell_qef(const QefParams& P, int num_sms, cudaStream_t s) {
+    if (P.nactive <= 0) return cudaSuccess;
+    long long blocks = (P.nactive + 127) / 128;
+    const long long cap = (long long)num_sms * 32;
+    if (blocks > cap) blocks = cap;
+    if (P.B.n == 1) k_cell_qef<true><<<(unsigned)blocks, 128, 0, s>>>(P);
+    else            k_cell_qef<false><<<(unsigned)blocks, 128, 0, s>>>(P);
+    return cudaGetLastError();
+}
 
 // ---- k_cell_jacobi ----------------------------------------------------------------------
 

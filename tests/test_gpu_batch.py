@@ -96,22 +96,6 @@ def test_autotune_keeps_the_results(backend):
     print("autotuned mark tiling: %d waves, 256-cell tiles up to %d cells wide, %.3f ms" % (waves, narrow, ms))
 
 
-def test_band_autotune_keeps_the_results(backend):
-    """The band kernel's width autotuner picks a CTA count per SM within the occupancy limit and
-    the extraction's output does not change with it."""
-    import torch
-    from contouring_b200 import synth
-    grids = synth.csg_batch(24, seed=6, device="cuda")
-    before, _ = backend.extract_batch(grids)
-    before = [(V.clone(), F.clone()) for V, F in before]
-    w, ms = backend.autotune_band(grids)
-    assert 1 <= w <= 16 and ms > 0
-    after, _ = backend.extract_batch(grids)
-    for (Va, Fa), (Vb, Fb) in zip(before, after):
-        assert torch.equal(Va, Vb) and torch.equal(Fa, Fb)
-    print("autotuned band kernel: %d CTAs per SM, %.3f ms" % (w, ms))
-
-
 # ---- the batch captured in a CUDA graph (dcb_batch_graph_*) -----------------------------------
 
 def _same(meshes_a, meshes_b):
