@@ -29,7 +29,7 @@ EXPORTED = (
     "dcb_create", "dcb_destroy", "dcb_extract_device", "dcb_extract_host",
     "dcb_copy_mesh_to_host", "dcb_copy_mesh_device", "dcb_copy_cells_to_host",
     "dcb_mark_active_cells_noalloc", "dcb_mesh_to_sdf_device", "dcb_mesh_to_sdf_host",
-    "dcb_extract_batch_device", "dcb_backward", "dcb_autotune_mark"
+    "dcb_extract_batch_device", "dcb_backward", "dcb_autotune_mark",
     "dcb_write_obj", "dcb_read_sdf", "dcb_write_sdf", "dcb_extract_upload", "dcb_mesh_to_sdf_device_ex",
     "dcb_mesh_to_sdf_host_ex", "dcb_batch_graph_create", "dcb_batch_graph_launch", "dcb_batch_graph_finish",
     "dcb_batch_graph_destroy", "dcb_postprocess_device", "dcb_postprocess_host", "dcb_copy_post_mesh",
