@@ -636,8 +636,8 @@ int run_ours(dcb_context* h, const dcb_grid* in, const dcb_opts* o, cudaStream_t
     BatchLayout L;
     rc = layout_batch(h, in, 1, L);
     if (rc != DCB_OK) return rc;
-    size_t cub_bytes = 0;
-    const size_t ws = ours_workspace_bytes(nv, nq, npts, &cub_bytes);
+    size_t sort_bytes = 0;
+    const size_t ws = ours_workspace_bytes(nv, nq, npts, &sort_bytes);
     DCB_TRY(h, ensure(h->ours_ws, ws), "alloc refinement workspace");
     const bool tri = o->emit_triangles != 0;
     if (tri) DCB_TRY(h, ensure(h->tris, sizeof(int32_t) * 6 * (size_t)std::max(1LL, nq)), "alloc triangles");
@@ -679,7 +679,7 @@ int run_ours(dcb_context* h, const dcb_grid* in, const dcb_opts* o, cudaStream_t
     Counters* dc_counters = as<Counters>(h->counters);
     P.err = &dc_counters->err;
     R.workspace = h->ours_ws.p;
-    R.cub_bytes = cub_bytes;
+    R.sort_bytes = sort_bytes;
     R.outer_iters = o->outer_iters;
     R.hermite_update = o->hermite_update;
     R.batch_size = o->batch_size;

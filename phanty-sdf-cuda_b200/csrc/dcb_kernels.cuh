@@ -307,7 +307,7 @@ struct OursParams {
 struct OursRun {
     OursParams P;
     void* workspace;
-    size_t cub_bytes;
+    size_t sort_bytes;
     int outer_iters;
     int hermite_update;
     long long batch_size;
@@ -315,7 +315,7 @@ struct OursRun {
     int triangles;
     int num_sms;
 };
-size_t ours_workspace_bytes(long long nv, long long nq, long long npts, size_t* cub_bytes);
+size_t ours_workspace_bytes(long long nv, long long nq, long long npts, size_t* sort_bytes);
 cudaError_t ours_run(OursRun& R, cudaStream_t s);
 
 // ---- mesh -> SDF (dcb_mesh_sdf.cu) ----
@@ -431,7 +431,7 @@ enum PostStatIndex {
 
 // Device workspace of the post-pass; kept by the handle between calls (buffers only grow).
 struct PostWork {
-    PostBuf count, key, key2, val, val2, u0, u1, u2, u3, ft, flag8, cub;
+    PostBuf count, key, key2, val, val2, u0, u1, u2, u3, ft, flag8, scratch;
     PostBuf Vw, Fw, kept, parent, csize, bnd;
     PostBuf deg, bot, top, pos, vparent, skey, sdeg, shead, soff, sgid, stack, lverts, lflag, lkey, llen;
     PostBuf lpos, lorder, lkey2, nvl, nfl, vb, fb, fillV, fillF;

@@ -23,9 +23,9 @@
 //      than 1e-6 (contouring.cpp:1288-1309).
 // Everything is FP64 and compiled with --fmad=false, like the CPU restatement it is checked
 // against. One thread per cell (steps 3-5), per quad (1), per grid point (2).
-#include <cub/device/device_radix_sort.cuh>
 #include <cfloat>
 #include "dcb_f64.cuh"
+#include "dcb_sort.cuh"
 
 namespace dcb {
 
@@ -918,19 +918,11 @@ inline unsigned grid_for(long long n, int threads, int num_sms) {
 inline size_t al(size_t x) { return (x + 255) & ~size_t(255); }
 }  // namespace
 
-size_t ours_workspace_bytes(long long nv, long long nq, long long npts, size_t* cub_bytes) {
+size_t ours_workspace_bytes(long long nv, long long nq, long long npts, size_t* sort_bytes) {
     const long long nt = 2 * nq;
-    size_t tb1 = 0, tb2 = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, tb1, (uint32_t*)nullptr, (uint32_t*)nullptr, (uint32_t*)nullptr,
-                                    (uint32_t*)nullptr, (int)std::max(1LL, nt));
-    size_t tb0 = 0;
-    cub::DeviceRadixSort::SortKeys(nullptr, tb0, (unsigned long long*)nullptr, (unsigned long long*)nullptr,
-                                   (int)std::max(1LL, nt));
-    cub::DeviceRadixSort::SortPairs(nullptr, tb2, (unsigned long long*)nullptr, (unsigned long long*)nullptr,
-                                    (uint32_t*)nullptr, (uint32_t*)nullptr, (int)std::max(1LL, npts));
-    size_t tb3 = 0;
-    cub::DeviceRadixSort::SortKeys(nullptr, tb3, (uint32_t*)nullptr, (uint32_t*)nullptr, (int)std::max(1LL, npts));
-    *cub_bytes = std::max(std::max(tb0, tb1), std::max(tb2, tb3));
+    // radix sorts: triangle codes (32-bit keys) and point keys (64-bit keys), 32-bit values
+    *sort_bytes = std::max(radix_sort_temp_bytes(std::max(1LL, nt), 4, true),
+                          radix_sort_temp_bytes(std::max(1LL, npts), 8, true));
     size_t b = 0;
     b += al(sizeof(OursCell) * nv) + al(sizeof(double) * 3 * nv);            // cells, Vm
     b += al(sizeof(int4) * nq) + al(sizeof(double) * 3 * nq);               // quads, gsum
@@ -944,7 +936,7 @@ size_t ours_workspace_bytes(long long nv, long long nq, long long npts, size_t* 
     b += 4 * al(sizeof(uint32_t) * nt);                                      // triangle codes / indices
     b += 2 * al(sizeof(float4) * 2 * nt) + al(sizeof(unsigned int) * nt) + al(sizeof(double) * 9 * nt);
     b += al(sizeof(uint32_t) * (scan_partials_len(nv + 1) + 1)) + al(64);    // scan partials, counters
-    b += al(*cub_bytes);
+    b += al(*sort_bytes);
     return b + 4096;
 }
 
@@ -983,7 +975,7 @@ cudaError_t ours_run(OursRun& R, cudaStream_t s) {
     P.tri9 = (double*)take(sizeof(double) * 9 * nt);
     uint32_t* partials = (uint32_t*)take(sizeof(uint32_t) * (scan_partials_len(nv + 1) + 1));
     unsigned int* counters = (unsigned int*)take(64);
-    void* cub_temp = take(R.cub_bytes);
+    void* sort_temp = take(R.sort_bytes);
     uint32_t* sel_sorted = (uint32_t*)take(sizeof(uint32_t) * npts);
     P.prev_tri = (int*)take(sizeof(int) * npts);
     P.heavy_count = counters + 8;
@@ -1009,15 +1001,12 @@ cudaError_t ours_run(OursRun& R, cudaStream_t s) {
     // a compact block of the grid); a random fill is ordered again every outer iteration
     if (nband > 0) {
         k_ours_point_keys<<<grid_for(nband, 256, sms), 256, 0, s>>>(P, band, nband, fk);
-        size_t tb4 = R.cub_bytes;
-        OURS_TRY(cub::DeviceRadixSort::SortPairs(cub_temp, tb4, fk, fk2, band, sel_sorted, (int)nband, 0, 63, s));
+        OURS_TRY(radix_sort_pairs(sort_temp, R.sort_bytes, fk, fk2, band, sel_sorted, nband, 0, 63, s));
     }
     for (int it = 0; it < R.outer_iters; ++it) {
         if (nq > 0) {
             k_ours_tris<<<grid_for(nq, 128, sms), 128, 0, s>>>(P);
-            size_t tb = R.cub_bytes;
-            OURS_TRY(cub::DeviceRadixSort::SortPairs(cub_temp, tb, P.tcode, P.tcode_sorted, P.tidx, P.tidx_sorted,
-                                                     (int)nt, 0, 30, s));
+            OURS_TRY(radix_sort_pairs(sort_temp, R.sort_bytes, P.tcode, P.tcode_sorted, P.tidx, P.tidx_sorted, nt, 0, 30, s));
             k_bvh_keys<<<grid_for(nt, 256, sms), 256, 0, s>>>(P);
             OURS_TRY(cudaMemsetAsync(P.flags, 0, sizeof(unsigned int) * nt, s));
             if (nt > 1) k_bvh_tree<<<grid_for(nt - 1, 128, sms), 128, 0, s>>>(P);
@@ -1025,12 +1014,9 @@ cudaError_t ours_run(OursRun& R, cudaStream_t s) {
             k_bvh_boxes<<<grid_for(nt, 128, sms), 128, 0, s>>>(P);
             if (nfill > 0) {
                 k_ours_fill_keys<<<grid_for(nrest, 256, sms), 256, 0, s>>>(rest, nrest, R.seed, it, fk);
-                size_t tb2 = R.cub_bytes;
-                OURS_TRY(cub::DeviceRadixSort::SortPairs(cub_temp, tb2, fk, fk2, rest, fv2, (int)nrest, 0, 64, s));
+                OURS_TRY(radix_sort_pairs(sort_temp, R.sort_bytes, fk, fk2, rest, fv2, nrest, 0, 64, s));
                 k_ours_point_keys<<<grid_for(nfill, 256, sms), 256, 0, s>>>(P, fv2, nfill, fk);
-                size_t tb3 = R.cub_bytes;
-                OURS_TRY(cub::DeviceRadixSort::SortPairs(cub_temp, tb3, fk, fk2, fv2, sel_sorted + nband, (int)nfill,
-                                                         0, 63, s));
+                OURS_TRY(radix_sort_pairs(sort_temp, R.sort_bytes, fk, fk2, fv2, sel_sorted + nband, nfill, 0, 63, s));
             }
             OURS_TRY(cudaMemsetAsync(P.cell_count, 0, sizeof(unsigned int) * (nv + 1), s));
             OURS_TRY(cudaMemsetAsync(P.cell_fill, 0, sizeof(unsigned int) * (nv + 1), s));

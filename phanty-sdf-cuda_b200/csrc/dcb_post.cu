@@ -31,11 +31,8 @@
 #include <algorithm>
 #include <cstdint>
 #include <cstring>
-#include <cub/device/device_radix_sort.cuh>
-#include <cub/device/device_scan.cuh>
-#include <cub/device/device_select.cuh>
-#include <thrust/iterator/counting_iterator.h>
 #include "dcb_kernels.cuh"
+#include "dcb_sort.cuh"
 
 namespace dcb {
 
@@ -928,28 +925,23 @@ cudaError_t weld(PostWork& W, PostRun& R, const float* V, long long nv, const in
     PP_TRY(grow(Vout, sizeof(float) * 3 * nv));
     PP_TRY(grow(Fout, sizeof(int4) * nf));
     size_t t0 = 0, t1 = 0, t2 = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, t0, (unsigned long long*)nullptr, (unsigned long long*)nullptr, (int*)nullptr,
-                                    (int*)nullptr, (int)nv, 0, 3 * kKeyBits, s);
-    cub::DeviceScan::ExclusiveSum(nullptr, t1, (unsigned int*)nullptr, (unsigned int*)nullptr, (int)nv, s);
-    cub::DeviceSelect::Flagged(nullptr, t2, (int4*)nullptr, (unsigned char*)nullptr, (int4*)nullptr,
-                               (unsigned long long*)nullptr, (int)nf, s);
+    t0 = radix_sort_temp_bytes(nv, 8, true);
+    t1 = scan_temp_bytes(nv);
+    t2 = select_temp_bytes(nf);
     const size_t tb = std::max(t0, std::max(t1, t2));
-    PP_TRY(grow(W.cub, tb));
+    PP_TRY(grow(W.scratch, tb));
     const unsigned g = grid_for(nv, kThreads, sms);
     k_post_reset<<<1, 32, 0, s>>>(C);
     k_bbox<<<g, kThreads, 0, s>>>(V, nv, C);
     k_weld_params<<<1, 32, 0, s>>>(C);
     k_weld_keys<<<g, kThreads, 0, s>>>(V, nv, C, as<unsigned long long>(W.key), as<int>(W.val));
     PP_TRY(cudaGetLastError());
-    size_t tt = W.cub.bytes;
-    PP_TRY(cub::DeviceRadixSort::SortPairs(W.cub.p, tt, as<unsigned long long>(W.key), as<unsigned long long>(W.key2),
-                                           as<int>(W.val), as<int>(W.val2), (int)nv, 0, 3 * kKeyBits, s));
+    PP_TRY(radix_sort_pairs(W.scratch.p, W.scratch.bytes, as<unsigned long long>(W.key),
+                            as<unsigned long long>(W.key2), as<uint32_t>(W.val), as<uint32_t>(W.val2), nv, 0, 3 * kKeyBits, s));
     k_weld_heads<<<g, kThreads, 0, s>>>(as<unsigned long long>(W.key2), as<int>(W.val2), nv, as<unsigned int>(W.u0),
                                         as<unsigned int>(W.u1));
-    tt = W.cub.bytes;
-    PP_TRY(cub::DeviceScan::ExclusiveSum(W.cub.p, tt, as<unsigned int>(W.u1), as<unsigned int>(W.u2), (int)nv, s));
-    tt = W.cub.bytes;
-    PP_TRY(cub::DeviceScan::InclusiveSum(W.cub.p, tt, as<unsigned int>(W.u0), as<unsigned int>(W.u3), (int)nv, s));
+    PP_TRY(exclusive_sum(W.scratch.p, W.scratch.bytes, as<unsigned int>(W.u1), as<unsigned int>(W.u2), nv, s));
+    PP_TRY(inclusive_sum(W.scratch.p, W.scratch.bytes, as<unsigned int>(W.u0), as<unsigned int>(W.u3), nv, s));
     // u0 head, u3 group (1-based), u2 new index of representatives; u1 -> group's new index
     k_weld_groups<<<g, kThreads, 0, s>>>(as<int>(W.val2), as<unsigned int>(W.u0), as<unsigned int>(W.u3),
                                          as<unsigned int>(W.u2), V, nv, as<unsigned int>(W.u1), as<float>(Vout), C);
@@ -958,9 +950,8 @@ cudaError_t weld(PostWork& W, PostRun& R, const float* V, long long nv, const in
     k_weld_faces<<<grid_for(nf, kThreads, sms), kThreads, 0, s>>>(F, nf, nv, as<int>(W.val), as<int4>(W.ft),
                                                                    as<unsigned char>(W.flag8), C);
     PP_TRY(cudaGetLastError());
-    tt = W.cub.bytes;
-    PP_TRY(cub::DeviceSelect::Flagged(W.cub.p, tt, as<int4>(W.ft), as<unsigned char>(W.flag8), as<int4>(Fout),
-                                      &C->nsel, (int)nf, s));
+    PP_TRY(select_flagged(W.scratch.p, W.scratch.bytes, as<int4>(W.ft), as<unsigned char>(W.flag8),
+                          as<int4>(Fout), &C->nsel, (int)nf, s));
     cudaError_t e = read_counters(W, R, s);
     if (e != cudaSuccess) return e;
     nvw = (long long)host_counters(W).nvw;
@@ -971,7 +962,7 @@ cudaError_t weld(PostWork& W, PostRun& R, const float* V, long long nv, const in
 }  // namespace
 
 void post_release(PostWork& W) {
-    PostBuf* all[] = {&W.count, &W.key, &W.key2, &W.val, &W.val2, &W.u0, &W.u1, &W.u2, &W.u3, &W.ft, &W.flag8, &W.cub,
+    PostBuf* all[] = {&W.count, &W.key, &W.key2, &W.val, &W.val2, &W.u0, &W.u1, &W.u2, &W.u3, &W.ft, &W.flag8, &W.scratch,
                       &W.Vw, &W.Fw, &W.kept, &W.parent, &W.csize, &W.bnd, &W.deg, &W.bot, &W.top, &W.pos, &W.vparent,
                       &W.skey, &W.sdeg, &W.shead, &W.soff, &W.sgid, &W.stack, &W.lverts, &W.lflag, &W.lkey, &W.llen,
                       &W.lpos, &W.lorder, &W.lkey2, &W.nvl, &W.nfl, &W.vb, &W.fb, &W.fillV, &W.fillF, &W.first,
@@ -1033,17 +1024,14 @@ cudaError_t post_run(PostWork& W, PostRun& R, cudaStream_t s) {
     PP_TRY(grow(W.flag8, nfw));
     {
         size_t t0 = 0, t1 = 0;
-        cub::DeviceRadixSort::SortPairs(nullptr, t0, (unsigned long long*)nullptr, (unsigned long long*)nullptr,
-                                        (int*)nullptr, (int*)nullptr, (int)ne, 0, 2 * b, s);
-        cub::DeviceSelect::Flagged(nullptr, t1, (int4*)nullptr, (unsigned char*)nullptr, (int4*)nullptr,
-                                   (unsigned long long*)nullptr, (int)nfw, s);
-        PP_TRY(grow(W.cub, std::max(t0, t1)));
+        t0 = radix_sort_temp_bytes(ne, 8, true);
+        t1 = select_temp_bytes(nfw);
+        PP_TRY(grow(W.scratch, std::max(t0, t1)));
     }
     const int4* Fw = as<int4>(W.Fw);
     k_edge_uses<<<grid_for(ne, kThreads, sms), kThreads, 0, s>>>(Fw, nfw, b, as<unsigned long long>(W.key), as<int>(W.val));
-    size_t tt = W.cub.bytes;
-    PP_TRY(cub::DeviceRadixSort::SortPairs(W.cub.p, tt, as<unsigned long long>(W.key), as<unsigned long long>(W.key2),
-                                           as<int>(W.val), as<int>(W.val2), (int)ne, 0, 2 * b, s));
+    PP_TRY(radix_sort_pairs(W.scratch.p, W.scratch.bytes, as<unsigned long long>(W.key),
+                            as<unsigned long long>(W.key2), as<uint32_t>(W.val), as<uint32_t>(W.val2), ne, 0, 2 * b, s));
     if (R.remove_floaters) {
         k_iota<<<grid_for(nfw, kThreads, sms), kThreads, 0, s>>>(as<int>(W.parent), nfw);
         PP_TRY(cudaMemsetAsync(W.csize.p, 0, sizeof(unsigned int) * nfw, s));
@@ -1064,8 +1052,7 @@ cudaError_t post_run(PostWork& W, PostRun& R, cudaStream_t s) {
         k_keep_flags<<<grid_for(nfw, kThreads, sms), kThreads, 0, s>>>(as<int>(W.parent), nfw, C, as<unsigned char>(W.flag8));
         PP_TRY(cudaGetLastError());
         PP_TRY(cudaMemsetAsync(&C->nsel, 0, sizeof(unsigned long long), s));
-        tt = W.cub.bytes;
-        PP_TRY(cub::DeviceSelect::Flagged(W.cub.p, tt, Fw, as<unsigned char>(W.flag8), as<int4>(W.kept), &C->nsel,
+        PP_TRY(select_flagged(W.scratch.p, W.scratch.bytes, Fw, as<unsigned char>(W.flag8), as<int4>(W.kept), &C->nsel,
                                           (int)nfw, s));
         kept = as<int4>(W.kept);
     }
@@ -1096,15 +1083,12 @@ cudaError_t post_run(PostWork& W, PostRun& R, cudaStream_t s) {
                                                                      R.remove_floaters, b, as<unsigned long long>(W.key),
                                                                      as<unsigned int>(W.deg), C);
         size_t t0 = 0, t1 = 0;
-        cub::DeviceRadixSort::SortKeys(nullptr, t0, (unsigned long long*)nullptr, (unsigned long long*)nullptr, (int)nb,
-                                       0, 2 * b, s);
-        cub::DeviceScan::ExclusiveSum(nullptr, t1, (unsigned int*)nullptr, (unsigned int*)nullptr, (int)nvw, s);
-        PP_TRY(grow(W.cub, std::max(t0, t1)));
-        tt = W.cub.bytes;
-        PP_TRY(cub::DeviceRadixSort::SortKeys(W.cub.p, tt, as<unsigned long long>(W.key), as<unsigned long long>(W.key2),
-                                              (int)nb, 0, 2 * b, s));
-        tt = W.cub.bytes;
-        PP_TRY(cub::DeviceScan::ExclusiveSum(W.cub.p, tt, as<unsigned int>(W.deg), as<unsigned int>(W.bot), (int)nvw, s));
+        t0 = radix_sort_temp_bytes(nb, 8, false);
+        t1 = scan_temp_bytes(nvw);
+        PP_TRY(grow(W.scratch, std::max(t0, t1)));
+        PP_TRY(radix_sort_keys(W.scratch.p, W.scratch.bytes, as<unsigned long long>(W.key),
+                               as<unsigned long long>(W.key2), nb, 0, 2 * b, s));
+        PP_TRY(exclusive_sum(W.scratch.p, W.scratch.bytes, as<unsigned int>(W.deg), as<unsigned int>(W.bot), nvw, s));
         e = read_counters(W, R, s);
         if (e != cudaSuccess) return e;
         const long long nbk = (long long)host_counters(W).nbk;
@@ -1124,16 +1108,13 @@ cudaError_t post_run(PostWork& W, PostRun& R, cudaStream_t s) {
             const long long ns = (long long)host_counters(W).nstarts;
             {
                 size_t ta = 0, tb2 = 0, tc = 0;
-                cub::DeviceRadixSort::SortKeys(nullptr, ta, (unsigned long long*)nullptr, (unsigned long long*)nullptr,
-                                               (int)ns, 0, 2 * b, s);
-                cub::DeviceScan::ExclusiveSum(nullptr, tb2, (unsigned long long*)nullptr, (unsigned long long*)nullptr,
-                                              (int)ns, s);
-                cub::DeviceScan::InclusiveSum(nullptr, tc, (unsigned int*)nullptr, (unsigned int*)nullptr, (int)ns, s);
-                PP_TRY(grow(W.cub, std::max(ta, std::max(tb2, tc))));
+                ta = radix_sort_temp_bytes(ns, 8, false);
+                tb2 = scan_temp_bytes(ns);
+                tc = scan_temp_bytes(ns);
+                PP_TRY(grow(W.scratch, std::max(ta, std::max(tb2, tc))));
             }
-            tt = W.cub.bytes;
-            PP_TRY(cub::DeviceRadixSort::SortKeys(W.cub.p, tt, as<unsigned long long>(W.skey),
-                                                  as<unsigned long long>(W.lkey2), (int)ns, 0, 2 * b, s));
+            PP_TRY(radix_sort_keys(W.scratch.p, W.scratch.bytes, as<unsigned long long>(W.skey),
+                                   as<unsigned long long>(W.lkey2), ns, 0, 2 * b, s));
             PP_TRY(grow(W.sdeg, sizeof(unsigned long long) * ns));
             PP_TRY(grow(W.shead, sizeof(unsigned int) * ns));
             PP_TRY(grow(W.soff, sizeof(unsigned long long) * ns));
@@ -1142,11 +1123,10 @@ cudaError_t post_run(PostWork& W, PostRun& R, cudaStream_t s) {
                                                                           as<unsigned int>(W.deg),
                                                                           as<unsigned long long>(W.sdeg),
                                                                           as<unsigned int>(W.shead));
-            tt = W.cub.bytes;
-            PP_TRY(cub::DeviceScan::ExclusiveSum(W.cub.p, tt, as<unsigned long long>(W.sdeg), as<unsigned long long>(W.soff),
-                                                 (int)ns, s));
-            tt = W.cub.bytes;
-            PP_TRY(cub::DeviceScan::InclusiveSum(W.cub.p, tt, as<unsigned int>(W.shead), as<unsigned int>(W.sgid), (int)ns, s));
+            PP_TRY(exclusive_sum(W.scratch.p, W.scratch.bytes, as<unsigned long long>(W.sdeg),
+                                 as<unsigned long long>(W.soff), ns, s));
+            PP_TRY(inclusive_sum(W.scratch.p, W.scratch.bytes, as<unsigned int>(W.shead),
+                                 as<unsigned int>(W.sgid), ns, s));
             PP_TRY(grow(W.succ, sizeof(int) * nvw));
             k_tops<<<grid_for(nvw, kThreads, sms), kThreads, 0, s>>>(as<unsigned int>(W.bot), as<unsigned int>(W.deg),
                                                                      as<unsigned long long>(W.key2), b, nvw,
@@ -1210,14 +1190,12 @@ cudaError_t post_run(PostWork& W, PostRun& R, cudaStream_t s) {
             PP_TRY(grow(W.lorder, sizeof(int) * nbk));
             {
                 size_t ta = 0;
-                cub::DeviceSelect::Flagged(nullptr, ta, thrust::counting_iterator<int>(0), (unsigned char*)nullptr,
-                                           (int*)nullptr, (unsigned long long*)nullptr, (int)nbk, s);
-                PP_TRY(grow(W.cub, ta));
+                ta = select_temp_bytes(nbk);
+                PP_TRY(grow(W.scratch, ta));
             }
             PP_TRY(cudaMemsetAsync(&C->nsel, 0, sizeof(unsigned long long), s));
-            tt = W.cub.bytes;
-            PP_TRY(cub::DeviceSelect::Flagged(W.cub.p, tt, thrust::counting_iterator<int>(0), as<unsigned char>(W.lflag),
-                                              as<int>(W.lpos), &C->nsel, (int)nbk, s));
+            PP_TRY(select_flagged_index(W.scratch.p, W.scratch.bytes, as<unsigned char>(W.lflag),
+                                        as<int>(W.lpos), &C->nsel, (int)nbk, s));
             e = read_counters(W, R, s);
             if (e != cudaSuccess) return e;
             R.err = host_counters(W).err;
@@ -1233,16 +1211,13 @@ cudaError_t post_run(PostWork& W, PostRun& R, cudaStream_t s) {
                                                                             nloops, as<unsigned long long>(W.key));
         {
             size_t ta = 0, tb2 = 0;
-            cub::DeviceRadixSort::SortPairs(nullptr, ta, (unsigned long long*)nullptr, (unsigned long long*)nullptr,
-                                            (int*)nullptr, (int*)nullptr, (int)nloops, 0, 64, s);
-            cub::DeviceScan::ExclusiveSum(nullptr, tb2, (unsigned long long*)nullptr, (unsigned long long*)nullptr,
-                                          (int)nloops, s);
-            PP_TRY(grow(W.cub, std::max(ta, tb2)));
+            ta = radix_sort_temp_bytes(nloops, 8, true);
+            tb2 = scan_temp_bytes(nloops);
+            PP_TRY(grow(W.scratch, std::max(ta, tb2)));
         }
         PP_TRY(grow(W.lkey2, sizeof(unsigned long long) * nloops));
-        tt = W.cub.bytes;
-        PP_TRY(cub::DeviceRadixSort::SortPairs(W.cub.p, tt, as<unsigned long long>(W.key), as<unsigned long long>(W.lkey2),
-                                               as<int>(W.lpos), as<int>(W.lorder), (int)nloops, 0, 64, s));
+        PP_TRY(radix_sort_pairs(W.scratch.p, W.scratch.bytes, as<unsigned long long>(W.key),
+                                as<unsigned long long>(W.lkey2), as<uint32_t>(W.lpos), as<uint32_t>(W.lorder), nloops, 0, 64, s));
         PP_TRY(grow(W.nvl, sizeof(unsigned long long) * nloops));
         PP_TRY(grow(W.nfl, sizeof(unsigned long long) * nloops));
         PP_TRY(grow(W.vb, sizeof(unsigned long long) * nloops));
@@ -1266,12 +1241,10 @@ cudaError_t post_run(PostWork& W, PostRun& R, cudaStream_t s) {
         const unsigned fg = (unsigned)std::min<long long>(nloops, (long long)sms * 2);
         k_fill<false><<<fg, kFillThreads, smem, s>>>(fp);
         PP_TRY(cudaGetLastError());
-        tt = W.cub.bytes;
-        PP_TRY(cub::DeviceScan::ExclusiveSum(W.cub.p, tt, as<unsigned long long>(W.nvl), as<unsigned long long>(W.vb),
-                                             (int)nloops, s));
-        tt = W.cub.bytes;
-        PP_TRY(cub::DeviceScan::ExclusiveSum(W.cub.p, tt, as<unsigned long long>(W.nfl), as<unsigned long long>(W.fb),
-                                             (int)nloops, s));
+        PP_TRY(exclusive_sum(W.scratch.p, W.scratch.bytes, as<unsigned long long>(W.nvl),
+                             as<unsigned long long>(W.vb), nloops, s));
+        PP_TRY(exclusive_sum(W.scratch.p, W.scratch.bytes, as<unsigned long long>(W.nfl),
+                             as<unsigned long long>(W.fb), nloops, s));
         k_fill_totals<<<1, 32, 0, s>>>(as<unsigned long long>(W.vb), as<unsigned long long>(W.nvl),
                                        as<unsigned long long>(W.fb), as<unsigned long long>(W.nfl), nloops, C);
         e = read_counters(W, R, s);
@@ -1320,16 +1293,15 @@ cudaError_t post_run(PostWork& W, PostRun& R, cudaStream_t s) {
     PP_TRY(grow(dstF, sizeof(int32_t) * nA));
     {
         size_t ta = 0;
-        cub::DeviceScan::ExclusiveSum(nullptr, ta, (unsigned int*)nullptr, (unsigned int*)nullptr, (int)nA, s);
-        PP_TRY(grow(W.cub, ta));
+        ta = scan_temp_bytes(nA);
+        PP_TRY(grow(W.scratch, ta));
     }
     FaceList A;
     A.kept = kept; A.nkept = nkept; A.fill = as<int4>(W.fillF);
     PP_TRY(cudaMemsetAsync(W.first.p, 0xff, sizeof(unsigned int) * nall, s));
     k_first_use<<<grid_for(nA, kThreads, sms), kThreads, 0, s>>>(A, nA, as<unsigned int>(W.first));
     k_first_flags<<<grid_for(nA, kThreads, sms), kThreads, 0, s>>>(A, nA, as<unsigned int>(W.first), as<unsigned int>(W.fflag));
-    tt = W.cub.bytes;
-    PP_TRY(cub::DeviceScan::ExclusiveSum(W.cub.p, tt, as<unsigned int>(W.fflag), as<unsigned int>(W.slot), (int)nA, s));
+    PP_TRY(exclusive_sum(W.scratch.p, W.scratch.bytes, as<unsigned int>(W.fflag), as<unsigned int>(W.slot), nA, s));
     k_renumber<<<grid_for(nA, kThreads, sms), kThreads, 0, s>>>(A, nA, as<unsigned int>(W.first), as<unsigned int>(W.fflag),
                                                                  as<unsigned int>(W.slot), as<float>(W.Vw), nvw,
                                                                  as<float>(W.fillV), as<float>(dstV), as<int32_t>(dstF), C);
