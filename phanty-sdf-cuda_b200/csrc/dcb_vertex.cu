@@ -41,11 +41,9 @@ namespace dcb {
 // set, else the cell's own trilinear normal at its sample. The average is a function of
 // the edge alone, so every cell sharing the edge computes the same value.
 // lo: global low endpoint; o1/o2: offset (0/1) of the low endpoint from the cell along d1/d2.
-template <int AXIS>
-__device__ __forceinline__ float3 edge_normal(const GridDesc& g, int3 lo, int o1, int o2, float s_lo, float s_hi,
-                                              float t_lo, float pu, float pv, float pw, const float cc[8],
-                                              const Widths& W, bool& ill) {
-    constexpr int axis = AXIS;
+__device__ float3 edge_normal(const GridDesc& g, int3 lo, int axis, int o1, int o2, float s_lo, float s_hi,
+                              float t_lo, float pu, float pv, float pw, const float cc[8],
+                              const Widths& W, bool& ill) {
     const int3 hi = add3(lo, axis, 1);
     const bool in0 = lo.x > 0 && lo.x < g.nx - 1 && lo.y > 0 && lo.y < g.ny - 1 && lo.z > 0 && lo.z < g.nz - 1;
     const bool in1 = hi.x > 0 && hi.x < g.nx - 1 && hi.y > 0 && hi.y < g.ny - 1 && hi.z > 0 && hi.z < g.nz - 1;
@@ -110,49 +108,6 @@ __device__ __forceinline__ float3 edge_normal(const GridDesc& g, int3 lo, int o1
     return normalized(acc);
 }
 
-// The Hermite normals of a cell's crossing edges along AXIS (edges 0,2,4,6 along x, 1,3,5,7
-// along y, 8..11 along z) and each edge's n . (p - centroid) term, into shared memory. With the
-// axis a compile-time constant, edge_normal's neighbour strides, width picks and gradient
-// components fold to constants, and the edge geometry comes from four constants.
-template <int AXIS>
-__device__ __forceinline__ void axis_normals(const GridDesc& g, int i, int j, int k, uint32_t hmask, const float c[8],
-                                             const Widths& W, float cu, float cv, float cw, float fy, float fz,
-                                             const float (&s_c)[8][128], const float (&s_t)[12][128],
-                                             float (&s_n)[4][12][128], int tid, bool& ill) {
-    uint32_t m4;                                   // bit q: the axis' q-th edge crosses
-    if (AXIS == 2) {
-        m4 = (hmask >> 8) & 15u;
-    } else {
-        const uint32_t h = hmask >> AXIS;
-        m4 = (h & 1u) | ((h >> 1) & 2u) | ((h >> 2) & 4u) | ((h >> 3) & 8u);
-    }
-    constexpr uint32_t G0 = edge_geo(AXIS == 2 ? 8 : AXIS), G1 = edge_geo(AXIS == 2 ? 9 : 2 + AXIS);
-    constexpr uint32_t G2 = edge_geo(AXIS == 2 ? 10 : 4 + AXIS), G3 = edge_geo(AXIS == 2 ? 11 : 6 + AXIS);
-    for (; m4; m4 &= m4 - 1) {
-        const int q = __ffs(m4) - 1;
-        const int e = AXIS == 2 ? 8 + q : 2 * q + AXIS;
-        const uint32_t geo = q == 0 ? G0 : (q == 1 ? G1 : (q == 2 ? G2 : G3));
-        const int lox = (geo >> 2) & 1, loy = (geo >> 3) & 1, loz = (geo >> 4) & 1;
-        const bool own_low = (geo >> 5) & 1;
-        const float s_lo = s_c[(geo >> 6) & 7][tid], s_hi = s_c[(geo >> 9) & 7][tid];
-        // this cell's own sample (pass 1): t in its own orientation
-        const float t = s_t[e][tid];
-        const float along = own_low ? t : 1.f - t;
-        const float t_lo = own_low ? t : lerp_t(s_lo, s_hi);
-        const float pu = AXIS == 0 ? along : (float)lox;
-        const float pv = AXIS == 1 ? along : (float)loy;
-        const float pw = AXIS == 2 ? along : (float)loz;
-        const int o1 = AXIS == 0 ? loy : lox, o2 = AXIS == 2 ? loy : loz;
-        const float3 n = edge_normal<AXIS>(g, make_int3(i + lox, j + loy, k + loz), o1, o2, s_lo, s_hi, t_lo, pu, pv, pw,
-                                           c, W, ill);
-        const float qx = pu - cu, qy = (pv - cv) * fy, qz = (pw - cw) * fz;
-        s_n[0][e][tid] = n.x;
-        s_n[1][e][tid] = n.y;
-        s_n[2][e][tid] = n.z;
-        s_n[3][e][tid] = n.x * qx + n.y * qy + n.z * qz;
-    }
-}
-
 // ---- k_cell_qef -------------------------------------------------------------------------
 
 template <bool ONE>
@@ -161,7 +116,6 @@ k_cell_qef(const __grid_constant__ QefParams P) {
     __shared__ unsigned int s_hist;
     __shared__ float s_c[8][128];    // per-thread corner values (dynamically indexed)
     __shared__ float s_t[12][128];   // per-thread lerp parameter of each crossing edge
-    __shared__ float s_n[4][12][128];   // per-thread normal of each crossing edge and its n . (p - c)
     const int tid = threadIdx.x;
     if (tid == 0) s_hist = 0;
     __syncthreads();
@@ -220,19 +174,31 @@ k_cell_qef(const __grid_constant__ QefParams P) {
         cell_widths(g, i, j, k, W);
         const float fy = W.w[1][1] * W.r[0][1], fz = W.w[2][1] * W.r[0][1];
 
-        // Pass 2: each lane walks its own crossing edges an axis at a time (warp iterations =
-        // max count per axis) for the normals, then sums the rows of the normal equations in
-        // edge order with Kahan compensation.
-        bool ill = false;
-        axis_normals<0>(g, i, j, k, hmask, c, W, cu, cv, cw, fy, fz, s_c, s_t, s_n, tid, ill);
-        axis_normals<1>(g, i, j, k, hmask, c, W, cu, cv, cw, fy, fz, s_c, s_t, s_n, tid, ill);
-        axis_normals<2>(g, i, j, k, hmask, c, W, cu, cv, cw, fy, fz, s_c, s_t, s_n, tid, ill);
+        // Pass 2: each lane walks its own crossing edges (warp iterations = max count).
         float M00 = 0, M01 = 0, M02 = 0, M11 = 0, M12 = 0, M22 = 0, R0 = 0, R1 = 0, R2 = 0;
         float K00 = 0, K01 = 0, K02 = 0, K11 = 0, K12 = 0, K22 = 0, Q0 = 0, Q1 = 0, Q2 = 0;
-        for (uint32_t rem = hmask; rem; rem &= rem - 1) {
+        bool ill = false;
+        uint32_t rem = hmask;
+        while (rem) {
             const int e = __ffs(rem) - 1;
-            const float3 n = make_float3(s_n[0][e][tid], s_n[1][e][tid], s_n[2][e][tid]);
-            const float nb = s_n[3][e][tid];
+            rem &= rem - 1;
+            const uint32_t geo = c_edge_geo[e];
+            const int axis = geo & 3;
+            const int lox = (geo >> 2) & 1, loy = (geo >> 3) & 1, loz = (geo >> 4) & 1;
+            const bool own_low = (geo >> 5) & 1;
+            const float s_lo = s_c[(geo >> 6) & 7][tid], s_hi = s_c[(geo >> 9) & 7][tid];
+            // this cell's own sample (pass 1): t in its own orientation
+            const float t = s_t[e][tid];
+            const float along = own_low ? t : 1.f - t;
+            const float t_lo = own_low ? t : lerp_t(s_lo, s_hi);
+            const float pu = axis == 0 ? along : (float)lox;
+            const float pv = axis == 1 ? along : (float)loy;
+            const float pw = axis == 2 ? along : (float)loz;
+            const int o1 = axis == 0 ? loy : lox, o2 = axis == 2 ? loy : loz;
+            const float3 n = edge_normal(g, make_int3(i + lox, j + loy, k + loz), axis, o1, o2, s_lo, s_hi, t_lo,
+                                         pu, pv, pw, c, W, ill);
+            const float qx = pu - cu, qy = (pv - cv) * fy, qz = (pw - cw) * fz;
+            const float nb = n.x * qx + n.y * qy + n.z * qz;
             kahan_add(M00, K00, n.x * n.x); kahan_add(M01, K01, n.x * n.y); kahan_add(M02, K02, n.x * n.z);
             kahan_add(M11, K11, n.y * n.y); kahan_add(M12, K12, n.y * n.z); kahan_add(M22, K22, n.z * n.z);
             kahan_add(R0, Q0, n.x * nb); kahan_add(R1, Q1, n.y * nb); kahan_add(R2, Q2, n.z * nb);
