@@ -31,18 +31,6 @@
 namespace dcb {
 
 // Small device-side counters, cleared at the start of every extraction.
-// z-slabs of the single-grid pipeline (run_slabs), at most
-constexpr int kMaxSlabs = 16;
-#ifndef DCB_DEFAULT_SLABS
-#define DCB_DEFAULT_SLABS 8
-#endif
-#ifndef DCB_SLAB_MARK_SMEM
-#define DCB_SLAB_MARK_SMEM 0
-#endif
-#ifndef DCB_SLAB_WAVES
-#define DCB_SLAB_WAVES 2
-#endif
-
 struct Counters {
     int err;
     unsigned int esc_count;
@@ -54,7 +42,6 @@ struct Counters {
     unsigned long long rank_hist[4];
     unsigned long long face_total;
     int nonfinite;                    // the mark met a NaN or infinite grid value
-    unsigned long long slab_total[kMaxSlabs];   // active cells of z-slabs 0..s (run_slabs)
 };
 
 struct DevBuf {
@@ -99,15 +86,6 @@ struct dcb_context {
     // (cells along x) that marches 256-cell x-tiles instead of 1024-cell ones
     int tune_waves = 4;
     int tune_narrow_cells = 256;
-    // z-slab pipeline of single-grid extractions (run_slabs): the slab count, the dynamic
-    // shared memory of a slab's mark CTAs (it bounds them per SM, leaving room for the vertex
-    // kernel beside them), mark waves per slab, the stream that runs each slab's ranks and
-    // vertices behind the next slab's mark, the events between them
-    int tune_slabs = DCB_DEFAULT_SLABS;
-    int tune_slab_mark_smem = DCB_SLAB_MARK_SMEM;
-    int tune_slab_waves = DCB_SLAB_WAVES;
-    cudaStream_t aux = nullptr;
-    cudaEvent_t slab_ev[kMaxSlabs + 1] = {};
     int cx = 0, cy = 0, cz = 0;
     // batch layout table (device + pinned staging) and the last batch's per-grid offsets
     DevBuf table, cell_slot;
@@ -230,9 +208,7 @@ struct BatchLayout {
     float hmax = 0.f;
 };
 
-// slabs > 1: a single grid marched as that many z-slabs (run_slabs); its z-chunks are cut so
-// that each slab's mark launch holds tune_slab_waves waves of CTAs.
-int layout_batch(dcb_context* h, const dcb_grid* in, int n, BatchLayout& L, int slabs = 0) {
+int layout_batch(dcb_context* h, const dcb_grid* in, int n, BatchLayout& L) {
     L.slots.resize(n);
     L.seg_off.assign(n + 1, 0);
     L.col_off.assign(n + 1, 0);
@@ -257,9 +233,7 @@ int layout_batch(dcb_context* h, const dcb_grid* in, int n, BatchLayout& L, int 
         // measured slower at 1024^3: 0.887 vs 0.848 ms).
         if (h->mark_ctas[n == 1] == 0) h->mark_ctas[n == 1] = mark_ctas_per_sm(n == 1);
         const long long slots = (long long)h->num_sms * h->mark_ctas[n == 1] * h->tune_waves;
-        const long long per_kz = (n == 1 && slabs > 1)
-                                     ? (long long)h->num_sms * h->mark_ctas[1] * h->tune_slab_waves * slabs : slots;
-        S.KZ = (int)std::max(8LL, std::min(64LL, (g.cz * S.nxt * (long long)S.nrb + per_kz - 1) / per_kz));
+        S.KZ = (int)std::max(8LL, std::min(64LL, (g.cz * S.nxt * (long long)S.nrb + slots - 1) / slots));
         S.nzc = (g.cz + S.KZ - 1) / S.KZ;
         S.bits_off = L.bits;
         S.super_off = L.super;
@@ -380,9 +354,8 @@ int launch_marks(dcb_context* h, const BatchLayout& L, const TableView& T, cudaS
 // ev[1] must already be recorded. Vertices are numbered over the whole batch while running;
 // for n > 1 the faces are rebased to their own grid's vertices at the end.
 // Layout, table upload and the buffers whose sizes do not depend on the active count.
-int batch_prepare(dcb_context* h, const dcb_grid* in, int n, cudaStream_t s, BatchLayout& L, TableView& T,
-                  int slabs = 0) {
-    int rc = layout_batch(h, in, n, L, slabs);
+int batch_prepare(dcb_context* h, const dcb_grid* in, int n, cudaStream_t s, BatchLayout& L, TableView& T) {
+    int rc = layout_batch(h, in, n, L);
     if (rc != DCB_OK) return rc;
     rc = upload_table(h, L, s, T);
     if (rc != DCB_OK) return rc;
@@ -469,31 +442,30 @@ void batch_state(dcb_context* h, const BatchLayout& L, int n, const dcb_opts* o,
     for (int b = 0; b <= n; ++b) h->vert_offsets[b] = (int64_t)h_vert_off[b];
 }
 
-// Per-call zeroing of the column counts and fills and the FP64 vertex slots.
-int batch_clear(dcb_context* h, const BatchLayout& L, cudaStream_t s, long long cap) {
-    DCB_TRY(h, cudaMemsetAsync(h->col_count.p, 0, sizeof(uint32_t) * L.ncol, s), "memset");
-    DCB_TRY(h, cudaMemsetAsync(h->col_fill.p, 0, sizeof(uint32_t) * L.ncol, s), "memset");
-    DCB_TRY(h, cudaMemsetAsync(h->v64_index.p, 0xff, sizeof(int) * cap, s), "memset");
-    return DCB_OK;
-}
-
-ExpandParams expand_params(dcb_context* h, const BatchLayout& L, const TableView& T, long long cap) {
+// Everything after the mark for up to `cap` active cells: ranks and list, vertices, faces.
+// With `live` (a device count, as in a captured graph) the kernels take the active count from
+// there, bounded by cap; otherwise it is cap.
+int batch_rest(dcb_context* h, const BatchLayout& L, TableView& T, const dcb_opts* o, cudaStream_t s, long long cap,
+               const unsigned long long* live, bool events) {
     const int n = (int)L.slots.size();
+    const long long nseg = L.nseg, ncol = L.ncol;
+    Counters* dc = as<Counters>(h->counters);
+    const long long wind_cap = std::min(0x7fffffffLL, 3 * cap);
+    const long long v64_cap = cap;
+    DCB_TRY(h, cudaMemsetAsync(h->col_count.p, 0, sizeof(uint32_t) * ncol, s), "memset");
+    DCB_TRY(h, cudaMemsetAsync(h->col_fill.p, 0, sizeof(uint32_t) * ncol, s), "memset");
+    DCB_TRY(h, cudaMemsetAsync(h->v64_index.p, 0xff, sizeof(int) * cap, s), "memset");
+
+    // 2) ranks + list, QEF with fused edge normals (rank-1 fast path, Jacobi list, FP64).
     ExpandParams xp;
-    xp.B = T.B; xp.nseg = L.nseg; xp.bits = as<uint32_t>(h->bits); xp.seg_count = as<uint32_t>(h->seg_count);
+    xp.B = T.B; xp.nseg = nseg; xp.bits = as<uint32_t>(h->bits); xp.seg_count = as<uint32_t>(h->seg_count);
     xp.seg_start = as<uint32_t>(h->seg_start); xp.super = as<uint32_t>(h->super); xp.list = as<uint64_t>(h->list);
     xp.cell_slot = n > 1 ? as<uint32_t>(h->cell_slot) : nullptr;
     xp.B.cell_slot = nullptr;                      // expand finds grids by segment
     xp.list_cap = cap;
-    return xp;
-}
-
-QefParams qef_params(dcb_context* h, const TableView& T, const dcb_opts* o, long long cap,
-                     const unsigned long long* live) {
-    Counters* dc = as<Counters>(h->counters);
+    DCB_TRY(h, launch_expand(xp, h->num_sms, s), "launch expand");
     QefParams qp;
-    qp.B = T.B; qp.list = as<uint64_t>(h->list); qp.nactive = cap; qp.live = live; qp.V = as<float>(h->V);
-    qp.vclass = as<uint8_t>(h->vclass);
+    qp.B = T.B; qp.list = xp.list; qp.nactive = cap; qp.live = live; qp.V = as<float>(h->V); qp.vclass = as<uint8_t>(h->vclass);
     qp.fmask = as<uint8_t>(h->fmask); qp.col_count = as<uint32_t>(h->col_count);
     qp.esc_list = as<uint32_t>(h->esc_list); qp.esc_count = &dc->esc_count;
     qp.hard_list = as<uint32_t>(h->hard_list); qp.hard_data = as<float4>(h->hard_data); qp.hard_count = &dc->hard_count;
@@ -502,38 +474,7 @@ QefParams qef_params(dcb_context* h, const TableView& T, const dcb_opts* o, long
     qp.nonfinite = &dc->nonfinite;
     qp.thr = (float)o->svd_threshold; qp.band = (float)o->fp64_threshold_band;
     qp.cond_max = (float)std::min(o->fp64_escalation_cond, 3.0e38); qp.force64 = o->force_fp64;
-    return qp;
-}
-
-// Everything after the vertices' FP32 pass for up to `cap` active cells: Jacobi and FP64
-// vertices, faces. With `live` (a device count) the kernels take the active count from there,
-// bounded by cap; otherwise it is cap.
-int batch_tail(dcb_context* h, const BatchLayout& L, TableView& T, const dcb_opts* o, cudaStream_t s, long long cap,
-               const unsigned long long* live, bool events);
-
-// Everything after the mark for up to `cap` active cells: ranks and list, vertices, faces.
-// With `live` (a device count, as in a captured graph) the kernels take the active count from
-// there, bounded by cap; otherwise it is cap.
-int batch_rest(dcb_context* h, const BatchLayout& L, TableView& T, const dcb_opts* o, cudaStream_t s, long long cap,
-               const unsigned long long* live, bool events) {
-    int rc = batch_clear(h, L, s, cap);
-    if (rc != DCB_OK) return rc;
-    // 2) ranks + list, QEF with fused edge normals (rank-1 fast path, Jacobi list, FP64).
-    const ExpandParams xp = expand_params(h, L, T, cap);
-    DCB_TRY(h, launch_expand(xp, h->num_sms, s), "launch expand");
-    DCB_TRY(h, launch_cell_qef(qef_params(h, T, o, cap, live), h->num_sms, s), "launch qef");
-    return batch_tail(h, L, T, o, s, cap, live, events);
-}
-
-int batch_tail(dcb_context* h, const BatchLayout& L, TableView& T, const dcb_opts* o, cudaStream_t s, long long cap,
-               const unsigned long long* live, bool events) {
-    const int n = (int)L.slots.size();
-    const long long ncol = L.ncol;
-    Counters* dc = as<Counters>(h->counters);
-    const long long wind_cap = std::min(0x7fffffffLL, 3 * cap);
-    const long long v64_cap = cap;
-    const ExpandParams xp = expand_params(h, L, T, cap);
-    const QefParams qp = qef_params(h, T, o, cap, live);
+    DCB_TRY(h, launch_cell_qef(qp, h->num_sms, s), "launch qef");
     DCB_TRY(h, launch_cell_jacobi(qp, cap, h->num_sms, s), "launch jacobi");
     Vertex64Params v64;
     v64.B = T.B; v64.list = xp.list; v64.cells = qp.esc_list; v64.count = &dc->esc_count; v64.cap = (unsigned int)cap;
@@ -632,142 +573,12 @@ int batch_finish(dcb_context* h, int n, const dcb_opts* o, dcb_stats* st) {
     return DCB_OK;
 }
 
-// Active cells every per-cell buffer of the workspace holds (0 before the first extraction).
-long long cell_capacity(const dcb_context* h, const dcb_opts* o) {
-    long long c = (long long)(h->list.bytes / sizeof(uint64_t));
-    auto lim = [&c](const DevBuf& b, size_t per) { c = std::min(c, (long long)(b.bytes / per)); };
-    lim(h->V, 3 * sizeof(float)); lim(h->fmask, 1); lim(h->vclass, 1);
-    lim(h->esc_list, sizeof(uint32_t)); lim(h->hard_list, sizeof(uint32_t)); lim(h->hard_data, 3 * sizeof(float4));
-    lim(h->stage_quad, 3 * sizeof(int4)); lim(h->stage_key, 3 * sizeof(uint2)); lim(h->faces, 3 * sizeof(int4));
-    lim(h->v64_index, sizeof(int)); lim(h->wind_items, 3 * sizeof(uint4)); lim(h->v64_cells, sizeof(uint32_t));
-    lim(h->V64, 3 * sizeof(double));
-    if (o->emit_triangles) { lim(h->tris, 18 * sizeof(int)); lim(h->tri_items, 3 * sizeof(uint32_t)); }
-    return std::min(c, 0x7fffffffLL / 3);      // the winding list holds exactly 3 entries per cell
-}
-
-// One grid as a z-slab pipeline. Slab s (a run of the mark's z-chunks) is marked on the
-// caller's stream; a second, higher-priority stream then scans its segments (carrying the
-// active count of the slabs before it), writes their super ranks and cell list and runs the
-// FP32 vertex kernel on its cells, while the caller's stream marks slab s+1: the vertex work,
-// bound by latency and issue, runs beside the HBM-bound mark. Faces follow once every slab is
-// done. No host synchronisation until the end: the buffers are those of an earlier call
-// (their capacity in active cells); a grid with more active cells is finished on the exact
-// path once its count is known. done = false: the slab path does not apply.
-int run_slabs(dcb_context* h, const BatchLayout& L, TableView& T, const dcb_opts* o, cudaStream_t s, dcb_stats* st,
-              bool& done) {
-    done = false;
-    if (L.slots.size() != 1) return DCB_OK;
-    const GridSlot& S = L.slots[0];
-    const GridDesc& g = S.g;
-    const long long cap = cell_capacity(h, o);
-    const int nsl = (int)std::min<long long>(std::min<long long>(h->tune_slabs, S.nzc), kMaxSlabs);
-    if (nsl < 2 || cap <= 0) return DCB_OK;
-    if (!h->aux) {
-        int least = 0, greatest = 0;
-        DCB_TRY(h, cudaDeviceGetStreamPriorityRange(&least, &greatest), "stream priorities");
-        DCB_TRY(h, cudaStreamCreateWithPriority(&h->aux, cudaStreamNonBlocking, greatest), "create stream");
-    }
-    for (auto& e : h->slab_ev)
-        if (!e) DCB_TRY(h, cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "create event");
-    done = true;
-    Counters* dc = as<Counters>(h->counters);
-    Counters* hc = reinterpret_cast<Counters*>(h->h_counters);
-    unsigned long long* h_vert_off = reinterpret_cast<unsigned long long*>(h->h_offsets);
-    cudaEvent_t fork = h->slab_ev[kMaxSlabs];
-    DCB_TRY(h, cudaMemsetAsync(h->counters.p, 0, sizeof(Counters), s), "memset counters");
-    int rc = batch_clear(h, L, s, cap);
-    if (rc != DCB_OK) return rc;
-    DCB_TRY(h, cudaEventRecord(fork, s), "event");
-    DCB_TRY(h, cudaStreamWaitEvent(h->aux, fork, 0), "wait");
-
-    const int v = S.tw == mark_narrow_tile_words() ? 1 : 0;
-    MarkParams mp;
-    mp.B = T.B; mp.tile_slot = T.tile_slot[v]; mp.tile_off = T.tile_off[v]; mp.m = 1;
-    mp.bits = as<uint32_t>(h->bits); mp.seg_count = as<uint32_t>(h->seg_count); mp.nonfinite = &dc->nonfinite;
-    ExpandParams xp = expand_params(h, L, T, cap);
-    QefParams qp = qef_params(h, T, o, cap, nullptr);
-    const long long tiles_per_chunk = (long long)S.nxt * S.nrb;    // tiles: x-tile fastest, z-chunk slowest
-    const long long segs_per_plane = (long long)g.cy * S.nxt;      // segments: (plane, row, x-tile)
-    const int64_t plane = (int64_t)g.nx * g.ny;
-    for (int sl = 0; sl < nsl; ++sl) {
-        const long long c0 = (long long)S.nzc * sl / nsl, c1 = (long long)S.nzc * (sl + 1) / nsl;
-        const long long k0 = c0 * S.KZ, k1 = std::min<long long>(g.cz, c1 * S.KZ);   // cell planes
-        mp.kb0 = (int)k0;
-        mp.ntiles = (c1 - c0) * tiles_per_chunk;
-        DCB_TRY(h, launch_mark(mp, v ? mark_narrow_tile_words() : mark_tile_words(), s, h->tune_slab_mark_smem),
-                "launch mark");
-        // the mark read point planes k0..k1; the slab's normal stencils also reach k1 + 1, and a
-        // non-finite value there must send its cells to the FP64 path before they are solved
-        if (k1 + 1 < g.nz)
-            DCB_TRY(h, launch_check_finite(g.v + (k1 + 1) * plane, plane, &dc->nonfinite, h->num_sms, s), "check plane");
-        DCB_TRY(h, cudaEventRecord(h->slab_ev[sl], s), "event");
-        DCB_TRY(h, cudaStreamWaitEvent(h->aux, h->slab_ev[sl], 0), "wait");
-        const long long seg0 = k0 * segs_per_plane, nseg = (k1 - k0) * segs_per_plane;
-        unsigned long long* total = sl + 1 < nsl ? &dc->slab_total[sl] : &dc->total_active;
-        const unsigned long long* before = sl ? &dc->slab_total[sl - 1] : nullptr;
-        DCB_TRY(h, launch_scan(as<uint32_t>(h->seg_count) + seg0, nseg, as<uint32_t>(h->partials),
-                               as<uint32_t>(h->seg_start) + seg0, total, h->aux, before), "launch segment scan");
-        xp.seg0 = seg0;
-        xp.nseg = nseg;
-        DCB_TRY(h, launch_expand(xp, h->num_sms, h->aux), "launch expand");
-        qp.first = before;
-        qp.live = total;
-        DCB_TRY(h, launch_cell_qef(qp, h->num_sms, h->aux), "launch qef");
-    }
-    // stage times on the critical path: the marking ends with the last slab's mark; what the
-    // vertex stage adds is the slab work still running after it
-    DCB_TRY(h, cudaEventRecord(h->ev[6], s), "event");
-    DCB_TRY(h, cudaEventRecord(h->ev[2], s), "event");
-    DCB_TRY(h, cudaEventRecord(fork, h->aux), "event");
-    DCB_TRY(h, cudaStreamWaitEvent(s, fork, 0), "wait");
-    DCB_TRY(h, launch_vert_offsets(T.B, as<uint32_t>(h->seg_start), &dc->total_active, T.vert_off, s), "vertex offsets");
-    rc = batch_tail(h, L, T, o, s, cap, &dc->total_active, true);
-    if (rc != DCB_OK) return rc;
-    DCB_TRY(h, cudaEventRecord(h->ev[4], s), "event");
-    DCB_TRY(h, cudaMemcpyAsync(hc, dc, sizeof(Counters), cudaMemcpyDeviceToHost, s), "read counters");
-    DCB_TRY(h, cudaMemcpyAsync(h_vert_off, T.vert_off, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s),
-            "read vertex offsets");
-    DCB_TRY(h, cudaStreamSynchronize(s), "pipeline");
-    const long long nv = (long long)hc->total_active;
-    if (nv >= 0x7fffffffLL) return fail(h, DCB_ERR_TOO_LARGE, "more than 2^31-1 vertices");
-    batch_state(h, L, 1, o, nv);
-    if (st) {
-        st->nx = g.nx; st->ny = g.ny; st->nz = g.nz;
-        st->total_cells = L.ncell; st->active_cells = nv; st->vertex_count = nv;
-    }
-    if (nv > cap) {
-        // more active cells than the buffers hold (the kernels past the mark left the cells at
-        // or above cap alone): the marks, counts and segment ranks stand; everything after
-        // them runs again with buffers for nv cells
-        const Counters keep = *hc;
-        std::memset(hc, 0, sizeof(Counters));
-        hc->total_active = keep.total_active;
-        hc->nonfinite = keep.nonfinite;
-        DCB_TRY(h, cudaMemcpyAsync(dc, hc, sizeof(Counters), cudaMemcpyHostToDevice, s), "reset counters");
-        rc = batch_alloc(h, 1, nv, o, T);
-        if (rc != DCB_OK) return rc;
-        rc = batch_rest(h, L, T, o, s, nv, nullptr, true);
-        if (rc != DCB_OK) return rc;
-        DCB_TRY(h, cudaEventRecord(h->ev[4], s), "event");
-        DCB_TRY(h, cudaMemcpyAsync(hc, dc, sizeof(Counters), cudaMemcpyDeviceToHost, s), "read counters");
-        DCB_TRY(h, cudaStreamSynchronize(s), "pipeline");
-    }
-    return batch_finish(h, 1, o, st);
-}
-
 int run_batch(dcb_context* h, const dcb_grid* in, int n, const dcb_opts* o, cudaStream_t s, dcb_stats* st) {
     ++h->gen;
     BatchLayout L;
     TableView T;
-    // a single grid on the buffers of an earlier call runs as z-slabs (run_slabs)
-    const int slabs = (n == 1 && cell_capacity(h, o) > 0) ? h->tune_slabs : 0;
-    int rc = batch_prepare(h, in, n, s, L, T, slabs);
+    int rc = batch_prepare(h, in, n, s, L, T);
     if (rc != DCB_OK) return rc;
-    if (slabs > 1) {
-        bool done = false;
-        rc = run_slabs(h, L, T, o, s, st, done);
-        if (rc != DCB_OK || done) return rc;
-    }
     Counters* dc = as<Counters>(h->counters);
     Counters* hc = reinterpret_cast<Counters*>(h->h_counters);
     unsigned long long* h_vert_off = reinterpret_cast<unsigned long long*>(h->h_offsets);
@@ -1314,8 +1125,6 @@ int dcb_destroy(dcb_handle h) {
     if (h->hV) cudaFreeHost(h->hV);
     if (h->hF) cudaFreeHost(h->hF);
     for (auto& ev : h->ev) if (ev) cudaEventDestroy(ev);
-    for (auto& ev : h->slab_ev) if (ev) cudaEventDestroy(ev);
-    if (h->aux) cudaStreamDestroy(h->aux);
     delete h;
     return DCB_OK;
 }

@@ -59,10 +59,9 @@ k_scan_partials(const uint32_t* __restrict__ in, long long n, uint32_t* partials
 }
 
 __global__ void __launch_bounds__(kScanThreads)
-k_scan_single(uint32_t* partials, long long nb, unsigned long long* grand_total,
-              const unsigned long long* __restrict__ carry_in) {
+k_scan_single(uint32_t* partials, long long nb, unsigned long long* grand_total) {
     __shared__ uint32_t s_warp[kScanThreads / 32];
-    uint32_t carry = carry_in ? (uint32_t)*carry_in : 0u;
+    uint32_t carry = 0;
     for (long long c0 = 0; c0 < nb; c0 += kScanThreads) {
         const long long idx = c0 + threadIdx.x;
         const uint32_t v = idx < nb ? partials[idx] : 0u;
@@ -92,14 +91,12 @@ k_scan_apply(const uint32_t* __restrict__ in, long long n, const uint32_t* __res
     }
 }
 
-// Exclusive scan of n counts; the total goes to grand_total. With carry_in (a device value
-// below 2^32) every output and the total start from it.
 cudaError_t launch_scan(const uint32_t* in, long long n, uint32_t* partials, uint32_t* out,
-                        unsigned long long* grand_total, cudaStream_t s, const unsigned long long* carry_in) {
+                        unsigned long long* grand_total, cudaStream_t s) {
     const long long nb = (n + kScanTile - 1) / kScanTile;
     if (nb <= 0) return cudaSuccess;
     k_scan_partials<<<(unsigned)nb, kScanThreads, 0, s>>>(in, n, partials);
-    k_scan_single<<<1, kScanThreads, 0, s>>>(partials, nb, grand_total, carry_in);
+    k_scan_single<<<1, kScanThreads, 0, s>>>(partials, nb, grand_total);
     k_scan_apply<<<(unsigned)nb, kScanThreads, 0, s>>>(in, n, partials, out);
     return cudaGetLastError();
 }
@@ -237,11 +234,9 @@ k_face_scatter(const __grid_constant__ FaceParams P) {
     __shared__ uint8_t s_item[kFaceThreads / 32][96];
     const int lane = threadIdx.x & 31, wb = threadIdx.x >> 5;
     const long long stride = (long long)gridDim.x * blockDim.x;
-    // with a device count of active cells above the capacity the buffers were sized for (a
-    // captured graph, or a z-slab pipeline on an earlier call's buffers), the cells below the
-    // capacity are processed, every kernel alike (their faces only reach lower ranks); the
-    // host reports the overflow or runs the grid again
-    const long long nact = P.live ? std::min((long long)*P.live, P.nactive) : P.nactive;
+    // a captured graph whose live count exceeds the capacity it was built for does nothing
+    // (the host reports the overflow after the replay)
+    const long long nact = P.live ? ((long long)*P.live > P.nactive ? 0 : (long long)*P.live) : P.nactive;
     for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x - lane); base < nact;
          base += stride) {                                                // warp-uniform
         const long long rr = base + lane;

@@ -75,10 +75,8 @@ struct MarkParams {
     uint32_t* bits;                // all grids' active bits
     uint32_t* seg_count;           // all grids' segment counts
     int* nonfinite;                // optional: set to 1 when a grid value is NaN or infinite
-    int kb0 = 0;                   // first cell plane of this launch (a z-slab of a single grid,
-                                   // whose tiles are numbered from it)
 };
-cudaError_t launch_mark(const MarkParams& P, int tw, cudaStream_t s, int smem_pad = 0);
+cudaError_t launch_mark(const MarkParams& P, int tw, cudaStream_t s);
 int mark_tile_words();
 int mark_narrow_tile_words();
 int mark_ctas_per_sm(bool one);   // resident CTAs of the mark kernel per SM (single grid / batch)
@@ -94,12 +92,10 @@ struct ExpandParams {
     uint64_t* list;                // [active] packed cells, grid-local coordinates
     uint32_t* cell_slot;           // [active] grid of every vertex (batches only; may be null)
     long long list_cap;            // entries of list / cell_slot; <= 0: sized for every active cell
-    long long seg0 = 0;            // first segment of this launch (a z-slab of a single grid)
 };
 cudaError_t launch_expand(const ExpandParams& P, int num_sms, cudaStream_t s);
 
 // vert_off[b] = seg_start[seg_off[b]] (b < n), vert_off[n] = total.
-cudaError_t launch_check_finite(const float* v, long long n, int* nonfinite, int num_sms, cudaStream_t s);
 cudaError_t launch_vert_offsets(const BatchTable& B, const uint32_t* seg_start, const unsigned long long* total,
                                 unsigned long long* vert_off, cudaStream_t s);
 // face_off[b] = col_start[col_off[b]] (b < n), face_off[n] = total.
@@ -117,10 +113,8 @@ struct QefParams {
     BatchTable B;
     const uint64_t* list;
     long long nactive;             // active cells (capacity when live is set)
-    const unsigned long long* live; // device count of active cells, or null (a captured graph or a
-                                    // z-slab; cells at or above nactive are not processed)
-    const unsigned long long* first = nullptr;  // device rank of the first cell to process (a
-                                    // z-slab: the active cells before it), or null for 0
+    const unsigned long long* live; // device count of active cells (a captured graph; above
+                                    // nactive, nothing is processed), or null
     float* V;
     uint8_t* vclass;                // [active] VertexClass
     uint8_t* fmask;                 // bit a: cell owns a face on its min-corner edge a
@@ -168,15 +162,15 @@ struct Winding64Params {
 cudaError_t launch_winding_fp64(const Winding64Params& P, long long max_items, int num_sms, cudaStream_t s);
 
 cudaError_t launch_scan(const uint32_t* in, long long n, uint32_t* partials, uint32_t* out,
-                        unsigned long long* grand_total, cudaStream_t s, const unsigned long long* carry_in = nullptr);
+                        unsigned long long* grand_total, cudaStream_t s);
 long long scan_partials_len(long long n);
 
 struct FaceParams {
     BatchTable B;
     const uint64_t* list;
     long long nactive;             // active cells (capacity when live is set)
-    const unsigned long long* live; // device count of active cells, or null (a captured graph or a
-                                    // z-slab; cells at or above nactive are not processed)
+    const unsigned long long* live; // device count of active cells (a captured graph; above
+                                    // nactive, nothing is processed), or null
     const uint8_t* fmask;
     const float* V;
     const uint8_t* vclass;

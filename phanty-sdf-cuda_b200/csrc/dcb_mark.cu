@@ -90,7 +90,7 @@ k_mark_zmarch(const __grid_constant__ MarkParams P) {
     const long long local = ONE ? tile : tile - P.tile_off[mi];
     const int xt = (int)(local % nxt);         // x-tile
     const int j0 = (int)((local / nxt) % S.nrb) * R;   // first cell row
-    const int kb = (int)(local / ((long long)nxt * S.nrb)) * KZ + P.kb0;   // first cell plane
+    const int kb = (int)(local / ((long long)nxt * S.nrb)) * KZ;   // first cell plane
     uint32_t* const bits = P.bits + S.bits_off;
     uint32_t* const seg_count = P.seg_count + S.seg_off;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -141,23 +141,6 @@ k_mark_zmarch(const __grid_constant__ MarkParams P) {
     if (__syncthreads_or(bad) && threadIdx.x == 0 && P.nonfinite) atomicOr(P.nonfinite, 1);
 }
 
-// Sets *nonfinite when one of n values is NaN or infinite: the point plane just past a z-slab,
-// which that slab's cells read in their normal stencils but its mark launch does not.
-__global__ void __launch_bounds__(256) k_check_finite(const float* __restrict__ v, long long n, int* nonfinite) {
-    bool bad = false;
-    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x)
-        bad |= !(fabsf(__ldg(v + q)) <= 3.402823466e38f);
-    if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(nonfinite, 1);
-}
-
-cudaError_t launch_check_finite(const float* v, long long n, int* nonfinite, int num_sms, cudaStream_t s) {
-    if (n <= 0) return cudaSuccess;
-    long long blocks = (n + 255) / 256;
-    if (blocks > (long long)num_sms * 8) blocks = (long long)num_sms * 8;
-    k_check_finite<<<(unsigned)blocks, 256, 0, s>>>(v, n, nonfinite);
-    return cudaGetLastError();
-}
-
 // Segments with at most this many active cells are expanded by one lane.
 constexpr uint32_t kLaneSegmentCells = 96;
 
@@ -168,12 +151,12 @@ template <bool ONE>
 __global__ void __launch_bounds__(256)
 k_expand_ranks(const __grid_constant__ ExpandParams P) {
     const int lane = threadIdx.x & 31;
-    const long long send = P.seg0 + P.nseg;       // segments [seg0, seg0 + nseg)
-    const long long ngroups = (P.nseg + 31) / 32;
+    const long long nseg = P.nseg;
+    const long long ngroups = (nseg + 31) / 32;
     for (long long grp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; grp < ngroups;
          grp += ((long long)gridDim.x * blockDim.x) >> 5) {
-        const long long s0 = P.seg0 + grp * 32;
-        const bool have = s0 + lane < send;
+        const long long s0 = grp * 32;
+        const bool have = s0 + lane < nseg;
         const uint32_t cnt = have ? P.seg_count[s0 + lane] : 0u;
         uint32_t live = __ballot_sync(0xffffffffu, cnt != 0);
         const uint32_t my_start = (have && cnt) ? P.seg_start[s0 + lane] : 0u;
@@ -276,22 +259,16 @@ cudaError_t launch_vert_offsets(const BatchTable& B, const uint32_t* seg_start, 
     return cudaGetLastError();
 }
 
-template <bool ONE, int TW>
-void launch_mark_t(const MarkParams& P, int pad, cudaStream_t s) {
-    // unused dynamic shared memory bounds the CTAs per SM (room for kernels running beside it)
-    if (pad > 0) cudaFuncSetAttribute(k_mark_zmarch<ONE, TW>, cudaFuncAttributeMaxDynamicSharedMemorySize, pad);
-    k_mark_zmarch<ONE, TW><<<(unsigned)P.ntiles, kMarkWarps * 32, pad > 0 ? pad : 0, s>>>(P);
+template <bool ONE>
+void launch_mark_tw(const MarkParams& P, int tw, cudaStream_t s) {
+    if (tw == kNarrowTileWords) k_mark_zmarch<ONE, kNarrowTileWords><<<(unsigned)P.ntiles, kMarkWarps * 32, 0, s>>>(P);
+    else                        k_mark_zmarch<ONE, kTileWords><<<(unsigned)P.ntiles, kMarkWarps * 32, 0, s>>>(P);
 }
 
-cudaError_t launch_mark(const MarkParams& P, int tw, cudaStream_t s, int smem_pad) {
+cudaError_t launch_mark(const MarkParams& P, int tw, cudaStream_t s) {
     if (P.ntiles <= 0) return cudaSuccess;
-    if (P.B.n == 1) {
-        if (tw == kNarrowTileWords) launch_mark_t<true, kNarrowTileWords>(P, smem_pad, s);
-        else                        launch_mark_t<true, kTileWords>(P, smem_pad, s);
-    } else {
-        if (tw == kNarrowTileWords) launch_mark_t<false, kNarrowTileWords>(P, smem_pad, s);
-        else                        launch_mark_t<false, kTileWords>(P, smem_pad, s);
-    }
+    if (P.B.n == 1) launch_mark_tw<true>(P, tw, s);
+    else            launch_mark_tw<false>(P, tw, s);
     return cudaGetLastError();
 }
 

@@ -119,13 +119,10 @@ k_cell_qef(const __grid_constant__ QefParams P) {
     const int tid = threadIdx.x;
     if (tid == 0) s_hist = 0;
     __syncthreads();
-    // with a device count of active cells above the capacity the buffers were sized for (a
-    // captured graph, or a z-slab pipeline on an earlier call's buffers), the cells below the
-    // capacity are processed, every kernel alike (their faces only reach lower ranks); the
-    // host reports the overflow or runs the grid again
-    const long long nact = P.live ? std::min((long long)*P.live, P.nactive) : P.nactive;
-    const long long r0 = P.first ? (long long)*P.first : 0;    // a z-slab's first active cell
-    for (long long r = r0 + (long long)blockIdx.x * blockDim.x + tid; r < nact;
+    // a captured graph whose live count exceeds the capacity it was built for does nothing
+    // (the host reports the overflow after the replay)
+    const long long nact = P.live ? ((long long)*P.live > P.nactive ? 0 : (long long)*P.live) : P.nactive;
+    for (long long r = (long long)blockIdx.x * blockDim.x + tid; r < nact;
          r += (long long)gridDim.x * blockDim.x) {
         const GridSlot& S = slot_ref<ONE>(P.B, ONE ? 0 : slot_of_rank(P.B, (unsigned long long)r));
         const GridDesc& g = S.g;
