@@ -340,6 +340,7 @@ def run_batch_workload(args):
     be = B200DualContouringBackend(0)
     ncell = sum((d[0] - 1) * (d[1] - 1) * (d[2] - 1) for _, d, _, _ in grids)
     waves, narrow, tune_ms = be.autotune_mark(grids)         # tile shapes for this batch
+    qef_minb, qef_bps, face_bps, cells_ms = be.autotune_cells(grids)   # vertex / face kernel shapes
     stream = torch.cuda.current_stream()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     for _ in range(args.warmup):
@@ -395,6 +396,8 @@ def run_batch_workload(args):
                      "qef": round(st.qef_ms, 4), "faces": round(st.face_emission_ms, 4)},
         "escalated_fp64_cells": st.escalated_fp64_cells, "winding_fp64_faces": st.winding_fp64_faces,
         "mark_tiles": {"waves": waves, "narrow_tile_max_cells": narrow, "autotune_mark_ms": round(tune_ms, 4)},
+        "cell_kernels": {"qef_min_blocks_per_sm": qef_minb, "qef_blocks_per_sm": qef_bps,
+                         "face_blocks_per_sm": face_bps, "autotune_stage_ms": round(cells_ms, 4)},
         "sequential_plain_ms": round(ms_seq, 3) if ms_seq else None,
         "batched_speedup": round(ms_seq / ms_batch, 2) if ms_seq else None,
         "graph": {"ms_per_step": round(ms_graph, 4), "mcells_per_s": round(ncell / (ms_graph / 1e3) / 1e6, 2),

@@ -26,7 +26,7 @@ extern "C" {
 /* 4 adds, without changing earlier layouts: the batch CUDA-graph calls, the mesh post-pass
  * (dcb_postprocess_*, dcb_copy_post_mesh, dcb_post_stats) and the OBJ reader (dcb_read_obj,
  * dcb_obj_grid). */
-#define DCB_ABI_VERSION 5
+#define DCB_ABI_VERSION 6
 
 enum dcb_status {
     DCB_OK = 0,
@@ -315,6 +315,19 @@ int dcb_batch_graph_destroy(dcb_handle h);
  * width limit and the median mark time (ms) are returned through the optional pointers. */
 int dcb_autotune_mark(dcb_handle h, const dcb_grid* grids, int n, int* waves_out, int* narrow_cells_out,
                       float* best_ms_out, void* cuda_stream);
+
+/* Autotuner for the vertex and face kernels (no counterpart in the reference): extracts these
+ * device grids (one batch) repeatedly, first for every register cap of the FP32 vertex
+ * kernel (4, 5 or 6 resident blocks of 128 threads per SM) with every launch width (8, 16 or
+ * 32 blocks per SM of its grid-stride loop), timing the vertex stage, then for every width of
+ * the face scatter (8, 16 or 32 blocks per SM), timing the face stage; keeps the fastest of
+ * each for this handle's later extractions, batches and captured graphs. Results do not depend
+ * on these choices (same arithmetic per cell and face). The choices and the sum of the two
+ * median stage times (ms) are returned through the optional pointers. opts may be null
+ * (defaults); dual contouring only. */
+int dcb_autotune_cells(dcb_handle h, const dcb_grid* grids, int n, const dcb_opts* opts, int* qef_min_blocks_out,
+                       int* qef_blocks_per_sm_out, int* face_blocks_per_sm_out, float* best_ms_out,
+                       void* cuda_stream);
 
 /* ---- mesh -> signed distance grid ------------------------------------------------------ */
 

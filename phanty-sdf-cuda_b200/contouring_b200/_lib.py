@@ -29,7 +29,7 @@ EXPORTED = (
     "dcb_create", "dcb_destroy", "dcb_extract_device", "dcb_extract_host",
     "dcb_copy_mesh_to_host", "dcb_copy_mesh_device", "dcb_copy_cells_to_host",
     "dcb_mark_active_cells_noalloc", "dcb_mesh_to_sdf_device", "dcb_mesh_to_sdf_host",
-    "dcb_extract_batch_device", "dcb_backward", "dcb_autotune_mark",
+    "dcb_extract_batch_device", "dcb_backward", "dcb_autotune_mark", "dcb_autotune_cells",
     "dcb_write_obj", "dcb_read_sdf", "dcb_write_sdf", "dcb_extract_upload", "dcb_mesh_to_sdf_device_ex",
     "dcb_mesh_to_sdf_host_ex", "dcb_batch_graph_create", "dcb_batch_graph_launch", "dcb_batch_graph_finish",
     "dcb_batch_graph_destroy", "dcb_postprocess_device", "dcb_postprocess_host", "dcb_copy_post_mesh",
@@ -184,6 +184,9 @@ def lib():
     L.dcb_autotune_mark.argtypes = [ctypes.c_void_p, P(DcbGrid), ctypes.c_int, P(ctypes.c_int), P(ctypes.c_int),
                                     P(ctypes.c_float), ctypes.c_void_p]
     L.dcb_autotune_mark.restype = ctypes.c_int
+    L.dcb_autotune_cells.argtypes = [ctypes.c_void_p, P(DcbGrid), ctypes.c_int, P(DcbOpts), P(ctypes.c_int),
+                                     P(ctypes.c_int), P(ctypes.c_int), P(ctypes.c_float), ctypes.c_void_p]
+    L.dcb_autotune_cells.restype = ctypes.c_int
     L.dcb_backward.argtypes = [ctypes.c_void_p, P(DcbGrid), P(DcbOpts), ctypes.c_void_p, ctypes.c_void_p,
                                ctypes.c_int, ctypes.c_void_p]
     L.dcb_backward.restype = ctypes.c_int

@@ -380,6 +380,20 @@ class B200DualContouringBackend:
                                              ctypes.c_void_p(s)), self._h)
         return w.value, nc.value, ms.value
 
+    def autotune_cells(self, grids, stream=None):
+        """Time the vertex kernel's register caps and launch widths and the face kernel's launch
+        widths on ``grids`` = [(CUDA float32 values, dims, spacing, origin)] with this backend's
+        options, and keep the fastest; returns (qef_min_blocks, qef_blocks_per_sm,
+        face_blocks_per_sm, ms)."""
+        arr = self._grid_array(grids)
+        m, q, f, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_float()
+        s = _current_stream() if stream is None else stream
+        _lib.check(self._L.dcb_autotune_cells(self._h, arr, len(grids), ctypes.byref(self.options.to_c()),
+                                              ctypes.byref(m), ctypes.byref(q), ctypes.byref(f), ctypes.byref(ms),
+                                              ctypes.c_void_p(s)), self._h)
+        self._generation += 1
+        return m.value, q.value, f.value, ms.value
+
     def extract_batch(self, grids, stream=None):
         """Batched extraction of ``grids`` = [(CUDA float32 values, dims, spacing, origin)] in one
         pass of the pipeline. Returns ``[(V (nv,3) float32, F (nf,vpf) int32)]`` CUDA tensors per

@@ -86,6 +86,11 @@ struct dcb_context {
     // (cells along x) that marches 256-cell x-tiles instead of 1024-cell ones
     int tune_waves = 4;
     int tune_narrow_cells = 256;
+    // vertex and face kernels (dcb_autotune_cells): k_cell_qef's register cap (resident blocks
+    // per SM its allocation allows) and grid-stride width, k_face_scatter's width (blocks per SM)
+    int tune_qef_minb = 5;
+    int tune_qef_bps = 32;
+    int tune_face_bps = 16;
     int cx = 0, cy = 0, cz = 0;
     // batch layout table (device + pinned staging) and the last batch's per-grid offsets
     DevBuf table, cell_slot;
@@ -474,7 +479,7 @@ int batch_rest(dcb_context* h, const BatchLayout& L, TableView& T, const dcb_opt
     qp.nonfinite = &dc->nonfinite;
     qp.thr = (float)o->svd_threshold; qp.band = (float)o->fp64_threshold_band;
     qp.cond_max = (float)std::min(o->fp64_escalation_cond, 3.0e38); qp.force64 = o->force_fp64;
-    DCB_TRY(h, launch_cell_qef(qp, h->num_sms, s), "launch qef");
+    DCB_TRY(h, launch_cell_qef(qp, h->num_sms, s, h->tune_qef_minb, h->tune_qef_bps), "launch qef");
     DCB_TRY(h, launch_cell_jacobi(qp, cap, h->num_sms, s), "launch jacobi");
     Vertex64Params v64;
     v64.B = T.B; v64.list = xp.list; v64.cells = qp.esc_list; v64.count = &dc->esc_count; v64.cap = (unsigned int)cap;
@@ -505,7 +510,7 @@ int batch_rest(dcb_context* h, const BatchLayout& L, TableView& T, const dcb_opt
     fp.v64_count = &dc->v64_count; fp.v64_cap = (unsigned long long)v64_cap;
     fp.err = &dc->err;
     fp.hmax = L.hmax;
-    DCB_TRY(h, launch_face_scatter(fp, h->num_sms, s), "launch face scatter");
+    DCB_TRY(h, launch_face_scatter(fp, h->num_sms, s, h->tune_face_bps), "launch face scatter");
     Vertex64Params w64;
     w64.B = T.B; w64.list = xp.list; w64.cells = fp.v64_cells; w64.count = fp.v64_count; w64.cap = (unsigned int)v64_cap;
     w64.Vf = nullptr; w64.vclass = nullptr; w64.V64 = as<double>(h->V64); w64.thr = o->svd_threshold;
@@ -1467,6 +1472,71 @@ int dcb_autotune_mark(dcb_handle h, const dcb_grid* grids, int n, int* waves_out
     if (waves_out) *waves_out = best_w;
     if (narrow_cells_out) *narrow_cells_out = best_n;
     if (best_ms_out) *best_ms_out = best;
+    return DCB_OK;
+}
+
+int dcb_autotune_cells(dcb_handle h, const dcb_grid* grids, int n, const dcb_opts* opts, int* qef_min_blocks_out,
+                       int* qef_blocks_per_sm_out, int* face_blocks_per_sm_out, float* best_ms_out, void* cuda_stream) {
+    if (h) ++h->gen;                        // reuses the extraction workspace
+    if (!h) return DCB_ERR_INVALID_ARGUMENT;
+    if (!grids || n < 1) return fail(h, DCB_ERR_INVALID_ARGUMENT, "empty batch");
+    for (int b = 0; b < n; ++b) {
+        const int rc = validate(h, grids + b);
+        if (rc != DCB_OK) return rc;
+    }
+    dcb_opts def;
+    dcb_default_opts(&def);
+    const dcb_opts* o = opts ? opts : &def;
+    if (o->method != DCB_METHOD_DUAL_CONTOURING) return fail(h, DCB_ERR_NOT_SUPPORTED, "tunes the dual contouring kernels");
+    if (cudaSetDevice(h->device) != cudaSuccess) { cudaGetLastError(); return fail(h, DCB_ERR_CUDA, "set device"); }
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(cuda_stream);
+    // median of three timed extractions after one untimed: the vertex stage (expand, k_cell_qef,
+    // Jacobi, FP64 vertices) or the face stage
+    auto stage_ms = [&](bool faces, float& out) -> int {
+        float ms[3];
+        for (int r = 0; r < 4; ++r) {
+            dcb_stats st;
+            std::memset(&st, 0, sizeof(st));
+            DCB_TRY(h, cudaEventRecord(h->ev[0], s), "event");
+            DCB_TRY(h, cudaEventRecord(h->ev[1], s), "event");
+            const int rc = run_batch(h, grids, n, o, s, &st);
+            if (rc != DCB_OK) return rc;
+            fill_times(h, &st, false);
+            if (r > 0) ms[r - 1] = faces ? st.face_emission_ms : st.qef_ms;
+        }
+        std::sort(ms, ms + 3);
+        out = ms[1];
+        return DCB_OK;
+    };
+    static const int kMinB[3] = {4, 5, 6};
+    static const int kWidth[3] = {8, 16, 32};
+    const int keep_m = h->tune_qef_minb, keep_q = h->tune_qef_bps, keep_f = h->tune_face_bps;
+    float best_q = 1e30f, best_f = 1e30f;
+    int bm = keep_m, bq = keep_q, bf = keep_f;
+    for (int a = 0; a < 3; ++a) {
+        for (int w = 0; w < 3; ++w) {
+            h->tune_qef_minb = kMinB[a];
+            h->tune_qef_bps = kWidth[w];
+            float t = 0.f;
+            const int rc = stage_ms(false, t);
+            if (rc != DCB_OK) { h->tune_qef_minb = keep_m; h->tune_qef_bps = keep_q; return rc; }
+            if (t < best_q) { best_q = t; bm = kMinB[a]; bq = kWidth[w]; }
+        }
+    }
+    h->tune_qef_minb = bm;
+    h->tune_qef_bps = bq;
+    for (int w = 0; w < 3; ++w) {
+        h->tune_face_bps = kWidth[w];
+        float t = 0.f;
+        const int rc = stage_ms(true, t);
+        if (rc != DCB_OK) { h->tune_face_bps = keep_f; return rc; }
+        if (t < best_f) { best_f = t; bf = kWidth[w]; }
+    }
+    h->tune_face_bps = bf;
+    if (qef_min_blocks_out) *qef_min_blocks_out = bm;
+    if (qef_blocks_per_sm_out) *qef_blocks_per_sm_out = bq;
+    if (face_blocks_per_sm_out) *face_blocks_per_sm_out = bf;
+    if (best_ms_out) *best_ms_out = best_q + best_f;
     return DCB_OK;
 }
 

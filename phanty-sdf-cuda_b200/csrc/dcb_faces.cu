@@ -286,10 +286,10 @@ k_face_scatter(const __grid_constant__ FaceParams P) {
     }
 }
 
-cudaError_t launch_face_scatter(const FaceParams& P, int num_sms, cudaStream_t s) {
+cudaError_t launch_face_scatter(const FaceParams& P, int num_sms, cudaStream_t s, int blocks_per_sm) {
     if (P.nactive <= 0) return cudaSuccess;
     long long blocks = (P.nactive + kFaceThreads - 1) / kFaceThreads;
-    const long long cap = (long long)num_sms * 16;
+    const long long cap = (long long)num_sms * blocks_per_sm;
     if (blocks > cap) blocks = cap;
     if (P.B.n == 1) k_face_scatter<true><<<(unsigned)blocks, kFaceThreads, 0, s>>>(P);
     else            k_face_scatter<false><<<(unsigned)blocks, kFaceThreads, 0, s>>>(P);

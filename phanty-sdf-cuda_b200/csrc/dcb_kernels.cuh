@@ -133,7 +133,9 @@ struct QefParams {
     float cond_max;
     int force64;
 };
-cudaError_t launch_cell_qef(const QefParams& P, int num_sms, cudaStream_t s);
+// minb: k_cell_qef's register cap (resident blocks per SM: 4, 5 or 6); blocks_per_sm: the width
+// of its grid-stride launch
+cudaError_t launch_cell_qef(const QefParams& P, int num_sms, cudaStream_t s, int minb = 5, int blocks_per_sm = 32);
 cudaError_t launch_cell_jacobi(const QefParams& P, long long max_items, int num_sms, cudaStream_t s);
 
 struct Vertex64Params {
@@ -191,7 +193,7 @@ struct FaceParams {
     int* err;
     float hmax;                    // unused: each grid's slot holds its own cell width
 };
-cudaError_t launch_face_scatter(const FaceParams& P, int num_sms, cudaStream_t s);
+cudaError_t launch_face_scatter(const FaceParams& P, int num_sms, cudaStream_t s, int blocks_per_sm = 16);
 cudaError_t launch_face_order(const int4* stage_quad, const uint2* stage_key, const uint32_t* col_start,
                               const uint32_t* col_count, const unsigned long long* nfaces, int4* faces,
                               long long max_faces, int num_sms, cudaStream_t s);

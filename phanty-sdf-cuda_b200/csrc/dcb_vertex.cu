@@ -110,8 +110,10 @@ __device__ float3 edge_normal(const GridDesc& g, int3 lo, int axis, int o1, int 
 
 // ---- k_cell_qef -------------------------------------------------------------------------
 
-template <bool ONE>
-__global__ void __launch_bounds__(128, 5)
+// MINB: resident blocks per SM the register allocation must allow (the register cap); the
+// autotuner picks 4, 5 or 6 per handle.
+template <bool ONE, int MINB>
+__global__ void __launch_bounds__(128, MINB)
 k_cell_qef(const __grid_constant__ QefParams P) {
     __shared__ unsigned int s_hist;
     __shared__ float s_c[8][128];    // per-thread corner values (dynamically indexed)
@@ -234,13 +236,20 @@ k_cell_qef(const __grid_constant__ QefParams P) {
     if (threadIdx.x == 0 && s_hist) atomicAdd(P.rank_hist + 1, (unsigned long long)s_hist);
 }
 
-cudaError_t launch_cell_qef(const QefParams& P, int num_sms, cudaStream_t s) {
+template <bool ONE>
+void launch_cell_qef_t(const QefParams& P, unsigned blocks, int minb, cudaStream_t s) {
+    if (minb <= 4)      k_cell_qef<ONE, 4><<<blocks, 128, 0, s>>>(P);
+    else if (minb == 5) k_cell_qef<ONE, 5><<<blocks, 128, 0, s>>>(P);
+    else                k_cell_qef<ONE, 6><<<blocks, 128, 0, s>>>(P);
+}
+
+cudaError_t launch_cell_qef(const QefParams& P, int num_sms, cudaStream_t s, int minb, int blocks_per_sm) {
     if (P.nactive <= 0) return cudaSuccess;
     long long blocks = (P.nactive + 127) / 128;
-    const long long cap = (long long)num_sms * 32;
+    const long long cap = (long long)num_sms * blocks_per_sm;
     if (blocks > cap) blocks = cap;
-    if (P.B.n == 1) k_cell_qef<true><<<(unsigned)blocks, 128, 0, s>>>(P);
-    else            k_cell_qef<false><<<(unsigned)blocks, 128, 0, s>>>(P);
+    if (P.B.n == 1) launch_cell_qef_t<true>(P, (unsigned)blocks, minb, s);
+    else            launch_cell_qef_t<false>(P, (unsigned)blocks, minb, s);
     return cudaGetLastError();
 }
 

@@ -96,6 +96,31 @@ def test_autotune_keeps_the_results(backend):
     print("autotuned mark tiling: %d waves, 256-cell tiles up to %d cells wide, %.3f ms" % (waves, narrow, ms))
 
 
+def test_cell_autotune_keeps_the_results():
+    """The vertex/face autotuner picks a register cap and launch widths among its candidates;
+    batches and single extractions afterwards equal those before it bit for bit."""
+    import torch
+    from contouring_b200 import B200DualContouringBackend, synth
+    be = B200DualContouringBackend(0)
+    try:
+        grids = synth.csg_batch(24, seed=6, device="cuda")
+        single = grids[0]
+        before, _ = be.extract_batch(grids)
+        before = [(V.clone(), F.clone()) for V, F in before]
+        V1, F1, _ = be.extract_tensor(*single)
+        V1, F1 = V1.clone(), F1.clone()
+        m, q, f, ms = be.autotune_cells(grids)
+        assert m in (4, 5, 6) and q in (8, 16, 32) and f in (8, 16, 32) and ms > 0
+        after, _ = be.extract_batch(grids)
+        for (Va, Fa), (Vb, Fb) in zip(before, after):
+            assert torch.equal(Va, Vb) and torch.equal(Fa, Fb)
+        V2, F2, _ = be.extract_tensor(*single)
+        assert torch.equal(V1, V2) and torch.equal(F1, F2)
+        print("autotuned cell kernels: vertex cap %d blocks/SM, width %d, faces width %d; %.3f ms" % (m, q, f, ms))
+    finally:
+        be.close()
+
+
 # ---- the batch captured in a CUDA graph (dcb_batch_graph_*) -----------------------------------
 
 def _same(meshes_a, meshes_b):
