@@ -39,8 +39,11 @@ MARK_TRAFFIC_BYTES_PER_POINT = (563.814656e6 + 18.4768e6) / 512 ** 3
 # point plus band-proportional bytes per active cell, from single-kernel-list ncu captures
 # (dram__bytes_read.sum + dram__bytes_write.sum summed over the step's launches). None = not
 # measured.
-PIPELINE_TRAFFIC_BYTES_PER_POINT = None
-PIPELINE_TRAFFIC_BYTES_PER_ACTIVE = None
+# From one extraction of the 512^3 CSG workload (1,534,557 active cells): the mark and the scans
+# of segments and columns 5.89068e+08 B (grid-proportional), every other kernel 3.56506e+08 B
+# (band-proportional).
+PIPELINE_TRAFFIC_BYTES_PER_POINT = 5.89068e+08 / 512 ** 3
+PIPELINE_TRAFFIC_BYTES_PER_ACTIVE = 3.56506e+08 / 1534557
 
 
 def max_over_ranks(local, dist, device):
