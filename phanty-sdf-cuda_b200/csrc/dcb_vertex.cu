@@ -153,6 +153,18 @@ k_cell_qef(const __grid_constant__ QefParams P) {
         // (contouring.cpp:560-594); the host reports DCB_ERR_INVALID_ARGUMENT
         if (((fm & 1) && isinf(c[1])) || ((fm & 6) && isinf(c[0]))) set_error(P.err, kErrNonFinite);
         P.fmask[r] = fm;
+        // The winding test of each face owned here (k_face_scatter) needs gradientAt at both ends
+        // of the face edge (contouring.cpp:624-641): formed now, while this cell's corner and
+        // stencil values sit in L1, and stored as one coalesced record per face.
+        if (fm) {
+            const float3 g0 = grid_gradient32(g, i, j, k);
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                if (!((fm >> a) & 1)) continue;
+                const float3 g1 = grid_gradient32(g, i + (a == 0), j + (a == 1), k + (a == 2));
+                P.fgrad[(long long)a * P.fgrad_stride + r] = make_float4(g0.x + g1.x, g0.y + g1.y, g0.z + g1.z, 0.f);
+            }
+        }
 
         // Pass 1: crossing edges and the centroid in local units.
         uint32_t hmask = 0;
