@@ -865,6 +865,8 @@ def main():
     stream = torch.cuda.current_stream()
     gdev = DenseSdfGridDevice(*dims, *spacing, *origin, d_values=vals)
     ncell = (dims[0] - 1) * (dims[1] - 1) * (dims[2] - 1)
+    # vertex / face kernel shapes for this grid, kept by the handle (untimed, before warm-up)
+    qef_minb, qef_bps, face_bps, _ = be.autotune_cells([(vals, dims, spacing, origin)])
 
     def barrier():
         if dist is not None:
@@ -982,7 +984,9 @@ def main():
             "config": {"workload": "csg%d_dense_dc" % args.res, "grid": list(dims),
                        "cells": ncell, "vertices": nv, "quads": nf,
                        "l2": "input (%.2f GB) larger than L2; no flush needed" % (4 * npts / 1e9),
-                       "parallelism": "replicas: one independent grid per rank"},
+                       "parallelism": "replicas: one independent grid per rank",
+                       "cell_kernels": {"qef_min_blocks_per_sm": qef_minb, "qef_blocks_per_sm": qef_bps,
+                                        "face_blocks_per_sm": face_bps}},
             # the whole extraction (every kernel of a step) against the measured copy bandwidth
             "roofline": {"bound": "hbm", "kernel": "whole extraction (%d launches)" % KERNELS_PER_STEP,
                          "achieved": round(pipe_gbs, 1), "peak": peak, "unit": "GB/s",

@@ -473,20 +473,27 @@ void post_release(PostWork& W);
 
 // gradientAt (contouring.cpp:141-207) in FP32 (orientation tests only: a 2-ulp quotient is
 // far inside the uncertainty margin, and uncertain faces are re-decided in FP64).
+// gradientAt from each axis' central difference (value above minus value below) and the
+// position difference it spans (a span <= 1e-12 gives 0), normalised.
+__device__ __forceinline__ float3 gradient_from(float ddx, float dx, float ddy, float dy, float ddz, float dz) {
+    float3 o = make_float3(0.f, 0.f, 0.f);
+    if (fabsf(dx) > 1e-12f) o.x = __fdividef(ddx, dx);
+    if (fabsf(dy) > 1e-12f) o.y = __fdividef(ddy, dy);
+    if (fabsf(dz) > 1e-12f) o.z = __fdividef(ddz, dz);
+    const float n2 = o.x * o.x + o.y * o.y + o.z * o.z;
+    if (n2 > 0.f) { const float r = rsqrtf(n2); o.x *= r; o.y *= r; o.z *= r; }
+    return o;
+}
 __device__ __forceinline__ float3 grid_gradient32(const GridDesc& g, int i, int j, int k) {
     const int im = max(i - 1, 0), ip = min(i + 1, g.nx - 1);
     const int jm = max(j - 1, 0), jp = min(j + 1, g.ny - 1);
     const int km = max(k - 1, 0), kp = min(k + 1, g.nz - 1);
-    float3 o = make_float3(0.f, 0.f, 0.f);
-    const float dx = pos_axis(g.ox, g.vx, ip) - pos_axis(g.ox, g.vx, im);
-    if (fabsf(dx) > 1e-12f) o.x = __fdividef(__ldg(g.v + pidx(g, ip, j, k)) - __ldg(g.v + pidx(g, im, j, k)), dx);
-    const float dy = pos_axis(g.oy, g.vy, jp) - pos_axis(g.oy, g.vy, jm);
-    if (fabsf(dy) > 1e-12f) o.y = __fdividef(__ldg(g.v + pidx(g, i, jp, k)) - __ldg(g.v + pidx(g, i, jm, k)), dy);
-    const float dz = pos_axis(g.oz, g.vz, kp) - pos_axis(g.oz, g.vz, km);
-    if (fabsf(dz) > 1e-12f) o.z = __fdividef(__ldg(g.v + pidx(g, i, j, kp)) - __ldg(g.v + pidx(g, i, j, km)), dz);
-    const float n2 = o.x * o.x + o.y * o.y + o.z * o.z;
-    if (n2 > 0.f) { const float r = rsqrtf(n2); o.x *= r; o.y *= r; o.z *= r; }
-    return o;
+    return gradient_from(__ldg(g.v + pidx(g, ip, j, k)) - __ldg(g.v + pidx(g, im, j, k)),
+                         pos_axis(g.ox, g.vx, ip) - pos_axis(g.ox, g.vx, im),
+                         __ldg(g.v + pidx(g, i, jp, k)) - __ldg(g.v + pidx(g, i, jm, k)),
+                         pos_axis(g.oy, g.vy, jp) - pos_axis(g.oy, g.vy, jm),
+                         __ldg(g.v + pidx(g, i, j, kp)) - __ldg(g.v + pidx(g, i, j, km)),
+                         pos_axis(g.oz, g.vz, kp) - pos_axis(g.oz, g.vz, km));
 }
 
 }  // namespace dcb
