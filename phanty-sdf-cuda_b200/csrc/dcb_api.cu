@@ -61,7 +61,7 @@ struct dcb_context {
     bool substage_events = false;     // ev[8] / ev[9] hold the face sub-stages of the last call
     DevBuf grid, bits, super, list, seg_count, seg_start, counters, V, vclass, fmask, col_count, col_fill,
         col_start, partials, esc_list, hard_list, hard_data, stage_quad, stage_key, faces, wind_items,
-        v64_index, v64_cells, V64, tris, tri_items, adj_rows, adj_owners, ours_ws, fgrad;
+        v64_index, v64_cells, V64, tris, tri_items, adj_rows, adj_owners, ours_ws;
     // sparse backends
     DevBuf sp_words, sp_brick, sp_vcount, sp_vstart, sp_vtmp, sp_ntmp, sp_N, sp_vcell, sp_fcount, sp_fstart,
         sp_stage, sp_counters;
@@ -388,7 +388,6 @@ int batch_alloc(dcb_context* h, int n, long long cap, const dcb_opts* o, TableVi
     DCB_TRY(h, ensure(h->list, sizeof(uint64_t) * cap), "alloc active list");
     DCB_TRY(h, ensure(h->V, sizeof(float) * 3 * cap), "alloc vertices");
     DCB_TRY(h, ensure(h->fmask, cap), "alloc face masks");
-    DCB_TRY(h, ensure(h->fgrad, sizeof(float4) * 3 * cap), "alloc face gradients");
     DCB_TRY(h, ensure(h->vclass, cap), "alloc vertex classes");
     DCB_TRY(h, ensure(h->esc_list, sizeof(uint32_t) * cap), "alloc escalation list");
     DCB_TRY(h, ensure(h->hard_list, sizeof(uint32_t) * cap), "alloc hard list");
@@ -473,7 +472,6 @@ int batch_rest(dcb_context* h, const BatchLayout& L, TableView& T, const dcb_opt
     QefParams qp;
     qp.B = T.B; qp.list = xp.list; qp.nactive = cap; qp.live = live; qp.V = as<float>(h->V); qp.vclass = as<uint8_t>(h->vclass);
     qp.fmask = as<uint8_t>(h->fmask); qp.col_count = as<uint32_t>(h->col_count);
-    qp.fgrad = as<float4>(h->fgrad); qp.fgrad_stride = cap;
     qp.esc_list = as<uint32_t>(h->esc_list); qp.esc_count = &dc->esc_count;
     qp.hard_list = as<uint32_t>(h->hard_list); qp.hard_data = as<float4>(h->hard_data); qp.hard_count = &dc->hard_count;
     qp.rank_hist = dc->rank_hist;
@@ -502,7 +500,6 @@ int batch_rest(dcb_context* h, const BatchLayout& L, TableView& T, const dcb_opt
         DCB_TRY(h, launch_face_offsets(T.B, as<uint32_t>(h->col_start), &dc->face_total, T.face_off, s), "face offsets");
     FaceParams fp;
     fp.B = T.B; fp.list = xp.list; fp.nactive = cap; fp.live = live; fp.fmask = qp.fmask; fp.V = qp.V; fp.vclass = qp.vclass;
-    fp.fgrad = qp.fgrad; fp.fgrad_stride = qp.fgrad_stride;
     fp.bits = xp.bits; fp.super = xp.super;
     fp.col_start = as<uint32_t>(h->col_start); fp.col_count = as<uint32_t>(h->col_count);
     fp.col_fill = as<uint32_t>(h->col_fill);
@@ -1117,7 +1114,7 @@ int dcb_destroy(dcb_handle h) {
                       &h->tris, &h->tri_items, &h->m_verts, &h->m_faces, &h->m_out, &h->m_tris,
                       &h->m_bin_count, &h->m_bin_start, &h->m_bin_fill, &h->m_bin_scratch, &h->m_bin_tris,
                       &h->m_bin_active, &h->m_active_list, &h->m_axis_start, &h->m_far, &h->m_ext, &h->m_tmp,
-                      &h->m_partials, &h->m_counters, &h->m_vox, &h->table, &h->cell_slot, &h->adj_rows, &h->adj_owners, &h->ours_ws, &h->fgrad,
+                      &h->m_partials, &h->m_counters, &h->m_vox, &h->table, &h->cell_slot, &h->adj_rows, &h->adj_owners, &h->ours_ws,
                       &h->sp_words, &h->sp_brick, &h->sp_vcount, &h->sp_vstart, &h->sp_vtmp, &h->sp_ntmp,
                       &h->sp_N, &h->sp_vcell, &h->sp_fcount, &h->sp_fstart, &h->sp_stage, &h->sp_counters};
     for (DevBuf* b : bufs) if (b->p) cudaFree(b->p);

@@ -108,6 +108,23 @@ long long scan_partials_len(long long n) { return (n + kScanTile - 1) / kScanTil
 constexpr int kFaceThreads = 128;
 
 
+// gradientAt (contouring.cpp:141-207) in FP32 (orientation tests only: a 2-ulp quotient is
+// far inside the uncertainty margin, and uncertain faces are re-decided in FP64).
+__device__ __forceinline__ float3 grid_gradient32(const GridDesc& g, int i, int j, int k) {
+    const int im = max(i - 1, 0), ip = min(i + 1, g.nx - 1);
+    const int jm = max(j - 1, 0), jp = min(j + 1, g.ny - 1);
+    const int km = max(k - 1, 0), kp = min(k + 1, g.nz - 1);
+    float3 o = make_float3(0.f, 0.f, 0.f);
+    const float dx = pos_axis(g.ox, g.vx, ip) - pos_axis(g.ox, g.vx, im);
+    if (fabsf(dx) > 1e-12f) o.x = __fdividef(__ldg(g.v + pidx(g, ip, j, k)) - __ldg(g.v + pidx(g, im, j, k)), dx);
+    const float dy = pos_axis(g.oy, g.vy, jp) - pos_axis(g.oy, g.vy, jm);
+    if (fabsf(dy) > 1e-12f) o.y = __fdividef(__ldg(g.v + pidx(g, i, jp, k)) - __ldg(g.v + pidx(g, i, jm, k)), dy);
+    const float dz = pos_axis(g.oz, g.vz, kp) - pos_axis(g.oz, g.vz, km);
+    if (fabsf(dz) > 1e-12f) o.z = __fdividef(__ldg(g.v + pidx(g, i, j, kp)) - __ldg(g.v + pidx(g, i, j, km)), dz);
+    const float n2 = o.x * o.x + o.y * o.y + o.z * o.z;
+    if (n2 > 0.f) { const float r = rsqrtf(n2); o.x *= r; o.y *= r; o.z *= r; }
+    return o;
+}
 
 __device__ __forceinline__ float3 ldv(const float* V, uint32_t r) {
     return make_float3(__ldg(V + 3 * (size_t)r), __ldg(V + 3 * (size_t)r + 1), __ldg(V + 3 * (size_t)r + 2));
@@ -154,7 +171,7 @@ __device__ __forceinline__ void request_fp64_vertex(int* v64_index, uint32_t* v6
 // work items.
 template <bool ONE>
 __device__ __forceinline__ void emit_face(const FaceParams& P, int gi, int i, int j, int k, uint32_t r, int axis,
-                                          uint32_t r_k1, uint32_t r_j1, uint32_t r_jk) {
+                                          float3 g0, uint32_t r_k1, uint32_t r_j1, uint32_t r_jk) {
     const GridSlot& S = slot_ref<ONE>(P.B, gi);
     const GridDesc& g = S.g;
     const long long cxcy = (long long)g.cx * g.cy;
@@ -163,9 +180,8 @@ __device__ __forceinline__ void emit_face(const FaceParams& P, int gi, int i, in
     else if (axis == 1) { r0 = r_k1 - 1u; r1 = r_k1; r3 = r - 1u; }    // (i-1,j,k-1) (i,j,k-1) (i-1,j,k)
     else { r0 = r_j1 - 1u; r1 = r_j1; r3 = r - 1u; }                   // (i-1,j-1,k) (i,j-1,k) (i-1,j,k)
     const uint32_t r2 = r;
-    // gradientAt(p0) + gradientAt(p1) of the face edge, formed by k_cell_qef
-    const float4 gs = P.fgrad[(long long)axis * P.fgrad_stride + r];
-    const float3 gn = make_float3(gs.x, gs.y, gs.z);
+    const float3 g1 = grid_gradient32(g, i + (axis == 0), j + (axis == 1), k + (axis == 2));
+    const float3 gn = make_float3(g0.x + g1.x, g0.y + g1.y, g0.z + g1.z);
     const float3 pa = ldv(P.V, r0), pb = ldv(P.V, r1), pc = ldv(P.V, r2), pd = ldv(P.V, r3);
     const float dv = quad_vertex_bound(P.vclass, r0, r1, r2, r3, pa, pb, pc, pd, S.hmax);
     const float3 ba = sub3(pb, pa), da = sub3(pd, pa), ca = sub3(pc, pa);
@@ -209,7 +225,7 @@ __device__ __forceinline__ void emit_face(const FaceParams& P, int gi, int i, in
 
 // A warp takes 32 consecutive active cells. Each lane reads its cell's face mask (the cell's
 // min-corner edges with a strict sign change, contouring.cpp:609-729) and, when it owns a
-// face, the ranks of the face neighbours; then the warp's faces
+// face, the cell's gradient and the ranks of the face neighbours; then the warp's faces
 // (about one per cell) are dealt out a lane each, the owner's data passed by shuffle, so
 // the per-face work runs with the lanes full.
 template <bool ONE>
@@ -226,6 +242,7 @@ k_face_scatter(const __grid_constant__ FaceParams P) {
         const long long rr = base + lane;
         uint32_t fm = 0;
         int gi = 0, i = 0, j = 0, k = 0;
+        float3 g0 = make_float3(0.f, 0.f, 0.f);
         uint32_t r_k1 = 0xffffffffu, r_j1 = 0xffffffffu, r_jk = 0xffffffffu;
         if (rr < nact) fm = P.fmask[rr];
         if (fm) {
@@ -234,6 +251,7 @@ k_face_scatter(const __grid_constant__ FaceParams P) {
             const uint32_t* const bits = P.bits + S.bits_off;
             const uint32_t* const super = P.super + S.super_off;
             unpack_cell(P.list[rr], i, j, k);
+            g0 = grid_gradient32(S.g, i, j, k);
             // All four cells of a face are active, so a cell's x-1 neighbour in a face is the
             // previous active cell in linear order (rank - 1).
             if (fm & 3) r_k1 = cell_rank(bits, super, S.g, i, j, k - 1);
@@ -257,10 +275,12 @@ k_face_scatter(const __grid_constant__ FaceParams P) {
             const int src = (int)(it >> 2), axis = (int)(it & 3);
             const int fi = __shfl_sync(0xffffffffu, i, src), fj = __shfl_sync(0xffffffffu, j, src);
             const int fk = __shfl_sync(0xffffffffu, k, src), fg = __shfl_sync(0xffffffffu, gi, src);
+            const float3 f0 = make_float3(__shfl_sync(0xffffffffu, g0.x, src), __shfl_sync(0xffffffffu, g0.y, src),
+                                          __shfl_sync(0xffffffffu, g0.z, src));
             const uint32_t fk1 = __shfl_sync(0xffffffffu, r_k1, src), fj1 = __shfl_sync(0xffffffffu, r_j1, src);
             const uint32_t fjk = __shfl_sync(0xffffffffu, r_jk, src);
             if (t < total)
-                emit_face<ONE>(P, fg, fi, fj, fk, (uint32_t)(base + src), axis, fk1, fj1, fjk);
+                emit_face<ONE>(P, fg, fi, fj, fk, (uint32_t)(base + src), axis, f0, fk1, fj1, fjk);
         }
         __syncwarp();
     }

@@ -119,9 +119,6 @@ struct QefParams {
     uint8_t* vclass;                // [active] VertexClass
     uint8_t* fmask;                 // bit a: cell owns a face on its min-corner edge a
     uint32_t* col_count;            // per grid [3][cx*cy]: col_off + a*cx*cy + i*cy + j
-    float4* fgrad;                  // [3][fgrad_stride]: a face owner's gradient sum at the two ends of
-                                    // its face edge a (x, y, z; w unused)
-    long long fgrad_stride;
     uint32_t* esc_list;
     unsigned int* esc_count;
     uint32_t* hard_list;            // cells not certified rank 1
@@ -177,8 +174,6 @@ struct FaceParams {
     const unsigned long long* live; // device count of active cells (a captured graph; above
                                     // nactive, nothing is processed), or null
     const uint8_t* fmask;
-    const float4* fgrad;            // gradient sums of the face edges, written by k_cell_qef
-    long long fgrad_stride;
     const float* V;
     const uint8_t* vclass;
     const uint32_t* bits;
@@ -470,30 +465,5 @@ struct PostRun {
 
 cudaError_t post_run(PostWork& W, PostRun& R, cudaStream_t s);
 void post_release(PostWork& W);
-
-// gradientAt (contouring.cpp:141-207) in FP32 (orientation tests only: a 2-ulp quotient is
-// far inside the uncertainty margin, and uncertain faces are re-decided in FP64).
-// gradientAt from each axis' central difference (value above minus value below) and the
-// position difference it spans (a span <= 1e-12 gives 0), normalised.
-__device__ __forceinline__ float3 gradient_from(float ddx, float dx, float ddy, float dy, float ddz, float dz) {
-    float3 o = make_float3(0.f, 0.f, 0.f);
-    if (fabsf(dx) > 1e-12f) o.x = __fdividef(ddx, dx);
-    if (fabsf(dy) > 1e-12f) o.y = __fdividef(ddy, dy);
-    if (fabsf(dz) > 1e-12f) o.z = __fdividef(ddz, dz);
-    const float n2 = o.x * o.x + o.y * o.y + o.z * o.z;
-    if (n2 > 0.f) { const float r = rsqrtf(n2); o.x *= r; o.y *= r; o.z *= r; }
-    return o;
-}
-__device__ __forceinline__ float3 grid_gradient32(const GridDesc& g, int i, int j, int k) {
-    const int im = max(i - 1, 0), ip = min(i + 1, g.nx - 1);
-    const int jm = max(j - 1, 0), jp = min(j + 1, g.ny - 1);
-    const int km = max(k - 1, 0), kp = min(k + 1, g.nz - 1);
-    return gradient_from(__ldg(g.v + pidx(g, ip, j, k)) - __ldg(g.v + pidx(g, im, j, k)),
-                         pos_axis(g.ox, g.vx, ip) - pos_axis(g.ox, g.vx, im),
-                         __ldg(g.v + pidx(g, i, jp, k)) - __ldg(g.v + pidx(g, i, jm, k)),
-                         pos_axis(g.oy, g.vy, jp) - pos_axis(g.oy, g.vy, jm),
-                         __ldg(g.v + pidx(g, i, j, kp)) - __ldg(g.v + pidx(g, i, j, km)),
-                         pos_axis(g.oz, g.vz, kp) - pos_axis(g.oz, g.vz, km));
-}
 
 }  // namespace dcb

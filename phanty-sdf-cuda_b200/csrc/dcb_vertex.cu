@@ -41,13 +41,9 @@ namespace dcb {
 // set, else the cell's own trilinear normal at its sample. The average is a function of
 // the edge alone, so every cell sharing the edge computes the same value.
 // lo: global low endpoint; o1/o2: offset (0/1) of the low endpoint from the cell along d1/d2.
-// face: the edge is a face edge this cell owns (its min-corner edge with a strict sign change);
-// gsum then receives gradientAt(lo) + gradientAt(hi) for the face's winding test, formed from
-// the averaged normal's stencil and two more values along the edge (got = true), or left to
-// the caller (got = false) when the edge is outside the averaging set.
 __device__ float3 edge_normal(const GridDesc& g, int3 lo, int axis, int o1, int o2, float s_lo, float s_hi,
                               float t_lo, float pu, float pv, float pw, const float cc[8],
-                              const Widths& W, bool& ill, bool face, float3& gsum, bool& got) {
+                              const Widths& W, bool& ill) {
     const int3 hi = add3(lo, axis, 1);
     const bool in0 = lo.x > 0 && lo.x < g.nx - 1 && lo.y > 0 && lo.y < g.ny - 1 && lo.z > 0 && lo.z < g.nz - 1;
     const bool in1 = hi.x > 0 && hi.x < g.nx - 1 && hi.y > 0 && hi.y < g.ny - 1 && hi.z > 0 && hi.z < g.nz - 1;
@@ -74,43 +70,11 @@ __device__ float3 edge_normal(const GridDesc& g, int3 lo, int axis, int o1, int 
     const float* plo = g.v + pidx(g, lo.x, lo.y, lo.z);
     const float* phi = g.v + pidx(g, hi.x, hi.y, hi.z);
     const float ga = (s_hi - s_lo) * pick_r(W, axis, 1);
-    const float l1p = __ldg(plo + st1), l1m = __ldg(plo - st1), h1p = __ldg(phi + st1), h1m = __ldg(phi - st1);
-    const float l2p = __ldg(plo + st2), l2m = __ldg(plo - st2), h2p = __ldg(phi + st2), h2m = __ldg(phi - st2);
-    if (face) {
-        // gradientAt at both ends (as grid_gradient32): the perpendicular neighbours are the
-        // stencil's (interior here), along the edge the values one beyond each end (clamped)
-        const int la = comp(lo, axis), na = axis == 0 ? g.nx : (axis == 1 ? g.ny : g.nz);
-        const int64_t sta = axis == 0 ? 1 : (axis == 1 ? (int64_t)g.nx : (int64_t)g.nx * g.ny);
-        const float oa = axis == 0 ? g.ox : (axis == 1 ? g.oy : g.oz), va = axis == 0 ? g.vx : (axis == 1 ? g.vy : g.vz);
-        const float o1v = d1 == 0 ? g.ox : g.oy, v1v = d1 == 0 ? g.vx : g.vy;
-        const float o2v = d2 == 1 ? g.oy : g.oz, v2v = d2 == 1 ? g.vy : g.vz;
-        const int i1 = comp(lo, d1), i2 = comp(lo, d2);
-        const int lam = max(la - 1, 0), hap = min(la + 2, na - 1);
-        const float vlam = lam < la ? __ldg(plo - sta) : s_lo;
-        const float vhap = hap > la + 1 ? __ldg(phi + sta) : s_hi;
-        const float dal = pos_axis(oa, va, la + 1) - pos_axis(oa, va, lam);
-        const float dah = pos_axis(oa, va, hap) - pos_axis(oa, va, la);
-        const float dd1 = pos_axis(o1v, v1v, i1 + 1) - pos_axis(o1v, v1v, i1 - 1);
-        const float dd2 = pos_axis(o2v, v2v, i2 + 1) - pos_axis(o2v, v2v, i2 - 1);
-        float3 gl, gh;
-        if (axis == 0) {
-            gl = gradient_from(s_hi - vlam, dal, l1p - l1m, dd1, l2p - l2m, dd2);
-            gh = gradient_from(vhap - s_lo, dah, h1p - h1m, dd1, h2p - h2m, dd2);
-        } else if (axis == 1) {
-            gl = gradient_from(l1p - l1m, dd1, s_hi - vlam, dal, l2p - l2m, dd2);
-            gh = gradient_from(h1p - h1m, dd1, vhap - s_lo, dah, h2p - h2m, dd2);
-        } else {
-            gl = gradient_from(l1p - l1m, dd1, l2p - l2m, dd2, s_hi - vlam, dal);
-            gh = gradient_from(h1p - h1m, dd1, h2p - h2m, dd2, vhap - s_lo, dah);
-        }
-        gsum = make_float3(gl.x + gh.x, gl.y + gh.y, gl.z + gh.z);
-        got = true;
-    }
     // perpendicular differences at both edge ends: forward (m=0) and backward (m=1)
-    const float a0p = l1p - s_lo, a0m = s_lo - l1m;
-    const float a1p = h1p - s_hi, a1m = s_hi - h1m;
-    const float b0p = l2p - s_lo, b0m = s_lo - l2m;
-    const float b1p = h2p - s_hi, b1m = s_hi - h2m;
+    const float a0p = __ldg(plo + st1) - s_lo, a0m = s_lo - __ldg(plo - st1);
+    const float a1p = __ldg(phi + st1) - s_hi, a1m = s_hi - __ldg(phi - st1);
+    const float b0p = __ldg(plo + st2) - s_lo, b0m = s_lo - __ldg(plo - st2);
+    const float b1p = __ldg(phi + st2) - s_hi, b1m = s_hi - __ldg(phi - st2);
     // widths of the cells on either side of the edge: the cell index along d is
     // (cell coordinate + o) for m = 0 and one less for m = 1
     const float rw1p = pick_r(W, d1, 1 + o1), rw1m = pick_r(W, d1, o1);
@@ -233,20 +197,8 @@ k_cell_qef(const __grid_constant__ QefParams P) {
             const float pv = axis == 1 ? along : (float)loy;
             const float pw = axis == 2 ? along : (float)loz;
             const int o1 = axis == 0 ? loy : lox, o2 = axis == 2 ? loy : loz;
-            // the min-corner edge of a face this cell owns: its winding gradients come along
-            const bool face = !(lox | loy | loz) && ((fm >> axis) & 1);
-            float3 gsum;
-            bool got = false;
             const float3 n = edge_normal(g, make_int3(i + lox, j + loy, k + loz), axis, o1, o2, s_lo, s_hi, t_lo,
-                                         pu, pv, pw, c, W, ill, face, gsum, got);
-            if (face) {
-                if (!got) {                 // outside the averaging set (a grid 2 points wide)
-                    const float3 g0 = grid_gradient32(g, i, j, k);
-                    const float3 g1 = grid_gradient32(g, i + (axis == 0), j + (axis == 1), k + (axis == 2));
-                    gsum = make_float3(g0.x + g1.x, g0.y + g1.y, g0.z + g1.z);
-                }
-                P.fgrad[(long long)axis * P.fgrad_stride + r] = make_float4(gsum.x, gsum.y, gsum.z, 0.f);
-            }
+                                         pu, pv, pw, c, W, ill);
             const float qx = pu - cu, qy = (pv - cv) * fy, qz = (pw - cw) * fz;
             const float nb = n.x * qx + n.y * qy + n.z * qz;
             kahan_add(M00, K00, n.x * n.x); kahan_add(M01, K01, n.x * n.y); kahan_add(M02, K02, n.x * n.z);
