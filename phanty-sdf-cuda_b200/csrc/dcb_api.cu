@@ -458,7 +458,6 @@ int batch_rest(dcb_context* h, const BatchLayout& L, TableView& T, const dcb_opt
     const long long wind_cap = std::min(0x7fffffffLL, 3 * cap);
     const long long v64_cap = cap;
     DCB_TRY(h, cudaMemsetAsync(h->col_count.p, 0, sizeof(uint32_t) * ncol, s), "memset");
-    DCB_TRY(h, cudaMemsetAsync(h->col_fill.p, 0, sizeof(uint32_t) * ncol, s), "memset");
     DCB_TRY(h, cudaMemsetAsync(h->v64_index.p, 0xff, sizeof(int) * cap, s), "memset");
 
     // 2) ranks + list, QEF with fused edge normals (rank-1 fast path, Jacobi list, FP64).
@@ -492,6 +491,8 @@ int batch_rest(dcb_context* h, const BatchLayout& L, TableView& T, const dcb_opt
     // 3) faces: column scan, scatter with FP32 winding, FP64 re-decisions, in-column order.
     DCB_TRY(h, launch_scan(as<uint32_t>(h->col_count), ncol, as<uint32_t>(h->partials),
                            as<uint32_t>(h->col_start), &dc->face_total, s), "launch scan");
+    DCB_TRY(h, cudaMemcpyAsync(h->col_fill.p, h->col_start.p, sizeof(uint32_t) * ncol, cudaMemcpyDeviceToDevice, s),
+            "column slots");
     if (events) {
         DCB_TRY(h, cudaEventRecord(h->ev[9], s), "event");
         h->substage_events = true;

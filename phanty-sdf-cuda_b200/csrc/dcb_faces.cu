@@ -180,6 +180,10 @@ __device__ __forceinline__ void emit_face(const FaceParams& P, int gi, int i, in
     else if (axis == 1) { r0 = r_k1 - 1u; r1 = r_k1; r3 = r - 1u; }    // (i-1,j,k-1) (i,j,k-1) (i-1,j,k)
     else { r0 = r_j1 - 1u; r1 = r_j1; r3 = r - 1u; }                   // (i-1,j-1,k) (i,j-1,k) (i-1,j,k)
     const uint32_t r2 = r;
+    // the staging slot first: it depends on the column alone, so its atomic round trip overlaps
+    // the gradient and vertex loads below (col_fill starts at each column's first slot)
+    const long long col = S.col_off + axis * cxcy + (long long)i * g.cy + j;
+    const uint32_t slot = atomicAdd(&P.col_fill[col], 1u);
     const float3 g1 = grid_gradient32(g, i + (axis == 0), j + (axis == 1), k + (axis == 2));
     const float3 gn = make_float3(g0.x + g1.x, g0.y + g1.y, g0.z + g1.z);
     const float3 pa = ldv(P.V, r0), pb = ldv(P.V, r1), pc = ldv(P.V, r2), pd = ldv(P.V, r3);
@@ -202,8 +206,6 @@ __device__ __forceinline__ void emit_face(const FaceParams& P, int gi, int i, in
     const bool uncertain = near_fallback || gn2 < 1e-4f ||
                            fabsf(d) <= 4.f * dq * gnl + 1e-5f * qnl * gnl;
     bool swap = !uncertain && gn2 > 0.f && qn2 > 0.f && d < 0.f;
-    const long long col = S.col_off + axis * cxcy + (long long)i * g.cy + j;
-    const uint32_t slot = P.col_start[col] + atomicAdd(&P.col_fill[col], 1u);
     P.stage_quad[slot] = swap ? make_int4((int)r0, (int)r3, (int)r2, (int)r1)
                               : make_int4((int)r0, (int)r1, (int)r2, (int)r3);
     P.stage_key[slot] = make_uint2((uint32_t)k, (uint32_t)col);

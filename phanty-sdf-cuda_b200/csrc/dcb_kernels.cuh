@@ -180,7 +180,7 @@ struct FaceParams {
     const uint32_t* super;
     const uint32_t* col_start;     // per grid [3][cx*cy] (global column index)
     const uint32_t* col_count;
-    uint32_t* col_fill;
+    uint32_t* col_fill;            // next free slot of each column (starts as a copy of col_start)
     int4* stage_quad;
     uint2* stage_key;              // {k, column}
     uint4* wind_items;             // {slot, axis | grid << 2, packed lo, packed hi}
