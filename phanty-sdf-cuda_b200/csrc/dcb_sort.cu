@@ -7,10 +7,9 @@
 //
 // Radix sort, one pass per digit: tile t (2048 items, one block) counts its digits into
 // hist[digit * tiles + t]; an exclusive scan of hist in that digit-major order gives every
-// (digit, tile) its first output position; the tile then places its items round by round
-// (256 items a round, item order = round, then thread): an item's position is its digit's base,
-// plus the items of that digit in earlier warps of the round (per-warp counts in shared
-// memory), plus the lanes below it with the same digit (__match_any_sync). Passes alternate
+// (digit, tile) its first output position; the tile then places its items, each warp ranking
+// a contiguous eighth (256 items) of them in its own digit counters: an item's position is its digit's
+// base, plus that digit's items in earlier warps, plus its rank in its warp. Passes alternate
 // between the output and one scratch buffer, starting so that the last pass writes the output.
 #include "dcb_kernels.cuh"
 #include "dcb_sort.cuh"
@@ -214,43 +213,55 @@ __global__ void __launch_bounds__(kThreads) k_radix_hist(const K* __restrict__ k
     for (int d = threadIdx.x; d < kRadix; d += kThreads) hist[(long long)d * ntiles + blockIdx.x] = s_cnt[d];
 }
 
+// Warp w of the tile takes items [w*256, (w+1)*256) of it, lane l of round q the item
+// w*256 + 32q + l: item order is (warp, round, lane). Each warp ranks its items in its own
+// digit counters (__match_any_sync groups the lanes with the same digit; the lowest of them
+// advances the counter after the others have read it), then one pass over the digits turns
+// the per-warp counts into each warp's first position per digit.
 template <typename K, bool PAIRS>
 __global__ void __launch_bounds__(kThreads)
 k_radix_scatter(const K* __restrict__ kin, const uint32_t* __restrict__ vin, K* __restrict__ kout, uint32_t* __restrict__ vout,
                 long long n, int shift, uint32_t mask, const uint32_t* __restrict__ offs, long long ntiles) {
-    __shared__ uint32_t s_base[kRadix];            // next position of each digit for this tile
-    __shared__ uint32_t s_wcnt[kWarps][kRadix];    // items of each digit per warp in this round
+    __shared__ uint32_t s_cnt[kWarps][kRadix];     // per warp: its items of each digit, then its first position
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (int d = tid; d < kRadix; d += kThreads) s_base[d] = offs[(long long)d * ntiles + blockIdx.x];
-    const long long base = (long long)blockIdx.x * kTile;
+    for (int x = tid; x < kWarps * kRadix; x += kThreads) s_cnt[x / kRadix][x % kRadix] = 0u;
+    __syncthreads();
+    const long long base = (long long)blockIdx.x * kTile + (long long)warp * (kItems * 32);
+    K key[kItems];
+    uint32_t val[kItems], dig[kItems], rank[kItems];
+#pragma unroll
     for (int q = 0; q < kItems; ++q) {
-        for (int x = tid; x < kWarps * kRadix; x += kThreads) s_wcnt[x / kRadix][x % kRadix] = 0u;
-        __syncthreads();
-        const long long i = base + q * kThreads + tid;
+        const long long i = base + q * 32 + lane;
         const bool have = i < n;
-        const K key = have ? kin[i] : K(0);
-        const uint32_t d = have ? ((uint32_t)(key >> shift) & mask) : 0xffffffffu;
+        key[q] = have ? kin[i] : K(0);
+        if (PAIRS) val[q] = have ? vin[i] : 0u;
+        const uint32_t d = have ? ((uint32_t)(key[q] >> shift) & mask) : 0xffffffffu;
+        dig[q] = d;
         const uint32_t peers = __match_any_sync(0xffffffffu, d);
         const uint32_t below = __popc(peers & ((1u << lane) - 1u));
-        if (have && below == 0) s_wcnt[warp][d] = (uint32_t)__popc(peers);
-        __syncthreads();
-        uint32_t pos = 0;
-        if (have) {
-            pos = s_base[d] + below;
-            for (int w = 0; w < warp; ++w) pos += s_wcnt[w][d];
-        }
-        __syncthreads();
-        for (int dd = tid; dd < kRadix; dd += kThreads) {
-            uint32_t t = 0;
+        rank[q] = have ? s_cnt[warp][d] + below : 0u;
+        __syncwarp();
+        if (have && below == 0) s_cnt[warp][d] += (uint32_t)__popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+    // digit d: the tile's first position from the global scan, then the warps in order
+    for (int d = tid; d < kRadix; d += kThreads) {
+        uint32_t run = offs[(long long)d * ntiles + blockIdx.x];
 #pragma unroll
-            for (int w = 0; w < kWarps; ++w) t += s_wcnt[w][dd];
-            s_base[dd] += t;
+        for (int w = 0; w < kWarps; ++w) {
+            const uint32_t c = s_cnt[w][d];
+            s_cnt[w][d] = run;
+            run += c;
         }
-        if (have) {
-            kout[pos] = key;
-            if (PAIRS) vout[pos] = vin[i];
-        }
-        __syncthreads();
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < kItems; ++q) {
+        if (dig[q] == 0xffffffffu) continue;
+        const uint32_t pos = s_cnt[warp][dig[q]] + rank[q];
+        kout[pos] = key[q];
+        if (PAIRS) vout[pos] = val[q];
     }
 }
 
