@@ -321,8 +321,9 @@ int dcb_autotune_mark(dcb_handle h, const dcb_grid* grids, int n, int* waves_out
  * kernel (4, 5 or 6 resident blocks of 128 threads per SM) with every launch width (8, 16 or
  * 32 blocks per SM of its grid-stride loop), timing the vertex stage, then for every width of
  * the face scatter (8, 16 or 32 blocks per SM), timing the face stage; keeps the fastest of
- * each for this handle's later extractions, batches and captured graphs. Results do not depend
- * on these choices (same arithmetic per cell and face). The choices and the sum of the two
+ * each for this handle's later extractions, batches and captured graphs. Cells and quads do not
+ * depend on these choices; vertices may differ in the last float bits between register caps
+ * (separately compiled kernels), within the same tolerance. The choices and the sum of the two
  * median stage times (ms) are returned through the optional pointers. opts may be null
  * (defaults); dual contouring only. */
 int dcb_autotune_cells(dcb_handle h, const dcb_grid* grids, int n, const dcb_opts* opts, int* qef_min_blocks_out,

@@ -69,7 +69,7 @@ __device__ float3 edge_normal(const GridDesc& g, int3 lo, int axis, int o1, int 
     const int64_t st2 = d2 == 1 ? (int64_t)g.nx : (int64_t)g.nx * g.ny;
     const float* plo = g.v + pidx(g, lo.x, lo.y, lo.z);
     const float* phi = g.v + pidx(g, hi.x, hi.y, hi.z);
-    const float ga = (s_hi - s_lo) * pick_r(W, axis, 1);
+    const float ga = (s_hi - s_lo) * (axis == 0 ? W.r[0][1] : (axis == 1 ? W.r[1][1] : W.r[2][1]));
     // perpendicular differences at both edge ends: forward (m=0) and backward (m=1)
     const float a0p = __ldg(plo + st1) - s_lo, a0m = s_lo - __ldg(plo - st1);
     const float a1p = __ldg(phi + st1) - s_hi, a1m = s_hi - __ldg(phi - st1);
@@ -77,13 +77,18 @@ __device__ float3 edge_normal(const GridDesc& g, int3 lo, int axis, int o1, int 
     const float b1p = __ldg(phi + st2) - s_hi, b1m = s_hi - __ldg(phi - st2);
     // widths of the cells on either side of the edge: the cell index along d is
     // (cell coordinate + o) for m = 0 and one less for m = 1
-    const float rw1p = pick_r(W, d1, 1 + o1), rw1m = pick_r(W, d1, o1);
-    const float rw2p = pick_r(W, d2, 1 + o2), rw2m = pick_r(W, d2, o2);
+    // (d1 is y for X edges, else x; d2 is y for Z edges, else z)
+    const float rw1p = d1 == 0 ? (o1 ? W.r[0][2] : W.r[0][1]) : (o1 ? W.r[1][2] : W.r[1][1]);
+    const float rw1m = d1 == 0 ? (o1 ? W.r[0][1] : W.r[0][0]) : (o1 ? W.r[1][1] : W.r[1][0]);
+    const float rw2p = d2 == 1 ? (o2 ? W.r[1][2] : W.r[1][1]) : (o2 ? W.r[2][2] : W.r[2][1]);
+    const float rw2m = d2 == 1 ? (o2 ? W.r[1][1] : W.r[1][0]) : (o2 ? W.r[2][1] : W.r[2][0]);
     // one cancellation bound per edge (>= each cell's own bound)
     const float m1v = fmaxf(fmaxf(fabsf(a0p), fabsf(a1p)) * rw1p, fmaxf(fabsf(a0m), fabsf(a1m)) * rw1m);
     const float m2v = fmaxf(fmaxf(fabsf(b0p), fabsf(b1p)) * rw2p, fmaxf(fabsf(b0m), fabsf(b1m)) * rw2m);
     const float bound2 = kNormalCond2 * (ga * ga + m1v * m1v + m2v * m2v);
-    float3 acc = make_float3(0.f, 0.f, 0.f);
+    // the four gradients (along the edge, along d1, along d2) summed in the edge's own frame,
+    // then placed on x, y, z
+    float sa = 0.f, s1 = 0.f, s2 = 0.f;
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
         const int m1 = q & 1, m2 = q >> 1;
@@ -93,17 +98,17 @@ __device__ float3 edge_normal(const GridDesc& g, int3 lo, int axis, int o1, int 
         const float e2lo = m2 ? b0m : b0p, e2hi = m2 ? b1m : b1p;
         const float g1 = (e1lo + u * (e1hi - e1lo)) * (m1 ? rw1m : rw1p);
         const float g2 = (e2lo + u * (e2hi - e2lo)) * (m2 ? rw2m : rw2p);
-        float3 gv;
-        if (axis == 0) gv = make_float3(ga, g1, g2);
-        else if (axis == 1) gv = make_float3(g1, ga, g2);
-        else gv = make_float3(g1, g2, ga);
-        const float gn2 = gv.x * gv.x + gv.y * gv.y + gv.z * gv.z;
+        const float gn2 = ga * ga + g1 * g1 + g2 * g2;
         if (gn2 <= bound2) ill = true;
         if (gn2 > 0.f) {
             const float rn = rsqrtf(gn2);
-            acc.x += gv.x * rn; acc.y += gv.y * rn; acc.z += gv.z * rn;
+            sa += ga * rn; s1 += g1 * rn; s2 += g2 * rn;
         }
     }
+    float3 acc;
+    if (axis == 0) acc = make_float3(sa, s1, s2);
+    else if (axis == 1) acc = make_float3(s1, sa, s2);
+    else acc = make_float3(s1, s2, sa);
     if (acc.x * acc.x + acc.y * acc.y + acc.z * acc.z < 1e-4f) ill = true;
     return normalized(acc);
 }

@@ -98,7 +98,9 @@ def test_autotune_keeps_the_results(backend):
 
 def test_cell_autotune_keeps_the_results():
     """The vertex/face autotuner picks a register cap and launch widths among its candidates;
-    batches and single extractions afterwards equal those before it bit for bit."""
+    batches and single extractions afterwards give the same quads and vertices within the
+    parity tolerance (the register caps are separately compiled kernels, whose multiply-adds
+    may round differently in the last bit)."""
     import torch
     from contouring_b200 import B200DualContouringBackend, synth
     be = B200DualContouringBackend(0)
@@ -112,10 +114,12 @@ def test_cell_autotune_keeps_the_results():
         m, q, f, ms = be.autotune_cells(grids)
         assert m in (4, 5, 6) and q in (8, 16, 32) and f in (8, 16, 32) and ms > 0
         after, _ = be.extract_batch(grids)
-        for (Va, Fa), (Vb, Fb) in zip(before, after):
-            assert torch.equal(Va, Vb) and torch.equal(Fa, Fb)
+        for (Va, Fa), (Vb, Fb), (_, _, sp, _) in zip(before, after, grids):
+            assert torch.equal(Fa, Fb)
+            assert float((Va - Vb).abs().max()) <= VERTEX_TOL * min(sp)
         V2, F2, _ = be.extract_tensor(*single)
-        assert torch.equal(V1, V2) and torch.equal(F1, F2)
+        assert torch.equal(F1, F2)
+        assert float((V1 - V2).abs().max()) <= VERTEX_TOL * min(single[2])
         print("autotuned cell kernels: vertex cap %d blocks/SM, width %d, faces width %d; %.3f ms" % (m, q, f, ms))
     finally:
         be.close()
