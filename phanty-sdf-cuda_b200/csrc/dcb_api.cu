@@ -61,7 +61,7 @@ struct dcb_context {
     bool substage_events = false;     // ev[8] / ev[9] hold the face sub-stages of the last call
     DevBuf grid, bits, super, list, seg_count, seg_start, counters, V, vclass, fmask, col_count, col_fill,
         col_start, partials, esc_list, hard_list, hard_data, stage_quad, stage_key, faces, wind_items,
-        v64_index, v64_cells, V64, tris, tri_items, adj_rows, adj_owners, ours_ws;
+        v64_index, v64_cells, V64, tris, tri_items, adj_rows, adj_owners, ours_ws, wt;
     // sparse backends
     DevBuf sp_words, sp_brick, sp_vcount, sp_vstart, sp_vtmp, sp_ntmp, sp_N, sp_vcell, sp_fcount, sp_fstart,
         sp_stage, sp_counters;
@@ -209,7 +209,7 @@ struct BatchLayout {
     // mark launches: index 1 for 256-cell x-tiles, 0 for 1024-cell ones
     std::vector<int> tile_slot[2];                    // grids of each mark launch
     std::vector<long long> tile_off[2];               // their first tiles (+ total)
-    long long bits = 0, super = 0, nseg = 0, ncol = 0, ncell = 0;
+    long long bits = 0, super = 0, nseg = 0, ncol = 0, ncell = 0, wt = 0;
     float hmax = 0.f;
 };
 
@@ -255,6 +255,8 @@ int layout_batch(dcb_context* h, const dcb_grid* in, int n, BatchLayout& L) {
         L.tile_slot[grp].push_back(b);
         L.tile_off[grp].push_back(L.tile_off[grp].back() + (long long)S.nxt * S.nrb * S.nzc);
         S.hmax = std::max(std::fabs(g.vx), std::max(std::fabs(g.vy), std::fabs(g.vz)));
+        S.wt_off = L.wt;
+        L.wt += width_table_len(g.cx, g.cy, g.cz);
         L.hmax = std::max(L.hmax, S.hmax);
     }
     L.seg_off[n] = L.nseg;
@@ -374,6 +376,7 @@ int batch_prepare(dcb_context* h, const dcb_grid* in, int n, cudaStream_t s, Bat
     DCB_TRY(h, ensure(h->col_count, sizeof(uint32_t) * ncol), "alloc column counts");
     DCB_TRY(h, ensure(h->col_fill, sizeof(uint32_t) * ncol), "alloc column fill");
     DCB_TRY(h, ensure(h->col_start, sizeof(uint32_t) * ncol), "alloc column starts");
+    DCB_TRY(h, ensure(h->wt, sizeof(float) * L.wt), "alloc cell-width tables");
     const long long plen = std::max(scan_partials_len(ncol), scan_partials_len(nseg));
     DCB_TRY(h, ensure(h->partials, sizeof(uint32_t) * std::max(1LL, plen)), "alloc scan");
     if (!h->h_counters) DCB_TRY(h, host_malloc(&h->h_counters, sizeof(Counters)), "alloc pinned counters");
@@ -468,9 +471,11 @@ int batch_rest(dcb_context* h, const BatchLayout& L, TableView& T, const dcb_opt
     xp.B.cell_slot = nullptr;                      // expand finds grids by segment
     xp.list_cap = cap;
     DCB_TRY(h, launch_expand(xp, h->num_sms, s), "launch expand");
+    DCB_TRY(h, launch_width_tables(T.B, as<float>(h->wt), s), "launch width tables");
     QefParams qp;
     qp.B = T.B; qp.list = xp.list; qp.nactive = cap; qp.live = live; qp.V = as<float>(h->V); qp.vclass = as<uint8_t>(h->vclass);
     qp.fmask = as<uint8_t>(h->fmask); qp.col_count = as<uint32_t>(h->col_count);
+    qp.wt = as<float>(h->wt);
     qp.esc_list = as<uint32_t>(h->esc_list); qp.esc_count = &dc->esc_count;
     qp.hard_list = as<uint32_t>(h->hard_list); qp.hard_data = as<float4>(h->hard_data); qp.hard_count = &dc->hard_count;
     qp.rank_hist = dc->rank_hist;
@@ -1115,7 +1120,7 @@ int dcb_destroy(dcb_handle h) {
                       &h->tris, &h->tri_items, &h->m_verts, &h->m_faces, &h->m_out, &h->m_tris,
                       &h->m_bin_count, &h->m_bin_start, &h->m_bin_fill, &h->m_bin_scratch, &h->m_bin_tris,
                       &h->m_bin_active, &h->m_active_list, &h->m_axis_start, &h->m_far, &h->m_ext, &h->m_tmp,
-                      &h->m_partials, &h->m_counters, &h->m_vox, &h->table, &h->cell_slot, &h->adj_rows, &h->adj_owners, &h->ours_ws,
+                      &h->m_partials, &h->m_counters, &h->m_vox, &h->table, &h->cell_slot, &h->adj_rows, &h->adj_owners, &h->ours_ws, &h->wt,
                       &h->sp_words, &h->sp_brick, &h->sp_vcount, &h->sp_vstart, &h->sp_vtmp, &h->sp_ntmp,
                       &h->sp_N, &h->sp_vcell, &h->sp_fcount, &h->sp_fstart, &h->sp_stage, &h->sp_counters};
     for (DevBuf* b : bufs) if (b->p) cudaFree(b->p);

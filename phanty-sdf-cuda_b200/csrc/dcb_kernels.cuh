@@ -22,7 +22,14 @@ struct GridSlot {
     int nzc;                       // mark: z-chunks
     int tw;                        // mark: cell words per x-tile (32, or 8 for narrow grids)
     float hmax;                    // largest cell width of the grid (world units)
+    long long wt_off;              // first entry of the grid's cell-width tables (width_tables)
 };
+
+// Cell-width tables of a grid (k_width_tables): for each axis the widths of cells -1..n (n the
+// cells along it), entry c + 1 for cell c, then their reciprocals: w_x, w_y, w_z, r_x, r_y, r_z.
+__host__ __device__ inline long long width_table_len(int cx, int cy, int cz) {
+    return 2LL * ((long long)cx + cy + cz + 6);
+}
 
 struct BatchTable {
     GridSlot s0;                           // the grid when n == 1 (read from kernel parameters)
@@ -115,6 +122,7 @@ struct QefParams {
     long long nactive;             // active cells (capacity when live is set)
     const unsigned long long* live; // device count of active cells (a captured graph; above
                                     // nactive, nothing is processed), or null
+    const float* wt;                // cell-width tables of every grid (k_width_tables)
     float* V;
     uint8_t* vclass;                // [active] VertexClass
     uint8_t* fmask;                 // bit a: cell owns a face on its min-corner edge a
@@ -135,6 +143,7 @@ struct QefParams {
 };
 // minb: k_cell_qef's register cap (resident blocks per SM: 4, 5 or 6); blocks_per_sm: the width
 // of its grid-stride launch
+cudaError_t launch_width_tables(const BatchTable& B, float* wt, cudaStream_t s);
 cudaError_t launch_cell_qef(const QefParams& P, int num_sms, cudaStream_t s, int minb = 5, int blocks_per_sm = 32);
 cudaError_t launch_cell_jacobi(const QefParams& P, long long max_items, int num_sms, cudaStream_t s);
 

@@ -102,23 +102,12 @@ static __constant__ uint32_t c_edge_geo[12] = {edge_geo(0), edge_geo(1), edge_ge
                                         edge_geo(6), edge_geo(7), edge_geo(8), edge_geo(9), edge_geo(10), edge_geo(11)};
 
 // Widths (and reciprocals) of the cells i-1, i, i+1 along each axis, exact float
-// differences of the float grid positions (the CPU forms positions the same way).
+// differences of the float grid positions (the CPU forms positions the same way), read from
+// the per-grid tables of k_width_tables.
 struct Widths {
     float w[3][3];   // [axis][offset+1]
     float r[3][3];
 };
-__device__ __forceinline__ void cell_widths(const GridDesc& g, int i, int j, int k, Widths& W) {
-    const int idx[3] = {i, j, k};
-    const float o[3] = {g.ox, g.oy, g.oz}, v[3] = {g.vx, g.vy, g.vz};
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        float pm = pos_axis(o[a], v[a], idx[a] - 1), p0 = pos_axis(o[a], v[a], idx[a]);
-        float p1 = pos_axis(o[a], v[a], idx[a] + 1), p2 = pos_axis(o[a], v[a], idx[a] + 2);
-        W.w[a][0] = p0 - pm; W.w[a][1] = p1 - p0; W.w[a][2] = p2 - p1;
-#pragma unroll
-        for (int q = 0; q < 3; ++q) W.r[a][q] = 1.f / W.w[a][q];
-    }
-}
 
 // W.r[a][q] for runtime a, q with literal array indices only (keeps W in registers).
 __device__ __forceinline__ float pick_r(const Widths& W, int a, int q) {

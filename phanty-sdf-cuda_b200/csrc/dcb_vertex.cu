@@ -113,6 +113,35 @@ __device__ float3 edge_normal(const GridDesc& g, int3 lo, int axis, int o1, int 
     return normalized(acc);
 }
 
+// ---- cell-width tables ------------------------------------------------------------------
+
+// Block row b fills grid b's tables: the width of cell c along an axis is the difference of
+// the float positions of its two planes (grid.ox + i * grid.vx rounded in float, as the CPU
+// backend forms positions, dc_backend.cpp:63-65), its reciprocal 1 / width.
+__global__ void __launch_bounds__(256) k_width_tables(const BatchTable B, float* __restrict__ wt) {
+    const GridSlot& S = B.n == 1 ? B.s0 : B.slots[blockIdx.y];
+    const GridDesc& g = S.g;
+    const int nx = g.cx + 2, ny = g.cy + 2, nz = g.cz + 2;
+    const int total = nx + ny + nz;
+    float* const t = wt + S.wt_off;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
+        float o, vv;
+        int c;
+        if (e < nx)           { o = g.ox; vv = g.vx; c = e - 1; }
+        else if (e < nx + ny) { o = g.oy; vv = g.vy; c = e - nx - 1; }
+        else                  { o = g.oz; vv = g.vz; c = e - nx - ny - 1; }
+        const float w = pos_axis(o, vv, c + 1) - pos_axis(o, vv, c);
+        t[e] = w;
+        t[total + e] = 1.f / w;
+    }
+}
+
+cudaError_t launch_width_tables(const BatchTable& B, float* wt, cudaStream_t s) {
+    if (B.n <= 0) return cudaSuccess;
+    k_width_tables<<<dim3(4, (unsigned)B.n), 256, 0, s>>>(B, wt);
+    return cudaGetLastError();
+}
+
 // ---- k_cell_qef -------------------------------------------------------------------------
 
 // MINB: resident blocks per SM the register allocation must allow (the register cap); the
@@ -177,8 +206,20 @@ k_cell_qef(const __grid_constant__ QefParams P) {
         }
         const float invm = 1.f / (float)__popc(hmask);
         cu *= invm; cv *= invm; cw *= invm;
+        // this cell's and its two neighbours' widths along each axis, from the tables
         Widths W;
-        cell_widths(g, i, j, k, W);
+        {
+            const float* const t = P.wt + S.wt_off;
+            const int nx = g.cx + 2, ny = g.cy + 2, nz = g.cz + 2, tot = nx + ny + nz;
+            const int e0[3] = {i, nx + j, nx + ny + k};   // entry of cell index - 1
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+#pragma unroll
+                for (int q = 0; q < 3; ++q) {
+                    W.w[a][q] = __ldg(t + e0[a] + q);
+                    W.r[a][q] = __ldg(t + tot + e0[a] + q);
+                }
+        }
         const float fy = W.w[1][1] * W.r[0][1], fz = W.w[2][1] * W.r[0][1];
 
         // Pass 2: each lane walks its own crossing edges (warp iterations = max count).
