@@ -21,6 +21,7 @@ import statistics
 import subprocess
 import sys
 import tempfile
+import threading
 import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
@@ -73,17 +74,58 @@ def _peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clock / throttle sampling during the timed region."""
+    """SM clock and throttle-reason sampling during the timed region: NVML polled every 2 ms
+    from a thread (the timed calls release the GIL while they wait on the device), so a region
+    of tens of milliseconds still gets samples; nvidia-smi every 100 ms when NVML is missing."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clock event reason bits
+    REASONS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40}
 
     def __init__(self, gpu_index):
         self.gpu = gpu_index
         self.proc = None
         self.path = None
+        self.nvml = None
+        self.thread = None
+        self.stop = False
+        self.sm, self.mx, self.bits = [], None, 0
+
+    def _nvml_handle(self):
+        """This process's CUDA device as an NVML handle, found by its UUID (or its PCI
+        address); only strings reach NVML's string arguments."""
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        props = torch.cuda.get_device_properties(self.gpu)
+        uuid = str(getattr(props, "uuid", "") or "")
+        if uuid:
+            return pynvml, pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        bus = "%08x:%02x:%02x.0" % (int(props.pci_domain_id), int(props.pci_bus_id), int(props.pci_device_id))
+        return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+
+    def _poll(self, pynvml, h):
+        get_reasons = getattr(pynvml, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            pynvml.nvmlDeviceGetCurrentClocksThrottleReasons
+        while not self.stop:
+            try:
+                self.sm.append(float(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)))
+                self.bits |= int(get_reasons(h))
+            except Exception:
+                pass
+            time.sleep(0.002)
 
     def __enter__(self):
+        try:
+            pynvml, h = self._nvml_handle()
+            self.mx = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+            self.nvml = pynvml
+            self.thread = threading.Thread(target=self._poll, args=(pynvml, h), daemon=True)
+            self.thread.start()
+            return self
+        except Exception:
+            self.nvml = None
         fd, self.path = tempfile.mkstemp(suffix=".csv")
         os.close(fd)
         try:
@@ -96,6 +138,9 @@ class ClockSampler:
         return self
 
     def __exit__(self, *a):
+        if self.thread:
+            self.stop = True
+            self.thread.join(timeout=5)
         if self.proc:
             self.proc.terminate()
             try:
@@ -104,6 +149,10 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
+        if self.nvml is not None:
+            reasons = sorted(n for n, bit in self.REASONS.items() if self.bits & bit)
+            return {"sm_mhz": statistics.median(self.sm) if self.sm else None, "sm_max_mhz": self.mx,
+                    "reasons": reasons, "samples": len(self.sm), "source": "nvml"}
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         try:
@@ -123,7 +172,7 @@ class ClockSampler:
         except Exception:
             pass
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm), "source": "nvidia-smi"}
 
 
 def make_grid(res, device):
