@@ -27,10 +27,11 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "phanty-sdf-cuda_b200"))
 
-# Launches of the engine's own kernels per extraction: mark, 3 scan passes, rank expansion,
-# edge normals, QEF, Jacobi list, FP64 vertices, 3 column-scan passes, face scatter,
-# FP64 vertices for windings, FP64 windings, face order.
-KERNELS_PER_STEP = 16
+# Launches of the engine's own kernels per extraction: mark, 3 segment-scan passes, vertex
+# offsets, rank expansion, cell-width tables, QEF (with the edge normals), Jacobi list, FP64
+# vertices, 3 column-scan passes, face scatter, FP64 vertices for windings, FP64 windings,
+# face order.
+KERNELS_PER_STEP = 17
 # DRAM traffic of k_mark_zmarch per grid point, from a single-kernel ncu capture of the 512^3
 # CSG workload (dram__bytes_read.sum + dram__bytes_write.sum divided by the grid points of
 # that capture; the kernel streams the grid once, so traffic scales with the number of
