@@ -584,6 +584,19 @@ int batch_finish(dcb_context* h, int n, const dcb_opts* o, dcb_stats* st) {
     return DCB_OK;
 }
 
+// Active cells every per-cell buffer of the workspace holds (0 before the first extraction).
+long long cell_capacity(const dcb_context* h, const dcb_opts* o) {
+    long long c = (long long)(h->list.bytes / sizeof(uint64_t));
+    auto lim = [&c](const DevBuf& b, size_t per) { c = std::min(c, (long long)(b.bytes / per)); };
+    lim(h->V, 3 * sizeof(float)); lim(h->fmask, 1); lim(h->vclass, 1);
+    lim(h->esc_list, sizeof(uint32_t)); lim(h->hard_list, sizeof(uint32_t)); lim(h->hard_data, 3 * sizeof(float4));
+    lim(h->stage_quad, 3 * sizeof(int4)); lim(h->stage_key, 3 * sizeof(uint2)); lim(h->faces, 3 * sizeof(int4));
+    lim(h->v64_index, sizeof(int)); lim(h->wind_items, 3 * sizeof(uint4)); lim(h->v64_cells, sizeof(uint32_t));
+    lim(h->V64, 3 * sizeof(double));
+    if (o->emit_triangles) { lim(h->tris, 18 * sizeof(int)); lim(h->tri_items, 3 * sizeof(uint32_t)); }
+    return std::min(c, 0x7fffffffLL / 3);      // the winding list holds exactly 3 entries per cell
+}
+
 int run_batch(dcb_context* h, const dcb_grid* in, int n, const dcb_opts* o, cudaStream_t s, dcb_stats* st) {
     ++h->gen;
     BatchLayout L;
@@ -597,6 +610,35 @@ int run_batch(dcb_context* h, const dcb_grid* in, int n, const dcb_opts* o, cuda
     // 1) mark: active bits + per-segment counts; scan -> segment starts and the total.
     rc = batch_mark(h, L, T, s, true);
     if (rc != DCB_OK) return rc;
+    const long long cap = cell_capacity(h, o);
+    if (cap > 0) {
+        // 2) on the buffers of an earlier call, with no wait for the count: the kernels read it
+        // on the device (above cap, every kernel past the mark does nothing)
+        rc = batch_alloc(h, n, cap, o, T);
+        if (rc != DCB_OK) return rc;
+        rc = batch_rest(h, L, T, o, s, cap, &dc->total_active, true);
+        if (rc != DCB_OK) return rc;
+        DCB_TRY(h, cudaEventRecord(h->ev[4], s), "event");
+        DCB_TRY(h, cudaMemcpyAsync(hc, dc, sizeof(Counters), cudaMemcpyDeviceToHost, s), "read counters");
+        DCB_TRY(h, cudaMemcpyAsync(h_vert_off, T.vert_off, sizeof(unsigned long long) * (n + 1),
+                                   cudaMemcpyDeviceToHost, s), "read vertex offsets");
+        DCB_TRY(h, cudaStreamSynchronize(s), "pipeline");
+        const long long nv = (long long)hc->total_active;
+        if (nv >= 0x7fffffffLL) return fail(h, DCB_ERR_TOO_LARGE, "more than 2^31-1 vertices");
+        batch_state(h, L, n, o, nv);
+        if (st) {
+            st->nx = L.slots[0].g.nx; st->ny = L.slots[0].g.ny; st->nz = L.slots[0].g.nz;
+            st->total_cells = L.ncell; st->active_cells = nv; st->vertex_count = nv;
+        }
+        if (nv <= cap) return batch_finish(h, n, o, st);
+        // more active cells than those buffers hold: the marks, counts and ranks stand; the rest
+        // runs again below with buffers for nv cells (the counters past the mark start over)
+        const Counters keep = *hc;
+        std::memset(hc, 0, sizeof(Counters));
+        hc->total_active = keep.total_active;
+        hc->nonfinite = keep.nonfinite;
+        DCB_TRY(h, cudaMemcpyAsync(dc, hc, sizeof(Counters), cudaMemcpyHostToDevice, s), "reset counters");
+    }
     DCB_TRY(h, cudaMemcpyAsync(hc, dc, sizeof(Counters), cudaMemcpyDeviceToHost, s), "read count");
     DCB_TRY(h, cudaMemcpyAsync(h_vert_off, T.vert_off, sizeof(unsigned long long) * (n + 1), cudaMemcpyDeviceToHost, s),
             "read vertex offsets");
