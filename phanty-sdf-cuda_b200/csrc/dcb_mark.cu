@@ -57,7 +57,9 @@ __device__ __forceinline__ void load_row(const float* __restrict__ row, int x0, 
 
 // Negative / positive bit words of the loaded segment (word q covers points x0+32q..+31).
 template <int TW>
-__device__ __forceinline__ void row_words(const RowRegs<TW>& R, int lane, uint32_t* nw, uint32_t* pw, bool& bad) {
+// inf_nan: stays 0 while every value is finite; fma(q, 0, x) turns it NaN for good at an
+// infinite or NaN q (one instruction a point; the intrinsic is never simplified away).
+__device__ __forceinline__ void row_words(const RowRegs<TW>& R, int lane, uint32_t* nw, uint32_t* pw, float& inf_nan) {
     constexpr int kPtWords = Tile<TW>::kPtWords;
 #pragma unroll
     for (int c = 0; c < Tile<TW>::kChunks; ++c) {
@@ -66,7 +68,7 @@ __device__ __forceinline__ void row_words(const RowRegs<TW>& R, int lane, uint32
         for (int s = 0; s < 4; ++s) {
             const int w = 4 * c + s;
             if (w >= kPtWords) break;
-            bad |= !(fabsf(q[s]) <= 3.402823466e38f);           // NaN or infinite
+            inf_nan = __fmaf_rn(q[s], 0.f, inf_nan);
             const uint32_t n = __ballot_sync(0xffffffffu, q[s] < 0.f);
             const uint32_t p = __ballot_sync(0xffffffffu, q[s] > 0.f);
             if (lane == 0) { nw[w] = n; pw[w] = p; }
@@ -102,10 +104,10 @@ k_mark_zmarch(const __grid_constant__ MarkParams P) {
     const int64_t plane = (int64_t)g.nx * g.ny;
 
     RowRegs<TW> cur;
-    bool bad = false;                          // a NaN or infinite value among this lane's points
+    float inf_nan = 0.f;                       // NaN once a NaN or infinite value is among this lane's points
     if (loader) {
         load_row<TW>(base + (int64_t)kb * plane, x0, g.nx, lane, cur);
-        row_words<TW>(cur, lane, s_nw[kb & 1][warp], s_pw[kb & 1][warp], bad);
+        row_words<TW>(cur, lane, s_nw[kb & 1][warp], s_pw[kb & 1][warp], inf_nan);
         load_row<TW>(base + (int64_t)(kb + 1) * plane, x0, g.nx, lane, cur);
     }
     const bool word_lane = TW == 32 || lane < TW;   // lanes beyond the tile's words idle
@@ -117,7 +119,7 @@ k_mark_zmarch(const __grid_constant__ MarkParams P) {
     for (int k = kb; k < ke; ++k) {
         const int p1 = (k + 1) & 1, p0 = k & 1;
         if (loader) {
-            row_words<TW>(cur, lane, s_nw[p1][warp], s_pw[p1][warp], bad);
+            row_words<TW>(cur, lane, s_nw[p1][warp], s_pw[p1][warp], inf_nan);
             if (k + 2 <= ke) load_row<TW>(base + (int64_t)(k + 2) * plane, x0, g.nx, lane, cur);
         }
         __syncthreads();
@@ -138,7 +140,7 @@ k_mark_zmarch(const __grid_constant__ MarkParams P) {
         __syncthreads();
     }
     // the host learns that the grid holds non-finite values (their cells take the FP64 path)
-    if (__syncthreads_or(bad) && threadIdx.x == 0 && P.nonfinite) atomicOr(P.nonfinite, 1);
+    if (__syncthreads_or(isnan(inf_nan)) && threadIdx.x == 0 && P.nonfinite) atomicOr(P.nonfinite, 1);
 }
 
 // Segments with at most this many active cells are expanded by one lane.
