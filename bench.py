@@ -36,7 +36,7 @@ KERNELS_PER_STEP = 17
 # CSG workload (dram__bytes_read.sum + dram__bytes_write.sum divided by the grid points of
 # that capture; the kernel streams the grid once, so traffic scales with the number of
 # points). None = not measured.
-MARK_TRAFFIC_BYTES_PER_POINT = (563.814656e6 + 18.4768e6) / 512 ** 3
+MARK_TRAFFIC_BYTES_PER_POINT = (564.13824e6 + 18.598144e6) / 512 ** 3
 # DRAM traffic of a whole extraction (every kernel of one step), as grid-proportional bytes per
 # point plus band-proportional bytes per active cell, from single-kernel-list ncu captures
 # (dram__bytes_read.sum + dram__bytes_write.sum summed over the step's launches). None = not
