@@ -239,20 +239,26 @@ k_face_scatter(const __grid_constant__ FaceParams P) {
     // a captured graph whose live count exceeds the capacity it was built for does nothing
     // (the host reports the overflow after the replay)
     const long long nact = P.live ? ((long long)*P.live > P.nactive ? 0 : (long long)*P.live) : P.nactive;
-    for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x - lane); base < nact;
-         base += stride) {                                                // warp-uniform
+    // the face mask and list entry of the next grid-stride step are loaded one step ahead
+    long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x - lane);
+    uint32_t fm_next = 0;
+    uint64_t pk_next = 0;
+    if (base + lane < nact) { fm_next = P.fmask[base + lane]; pk_next = P.list[base + lane]; }
+    for (; base < nact; base += stride) {                                 // warp-uniform
         const long long rr = base + lane;
-        uint32_t fm = 0;
+        const uint32_t fm = fm_next;
+        const uint64_t pk = pk_next;
+        fm_next = 0;
+        if (rr + stride < nact) { fm_next = P.fmask[rr + stride]; pk_next = P.list[rr + stride]; }
         int gi = 0, i = 0, j = 0, k = 0;
         float3 g0 = make_float3(0.f, 0.f, 0.f);
         uint32_t r_k1 = 0xffffffffu, r_j1 = 0xffffffffu, r_jk = 0xffffffffu;
-        if (rr < nact) fm = P.fmask[rr];
         if (fm) {
             gi = ONE ? 0 : slot_of_rank(P.B, (unsigned long long)rr);
             const GridSlot& S = slot_ref<ONE>(P.B, gi);
             const uint32_t* const bits = P.bits + S.bits_off;
             const uint32_t* const super = P.super + S.super_off;
-            unpack_cell(P.list[rr], i, j, k);
+            unpack_cell(pk, i, j, k);
             g0 = grid_gradient32(S.g, i, j, k);
             // All four cells of a face are active, so a cell's x-1 neighbour in a face is the
             // previous active cell in linear order (rank - 1).

@@ -158,14 +158,19 @@ k_cell_qef(const __grid_constant__ QefParams P) {
     // a captured graph whose live count exceeds the capacity it was built for does nothing
     // (the host reports the overflow after the replay)
     const long long nact = P.live ? ((long long)*P.live > P.nactive ? 0 : (long long)*P.live) : P.nactive;
-    for (long long r = (long long)blockIdx.x * blockDim.x + tid; r < nact;
-         r += (long long)gridDim.x * blockDim.x) {
+    // the list entry of the next grid-stride step is loaded one step ahead
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const long long first = (long long)blockIdx.x * blockDim.x + tid;
+    uint64_t pk_next = first < nact ? P.list[first] : 0;
+    for (long long r = first; r < nact; r += stride) {
+        const uint64_t pk = pk_next;
+        if (r + stride < nact) pk_next = P.list[r + stride];
         const GridSlot& S = slot_ref<ONE>(P.B, ONE ? 0 : slot_of_rank(P.B, (unsigned long long)r));
         const GridDesc& g = S.g;
         const long long cxcy = (long long)g.cx * g.cy;
         uint32_t* const col_count = P.col_count + S.col_off;
         int i, j, k;
-        unpack_cell(P.list[r], i, j, k);
+        unpack_cell(pk, i, j, k);
         float c[8];
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
