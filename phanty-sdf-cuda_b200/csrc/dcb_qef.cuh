@@ -47,8 +47,6 @@ __device__ __forceinline__ int3 add3(int3 a, int axis, int d) {
     if (axis == 0) a.x += d; else if (axis == 1) a.y += d; else a.z += d;
     return a;
 }
-__device__ __forceinline__ int comp(int3 a, int axis) { return axis == 0 ? a.x : (axis == 1 ? a.y : a.z); }
-__device__ __forceinline__ float ldp(const GridDesc& g, int3 p) { return ldv(g, p.x, p.y, p.z); }
 
 __device__ __forceinline__ void kahan_add(float& s, float& c, float x) {
     const float y = x - c;
@@ -108,14 +106,6 @@ struct Widths {
     float w[3][3];   // [axis][offset+1]
     float r[3][3];
 };
-
-// W.r[a][q] for runtime a, q with literal array indices only (keeps W in registers).
-__device__ __forceinline__ float pick_r(const Widths& W, int a, int q) {
-    const float r0 = q == 0 ? W.r[0][0] : (q == 1 ? W.r[0][1] : W.r[0][2]);
-    const float r1 = q == 0 ? W.r[1][0] : (q == 1 ? W.r[1][1] : W.r[1][2]);
-    const float r2 = q == 0 ? W.r[2][0] : (q == 1 ? W.r[2][1] : W.r[2][2]);
-    return a == 0 ? r0 : (a == 1 ? r1 : r2);
-}
 
 // Local -> world: one double combination per axis, one float rounding.
 __device__ __forceinline__ void store_vertex(float* __restrict__ V, const GridDesc& g, long long r, int i, int j, int k,
