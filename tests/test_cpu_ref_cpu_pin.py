@@ -69,3 +69,21 @@ def test_anisotropic_spacing_and_offset_origin():
     from contouring_b200 import synth
     vals, dims, sp, org = synth.noise((19, 14, 11), seed=12)
     _check(vals, dims, (0.05, 0.11, 0.031), (-0.73, 0.2, 1.5), "anisotropic")
+
+
+def test_tiny_differences_and_far_origin():
+    """A plane whose values differ by less than 1e-6 along z (the lerp parameter is then formed
+    in double, Cell.cpp:49-52) on a grid placed far from the origin, where the float positions
+    origin + i * spacing round (dc_backend.cpp:63-65)."""
+    n = (13, 11, 16)
+    k = np.arange(n[2], dtype=np.float64)[:, None, None]
+    j = np.arange(n[1], dtype=np.float64)[None, :, None]
+    i = np.arange(n[0], dtype=np.float64)[None, None, :]
+    vals = (1e-7 * (k - 7.3) + 2e-9 * np.sin(i + 2.0 * j)).astype(np.float32) * np.ones((1, n[1], n[0]), np.float32)
+    _check(vals.reshape(-1), n, (0.0625, 0.0625, 0.0625), (1000.25, -2048.5, 333.3), "tiny_far")
+
+
+@pytest.mark.parametrize("seed", [5, 6, 7, 8])
+def test_csg_seeds(seed):
+    from contouring_b200 import synth
+    _check(*synth.csg(28, seed=seed), "csg28_seed%d" % seed)
