@@ -191,3 +191,29 @@ def test_triangulate_flips_against_the_quad_normal():
     assert T.tolist() == [[0, 1, 2], [0, 3, 2]]
     Z = np.zeros((4, 3))
     assert O.triangulate(Z, np.array([[0, 1, 2, 3]])).tolist() == [[0, 1, 2], [0, 2, 3]]
+
+
+def test_negated_grid_flips_every_quad():
+    """Negating every value keeps the active cells and the vertices (the normal equations see
+    each normal twice, so its sign cancels; only lerp_t's +1e-16 moves the samples by ~1e-16)
+    and reverses every quad's winding: the orientation test is dot(quad normal, gradient sum),
+    and the gradients negate exactly (contouring.cpp:624-641)."""
+    vals, dims, sp, org = _np(_synth().csg(32, seed=4))
+    a = O.dc_extract(vals, dims, sp, org)
+    b = O.dc_extract(-vals, dims, sp, org)
+    assert np.array_equal(a["cells"], b["cells"])
+    assert np.abs(a["V"] - b["V"]).max() <= 1e-9 * min(sp)
+    assert len(a["F"]) == len(b["F"]) > 0
+    assert np.array_equal(b["F"], a["F"][:, [0, 3, 2, 1]])
+
+
+def test_power_of_two_scale_keeps_the_mesh():
+    """Scaling every value by 4 keeps every sign, every lerp parameter (up to lerp_t's +1e-16)
+    and every normal direction, so the same cells, quads and windings, and the vertices to
+    ~1e-13 (contouring.cpp:486-741, Cell.cpp:49-52, 80-155)."""
+    vals, dims, sp, org = _np(_synth().csg(32, seed=6))
+    a = O.dc_extract(vals, dims, sp, org)
+    b = O.dc_extract(vals * np.float32(4.0), dims, sp, org)
+    assert np.array_equal(a["cells"], b["cells"])
+    assert np.array_equal(a["F"], b["F"]) and len(a["F"]) > 0
+    assert np.abs(a["V"] - b["V"]).max() <= 1e-9 * min(sp)
